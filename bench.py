@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: world·cell-steps/s of the batched FP64 tissue step on B200 (one JSON line).
+
+Workload (the batched plain step): 4096 independent worlds per GPU, each a 16x16-grid pump-leak
+tissue (256 cells, 480 gap junctions, Na/K/Cl, GHK leaks, Na/K-ATPase, held bath), per-world
+parameters drawn from one seed; ARS(2,2,2) IMEX step in FP64 at dt = 1 ms
+(cells.solver.imex_ars222_face_electromigration@1). A bench step is one time step of every world.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torch.distributed.run, one rank per GPU, each with its own 4096 worlds (weak
+scaling; worlds never interact, so no collective is in the data path: NCCL carries only the
+timing barrier and the max over ranks). ``--impl reference`` times the reference's CPU step (the
+oracle, which reproduces it bit for bit) on the host cores instead, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "world·cell-steps/s"
+UNIT = "world·cell-steps/s"
+METHOD = "cells.solver.imex_ars222_face_electromigration@1"
+# Algorithmic bytes per world·cell·step of the plain FP64 step: the state read and written once
+# and the parameters read once per step (per cell: 2*8*(2S+4) state + 8*(4+S) parameters; per
+# junction: 2*8*(S+2) state + 8 + 8*(1+S) parameters; S = 3, 1.875 junctions per cell).
+BYTES_PER_CELL_STEP = 441.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--side", type=int, default=16)
+    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--fuse", type=int, default=1, help="time steps per kernel launch")
+    ap.add_argument("--e2e-calls", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_cell_step():
+    """DRAM bytes per world·cell·step of the step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ars222_traffic.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["dram_bytes_per_cell_step"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, flag in zip(names, r[5:9], strict=False):
+                if flag.strip().lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def build_batch(n_worlds, side, rank):
+    from cells_b200 import worlds
+
+    # Each rank its own worlds: world ids rank*n .. rank*n + n - 1 of seed 1.
+    ws = [worlds.grid_world(side, side, worlds.world_rng(1, rank * n_worlds + w))
+          for w in range(n_worlds)]
+    return worlds.pack(ws)
+
+
+def cpu_baseline(args, samples_per_core=2, steps=25):
+    """The oracle (the reference's step restated, bit-identical) over all host cores."""
+    from oracle import cpu_baseline as cb
+
+    cores = os.cpu_count() or 1
+    tasks = [("grid", w, 1, args.side, steps, args.dt) for w in range(cores * samples_per_core)]
+    cell_steps, wall, procs = cb.measure(tasks, cores)
+    return {
+        "value": cell_steps / wall,
+        "unit": UNIT,
+        "cores": procs,
+        "kind": "port",
+        "sample": (f"{len(tasks)} of the {args.worlds} worlds ({args.side}x{args.side} grid), "
+                   f"{steps} ARS(2,2,2) steps each, one world per process, 1 BLAS thread, "
+                   f"{wall:.1f} s wall"),
+    }
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    from oracle import cpu_baseline as cb
+
+    cores = os.cpu_count() or 1
+    steps = 25
+    tasks = [("grid", w, 1, args.side, steps, args.dt) for w in range(cores * 2)]
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for _ in range(max(args.warmup, 0)):
+            pool.map(cb.run_world, tasks[:cores], chunksize=1)
+        t0 = time.perf_counter()
+        done = 0
+        for _ in range(args.steps):
+            res = pool.map(cb.run_world, tasks, chunksize=1)
+            done += sum(r[0] for r in res)
+        wall = time.perf_counter() - t0
+    value = done / wall
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"batched plain step sample: {len(tasks)} worlds of "
+                               f"{args.side}x{args.side} cells x {steps} steps per bench step",
+                   "method": METHOD},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{len(tasks)} worlds x {steps} steps per bench step, "
+                                   "one world per process, 1 BLAS thread"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    # The CPU baseline pool is spawned before any CUDA call.
+    base = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(args)
+
+    import torch
+
+    from cells_b200.tissue import Tissue
+
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+
+    batch = build_batch(args.worlds, args.side, rank)
+    tissue = Tissue(batch, device=local_rank)
+    cells = batch.cells
+    fuse = max(1, args.fuse)
+    if args.steps % fuse:
+        raise SystemExit("--steps must be a multiple of --fuse")
+    state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    control = torch.from_numpy(tissue.pack_control()).to(dev)
+    status = torch.zeros(batch.worlds, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    handle = stream.cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(max(1, args.warmup // fuse)):
+        tissue.step(state, state, control, args.dt, fuse, status, stream=handle)
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(local_rank)
+    clocks.start()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = args.steps // fuse
+    start.record(stream)
+    for _ in range(launches):
+        tissue.step(state, state, control, args.dt, fuse, status, stream=handle)
+    stop.record(stream)
+    torch.cuda.synchronize(dev)
+    clock = clocks.stop()
+    ms = start.elapsed_time(stop)
+    refused = int((status != 0).sum().item())
+    barrier()
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        r = torch.tensor([refused], dtype=torch.int64, device=dev)
+        dist.all_reduce(r)
+        refused = int(r.item())
+    total_cell_steps = cells * args.steps * world_size
+    value = total_cell_steps / (ms_max * 1e-3)
+
+    # End to end through the public host entry point (cb_step_host): each call copies the packed
+    # state and controls host->device from pinned memory, takes `fuse` steps, and copies the state
+    # and status back.
+    host_state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).pin_memory()
+    host_ctl = torch.from_numpy(tissue.pack_control()).pin_memory()
+    host_out = torch.empty_like(host_state).pin_memory()
+    status_h = torch.zeros(batch.worlds, dtype=torch.int32).pin_memory()
+    taken_h = torch.zeros(batch.worlds, dtype=torch.int32).pin_memory()
+    import ctypes
+
+    from cells_b200 import _lib
+
+    def host_call():
+        _lib.check(tissue.lib.cb_step_host(
+            tissue.handle, _lib.METHOD_ARS222, ctypes.c_void_p(host_state.data_ptr()),
+            ctypes.c_void_p(host_out.data_ptr()), float(args.dt),
+            ctypes.c_void_p(host_ctl.data_ptr()), fuse, ctypes.c_void_p(status_h.data_ptr()),
+            ctypes.c_void_p(taken_h.data_ptr())))
+
+    host_call()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_calls):
+        host_call()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = cells * fuse * args.e2e_calls * world_size / e2e_s
+    h2d = (tissue.state_size + tissue.control_size) * 8 / fuse
+    d2h = (tissue.state_size * 8 + 2 * 4 * batch.worlds) / fuse
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        per_launch_s = ms * 1e-3 / launches
+        algorithmic = BYTES_PER_CELL_STEP * cells * fuse
+        achieved = algorithmic / per_launch_s / 1e9
+        traffic = traffic_per_cell_step()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded 16x16-grid pump-leak tissues)",
+            "config": {
+                "workload": (f"batched plain step: {args.worlds} worlds per GPU x "
+                             f"{args.side}x{args.side} grid tissues ({batch.cells // batch.worlds}"
+                             f" cells, {batch.edges // batch.worlds} junctions), FP64, "
+                             f"dt {args.dt:g} s"),
+                "method": METHOD, "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
+                "parallelism": f"independent worlds x{world_size} (no collective)",
+                "l2": (f"inputs larger than L2: state {tissue.state_size * 8 / 1e6:.0f} MB + "
+                       "parameters per GPU"),
+            },
+            "roofline": {
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": None if traffic is None else traffic * cells * fuse,
+                "algorithmic_bytes_per_launch": algorithmic, "launch_ms": per_launch_s * 1e3,
+            },
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps_per_call": fuse,
+                    "calls": args.e2e_calls},
+            "gpu_launches": launches,
+            "refused_worlds": refused,
+            "clocks": clock,
+        }
+        if base is not None:
+            line["cpu_baseline"] = base
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    tissue.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,137 @@
+"""ctypes binding of libcellsb200.so (the C ABI declared in include/cells_b200.h).
+
+The library is built in-tree by ``cells_b200.build`` (nvcc, sm_100a) and loaded from this
+package directory only. There is no fallback: a missing or unloadable library raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY = os.path.join(HERE, "libcellsb200.so")
+
+# include/cells_b200.h
+CB_OK = 0
+STATE_FIELDS = (
+    "amount_increment",
+    "membrane_transferred",
+    "membrane_dissipated",
+    "pump_cycles",
+    "pump_dissipated",
+    "metabolic_work",
+    "junction_transferred",
+    "junction_dissipated",
+    "junction_gate",
+    "reservoir_supplied",
+    "electrode_charge",
+    "reservoir_work",
+    "electrode_work",
+)
+CONTROL_FIELDS = ("membrane", "junction", "pump")
+METHOD_ARS222 = 0
+WORLD_BITS = {
+    1: "transport",
+    2: "pump_domain",
+    4: "gate_domain",
+    8: "control",
+    16: "residual",
+    32: "domain",
+}
+EXPORTS = (
+    "cb_bind",
+    "cb_free",
+    "cb_state_layout",
+    "cb_control_layout",
+    "cb_step",
+    "cb_step_host",
+    "cb_balances",
+    "cb_last_error",
+    "cb_version",
+)
+
+_p = ctypes.c_void_p
+_d = ctypes.POINTER(ctypes.c_double)
+_i64 = ctypes.POINTER(ctypes.c_int64)
+_i32 = ctypes.POINTER(ctypes.c_int32)
+
+
+class TissueDesc(ctypes.Structure):
+    """cb_tissue_desc (include/cells_b200.h)."""
+
+    _fields_ = [
+        ("n_worlds", ctypes.c_int32),
+        ("n_cells", ctypes.c_int64),
+        ("n_edges", ctypes.c_int64),
+        ("cell_offset", _i64),
+        ("edge_offset", _i64),
+        ("temperature", _d),
+        ("bath_amount", _d),
+        ("bath_volume", _d),
+        ("bath_potential", _d),
+        ("pump", _d),
+        ("volume", _d),
+        ("area", _d),
+        ("capacitance", _d),
+        ("permeability", _d),
+        ("pump_capacity", _d),
+        ("amount_reference", _d),
+        ("initial_charge", _d),
+        ("sender", _i32),
+        ("receiver", _i32),
+        ("junction_area", _d),
+        ("junction_permeability", _d),
+        ("gate_threshold", _d),
+        ("gate_minimum", _d),
+    ]
+
+
+class LibraryMissing(RuntimeError):
+    """The CUDA library is not built or cannot be loaded; nothing runs without it."""
+
+
+_lib = None
+
+
+def load(path=LIBRARY):
+    """Load (once) and type the library. Raises LibraryMissing if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise LibraryMissing(
+            f"{path} is not built; run `python -m cells_b200.build` (nvcc, sm_100a)"
+        )
+    try:
+        lib = ctypes.CDLL(path)
+    except OSError as error:
+        raise LibraryMissing(f"cannot load {path}: {error}") from error
+    lib.cb_bind.argtypes = [ctypes.POINTER(TissueDesc), ctypes.c_int, ctypes.POINTER(_p)]
+    lib.cb_bind.restype = ctypes.c_int
+    lib.cb_free.argtypes = [_p]
+    lib.cb_free.restype = None
+    lib.cb_state_layout.argtypes = [_p, _i64, _i64]
+    lib.cb_state_layout.restype = ctypes.c_int
+    lib.cb_control_layout.argtypes = [_p, _i64, _i64]
+    lib.cb_control_layout.restype = ctypes.c_int
+    lib.cb_step.argtypes = [_p, ctypes.c_int, _p, _p, ctypes.c_double, _p, ctypes.c_int, _p, _p,
+                            _p]
+    lib.cb_step.restype = ctypes.c_int
+    lib.cb_step_host.argtypes = [_p, ctypes.c_int, _p, _p, ctypes.c_double, _p, ctypes.c_int,
+                                 _p, _p]
+    lib.cb_step_host.restype = ctypes.c_int
+    lib.cb_balances.argtypes = [_p, _p, _p, _p]
+    lib.cb_balances.restype = ctypes.c_int
+    lib.cb_last_error.argtypes = []
+    lib.cb_last_error.restype = ctypes.c_char_p
+    lib.cb_version.argtypes = []
+    lib.cb_version.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def check(code):
+    if code != CB_OK:
+        message = _lib.cb_last_error().decode() if _lib is not None else "library not loaded"
+        raise RuntimeError(f"cells_b200 error {code}: {message}")

@@ -1,0 +1,1070 @@
+// tissue_step.cu - the B200 (sm_100a) pump-leak tissue step and its C ABI.
+//
+// One CTA advances one world. A thread owns one cell (its patch, its pump) and up to EPT
+// junctions of that world (edge-parallel). Per right-hand-side evaluation:
+//   1. cell phase: concentrations, their logs and the cell potential go to shared memory; the
+//      patch's constant-field flux and the Na/K-ATPase are evaluated in registers;
+//   2. edge phase: each junction's constant-field flux is evaluated once and stored in shared
+//      memory (species-major), its dissipation and gate rate kept in registers;
+//   3. gather phase: each cell sums its junction fluxes over its CSR adjacency in edge order
+//      (senders first, then receivers, as the reference's scatter-adds order them), so results
+//      are bit-identical run to run - no atomics anywhere.
+// World sums (the held bath's inflow, the electrode plate charge) are fixed-order block
+// reductions. State lives in registers across the n_steps of one launch; HBM sees it once in
+// and once out per launch.
+//
+// Arithmetic follows the reference expressions (Cells src/cells):
+//   laws/electrochemistry.py:25-48           bernoulli, ghk route flux
+//   laws/junctions/selective.py:28-50         selective_flux (residual 0, gate 1)
+//   laws/pumps/nak_atp_mass_action_positive.py:55-148  pump kinetics and domain
+//   laws/junctions/junction_voltage_relaxation.py:43-97 gate rate and domain
+//   numerics/surface_transport.py:298-386     route transport, scatters
+//   models/surface_pump.py:158-362            explicit_rates, imex_step (ARS(2,2,2)), ledgers
+//   numerics/surface_imex.py:47-69            the ARS(2,2,2) tableau
+// Two deliberate differences, both at the last-ulp level: the cell potential is Q/C plus the
+// bath potential (the reference reaches the same value through a diagonal Cholesky solve of the
+// scaled capacitor matrix), and the pair B(x), B(-x) comes from one expm1 (B(-x) = x + B(x),
+// taken on the side where it does not cancel).
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cells_b200.h"
+
+namespace {
+
+// Constants of laws/electrochemistry.py:11-15, formed by the same products.
+constexpr double kAvogadro = 6.02214076e23;
+constexpr double kF = kAvogadro * 1.602176634e-19;
+constexpr double kR = kAvogadro * 1.380649e-23;
+constexpr double kChargePerFmol = kF * 1e-15;
+constexpr double kMaxAbsX = 50.0;
+constexpr double kMaxAbsJunctionV = 0.120;
+constexpr double kMaxAbsIonPotentialOverRT = 1600.0;
+constexpr double kMaxAbsAffinityOverRT = 80.0;
+constexpr double kChargeAtol = 3e-25;
+constexpr double kChargeRtol = 2e-12;
+constexpr double kLog0065 = -2.7333680090865;  // log(0.065), the gate law's closing constant
+
+// Per-world constants (host-computed with the reference's expressions), stride in doubles.
+enum WorldConst {
+  WC_T = 0,
+  WC_RT,
+  WC_VB,
+  WC_CO,      // 3: bath concentrations
+  WC_LOGCO = WC_CO + 3,   // 3
+  WC_DRIVE = WC_LOGCO + 3,
+  WC_LK,      // logaddexp(0, 2 (log km_k - log k_o))
+  WC_LATP,    // logaddexp(0, log km_atp - log atp)
+  WC_LOGKMNA,
+  WC_AFF0,    // dG0/rt + log adp + log pi - log atp - log 1000 (pump domain affinity)
+  WC_RTDOM,   // rt of the pump domain predicate
+  WC_PUMPOK,  // 1 when temperature and pump parameters lie in the law's domain
+  WC_MUB,     // 3: bath mu (RT log co + z F Vb)
+  WC_STRIDE = WC_MUB + 3 + 1
+};
+
+struct Tissue {
+  int W;
+  int C;
+  int E;
+  const int *cell_offset;  // [W+1]
+  const int *edge_offset;  // [W+1]
+  const int *adj_ptr;      // [C+1], global cell -> adjacency entries
+  const int *adj_idx;      // local edge index << 1 | (1 if the cell is the receiver)
+  const double *world;     // [W * WC_STRIDE]
+  const double *vol;       // [C]
+  const double *ref;       // [3][C]
+  const double *ap;        // [3][C]  area * permeability
+  const double *cap;       // [C]
+  const double *q0;        // [C]
+  const double *pcap;      // [C]
+  const double *logpcap;   // [C] log of the pump capacity where positive, else 0
+  const int *snd;          // [E] local
+  const int *rcv;          // [E] local
+  const double *jap;       // [3][E]  junction area * permeability
+  const double *thr;       // [E]
+  const double *jmin;      // [E]
+};
+
+struct Layout {  // offsets in doubles
+  long long s[CB_STATE_FIELDS];
+  long long c[CB_CONTROL_FIELDS];
+};
+
+struct StepCoef {
+  double dt;
+  double gamma_dt;      // ARS(2,2,2) stage 1 weight times dt
+  double delta_dt;      // final weights times dt
+  double omdelta_dt;
+  double delta;         // for the applied reservoir flux
+  double omdelta;
+};
+
+__device__ __forceinline__ void bernoulli_pair(double x, double &bp, double &bm) {
+  // bp = B(x) = x/expm1(x), bm = B(-x), with the reference's series for |x| < 1e-4.
+  const double ax = fabs(x);
+  if (ax < 1e-4) {
+    const double x2 = x * x;
+    const double x4 = x2 * x2;
+    bp = ((1.0 - x / 2.0) + x2 / 12.0) - x4 / 720.0;
+    bm = ((1.0 + x / 2.0) + x2 / 12.0) - x4 / 720.0;
+  } else {
+    const double e = expm1(ax);
+    const double small = ax / e;     // B(|x|), in (0, 1)
+    const double large = ax + small; // B(-|x|) = |x| + B(|x|)
+    bp = x >= 0.0 ? small : large;
+    bm = x >= 0.0 ? large : small;
+  }
+}
+
+// numpy's logaddexp(0, y).
+__device__ __forceinline__ double logaddexp0(double y) {
+  if (y == 0.0) return 0.6931471805599453;  // 0 + ln 2
+  const double tmp = -y;
+  if (tmp > 0.0) return log1p(exp(-tmp));
+  if (tmp <= 0.0) return y + log1p(exp(tmp));
+  return tmp;  // NaN
+}
+
+__device__ __forceinline__ bool finite(double v) { return isfinite(v); }
+
+// Block-wide sum of NV values per thread, fixed tree order: xor-shuffle within warps, then the
+// warp partials in warp order. Every thread receives the totals.
+template <int BLOCK, int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *red) {
+  constexpr int WARPS = BLOCK / 32;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();  // red may still be read from a previous reduction
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) red[warp * NV + k] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = red[k];
+    for (int q = 1; q < WARPS; ++q) s += red[q * NV + k];
+    v[k] = s;
+  }
+}
+
+struct Cell {
+  double n[3];   // amount increments
+  double mt[3];  // membrane transferred
+  double md, pc, pd, mw;
+};
+
+struct Edge {
+  double jt[3];
+  double jd, g;
+};
+
+// Rates of one explicit stage (surface_pump.explicit_rates) for this thread's cell and edges.
+// n/g are the stage amounts and gates, V the stage potential of this thread's cell (sV holds
+// every cell's). Returns the cell's amount and ledger rates, the edges' rates, and the cell's
+// contribution to the bath inflow (patch flux plus pump transfer, per species).
+template <int BLOCK, int EPT>
+__device__ __forceinline__ void stage_rates(
+    const Tissue &T, const double *__restrict__ wc, int c0, int e0, int nc, int ne, int i,
+    bool has_cell, const double (&n)[3], double V, const double (&g)[EPT],
+    double mc, double pc_ctl, const double (&jc)[EPT], double *sV, double *sC, double *sL,
+    double *sJ, Cell &rate, Edge (&erate)[EPT], double (&inflow)[3], uint32_t &bits) {
+  const double RT = wc[WC_RT];
+  const double Vb = wc[WC_VB];
+  double c[3], lc[3];
+  double jm[3] = {0.0, 0.0, 0.0}, extra[3] = {0.0, 0.0, 0.0};
+  if (has_cell) {
+    const int gi = c0 + i;
+    const double vol = __ldg(T.vol + gi);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      c[s] = (__ldg(T.ref + (size_t)s * T.C + gi) + n[s]) / vol;
+      lc[s] = log(c[s]);
+      if (!(finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
+      sC[s * BLOCK + i] = c[s];
+      sL[s * BLOCK + i] = lc[s];
+    }
+    sV[i] = V;
+    if (!finite(V)) bits |= CB_WORLD_TRANSPORT;
+    // Patch: constant-field flux per species (selective_flux with residual 0, gate 1).
+    const double dv = V - Vb;
+    const double x = (kF * dv) / RT;
+    if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
+    double bp, bm;
+    bernoulli_pair(x, bp, bm);
+    double mu[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const double gs = (__ldg(T.ap + (size_t)s * T.C + gi) * mc) / 1e-15;
+      const double co = wc[WC_CO + s];
+      // Na, K: z = +1 -> (c_in B(-x) - c_out B(x)); Cl: z = -1 swaps the pair.
+      jm[s] = (s < 2) ? gs * (c[s] * bm - co * bp) : gs * (c[s] * bp - co * bm);
+      const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
+      mu[s] = RT * (lc[s] - wc[WC_LOGCO + s]) + zfdv;
+    }
+    rate.md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) rate.mt[s] = jm[s];
+    if (!(finite(jm[0]) && finite(jm[1]) && finite(jm[2]) && finite(rate.md)))
+      bits |= CB_WORLD_TRANSPORT;
+    if (!(finite(mc) && mc >= 0.0 && mc <= 1.0 && finite(pc_ctl) && pc_ctl >= 0.0 &&
+          pc_ctl <= 1.0))
+      bits |= CB_WORLD_CONTROL;
+    // Na/K-ATPase (nak_atp_mass_action_positive.kinetics), Na inside, K in the bath.
+    const double drive = wc[WC_DRIVE];
+    const double energy = (drive + (-3.0) * mu[0]) + 2.0 * mu[1];
+    const double a = energy / RT;
+    const double ls = ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
+    const double capacity = __ldg(T.pcap + gi);
+    double cycles = 0.0;
+    if (capacity > 0.0 && pc_ctl > 0.0) {
+      const double mag = exp(((__ldg(T.logpcap + gi) + log(pc_ctl)) + ls) + fmax(a, 0.0));
+      const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
+      cycles = mag * dep;
+    }
+    rate.pc = cycles;
+    rate.pd = (-1e-3 * cycles) * energy;
+    rate.mw = (-1e-3 * cycles) * drive;
+    extra[0] = 3.0 * cycles;   // -stoichiometry * cycles, outward-positive
+    extra[1] = -2.0 * cycles;
+    extra[2] = -0.0 * cycles;
+    // Pump domain (positive substrates, parameters, |mu/RT| <= 1600, |affinity| <= 80).
+    const double rtd = wc[WC_RTDOM];
+    const double sna = mu[0] / rtd, sk = mu[1] / rtd;
+    const double aff = (wc[WC_AFF0] + (-3.0) * sna) + 2.0 * sk;
+    const bool pump_ok = wc[WC_PUMPOK] != 0.0 && finite(capacity) && capacity >= 0.0 &&
+                         finite(sna) && fabs(sna) <= kMaxAbsIonPotentialOverRT && finite(sk) &&
+                         fabs(sk) <= kMaxAbsIonPotentialOverRT && finite(aff) &&
+                         fabs(aff) <= kMaxAbsAffinityOverRT;
+    if (!pump_ok) bits |= CB_WORLD_PUMP_DOMAIN;
+    if (!(finite(cycles) && finite(rate.pd) && finite(rate.mw))) bits |= CB_WORLD_TRANSPORT;
+  }
+  __syncthreads();
+  // Edge phase.
+#pragma unroll
+  for (int k = 0; k < EPT; ++k) {
+    const int e = threadIdx.x + k * BLOCK;
+    if (e < ne) {
+      const int ge = e0 + e;
+      const int s_ = __ldg(T.snd + ge), r_ = __ldg(T.rcv + ge);
+      const double dv = sV[s_] - sV[r_];
+      const double opening = jc[k] * g[k];
+      const double x = (kF * dv) / RT;
+      if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
+      double bp, bm;
+      bernoulli_pair(x, bp, bm);
+      double jj[3], mu[3];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const double gs = (__ldg(T.jap + (size_t)s * T.E + ge) * opening) / 1e-15;
+        const double cs = sC[s * BLOCK + s_], cr = sC[s * BLOCK + r_];
+        jj[s] = (s < 2) ? gs * (cs * bm - cr * bp) : gs * (cs * bp - cr * bm);
+        const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
+        mu[s] = RT * (sL[s * BLOCK + s_] - sL[s * BLOCK + r_]) + zfdv;
+        sJ[s * (EPT * BLOCK) + e] = jj[s];
+        erate[k].jt[s] = jj[s];
+      }
+      erate[k].jd = 1e-3 * ((jj[0] * mu[0] + jj[1] * mu[1]) + jj[2] * mu[2]);
+      // Junction gate (junction_voltage_relaxation.rhs); pinned gates (minimum 1) are exactly 0.
+      const double thr = __ldg(T.thr + ge), mn = __ldg(T.jmin + ge);
+      double gr = 0.0;
+      if (mn < 1.0) {
+        const double shift = fabs(dv) - thr;
+        const double alpha = 1.3 * exp(-77.0 * shift);
+        const double log_beta = kLog0065 + 140.0 * shift;
+        const double beta = 20.0 * exp(-logaddexp0(-log_beta));
+        gr = alpha * (1.0 - g[k]) - beta * (g[k] - mn);
+      }
+      erate[k].g = gr;
+      if (!(finite(jj[0]) && finite(jj[1]) && finite(jj[2]) && finite(erate[k].jd) &&
+            finite(gr)))
+        bits |= CB_WORLD_TRANSPORT;
+      const bool gate_ok = finite(thr) && thr >= 0.0 && thr <= kMaxAbsJunctionV && finite(mn) &&
+                           mn >= 0.0 && mn <= 1.0 && finite(dv) && fabs(dv) <= kMaxAbsJunctionV &&
+                           finite(g[k]) && g[k] >= mn && g[k] <= 1.0 && finite(jc[k]) &&
+                           jc[k] >= 0.0 && jc[k] <= 1.0;
+      if (!gate_ok) bits |= CB_WORLD_GATE_DOMAIN;
+    }
+  }
+  __syncthreads();
+  // Gather phase: cell rate = ((-J_m + sum_send(-J)) + sum_recv(J)) - extra.
+  if (has_cell) {
+    const int gi = c0 + i;
+    double send[3] = {0.0, 0.0, 0.0}, recv[3] = {0.0, 0.0, 0.0};
+    const int a0 = __ldg(T.adj_ptr + gi), a1 = __ldg(T.adj_ptr + gi + 1);
+    for (int a = a0; a < a1; ++a) {
+      const int code = __ldg(T.adj_idx + a);
+      const int e = code >> 1;
+      if (code & 1) {
+#pragma unroll
+        for (int s = 0; s < 3; ++s) recv[s] += sJ[s * (EPT * BLOCK) + e];
+      } else {
+#pragma unroll
+        for (int s = 0; s < 3; ++s) send[s] += -sJ[s * (EPT * BLOCK) + e];
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      rate.n[s] = ((-jm[s] + send[s]) + recv[s]) - extra[s];
+      inflow[s] = jm[s] + extra[s];
+      if (!finite(rate.n[s])) bits |= CB_WORLD_TRANSPORT;
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) inflow[s] = 0.0;
+  }
+}
+
+template <int BLOCK, int EPT>
+__global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
+    ars222_kernel(const Tissue T, const Layout L, const double *state_in, double *state_out,
+                  const double *__restrict__ control,
+                  const StepCoef k, int n_steps, uint32_t *__restrict__ world_status,
+                  int32_t *__restrict__ accepted_steps) {
+  extern __shared__ double smem[];
+  double *sV = smem;                   // [BLOCK]
+  double *sC = sV + BLOCK;             // [3][BLOCK]
+  double *sL = sC + 3 * BLOCK;         // [3][BLOCK]
+  double *sJ = sL + 3 * BLOCK;         // [3][EPT*BLOCK]
+  double *sRed = sJ + 3 * EPT * BLOCK; // [BLOCK/32][8]
+  __shared__ double sW[WC_STRIDE];
+  __shared__ unsigned int sBits;
+
+  const int w = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int c0 = T.cell_offset[w], nc = T.cell_offset[w + 1] - c0;
+  const int e0 = T.edge_offset[w], ne = T.edge_offset[w + 1] - e0;
+  if (tid < WC_STRIDE) sW[tid] = T.world[(size_t)w * WC_STRIDE + tid];
+  if (tid == 0) sBits = 0u;
+  const bool has_cell = tid < nc;
+  const int i = tid;
+  const int gi = c0 + i;
+
+  // Load the world's state into registers.
+  Cell y;
+  double mc = 0.0, pctl = 0.0, cap = 1.0, q0 = 0.0;
+  if (has_cell) {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      y.n[s] = state_in[L.s[CB_AMOUNT_INCREMENT] + (long long)s * T.C + gi];
+      y.mt[s] = state_in[L.s[CB_MEMBRANE_TRANSFERRED] + (long long)s * T.C + gi];
+    }
+    y.md = state_in[L.s[CB_MEMBRANE_DISSIPATED] + gi];
+    y.pc = state_in[L.s[CB_PUMP_CYCLES] + gi];
+    y.pd = state_in[L.s[CB_PUMP_DISSIPATED] + gi];
+    y.mw = state_in[L.s[CB_METABOLIC_WORK] + gi];
+    mc = control[L.c[CB_CONTROL_MEMBRANE] + gi];
+    pctl = control[L.c[CB_CONTROL_PUMP] + gi];
+    cap = __ldg(T.cap + gi);
+    q0 = __ldg(T.q0 + gi);
+  } else {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) y.n[s] = y.mt[s] = 0.0;
+    y.md = y.pc = y.pd = y.mw = 0.0;
+  }
+  Edge ye[EPT];
+  double jc[EPT];
+#pragma unroll
+  for (int q = 0; q < EPT; ++q) {
+    const int e = tid + q * BLOCK;
+    if (e < ne) {
+      const int ge = e0 + e;
+#pragma unroll
+      for (int s = 0; s < 3; ++s)
+        ye[q].jt[s] = state_in[L.s[CB_JUNCTION_TRANSFERRED] + (long long)s * T.E + ge];
+      ye[q].jd = state_in[L.s[CB_JUNCTION_DISSIPATED] + ge];
+      ye[q].g = state_in[L.s[CB_JUNCTION_GATE] + ge];
+      jc[q] = control[L.c[CB_CONTROL_JUNCTION] + ge];
+    } else {
+#pragma unroll
+      for (int s = 0; s < 3; ++s) ye[q].jt[s] = 0.0;
+      ye[q].jd = 0.0;
+      ye[q].g = 1.0;
+      jc[q] = 0.0;
+    }
+  }
+  double res[3];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) res[s] = state_in[L.s[CB_RESERVOIR_SUPPLIED] + (long long)s * T.W + w];
+  double ec = state_in[L.s[CB_ELECTRODE_CHARGE] + w];
+  double rw = state_in[L.s[CB_RESERVOIR_WORK] + w];
+  double ew = state_in[L.s[CB_ELECTRODE_WORK] + w];
+  __syncthreads();
+  const double Vb = sW[WC_VB];
+
+  // Bath plate charge of the charge-only increment (surface_tissue.capacitor_change): sum over
+  // the world's cells of -C_i dp_i, dp_i = q_i / C_i.
+  auto plate = [&](const double (&n)[3]) -> double {
+    if (!has_cell) return 0.0;
+    const double q = kChargePerFmol * ((n[0] + n[1]) + (-n[2]));
+    return -cap * (q / cap);
+  };
+  double plate0;
+  {
+    double v[1] = {plate(y.n)};
+    block_sum<BLOCK, 1>(v, sRed);
+    plate0 = v[0];
+  }
+
+  int taken = 0;
+  uint32_t refused = 0u;
+  for (int step = 0; step < n_steps; ++step) {
+    uint32_t bits = 0u;
+    // Stage 0: start potential from the capacitor solve, Q / C plus the bath potential.
+    const double Q0 = q0 + kChargePerFmol * ((y.n[0] + y.n[1]) + (-y.n[2]));
+    const double V0 = Q0 / cap + Vb;
+    Cell k0;
+    Edge k0e[EPT];
+    double in0[3];
+    double g0[EPT];
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) g0[q] = ye[q].g;
+    stage_rates<BLOCK, EPT>(T, sW, c0, e0, nc, ne, i, has_cell, y.n, V0, g0, mc, pctl, jc, sV,
+                            sC, sL, sJ, k0, k0e, in0, bits);
+    // Stage 1 state (only amounts and gates feed the next rates) and the final accumulator.
+    double n1[3], g1[EPT];
+    Cell acc;
+    Edge acce[EPT];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      n1[s] = y.n[s] + k.gamma_dt * k0.n[s];
+      acc.n[s] = y.n[s] + k.delta_dt * k0.n[s];
+      acc.mt[s] = y.mt[s] + k.delta_dt * k0.mt[s];
+    }
+    acc.md = y.md + k.delta_dt * k0.md;
+    acc.pc = y.pc + k.delta_dt * k0.pc;
+    acc.pd = y.pd + k.delta_dt * k0.pd;
+    acc.mw = y.mw + k.delta_dt * k0.mw;
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+      g1[q] = ye[q].g + k.gamma_dt * k0e[q].g;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) acce[q].jt[s] = ye[q].jt[s] + k.delta_dt * k0e[q].jt[s];
+      acce[q].jd = ye[q].jd + k.delta_dt * k0e[q].jd;
+      acce[q].g = ye[q].g + k.delta_dt * k0e[q].g;
+    }
+    // Stage 1 potential: the IMEX operator (capacitor only, no faces) solve.
+    const double Q1 = q0 + kChargePerFmol * ((n1[0] + n1[1]) + (-n1[2]));
+    const double V1 = Q1 / cap + Vb;
+    if (has_cell) {
+      const double image = cap * (V1 - Vb);
+      const double scale = fmax(fabs(Q1), fabs(image));
+      if (!(finite(V1) && fabs(image - Q1) <= kChargeAtol + kChargeRtol * scale))
+        bits |= CB_WORLD_RESIDUAL;
+    }
+    Cell k1;
+    Edge k1e[EPT];
+    double in1[3];
+    stage_rates<BLOCK, EPT>(T, sW, c0, e0, nc, ne, i, has_cell, n1, V1, g1, mc, pctl, jc, sV,
+                            sC, sL, sJ, k1, k1e, in1, bits);
+    Cell y2;
+    Edge y2e[EPT];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      y2.n[s] = acc.n[s] + k.omdelta_dt * k1.n[s];
+      y2.mt[s] = acc.mt[s] + k.omdelta_dt * k1.mt[s];
+    }
+    y2.md = acc.md + k.omdelta_dt * k1.md;
+    y2.pc = acc.pc + k.omdelta_dt * k1.pc;
+    y2.pd = acc.pd + k.omdelta_dt * k1.pd;
+    y2.mw = acc.mw + k.omdelta_dt * k1.mw;
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+#pragma unroll
+      for (int s = 0; s < 3; ++s) y2e[q].jt[s] = acce[q].jt[s] + k.omdelta_dt * k1e[q].jt[s];
+      y2e[q].jd = acce[q].jd + k.omdelta_dt * k1e[q].jd;
+      y2e[q].g = acce[q].g + k.omdelta_dt * k1e[q].g;
+    }
+    // The last stage's potential solve (its residual is part of the step's acceptance).
+    if (has_cell) {
+      const double Q2 = q0 + kChargePerFmol * ((y2.n[0] + y2.n[1]) + (-y2.n[2]));
+      const double V2 = Q2 / cap + Vb;
+      const double image = cap * (V2 - Vb);
+      const double scale = fmax(fabs(Q2), fabs(image));
+      if (!(finite(V2) && fabs(image - Q2) <= kChargeAtol + kChargeRtol * scale))
+        bits |= CB_WORLD_RESIDUAL;
+      // Accepted-state domain: positive finite amounts and finite ledgers.
+      bool ok = true;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const double amt = __ldg(T.ref + (size_t)s * T.C + gi) + y2.n[s];
+        ok = ok && finite(amt) && amt > 0.0 && finite(y2.mt[s]);
+      }
+      ok = ok && finite(y2.md) && finite(y2.pc) && finite(y2.pd) && finite(y2.mw);
+      if (!ok) bits |= CB_WORLD_DOMAIN;
+    }
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+      const int e = tid + q * BLOCK;
+      if (e < ne) {
+        const double mn = __ldg(T.jmin + e0 + e);
+        const bool ok = finite(y2e[q].jt[0]) && finite(y2e[q].jt[1]) && finite(y2e[q].jt[2]) &&
+                        finite(y2e[q].jd) && finite(y2e[q].g) && y2e[q].g >= mn &&
+                        y2e[q].g <= 1.0;
+        if (!ok) bits |= CB_WORLD_DOMAIN;
+      }
+    }
+    // World sums: bath inflow of both stages and the end plate charge.
+    double v[7] = {in0[0], in0[1], in0[2], in1[0], in1[1], in1[2], plate(y2.n)};
+    block_sum<BLOCK, 7>(v, sRed);
+    double res2[3], applied[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const double k0r = -v[s], k1r = -v[3 + s];
+      res2[s] = (res[s] + k.delta_dt * k0r) + k.omdelta_dt * k1r;
+      applied[s] = k.delta * k0r + k.omdelta * k1r;
+    }
+    const double electrode = v[6] - plate0;
+    const double ec2 = ec + electrode;
+    const double rw2 =
+        rw + 1e-3 * ((sW[WC_MUB] * (k.dt * applied[0]) + sW[WC_MUB + 1] * (k.dt * applied[1])) +
+                     sW[WC_MUB + 2] * (k.dt * applied[2]));
+    const double ew2 = ew + (1e12 * Vb) * electrode;
+    if (!(finite(res2[0]) && finite(res2[1]) && finite(res2[2]) && finite(ec2) && finite(rw2) &&
+          finite(ew2)))
+      bits |= CB_WORLD_DOMAIN;
+    // The step is accepted or refused for the whole world.
+    if (bits) atomicOr(&sBits, bits);
+    __syncthreads();
+    const uint32_t world_bits = sBits;
+    __syncthreads();
+    if (world_bits) {
+      refused = world_bits;
+      break;
+    }
+    y = y2;
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) ye[q] = y2e[q];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) res[s] = res2[s];
+    ec = ec2;
+    rw = rw2;
+    ew = ew2;
+    plate0 = v[6];
+    ++taken;
+  }
+
+  // Store the world's state.
+  if (has_cell) {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      state_out[L.s[CB_AMOUNT_INCREMENT] + (long long)s * T.C + gi] = y.n[s];
+      state_out[L.s[CB_MEMBRANE_TRANSFERRED] + (long long)s * T.C + gi] = y.mt[s];
+    }
+    state_out[L.s[CB_MEMBRANE_DISSIPATED] + gi] = y.md;
+    state_out[L.s[CB_PUMP_CYCLES] + gi] = y.pc;
+    state_out[L.s[CB_PUMP_DISSIPATED] + gi] = y.pd;
+    state_out[L.s[CB_METABOLIC_WORK] + gi] = y.mw;
+  }
+#pragma unroll
+  for (int q = 0; q < EPT; ++q) {
+    const int e = tid + q * BLOCK;
+    if (e < ne) {
+      const int ge = e0 + e;
+#pragma unroll
+      for (int s = 0; s < 3; ++s)
+        state_out[L.s[CB_JUNCTION_TRANSFERRED] + (long long)s * T.E + ge] = ye[q].jt[s];
+      state_out[L.s[CB_JUNCTION_DISSIPATED] + ge] = ye[q].jd;
+      state_out[L.s[CB_JUNCTION_GATE] + ge] = ye[q].g;
+    }
+  }
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) state_out[L.s[CB_RESERVOIR_SUPPLIED] + (long long)s * T.W + w] = res[s];
+    state_out[L.s[CB_ELECTRODE_CHARGE] + w] = ec;
+    state_out[L.s[CB_RESERVOIR_WORK] + w] = rw;
+    state_out[L.s[CB_ELECTRODE_WORK] + w] = ew;
+    world_status[w] = refused;
+    if (accepted_steps) accepted_steps[w] = taken;
+  }
+}
+
+// Ledger residuals per world (the reference's balances(), held-bath worlds).
+template <int BLOCK, int EPT>
+__global__ void __launch_bounds__(BLOCK) balances_kernel(const Tissue T, const Layout L,
+                                                         const double *__restrict__ st,
+                                                         double *__restrict__ out) {
+  extern __shared__ double smem[];
+  double *sJ = smem;                    // [3][EPT*BLOCK]
+  double *sRed = sJ + 3 * EPT * BLOCK;  // [BLOCK/32][8]
+  __shared__ double sW[WC_STRIDE];
+  const int w = blockIdx.x, tid = threadIdx.x;
+  const int c0 = T.cell_offset[w], nc = T.cell_offset[w + 1] - c0;
+  const int e0 = T.edge_offset[w], ne = T.edge_offset[w + 1] - e0;
+  if (tid < WC_STRIDE) sW[tid] = T.world[(size_t)w * WC_STRIDE + tid];
+  for (int q = 0; q < EPT; ++q) {
+    const int e = tid + q * BLOCK;
+    if (e < ne)
+      for (int s = 0; s < 3; ++s)
+        sJ[s * EPT * BLOCK + e] = st[L.s[CB_JUNCTION_TRANSFERRED] + (long long)s * T.E + e0 + e];
+  }
+  __syncthreads();
+  double local = 0.0, metabolic = 0.0, moved[3] = {0, 0, 0}, di[3] = {0, 0, 0}, pl = 0.0;
+  if (tid < nc) {
+    const int gi = c0 + tid;
+    const double stoich[3] = {-3.0, 2.0, 0.0};
+    const double pc = st[L.s[CB_PUMP_CYCLES] + gi];
+    double send[3] = {0, 0, 0}, recv[3] = {0, 0, 0};
+    for (int a = T.adj_ptr[gi]; a < T.adj_ptr[gi + 1]; ++a) {
+      const int code = T.adj_idx[a], e = code >> 1;
+      for (int s = 0; s < 3; ++s) {
+        if (code & 1) recv[s] += sJ[s * EPT * BLOCK + e];
+        else send[s] += sJ[s * EPT * BLOCK + e];
+      }
+    }
+    double n[3];
+    for (int s = 0; s < 3; ++s) {
+      n[s] = st[L.s[CB_AMOUNT_INCREMENT] + (long long)s * T.C + gi];
+      const double total_m = st[L.s[CB_MEMBRANE_TRANSFERRED] + (long long)s * T.C + gi] -
+                             stoich[s] * pc;
+      local = fmax(local, fabs(((n[s] + total_m) + send[s]) - recv[s]));
+      moved[s] = total_m;
+      di[s] = n[s];
+    }
+    metabolic = fabs(st[L.s[CB_METABOLIC_WORK] + gi] + 1e-3 * sW[WC_DRIVE] * pc);
+    const double cap = T.cap[gi];
+    const double q = kChargePerFmol * ((n[0] + n[1]) + (-n[2]));
+    pl = -cap * (q / cap);
+  }
+  double v[7] = {moved[0], moved[1], moved[2], di[0], di[1], di[2], pl};
+  block_sum<BLOCK, 7>(v, sRed);
+  double mx[2] = {local, metabolic};
+  // max-reduce through shared memory (fixed order)
+  __syncthreads();
+  for (int k2 = 0; k2 < 2; ++k2) {
+    double m = mx[k2];
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    mx[k2] = m;
+  }
+  if ((tid & 31) == 0) {
+    sRed[(tid >> 5) * 8 + 0] = mx[0];
+    sRed[(tid >> 5) * 8 + 1] = mx[1];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double ml = 0.0, mm = 0.0;
+    for (int q = 0; q < BLOCK / 32; ++q) {
+      ml = fmax(ml, sRed[q * 8]);
+      mm = fmax(mm, sRed[q * 8 + 1]);
+    }
+    double outside = 0.0, total = 0.0, supply_charge_terms[3];
+    for (int s = 0; s < 3; ++s) {
+      const double sup = st[L.s[CB_RESERVOIR_SUPPLIED] + (long long)s * T.W + w];
+      outside = fmax(outside, fabs(-v[s] - sup));
+      total = fmax(total, fabs(v[3 + s] - sup));
+      supply_charge_terms[s] = sup;
+    }
+    const double ec = st[L.s[CB_ELECTRODE_CHARGE] + w];
+    const double rw = st[L.s[CB_RESERVOIR_WORK] + w];
+    const double ew = st[L.s[CB_ELECTRODE_WORK] + w];
+    const double supply_charge =
+        kChargePerFmol * ((supply_charge_terms[0] + supply_charge_terms[1]) - supply_charge_terms[2]);
+    const double Vb = sW[WC_VB];
+    double* o = out + (size_t)w * 8;
+    o[0] = ml;
+    o[1] = outside;
+    o[2] = total;
+    o[3] = fabs(ec - v[6]);
+    o[4] = fabs(ec + supply_charge);
+    o[5] = fabs(rw - 1e-3 * ((sW[WC_MUB] * supply_charge_terms[0] + sW[WC_MUB + 1] * supply_charge_terms[1]) +
+                             sW[WC_MUB + 2] * supply_charge_terms[2]));
+    o[6] = fabs(ew - 1e12 * Vb * ec);
+    o[7] = mm;
+  }
+}
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  g_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return CB_ERR_CUDA;
+}
+
+// numpy's logaddexp(0, y) on the host (libm), for the per-world pump constants.
+double host_logaddexp0(double y) {
+  if (y == 0.0) return 0.6931471805599453;
+  const double tmp = -y;
+  if (tmp > 0.0) return std::log1p(std::exp(-tmp));
+  if (tmp <= 0.0) return y + std::log1p(std::exp(tmp));
+  return tmp;
+}
+
+long long pad32(long long n) { return (n + 31) / 32 * 32; }
+
+}  // namespace
+
+struct cb_tissue {
+  int device = 0;
+  int W = 0, C = 0, E = 0;
+  int block = 0, ept = 0;
+  Tissue t{};
+  Layout layout{};
+  long long state_total = 0, control_total = 0;
+  std::vector<void *> owned;  // device allocations
+  // Buffers of the host-pointer entry point, allocated on first use.
+  double *h_state = nullptr, *h_control = nullptr;
+  uint32_t *h_status = nullptr;
+  int32_t *h_taken = nullptr;
+};
+
+namespace {
+
+template <typename T>
+int upload(cb_tissue *t, const std::vector<T> &host, const T **dst) {
+  void *p = nullptr;
+  size_t bytes = std::max<size_t>(host.size() * sizeof(T), 16);
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+  t->owned.push_back(p);
+  if (!host.empty()) {
+    e = cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy");
+  }
+  *dst = static_cast<const T *>(p);
+  return CB_OK;
+}
+
+size_t step_smem(int block, int ept) {
+  return sizeof(double) * (size_t)(7 * block + 3 * ept * block + (block / 32) * 8);
+}
+
+size_t balances_smem(int block, int ept) {
+  return sizeof(double) * (size_t)(3 * ept * block + (block / 32) * 8);
+}
+
+template <int BLOCK, int EPT>
+int launch_step(cb_tissue *t, const double *in, double *out, const double *control,
+                const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
+                cudaStream_t stream) {
+  const size_t smem = step_smem(BLOCK, EPT);
+  auto kern = ars222_kernel<BLOCK, EPT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  kern<<<t->W, BLOCK, smem, stream>>>(t->t, t->layout, in, out, control, k, n_steps, status,
+                                      taken);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "ars222 launch");
+  return CB_OK;
+}
+
+template <int BLOCK, int EPT>
+int launch_balances(cb_tissue *t, const double *st, double *out, cudaStream_t stream) {
+  const size_t smem = balances_smem(BLOCK, EPT);
+  auto kern = balances_kernel<BLOCK, EPT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  kern<<<t->W, BLOCK, smem, stream>>>(t->t, t->layout, st, out);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "balances launch");
+  return CB_OK;
+}
+
+#define CB_DISPATCH(FN, ...)                                                     \
+  switch (t->block * 10 + t->ept) {                                              \
+    case 1281: return FN<128, 1>(t, __VA_ARGS__);                                \
+    case 1282: return FN<128, 2>(t, __VA_ARGS__);                                \
+    case 1283: return FN<128, 3>(t, __VA_ARGS__);                                \
+    case 1284: return FN<128, 4>(t, __VA_ARGS__);                                \
+    case 2561: return FN<256, 1>(t, __VA_ARGS__);                                \
+    case 2562: return FN<256, 2>(t, __VA_ARGS__);                                \
+    case 2563: return FN<256, 3>(t, __VA_ARGS__);                                \
+    case 2564: return FN<256, 4>(t, __VA_ARGS__);                                \
+    case 5121: return FN<512, 1>(t, __VA_ARGS__);                                \
+    case 5122: return FN<512, 2>(t, __VA_ARGS__);                                \
+    case 5123: return FN<512, 3>(t, __VA_ARGS__);                                \
+    case 5124: return FN<512, 4>(t, __VA_ARGS__);                                \
+    case 10241: return FN<1024, 1>(t, __VA_ARGS__);                              \
+    case 10242: return FN<1024, 2>(t, __VA_ARGS__);                              \
+    case 10243: return FN<1024, 3>(t, __VA_ARGS__);                              \
+    case 10244: return FN<1024, 4>(t, __VA_ARGS__);                              \
+    default: return fail(CB_ERR_UNSUPPORTED, "no kernel for this block/edge shape"); \
+  }
+
+}  // namespace
+
+extern "C" {
+
+const char *cb_last_error(void) { return g_error.c_str(); }
+
+const char *cb_version(void) { return "cells_b200 0.1 (sm_100a, fp64 ARS(2,2,2))"; }
+
+int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
+  if (!d || !out) return fail(CB_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  const int W = d->n_worlds;
+  const long long C = d->n_cells, E = d->n_edges;
+  if (W <= 0 || C <= 0 || E < 0 || C > (1LL << 30) || E > (1LL << 30))
+    return fail(CB_ERR_LAYOUT, "world, cell or junction count out of range");
+  if (!d->cell_offset || !d->edge_offset || !d->temperature || !d->bath_amount ||
+      !d->bath_volume || !d->bath_potential || !d->pump || !d->volume || !d->area ||
+      !d->capacitance || !d->permeability || !d->pump_capacity || !d->amount_reference ||
+      !d->initial_charge || (E > 0 && (!d->sender || !d->receiver || !d->junction_area ||
+                                       !d->junction_permeability || !d->gate_threshold ||
+                                       !d->gate_minimum)))
+    return fail(CB_ERR_ARGUMENT, "null array in the tissue description");
+  if (d->cell_offset[0] != 0 || d->edge_offset[0] != 0 || d->cell_offset[W] != C ||
+      d->edge_offset[W] != E)
+    return fail(CB_ERR_LAYOUT, "offsets must run from 0 to the totals");
+  int max_cells = 0;
+  long long max_edges = 0;
+  for (int w = 0; w < W; ++w) {
+    const long long nc = d->cell_offset[w + 1] - d->cell_offset[w];
+    const long long ne = d->edge_offset[w + 1] - d->edge_offset[w];
+    if (nc < 1) return fail(CB_ERR_LAYOUT, "every world needs at least one cell");
+    if (ne < 0) return fail(CB_ERR_LAYOUT, "junction offsets must not decrease");
+    if (nc > 1024) return fail(CB_ERR_UNSUPPORTED, "worlds of more than 1024 cells");
+    max_cells = std::max<int>(max_cells, (int)nc);
+    max_edges = std::max(max_edges, ne);
+  }
+  int block = 128;
+  while (block < max_cells) block *= 2;
+  const int ept = (int)std::max<long long>(1, (max_edges + block - 1) / block);
+  if (ept > 4) return fail(CB_ERR_UNSUPPORTED, "more than 4 junctions per thread");
+  // Adjacency (senders first, then receivers, each in edge order) and route checks.
+  std::vector<int> adj_ptr(C + 1, 0), adj_idx;
+  std::vector<std::vector<int>> out_e(C), in_e(C);
+  for (int w = 0; w < W; ++w) {
+    const long long c0 = d->cell_offset[w], nc = d->cell_offset[w + 1] - c0;
+    for (long long e = d->edge_offset[w]; e < d->edge_offset[w + 1]; ++e) {
+      const int s = d->sender[e], r = d->receiver[e];
+      if (s < 0 || r < 0 || s >= nc || r >= nc || s == r)
+        return fail(CB_ERR_LAYOUT, "junction endpoint out of its world or a self junction");
+      const int local = (int)(e - d->edge_offset[w]);
+      out_e[c0 + s].push_back(local << 1);
+      in_e[c0 + r].push_back((local << 1) | 1);
+    }
+  }
+  adj_idx.reserve(2 * E);
+  for (long long c = 0; c < C; ++c) {
+    for (int v : out_e[c]) adj_idx.push_back(v);
+    for (int v : in_e[c]) adj_idx.push_back(v);
+    adj_ptr[c + 1] = (int)adj_idx.size();
+  }
+  for (long long c = 0; c < C; ++c) {
+    if (!(d->volume[c] > 0) || !(d->capacitance[c] > 0) || !(d->area[c] > 0) ||
+        !std::isfinite(d->initial_charge[c]))
+      return fail(CB_ERR_LAYOUT, "cell volume, area and capacitance must be positive");
+  }
+  // Per-world constants with the reference's expressions.
+  const double ln1000 = std::log(1000.0);
+  std::vector<double> world((size_t)W * WC_STRIDE, 0.0);
+  for (int w = 0; w < W; ++w) {
+    double *c = world.data() + (size_t)w * WC_STRIDE;
+    const double T = d->temperature[w];
+    const double RT = kR * T;
+    const double vb = d->bath_potential[w], bv = d->bath_volume[w];
+    if (!(bv > 0)) return fail(CB_ERR_LAYOUT, "bath volume must be positive");
+    c[WC_T] = T;
+    c[WC_RT] = RT;
+    c[WC_VB] = vb;
+    const double z[3] = {1.0, 1.0, -1.0};
+    for (int s = 0; s < 3; ++s) {
+      const double co = d->bath_amount[(size_t)s * W + w] / bv;
+      if (!(co > 0) || !std::isfinite(co)) return fail(CB_ERR_LAYOUT, "bath must be positive");
+      c[WC_CO + s] = co;
+      c[WC_LOGCO + s] = std::log(co);
+      c[WC_MUB + s] = RT * std::log(co) + z[s] * kF * vb;
+    }
+    const double atp = d->pump[0 * W + w], adp = d->pump[1 * W + w], pi = d->pump[2 * W + w];
+    const double km_na = d->pump[3 * W + w], km_k = d->pump[4 * W + w];
+    const double km_atp = d->pump[5 * W + w], dg0 = d->pump[6 * W + w];
+    c[WC_DRIVE] = dg0 + RT * (((std::log(adp) + std::log(pi)) - std::log(atp)) - ln1000);
+    c[WC_LK] = host_logaddexp0(2.0 * (std::log(km_k) - std::log(c[WC_CO + 1])));
+    c[WC_LATP] = host_logaddexp0(std::log(km_atp) - std::log(atp));
+    c[WC_LOGKMNA] = std::log(km_na);
+    const bool t_ok = std::isfinite(T) && T >= 200.0 && T <= 400.0;
+    const double rtd = kR * (t_ok ? T : 298.15);
+    bool ok = t_ok;
+    for (double v : {atp, adp, pi, km_na, km_k, km_atp}) ok = ok && std::isfinite(v) && v > 0;
+    ok = ok && std::isfinite(dg0);
+    const double s_atp = ok ? atp : 1.0, s_adp = ok ? adp : 1.0, s_pi = ok ? pi : 1.0;
+    c[WC_AFF0] = (((dg0 / rtd + std::log(s_adp)) + std::log(s_pi)) - std::log(s_atp)) - ln1000;
+    c[WC_RTDOM] = rtd;
+    c[WC_PUMPOK] = ok ? 1.0 : 0.0;
+  }
+  std::vector<double> ap(3 * C), jap(3 * E), logpcap(C);
+  for (int s = 0; s < 3; ++s) {
+    for (long long c = 0; c < C; ++c)
+      ap[s * C + c] = d->area[c] * d->permeability[s * C + c];
+    for (long long e = 0; e < E; ++e)
+      jap[s * E + e] = d->junction_area[e] * d->junction_permeability[s * E + e];
+  }
+  for (long long c = 0; c < C; ++c)
+    logpcap[c] = d->pump_capacity[c] > 0 ? std::log(d->pump_capacity[c]) : 0.0;
+
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  cb_tissue *t = new cb_tissue();
+  t->device = device;
+  t->W = W;
+  t->C = (int)C;
+  t->E = (int)E;
+  t->block = block;
+  t->ept = ept;
+  std::vector<int> co32(W + 1), eo32(W + 1), snd(E), rcv(E);
+  for (int w = 0; w <= W; ++w) {
+    co32[w] = (int)d->cell_offset[w];
+    eo32[w] = (int)d->edge_offset[w];
+  }
+  for (long long e = 0; e < E; ++e) {
+    snd[e] = d->sender[e];
+    rcv[e] = d->receiver[e];
+  }
+  auto vec = [](const double *p, long long n) { return std::vector<double>(p, p + n); };
+  int rc = CB_OK;
+  Tissue &T = t->t;
+  T.W = W;
+  T.C = (int)C;
+  T.E = (int)E;
+  if (!rc) rc = upload(t, co32, &T.cell_offset);
+  if (!rc) rc = upload(t, eo32, &T.edge_offset);
+  if (!rc) rc = upload(t, adj_ptr, &T.adj_ptr);
+  if (!rc) rc = upload(t, adj_idx, &T.adj_idx);
+  if (!rc) rc = upload(t, world, &T.world);
+  if (!rc) rc = upload(t, vec(d->volume, C), &T.vol);
+  if (!rc) rc = upload(t, vec(d->amount_reference, 3 * C), &T.ref);
+  if (!rc) rc = upload(t, ap, &T.ap);
+  if (!rc) rc = upload(t, vec(d->capacitance, C), &T.cap);
+  if (!rc) rc = upload(t, vec(d->initial_charge, C), &T.q0);
+  if (!rc) rc = upload(t, vec(d->pump_capacity, C), &T.pcap);
+  if (!rc) rc = upload(t, logpcap, &T.logpcap);
+  if (!rc) rc = upload(t, snd, &T.snd);
+  if (!rc) rc = upload(t, rcv, &T.rcv);
+  if (!rc) rc = upload(t, jap, &T.jap);
+  if (!rc) rc = upload(t, E ? vec(d->gate_threshold, E) : std::vector<double>(), &T.thr);
+  if (!rc) rc = upload(t, E ? vec(d->gate_minimum, E) : std::vector<double>(), &T.jmin);
+  if (rc) {
+    cb_free(t);
+    return rc;
+  }
+  // Packed state and control layouts: each field padded to 32 doubles (256-byte aligned).
+  const long long sizes[CB_STATE_FIELDS] = {3 * C, 3 * C, C, C, C, C, 3 * E, E, E, 3 * (long long)W,
+                                            W, W, W};
+  long long off = 0;
+  for (int f = 0; f < CB_STATE_FIELDS; ++f) {
+    t->layout.s[f] = off;
+    off += pad32(sizes[f]);
+  }
+  t->state_total = off;
+  const long long csz[CB_CONTROL_FIELDS] = {C, E, C};
+  off = 0;
+  for (int f = 0; f < CB_CONTROL_FIELDS; ++f) {
+    t->layout.c[f] = off;
+    off += pad32(csz[f]);
+  }
+  t->control_total = off;
+  *out = t;
+  return CB_OK;
+}
+
+void cb_free(cb_tissue *t) {
+  if (!t) return;
+  cudaSetDevice(t->device);
+  for (void *p : t->owned) cudaFree(p);
+  if (t->h_state) cudaFree(t->h_state);
+  if (t->h_control) cudaFree(t->h_control);
+  if (t->h_status) cudaFree(t->h_status);
+  if (t->h_taken) cudaFree(t->h_taken);
+  delete t;
+}
+
+int cb_state_layout(const cb_tissue *t, int64_t offsets[CB_STATE_FIELDS], int64_t *total) {
+  if (!t || !offsets || !total) return fail(CB_ERR_ARGUMENT, "null argument");
+  for (int f = 0; f < CB_STATE_FIELDS; ++f) offsets[f] = t->layout.s[f];
+  *total = t->state_total;
+  return CB_OK;
+}
+
+int cb_control_layout(const cb_tissue *t, int64_t offsets[CB_CONTROL_FIELDS], int64_t *total) {
+  if (!t || !offsets || !total) return fail(CB_ERR_ARGUMENT, "null argument");
+  for (int f = 0; f < CB_CONTROL_FIELDS; ++f) offsets[f] = t->layout.c[f];
+  *total = t->control_total;
+  return CB_OK;
+}
+
+int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out, double dt,
+            const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
+            void *stream) {
+  if (!t || !state_in || !state_out || !control || !world_status)
+    return fail(CB_ERR_ARGUMENT, "null argument");
+  if (method != CB_METHOD_ARS222) return fail(CB_ERR_UNSUPPORTED, "unknown step method");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
+  if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  // ARS(2,2,2) (numerics/surface_imex.py:47-48, :63-66).
+  const double gamma = 1.0 - 1.0 / std::sqrt(2.0);
+  const double delta = 1.0 - 1.0 / (2.0 * gamma);
+  StepCoef k;
+  k.dt = dt;
+  k.gamma_dt = gamma * dt;
+  k.delta_dt = delta * dt;
+  k.omdelta_dt = (1.0 - delta) * dt;
+  k.delta = delta;
+  k.omdelta = 1.0 - delta;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CB_DISPATCH(launch_step, state_in, state_out, control, k, n_steps, world_status,
+              accepted_steps, s);
+}
+
+int cb_step_host(cb_tissue *t, int method, const double *state_in, double *state_out, double dt,
+                 const double *control, int n_steps, uint32_t *world_status,
+                 int32_t *accepted_steps) {
+  if (!t || !state_in || !state_out || !control || !world_status)
+    return fail(CB_ERR_ARGUMENT, "null argument");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  if (!t->h_state) {
+    ce = cudaMalloc(&t->h_state, sizeof(double) * t->state_total);
+    if (ce == cudaSuccess) ce = cudaMalloc(&t->h_control, sizeof(double) * t->control_total);
+    if (ce == cudaSuccess) ce = cudaMalloc(&t->h_status, sizeof(uint32_t) * t->W);
+    if (ce == cudaSuccess) ce = cudaMalloc(&t->h_taken, sizeof(int32_t) * t->W);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaMalloc");
+  }
+  ce = cudaMemcpy(t->h_state, state_in, sizeof(double) * t->state_total, cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpy(t->h_control, control, sizeof(double) * t->control_total,
+                    cudaMemcpyHostToDevice);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy to device");
+  int rc = cb_step(t, method, t->h_state, t->h_state, dt, t->h_control, n_steps, t->h_status,
+                   t->h_taken, nullptr);
+  if (rc) return rc;
+  ce = cudaMemcpy(state_out, t->h_state, sizeof(double) * t->state_total, cudaMemcpyDeviceToHost);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpy(world_status, t->h_status, sizeof(uint32_t) * t->W, cudaMemcpyDeviceToHost);
+  if (ce == cudaSuccess && accepted_steps)
+    ce = cudaMemcpy(accepted_steps, t->h_taken, sizeof(int32_t) * t->W, cudaMemcpyDeviceToHost);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy to host");
+  return CB_OK;
+}
+
+int cb_balances(cb_tissue *t, const double *state, double *out, void *stream) {
+  if (!t || !state || !out) return fail(CB_ERR_ARGUMENT, "null argument");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CB_DISPATCH(launch_balances, state, out, s);
+}
+
+}  // extern "C"

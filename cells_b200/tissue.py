@@ -1,0 +1,193 @@
+"""Host side of the device tissue step: bind a packed batch, pack/unpack state, step.
+
+This mirrors the reference's model-module protocol for the resolved pump-leak tissue
+(src/cells/models/surface_pump.py:124-369 and src/cells/models/surface_pump_v3.py:3989):
+
+* ``Tissue(batch)``            ~ ``initial_values(spec)``'s layout binding (cb_bind)
+* ``Tissue.initial_state()``   ~ ``initial_values(spec)``'s state (all increments zero)
+* ``Tissue.step(...)``         ~ ``checked_step`` repeated ``n_steps`` times, every world at once
+  on device buffers (cb_step); a refused world keeps its last accepted state, as the reference's
+  ``where(valid, new, old)`` does (surface_pump.py:362).
+* ``checked_step(...)``        ~ ``checked_step(state, dt, control, p, active) -> (state, valid)``
+  with host arrays (cb_step_host), one step.
+* ``Tissue.balances(...)``     ~ ``balances(state, p)``'s residuals (cb_balances).
+
+State is a dict of NumPy arrays in the packed layout (``_lib.STATE_FIELDS``; cell fields [3, C]
+or [C], junction fields [3, E] or [E], world fields [3, W] or [W]). Device buffers are torch
+float64 CUDA tensors; torch is only the allocator and stream provider here.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+SPECIES_FIELDS = {"amount_increment", "membrane_transferred", "junction_transferred",
+                  "reservoir_supplied"}
+CELL = ("amount_increment", "membrane_transferred", "membrane_dissipated", "pump_cycles",
+        "pump_dissipated", "metabolic_work")
+EDGE = ("junction_transferred", "junction_dissipated", "junction_gate")
+WORLD = ("reservoir_supplied", "electrode_charge", "reservoir_work", "electrode_work")
+
+
+def _ptr(a, ctype=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+class Tissue:
+    """A packed batch bound on one device (cb_bind)."""
+
+    def __init__(self, batch, device=0):
+        self.lib = _lib.load()
+        self.batch = batch
+        self.device = int(device)
+        b = batch
+        # Keep every host array alive for the duration of the bind call.
+        self._keep = keep = {
+            "cell_offset": np.ascontiguousarray(b.cell_offset, dtype=np.int64),
+            "edge_offset": np.ascontiguousarray(b.edge_offset, dtype=np.int64),
+            "temperature": np.ascontiguousarray(b.temperature, dtype=np.float64),
+            "bath_amount": np.ascontiguousarray(b.bath_amount, dtype=np.float64),
+            "bath_volume": np.ascontiguousarray(b.bath_volume, dtype=np.float64),
+            "bath_potential": np.ascontiguousarray(b.bath_potential, dtype=np.float64),
+            "pump": np.ascontiguousarray(b.pump, dtype=np.float64),
+            "volume": np.ascontiguousarray(b.volume, dtype=np.float64),
+            "area": np.ascontiguousarray(b.area, dtype=np.float64),
+            "capacitance": np.ascontiguousarray(b.capacitance, dtype=np.float64),
+            "permeability": np.ascontiguousarray(b.permeability, dtype=np.float64),
+            "pump_capacity": np.ascontiguousarray(b.pump_capacity, dtype=np.float64),
+            "amount_reference": np.ascontiguousarray(b.amount_reference, dtype=np.float64),
+            "initial_charge": np.ascontiguousarray(b.initial_charge, dtype=np.float64),
+            "sender": np.ascontiguousarray(b.sender, dtype=np.int32),
+            "receiver": np.ascontiguousarray(b.receiver, dtype=np.int32),
+            "junction_area": np.ascontiguousarray(b.junction_area, dtype=np.float64),
+            "junction_permeability": np.ascontiguousarray(b.junction_permeability,
+                                                          dtype=np.float64),
+            "gate_threshold": np.ascontiguousarray(b.gate_threshold, dtype=np.float64),
+            "gate_minimum": np.ascontiguousarray(b.gate_minimum, dtype=np.float64),
+        }
+        desc = _lib.TissueDesc()
+        desc.n_worlds = b.worlds
+        desc.n_cells = b.cells
+        desc.n_edges = b.edges
+        for name, arr in keep.items():
+            ctype = {np.int64: ctypes.c_int64, np.int32: ctypes.c_int32}.get(arr.dtype.type,
+                                                                            ctypes.c_double)
+            setattr(desc, name, _ptr(arr, ctype))
+        handle = ctypes.c_void_p()
+        _lib.check(self.lib.cb_bind(ctypes.byref(desc), self.device, ctypes.byref(handle)))
+        self.handle = handle
+        off = np.zeros(len(_lib.STATE_FIELDS), dtype=np.int64)
+        total = np.zeros(1, dtype=np.int64)
+        _lib.check(self.lib.cb_state_layout(self.handle, _ptr(off, ctypes.c_int64),
+                                            _ptr(total, ctypes.c_int64)))
+        self.state_offsets = dict(zip(_lib.STATE_FIELDS, off.tolist(), strict=True))
+        self.state_size = int(total[0])
+        coff = np.zeros(len(_lib.CONTROL_FIELDS), dtype=np.int64)
+        _lib.check(self.lib.cb_control_layout(self.handle, _ptr(coff, ctypes.c_int64),
+                                              _ptr(total, ctypes.c_int64)))
+        self.control_offsets = dict(zip(_lib.CONTROL_FIELDS, coff.tolist(), strict=True))
+        self.control_size = int(total[0])
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.lib.cb_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- packing (host)
+    def _shape(self, name):
+        b = self.batch
+        n = b.cells if name in CELL else b.edges if name in EDGE else b.worlds
+        return (3, n) if name in SPECIES_FIELDS else (n,)
+
+    def pack_state(self, state):
+        flat = np.zeros(self.state_size)
+        for name in _lib.STATE_FIELDS:
+            v = np.asarray(state[name], dtype=np.float64)
+            shape = self._shape(name)
+            if v.shape != shape:
+                raise ValueError(f"state field {name}: shape {v.shape}, expected {shape}")
+            o = self.state_offsets[name]
+            flat[o:o + v.size] = v.reshape(-1)
+        return flat
+
+    def unpack_state(self, flat):
+        flat = np.asarray(flat)
+        out = {}
+        for name in _lib.STATE_FIELDS:
+            shape = self._shape(name)
+            o = self.state_offsets[name]
+            out[name] = flat[o:o + int(np.prod(shape))].reshape(shape).copy()
+        return out
+
+    def pack_control(self, membrane=1.0, junction=1.0, pump=1.0):
+        b = self.batch
+        flat = np.zeros(self.control_size)
+        for name, value, n in (("membrane", membrane, b.cells), ("junction", junction, b.edges),
+                               ("pump", pump, b.cells)):
+            o = self.control_offsets[name]
+            flat[o:o + n] = np.broadcast_to(np.asarray(value, dtype=np.float64), (n,))
+        return flat
+
+    def initial_state(self):
+        b = self.batch
+        state = {name: np.zeros(self._shape(name)) for name in _lib.STATE_FIELDS}
+        state["junction_gate"] = np.asarray(b.gate_initial, dtype=np.float64).copy()
+        return state
+
+    # ---------------------------------------------------------------- device entry points
+    def step(self, state_in, state_out, control, dt, n_steps, status, accepted=None, stream=None,
+             method=_lib.METHOD_ARS222):
+        """cb_step on device tensors (float64 state/control, int32 status/accepted)."""
+        _lib.check(self.lib.cb_step(
+            self.handle, int(method), ctypes.c_void_p(state_in.data_ptr()),
+            ctypes.c_void_p(state_out.data_ptr()), float(dt),
+            ctypes.c_void_p(control.data_ptr()), int(n_steps),
+            ctypes.c_void_p(status.data_ptr()),
+            None if accepted is None else ctypes.c_void_p(accepted.data_ptr()),
+            None if stream is None else ctypes.c_void_p(stream),
+        ))  # fmt: skip
+
+    def step_host(self, state_in, control, dt, n_steps, method=_lib.METHOD_ARS222):
+        """cb_step_host on packed host arrays; returns (state, status[W], accepted[W])."""
+        src = np.ascontiguousarray(state_in, dtype=np.float64)
+        ctl = np.ascontiguousarray(control, dtype=np.float64)
+        out = np.empty(self.state_size)
+        status = np.zeros(self.batch.worlds, dtype=np.uint32)
+        taken = np.zeros(self.batch.worlds, dtype=np.int32)
+        _lib.check(self.lib.cb_step_host(
+            self.handle, int(method), _ptr(src), _ptr(out), float(dt), _ptr(ctl), int(n_steps),
+            _ptr(status, ctypes.c_uint32), _ptr(taken, ctypes.c_int32),
+        ))  # fmt: skip
+        return out, status, taken
+
+    def balances(self, state_dev, out_dev, stream=None):
+        """cb_balances: out_dev [W*8] float64 device tensor."""
+        _lib.check(self.lib.cb_balances(
+            self.handle, ctypes.c_void_p(state_dev.data_ptr()),
+            ctypes.c_void_p(out_dev.data_ptr()),
+            None if stream is None else ctypes.c_void_p(stream),
+        ))  # fmt: skip
+
+
+def checked_step(state, dt, control, tissue):
+    """One step with host arrays: (state, valid[W]) as the reference's checked_step returns,
+    every world at once. ``control`` is a dict with membrane/junction/pump availabilities."""
+    flat = tissue.pack_state(state)
+    ctl = tissue.pack_control(**control) if isinstance(control, dict) else control
+    out, status, _ = tissue.step_host(flat, ctl, dt, 1)
+    return tissue.unpack_state(out), status == 0
+
+
+def decode_status(bits):
+    """Names of the refusal bits of one world's status word."""
+    return [name for bit, name in _lib.WORLD_BITS.items() if int(bits) & bit]

@@ -1,0 +1,509 @@
+"""Seeded synthetic pump-leak tissues, packed structure-of-arrays for the device step.
+
+A *world* is one tissue: N cells, each with one membrane patch facing a held bath (a reservoir
+outside node clamped at a boundary potential), E gap junctions between cells, Na/K/Cl with
+valences +1/+1/-1, a Na/K-ATPase on every patch, and junction gates of the reference's
+voltage-relaxation law. Worlds never interact. A *batch* packs W worlds of possibly different
+sizes back to back: world w owns cells ``cell_offset[w]:cell_offset[w+1]`` and junctions
+``edge_offset[w]:edge_offset[w+1]``; junction endpoints are world-local cell indices.
+
+Units follow the reference's definition schema (models/surface_tissue.py:135-257): volumes in
+pL, amounts in fmol, areas in m^2, permeabilities in m/s, capacitances in F, temperature in K,
+potentials in V. Pump parameters follow laws/pumps/nak_atp_mass_action_positive.py:36-50.
+
+The shapes are the pump-leak tissues of the benchmark suite: a square grid with 4-neighbour
+junctions (16 cells for the single CPU world, 16x16 for the batched plain step), and Delaunay
+contact graphs of Poisson-disk points for uneven batches. ``reference_definition`` writes one
+world in the reference's JSON schema so that its own parser and step can run it.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+SPECIES = ("Na", "K", "Cl")
+VALENCE = np.array([1.0, 1.0, -1.0])
+SODIUM, POTASSIUM = 0, 1
+STOICHIOMETRY = np.array([-3.0, 2.0, 0.0])  # Inward-positive per cycle (Na out, K in).
+
+# Constants of laws/electrochemistry.py:11-15 (same expressions, so the same doubles).
+AVOGADRO = 6.02214076e23
+F = AVOGADRO * 1.602176634e-19
+R = AVOGADRO * 1.380649e-23
+MOL_PER_FMOL = 1e-15
+CHARGE_PER_FMOL = F * MOL_PER_FMOL
+
+# The benchmark tissue's laws (cm/s figures converted to m/s).
+CELL_RADIUS_M = 5e-6
+SPECIFIC_CAPACITANCE_F_M2 = 0.01  # 1 uF/cm^2
+TEMPERATURE_K = 310.15  # 37 C
+BATH_mM = np.array([145.0, 5.0, 110.0])
+BATH_VOLUME_PL = 1.0e4
+LEAK_MEDIAN_M_S = np.array([1e-12, 1e-10, 1e-11])  # P_Na 1e-10, P_K 1e-8, P_Cl 1e-9 cm/s
+LEAK_SIGMA = 0.3
+JUNCTION_M_S = 1e-9  # 1e-7 cm/s
+JUNCTION_AREA_M2 = 1e-11  # Not given by the benchmark: declared here.
+INITIAL_mM_RANGES = np.array([[10.0, 15.0], [130.0, 145.0], [5.0, 20.0]])
+# Pump declaration of the reference's configs/resolved_pump_tissue.json, capacity scaled by area
+# (0.02 fmol/s on 4e-10 m^2).
+PUMP_CAPACITY_PER_M2 = 0.02 / 4e-10
+PUMP_KM_NA, PUMP_KM_K, PUMP_KM_ATP = 12.0, 0.2, 0.5
+PUMP_ATP, PUMP_ADP, PUMP_PI = 1.5, 0.1, 0.1
+PUMP_DG0 = -37000.0
+
+
+@dataclass
+class World:
+    """One tissue, host arrays, world-local indices."""
+
+    volume: np.ndarray  # [N] pL
+    area: np.ndarray  # [N] m^2 (the cell's one membrane patch)
+    capacitance: np.ndarray  # [N] F
+    permeability: np.ndarray  # [S, N] m/s
+    pump_capacity: np.ndarray  # [N] fmol cycles/s
+    amount: np.ndarray  # [S, N] fmol, initial
+    fixed_charge_fmol: np.ndarray  # [N] fixed background, charge-equivalent fmol
+    initial_charge: np.ndarray  # [N] C
+    sender: np.ndarray  # [E] int
+    receiver: np.ndarray  # [E] int
+    junction_area: np.ndarray  # [E] m^2
+    junction_permeability: np.ndarray  # [S, E] m/s
+    gate_threshold: np.ndarray  # [E] V
+    gate_minimum: np.ndarray  # [E]
+    gate_initial: np.ndarray  # [E]
+    temperature: float = TEMPERATURE_K
+    bath_mM: np.ndarray = field(default_factory=lambda: BATH_mM.copy())
+    bath_volume: float = BATH_VOLUME_PL
+    bath_potential: float = 0.0
+    pump: tuple = (PUMP_ATP, PUMP_ADP, PUMP_PI, PUMP_KM_NA, PUMP_KM_K, PUMP_KM_ATP, PUMP_DG0)
+
+    @property
+    def cells(self):
+        return self.volume.size
+
+    @property
+    def edges(self):
+        return self.sender.size
+
+
+def anchor_charge(amount, fixed):
+    """Charge anchor (C) as the reference's definition check forms it
+    (models/surface_tissue.py:484-486): F * fsum(fixed, z n)."""
+    out = np.empty(amount.shape[1])
+    for i in range(amount.shape[1]):
+        terms = [z * a for z, a in zip(VALENCE, amount[:, i], strict=True)]
+        out[i] = CHARGE_PER_FMOL * math.fsum((float(fixed[i]), *terms))
+    return out
+
+
+def grid_edges(nx, ny):
+    """4-neighbour junctions of an nx-by-ny grid, row-major cells, each pair once."""
+    senders, receivers = [], []
+    for y in range(ny):
+        for x in range(nx):
+            i = y * nx + x
+            if x + 1 < nx:
+                senders.append(i)
+                receivers.append(i + 1)
+            if y + 1 < ny:
+                senders.append(i)
+                receivers.append(i + nx)
+    return np.asarray(senders, dtype=np.int64), np.asarray(receivers, dtype=np.int64)
+
+
+def _cells(rng, n):
+    radius = CELL_RADIUS_M
+    area = np.full(n, 4.0 * math.pi * radius**2)
+    volume = np.full(n, 4.0 / 3.0 * math.pi * radius**3 * 1e15)  # m^3 -> pL
+    capacitance = SPECIFIC_CAPACITANCE_F_M2 * area
+    permeability = LEAK_MEDIAN_M_S[:, None] * np.exp(LEAK_SIGMA * rng.standard_normal((3, n)))
+    lo, hi = INITIAL_mM_RANGES[:, 0:1], INITIAL_mM_RANGES[:, 1:2]
+    conc = lo + (hi - lo) * rng.random((3, n))
+    amount = conc * volume
+    # Fixed anions set for electroneutrality: the background cancels the mobile ions' charge.
+    fixed = -(VALENCE @ amount)
+    return volume, area, capacitance, permeability, amount, fixed
+
+
+def grid_world(nx, ny, rng, *, junction_sigma=0.0, gate=None):
+    """A pump-leak tissue on an nx-by-ny grid (the benchmark's square tissues)."""
+    n = nx * ny
+    volume, area, capacitance, permeability, amount, fixed = _cells(rng, n)
+    sender, receiver = grid_edges(nx, ny)
+    return _assemble(
+        volume, area, capacitance, permeability, amount, fixed, sender, receiver, rng,
+        junction_sigma=junction_sigma, gate=gate,
+    )  # fmt: skip
+
+
+def _assemble(
+    volume, area, capacitance, permeability, amount, fixed, sender, receiver, rng, *,
+    junction_sigma, gate,
+):  # fmt: skip
+    e = sender.size
+    jp = np.full((3, e), JUNCTION_M_S)
+    if junction_sigma:
+        jp = jp * np.exp(junction_sigma * rng.standard_normal(e))[None, :]
+    if gate is None:  # Pinned open: minimum open fraction 1 keeps g = 1 exactly.
+        threshold, minimum, initial = np.full(e, 0.015), np.ones(e), np.ones(e)
+    else:
+        threshold, minimum, initial = (np.full(e, v) for v in gate)
+    return World(
+        volume=volume,
+        area=area,
+        capacitance=capacitance,
+        permeability=permeability,
+        pump_capacity=PUMP_CAPACITY_PER_M2 * area,
+        amount=amount,
+        fixed_charge_fmol=fixed,
+        initial_charge=anchor_charge(amount, fixed),
+        sender=sender,
+        receiver=receiver,
+        junction_area=np.full(e, JUNCTION_AREA_M2),
+        junction_permeability=jp,
+        gate_threshold=threshold,
+        gate_minimum=minimum,
+        gate_initial=initial,
+    )
+
+
+def poisson_disk(rng, n, *, k=30):
+    """About n points in the unit square with a minimum spacing (Bridson's dart throwing on a
+    background grid), then cut or topped up to exactly n points."""
+    r = 0.8 / math.sqrt(n)
+    cell = r / math.sqrt(2)
+    g = int(math.ceil(1 / cell))
+    grid = -np.ones((g, g), dtype=np.int64)
+    pts = [rng.random(2)]
+    grid[int(pts[0][0] / cell), int(pts[0][1] / cell)] = 0
+    active = [0]
+    while active and len(pts) < n:
+        idx = active[rng.integers(len(active))]
+        base = pts[idx]
+        placed = False
+        for _ in range(k):
+            ang = rng.random() * 2 * math.pi
+            rad = r * (1 + rng.random())
+            q = base + rad * np.array([math.cos(ang), math.sin(ang)])
+            if not (0 <= q[0] < 1 and 0 <= q[1] < 1):
+                continue
+            gx, gy = int(q[0] / cell), int(q[1] / cell)
+            ok = True
+            for ix in range(max(gx - 2, 0), min(gx + 3, g)):
+                for iy in range(max(gy - 2, 0), min(gy + 3, g)):
+                    j = grid[ix, iy]
+                    if j >= 0 and np.sum((pts[j] - q) ** 2) < r * r:
+                        ok = False
+                        break
+                if not ok:
+                    break
+            if ok:
+                grid[gx, gy] = len(pts)
+                active.append(len(pts))
+                pts.append(q)
+                placed = True
+                break
+        if not placed:
+            active.remove(idx)
+    pts = np.asarray(pts)
+    while len(pts) < n:  # Rare: top up with uniform points.
+        pts = np.vstack([pts, rng.random((n - len(pts), 2))])
+    return pts[:n]
+
+
+def delaunay_edges(points):
+    from scipy.spatial import Delaunay
+
+    tri = Delaunay(points)
+    pairs = set()
+    for a, b, c in tri.simplices:
+        for u, v in ((a, b), (b, c), (a, c)):
+            pairs.add((min(u, v), max(u, v)))
+    pairs = np.asarray(sorted(pairs), dtype=np.int64)
+    return pairs[:, 0], pairs[:, 1]
+
+
+def delaunay_world(n, rng, *, junction_sigma=0.3, gate=None):
+    """A pump-leak tissue whose contact graph is the Delaunay triangulation of Poisson-disk
+    points (mean degree about 6), junction permeabilities log-normal."""
+    volume, area, capacitance, permeability, amount, fixed = _cells(rng, n)
+    sender, receiver = delaunay_edges(poisson_disk(rng, n))
+    return _assemble(
+        volume, area, capacitance, permeability, amount, fixed, sender, receiver, rng,
+        junction_sigma=junction_sigma, gate=gate,
+    )  # fmt: skip
+
+
+def world_rng(seed, world):
+    """Independent stream per (seed, world id)."""
+    return np.random.default_rng([int(seed), int(world)])
+
+
+def single_grid_tissue(seed=0):
+    """The single CPU world: 16 cells on a 4x4 grid."""
+    return grid_world(4, 4, world_rng(seed, 0))
+
+
+def grid_tissues(worlds, side=16, seed=1):
+    """The batched plain step: ``worlds`` independent side-by-side grid tissues."""
+    return [grid_world(side, side, world_rng(seed, w)) for w in range(worlds)]
+
+
+def uneven_sizes(worlds, lo=32, hi=4096, seed=2):
+    rng = np.random.default_rng([int(seed), 1 << 20])
+    return np.floor(np.exp(rng.uniform(math.log(lo), math.log(hi + 1), worlds))).astype(np.int64)
+
+
+def delaunay_tissues(worlds, lo=32, hi=4096, seed=2):
+    """Uneven batch: cell counts log-uniform in [lo, hi], Delaunay contact graphs."""
+    sizes = uneven_sizes(worlds, lo, hi, seed)
+    return [delaunay_world(int(n), world_rng(seed, w)) for w, n in enumerate(sizes)]
+
+
+# --------------------------------------------------------------------------------------------
+# Packing
+
+
+@dataclass
+class Batch:
+    """W worlds packed back to back (structure of arrays, float64 unless noted)."""
+
+    cell_offset: np.ndarray  # [W+1] int64
+    edge_offset: np.ndarray  # [W+1] int64
+    temperature: np.ndarray  # [W]
+    bath_amount: np.ndarray  # [S, W] fmol (held reservoir reference amounts)
+    bath_volume: np.ndarray  # [W] pL
+    bath_potential: np.ndarray  # [W] V
+    pump: np.ndarray  # [7, W]: atp, adp, pi, km_na, km_k, km_atp (mM), delta_g0 (J/mol)
+    volume: np.ndarray  # [C]
+    area: np.ndarray  # [C]
+    capacitance: np.ndarray  # [C]
+    permeability: np.ndarray  # [S, C]
+    pump_capacity: np.ndarray  # [C]
+    amount_reference: np.ndarray  # [S, C]
+    initial_charge: np.ndarray  # [C]
+    sender: np.ndarray  # [E] int32, world-local
+    receiver: np.ndarray  # [E] int32, world-local
+    junction_area: np.ndarray  # [E]
+    junction_permeability: np.ndarray  # [S, E]
+    gate_threshold: np.ndarray  # [E]
+    gate_minimum: np.ndarray  # [E]
+    gate_initial: np.ndarray  # [E]
+
+    @property
+    def worlds(self):
+        return self.cell_offset.size - 1
+
+    @property
+    def cells(self):
+        return int(self.cell_offset[-1])
+
+    @property
+    def edges(self):
+        return int(self.edge_offset[-1])
+
+    def world(self, w):
+        """World w back as a World (host views)."""
+        c0, c1 = self.cell_offset[w], self.cell_offset[w + 1]
+        e0, e1 = self.edge_offset[w], self.edge_offset[w + 1]
+        return World(
+            volume=self.volume[c0:c1],
+            area=self.area[c0:c1],
+            capacitance=self.capacitance[c0:c1],
+            permeability=self.permeability[:, c0:c1],
+            pump_capacity=self.pump_capacity[c0:c1],
+            amount=self.amount_reference[:, c0:c1],
+            fixed_charge_fmol=-(VALENCE @ self.amount_reference[:, c0:c1]),
+            initial_charge=self.initial_charge[c0:c1],
+            sender=self.sender[e0:e1].astype(np.int64),
+            receiver=self.receiver[e0:e1].astype(np.int64),
+            junction_area=self.junction_area[e0:e1],
+            junction_permeability=self.junction_permeability[:, e0:e1],
+            gate_threshold=self.gate_threshold[e0:e1],
+            gate_minimum=self.gate_minimum[e0:e1],
+            gate_initial=self.gate_initial[e0:e1],
+            temperature=float(self.temperature[w]),
+            bath_mM=self.bath_amount[:, w] / self.bath_volume[w],
+            bath_volume=float(self.bath_volume[w]),
+            bath_potential=float(self.bath_potential[w]),
+            pump=tuple(float(v) for v in self.pump[:, w]),
+        )
+
+
+def pack(worlds):
+    """Pack a list of World into one Batch."""
+    cells = np.array([w.cells for w in worlds], dtype=np.int64)
+    edges = np.array([w.edges for w in worlds], dtype=np.int64)
+    cat = np.concatenate
+
+    def cells_of(name):
+        return cat([getattr(w, name) for w in worlds], axis=-1)
+
+    return Batch(
+        cell_offset=np.r_[0, np.cumsum(cells)].astype(np.int64),
+        edge_offset=np.r_[0, np.cumsum(edges)].astype(np.int64),
+        temperature=np.array([w.temperature for w in worlds]),
+        bath_amount=np.stack([w.bath_mM * w.bath_volume for w in worlds], axis=1),
+        bath_volume=np.array([w.bath_volume for w in worlds]),
+        bath_potential=np.array([w.bath_potential for w in worlds]),
+        pump=np.array([w.pump for w in worlds], dtype=float).T.copy(),
+        volume=cells_of("volume"),
+        area=cells_of("area"),
+        capacitance=cells_of("capacitance"),
+        permeability=cells_of("permeability"),
+        pump_capacity=cells_of("pump_capacity"),
+        amount_reference=cells_of("amount"),
+        initial_charge=cells_of("initial_charge"),
+        sender=cells_of("sender").astype(np.int32),
+        receiver=cells_of("receiver").astype(np.int32),
+        junction_area=cells_of("junction_area"),
+        junction_permeability=cells_of("junction_permeability"),
+        gate_threshold=cells_of("gate_threshold"),
+        gate_minimum=cells_of("gate_minimum"),
+        gate_initial=cells_of("gate_initial"),
+    )
+
+
+# --------------------------------------------------------------------------------------------
+# The reference's definition schema (configs/resolved_pump_tissue.json's fields)
+
+
+def reference_definition(world, *, dt, steps, model="cells.model.resolved_pump_tissue@1",
+                         solver="cells.solver.imex_ars222_face_electromigration@1",
+                         membrane_control=None, junction_control=None, pump_control=None):
+    """One World as a reference definition dict (schema_version 1)."""
+    n, e = world.cells, world.edges
+    mc = np.ones(n) if membrane_control is None else np.broadcast_to(membrane_control, (n,))
+    jc = np.ones(e) if junction_control is None else np.broadcast_to(junction_control, (e,))
+    pc = np.ones(n) if pump_control is None else np.broadcast_to(pump_control, (n,))
+    atp, adp, pi, km_na, km_k, km_atp, dg0 = world.pump
+    bath_amount = world.bath_mM * world.bath_volume
+    bath_fixed = -float(VALENCE @ bath_amount)
+    cells = []
+    for i in range(n):
+        cells.append({
+            "id": f"cell_{i}",
+            "volume_pL": float(world.volume[i]),
+            "initial_amount_fmol": {s: float(world.amount[k, i]) for k, s in enumerate(SPECIES)},
+            "fixed_charge_equivalent_fmol": float(world.fixed_charge_fmol[i]),
+            "initial_charge_C": float(world.initial_charge[i]),
+        })
+    bath = {
+        "id": "bath",
+        "volume_pL": float(world.bath_volume),
+        "initial_amount_fmol": {s: float(bath_amount[k]) for k, s in enumerate(SPECIES)},
+        "fixed_charge_equivalent_fmol": bath_fixed,
+        "initial_charge_C": float(anchor_charge(bath_amount[:, None], [bath_fixed])[0]),
+        "reservoir": True,
+        "boundary_potential_V": float(world.bath_potential),
+    }
+    membranes = []
+    for i in range(n):
+        membranes.append({
+            "id": f"membrane_{i}",
+            "inside": f"cell_{i}",
+            "outside": "bath",
+            "area_m2": float(world.area[i]),
+            "capacitance_F": float(world.capacitance[i]),
+            "permeability_m_per_s": {
+                s: float(world.permeability[k, i]) for k, s in enumerate(SPECIES)
+            },
+            "law": "cells.route.constant_field@1",
+            "pump": {
+                "id": f"pump_{i}",
+                "law": "cells.cycle.nak_atp_mass_action_positive@1",
+                "roles": {"sodium": "Na", "potassium": "K"},
+                "stoichiometry": {"Na": -3, "K": 2},
+                "capacity_fmol_per_s": float(world.pump_capacity[i]),
+                "km_na_mM": km_na,
+                "km_k_mM": km_k,
+                "km_atp_mM": km_atp,
+                "metabolism": {
+                    "kind": "cells.fuel_kind.maintained_chemical_reservoirs@1",
+                    "atp_mM": atp,
+                    "adp_mM": adp,
+                    "pi_mM": pi,
+                    "delta_g0_J_per_mol": dg0,
+                },
+            },
+        })
+    junctions = []
+    for k in range(e):
+        junctions.append({
+            "id": f"junction_{k}",
+            "sender": f"cell_{int(world.sender[k])}",
+            "receiver": f"cell_{int(world.receiver[k])}",
+            "area_m2": float(world.junction_area[k]),
+            "permeability_m_per_s": {
+                s: float(world.junction_permeability[j, k]) for j, s in enumerate(SPECIES)
+            },
+            "law": "cells.route.constant_field@1",
+            "gate": {
+                "law": "cells.junction.junction_voltage_relaxation@1",
+                "threshold_voltage_V": float(world.gate_threshold[k]),
+                "minimum_open_fraction": float(world.gate_minimum[k]),
+                "initial_gate": float(world.gate_initial[k]),
+            },
+        })
+    end = float(dt * steps)
+    v3 = model.endswith("@3")
+    out = {
+        "schema_version": 1,
+        "model": {
+            "id": model,
+            "temperature_K": float(world.temperature),
+            "species": [{"id": s, "valence": int(z)} for s, z in zip(SPECIES, VALENCE, strict=True)],
+            "cells": cells,
+            "extracellular": [bath],
+            "membranes": membranes,
+            "junctions": junctions,
+            "faces": [],
+            "closure": {
+                "law": "cells.field_closure.resolved_capacitor_components_current_continuity@1",
+                "gauge_reference": None,
+            },
+        },
+        "experiment": {
+            "end_time": end,
+            "observation_times": [0.0, end],
+            "membrane_controls": [
+                {"membrane_id": f"membrane_{i}", "schedule": [{"time": 0.0, "availability": float(mc[i])}]}
+                for i in range(n)
+            ],
+            "junction_controls": [
+                {"junction_id": f"junction_{k}", "schedule": [{"time": 0.0, "availability": float(jc[k])}]}
+                for k in range(e)
+            ],
+            "pump_controls": [
+                {"pump_id": f"pump_{i}", "schedule": [{"time": 0.0, "availability": float(pc[i])}]}
+                for i in range(n)
+            ],
+        },
+        "execution": {
+            "dt": float(dt),
+            "capacity": n,
+            "extracellular_capacity": 1,
+            "membrane_capacity": n,
+            "edge_capacity": e,
+            "face_capacity": 0,
+            "backend": "cpu",
+            "jit": True,
+            "precision": "float64",
+            "solver": solver,
+            "field_solver": "cells.solver.capacitive_reduction_gauged_damped_newton@2",
+            "max_steps": int(steps),
+            "max_trace_bytes": 536870912,
+            "material_balance_atol_fmol": {s: 2e-11 for s in SPECIES},
+        },
+    }
+    if v3:  # @3 declares its (here empty) channel population and Ca pumps explicitly.
+        out["model"]["channels"] = []
+        out["experiment"]["channel_controls"] = []
+        out["execution"]["channel_capacity"] = 0
+        for membrane in out["model"]["membranes"]:
+            membrane["calcium_pump"] = None
+        out["experiment"]["calcium_pump_controls"] = []
+    return out

@@ -1,0 +1,162 @@
+/*
+ * cells_b200.h - C ABI of the B200 tissue electrodiffusion step.
+ *
+ * The library replaces the reference's model-module protocol for the resolved pump-leak tissue
+ * (Cells, src/cells/models/surface_pump.py and src/cells/models/surface_pump_v3.py):
+ *
+ *   initial_values(spec) -> (state, layout)      ~ cb_bind            (surface_pump.py:124-138,
+ *                                                                      surface_tissue.py:135-257)
+ *   checked_step(state, dt, control, p, active)  ~ cb_step / cb_step_host
+ *                                                  (surface_pump.py:365-369 -> imex_step :259-362;
+ *                                                   surface_pump_v3.py:3989 -> imex_step :3547)
+ *   balances(state, p)                            ~ cb_balances       (surface_tissue.py:536-611,
+ *                                                                      surface_kinetic.py:470-482)
+ *
+ * Worlds are packed back to back (see cells_b200/worlds.py): world w owns cells
+ * cell_offset[w] .. cell_offset[w+1]-1 and junctions edge_offset[w] .. edge_offset[w+1]-1.
+ * Every cell has one membrane patch that faces its world's one held bath (a reservoir outside
+ * node clamped at bath_potential). Species are Na, K, Cl with valences +1, +1, -1; the pump is
+ * the Na/K-ATPase (3 Na out, 2 K in) of laws/pumps/nak_atp_mass_action_positive.py.
+ *
+ * Error convention (the reference's: a traced step never raises; it returns valid=False and the
+ * unchanged state, surface_pump_v3.py:3934): cb_step returns 0 when the launch is well formed and
+ * reports each world's refusal in world_status (bit mask below); a refused world keeps its last
+ * accepted state and takes no further steps in that call. A nonzero return is a configuration
+ * or CUDA error; cb_last_error() gives the message. Nothing falls back to the CPU.
+ *
+ * Threading: a handle is used by one host thread at a time. Every device pointer argument must
+ * be device memory of the handle's device; stream may be NULL (the legacy default stream).
+ */
+#ifndef CELLS_B200_H
+#define CELLS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cb_tissue cb_tissue;
+
+/* Per-world refusal bits (world_status). */
+#define CB_WORLD_OK 0u
+#define CB_WORLD_TRANSPORT 1u      /* concentration <= 0 or non-finite, |zF dV/RT| > 50, flux */
+#define CB_WORLD_PUMP_DOMAIN 2u    /* nak_atp_mass_action_positive.domain_valid */
+#define CB_WORLD_GATE_DOMAIN 4u    /* junction_voltage_relaxation.domain_valid */
+#define CB_WORLD_CONTROL 8u        /* an availability outside [0, 1] or non-finite */
+#define CB_WORLD_RESIDUAL 16u      /* stage charge residual above 3e-25 C + 2e-12 |q| */
+#define CB_WORLD_DOMAIN 32u        /* accepted-state domain: amounts, gates, finite ledgers */
+
+/* Return codes. */
+#define CB_OK 0
+#define CB_ERR_ARGUMENT 1
+#define CB_ERR_LAYOUT 2
+#define CB_ERR_CUDA 3
+#define CB_ERR_UNSUPPORTED 4
+
+/*
+ * Packed world description (HOST pointers; copied at bind). Units: pL, fmol, m^2, m/s, F, K, V,
+ * mM, J/mol, as the reference's definition schema. Arrays marked [3*X] are species-major
+ * (Na block, then K, then Cl).
+ */
+typedef struct cb_tissue_desc {
+  int32_t n_worlds;
+  int64_t n_cells;              /* total over worlds */
+  int64_t n_edges;              /* total over worlds */
+  const int64_t *cell_offset;   /* [n_worlds+1] */
+  const int64_t *edge_offset;   /* [n_worlds+1] */
+  const double *temperature;    /* [W] K */
+  const double *bath_amount;    /* [3*W] fmol, the held bath's reference amounts */
+  const double *bath_volume;    /* [W] pL */
+  const double *bath_potential; /* [W] V */
+  const double *pump;           /* [7*W]: atp, adp, pi, km_na, km_k, km_atp (mM), dG0 (J/mol) */
+  const double *volume;         /* [C] pL */
+  const double *area;           /* [C] m^2 */
+  const double *capacitance;    /* [C] F */
+  const double *permeability;   /* [3*C] m/s */
+  const double *pump_capacity;  /* [C] fmol cycles/s */
+  const double *amount_reference; /* [3*C] fmol (the state stores increments over these) */
+  const double *initial_charge; /* [C] C, the charge anchor of each cell */
+  const int32_t *sender;        /* [E] world-local cell index */
+  const int32_t *receiver;      /* [E] world-local cell index */
+  const double *junction_area;  /* [E] m^2 */
+  const double *junction_permeability; /* [3*E] m/s */
+  const double *gate_threshold; /* [E] V */
+  const double *gate_minimum;   /* [E] minimum open fraction */
+} cb_tissue_desc;
+
+/* State fields in a packed state buffer, in this order (cb_state_layout gives each offset). */
+enum cb_state_field {
+  CB_AMOUNT_INCREMENT = 0,      /* [3][C] fmol over amount_reference (STATE amount_increment) */
+  CB_MEMBRANE_TRANSFERRED,      /* [3][C] fmol, passive, outward-positive */
+  CB_MEMBRANE_DISSIPATED,       /* [C] pJ */
+  CB_PUMP_CYCLES,               /* [C] fmol cycles */
+  CB_PUMP_DISSIPATED,           /* [C] pJ */
+  CB_METABOLIC_WORK,            /* [C] pJ */
+  CB_JUNCTION_TRANSFERRED,      /* [3][E] fmol, sender -> receiver */
+  CB_JUNCTION_DISSIPATED,       /* [E] pJ */
+  CB_JUNCTION_GATE,             /* [E] relative conductance g */
+  CB_RESERVOIR_SUPPLIED,        /* [3][W] fmol into the finite system */
+  CB_ELECTRODE_CHARGE,          /* [W] C */
+  CB_RESERVOIR_WORK,            /* [W] pJ */
+  CB_ELECTRODE_WORK,            /* [W] pJ */
+  CB_STATE_FIELDS
+};
+
+/* Control fields (availabilities in [0,1]; SurfaceKineticControl, execution/schedule.py:18-22). */
+enum cb_control_field {
+  CB_CONTROL_MEMBRANE = 0, /* [C] */
+  CB_CONTROL_JUNCTION,     /* [E] */
+  CB_CONTROL_PUMP,         /* [C] */
+  CB_CONTROL_FIELDS
+};
+
+/* Step methods. */
+#define CB_METHOD_ARS222 0 /* cells.solver.imex_ars222_face_electromigration@1 */
+
+/*
+ * Host symbolic bind (replaces initial_values' layout binding, surface_tissue.py:135-257 and
+ * surface_field.bind :253-361): validates the packed description, builds each cell's junction
+ * adjacency (CSR, edge order), uploads parameters to `device`. Worlds of up to 1024 cells.
+ */
+int cb_bind(const cb_tissue_desc *desc, int device, cb_tissue **out);
+void cb_free(cb_tissue *t);
+
+/* Offsets (in doubles) of each state field in a packed state buffer, and its total length. */
+int cb_state_layout(const cb_tissue *t, int64_t offsets[CB_STATE_FIELDS], int64_t *total);
+/* Offsets (in doubles) of each control field in a packed control buffer, and its total length. */
+int cb_control_layout(const cb_tissue *t, int64_t offsets[CB_CONTROL_FIELDS], int64_t *total);
+
+/*
+ * n_steps steps of length dt (s) for every world (checked_step, repeated). state_in and
+ * state_out may alias. DEVICE pointers. world_status [W] receives the refusal bits of the first
+ * refused step (0 if all accepted); accepted_steps [W] (may be NULL) the steps each world took.
+ */
+int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out, double dt,
+            const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
+            void *stream);
+
+/* cb_step with HOST buffers: copies in, steps, copies out, synchronizes (end-to-end call). */
+int cb_step_host(cb_tissue *t, int method, const double *state_in, double *state_out, double dt,
+                 const double *control, int n_steps, uint32_t *world_status,
+                 int32_t *accepted_steps);
+
+/*
+ * Conservation ledgers of one packed state (DEVICE pointers), per world:
+ * out[w*8 + k] = max |residual| of ledger k: 0 local material (fmol), 1 bath material (fmol),
+ * 2 world total material (fmol), 3 electrode charge (C), 4 global charge (C),
+ * 5 reservoir work (pJ), 6 electrode work (pJ), 7 metabolic work (pJ).
+ */
+int cb_balances(cb_tissue *t, const double *state, double *out, void *stream);
+
+/* Message of the last error on this thread. */
+const char *cb_last_error(void);
+/* Library version string. */
+const char *cb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CELLS_B200_H */

@@ -1,0 +1,210 @@
+"""Generate the golden fixtures under tests/golden/ by running the REFERENCE's own step.
+
+Run in a container that holds the reference source (default /root/reference), never on the GPU
+box and never from the test suite:
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+The reference is a JAX program; jax is absent here, so ``jax_shim/`` (a NumPy stand-in for the
+few jax names it touches) goes first on sys.path and the reference's step runs on its own
+``xp=np`` branch (models/surface_pump.py:259-362 imex_step, models/surface_pump_v3.py:3547
+imex_step, numerics/fixed_step.py:25 rk4_checked_step). Each fixture stores the world (the packed
+arrays of cells_b200.worlds) and the reference's state at chosen steps, converted to the packed
+layout of oracle/tissue.py (membrane i is cell i's patch; the world has one held bath).
+
+Fixtures:
+  ars222_grid4x4.npz     The single 4x4 CPU world (seed 0), ARS(2,2,2), dt 1 ms, 10,000 steps,
+                         @1; snapshots at a few early steps and every 500 steps.
+  ars222_v3_grid4x4.npz  The same world through @3's imex_step for 200 steps (the live model).
+  ars222_gated.npz       A 3x3 world with voltage-gated junctions (minimum 0.1), partial controls
+                         and a bath at -4 mV, 400 steps at 1 ms (@1).
+  rk4_grid4x4.npz        The 4x4 world by RK4 at dt 0.1 ms, 100 steps (@1).
+  laws.npz               Point laws on grids of inputs: bernoulli, the pump kinetics and the
+                         junction gate rate.
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def _setup(reference):
+    sys.path.insert(0, os.path.join(HERE, "jax_shim"))
+    sys.path.insert(0, os.path.join(reference, "src"))
+    sys.path.insert(0, reference)
+    sys.path.insert(0, REPO)
+
+
+def _state_to_packed(state):
+    """Reference STATE_TYPE (one world, held bath at outside slot 0) -> packed dict."""
+    return dict(
+        amount_increment=np.asarray(state.amount_increment),
+        membrane_transferred=np.asarray(state.membrane_transferred),
+        membrane_dissipated=np.asarray(state.membrane_dissipated_energy_pJ),
+        pump_cycles=np.asarray(state.pump_cycles),
+        pump_dissipated=np.asarray(state.pump_dissipated_energy_pJ),
+        metabolic_work=np.asarray(state.metabolic_work_pJ),
+        junction_transferred=np.asarray(state.junction_transferred),
+        junction_dissipated=np.asarray(state.junction_dissipated_energy_pJ),
+        junction_gate=np.asarray(state.junction_gate),
+        reservoir_supplied=np.asarray(state.reservoir_supplied)[:, :1],
+        electrode_charge=np.asarray(state.electrode_charge_transferred_C)[:1],
+        reservoir_work=np.asarray(state.reservoir_work_pJ)[:1],
+        electrode_work=np.asarray(state.electrode_work_pJ)[:1],
+    )
+
+
+def _batch_arrays(batch):
+    from dataclasses import fields
+
+    return {"batch_" + f.name: getattr(batch, f.name) for f in fields(batch)}
+
+
+def _run(world, *, model_id, dt, steps, keep, solver, controls=None):
+    from cells.definitions.specs import parse_spec
+    from cells.registry.models import get_model
+
+    from cells_b200 import worlds
+
+    controls = controls or {}
+    raw = worlds.reference_definition(world, dt=dt, steps=steps, model=model_id, solver=solver,
+                                      **controls)
+    spec = parse_spec(raw)
+    model = get_model(spec.model)
+    state, p = model.initial_values(spec)
+    if model_id.endswith("@3"):
+        from cells.definitions.surface_pump_v3_spec import control_values
+    else:
+        from cells.execution.schedule import control_values
+    cv = control_values(spec, [0.0])
+    control = type(cv)(*(v[0] for v in cv))
+    snaps, kept = [], []
+    if 0 in keep:
+        snaps.append(_state_to_packed(state))
+        kept.append(0)
+    t0 = time.perf_counter()
+    for k in range(1, steps + 1):
+        if solver == "rk4":
+            state, ok = model.checked_step(state, dt, control, p, p.active)
+        else:
+            out = model.imex_step(state, dt, control, p, xp=np)
+            state, ok = out[0], out[1]
+        if not bool(ok):
+            raise RuntimeError(f"reference refused step {k}")
+        if k in keep:
+            snaps.append(_state_to_packed(state))
+            kept.append(k)
+    elapsed = time.perf_counter() - t0
+    stacked = {"ref_" + key: np.stack([s[key] for s in snaps]) for key in snaps[0]}
+    return stacked, np.asarray(kept), elapsed
+
+
+def _save(name, batch, stacked, kept, *, dt, model_id, solver, elapsed, extra=None):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(
+        path, **_batch_arrays(batch), **stacked, steps=kept, dt=np.asarray(dt),
+        model_id=np.asarray(model_id), solver=np.asarray(solver),
+        reference_seconds=np.asarray(elapsed), **(extra or {}),
+    )  # fmt: skip
+    print(f"{name}: {len(kept)} snapshots, reference {elapsed:.1f} s")
+
+
+def make_trajectories():
+    from cells_b200 import worlds
+
+    ars = "cells.solver.imex_ars222_face_electromigration@1"
+    world = worlds.single_grid_tissue(0)
+    batch = worlds.pack([world])
+    keep = {0, 1, 2, 3, 10, 100} | set(range(500, 10001, 500))
+    stacked, kept, el = _run(world, model_id="cells.model.resolved_pump_tissue@1", dt=1e-3,
+                             steps=10000, keep=keep, solver=ars)
+    _save("ars222_grid4x4.npz", batch, stacked, kept, dt=1e-3,
+          model_id="cells.model.resolved_pump_tissue@1", solver=ars, elapsed=el)
+
+    keep = {0, 1, 2, 10, 50, 100, 200}
+    stacked, kept, el = _run(world, model_id="cells.model.resolved_pump_tissue@3", dt=1e-3,
+                             steps=200, keep=keep, solver=ars)
+    _save("ars222_v3_grid4x4.npz", batch, stacked, kept, dt=1e-3,
+          model_id="cells.model.resolved_pump_tissue@3", solver=ars, elapsed=el)
+
+    gated = worlds.grid_world(3, 3, worlds.world_rng(7, 0), junction_sigma=0.3,
+                              gate=(0.015, 0.1, 0.6))
+    gated.bath_potential = -0.004
+    rng = np.random.default_rng(11)
+    controls = dict(
+        membrane_control=rng.uniform(0.5, 1.0, gated.cells),
+        junction_control=rng.uniform(0.5, 1.0, gated.edges),
+        pump_control=rng.uniform(0.5, 1.0, gated.cells),
+    )
+    batch = worlds.pack([gated])
+    keep = {0, 1, 2, 5, 50, 100, 200, 400}
+    stacked, kept, el = _run(gated, model_id="cells.model.resolved_pump_tissue@1", dt=1e-3,
+                             steps=400, keep=keep, solver=ars, controls=controls)
+    _save("ars222_gated.npz", batch, stacked, kept, dt=1e-3,
+          model_id="cells.model.resolved_pump_tissue@1", solver=ars, elapsed=el,
+          extra={"control_" + k.split("_")[0]: v for k, v in controls.items()})
+
+    keep = {0, 1, 2, 10, 50, 100}
+    stacked, kept, el = _run(world, model_id="cells.model.resolved_pump_tissue@1", dt=1e-4,
+                             steps=100, keep=keep, solver="rk4")
+    _save("rk4_grid4x4.npz", worlds.pack([world]), stacked, kept, dt=1e-4,
+          model_id="cells.model.resolved_pump_tissue@1", solver="rk4", elapsed=el)
+
+
+def make_laws():
+    from cells.laws import electrochemistry as ec
+    from cells.laws.junctions import junction_voltage_relaxation as jg
+    from cells.laws.pumps import nak_atp_mass_action_positive as pump
+
+    x = np.concatenate([
+        -np.logspace(-8, np.log10(50), 200)[::-1], [0.0],
+        np.logspace(-8, np.log10(50), 200), [-1e-4, 1e-4, -9.999e-5, 9.999e-5],
+    ])  # fmt: skip
+    b = ec.bernoulli(x, xp=np)
+    rng = np.random.default_rng(3)
+    n = 500
+    na = np.exp(rng.uniform(np.log(0.5), np.log(60.0), n))
+    ko = np.exp(rng.uniform(np.log(1.0), np.log(20.0), n))
+    mu_na = rng.uniform(-25000.0, 5000.0, n)
+    mu_k = rng.uniform(-5000.0, 25000.0, n)
+    cap = np.exp(rng.uniform(np.log(1e-3), np.log(0.1), n))
+    avail = rng.uniform(0.0, 1.0, n)
+    avail[:5] = 0.0
+    params = pump.Parameters(cap, 1.5, 0.1, 0.1, 12.0, 0.2, 0.5, -37000.0)
+    rates = pump.kinetics(na, ko, mu_na, mu_k, 310.15, params, avail, xp=np)
+    v = rng.uniform(-0.12, 0.12, n)
+    g = rng.uniform(0.1, 1.0, n)
+    thr = rng.uniform(0.0, 0.05, n)
+    gate = jg.rhs(g, v, jg.Parameters(thr, 0.1), xp=np)
+    np.savez_compressed(
+        os.path.join(HERE, "laws.npz"), bernoulli_x=x, bernoulli=b,
+        pump_na=na, pump_ko=ko, pump_mu_na=mu_na, pump_mu_k=mu_k, pump_capacity=cap,
+        pump_availability=avail, pump_cycles=rates.cycles_fmol_s,
+        pump_energy=rates.cycle_free_energy_J_mol, pump_drive=rates.chemical_drive_J_mol,
+        gate_g=g, gate_v=v, gate_threshold=thr, gate_rate=gate,
+    )  # fmt: skip
+    print("laws.npz written")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=("laws", "trajectories"))
+    args = ap.parse_args()
+    _setup(args.reference)
+    if args.only in (None, "laws"):
+        make_laws()
+    if args.only in (None, "trajectories"):
+        make_trajectories()
+
+
+if __name__ == "__main__":
+    main()
