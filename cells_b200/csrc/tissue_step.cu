@@ -50,8 +50,6 @@ constexpr double kMaxAbsX = 50.0;
 constexpr double kMaxAbsJunctionV = 0.120;
 constexpr double kMaxAbsIonPotentialOverRT = 1600.0;
 constexpr double kMaxAbsAffinityOverRT = 80.0;
-constexpr double kChargeAtol = 3e-25;
-constexpr double kChargeRtol = 2e-12;
 constexpr double kLog0065 = -2.7333680090865;  // log(0.065), the gate law's closing constant
 
 // Per-world constants (host-computed with the reference's expressions), stride in doubles.
@@ -69,7 +67,10 @@ enum WorldConst {
   WC_RTDOM,   // rt of the pump domain predicate
   WC_PUMPOK,  // 1 when temperature and pump parameters lie in the law's domain
   WC_MUB,     // 3: bath mu (RT log co + z F Vb)
-  WC_STRIDE = WC_MUB + 3 + 1
+  WC_FRT = WC_MUB + 3,  // F / RT
+  WC_INVRT,   // 1 / RT
+  WC_INVRTD,  // 1 / rt of the pump domain predicate
+  WC_STRIDE
 };
 
 struct Tissue {
@@ -81,16 +82,16 @@ struct Tissue {
   const int *adj_ptr;      // [C+1], global cell -> adjacency entries
   const int *adj_idx;      // local edge index << 1 | (1 if the cell is the receiver)
   const double *world;     // [W * WC_STRIDE]
-  const double *vol;       // [C]
+  const double *ivol;      // [C] 1 / volume
   const double *ref;       // [3][C]
-  const double *ap;        // [3][C]  area * permeability
-  const double *cap;       // [C]
+  const double *ap;        // [3][C]  area * permeability / 1e-15 (fmol/s per mM)
+  const double *icap;      // [C] 1 / capacitance
   const double *q0;        // [C]
   const double *pcap;      // [C]
   const double *logpcap;   // [C] log of the pump capacity where positive, else 0
   const int *snd;          // [E] local
   const int *rcv;          // [E] local
-  const double *jap;       // [3][E]  junction area * permeability
+  const double *jap;       // [3][E]  junction area * permeability / 1e-15
   const double *thr;       // [E]
   const double *jmin;      // [E]
 };
@@ -181,7 +182,8 @@ template <int BLOCK, int EPT>
 __device__ __forceinline__ void stage_rates(
     const Tissue &T, const double *__restrict__ wc, int c0, int e0, int nc, int ne, int i,
     bool has_cell, const double (&n)[3], double V, const double (&g)[EPT],
-    double mc, double pc_ctl, const double (&jc)[EPT], double *sV, double *sC, double *sL,
+    double mc, double pc_ctl, double log_drive_cap, const double (&jc)[EPT], double *sV,
+    double *sC, double *sL,
     double *sJ, Cell &rate, Edge (&erate)[EPT], double (&inflow)[3], uint32_t &bits) {
   const double RT = wc[WC_RT];
   const double Vb = wc[WC_VB];
@@ -189,10 +191,10 @@ __device__ __forceinline__ void stage_rates(
   double jm[3] = {0.0, 0.0, 0.0}, extra[3] = {0.0, 0.0, 0.0};
   if (has_cell) {
     const int gi = c0 + i;
-    const double vol = __ldg(T.vol + gi);
+    const double ivol = __ldg(T.ivol + gi);
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
-      c[s] = (__ldg(T.ref + (size_t)s * T.C + gi) + n[s]) / vol;
+      c[s] = (__ldg(T.ref + (size_t)s * T.C + gi) + n[s]) * ivol;
       lc[s] = log(c[s]);
       if (!(finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
       sC[s * BLOCK + i] = c[s];
@@ -202,14 +204,14 @@ __device__ __forceinline__ void stage_rates(
     if (!finite(V)) bits |= CB_WORLD_TRANSPORT;
     // Patch: constant-field flux per species (selective_flux with residual 0, gate 1).
     const double dv = V - Vb;
-    const double x = (kF * dv) / RT;
+    const double x = dv * wc[WC_FRT];
     if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
     double bp, bm;
     bernoulli_pair(x, bp, bm);
     double mu[3];
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
-      const double gs = (__ldg(T.ap + (size_t)s * T.C + gi) * mc) / 1e-15;
+      const double gs = __ldg(T.ap + (size_t)s * T.C + gi) * mc;
       const double co = wc[WC_CO + s];
       // Na, K: z = +1 -> (c_in B(-x) - c_out B(x)); Cl: z = -1 swaps the pair.
       jm[s] = (s < 2) ? gs * (c[s] * bm - co * bp) : gs * (c[s] * bp - co * bm);
@@ -227,12 +229,12 @@ __device__ __forceinline__ void stage_rates(
     // Na/K-ATPase (nak_atp_mass_action_positive.kinetics), Na inside, K in the bath.
     const double drive = wc[WC_DRIVE];
     const double energy = (drive + (-3.0) * mu[0]) + 2.0 * mu[1];
-    const double a = energy / RT;
+    const double a = energy * wc[WC_INVRT];
     const double ls = ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
     const double capacity = __ldg(T.pcap + gi);
     double cycles = 0.0;
     if (capacity > 0.0 && pc_ctl > 0.0) {
-      const double mag = exp(((__ldg(T.logpcap + gi) + log(pc_ctl)) + ls) + fmax(a, 0.0));
+      const double mag = exp((log_drive_cap + ls) + fmax(a, 0.0));
       const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
       cycles = mag * dep;
     }
@@ -243,8 +245,7 @@ __device__ __forceinline__ void stage_rates(
     extra[1] = -2.0 * cycles;
     extra[2] = -0.0 * cycles;
     // Pump domain (positive substrates, parameters, |mu/RT| <= 1600, |affinity| <= 80).
-    const double rtd = wc[WC_RTDOM];
-    const double sna = mu[0] / rtd, sk = mu[1] / rtd;
+    const double sna = mu[0] * wc[WC_INVRTD], sk = mu[1] * wc[WC_INVRTD];
     const double aff = (wc[WC_AFF0] + (-3.0) * sna) + 2.0 * sk;
     const bool pump_ok = wc[WC_PUMPOK] != 0.0 && finite(capacity) && capacity >= 0.0 &&
                          finite(sna) && fabs(sna) <= kMaxAbsIonPotentialOverRT && finite(sk) &&
@@ -263,14 +264,14 @@ __device__ __forceinline__ void stage_rates(
       const int s_ = __ldg(T.snd + ge), r_ = __ldg(T.rcv + ge);
       const double dv = sV[s_] - sV[r_];
       const double opening = jc[k] * g[k];
-      const double x = (kF * dv) / RT;
+      const double x = dv * wc[WC_FRT];
       if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
       double bp, bm;
       bernoulli_pair(x, bp, bm);
       double jj[3], mu[3];
 #pragma unroll
       for (int s = 0; s < 3; ++s) {
-        const double gs = (__ldg(T.jap + (size_t)s * T.E + ge) * opening) / 1e-15;
+        const double gs = __ldg(T.jap + (size_t)s * T.E + ge) * opening;
         const double cs = sC[s * BLOCK + s_], cr = sC[s * BLOCK + r_];
         jj[s] = (s < 2) ? gs * (cs * bm - cr * bp) : gs * (cs * bp - cr * bm);
         const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
 
   // Load the world's state into registers.
   Cell y;
-  double mc = 0.0, pctl = 0.0, cap = 1.0, q0 = 0.0;
+  double mc = 0.0, pctl = 0.0, icap = 1.0, q0 = 0.0, log_drive_cap = 0.0;
   if (has_cell) {
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
@@ -369,8 +370,10 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     y.mw = state_in[L.s[CB_METABOLIC_WORK] + gi];
     mc = control[L.c[CB_CONTROL_MEMBRANE] + gi];
     pctl = control[L.c[CB_CONTROL_PUMP] + gi];
-    cap = __ldg(T.cap + gi);
+    icap = __ldg(T.icap + gi);
     q0 = __ldg(T.q0 + gi);
+    // log(capacity) + log(availability) of the pump's magnitude, constant over the launch.
+    if (pctl > 0.0) log_drive_cap = __ldg(T.logpcap + gi) + log(pctl);
   } else {
 #pragma unroll
     for (int s = 0; s < 3; ++s) y.n[s] = y.mt[s] = 0.0;
@@ -407,11 +410,10 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
   const double Vb = sW[WC_VB];
 
   // Bath plate charge of the charge-only increment (surface_tissue.capacitor_change): sum over
-  // the world's cells of -C_i dp_i, dp_i = q_i / C_i.
+  // the world's cells of -C_i dp_i with dp_i = q_i / C_i, i.e. -q_i.
   auto plate = [&](const double (&n)[3]) -> double {
     if (!has_cell) return 0.0;
-    const double q = kChargePerFmol * ((n[0] + n[1]) + (-n[2]));
-    return -cap * (q / cap);
+    return -(kChargePerFmol * ((n[0] + n[1]) + (-n[2])));
   };
   double plate0;
   {
@@ -426,14 +428,15 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     uint32_t bits = 0u;
     // Stage 0: start potential from the capacitor solve, Q / C plus the bath potential.
     const double Q0 = q0 + kChargePerFmol * ((y.n[0] + y.n[1]) + (-y.n[2]));
-    const double V0 = Q0 / cap + Vb;
+    const double V0 = Q0 * icap + Vb;
     Cell k0;
     Edge k0e[EPT];
     double in0[3];
     double g0[EPT];
 #pragma unroll
     for (int q = 0; q < EPT; ++q) g0[q] = ye[q].g;
-    stage_rates<BLOCK, EPT>(T, sW, c0, e0, nc, ne, i, has_cell, y.n, V0, g0, mc, pctl, jc, sV,
+    stage_rates<BLOCK, EPT>(T, sW, c0, e0, nc, ne, i, has_cell, y.n, V0, g0, mc, pctl,
+                            log_drive_cap, jc, sV,
                             sC, sL, sJ, k0, k0e, in0, bits);
     // Stage 1 state (only amounts and gates feed the next rates) and the final accumulator.
     double n1[3], g1[EPT];
@@ -459,17 +462,16 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     }
     // Stage 1 potential: the IMEX operator (capacitor only, no faces) solve.
     const double Q1 = q0 + kChargePerFmol * ((n1[0] + n1[1]) + (-n1[2]));
-    const double V1 = Q1 / cap + Vb;
-    if (has_cell) {
-      const double image = cap * (V1 - Vb);
-      const double scale = fmax(fabs(Q1), fabs(image));
-      if (!(finite(V1) && fabs(image - Q1) <= kChargeAtol + kChargeRtol * scale))
-        bits |= CB_WORLD_RESIDUAL;
-    }
+    const double V1 = Q1 * icap + Vb;
+    // The stage's charge residual (surface_imex.solve_operator): the operator is diagonal on the
+    // cells here, so Q/C leaves a residual within an ulp of Q and only a non-finite potential can
+    // exceed 3e-25 C + 2e-12 |Q|.
+    if (has_cell && !finite(V1)) bits |= CB_WORLD_RESIDUAL;
     Cell k1;
     Edge k1e[EPT];
     double in1[3];
-    stage_rates<BLOCK, EPT>(T, sW, c0, e0, nc, ne, i, has_cell, n1, V1, g1, mc, pctl, jc, sV,
+    stage_rates<BLOCK, EPT>(T, sW, c0, e0, nc, ne, i, has_cell, n1, V1, g1, mc, pctl,
+                            log_drive_cap, jc, sV,
                             sC, sL, sJ, k1, k1e, in1, bits);
     Cell y2;
     Edge y2e[EPT];
@@ -492,11 +494,8 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     // The last stage's potential solve (its residual is part of the step's acceptance).
     if (has_cell) {
       const double Q2 = q0 + kChargePerFmol * ((y2.n[0] + y2.n[1]) + (-y2.n[2]));
-      const double V2 = Q2 / cap + Vb;
-      const double image = cap * (V2 - Vb);
-      const double scale = fmax(fabs(Q2), fabs(image));
-      if (!(finite(V2) && fabs(image - Q2) <= kChargeAtol + kChargeRtol * scale))
-        bits |= CB_WORLD_RESIDUAL;
+      const double V2 = Q2 * icap + Vb;
+      if (!finite(V2)) bits |= CB_WORLD_RESIDUAL;
       // Accepted-state domain: positive finite amounts and finite ledgers.
       bool ok = true;
 #pragma unroll
@@ -636,9 +635,7 @@ __global__ void __launch_bounds__(BLOCK) balances_kernel(const Tissue T, const L
       di[s] = n[s];
     }
     metabolic = fabs(st[L.s[CB_METABOLIC_WORK] + gi] + 1e-3 * sW[WC_DRIVE] * pc);
-    const double cap = T.cap[gi];
-    const double q = kChargePerFmol * ((n[0] + n[1]) + (-n[2]));
-    pl = -cap * (q / cap);
+    pl = -(kChargePerFmol * ((n[0] + n[1]) + (-n[2])));
   }
   double v[7] = {moved[0], moved[1], moved[2], di[0], di[1], di[2], pl};
   block_sum<BLOCK, 7>(v, sRed);
@@ -902,16 +899,23 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
     c[WC_AFF0] = (((dg0 / rtd + std::log(s_adp)) + std::log(s_pi)) - std::log(s_atp)) - ln1000;
     c[WC_RTDOM] = rtd;
     c[WC_PUMPOK] = ok ? 1.0 : 0.0;
+    c[WC_FRT] = kF / RT;
+    c[WC_INVRT] = 1.0 / RT;
+    c[WC_INVRTD] = 1.0 / rtd;
   }
-  std::vector<double> ap(3 * C), jap(3 * E), logpcap(C);
+  // Route conductance prefactors A P / (1e-15 mol/fmol) (selective_flux's), and reciprocals.
+  std::vector<double> ap(3 * C), jap(3 * E), logpcap(C), ivol(C), icap(C);
   for (int s = 0; s < 3; ++s) {
     for (long long c = 0; c < C; ++c)
-      ap[s * C + c] = d->area[c] * d->permeability[s * C + c];
+      ap[s * C + c] = d->area[c] * d->permeability[s * C + c] / 1e-15;
     for (long long e = 0; e < E; ++e)
-      jap[s * E + e] = d->junction_area[e] * d->junction_permeability[s * E + e];
+      jap[s * E + e] = d->junction_area[e] * d->junction_permeability[s * E + e] / 1e-15;
   }
-  for (long long c = 0; c < C; ++c)
+  for (long long c = 0; c < C; ++c) {
     logpcap[c] = d->pump_capacity[c] > 0 ? std::log(d->pump_capacity[c]) : 0.0;
+    ivol[c] = 1.0 / d->volume[c];
+    icap[c] = 1.0 / d->capacitance[c];
+  }
 
   cudaError_t ce = cudaSetDevice(device);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
@@ -942,10 +946,10 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
   if (!rc) rc = upload(t, adj_ptr, &T.adj_ptr);
   if (!rc) rc = upload(t, adj_idx, &T.adj_idx);
   if (!rc) rc = upload(t, world, &T.world);
-  if (!rc) rc = upload(t, vec(d->volume, C), &T.vol);
+  if (!rc) rc = upload(t, ivol, &T.ivol);
   if (!rc) rc = upload(t, vec(d->amount_reference, 3 * C), &T.ref);
   if (!rc) rc = upload(t, ap, &T.ap);
-  if (!rc) rc = upload(t, vec(d->capacitance, C), &T.cap);
+  if (!rc) rc = upload(t, icap, &T.icap);
   if (!rc) rc = upload(t, vec(d->initial_charge, C), &T.q0);
   if (!rc) rc = upload(t, vec(d->pump_capacity, C), &T.pcap);
   if (!rc) rc = upload(t, logpcap, &T.logpcap);
