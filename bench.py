@@ -42,13 +42,14 @@ BYTES_PER_CELL_STEP = 441.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=100)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--side", type=int, default=16)
     ap.add_argument("--dt", type=float, default=1e-3)
-    ap.add_argument("--fuse", type=int, default=1, help="time steps per kernel launch")
+    ap.add_argument("--fuse", type=int, default=100,
+                    help="time steps per kernel launch (the largest divisor of --steps up to it)")
     ap.add_argument("--e2e-calls", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -223,9 +224,7 @@ def main():
     batch = build_batch(args.worlds, args.side, rank)
     tissue = Tissue(batch, device=local_rank)
     cells = batch.cells
-    fuse = max(1, args.fuse)
-    if args.steps % fuse:
-        raise SystemExit("--steps must be a multiple of --fuse")
+    fuse = max(d for d in range(1, max(1, min(args.fuse, args.steps)) + 1) if args.steps % d == 0)
     state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
     control = torch.from_numpy(tissue.pack_control()).to(dev)
     status = torch.zeros(batch.worlds, dtype=torch.int32, device=dev)
@@ -236,8 +235,10 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    for _ in range(max(1, args.warmup // fuse)):
-        tissue.step(state, state, control, args.dt, fuse, status, stream=handle)
+    left = max(args.warmup, 1)
+    while left > 0:  # warm-up steps, in launches of at most `fuse` steps
+        tissue.step(state, state, control, args.dt, min(fuse, left), status, stream=handle)
+        left -= fuse
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)

@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -163,38 +164,43 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *red) {
   }
 }
 
-struct Cell {
-  double n[3];   // amount increments
-  double mt[3];  // membrane transferred
-  double md, pc, pd, mw;
-};
-
-struct Edge {
-  double jt[3];
-  double jd, g;
-};
-
-// Rates of one explicit stage (surface_pump.explicit_rates) for this thread's cell and edges.
-// n/g are the stage amounts and gates, V the stage potential of this thread's cell (sV holds
-// every cell's). Returns the cell's amount and ledger rates, the edges' rates, and the cell's
-// contribution to the bath inflow (patch flux plus pump transfer, per species).
-template <int BLOCK, int EPT>
-__device__ __forceinline__ void stage_rates(
-    const Tissue &T, const double *__restrict__ wc, int c0, int e0, int nc, int ne, int i,
-    bool has_cell, const double (&n)[3], double V, const double (&g)[EPT],
-    double mc, double pc_ctl, double log_drive_cap, const double (&jc)[EPT], double *sV,
-    double *sC, double *sL,
-    double *sJ, Cell &rate, Edge (&erate)[EPT], double (&inflow)[3], uint32_t &bits) {
+// One explicit stage (surface_pump.explicit_rates, surface_pump.py:158-240) for this thread's
+// cell and junction slots, each rate folded into the step accumulator as soon as it is formed
+// (surface_pump._combine's y + (w dt) k, one term at a time):
+//   FIRST  (stage 0): acc = y + (delta dt) k, with y read from `cur`; and the stage-1 amounts
+//                     and gates n1 = n + (gamma dt) k_n, g1 = g + (gamma dt) k_g;
+//   !FIRST (stage 1): acc = acc + ((1 - delta) dt) k.
+// n, g: the stage's amounts and gates; V: this thread's cell potential. sA/sE hold the cell and
+// junction accumulators in slots private to each thread. inflow: this cell's patch flux plus pump
+// transfer (the held bath's inflow terms).
+template <int BLOCK, int EPT, bool FIRST>
+__device__ __forceinline__ void stage(
+    const Tissue &T, const Layout &L, const double *__restrict__ wc, const StepCoef &k,
+    const double *cur, int c0, int e0, int ne, int i, bool has_cell, const double (&n)[3],
+    double V, const double (&g)[EPT], double mc, double pc_ctl, double log_drive_cap,
+    const double *__restrict__ jctl, double *sV, double *sC, double *sL, double *sJ, double *sA,
+    double *sE, double (&n1)[3], double (&g1)[EPT], double (&inflow)[3], uint32_t &bits) {
+  constexpr int EB = EPT * BLOCK;
+  const double w = FIRST ? k.delta_dt : k.omdelta_dt;
+  const long long C = T.C, E = T.E;
   const double RT = wc[WC_RT];
   const double Vb = wc[WC_VB];
-  double c[3], lc[3];
+  const int gi = c0 + i;
+  // Accumulate one cell ledger field f (slot f of sA) with rate r.
+  auto cell_acc = [&](int f, long long off, double r) {
+    double *slot = sA + f * BLOCK + i;
+    if (FIRST)
+      *slot = cur[off + gi] + w * r;
+    else
+      *slot = *slot + w * r;
+  };
   double jm[3] = {0.0, 0.0, 0.0}, extra[3] = {0.0, 0.0, 0.0};
   if (has_cell) {
-    const int gi = c0 + i;
+    double c[3], lc[3];
     const double ivol = __ldg(T.ivol + gi);
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
-      c[s] = (__ldg(T.ref + (size_t)s * T.C + gi) + n[s]) * ivol;
+      c[s] = (__ldg(T.ref + s * C + gi) + n[s]) * ivol;
       lc[s] = log(c[s]);
       if (!(finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
       sC[s * BLOCK + i] = c[s];
@@ -211,17 +217,17 @@ __device__ __forceinline__ void stage_rates(
     double mu[3];
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
-      const double gs = __ldg(T.ap + (size_t)s * T.C + gi) * mc;
+      const double gs = __ldg(T.ap + s * C + gi) * mc;
       const double co = wc[WC_CO + s];
       // Na, K: z = +1 -> (c_in B(-x) - c_out B(x)); Cl: z = -1 swaps the pair.
       jm[s] = (s < 2) ? gs * (c[s] * bm - co * bp) : gs * (c[s] * bp - co * bm);
       const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
       mu[s] = RT * (lc[s] - wc[WC_LOGCO + s]) + zfdv;
+      cell_acc(3 + s, L.s[CB_MEMBRANE_TRANSFERRED] + s * C, jm[s]);
     }
-    rate.md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
-#pragma unroll
-    for (int s = 0; s < 3; ++s) rate.mt[s] = jm[s];
-    if (!(finite(jm[0]) && finite(jm[1]) && finite(jm[2]) && finite(rate.md)))
+    const double md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
+    cell_acc(6, L.s[CB_MEMBRANE_DISSIPATED], md);
+    if (!(finite(jm[0]) && finite(jm[1]) && finite(jm[2]) && finite(md)))
       bits |= CB_WORLD_TRANSPORT;
     if (!(finite(mc) && mc >= 0.0 && mc <= 1.0 && finite(pc_ctl) && pc_ctl >= 0.0 &&
           pc_ctl <= 1.0))
@@ -230,40 +236,45 @@ __device__ __forceinline__ void stage_rates(
     const double drive = wc[WC_DRIVE];
     const double energy = (drive + (-3.0) * mu[0]) + 2.0 * mu[1];
     const double a = energy * wc[WC_INVRT];
-    const double ls = ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
-    const double capacity = __ldg(T.pcap + gi);
     double cycles = 0.0;
-    if (capacity > 0.0 && pc_ctl > 0.0) {
+    if (__ldg(T.pcap + gi) > 0.0 && pc_ctl > 0.0) {
+      const double ls =
+          ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
       const double mag = exp((log_drive_cap + ls) + fmax(a, 0.0));
       const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
       cycles = mag * dep;
     }
-    rate.pc = cycles;
-    rate.pd = (-1e-3 * cycles) * energy;
-    rate.mw = (-1e-3 * cycles) * drive;
-    extra[0] = 3.0 * cycles;   // -stoichiometry * cycles, outward-positive
+    const double pd = (-1e-3 * cycles) * energy;
+    const double mw = (-1e-3 * cycles) * drive;
+    cell_acc(7, L.s[CB_PUMP_CYCLES], cycles);
+    cell_acc(8, L.s[CB_PUMP_DISSIPATED], pd);
+    cell_acc(9, L.s[CB_METABOLIC_WORK], mw);
+    extra[0] = 3.0 * cycles;  // -stoichiometry * cycles, outward-positive
     extra[1] = -2.0 * cycles;
     extra[2] = -0.0 * cycles;
     // Pump domain (positive substrates, parameters, |mu/RT| <= 1600, |affinity| <= 80).
     const double sna = mu[0] * wc[WC_INVRTD], sk = mu[1] * wc[WC_INVRTD];
     const double aff = (wc[WC_AFF0] + (-3.0) * sna) + 2.0 * sk;
+    const double capacity = __ldg(T.pcap + gi);
     const bool pump_ok = wc[WC_PUMPOK] != 0.0 && finite(capacity) && capacity >= 0.0 &&
                          finite(sna) && fabs(sna) <= kMaxAbsIonPotentialOverRT && finite(sk) &&
                          fabs(sk) <= kMaxAbsIonPotentialOverRT && finite(aff) &&
                          fabs(aff) <= kMaxAbsAffinityOverRT;
     if (!pump_ok) bits |= CB_WORLD_PUMP_DOMAIN;
-    if (!(finite(cycles) && finite(rate.pd) && finite(rate.mw))) bits |= CB_WORLD_TRANSPORT;
+    if (!(finite(cycles) && finite(pd) && finite(mw))) bits |= CB_WORLD_TRANSPORT;
   }
   __syncthreads();
-  // Edge phase.
+  // Edge phase: each junction once, its fluxes to shared memory for the gather.
 #pragma unroll
-  for (int k = 0; k < EPT; ++k) {
-    const int e = threadIdx.x + k * BLOCK;
+  for (int q = 0; q < EPT; ++q) {
+    const int e = threadIdx.x + q * BLOCK;
+    g1[q] = g[q];
     if (e < ne) {
       const int ge = e0 + e;
       const int s_ = __ldg(T.snd + ge), r_ = __ldg(T.rcv + ge);
       const double dv = sV[s_] - sV[r_];
-      const double opening = jc[k] * g[k];
+      const double jc = __ldg(jctl + e);
+      const double opening = jc * g[q];
       const double x = dv * wc[WC_FRT];
       if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
       double bp, bm;
@@ -271,15 +282,14 @@ __device__ __forceinline__ void stage_rates(
       double jj[3], mu[3];
 #pragma unroll
       for (int s = 0; s < 3; ++s) {
-        const double gs = __ldg(T.jap + (size_t)s * T.E + ge) * opening;
+        const double gs = __ldg(T.jap + s * E + ge) * opening;
         const double cs = sC[s * BLOCK + s_], cr = sC[s * BLOCK + r_];
         jj[s] = (s < 2) ? gs * (cs * bm - cr * bp) : gs * (cs * bp - cr * bm);
         const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
         mu[s] = RT * (sL[s * BLOCK + s_] - sL[s * BLOCK + r_]) + zfdv;
-        sJ[s * (EPT * BLOCK) + e] = jj[s];
-        erate[k].jt[s] = jj[s];
+        sJ[s * EB + e] = jj[s];
       }
-      erate[k].jd = 1e-3 * ((jj[0] * mu[0] + jj[1] * mu[1]) + jj[2] * mu[2]);
+      const double jd = 1e-3 * ((jj[0] * mu[0] + jj[1] * mu[1]) + jj[2] * mu[2]);
       // Junction gate (junction_voltage_relaxation.rhs); pinned gates (minimum 1) are exactly 0.
       const double thr = __ldg(T.thr + ge), mn = __ldg(T.jmin + ge);
       double gr = 0.0;
@@ -288,23 +298,33 @@ __device__ __forceinline__ void stage_rates(
         const double alpha = 1.3 * exp(-77.0 * shift);
         const double log_beta = kLog0065 + 140.0 * shift;
         const double beta = 20.0 * exp(-logaddexp0(-log_beta));
-        gr = alpha * (1.0 - g[k]) - beta * (g[k] - mn);
+        gr = alpha * (1.0 - g[q]) - beta * (g[q] - mn);
       }
-      erate[k].g = gr;
-      if (!(finite(jj[0]) && finite(jj[1]) && finite(jj[2]) && finite(erate[k].jd) &&
-            finite(gr)))
+      if (FIRST) {
+#pragma unroll
+        for (int s = 0; s < 3; ++s)
+          sE[s * EB + e] = cur[L.s[CB_JUNCTION_TRANSFERRED] + s * E + ge] + w * jj[s];
+        sE[3 * EB + e] = cur[L.s[CB_JUNCTION_DISSIPATED] + ge] + w * jd;
+        sE[4 * EB + e] = g[q] + w * gr;
+        g1[q] = g[q] + k.gamma_dt * gr;
+      } else {
+#pragma unroll
+        for (int s = 0; s < 3; ++s) sE[s * EB + e] = sE[s * EB + e] + w * jj[s];
+        sE[3 * EB + e] = sE[3 * EB + e] + w * jd;
+        sE[4 * EB + e] = sE[4 * EB + e] + w * gr;
+      }
+      if (!(finite(jj[0]) && finite(jj[1]) && finite(jj[2]) && finite(jd) && finite(gr)))
         bits |= CB_WORLD_TRANSPORT;
       const bool gate_ok = finite(thr) && thr >= 0.0 && thr <= kMaxAbsJunctionV && finite(mn) &&
                            mn >= 0.0 && mn <= 1.0 && finite(dv) && fabs(dv) <= kMaxAbsJunctionV &&
-                           finite(g[k]) && g[k] >= mn && g[k] <= 1.0 && finite(jc[k]) &&
-                           jc[k] >= 0.0 && jc[k] <= 1.0;
+                           finite(g[q]) && g[q] >= mn && g[q] <= 1.0 && finite(jc) &&
+                           jc >= 0.0 && jc <= 1.0;
       if (!gate_ok) bits |= CB_WORLD_GATE_DOMAIN;
     }
   }
   __syncthreads();
-  // Gather phase: cell rate = ((-J_m + sum_send(-J)) + sum_recv(J)) - extra.
+  // Gather phase: amount rate = ((-J_m + sum_send(-J)) + sum_recv(J)) - extra.
   if (has_cell) {
-    const int gi = c0 + i;
     double send[3] = {0.0, 0.0, 0.0}, recv[3] = {0.0, 0.0, 0.0};
     const int a0 = __ldg(T.adj_ptr + gi), a1 = __ldg(T.adj_ptr + gi + 1);
     for (int a = a0; a < a1; ++a) {
@@ -312,36 +332,58 @@ __device__ __forceinline__ void stage_rates(
       const int e = code >> 1;
       if (code & 1) {
 #pragma unroll
-        for (int s = 0; s < 3; ++s) recv[s] += sJ[s * (EPT * BLOCK) + e];
+        for (int s = 0; s < 3; ++s) recv[s] += sJ[s * EB + e];
       } else {
 #pragma unroll
-        for (int s = 0; s < 3; ++s) send[s] += -sJ[s * (EPT * BLOCK) + e];
+        for (int s = 0; s < 3; ++s) send[s] += -sJ[s * EB + e];
       }
     }
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
-      rate.n[s] = ((-jm[s] + send[s]) + recv[s]) - extra[s];
+      const double rate = ((-jm[s] + send[s]) + recv[s]) - extra[s];
       inflow[s] = jm[s] + extra[s];
-      if (!finite(rate.n[s])) bits |= CB_WORLD_TRANSPORT;
+      if (!finite(rate)) bits |= CB_WORLD_TRANSPORT;
+      if (FIRST) {
+        n1[s] = n[s] + k.gamma_dt * rate;
+        sA[s * BLOCK + i] = n[s] + w * rate;
+      } else {
+        sA[s * BLOCK + i] = sA[s * BLOCK + i] + w * rate;
+      }
     }
   } else {
 #pragma unroll
-    for (int s = 0; s < 3; ++s) inflow[s] = 0.0;
+    for (int s = 0; s < 3; ++s) {
+      inflow[s] = 0.0;
+      if (FIRST) n1[s] = 0.0;
+    }
   }
 }
 
-template <int BLOCK, int EPT>
-__global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
+// Shared-memory words of one step CTA: stage potentials, concentrations and their logs, junction
+// fluxes, the step accumulator (cells, junctions) and the reduction scratch.
+__host__ __device__ constexpr size_t step_smem_words(int block, int ept) {
+  return (size_t)(7 * block + 3 * ept * block + 10 * block + 5 * ept * block + (block / 32) * 8);
+}
+
+// The ARS(2,2,2) step of surface_pump.imex_step (surface_pump.py:259-362) for one world per CTA,
+// n_steps times. Registers hold only one stage's transients: the step's start state is read from
+// global memory (the launch's input, then this CTA's own last accepted state, which stays in L2
+// across fused steps), and the accumulator y + delta dt k0 + (1 - delta) dt k1 lives in shared
+// memory, in slots private to each thread.
+template <int BLOCK, int EPT, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
     ars222_kernel(const Tissue T, const Layout L, const double *state_in, double *state_out,
-                  const double *__restrict__ control,
-                  const StepCoef k, int n_steps, uint32_t *__restrict__ world_status,
-                  int32_t *__restrict__ accepted_steps) {
+                  const double *__restrict__ control, const StepCoef k, int n_steps,
+                  uint32_t *__restrict__ world_status, int32_t *__restrict__ accepted_steps) {
+  constexpr int EB = EPT * BLOCK;
   extern __shared__ double smem[];
-  double *sV = smem;                   // [BLOCK]
-  double *sC = sV + BLOCK;             // [3][BLOCK]
-  double *sL = sC + 3 * BLOCK;         // [3][BLOCK]
-  double *sJ = sL + 3 * BLOCK;         // [3][EPT*BLOCK]
-  double *sRed = sJ + 3 * EPT * BLOCK; // [BLOCK/32][8]
+  double *sV = smem;            // [BLOCK]
+  double *sC = sV + BLOCK;      // [3][BLOCK]
+  double *sL = sC + 3 * BLOCK;  // [3][BLOCK]
+  double *sJ = sL + 3 * BLOCK;  // [3][EB]
+  double *sA = sJ + 3 * EB;     // [10][BLOCK]: n[3], mt[3], md, pc, pd, mw
+  double *sE = sA + 10 * BLOCK; // [5][EB]: jt[3], jd, g
+  double *sRed = sE + 5 * EB;   // [BLOCK/32][8]
   __shared__ double sW[WC_STRIDE];
   __shared__ unsigned int sBits;
 
@@ -354,70 +396,35 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
   const bool has_cell = tid < nc;
   const int i = tid;
   const int gi = c0 + i;
+  const long long C = T.C, E = T.E;
 
-  // Load the world's state into registers.
-  Cell y;
-  double mc = 0.0, pctl = 0.0, icap = 1.0, q0 = 0.0, log_drive_cap = 0.0;
+  double mc = 0.0, pctl = 0.0, log_drive_cap = 0.0;
   if (has_cell) {
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      y.n[s] = state_in[L.s[CB_AMOUNT_INCREMENT] + (long long)s * T.C + gi];
-      y.mt[s] = state_in[L.s[CB_MEMBRANE_TRANSFERRED] + (long long)s * T.C + gi];
-    }
-    y.md = state_in[L.s[CB_MEMBRANE_DISSIPATED] + gi];
-    y.pc = state_in[L.s[CB_PUMP_CYCLES] + gi];
-    y.pd = state_in[L.s[CB_PUMP_DISSIPATED] + gi];
-    y.mw = state_in[L.s[CB_METABOLIC_WORK] + gi];
     mc = control[L.c[CB_CONTROL_MEMBRANE] + gi];
     pctl = control[L.c[CB_CONTROL_PUMP] + gi];
-    icap = __ldg(T.icap + gi);
-    q0 = __ldg(T.q0 + gi);
     // log(capacity) + log(availability) of the pump's magnitude, constant over the launch.
     if (pctl > 0.0) log_drive_cap = __ldg(T.logpcap + gi) + log(pctl);
-  } else {
-#pragma unroll
-    for (int s = 0; s < 3; ++s) y.n[s] = y.mt[s] = 0.0;
-    y.md = y.pc = y.pd = y.mw = 0.0;
   }
-  Edge ye[EPT];
-  double jc[EPT];
-#pragma unroll
-  for (int q = 0; q < EPT; ++q) {
-    const int e = tid + q * BLOCK;
-    if (e < ne) {
-      const int ge = e0 + e;
-#pragma unroll
-      for (int s = 0; s < 3; ++s)
-        ye[q].jt[s] = state_in[L.s[CB_JUNCTION_TRANSFERRED] + (long long)s * T.E + ge];
-      ye[q].jd = state_in[L.s[CB_JUNCTION_DISSIPATED] + ge];
-      ye[q].g = state_in[L.s[CB_JUNCTION_GATE] + ge];
-      jc[q] = control[L.c[CB_CONTROL_JUNCTION] + ge];
-    } else {
-#pragma unroll
-      for (int s = 0; s < 3; ++s) ye[q].jt[s] = 0.0;
-      ye[q].jd = 0.0;
-      ye[q].g = 1.0;
-      jc[q] = 0.0;
-    }
-  }
+  const double *jctl = control + L.c[CB_CONTROL_JUNCTION] + e0;
   double res[3];
 #pragma unroll
-  for (int s = 0; s < 3; ++s) res[s] = state_in[L.s[CB_RESERVOIR_SUPPLIED] + (long long)s * T.W + w];
+  for (int s = 0; s < 3; ++s) res[s] = state_in[L.s[CB_RESERVOIR_SUPPLIED] + s * (long long)T.W + w];
   double ec = state_in[L.s[CB_ELECTRODE_CHARGE] + w];
   double rw = state_in[L.s[CB_RESERVOIR_WORK] + w];
   double ew = state_in[L.s[CB_ELECTRODE_WORK] + w];
   __syncthreads();
   const double Vb = sW[WC_VB];
 
-  // Bath plate charge of the charge-only increment (surface_tissue.capacitor_change): sum over
-  // the world's cells of -C_i dp_i with dp_i = q_i / C_i, i.e. -q_i.
-  auto plate = [&](const double (&n)[3]) -> double {
-    if (!has_cell) return 0.0;
-    return -(kChargePerFmol * ((n[0] + n[1]) + (-n[2])));
-  };
+  // Bath plate charge of the charge-only increment (surface_tissue.capacitor_change): the sum
+  // over the world's cells of -C_i dp_i with dp_i = q_i / C_i, i.e. -q_i.
+  const double *cur = state_in;
   double plate0;
   {
-    double v[1] = {plate(y.n)};
+    double v[1] = {0.0};
+    if (has_cell) {
+      const double *n = cur + L.s[CB_AMOUNT_INCREMENT] + gi;
+      v[0] = -(kChargePerFmol * ((n[0] + n[C]) + (-n[2 * C])));
+    }
     block_sum<BLOCK, 1>(v, sRed);
     plate0 = v[0];
   }
@@ -426,99 +433,62 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
   uint32_t refused = 0u;
   for (int step = 0; step < n_steps; ++step) {
     uint32_t bits = 0u;
-    // Stage 0: start potential from the capacitor solve, Q / C plus the bath potential.
-    const double Q0 = q0 + kChargePerFmol * ((y.n[0] + y.n[1]) + (-y.n[2]));
-    const double V0 = Q0 * icap + Vb;
-    Cell k0;
-    Edge k0e[EPT];
-    double in0[3];
-    double g0[EPT];
-#pragma unroll
-    for (int q = 0; q < EPT; ++q) g0[q] = ye[q].g;
-    stage_rates<BLOCK, EPT>(T, sW, c0, e0, nc, ne, i, has_cell, y.n, V0, g0, mc, pctl,
-                            log_drive_cap, jc, sV,
-                            sC, sL, sJ, k0, k0e, in0, bits);
-    // Stage 1 state (only amounts and gates feed the next rates) and the final accumulator.
-    double n1[3], g1[EPT];
-    Cell acc;
-    Edge acce[EPT];
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      n1[s] = y.n[s] + k.gamma_dt * k0.n[s];
-      acc.n[s] = y.n[s] + k.delta_dt * k0.n[s];
-      acc.mt[s] = y.mt[s] + k.delta_dt * k0.mt[s];
-    }
-    acc.md = y.md + k.delta_dt * k0.md;
-    acc.pc = y.pc + k.delta_dt * k0.pc;
-    acc.pd = y.pd + k.delta_dt * k0.pd;
-    acc.mw = y.mw + k.delta_dt * k0.mw;
-#pragma unroll
-    for (int q = 0; q < EPT; ++q) {
-      g1[q] = ye[q].g + k.gamma_dt * k0e[q].g;
-#pragma unroll
-      for (int s = 0; s < 3; ++s) acce[q].jt[s] = ye[q].jt[s] + k.delta_dt * k0e[q].jt[s];
-      acce[q].jd = ye[q].jd + k.delta_dt * k0e[q].jd;
-      acce[q].g = ye[q].g + k.delta_dt * k0e[q].g;
-    }
-    // Stage 1 potential: the IMEX operator (capacitor only, no faces) solve.
-    const double Q1 = q0 + kChargePerFmol * ((n1[0] + n1[1]) + (-n1[2]));
-    const double V1 = Q1 * icap + Vb;
-    // The stage's charge residual (surface_imex.solve_operator): the operator is diagonal on the
-    // cells here, so Q/C leaves a residual within an ulp of Q and only a non-finite potential can
-    // exceed 3e-25 C + 2e-12 |Q|.
-    if (has_cell && !finite(V1)) bits |= CB_WORLD_RESIDUAL;
-    Cell k1;
-    Edge k1e[EPT];
-    double in1[3];
-    stage_rates<BLOCK, EPT>(T, sW, c0, e0, nc, ne, i, has_cell, n1, V1, g1, mc, pctl,
-                            log_drive_cap, jc, sV,
-                            sC, sL, sJ, k1, k1e, in1, bits);
-    Cell y2;
-    Edge y2e[EPT];
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      y2.n[s] = acc.n[s] + k.omdelta_dt * k1.n[s];
-      y2.mt[s] = acc.mt[s] + k.omdelta_dt * k1.mt[s];
-    }
-    y2.md = acc.md + k.omdelta_dt * k1.md;
-    y2.pc = acc.pc + k.omdelta_dt * k1.pc;
-    y2.pd = acc.pd + k.omdelta_dt * k1.pd;
-    y2.mw = acc.mw + k.omdelta_dt * k1.mw;
-#pragma unroll
-    for (int q = 0; q < EPT; ++q) {
-#pragma unroll
-      for (int s = 0; s < 3; ++s) y2e[q].jt[s] = acce[q].jt[s] + k.omdelta_dt * k1e[q].jt[s];
-      y2e[q].jd = acce[q].jd + k.omdelta_dt * k1e[q].jd;
-      y2e[q].g = acce[q].g + k.omdelta_dt * k1e[q].g;
-    }
-    // The last stage's potential solve (its residual is part of the step's acceptance).
+    // Stage 0 at the step's start: potential from the capacitor solve, Q / C plus the bath's.
+    double n0[3] = {0.0, 0.0, 0.0}, g0[EPT];
+    double icap = 1.0, q0 = 0.0;
     if (has_cell) {
-      const double Q2 = q0 + kChargePerFmol * ((y2.n[0] + y2.n[1]) + (-y2.n[2]));
-      const double V2 = Q2 * icap + Vb;
-      if (!finite(V2)) bits |= CB_WORLD_RESIDUAL;
-      // Accepted-state domain: positive finite amounts and finite ledgers.
+#pragma unroll
+      for (int s = 0; s < 3; ++s) n0[s] = cur[L.s[CB_AMOUNT_INCREMENT] + s * C + gi];
+      icap = __ldg(T.icap + gi);
+      q0 = __ldg(T.q0 + gi);
+    }
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+      const int e = tid + q * BLOCK;
+      g0[q] = e < ne ? cur[L.s[CB_JUNCTION_GATE] + e0 + e] : 1.0;
+    }
+    const double V0 = (q0 + kChargePerFmol * ((n0[0] + n0[1]) + (-n0[2]))) * icap + Vb;
+    double n1[3], g1[EPT], in0[3], in1[3];
+    stage<BLOCK, EPT, true>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n0, V0, g0, mc, pctl,
+                            log_drive_cap, jctl, sV, sC, sL, sJ, sA, sE, n1, g1, in0, bits);
+    // Stage 1 potential: the IMEX operator (capacitor only, no faces) solve. The operator is
+    // diagonal on the cells, so Q/C leaves a charge residual within an ulp of Q and only a
+    // non-finite potential exceeds 3e-25 C + 2e-12 |Q| (surface_imex.solve_operator).
+    const double V1 = (q0 + kChargePerFmol * ((n1[0] + n1[1]) + (-n1[2]))) * icap + Vb;
+    if (has_cell && !finite(V1)) bits |= CB_WORLD_RESIDUAL;
+    {
+      double nd[3], gd[EPT];
+      stage<BLOCK, EPT, false>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n1, V1, g1, mc, pctl,
+                               log_drive_cap, jctl, sV, sC, sL, sJ, sA, sE, nd, gd, in1, bits);
+    }
+    // The new state's domain (surface_kinetic.domain_valid): positive amounts, finite ledgers,
+    // gates in [minimum, 1].
+    if (has_cell) {
       bool ok = true;
 #pragma unroll
-      for (int s = 0; s < 3; ++s) {
-        const double amt = __ldg(T.ref + (size_t)s * T.C + gi) + y2.n[s];
-        ok = ok && finite(amt) && amt > 0.0 && finite(y2.mt[s]);
-      }
-      ok = ok && finite(y2.md) && finite(y2.pc) && finite(y2.pd) && finite(y2.mw);
+      for (int f = 0; f < 10; ++f) ok = ok && finite(sA[f * BLOCK + i]);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) ok = ok && (__ldg(T.ref + s * C + gi) + sA[s * BLOCK + i]) > 0.0;
+      const double q2 = q0 + kChargePerFmol * ((sA[i] + sA[BLOCK + i]) + (-sA[2 * BLOCK + i]));
+      if (!finite(q2 * icap + Vb)) bits |= CB_WORLD_RESIDUAL;
       if (!ok) bits |= CB_WORLD_DOMAIN;
     }
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
       const int e = tid + q * BLOCK;
       if (e < ne) {
-        const double mn = __ldg(T.jmin + e0 + e);
-        const bool ok = finite(y2e[q].jt[0]) && finite(y2e[q].jt[1]) && finite(y2e[q].jt[2]) &&
-                        finite(y2e[q].jd) && finite(y2e[q].g) && y2e[q].g >= mn &&
-                        y2e[q].g <= 1.0;
+        bool ok = true;
+#pragma unroll
+        for (int f = 0; f < 5; ++f) ok = ok && finite(sE[f * EB + e]);
+        const double g = sE[4 * EB + e];
+        ok = ok && g >= __ldg(T.jmin + e0 + e) && g <= 1.0;
         if (!ok) bits |= CB_WORLD_DOMAIN;
       }
     }
-    // World sums: bath inflow of both stages and the end plate charge.
-    double v[7] = {in0[0], in0[1], in0[2], in1[0], in1[1], in1[2], plate(y2.n)};
+    // World sums: the bath inflow of both stages and the end plate charge.
+    double v[7] = {in0[0], in0[1], in0[2], in1[0], in1[1], in1[2], 0.0};
+    if (has_cell)
+      v[6] = -(kChargePerFmol * ((sA[i] + sA[BLOCK + i]) + (-sA[2 * BLOCK + i])));
     block_sum<BLOCK, 7>(v, sRed);
     double res2[3], applied[3];
 #pragma unroll
@@ -540,14 +510,34 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     if (bits) atomicOr(&sBits, bits);
     __syncthreads();
     const uint32_t world_bits = sBits;
-    __syncthreads();
     if (world_bits) {
       refused = world_bits;
       break;
     }
-    y = y2;
+    // Commit the accepted state (each thread its own slots).
+    if (has_cell) {
 #pragma unroll
-    for (int q = 0; q < EPT; ++q) ye[q] = y2e[q];
+      for (int s = 0; s < 3; ++s) {
+        state_out[L.s[CB_AMOUNT_INCREMENT] + s * C + gi] = sA[s * BLOCK + i];
+        state_out[L.s[CB_MEMBRANE_TRANSFERRED] + s * C + gi] = sA[(3 + s) * BLOCK + i];
+      }
+      state_out[L.s[CB_MEMBRANE_DISSIPATED] + gi] = sA[6 * BLOCK + i];
+      state_out[L.s[CB_PUMP_CYCLES] + gi] = sA[7 * BLOCK + i];
+      state_out[L.s[CB_PUMP_DISSIPATED] + gi] = sA[8 * BLOCK + i];
+      state_out[L.s[CB_METABOLIC_WORK] + gi] = sA[9 * BLOCK + i];
+    }
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+      const int e = tid + q * BLOCK;
+      if (e < ne) {
+        const long long ge = e0 + e;
+#pragma unroll
+        for (int s = 0; s < 3; ++s)
+          state_out[L.s[CB_JUNCTION_TRANSFERRED] + s * E + ge] = sE[s * EB + e];
+        state_out[L.s[CB_JUNCTION_DISSIPATED] + ge] = sE[3 * EB + e];
+        state_out[L.s[CB_JUNCTION_GATE] + ge] = sE[4 * EB + e];
+      }
+    }
 #pragma unroll
     for (int s = 0; s < 3; ++s) res[s] = res2[s];
     ec = ec2;
@@ -555,35 +545,32 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     ew = ew2;
     plate0 = v[6];
     ++taken;
+    cur = state_out;
   }
 
-  // Store the world's state.
-  if (has_cell) {
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      state_out[L.s[CB_AMOUNT_INCREMENT] + (long long)s * T.C + gi] = y.n[s];
-      state_out[L.s[CB_MEMBRANE_TRANSFERRED] + (long long)s * T.C + gi] = y.mt[s];
+  // A world refused at its first step keeps its input state.
+  if (taken == 0 && state_in != state_out) {
+    if (has_cell) {
+      for (int f = CB_AMOUNT_INCREMENT; f <= CB_METABOLIC_WORK; ++f) {
+        const int reps = (f <= CB_MEMBRANE_TRANSFERRED) ? 3 : 1;
+        for (int s = 0; s < reps; ++s)
+          state_out[L.s[f] + s * C + gi] = state_in[L.s[f] + s * C + gi];
+      }
     }
-    state_out[L.s[CB_MEMBRANE_DISSIPATED] + gi] = y.md;
-    state_out[L.s[CB_PUMP_CYCLES] + gi] = y.pc;
-    state_out[L.s[CB_PUMP_DISSIPATED] + gi] = y.pd;
-    state_out[L.s[CB_METABOLIC_WORK] + gi] = y.mw;
-  }
-#pragma unroll
-  for (int q = 0; q < EPT; ++q) {
-    const int e = tid + q * BLOCK;
-    if (e < ne) {
-      const int ge = e0 + e;
-#pragma unroll
-      for (int s = 0; s < 3; ++s)
-        state_out[L.s[CB_JUNCTION_TRANSFERRED] + (long long)s * T.E + ge] = ye[q].jt[s];
-      state_out[L.s[CB_JUNCTION_DISSIPATED] + ge] = ye[q].jd;
-      state_out[L.s[CB_JUNCTION_GATE] + ge] = ye[q].g;
+    for (int q = 0; q < EPT; ++q) {
+      const int e = tid + q * BLOCK;
+      if (e < ne) {
+        for (int f = CB_JUNCTION_TRANSFERRED; f <= CB_JUNCTION_GATE; ++f) {
+          const int reps = (f == CB_JUNCTION_TRANSFERRED) ? 3 : 1;
+          for (int s = 0; s < reps; ++s)
+            state_out[L.s[f] + s * E + e0 + e] = state_in[L.s[f] + s * E + e0 + e];
+        }
+      }
     }
   }
   if (tid == 0) {
 #pragma unroll
-    for (int s = 0; s < 3; ++s) state_out[L.s[CB_RESERVOIR_SUPPLIED] + (long long)s * T.W + w] = res[s];
+    for (int s = 0; s < 3; ++s) state_out[L.s[CB_RESERVOIR_SUPPLIED] + s * (long long)T.W + w] = res[s];
     state_out[L.s[CB_ELECTRODE_CHARGE] + w] = ec;
     state_out[L.s[CB_RESERVOIR_WORK] + w] = rw;
     state_out[L.s[CB_ELECTRODE_WORK] + w] = ew;
@@ -713,6 +700,7 @@ struct cb_tissue {
   int device = 0;
   int W = 0, C = 0, E = 0;
   int block = 0, ept = 0;
+  int occupancy = 3;  // target resident 256-thread CTAs per SM (3, measured faster, or 2)
   Tissue t{};
   Layout layout{};
   long long state_total = 0, control_total = 0;
@@ -740,9 +728,7 @@ int upload(cb_tissue *t, const std::vector<T> &host, const T **dst) {
   return CB_OK;
 }
 
-size_t step_smem(int block, int ept) {
-  return sizeof(double) * (size_t)(7 * block + 3 * ept * block + (block / 32) * 8);
-}
+size_t step_smem(int block, int ept) { return sizeof(double) * step_smem_words(block, ept); }
 
 size_t balances_smem(int block, int ept) {
   return sizeof(double) * (size_t)(3 * ept * block + (block / 32) * 8);
@@ -753,7 +739,13 @@ int launch_step(cb_tissue *t, const double *in, double *out, const double *contr
                 const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
                 cudaStream_t stream) {
   const size_t smem = step_smem(BLOCK, EPT);
-  auto kern = ars222_kernel<BLOCK, EPT>;
+  // Resident CTAs per SM that the register budget targets: 128-thread CTAs at 2 (no spills),
+  // 256-thread CTAs at 2 (no spills) or 3 (a few spilled words), larger CTAs at 1.
+  constexpr int kMin = BLOCK <= 256 ? 2 : 1;
+  auto kern = ars222_kernel<BLOCK, EPT, kMin>;
+  if constexpr (BLOCK == 256) {
+    if (t->occupancy == 3) kern = ars222_kernel<BLOCK, EPT, 3>;
+  }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
@@ -926,6 +918,7 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
   t->E = (int)E;
   t->block = block;
   t->ept = ept;
+  if (const char *env = std::getenv("CELLS_B200_OCCUPANCY")) t->occupancy = std::atoi(env) == 2 ? 2 : 3;
   std::vector<int> co32(W + 1), eo32(W + 1), snd(E), rcv(E);
   for (int w = 0; w <= W; ++w) {
     co32[w] = (int)d->cell_offset[w];
