@@ -65,12 +65,13 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_cell_step():
-    """DRAM bytes per world·cell·step of the step kernel from the committed ncu summary."""
+def traffic_per_cell_launch():
+    """DRAM bytes per cell per launch of the step kernel (ncu, committed summary): a launch reads
+    and writes its worlds' state once, whatever its step count."""
     path = os.path.join(ROOT, "profiles", "ars222_traffic.json")
     try:
         with open(path) as f:
-            return float(json.load(f)["dram_bytes_per_cell_step"])
+            return float(json.load(f)["dram_bytes_per_cell_per_launch"])
     except (OSError, KeyError, ValueError):
         return None
 
@@ -137,38 +138,43 @@ def build_batch(n_worlds, side, rank):
     return worlds.pack(ws)
 
 
-def cpu_baseline(args, samples_per_core=2, steps=25):
-    """The oracle (the reference's step restated, bit-identical) over all host cores."""
+def cpu_baseline(args, samples_per_core=2, steps=100):
+    """The oracle (the reference's step restated, bit-identical) over all host cores: a strided
+    sample of the workload's worlds, about 10 s of CPU work."""
     from oracle import cpu_baseline as cb
 
     cores = os.cpu_count() or 1
-    tasks = [("grid", w, 1, args.side, steps, args.dt) for w in range(cores * samples_per_core)]
+    n = cores * samples_per_core
+    stride = max(1, args.worlds // n)
+    tasks = [("grid", w * stride, 1, args.side, steps, args.dt) for w in range(n)]
     cell_steps, wall, procs = cb.measure(tasks, cores)
     return {
         "value": cell_steps / wall,
         "unit": UNIT,
         "cores": procs,
         "kind": "port",
-        "sample": (f"{len(tasks)} of the {args.worlds} worlds ({args.side}x{args.side} grid), "
-                   f"{steps} ARS(2,2,2) steps each, one world per process, 1 BLAS thread, "
+        "sample": (f"{n} of the {args.worlds} worlds (every {stride}th, {args.side}x{args.side} "
+                   f"grid), {steps} ARS(2,2,2) steps each, one world per process, 1 BLAS thread, "
                    f"{wall:.1f} s wall"),
     }
 
 
 def run_reference(args, rank):
+    """The reference's CPU step (its oracle restatement) on the host cores: each bench step
+    advances a strided sample of the workload's worlds (two per core) by ten time steps."""
     if rank != 0:
         return 0
     from oracle import cpu_baseline as cb
 
     cores = os.cpu_count() or 1
-    steps = 25
-    tasks = [("grid", w, 1, args.side, steps, args.dt) for w in range(cores * 2)]
-    import multiprocessing as mp
-
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
+    n = cores * 2
+    stride = max(1, args.worlds // n)
+    per_task = 10
+    tasks = [("grid", w * stride, 1, args.side, per_task, args.dt) for w in range(n)]
+    with cb.pool(cores) as pool:
+        pool.map(cb.prepare, tasks, chunksize=1)
         for _ in range(max(args.warmup, 0)):
-            pool.map(cb.run_world, tasks[:cores], chunksize=1)
+            pool.map(cb.run_world, tasks, chunksize=1)
         t0 = time.perf_counter()
         done = 0
         for _ in range(args.steps):
@@ -176,17 +182,19 @@ def run_reference(args, rank):
             done += sum(r[0] for r in res)
         wall = time.perf_counter() - t0
     value = done / wall
+    sample = (f"{n} of the {args.worlds} worlds (every {stride}th, {args.side}x{args.side} grid) "
+              f"advanced {per_task} ARS(2,2,2) steps per bench step, one world per process, "
+              "1 BLAS thread")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"batched plain step sample: {len(tasks)} worlds of "
-                               f"{args.side}x{args.side} cells x {steps} steps per bench step",
-                   "method": METHOD},
+        "data": "synthetic (seeded 16x16-grid pump-leak tissues)", "impl": "reference",
+        "config": {"workload": (f"batched plain step: {args.worlds} worlds x {args.side}x"
+                                f"{args.side} grid tissues, FP64, dt {args.dt:g} s (sampled)"),
+                   "method": METHOD, "sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{len(tasks)} worlds x {steps} steps per bench step, "
-                                   "one world per process, 1 BLAS thread"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -306,7 +314,7 @@ def main():
         per_launch_s = ms * 1e-3 / launches
         algorithmic = BYTES_PER_CELL_STEP * cells * fuse
         achieved = algorithmic / per_launch_s / 1e9
-        traffic = traffic_per_cell_step()
+        traffic = traffic_per_cell_launch()
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -325,7 +333,7 @@ def main():
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": None if traffic is None else traffic * cells * fuse,
+                "traffic": None if traffic is None else traffic * cells,
                 "algorithmic_bytes_per_launch": algorithmic, "launch_ms": per_launch_s * 1e3,
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,

@@ -1,0 +1,219 @@
+"""Drop-in for the reference's checked step on its own pytrees.
+
+The reference resolves a model module whose hot entry is
+``checked_step(state, dt, control, p, active) -> (state, valid)``
+(src/cells/models/surface_pump.py:365-369, src/cells/models/surface_pump_v3.py:3989) on
+NamedTuple pytrees: ``state`` of STATE_TYPE (src/cells/models/surface_kinetic.py:36-44 with
+src/cells/models/surface_tissue.py:31-45), ``p`` the bound layout, ``control`` a
+SurfaceKineticControl (src/cells/execution/schedule.py:18-22), all padded to capacities with
+``*_active`` masks. ``DeviceStep(p)`` binds such a layout once (host analysis, upload) and is
+then called with the reference's own arguments; it returns a new state of the same type (inputs
+are never mutated) and ``valid``, the unchanged state when the step is refused, like the
+reference (surface_pump.py:362).
+
+Scope: the held-bath pump-leak tissue — every active cell has exactly one active membrane
+patch, every patch faces its world's held bath (a reservoir outside node), no faces, no channel
+population, species Na/K/Cl (+1/+1/-1), the Na/K-ATPase with one set of pump constants per
+world. Other worlds raise ``Unsupported`` at bind; nothing falls back to the CPU.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import worlds
+from .tissue import Tissue
+
+ARS222_ID = "cells.solver.imex_ars222_face_electromigration@1"
+PUMP_FIELDS = ("atp_mM", "adp_mM", "pi_mM", "km_na_mM", "km_k_mM", "km_atp_mM",
+               "delta_g0_J_mol")
+
+
+class Unsupported(ValueError):
+    """The layout is outside the device step's scope (module docstring)."""
+
+
+def _a(p, name):
+    return np.asarray(getattr(p, name))
+
+
+def _active(p, name, size):
+    if hasattr(p, name):
+        return _a(p, name).astype(bool)
+    return np.ones(size, dtype=bool)
+
+
+class Mapping:
+    """Active-entity indices of one reference layout, in the reference's slot order."""
+
+    def __init__(self, p):
+        cell_active = _a(p, "active").astype(bool) if hasattr(p, "active") else _a(
+            p, "cell_active").astype(bool)
+        self.cells = np.flatnonzero(cell_active)
+        membrane_active = _active(p, "membrane_active", _a(p, "membrane_cell").size)
+        self.membranes = np.flatnonzero(membrane_active)
+        junction_active = _active(p, "junction_active", _a(p, "junction_sender").size)
+        self.junctions = np.flatnonzero(junction_active)
+        reservoir = _a(p, "reservoir").astype(bool)
+        outside_active = _active(p, "outside_active", reservoir.size)
+        self.baths = np.flatnonzero(reservoir & outside_active)
+        # One patch per cell, in cell order.
+        owner = _a(p, "membrane_cell")[self.membranes]
+        if sorted(owner.tolist()) != self.cells.tolist():
+            raise Unsupported("every active cell needs exactly one active membrane patch")
+        self.patch_of_cell = self.membranes[np.argsort(owner, kind="stable")]
+        outside = _a(p, "membrane_outside")[self.patch_of_cell]
+        if self.baths.size != 1 or np.any(outside != self.baths[0]):
+            raise Unsupported("every patch must face the world's one held bath")
+        if np.any(outside_active & ~reservoir):
+            raise Unsupported("finite (unheld) outside nodes need the field solve")
+        if hasattr(p, "face_active") and np.any(_a(p, "face_active")):
+            raise Unsupported("extracellular faces need the field solve")
+        if hasattr(p, "channel_active") and np.any(_a(p, "channel_active")):
+            raise Unsupported("channel populations are not in the device step yet")
+        self.bath = int(self.baths[0])
+        local = -np.ones(cell_active.size, dtype=np.int64)
+        local[self.cells] = np.arange(self.cells.size)
+        self.sender = local[_a(p, "junction_sender")[self.junctions]]
+        self.receiver = local[_a(p, "junction_receiver")[self.junctions]]
+
+
+def world_from_layout(p):
+    """One reference layout -> (worlds.World, Mapping)."""
+    m = Mapping(p)
+    valence = _a(p, "valence").reshape(-1)
+    if not np.array_equal(valence, worlds.VALENCE):
+        raise Unsupported("species must be Na, K, Cl with valences +1, +1, -1")
+    patch = m.patch_of_cell
+    if hasattr(p, "pump_present"):
+        present = _a(p, "pump_present")[patch].astype(bool)
+        stoich = _a(p, "stoichiometry")[:, patch]
+        if np.any(stoich[:, present] != worlds.STOICHIOMETRY[:, None]):
+            raise Unsupported("pumps must move 3 Na out and 2 K in per cycle")
+        if np.any(_a(p, "pump_sodium_species")[patch][present] != worlds.SODIUM) or np.any(
+                _a(p, "pump_potassium_species")[patch][present] != worlds.POTASSIUM):
+            raise Unsupported("pump roles must be Na (sodium) and K (potassium)")
+        capacity = np.where(present, _a(p, "pump_capacity")[patch], 0.0)
+        constants = []
+        for name in PUMP_FIELDS:
+            v = _a(p, "pump_" + name)[patch][present]
+            if v.size and np.any(v != v[0]):
+                raise Unsupported(f"pump {name} must be one value per world")
+            constants.append(float(v[0]) if v.size else 1.0)
+    else:
+        capacity = np.zeros(m.cells.size)
+        constants = [1.5, 0.1, 0.1, 12.0, 0.2, 0.5, -37000.0]
+    bath_volume = float(_a(p, "extracellular_volume")[m.bath])
+    bath_amount = _a(p, "extracellular_amount_reference")[:, m.bath]
+    n = m.cells.size
+    world = worlds.World(
+        volume=_a(p, "volume")[m.cells].astype(float),
+        area=_a(p, "membrane_area")[patch].astype(float),
+        capacitance=_a(p, "membrane_capacitance")[patch].astype(float),
+        permeability=_a(p, "membrane_permeability")[:, patch].astype(float),
+        pump_capacity=capacity.astype(float),
+        amount=_a(p, "amount_reference")[:, m.cells].astype(float),
+        fixed_charge_fmol=np.zeros(n),
+        initial_charge=_a(p, "initial_cell_charge_C")[m.cells].astype(float),
+        sender=m.sender,
+        receiver=m.receiver,
+        junction_area=_a(p, "junction_area")[m.junctions].astype(float),
+        junction_permeability=_a(p, "junction_permeability")[:, m.junctions].astype(float),
+        gate_threshold=_a(p, "junction_threshold_voltage")[m.junctions].astype(float),
+        gate_minimum=_a(p, "junction_minimum")[m.junctions].astype(float),
+        gate_initial=np.ones(m.junctions.size),
+        temperature=float(_a(p, "temperature")),
+        bath_mM=bath_amount / bath_volume,
+        bath_volume=bath_volume,
+        bath_potential=float(_a(p, "boundary_V")[m.bath]),
+        pump=tuple(constants),
+    )
+    return world, m
+
+
+# Reference state fields <-> packed fields (one world; the bath at mapping.bath).
+_CELL_MAP = (
+    ("amount_increment", "amount_increment", "cell"),
+    ("membrane_transferred", "membrane_transferred", "patch"),
+    ("membrane_dissipated_energy_pJ", "membrane_dissipated", "patch"),
+    ("pump_cycles", "pump_cycles", "patch"),
+    ("pump_dissipated_energy_pJ", "pump_dissipated", "patch"),
+    ("metabolic_work_pJ", "metabolic_work", "patch"),
+)
+_EDGE_MAP = (
+    ("junction_transferred", "junction_transferred"),
+    ("junction_dissipated_energy_pJ", "junction_dissipated"),
+    ("junction_gate", "junction_gate"),
+)
+_BATH_MAP = (
+    ("reservoir_supplied", "reservoir_supplied"),
+    ("electrode_charge_transferred_C", "electrode_charge"),
+    ("reservoir_work_pJ", "reservoir_work"),
+    ("electrode_work_pJ", "electrode_work"),
+)
+_ZERO_FIELDS = ("extracellular_amount_increment", "face_transferred",
+                "face_dissipated_energy_pJ", "channel_transferred",
+                "channel_dissipated_energy_pJ")
+
+
+def packed_state(state, m):
+    """Reference state (one world) -> packed dict of the device layout."""
+    out = {}
+    for ref, name, kind in _CELL_MAP:
+        v = np.asarray(getattr(state, ref))
+        idx = m.cells if kind == "cell" else m.patch_of_cell
+        out[name] = v[..., idx].astype(float)
+    for ref, name in _EDGE_MAP:
+        out[name] = np.asarray(getattr(state, ref))[..., m.junctions].astype(float)
+    for ref, name in _BATH_MAP:
+        out[name] = np.asarray(getattr(state, ref))[..., m.bath:m.bath + 1].astype(float)
+    return out
+
+
+def reference_state(packed, like, m):
+    """Packed dict -> a new reference state of like's type (like's padding kept)."""
+    fields = {k: np.array(v, copy=True) for k, v in like._asdict().items()}
+    for ref, name, kind in _CELL_MAP:
+        idx = m.cells if kind == "cell" else m.patch_of_cell
+        fields[ref][..., idx] = packed[name]
+    for ref, name in _EDGE_MAP:
+        fields[ref][..., m.junctions] = packed[name]
+    for ref, name in _BATH_MAP:
+        fields[ref][..., m.bath:m.bath + 1] = packed[name]
+    return type(like)(**fields)
+
+
+class DeviceStep:
+    """checked_step(state, dt, control, p, active) of the held-bath pump tissue on the device.
+
+    Bind once per layout: ``step = DeviceStep(p)``; then ``state, valid = step(state, dt,
+    control, p, active)`` as the reference's checked_step. ``solver`` is the layout's IMEX
+    method; only ARS(2,2,2) (the reference's imex_ars222_face_electromigration@1) runs here."""
+
+    def __init__(self, p, device=0, solver=ARS222_ID):
+        if solver != ARS222_ID:
+            raise Unsupported(f"solver {solver} is not in the device step")
+        if hasattr(p, "imex_explicit") and np.asarray(p.imex_explicit).shape[0] != 3:
+            raise Unsupported("the layout's tableau is not ARS(2,2,2)")
+        world, self.mapping = world_from_layout(p)
+        self.batch = worlds.pack([world])
+        self.tissue = Tissue(self.batch, device=device)
+
+    def __call__(self, state, dt, control, p=None, active=None):
+        for name in _ZERO_FIELDS:
+            if hasattr(state, name) and np.any(np.asarray(getattr(state, name)) != 0):
+                raise Unsupported(f"{name} must stay zero in a held-bath tissue")
+        m = self.mapping
+        packed = packed_state(state, m)
+        ctl = self.tissue.pack_control(
+            membrane=np.asarray(control.membrane)[m.patch_of_cell],
+            junction=np.asarray(control.junction)[m.junctions],
+            pump=np.asarray(control.pump)[m.patch_of_cell],
+        )
+        out, status, _ = self.tissue.step_host(self.tissue.pack_state(packed), ctl, float(dt), 1)
+        valid = bool(status[0] == 0)
+        new = reference_state(self.tissue.unpack_state(out), state, m)
+        return new, np.asarray(valid)
+
+    def close(self):
+        self.tissue.close()

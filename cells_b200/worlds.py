@@ -373,8 +373,10 @@ def pack(worlds):
 
 def reference_definition(world, *, dt, steps, model="cells.model.resolved_pump_tissue@1",
                          solver="cells.solver.imex_ars222_face_electromigration@1",
-                         membrane_control=None, junction_control=None, pump_control=None):
-    """One World as a reference definition dict (schema_version 1)."""
+                         membrane_control=None, junction_control=None, pump_control=None,
+                         padding=0):
+    """One World as a reference definition dict (schema_version 1). ``padding`` adds that many
+    inactive slots to every capacity (the reference pads its arrays to capacities)."""
     n, e = world.cells, world.edges
     mc = np.ones(n) if membrane_control is None else np.broadcast_to(membrane_control, (n,))
     jc = np.ones(e) if junction_control is None else np.broadcast_to(junction_control, (e,))
@@ -484,11 +486,11 @@ def reference_definition(world, *, dt, steps, model="cells.model.resolved_pump_t
         },
         "execution": {
             "dt": float(dt),
-            "capacity": n,
-            "extracellular_capacity": 1,
-            "membrane_capacity": n,
-            "edge_capacity": e,
-            "face_capacity": 0,
+            "capacity": n + padding,
+            "extracellular_capacity": 1 + padding,
+            "membrane_capacity": n + padding,
+            "edge_capacity": e + padding,
+            "face_capacity": padding,
             "backend": "cpu",
             "jit": True,
             "precision": "float64",

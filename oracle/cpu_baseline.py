@@ -6,6 +6,9 @@ models/surface_pump.py imex_step, one world per process, BLAS pinned to one thre
 (src/cells/execution/blas_threads.py:28), a pool over the host's cores. The oracle reproduces
 that step bit for bit on the golden worlds (tests/test_oracle_golden.py), so its arithmetic is
 the reference's; its NumPy layout differs only in packing.
+
+Each worker process builds a world once and keeps its state, so a task times only the steps it
+takes (as the reference's runner keeps a world's state between dispatches).
 """
 
 from __future__ import annotations
@@ -13,44 +16,70 @@ from __future__ import annotations
 import os
 import time
 
+_WORLDS = {}
+
 
 def _pin_blas():
     for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[var] = "1"
 
 
+def _world(kind, w, seed, size):
+    key = (kind, w, seed, size)
+    if key not in _WORLDS:
+        from cells_b200 import worlds
+        from oracle import tissue as T
+
+        if kind == "grid":
+            world = worlds.grid_world(size, size, worlds.world_rng(seed, w))
+        else:
+            world = worlds.delaunay_world(size, worlds.world_rng(seed, w))
+        b = worlds.pack([world])
+        _WORLDS[key] = [b, T.topology(b), T.full_control(b), T.initial_state(b)]
+    return _WORLDS[key]
+
+
 def run_world(task):
-    """One world: (kind, world index, seed, side or size, steps, dt) -> (cell-steps, seconds)."""
+    """(kind, world index, seed, side or size, steps, dt) -> (cell-steps, seconds of stepping)."""
     _pin_blas()
-    from cells_b200 import worlds
     from oracle import tissue as T
 
     kind, w, seed, size, steps, dt = task
-    if kind == "grid":
-        world = worlds.grid_world(size, size, worlds.world_rng(seed, w))
-    else:
-        world = worlds.delaunay_world(size, worlds.world_rng(seed, w))
-    b = worlds.pack([world])
-    topo = T.topology(b)
-    ctl = T.full_control(b)
-    st = T.initial_state(b)
+    entry = _world(kind, w, seed, size)
+    b, topo, ctl, st = entry
     t0 = time.perf_counter()
     for _ in range(steps):
-        st, ok = T.ars222_step(st, dt, ctl, b, topo)
+        st, _ = T.ars222_step(st, dt, ctl, b, topo)
     elapsed = time.perf_counter() - t0
-    return world.cells * steps, elapsed
+    entry[3] = st
+    return b.cells * steps, elapsed
 
 
-def measure(tasks, processes=None):
-    """Run the tasks over a spawn pool; returns (cell-steps, wall seconds, processes)."""
+def prepare(task):
+    """Build (and keep) a task's world in this worker without stepping it."""
+    _pin_blas()
+    kind, w, seed, size, _, _ = task
+    _world(kind, w, seed, size)
+    return os.getpid()
+
+
+def pool(processes=None):
     import multiprocessing as mp
 
     _pin_blas()
-    processes = processes or os.cpu_count() or 1
     ctx = mp.get_context("spawn")
-    with ctx.Pool(processes) as pool:
-        pool.map(run_world, [(t[0], t[1], t[2], t[3], 1, t[5]) for t in tasks[:processes]])
+    return ctx.Pool(processes or os.cpu_count() or 1)
+
+
+def measure(tasks, processes=None):
+    """Run the tasks over a spawn pool; returns (cell-steps, wall seconds, processes).
+
+    Every task's world is built in a warm-up pass (one step each) before the timed pass, so the
+    wall time covers stepping and the pool's dispatch only."""
+    processes = processes or os.cpu_count() or 1
+    with pool(processes) as p:
+        p.map(run_world, [t[:4] + (1, t[5]) for t in tasks], chunksize=1)
         t0 = time.perf_counter()
-        results = pool.map(run_world, tasks, chunksize=1)
+        results = p.map(run_world, tasks, chunksize=1)
         wall = time.perf_counter() - t0
     return sum(r[0] for r in results), wall, processes

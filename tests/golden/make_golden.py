@@ -18,6 +18,9 @@ Fixtures:
   ars222_v3_grid4x4.npz  The same world through @3's imex_step for 200 steps (the live model).
   ars222_gated.npz       A 3x3 world with voltage-gated junctions (minimum 0.1), partial controls
                          and a bath at -4 mV, 400 steps at 1 ms (@1).
+  pytrees_gated_padded.npz  The gated world with every capacity 3 above its count: the
+                         reference's own layout fields, controls and padded states (60 steps),
+                         for the drop-in checked step (cells_b200/model.py).
   rk4_grid4x4.npz        The 4x4 world by RK4 at dt 0.1 ms, 100 steps (@1).
   laws.npz               Point laws on grids of inputs: bernoulli, the pump kinetics and the
                          junction gate rate.
@@ -66,6 +69,53 @@ def _batch_arrays(batch):
     from dataclasses import fields
 
     return {"batch_" + f.name: getattr(batch, f.name) for f in fields(batch)}
+
+
+LAYOUT_FIELDS = (
+    "active", "membrane_active", "membrane_cell", "membrane_outside", "junction_active",
+    "junction_sender", "junction_receiver", "reservoir", "outside_active", "face_active",
+    "channel_active", "valence", "temperature", "pump_present", "stoichiometry",
+    "pump_sodium_species", "pump_potassium_species", "pump_capacity", "pump_atp_mM",
+    "pump_adp_mM", "pump_pi_mM", "pump_km_na_mM", "pump_km_k_mM", "pump_km_atp_mM",
+    "pump_delta_g0_J_mol", "extracellular_volume", "extracellular_amount_reference", "volume",
+    "membrane_area", "membrane_capacitance", "membrane_permeability", "amount_reference",
+    "initial_cell_charge_C", "junction_area", "junction_permeability",
+    "junction_threshold_voltage", "junction_minimum", "boundary_V", "imex_explicit",
+)
+
+
+def _run_reference_pytrees(world, *, model_id, dt, steps, keep, padding, controls):
+    """The reference's own pytrees: layout fields, controls and full states (padded slots)."""
+    from cells.definitions.specs import parse_spec
+    from cells.registry.models import get_model
+
+    from cells_b200 import worlds
+
+    raw = worlds.reference_definition(world, dt=dt, steps=steps, model=model_id,
+                                      padding=padding, **controls)
+    spec = parse_spec(raw)
+    model = get_model(spec.model)
+    state, p = model.initial_values(spec)
+    from cells.execution.schedule import control_values
+
+    cv = control_values(spec, [0.0])
+    control = type(cv)(*(v[0] for v in cv))
+    out = {"layout_" + f: np.asarray(getattr(p, f)) for f in LAYOUT_FIELDS}
+    out.update({"control_ref_" + f: np.asarray(v) for f, v in control._asdict().items()})
+    snaps = []
+    for k in range(0, steps + 1):
+        if k:
+            state, ok = model.imex_step(state, dt, control, p, xp=np)[:2]
+            if not bool(ok):
+                raise RuntimeError(f"reference refused step {k}")
+        if k in keep:
+            snaps.append({f: np.asarray(v) for f, v in state._asdict().items()})
+    for f in snaps[0]:
+        out["refstate_" + f] = np.stack([s_[f] for s_ in snaps])
+    out["steps"] = np.asarray(sorted(keep))
+    out["dt"] = np.asarray(dt)
+    out["state_fields"] = np.asarray(list(snaps[0]))
+    return out
 
 
 def _run(world, *, model_id, dt, steps, keep, solver, controls=None):
@@ -151,6 +201,12 @@ def make_trajectories():
     _save("ars222_gated.npz", batch, stacked, kept, dt=1e-3,
           model_id="cells.model.resolved_pump_tissue@1", solver=ars, elapsed=el,
           extra={"control_" + k.split("_")[0]: v for k, v in controls.items()})
+
+    # The reference's own padded pytrees (capacities 3 above the counts) for the drop-in step.
+    out = _run_reference_pytrees(gated, model_id="cells.model.resolved_pump_tissue@1", dt=1e-3,
+                                 steps=60, keep={0, 1, 2, 30, 60}, padding=3, controls=controls)
+    np.savez_compressed(os.path.join(HERE, "pytrees_gated_padded.npz"), **out)
+    print("pytrees_gated_padded.npz written")
 
     keep = {0, 1, 2, 10, 50, 100}
     stacked, kept, el = _run(world, model_id="cells.model.resolved_pump_tissue@1", dt=1e-4,

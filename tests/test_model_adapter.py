@@ -1,0 +1,51 @@
+"""The drop-in checked step's host side (cells_b200/model.py) on the reference's own padded
+pytrees: layout -> packed world, state round trips, refusals of out-of-scope layouts."""
+
+import numpy as np
+import pytest
+
+from cells_b200 import model
+from conftest import load_golden
+from pytree_util import load_pytrees
+
+
+def test_layout_maps_to_the_same_world():
+    _, p, _, _ = load_pytrees()
+    world, m = model.world_from_layout(p)
+    _, b = load_golden("ars222_gated.npz")
+    ref = b.world(0)
+    assert m.cells.tolist() == list(range(9)) and m.bath == 0
+    for name in ("volume", "area", "capacitance", "permeability", "pump_capacity",
+                 "junction_area", "junction_permeability", "gate_threshold", "gate_minimum",
+                 "initial_charge"):
+        assert np.array_equal(getattr(world, name), getattr(ref, name)), name
+    assert np.array_equal(world.sender, ref.sender)
+    assert np.array_equal(world.receiver, ref.receiver)
+    assert np.allclose(world.amount, ref.amount, rtol=0, atol=0)
+    assert world.bath_potential == ref.bath_potential
+    assert world.pump == ref.pump
+
+
+def test_state_round_trip_keeps_padding():
+    _, p, _, states = load_pytrees()
+    _, m = model.world_from_layout(p)
+    for st in states:
+        packed = model.packed_state(st, m)
+        back = model.reference_state(packed, st, m)
+        for f in st._fields:
+            assert np.array_equal(np.asarray(getattr(back, f)), np.asarray(getattr(st, f))), f
+
+
+def test_out_of_scope_layouts_are_refused():
+    _, p, _, _ = load_pytrees()
+    faces = np.asarray(p.face_active).copy()
+    faces[0] = True
+    with pytest.raises(model.Unsupported):
+        model.world_from_layout(p._replace(face_active=faces))
+    channels = np.ones(max(1, np.asarray(p.channel_active).size), dtype=bool)
+    with pytest.raises(model.Unsupported):
+        model.world_from_layout(p._replace(channel_active=channels))
+    outside = np.asarray(p.outside_active).copy()
+    outside[1] = True  # a finite, unheld outside node
+    with pytest.raises(model.Unsupported):
+        model.world_from_layout(p._replace(outside_active=outside))

@@ -195,3 +195,30 @@ def test_device_balances_match_oracle_balances(cuda):
     assert np.all(res[:, 0] <= 1e-12 * scale)
     assert np.allclose(res[:, 7], np.max(np.abs(ref["metabolic_work"].reshape(b.worlds, -1)),
                                          axis=1), rtol=0, atol=1e-9 * np.abs(st.metabolic_work).max())
+
+
+def test_drop_in_checked_step_on_reference_pytrees(cuda):
+    """model.DeviceStep called with the reference's own padded state, control and layout, step
+    by step, against the reference's trajectory; padded slots stay untouched."""
+    from cells_b200 import model
+    from pytree_util import load_pytrees
+
+    z, p, control, states = load_pytrees()
+    step = model.DeviceStep(p)
+    state = states[0]
+    steps = list(z["steps"])
+    done = 0
+    for idx, target in enumerate(steps):
+        while done < target:
+            state, valid = step(state, float(z["dt"]), control, p, p.active)
+            assert bool(valid)
+            done += 1
+        ref = states[idx]
+        assert type(state) is type(ref)
+        for f in ref._fields:
+            got, want = np.asarray(getattr(state, f)), np.asarray(getattr(ref, f))
+            assert got.shape == want.shape, f
+            assert scaled_difference(got, want) <= TRAJECTORY_TOL, f
+    pad = ~np.asarray(p.active).astype(bool)
+    assert np.all(np.asarray(state.amount_increment)[:, pad] == 0)
+    step.close()
