@@ -75,6 +75,14 @@ class World:
     gate_minimum: np.ndarray  # [E]
     gate_initial: np.ndarray  # [E]
     temperature: float = TEMPERATURE_K
+    # Voltage-gated channel populations: NCH slots per cell ([NCH, N]; NCH = 0 for none).
+    # Law codes: 0 Kv1.5 m h, 2 NaV1.2 m^3 h (the reference's catalogue codes), 100 the
+    # Hodgkin-Huxley K n^4 law of this package (channels.HH_K_N4).
+    channel_code: np.ndarray = field(default_factory=lambda: np.zeros((0, 0), dtype=np.int32))
+    channel_species: np.ndarray = field(default_factory=lambda: np.zeros((0, 0), dtype=np.int32))
+    channel_permeability: np.ndarray = field(default_factory=lambda: np.zeros((0, 0)))
+    channel_abundance: np.ndarray = field(default_factory=lambda: np.zeros((0, 0)))
+    channel_gate_initial: np.ndarray = field(default_factory=lambda: np.zeros((2, 0, 0)))
     bath_mM: np.ndarray = field(default_factory=lambda: BATH_mM.copy())
     bath_volume: float = BATH_VOLUME_PL
     bath_potential: float = 0.0
@@ -87,6 +95,39 @@ class World:
     @property
     def edges(self):
         return self.sender.size
+
+    @property
+    def channel_slots(self):
+        return int(self.channel_code.shape[0]) if self.channel_code.size else 0
+
+
+CHANNEL_LAW_IDS = {
+    0: "cells.channel.kv1p5_mh@1",
+    2: "cells.channel.nav1p2_m3h_regularized@1",
+    100: "cells_b200.channel.hh_k_n4@1",
+}
+
+
+def with_channels(world, rng, *, na=("nav", 2e-10, 0.5), k=("kv", 3e-10, 0.5), sigma=0.0):
+    """Give every cell a Na population and a K population. ``na``/``k``: (law, permeability
+    m/s, abundance); laws "nav" (NaV1.2 m^3 h), "kv" (Kv1.5 m h) or "hh" (HH K n^4). Initial gates
+    at the laws' steady state near -60 mV, as fixed values."""
+    n = world.cells
+    codes = {"nav": 2, "kv": 0, "hh": 100}
+    gate0 = {"nav": (0.05, 0.6), "kv": (0.2, 0.7), "hh": (0.32, 0.0)}
+    code = np.array([[codes[na[0]]] * n, [codes[k[0]]] * n], dtype=np.int32)
+    species = np.array([[SODIUM] * n, [POTASSIUM] * n], dtype=np.int32)
+    perm = np.array([[na[1]] * n, [k[1]] * n], dtype=float)
+    if sigma:
+        perm = perm * np.exp(sigma * rng.standard_normal(perm.shape))
+    abundance = np.array([[na[2]] * n, [k[2]] * n], dtype=float)
+    gates = np.zeros((2, 2, n))
+    for slot, law in enumerate((na[0], k[0])):
+        gates[0, slot], gates[1, slot] = gate0[law]
+    world.channel_code, world.channel_species = code, species
+    world.channel_permeability, world.channel_abundance = perm, abundance
+    world.channel_gate_initial = gates
+    return world
 
 
 def anchor_charge(amount, fixed):
@@ -292,6 +333,24 @@ class Batch:
     gate_threshold: np.ndarray  # [E]
     gate_minimum: np.ndarray  # [E]
     gate_initial: np.ndarray  # [E]
+    channel_code: np.ndarray = None  # [NCH, C] int32 (NCH = 0: no channel populations)
+    channel_species: np.ndarray = None  # [NCH, C] int32
+    channel_permeability: np.ndarray = None  # [NCH, C] m/s (max permeability x relative)
+    channel_abundance: np.ndarray = None  # [NCH, C]
+    channel_gate_initial: np.ndarray = None  # [2, NCH, C]
+
+    def __post_init__(self):
+        c = self.cells
+        if self.channel_code is None:
+            self.channel_code = np.zeros((0, c), dtype=np.int32)
+            self.channel_species = np.zeros((0, c), dtype=np.int32)
+            self.channel_permeability = np.zeros((0, c))
+            self.channel_abundance = np.zeros((0, c))
+            self.channel_gate_initial = np.zeros((2, 0, c))
+
+    @property
+    def channel_slots(self):
+        return int(self.channel_code.shape[0])
 
     @property
     def worlds(self):
@@ -326,6 +385,11 @@ class Batch:
             gate_minimum=self.gate_minimum[e0:e1],
             gate_initial=self.gate_initial[e0:e1],
             temperature=float(self.temperature[w]),
+            channel_code=self.channel_code[:, c0:c1],
+            channel_species=self.channel_species[:, c0:c1],
+            channel_permeability=self.channel_permeability[:, c0:c1],
+            channel_abundance=self.channel_abundance[:, c0:c1],
+            channel_gate_initial=self.channel_gate_initial[:, :, c0:c1],
             bath_mM=self.bath_amount[:, w] / self.bath_volume[w],
             bath_volume=float(self.bath_volume[w]),
             bath_potential=float(self.bath_potential[w]),
@@ -337,6 +401,10 @@ def pack(worlds):
     """Pack a list of World into one Batch."""
     cells = np.array([w.cells for w in worlds], dtype=np.int64)
     edges = np.array([w.edges for w in worlds], dtype=np.int64)
+    slots = {w.channel_slots for w in worlds}
+    if len(slots) != 1:
+        raise ValueError("every world of a batch needs the same number of channel slots")
+    nch = slots.pop()
     cat = np.concatenate
 
     def cells_of(name):
@@ -364,6 +432,16 @@ def pack(worlds):
         gate_threshold=cells_of("gate_threshold"),
         gate_minimum=cells_of("gate_minimum"),
         gate_initial=cells_of("gate_initial"),
+        channel_code=(cells_of("channel_code").astype(np.int32) if nch
+                      else np.zeros((0, int(cells.sum())), dtype=np.int32)),
+        channel_species=(cells_of("channel_species").astype(np.int32) if nch
+                         else np.zeros((0, int(cells.sum())), dtype=np.int32)),
+        channel_permeability=(cells_of("channel_permeability") if nch
+                              else np.zeros((0, int(cells.sum())))),
+        channel_abundance=(cells_of("channel_abundance") if nch
+                           else np.zeros((0, int(cells.sum())))),
+        channel_gate_initial=(cells_of("channel_gate_initial") if nch
+                              else np.zeros((2, 0, int(cells.sum())))),
     )
 
 
@@ -374,7 +452,7 @@ def pack(worlds):
 def reference_definition(world, *, dt, steps, model="cells.model.resolved_pump_tissue@1",
                          solver="cells.solver.imex_ars222_face_electromigration@1",
                          membrane_control=None, junction_control=None, pump_control=None,
-                         padding=0):
+                         channel_control=None, padding=0):
     """One World as a reference definition dict (schema_version 1). ``padding`` adds that many
     inactive slots to every capacity (the reference pads its arrays to capacities)."""
     n, e = world.cells, world.edges
@@ -501,10 +579,34 @@ def reference_definition(world, *, dt, steps, model="cells.model.resolved_pump_t
             "material_balance_atol_fmol": {s: 2e-11 for s in SPECIES},
         },
     }
-    if v3:  # @3 declares its (here empty) channel population and Ca pumps explicitly.
-        out["model"]["channels"] = []
-        out["experiment"]["channel_controls"] = []
-        out["execution"]["channel_capacity"] = 0
+    if v3:  # @3 declares its channel populations and (absent) Ca pumps explicitly.
+        chs = []
+        nch = world.channel_slots
+        cc = (np.ones((nch, n)) if channel_control is None
+              else np.broadcast_to(channel_control, (nch, n)))
+        for i in range(n):
+            for k in range(nch):
+                code = int(world.channel_code[k, i])
+                if code not in (0, 2):
+                    raise ValueError("the reference's catalogue has no law with code " + str(code))
+                chs.append({
+                    "id": f"channel_{k}_{i}",
+                    "membrane_id": f"membrane_{i}",
+                    "kinetic_law": CHANNEL_LAW_IDS[code],
+                    "max_permeability_m_per_s": float(world.channel_permeability[k, i]),
+                    "abundance": float(world.channel_abundance[k, i]),
+                    "initial_gate": [float(world.channel_gate_initial[0, k, i]),
+                                     float(world.channel_gate_initial[1, k, i])],
+                    "permeant_ions": [{"species_id": SPECIES[int(world.channel_species[k, i])],
+                                       "relative_permeability": 1.0}],
+                })
+        out["model"]["channels"] = chs
+        out["experiment"]["channel_controls"] = [
+            {"channel_id": f"channel_{k}_{i}",
+             "schedule": [{"time": 0.0, "availability": float(cc[k, i])}]}
+            for i in range(n) for k in range(nch)
+        ]
+        out["execution"]["channel_capacity"] = len(chs) + (padding if chs or padding else 0)
         for membrane in out["model"]["membranes"]:
             membrane["calcium_pump"] = None
         out["experiment"]["calcium_pump_controls"] = []

@@ -68,6 +68,10 @@ CELL_FIELDS = (
 )
 EDGE_FIELDS = ("junction_transferred", "junction_dissipated", "junction_gate")  # [S,E],[E],[E]
 WORLD_FIELDS = ("reservoir_supplied", "electrode_charge", "reservoir_work", "electrode_work")
+CHANNEL_FIELDS = ("channel_gate", "channel_transferred", "channel_dissipated")  # cell-indexed
+EXPLICIT_STEP_BOUND = 1.0  # dt x the Gershgorin membrane rate (surface_pump.py:112)
+VOLTAGE_DOMAIN_V = (-0.120, 0.060)  # the channel laws' domain (laws/channels/kv1p5_mh.py:26)
+GATE_SERIES_LIMIT = 1e-3  # numerics/exponential_gates.py:33
 
 
 class State(NamedTuple):
@@ -84,27 +88,32 @@ class State(NamedTuple):
     electrode_charge: np.ndarray
     reservoir_work: np.ndarray
     electrode_work: np.ndarray
+    channel_gate: np.ndarray  # [2, NCH, C] gate rows (m, h) of each population
+    channel_transferred: np.ndarray  # [NCH, C] fmol of the population's permeant species
+    channel_dissipated: np.ndarray  # [NCH, C] pJ
 
 
 class Control(NamedTuple):
     membrane: np.ndarray  # [C] availability of each cell's patch
     junction: np.ndarray  # [E]
     pump: np.ndarray  # [C]
+    channel: np.ndarray = None  # [NCH, C]
 
 
 def initial_state(b):
-    c, e, w = b.cells, b.edges, b.worlds
+    c, e, w, nch = b.cells, b.edges, b.worlds, b.channel_slots
     return State(
         np.zeros((3, c)), np.zeros((3, c)), np.zeros(c), np.zeros(c), np.zeros(c), np.zeros(c),
         np.zeros((3, e)), np.zeros(e), b.gate_initial.copy(),
         np.zeros((3, w)), np.zeros(w), np.zeros(w), np.zeros(w),
+        np.array(b.channel_gate_initial, dtype=float), np.zeros((nch, c)), np.zeros((nch, c)),
     )  # fmt: skip
 
 
-def full_control(b, membrane=1.0, junction=1.0, pump=1.0):
+def full_control(b, membrane=1.0, junction=1.0, pump=1.0, channel=1.0):
     return Control(
         np.full(b.cells, float(membrane)), np.full(b.edges, float(junction)),
-        np.full(b.cells, float(pump)),
+        np.full(b.cells, float(pump)), np.full((b.channel_slots, b.cells), float(channel)),
     )  # fmt: skip
 
 
@@ -238,6 +247,99 @@ def gate_domain(gate, voltage, threshold, minimum, availability):
 
 
 # ---------------------------------------------------------------------------------------------
+# Voltage-gated channel laws (targets [2, ...] and time constants [2, ...] in s; V in volts)
+
+KV1P5, NAV1P2, HH_K_N4 = 0, 2, 100
+
+
+def kv1p5_kinetics(v):
+    """cells.channel.kv1p5_mh@1 (laws/channels/kv1p5_mh.py:29-41)."""
+
+    def sigmoid(value):
+        e = np.exp(-np.abs(value))
+        return np.where(value >= 0, 1 / (1 + e), e / (1 + e))
+
+    targets = np.stack((sigmoid((v + 0.0060) / 0.0064), sigmoid(-(v + 0.0253) / 0.0035)))
+    tau = np.stack((0.008330 - 0.1163 * v, 1.620000 - 15.500 * v))
+    return targets, tau
+
+
+def nav1p2_kinetics(v):
+    """cells.channel.nav1p2_m3h_regularized@1 (laws/channels/nav1p2_m3h_regularized.py:22-44)."""
+    shifted = (v + 0.025) / 0.009
+    activation = 0.182 * 9 * bernoulli(-shifted)
+    deactivation = 0.124 * 9 * bernoulli(shifted)
+    recovery = 0.024 * 5 * bernoulli(-(v + 0.040) / 0.005)
+    inactivation = 0.0091 * 5 * bernoulli((v + 0.065000123) / 0.005)
+    targets = np.stack((activation / (activation + deactivation),
+                        1 / (1 + np.exp((v + 0.055) / 0.0062))))
+    tau = np.stack((0.001 / (activation + deactivation), 0.001 / (recovery + inactivation)))
+    return targets, tau
+
+
+def hh_k_n4_kinetics(v):
+    """Hodgkin-Huxley K activation n (Hodgkin and Huxley 1952, J. Physiol. 117:500, rest at
+    -65 mV): alpha_n = 0.01 (Vm + 55) / (1 - exp(-(Vm + 55)/10)) and beta_n = 0.125
+    exp(-(Vm + 65)/80) per ms, Vm in mV; alpha_n written as 0.1 B(-(Vm + 55)/10) with the
+    Bernoulli function, whose removable singularity takes its limit. One gate (row 1 unused)."""
+    vm = 1000.0 * v
+    alpha = 100.0 * bernoulli(-(vm + 55.0) / 10.0)  # 1/s
+    beta = 125.0 * np.exp(-(vm + 65.0) / 80.0)  # 1/s
+    targets = np.stack((alpha / (alpha + beta), np.zeros_like(v)))
+    tau = np.stack((1.0 / (alpha + beta), np.ones_like(v)))
+    return targets, tau
+
+
+def gate_rows_active(code):
+    """[2, ...] rows that relax (channel_gate_active): both for Kv1.5 and NaV1.2, n alone for
+    the HH n^4 law."""
+    code = np.asarray(code)
+    return np.stack((np.ones(code.shape, dtype=bool), code != HH_K_N4))
+
+
+def channel_kinetics(v, code):
+    """Each population's targets and time constants by its law code, [2, NCH, C]."""
+    out_t = np.zeros((2, *code.shape))
+    out_tau = np.ones((2, *code.shape))
+    with np.errstate(all="ignore"):
+        for law, fn in ((KV1P5, kv1p5_kinetics), (NAV1P2, nav1p2_kinetics),
+                        (HH_K_N4, hh_k_n4_kinetics)):
+            mask = code == law
+            if np.any(mask):
+                t, tau = fn(np.broadcast_to(v, code.shape))
+                out_t = np.where(mask[None], t, out_t)
+                out_tau = np.where(mask[None], tau, out_tau)
+    return out_t, out_tau
+
+
+def channel_opening(gate, code):
+    """m^3 h (NaV1.2), m h (Kv1.5), n^4 (HH), [NCH, C] (sodium_channels.opening)."""
+    m, h = gate[0], gate[1]
+    return np.where(code == NAV1P2, m**3 * h, np.where(code == HH_K_N4, m**4, m * h))
+
+
+def channel_domain(v, targets, tau):
+    """channel_domain_valid (surface_pump_v3.py:848-858) per population, [NCH, C]."""
+    inside = (v >= VOLTAGE_DOMAIN_V[0]) & (v <= VOLTAGE_DOMAIN_V[1])
+    kin = np.isfinite(targets) & (targets >= 0) & (targets <= 1) & np.isfinite(tau) & (tau > 0)
+    return inside & np.all(kin, axis=0)
+
+
+def lag_weight(z):
+    """1 - (1 - e^-z)/z (numerics/exponential_gates.py:36-41)."""
+    small = z < GATE_SERIES_LIMIT
+    safe = np.where(small, 1.0, z)
+    series = z * (0.5 - z * (1 / 6 - z * (1 / 24 - z / 120)))
+    return np.where(small, series, (np.expm1(-safe) + safe) / safe)
+
+
+def advance_gates(gate, target_start, tau_start, target_end, tau_end, dt):
+    """Exponential update with a linearly varying target (numerics/exponential_gates.py:44-51)."""
+    z = 0.5 * dt * (1 / tau_start + 1 / tau_end)
+    return gate + (target_start - gate) * -np.expm1(-z) + (target_end - target_start) * lag_weight(z)
+
+
+# ---------------------------------------------------------------------------------------------
 # Field closure (held-bath worlds: each cell's one patch faces its world's held bath)
 
 
@@ -331,7 +433,31 @@ def explicit_rates(state, potential, control, b, topo):
     pump = tuple(b.pump[k][w] for k in range(7))
     args = (ci[0], co_c[1], mu_m[0], mu_m[1], t_c, pump, b.pump_capacity, control.pump)
     cycles, energy, drive = pump_kinetics(*args)
-    extra = -STOICHIOMETRY[:, None] * cycles
+    # Channel populations (surface_pump_v3.channel_rates, :937-963): the permeant species'
+    # constant-field flux at the patch voltage, open fraction times availability times abundance.
+    nch, idx = b.channel_slots, np.arange(b.cells)
+    chan, chan_d = np.zeros((nch, b.cells)), np.zeros((nch, b.cells))
+    chsum = np.zeros((3, b.cells))
+    ch_ok = np.ones(b.cells, dtype=bool)
+    if nch:
+        opening = channel_opening(state.channel_gate, b.channel_code)
+        with np.errstate(all="ignore"):
+            for k in range(nch):
+                sp = b.channel_species[k]
+                x = VALENCE[sp] * F * dvm / (R * t_c)
+                available = (opening[k] * control.channel[k]) * (
+                    0.0 + (1 - 0.0) * b.channel_abundance[k])
+                g = b.area * b.channel_permeability[k] * available / MOL_PER_FMOL
+                flux = g * (ci[sp, idx] * bernoulli(-x) - co_c[sp, idx] * bernoulli(x))
+                chan[k] = flux
+                chan_d[k] = 1e-3 * flux * mu_m[sp, idx]
+                chsum[sp, idx] = chsum[sp, idx] + flux
+            targets, tau = channel_kinetics(dvm[None, :], b.channel_code)
+        ch_ok = np.all(channel_domain(dvm[None, :], targets, tau), axis=0)
+        ch_ok &= np.all(np.isfinite(control.channel) & (control.channel >= 0)
+                        & (control.channel <= 1), axis=0)
+        ch_ok &= np.all(np.isfinite(chan) & np.isfinite(chan_d), axis=0)
+    extra = (-STOICHIOMETRY[:, None] * cycles - 0.0) + chsum
     inflow = np.zeros((3, b.worlds))
     np.add.at(inflow, (slice(None), w), jm + extra)
     gate = gate_rhs(state.junction_gate, dve, b.gate_threshold, b.gate_minimum)
@@ -349,6 +475,9 @@ def explicit_rates(state, potential, control, b, topo):
         np.zeros(b.worlds),
         np.zeros(b.worlds),
         np.zeros(b.worlds),
+        np.zeros_like(state.channel_gate),
+        chan,
+        chan_d,
     )
     # Validity per world (transport validity, pump and gate domains, finiteness, controls).
     ok_c = (
@@ -361,6 +490,7 @@ def explicit_rates(state, potential, control, b, topo):
         & np.isfinite(rates.metabolic_work)
         & (control.membrane >= 0) & (control.membrane <= 1) & np.isfinite(control.membrane)
         & (control.pump >= 0) & (control.pump <= 1) & np.isfinite(control.pump)
+        & ch_ok
     )  # fmt: skip
     ok_e = (
         np.all(np.abs(VALENCE[:, None] * F * dve / (R * t_e)) <= MAX_ABS_X, axis=0)
@@ -373,6 +503,34 @@ def explicit_rates(state, potential, control, b, topo):
     np.logical_and.at(valid, topo.edge_world, ok_e)
     valid &= np.all(np.isfinite(inflow), axis=0)
     return Rates(rates, valid, dvm)
+
+
+def membrane_rate(state, control, b, topo):
+    """Gershgorin rate (1/s) of membrane charge relaxation at a stage's openings, per world
+    (surface_pump_v3.membrane_rate, :4588-4660, with _patch_slopes :4534-4585): max over cells of
+    F^2/RT sum z^2 P max(c) A (patch and open populations) over the cell's capacitance."""
+    w = topo.cell_world
+    ci, co = concentrations(state, b)
+    largest = np.maximum(ci, co[:, w])
+    slope = F * F / (R * b.temperature[w])
+    z2 = VALENCE[:, None] ** 2
+    terms = z2 * b.permeability * largest
+    passive = ((terms[0] + terms[1]) + terms[2]) * control.membrane
+    membrane = passive * b.area
+    extra = np.zeros(b.cells)
+    nch, idx = b.channel_slots, np.arange(b.cells)
+    if nch:
+        open_fraction = b.channel_abundance * channel_opening(state.channel_gate, b.channel_code)
+        for k in range(nch):
+            sp = b.channel_species[k]
+            ch = (VALENCE[sp] ** 2 * b.channel_permeability[k] * 1.0 * largest[sp, idx]) * (
+                open_fraction[k] * control.channel[k])
+            extra = extra + ch * b.area
+    membrane = membrane + extra
+    rate = slope * (0.0 + membrane) / (0.0 + b.capacitance)
+    out = np.zeros(b.worlds)
+    np.maximum.at(out, w, rate)
+    return out
 
 
 def _combine(state, dt, terms):
@@ -393,6 +551,11 @@ def domain_valid(state, b, topo):
         ok_c &= np.isfinite(getattr(state, name))
     ok_c &= np.all(np.where(b.permeability > 0, True, state.membrane_transferred == 0), axis=0)
     ok_c &= np.where(b.pump_capacity > 0, True, state.pump_cycles == 0)
+    if b.channel_slots:
+        g = state.channel_gate
+        ok_c &= np.all(np.isfinite(g) & (g >= 0) & (g <= 1), axis=(0, 1))
+        ok_c &= np.all(np.isfinite(state.channel_transferred), axis=0)
+        ok_c &= np.all(np.isfinite(state.channel_dissipated), axis=0)
     ok_e = np.all(np.isfinite(state.junction_transferred), axis=0)
     ok_e &= np.isfinite(state.junction_dissipated) & np.isfinite(state.junction_gate)
     ok_e &= (state.junction_gate >= b.gate_minimum) & (state.junction_gate <= 1)
@@ -411,7 +574,7 @@ def domain_valid(state, b, topo):
 def _select(valid, new, old, b, topo):
     out = []
     for field, n, o in zip(State._fields, new, old, strict=True):
-        if field in CELL_FIELDS:
+        if field in CELL_FIELDS or field in CHANNEL_FIELDS:
             m = valid[topo.cell_world]
         elif field in EDGE_FIELDS:
             m = valid[topo.edge_world]
@@ -429,12 +592,28 @@ def ars222_step(state, dt, control, b, topo=None):
     topo = topology(b) if topo is None else topo
     w = topo.cell_world
     e_mat = np.array([[0.0, 0.0, 0.0], [GAMMA, 0.0, 0.0], [DELTA, 1.0 - DELTA, 0.0]])
+    bath = b.bath_potential[w]
+    nch = b.channel_slots
     charge0 = node_charge(state, b)
     start = capacitor_potential(charge0, b, topo)
     k0 = explicit_rates(state, start, control, b, topo)
     valid = k0.valid.copy()
+    # The explicit-stability refusal at each explicit stage (surface_pump_v3.py:3668-3670).
+    valid &= dt * membrane_rate(state, control, b, topo) <= EXPLICIT_STEP_BOUND
     zero = State(*(np.zeros_like(v) for v in state))
     zero = zero._replace(reservoir_supplied=-zero.reservoir_supplied)  # implicit_rates' -0.0
+    rows = gate_rows_active(b.channel_code)
+    if nch:  # The start's kinetics (readouts at the start potentials).
+        start_kin = channel_kinetics((start - bath)[None, :], b.channel_code)
+
+    def stage_gates(potential, fraction):
+        """surface_pump_v3.stage_gates (:3061-3070): exponential update from the step start."""
+        kin = channel_kinetics((potential - bath)[None, :], b.channel_code)
+        moved = advance_gates(state.channel_gate, start_kin[0], start_kin[1], kin[0], kin[1],
+                              fraction * dt)
+        ok = np.all(channel_domain((potential - bath)[None, :], *kin), axis=0)
+        return np.where(rows, moved, state.channel_gate), ok
+
     # Stage 1.
     known = _combine(state, dt, [(e_mat[1, 0], k0.state)])
     charge = node_charge(known, b)
@@ -444,8 +623,14 @@ def ars222_step(state, dt, control, b, topo=None):
     ok = np.isfinite(potential) & (np.abs(residual) <= CHARGE_ATOL_C + CHARGE_RTOL * scale)
     np.logical_and.at(valid, w, ok)
     stage = _combine(known, dt, [(GAMMA, zero)])
+    if nch:
+        with np.errstate(all="ignore"):
+            gate, ok = stage_gates(potential, np.sum(e_mat[1]))
+        stage = stage._replace(channel_gate=gate)
+        np.logical_and.at(valid, w, ok)
     k1 = explicit_rates(stage, potential, control, b, topo)
     valid &= k1.valid
+    valid &= dt * membrane_rate(stage, control, b, topo) <= EXPLICIT_STEP_BOUND
     # Stage 2 (the last): explicit weights delta, 1 - delta; implicit 1 - gamma, gamma (zeros).
     known = _combine(state, dt, [(e_mat[2, 0], k0.state), (e_mat[2, 1], k1.state),
                                  (1.0 - GAMMA, zero)])
@@ -456,6 +641,11 @@ def ars222_step(state, dt, control, b, topo=None):
     ok = np.isfinite(potential) & (np.abs(residual) <= CHARGE_ATOL_C + CHARGE_RTOL * scale)
     np.logical_and.at(valid, w, ok)
     stage = _combine(known, dt, [(GAMMA, zero)])
+    if nch:
+        with np.errstate(all="ignore"):
+            gate, ok = stage_gates(potential, np.sum(e_mat[2]))
+        stage = stage._replace(channel_gate=gate)
+        np.logical_and.at(valid, w, ok)
     # Ledger bookings of the step (surface_pump.py:338-355).
     applied = (0 + e_mat[2, 0] * k0.state.reservoir_supplied) + e_mat[2, 1] * k1.state.reservoir_supplied
     applied = applied + ((0 + (1.0 - GAMMA) * zero.reservoir_supplied) + GAMMA * zero.reservoir_supplied)
@@ -486,6 +676,12 @@ def readout_rates(state, control, b, topo):
     np.add.at(electrode, w, -b.capacitance * dphi)
     co = b.bath_amount / b.bath_volume
     mu = R * b.temperature * np.log(co) + VALENCE[:, None] * F * b.bath_potential
+    if b.channel_slots:  # readouts' gate rate, (target - g)/tau (surface_kinetic.py:237)
+        targets, tau = channel_kinetics((potential - b.bath_potential[w])[None, :],
+                                        b.channel_code)
+        rate = np.where(gate_rows_active(b.channel_code),
+                        (targets - state.channel_gate) / tau, 0.0)
+        r = r._replace(state=r.state._replace(channel_gate=rate))
     d = r.state._replace(
         electrode_charge=electrode,
         reservoir_work=1e-3 * np.sum(mu * r.state.reservoir_supplied, axis=0),
@@ -529,7 +725,13 @@ def balances(state, b, topo=None):
     topo = topology(b) if topo is None else topo
     w = topo.cell_world
     di = state.amount_increment
-    total_m = state.membrane_transferred - STOICHIOMETRY[:, None] * state.pump_cycles
+    moved = state.membrane_transferred
+    if b.channel_slots:  # channel_to_membrane (surface_kinetic.py:197-207)
+        moved = moved.copy()
+        idx = np.arange(b.cells)
+        for k in range(b.channel_slots):
+            moved[b.channel_species[k], idx] += state.channel_transferred[k]
+    total_m = moved - STOICHIOMETRY[:, None] * state.pump_cycles
     local = di + total_m
     send = np.zeros_like(di)
     np.add.at(send, (slice(None), topo.sender), state.junction_transferred)

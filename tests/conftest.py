@@ -25,7 +25,8 @@ def load_golden(name):
     from cells_b200 import worlds
 
     z = np.load(os.path.join(GOLDEN, name))
-    batch = worlds.Batch(**{f.name: z["batch_" + f.name] for f in fields(worlds.Batch)})
+    batch = worlds.Batch(**{f.name: z["batch_" + f.name] for f in fields(worlds.Batch)
+                            if "batch_" + f.name in z.files})
     return z, batch
 
 

@@ -22,6 +22,10 @@ Fixtures:
                          reference's own layout fields, controls and padded states (60 steps),
                          for the drop-in checked step (cells_b200/model.py).
   rk4_grid4x4.npz        The 4x4 world by RK4 at dt 0.1 ms, 100 steps (@1).
+  ars222_v3_channels.npz The 4x4 world (seed 3) with a NaV1.2 (m^3 h) and a Kv1.5 (m h)
+                         population per cell, partial channel availabilities, @3, 300 steps.
+  ars222_v3_channels_delaunay.npz  A 40-cell Delaunay world with both populations, gated
+                         junctions, partial controls, a -4 mV bath, @3, 200 steps.
   laws.npz               Point laws on grids of inputs: bernoulli, the pump kinetics and the
                          junction gate rate.
 """
@@ -63,6 +67,18 @@ def _state_to_packed(state):
         reservoir_work=np.asarray(state.reservoir_work_pJ)[:1],
         electrode_work=np.asarray(state.electrode_work_pJ)[:1],
     )
+
+
+def _channels_to_packed(state, world):
+    """@3's channel fields [2, Ch] / [S, Ch] (channel j = cell i * NCH + slot k) -> packed
+    [2, NCH, C] and [NCH, C] (the permeant species only)."""
+    nch, n = world.channel_slots, world.cells
+    j = np.arange(n)[None, :] * nch + np.arange(nch)[:, None]  # [NCH, C]
+    species = world.channel_species
+    gate = np.asarray(state.channel_gate)[:, j]
+    moved = np.asarray(state.channel_transferred)[species, j]
+    heat = np.asarray(state.channel_dissipated_energy_pJ)[species, j]
+    return dict(channel_gate=gate, channel_transferred=moved, channel_dissipated=heat)
 
 
 def _batch_arrays(batch):
@@ -118,7 +134,7 @@ def _run_reference_pytrees(world, *, model_id, dt, steps, keep, padding, control
     return out
 
 
-def _run(world, *, model_id, dt, steps, keep, solver, controls=None):
+def _run(world, *, model_id, dt, steps, keep, solver, controls=None, channels=False):
     from cells.definitions.specs import parse_spec
     from cells.registry.models import get_model
 
@@ -136,9 +152,15 @@ def _run(world, *, model_id, dt, steps, keep, solver, controls=None):
         from cells.execution.schedule import control_values
     cv = control_values(spec, [0.0])
     control = type(cv)(*(v[0] for v in cv))
+    def packed(st):
+        out = _state_to_packed(st)
+        if channels:
+            out.update(_channels_to_packed(st, world))
+        return out
+
     snaps, kept = [], []
     if 0 in keep:
-        snaps.append(_state_to_packed(state))
+        snaps.append(packed(state))
         kept.append(0)
     t0 = time.perf_counter()
     for k in range(1, steps + 1):
@@ -150,7 +172,7 @@ def _run(world, *, model_id, dt, steps, keep, solver, controls=None):
         if not bool(ok):
             raise RuntimeError(f"reference refused step {k}")
         if k in keep:
-            snaps.append(_state_to_packed(state))
+            snaps.append(packed(state))
             kept.append(k)
     elapsed = time.perf_counter() - t0
     stacked = {"ref_" + key: np.stack([s[key] for s in snaps]) for key in snaps[0]}
@@ -215,6 +237,42 @@ def make_trajectories():
           model_id="cells.model.resolved_pump_tissue@1", solver="rk4", elapsed=el)
 
 
+def make_channel_trajectories():
+    """@3 (the live model) with voltage-gated Na (NaV1.2 m^3 h) and K (Kv1.5 m h) populations."""
+    from cells_b200 import worlds
+
+    ars = "cells.solver.imex_ars222_face_electromigration@1"
+    v3 = "cells.model.resolved_pump_tissue@3"
+    rng = np.random.default_rng(21)
+    world = worlds.with_channels(worlds.grid_world(4, 4, worlds.world_rng(3, 0)), rng,
+                                 na=("nav", 2e-10, 0.5), k=("kv", 3e-10, 0.5), sigma=0.3)
+    controls = dict(channel_control=rng.uniform(0.5, 1.0, (2, world.cells)))
+    keep = {0, 1, 2, 5, 50, 100, 200, 300}
+    stacked, kept, el = _run(world, model_id=v3, dt=1e-3, steps=300, keep=keep, solver=ars,
+                             controls=controls, channels=True)
+    _save("ars222_v3_channels.npz", worlds.pack([world]), stacked, kept, dt=1e-3,
+          model_id=v3, solver=ars, elapsed=el, extra={"control_channel": controls[
+              "channel_control"]})
+
+    dworld = worlds.with_channels(
+        worlds.delaunay_world(40, worlds.world_rng(4, 0), junction_sigma=0.3,
+                              gate=(0.02, 0.1, 0.8)), rng,
+        na=("nav", 4e-10, 0.4), k=("kv", 5e-10, 0.6), sigma=0.3)
+    dworld.bath_potential = -0.004
+    controls = dict(
+        membrane_control=rng.uniform(0.5, 1.0, dworld.cells),
+        junction_control=rng.uniform(0.5, 1.0, dworld.edges),
+        pump_control=rng.uniform(0.5, 1.0, dworld.cells),
+        channel_control=rng.uniform(0.3, 1.0, (2, dworld.cells)),
+    )
+    keep = {0, 1, 2, 10, 100, 200}
+    stacked, kept, el = _run(dworld, model_id=v3, dt=1e-3, steps=200, keep=keep, solver=ars,
+                             controls=controls, channels=True)
+    _save("ars222_v3_channels_delaunay.npz", worlds.pack([dworld]), stacked, kept, dt=1e-3,
+          model_id=v3, solver=ars, elapsed=el,
+          extra={"control_" + k.split("_")[0]: v for k, v in controls.items()})
+
+
 def make_laws():
     from cells.laws import electrochemistry as ec
     from cells.laws.junctions import junction_voltage_relaxation as jg
@@ -253,13 +311,15 @@ def make_laws():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("laws", "trajectories"))
+    ap.add_argument("--only", choices=("laws", "trajectories", "channels"))
     args = ap.parse_args()
     _setup(args.reference)
     if args.only in (None, "laws"):
         make_laws()
     if args.only in (None, "trajectories"):
         make_trajectories()
+    if args.only in (None, "channels"):
+        make_channel_trajectories()
 
 
 if __name__ == "__main__":

@@ -16,9 +16,9 @@ TOL = 1e-14  # rounding-level agreement with the reference's own arithmetic
 
 
 def _controls(z, b):
-    if "control_membrane" in z:
-        return T.Control(z["control_membrane"], z["control_junction"], z["control_pump"])
-    return T.full_control(b)
+    full = T.full_control(b)
+    return T.Control(*(z["control_" + f] if "control_" + f in z else getattr(full, f)
+                       for f in T.Control._fields))
 
 
 def _replay(name, step, limit=None):
@@ -37,7 +37,9 @@ def _replay(name, step, limit=None):
             assert ok.all(), f"oracle refused step {k} of {name}"
             k += 1
         for f in T.State._fields:
-            worst[f] = max(worst.get(f, 0.0), scaled_difference(getattr(st, f), z["ref_" + f][idx]))
+            if "ref_" + f in z:
+                worst[f] = max(worst.get(f, 0.0),
+                               scaled_difference(getattr(st, f), z["ref_" + f][idx]))
     return worst
 
 
@@ -45,6 +47,8 @@ def _replay(name, step, limit=None):
     ("ars222_grid4x4.npz", 2000),
     ("ars222_v3_grid4x4.npz", None),
     ("ars222_gated.npz", None),
+    ("ars222_v3_channels.npz", None),
+    ("ars222_v3_channels_delaunay.npz", None),
 ])
 def test_oracle_matches_reference_ars222(name, limit):
     worst = _replay(name, T.ars222_step, limit)
@@ -82,3 +86,44 @@ def test_planted_change_is_caught():
         st, _ = T.ars222_step(st, 1e-3, T.full_control(b), b, topo)
     idx = list(z["steps"]).index(100)
     assert scaled_difference(st.amount_increment, z["ref_amount_increment"][idx]) > 1e-12
+
+
+def test_hh_k_n4_law_matches_its_closed_form():
+    """The HH K n^4 law (this package's; the reference has no n^4 law): alpha_n and beta_n of
+    Hodgkin and Huxley (1952) at a -65 mV rest, per ms, written out directly."""
+    import math
+
+    for v in (-0.1, -0.08, -0.065, -0.0551, -0.04, 0.0, 0.03):
+        vm = 1000.0 * v
+        a = 0.01 * (vm + 55.0) / (1.0 - math.exp(-(vm + 55.0) / 10.0))
+        bta = 0.125 * math.exp(-(vm + 65.0) / 80.0)
+        t, tau = T.hh_k_n4_kinetics(np.asarray(v))
+        assert abs(float(t[0]) - a / (a + bta)) <= 1e-13
+        assert abs(float(tau[0]) - 1e-3 / (a + bta)) <= 1e-13 * 1e-3 / (a + bta)
+    t, _ = T.hh_k_n4_kinetics(np.asarray(-0.055))  # removable singularity: alpha = 0.1 / ms
+    assert abs(float(t[0]) - 0.1 / (0.1 + 0.125 * math.exp(-10.0 / 80.0))) <= 1e-13
+
+
+def test_exponential_gate_update_is_second_order():
+    """advance_gates with a linearly varying target (numerics/exponential_gates.py): for a smooth
+    target g_inf(t) = 0.3 + 50 t and tau(t) = 0.01 + 5 t, halving the step divides the one-step
+    error by about 8 (local error O(h^3))."""
+    def f(t, g):
+        return ((0.3 + 50.0 * t) - g) / (0.01 + 5.0 * t)
+
+    def exact(h, n=4000):
+        g, dt = 0.2, h / n
+        for i in range(n):  # classical RK4, far finer than h
+            t = i * dt
+            k1 = f(t, g)
+            k2 = f(t + dt / 2, g + dt / 2 * k1)
+            k3 = f(t + dt / 2, g + dt / 2 * k2)
+            k4 = f(t + dt, g + dt * k3)
+            g += dt / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
+        return g
+
+    errs = []
+    for h in (1e-3, 5e-4, 2.5e-4):
+        g = T.advance_gates(np.asarray(0.2), 0.3, 0.01, 0.3 + 50.0 * h, 0.01 + 5.0 * h, h)
+        errs.append(abs(float(g) - exact(h)))
+    assert errs[0] / errs[1] > 6.0 and errs[1] / errs[2] > 6.0, errs
