@@ -28,8 +28,11 @@ STATE_FIELDS = (
     "electrode_charge",
     "reservoir_work",
     "electrode_work",
+    "channel_gate",
+    "channel_transferred",
+    "channel_dissipated",
 )
-CONTROL_FIELDS = ("membrane", "junction", "pump")
+CONTROL_FIELDS = ("membrane", "junction", "pump", "channel")
 METHOD_ARS222 = 0
 WORLD_BITS = {
     1: "transport",
@@ -38,6 +41,8 @@ WORLD_BITS = {
     8: "control",
     16: "residual",
     32: "domain",
+    64: "stiff",
+    128: "channel_domain",
 }
 EXPORTS = (
     "cb_bind",
@@ -84,6 +89,11 @@ class TissueDesc(ctypes.Structure):
         ("junction_permeability", _d),
         ("gate_threshold", _d),
         ("gate_minimum", _d),
+        ("channel_slots", ctypes.c_int32),
+        ("channel_code", _i32),
+        ("channel_species", _i32),
+        ("channel_permeability", _d),
+        ("channel_abundance", _d),
     ]
 
 

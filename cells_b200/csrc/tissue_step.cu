@@ -71,6 +71,7 @@ enum WorldConst {
   WC_FRT = WC_MUB + 3,  // F / RT
   WC_INVRT,   // 1 / RT
   WC_INVRTD,  // 1 / rt of the pump domain predicate
+  WC_SLOPE,   // F^2 / RT, the constant-field slope of the explicit-stability rate
   WC_STRIDE
 };
 
@@ -95,6 +96,11 @@ struct Tissue {
   const double *jap;       // [3][E]  junction area * permeability / 1e-15
   const double *thr;       // [E]
   const double *jmin;      // [E]
+  int nch;                 // channel slots per cell (0 or 2)
+  const int *ch_code;      // [NCH][C] law code
+  const int *ch_species;   // [NCH][C] permeant species
+  const double *ch_ap;     // [NCH][C] area * permeability / 1e-15
+  const double *ch_ab;     // [NCH][C] abundance
 };
 
 struct Layout {  // offsets in doubles
@@ -104,6 +110,8 @@ struct Layout {  // offsets in doubles
 
 struct StepCoef {
   double dt;
+  double frac1_dt;      // the gates' stage-1 and final advance: sum of the tableau row times dt
+  double frac2_dt;
   double gamma_dt;      // ARS(2,2,2) stage 1 weight times dt
   double delta_dt;      // final weights times dt
   double omdelta_dt;
@@ -139,6 +147,83 @@ __device__ __forceinline__ double logaddexp0(double y) {
 
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
+// B(x) alone (laws/electrochemistry.py:25-32).
+__device__ __forceinline__ double bernoulli(double x) {
+  if (fabs(x) < 1e-4) {
+    const double x2 = x * x;
+    return ((1.0 - x / 2.0) + x2 / 12.0) - (x2 * x2) / 720.0;
+  }
+  return x / expm1(x);
+}
+
+// Voltage-gated channel laws: gate targets t[2] and time constants tau[2] (s) at membrane
+// voltage v (V). Codes: 0 Kv1.5 (laws/channels/kv1p5_mh.py:29-41), 2 NaV1.2
+// (laws/channels/nav1p2_m3h_regularized.py:22-44), 100 Hodgkin-Huxley K n (Hodgkin and Huxley
+// 1952: alpha_n = 0.01 (Vm+55)/(1 - exp(-(Vm+55)/10)), beta_n = 0.125 exp(-(Vm+65)/80) per ms,
+// Vm in mV, alpha_n = 0.1 B(-(Vm+55)/10); one gate, row 1 unused).
+constexpr int kKv1p5 = 0, kNav1p2 = 2, kHhKn4 = 100;
+
+__device__ __forceinline__ double kv_sigmoid(double value) {
+  const double e = exp(-fabs(value));
+  return value >= 0.0 ? 1.0 / (1.0 + e) : e / (1.0 + e);
+}
+
+__device__ __forceinline__ void channel_kinetics(int code, double v, double (&t)[2],
+                                                 double (&tau)[2]) {
+  if (code == kNav1p2) {
+    const double shifted = (v + 0.025) / 0.009;
+    double bp, bm;
+    bernoulli_pair(shifted, bp, bm);
+    const double activation = (0.182 * 9) * bm;
+    const double deactivation = (0.124 * 9) * bp;
+    const double recovery = (0.024 * 5) * bernoulli(-(v + 0.040) / 0.005);
+    const double inactivation = (0.0091 * 5) * bernoulli((v + 0.065000123) / 0.005);
+    t[0] = activation / (activation + deactivation);
+    t[1] = 1.0 / (1.0 + exp((v + 0.055) / 0.0062));
+    tau[0] = 0.001 / (activation + deactivation);
+    tau[1] = 0.001 / (recovery + inactivation);
+  } else if (code == kHhKn4) {
+    const double vm = 1000.0 * v;
+    const double alpha = 100.0 * bernoulli(-(vm + 55.0) / 10.0);
+    const double beta = 125.0 * exp(-(vm + 65.0) / 80.0);
+    t[0] = alpha / (alpha + beta);
+    t[1] = 0.0;
+    tau[0] = 1.0 / (alpha + beta);
+    tau[1] = 1.0;
+  } else {  // Kv1.5
+    t[0] = kv_sigmoid((v + 0.0060) / 0.0064);
+    t[1] = kv_sigmoid(-(v + 0.0253) / 0.0035);
+    tau[0] = 0.008330 - 0.1163 * v;
+    tau[1] = 1.620000 - 15.500 * v;
+  }
+}
+
+// channel_domain_valid (surface_pump_v3.py:848-858): the -120..60 mV domain, finite kinetics.
+__device__ __forceinline__ bool channel_kinetics_ok(double v, const double (&t)[2],
+                                                    const double (&tau)[2]) {
+  bool ok = v >= -0.120 && v <= 0.060;
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+    ok = ok && finite(t[r]) && t[r] >= 0.0 && t[r] <= 1.0 && finite(tau[r]) && tau[r] > 0.0;
+  return ok;
+}
+
+__device__ __forceinline__ double channel_opening(int code, double m, double h) {
+  if (code == kNav1p2) return ((m * m) * m) * h;
+  if (code == kHhKn4) return (m * m) * (m * m);
+  return m * h;
+}
+
+// Exponential gate update with a linearly varying target (numerics/exponential_gates.py:36-51).
+__device__ __forceinline__ double advance_gate(double g, double ts, double taus, double te,
+                                               double taue, double h) {
+  const double z = 0.5 * h * (1.0 / taus + 1.0 / taue);
+  const double em = expm1(-z);
+  const double lag = z < 1e-3 ? z * (0.5 - z * (1.0 / 6.0 - z * (1.0 / 24.0 - z / 120.0)))
+                              : (em + z) / z;
+  return g + (ts - g) * (-em) + (te - ts) * lag;
+}
+
 // Block-wide sum of NV values per thread, fixed tree order: xor-shuffle within warps, then the
 // warp partials in warp order. Every thread receives the totals.
 template <int BLOCK, int NV>
@@ -173,13 +258,15 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *red) {
 // n, g: the stage's amounts and gates; V: this thread's cell potential. sA/sE hold the cell and
 // junction accumulators in slots private to each thread. inflow: this cell's patch flux plus pump
 // transfer (the held bath's inflow terms).
-template <int BLOCK, int EPT, bool FIRST>
+template <int BLOCK, int EPT, int NCH, bool FIRST>
 __device__ __forceinline__ void stage(
     const Tissue &T, const Layout &L, const double *__restrict__ wc, const StepCoef &k,
     const double *cur, int c0, int e0, int ne, int i, bool has_cell, const double (&n)[3],
-    double V, const double (&g)[EPT], double mc, double pc_ctl, double log_drive_cap,
-    const double *__restrict__ jctl, double *sV, double *sC, double *sL, double *sJ, double *sA,
-    double *sE, double (&n1)[3], double (&g1)[EPT], double (&inflow)[3], uint32_t &bits) {
+    double V, const double (&g)[EPT], const double (&chg)[2][NCH > 0 ? NCH : 1], double mc,
+    double pc_ctl, double log_drive_cap, const double *__restrict__ jctl,
+    const double *__restrict__ chctl, double *sV, double *sC, double *sL, double *sJ, double *sA,
+    double *sE, double *sH, double (&n1)[3], double (&g1)[EPT], double (&inflow)[3],
+    uint32_t &bits) {
   constexpr int EB = EPT * BLOCK;
   const double w = FIRST ? k.delta_dt : k.omdelta_dt;
   const long long C = T.C, E = T.E;
@@ -232,6 +319,48 @@ __device__ __forceinline__ void stage(
     if (!(finite(mc) && mc >= 0.0 && mc <= 1.0 && finite(pc_ctl) && pc_ctl >= 0.0 &&
           pc_ctl <= 1.0))
       bits |= CB_WORLD_CONTROL;
+    // Explicit-stability refusal (surface_pump_v3.membrane_rate, :4588-4660): dt times the
+    // cell's constant-field slope conductance over its capacitance must stay <= 1.
+    double largest[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) largest[s] = fmax(c[s], wc[WC_CO + s]);
+    double membrane =
+        ((((__ldg(T.ap + gi) * largest[0]) + __ldg(T.ap + C + gi) * largest[1]) +
+          __ldg(T.ap + 2 * C + gi) * largest[2]) * 1e-15) * mc;
+    // Channel populations (surface_pump_v3.channel_rates, :937-963): the permeant species'
+    // constant-field flux at the patch voltage (the patch's Bernoulli pair), opening times
+    // availability times abundance.
+    double chm[3] = {0.0, 0.0, 0.0};
+    if constexpr (NCH > 0) {
+#pragma unroll
+      for (int q = 0; q < NCH; ++q) {
+        const int code = __ldg(T.ch_code + q * C + gi);
+        const int sp = __ldg(T.ch_species + q * C + gi);
+        const double ctl = __ldg(chctl + q * C);
+        if (!(finite(ctl) && ctl >= 0.0 && ctl <= 1.0)) bits |= CB_WORLD_CONTROL;
+        const double open = channel_opening(code, chg[0][q], chg[1][q]);
+        const double available = (open * ctl) * __ldg(T.ch_ab + q * C + gi);
+        const double gq = __ldg(T.ch_ap + q * C + gi) * available;
+        const double cs = sp == 0 ? c[0] : sp == 1 ? c[1] : c[2];
+        const double cos_ = wc[WC_CO + sp];
+        const double musp = sp == 0 ? mu[0] : sp == 1 ? mu[1] : mu[2];
+        const double J = sp < 2 ? gq * (cs * bm - cos_ * bp) : gq * (cs * bp - cos_ * bm);
+        const double Jd = 1e-3 * J * musp;
+        chm[sp] += J;
+        membrane += ((__ldg(T.ch_ap + q * C + gi) * 1e-15) * (sp == 0 ? largest[0]
+                     : sp == 1 ? largest[1] : largest[2])) * available;
+        double *tr = sH + q * BLOCK + i, *dd = sH + (NCH + q) * BLOCK + i;
+        if (FIRST) {
+          *tr = cur[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi] + w * J;
+          *dd = cur[L.s[CB_CHANNEL_DISSIPATED] + q * C + gi] + w * Jd;
+        } else {
+          *tr = *tr + w * J;
+          *dd = *dd + w * Jd;
+        }
+        if (!(finite(J) && finite(Jd))) bits |= CB_WORLD_TRANSPORT;
+      }
+    }
+    if (!(k.dt * (wc[WC_SLOPE] * membrane * __ldg(T.icap + gi)) <= 1.0)) bits |= CB_WORLD_STIFF;
     // Na/K-ATPase (nak_atp_mass_action_positive.kinetics), Na inside, K in the bath.
     const double drive = wc[WC_DRIVE];
     const double energy = (drive + (-3.0) * mu[0]) + 2.0 * mu[1];
@@ -249,9 +378,10 @@ __device__ __forceinline__ void stage(
     cell_acc(7, L.s[CB_PUMP_CYCLES], cycles);
     cell_acc(8, L.s[CB_PUMP_DISSIPATED], pd);
     cell_acc(9, L.s[CB_METABOLIC_WORK], mw);
-    extra[0] = 3.0 * cycles;  // -stoichiometry * cycles, outward-positive
-    extra[1] = -2.0 * cycles;
-    extra[2] = -0.0 * cycles;
+    // -stoichiometry * cycles (outward-positive) plus the channels' transfer.
+    extra[0] = (3.0 * cycles - 0.0) + chm[0];
+    extra[1] = (-2.0 * cycles - 0.0) + chm[1];
+    extra[2] = (-0.0 * cycles - 0.0) + chm[2];
     // Pump domain (positive substrates, parameters, |mu/RT| <= 1600, |affinity| <= 80).
     const double sna = mu[0] * wc[WC_INVRTD], sk = mu[1] * wc[WC_INVRTD];
     const double aff = (wc[WC_AFF0] + (-3.0) * sna) + 2.0 * sk;
@@ -361,8 +491,9 @@ __device__ __forceinline__ void stage(
 
 // Shared-memory words of one step CTA: stage potentials, concentrations and their logs, junction
 // fluxes, the step accumulator (cells, junctions) and the reduction scratch.
-__host__ __device__ constexpr size_t step_smem_words(int block, int ept) {
-  return (size_t)(7 * block + 3 * ept * block + 10 * block + 5 * ept * block + (block / 32) * 8);
+__host__ __device__ constexpr size_t step_smem_words(int block, int ept, int nch) {
+  return (size_t)(7 * block + 3 * ept * block + 10 * block + 5 * ept * block + 8 * nch * block +
+                  (block / 32) * 8);
 }
 
 // The ARS(2,2,2) step of surface_pump.imex_step (surface_pump.py:259-362) for one world per CTA,
@@ -370,7 +501,7 @@ __host__ __device__ constexpr size_t step_smem_words(int block, int ept) {
 // global memory (the launch's input, then this CTA's own last accepted state, which stays in L2
 // across fused steps), and the accumulator y + delta dt k0 + (1 - delta) dt k1 lives in shared
 // memory, in slots private to each thread.
-template <int BLOCK, int EPT, int MINB>
+template <int BLOCK, int EPT, int NCH, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB)
     ars222_kernel(const Tissue T, const Layout L, const double *state_in, double *state_out,
                   const double *__restrict__ control, const StepCoef k, int n_steps,
@@ -383,7 +514,10 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   double *sJ = sL + 3 * BLOCK;  // [3][EB]
   double *sA = sJ + 3 * EB;     // [10][BLOCK]: n[3], mt[3], md, pc, pd, mw
   double *sE = sA + 10 * BLOCK; // [5][EB]: jt[3], jd, g
-  double *sRed = sE + 5 * EB;   // [BLOCK/32][8]
+  double *sH = sE + 5 * EB;     // [2*NCH][BLOCK]: channel transferred, dissipated accumulators
+  double *sK = sH + 2 * NCH * BLOCK;  // [4*NCH][BLOCK]: start kinetics t[2][NCH], tau[2][NCH]
+  double *sG = sK + 4 * NCH * BLOCK;  // [2*NCH][BLOCK]: the new state's gates
+  double *sRed = sG + 2 * NCH * BLOCK;  // [BLOCK/32][8]
   __shared__ double sW[WC_STRIDE];
   __shared__ unsigned int sBits;
 
@@ -406,6 +540,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     if (pctl > 0.0) log_drive_cap = __ldg(T.logpcap + gi) + log(pctl);
   }
   const double *jctl = control + L.c[CB_CONTROL_JUNCTION] + e0;
+  const double *chctl = control + L.c[CB_CONTROL_CHANNEL] + gi;
   double res[3];
 #pragma unroll
   for (int s = 0; s < 3; ++s) res[s] = state_in[L.s[CB_RESERVOIR_SUPPLIED] + s * (long long)T.W + w];
@@ -429,10 +564,32 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     plate0 = v[0];
   }
 
+  // The start's channel kinetics (readouts at the start potentials), carried from step to step:
+  // a step's final potential is the next step's start potential here (both Q/C + V_bath).
+  bool k0_ok = true;
+  if constexpr (NCH > 0) {
+    if (has_cell) {
+      const double *n = cur + L.s[CB_AMOUNT_INCREMENT] + gi;
+      const double V = (__ldg(T.q0 + gi) + kChargePerFmol * ((n[0] + n[C]) + (-n[2 * C]))) *
+                           __ldg(T.icap + gi) + Vb;
+#pragma unroll
+      for (int q = 0; q < NCH; ++q) {
+        double t[2], tau[2];
+        channel_kinetics(__ldg(T.ch_code + q * C + gi), V - Vb, t, tau);
+        k0_ok = k0_ok && channel_kinetics_ok(V - Vb, t, tau);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          sK[(r * NCH + q) * BLOCK + i] = t[r];
+          sK[((2 + r) * NCH + q) * BLOCK + i] = tau[r];
+        }
+      }
+    }
+  }
+
   int taken = 0;
   uint32_t refused = 0u;
   for (int step = 0; step < n_steps; ++step) {
-    uint32_t bits = 0u;
+    uint32_t bits = k0_ok ? 0u : CB_WORLD_CHANNEL_DOMAIN;
     // Stage 0 at the step's start: potential from the capacitor solve, Q / C plus the bath's.
     double n0[3] = {0.0, 0.0, 0.0}, g0[EPT];
     double icap = 1.0, q0 = 0.0;
@@ -448,21 +605,52 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       g0[q] = e < ne ? cur[L.s[CB_JUNCTION_GATE] + e0 + e] : 1.0;
     }
     const double V0 = (q0 + kChargePerFmol * ((n0[0] + n0[1]) + (-n0[2]))) * icap + Vb;
+    constexpr int NQ = NCH > 0 ? NCH : 1;
+    double chg0[2][NQ], chg1[2][NQ];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int q = 0; q < NQ; ++q)
+        chg0[r][q] = (NCH > 0 && has_cell) ? cur[L.s[CB_CHANNEL_GATE] + (r * NCH + q) * C + gi]
+                                           : 0.0;
     double n1[3], g1[EPT], in0[3], in1[3];
-    stage<BLOCK, EPT, true>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n0, V0, g0, mc, pctl,
-                            log_drive_cap, jctl, sV, sC, sL, sJ, sA, sE, n1, g1, in0, bits);
+    stage<BLOCK, EPT, NCH, true>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n0, V0, g0, chg0, mc,
+                                 pctl, log_drive_cap, jctl, chctl, sV, sC, sL, sJ, sA, sE, sH, n1,
+                                 g1, in0, bits);
     // Stage 1 potential: the IMEX operator (capacitor only, no faces) solve. The operator is
     // diagonal on the cells, so Q/C leaves a charge residual within an ulp of Q and only a
     // non-finite potential exceeds 3e-25 C + 2e-12 |Q| (surface_imex.solve_operator).
     const double V1 = (q0 + kChargePerFmol * ((n1[0] + n1[1]) + (-n1[2]))) * icap + Vb;
     if (has_cell && !finite(V1)) bits |= CB_WORLD_RESIDUAL;
+    // Stage-1 channel gates: the exponential update from the step start to the stage potential
+    // (surface_pump_v3.stage_gates, :3061-3070; rows without a law keep their value).
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      chg1[0][q] = chg0[0][q];
+      chg1[1][q] = chg0[1][q];
+      if (NCH > 0 && has_cell) {
+        const int code = __ldg(T.ch_code + q * C + gi);
+        double t[2], tau[2];
+        channel_kinetics(code, V1 - Vb, t, tau);
+        if (!channel_kinetics_ok(V1 - Vb, t, tau)) bits |= CB_WORLD_CHANNEL_DOMAIN;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          if (r == 1 && code == kHhKn4) continue;
+          chg1[r][q] = advance_gate(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
+                                    sK[((2 + r) * NCH + q) * BLOCK + i], t[r], tau[r], k.frac1_dt);
+        }
+      }
+    }
     {
       double nd[3], gd[EPT];
-      stage<BLOCK, EPT, false>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n1, V1, g1, mc, pctl,
-                               log_drive_cap, jctl, sV, sC, sL, sJ, sA, sE, nd, gd, in1, bits);
+      stage<BLOCK, EPT, NCH, false>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n1, V1, g1, chg1,
+                                    mc, pctl, log_drive_cap, jctl, chctl, sV, sC, sL, sJ, sA, sE,
+                                    sH, nd, gd, in1, bits);
     }
     // The new state's domain (surface_kinetic.domain_valid): positive amounts, finite ledgers,
     // gates in [minimum, 1].
+    bool k2_ok = true;
+    double k2t[2][NQ], k2tau[2][NQ];
     if (has_cell) {
       bool ok = true;
 #pragma unroll
@@ -470,7 +658,31 @@ __global__ void __launch_bounds__(BLOCK, MINB)
 #pragma unroll
       for (int s = 0; s < 3; ++s) ok = ok && (__ldg(T.ref + s * C + gi) + sA[s * BLOCK + i]) > 0.0;
       const double q2 = q0 + kChargePerFmol * ((sA[i] + sA[BLOCK + i]) + (-sA[2 * BLOCK + i]));
-      if (!finite(q2 * icap + Vb)) bits |= CB_WORLD_RESIDUAL;
+      const double V2 = q2 * icap + Vb;
+      if (!finite(V2)) bits |= CB_WORLD_RESIDUAL;
+      // Final channel gates from the step start to the final potential; channel ledgers finite.
+      if constexpr (NCH > 0) {
+#pragma unroll
+        for (int q = 0; q < NCH; ++q) {
+          const int code = __ldg(T.ch_code + q * C + gi);
+          double t[2], tau[2];
+          channel_kinetics(code, V2 - Vb, t, tau);
+          k2_ok = k2_ok && channel_kinetics_ok(V2 - Vb, t, tau);
+#pragma unroll
+          for (int r = 0; r < 2; ++r) {
+            k2t[r][q] = t[r];
+            k2tau[r][q] = tau[r];
+            double g = chg0[r][q];
+            if (!(r == 1 && code == kHhKn4))
+              g = advance_gate(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
+                               sK[((2 + r) * NCH + q) * BLOCK + i], t[r], tau[r], k.frac2_dt);
+            sG[(r * NCH + q) * BLOCK + i] = g;
+            ok = ok && finite(g) && g >= 0.0 && g <= 1.0;
+          }
+          ok = ok && finite(sH[q * BLOCK + i]) && finite(sH[(NCH + q) * BLOCK + i]);
+        }
+        if (!k2_ok) bits |= CB_WORLD_CHANNEL_DOMAIN;
+      }
       if (!ok) bits |= CB_WORLD_DOMAIN;
     }
 #pragma unroll
@@ -525,7 +737,22 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       state_out[L.s[CB_PUMP_CYCLES] + gi] = sA[7 * BLOCK + i];
       state_out[L.s[CB_PUMP_DISSIPATED] + gi] = sA[8 * BLOCK + i];
       state_out[L.s[CB_METABOLIC_WORK] + gi] = sA[9 * BLOCK + i];
+      if constexpr (NCH > 0) {
+#pragma unroll
+        for (int q = 0; q < NCH; ++q) {
+          state_out[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi] = sH[q * BLOCK + i];
+          state_out[L.s[CB_CHANNEL_DISSIPATED] + q * C + gi] = sH[(NCH + q) * BLOCK + i];
+#pragma unroll
+          for (int r = 0; r < 2; ++r) {
+            state_out[L.s[CB_CHANNEL_GATE] + (r * NCH + q) * C + gi] =
+                sG[(r * NCH + q) * BLOCK + i];
+            sK[(r * NCH + q) * BLOCK + i] = k2t[r][q];
+            sK[((2 + r) * NCH + q) * BLOCK + i] = k2tau[r][q];
+          }
+        }
+      }
     }
+    k0_ok = k2_ok;
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
       const int e = tid + q * BLOCK;
@@ -553,6 +780,11 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     if (has_cell) {
       for (int f = CB_AMOUNT_INCREMENT; f <= CB_METABOLIC_WORK; ++f) {
         const int reps = (f <= CB_MEMBRANE_TRANSFERRED) ? 3 : 1;
+        for (int s = 0; s < reps; ++s)
+          state_out[L.s[f] + s * C + gi] = state_in[L.s[f] + s * C + gi];
+      }
+      for (int f = CB_CHANNEL_GATE; f <= CB_CHANNEL_DISSIPATED; ++f) {
+        const int reps = (f == CB_CHANNEL_GATE) ? 2 * NCH : NCH;
         for (int s = 0; s < reps; ++s)
           state_out[L.s[f] + s * C + gi] = state_in[L.s[f] + s * C + gi];
       }
@@ -728,7 +960,10 @@ int upload(cb_tissue *t, const std::vector<T> &host, const T **dst) {
   return CB_OK;
 }
 
-size_t step_smem(int block, int ept) { return sizeof(double) * step_smem_words(block, ept); }
+size_t step_smem(int block, int ept, int nch) {
+  return sizeof(double) * step_smem_words(block, ept, nch);
+}
+constexpr size_t kMaxSmemPerBlock = 227 * 1024;
 
 size_t balances_smem(int block, int ept) {
   return sizeof(double) * (size_t)(3 * ept * block + (block / 32) * 8);
@@ -738,13 +973,17 @@ template <int BLOCK, int EPT>
 int launch_step(cb_tissue *t, const double *in, double *out, const double *control,
                 const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
                 cudaStream_t stream) {
-  const size_t smem = step_smem(BLOCK, EPT);
+  const int nch = t->t.nch;
+  const size_t smem = step_smem(BLOCK, EPT, nch);
   // Resident CTAs per SM that the register budget targets: 128-thread CTAs at 2 (no spills),
-  // 256-thread CTAs at 2 (no spills) or 3 (a few spilled words), larger CTAs at 1.
+  // 256-thread CTAs at 2 (no spills) or 3 (a few spilled words; worlds without channels), larger
+  // CTAs at 1.
   constexpr int kMin = BLOCK <= 256 ? 2 : 1;
-  auto kern = ars222_kernel<BLOCK, EPT, kMin>;
-  if constexpr (BLOCK == 256) {
-    if (t->occupancy == 3) kern = ars222_kernel<BLOCK, EPT, 3>;
+  auto kern = ars222_kernel<BLOCK, EPT, 0, kMin>;
+  if (nch == 2) {
+    kern = ars222_kernel<BLOCK, EPT, 2, kMin>;
+  } else if constexpr (BLOCK == 256) {
+    if (t->occupancy == 3) kern = ars222_kernel<BLOCK, EPT, 0, 3>;
   }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
@@ -830,6 +1069,23 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
   while (block < max_cells) block *= 2;
   const int ept = (int)std::max<long long>(1, (max_edges + block - 1) / block);
   if (ept > 4) return fail(CB_ERR_UNSUPPORTED, "more than 4 junctions per thread");
+  const int desc_nch = d->channel_slots;
+  if (desc_nch != 0 && desc_nch != 2)
+    return fail(CB_ERR_UNSUPPORTED, "channel slots per cell must be 0 or 2");
+  if (desc_nch && (!d->channel_code || !d->channel_species || !d->channel_permeability ||
+                   !d->channel_abundance))
+    return fail(CB_ERR_ARGUMENT, "null channel array in the tissue description");
+  if (step_smem(block, ept, desc_nch) > kMaxSmemPerBlock)
+    return fail(CB_ERR_UNSUPPORTED, "world too large for the shared-memory step (cells x "
+                                    "junctions per world)");
+  for (long long q = 0; q < (long long)desc_nch * C; ++q) {
+    const int code = d->channel_code[q], sp = d->channel_species[q];
+    if (code != 0 && code != 2 && code != 100)
+      return fail(CB_ERR_UNSUPPORTED, "channel law code must be 0, 2 or 100");
+    if (sp < 0 || sp > 2) return fail(CB_ERR_LAYOUT, "channel species out of range");
+    if (!(d->channel_permeability[q] >= 0) || !(d->channel_abundance[q] >= 0))
+      return fail(CB_ERR_LAYOUT, "channel permeability and abundance must be non-negative");
+  }
   // Adjacency (senders first, then receivers, each in edge order) and route checks.
   std::vector<int> adj_ptr(C + 1, 0), adj_idx;
   std::vector<std::vector<int>> out_e(C), in_e(C);
@@ -894,6 +1150,7 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
     c[WC_FRT] = kF / RT;
     c[WC_INVRT] = 1.0 / RT;
     c[WC_INVRTD] = 1.0 / rtd;
+    c[WC_SLOPE] = kF * kF / RT;
   }
   // Route conductance prefactors A P / (1e-15 mol/fmol) (selective_flux's), and reciprocals.
   std::vector<double> ap(3 * C), jap(3 * E), logpcap(C), ivol(C), icap(C);
@@ -951,20 +1208,37 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
   if (!rc) rc = upload(t, jap, &T.jap);
   if (!rc) rc = upload(t, E ? vec(d->gate_threshold, E) : std::vector<double>(), &T.thr);
   if (!rc) rc = upload(t, E ? vec(d->gate_minimum, E) : std::vector<double>(), &T.jmin);
+  T.nch = desc_nch;
+  {
+    const long long nq = (long long)desc_nch * C;
+    std::vector<int> code(nq), species(nq);
+    std::vector<double> chap(nq), chab(nq);
+    for (long long q = 0; q < nq; ++q) {
+      code[q] = d->channel_code[q];
+      species[q] = d->channel_species[q];
+      chap[q] = d->area[q % C] * d->channel_permeability[q] / 1e-15;
+      chab[q] = d->channel_abundance[q];
+    }
+    if (!rc) rc = upload(t, code, &T.ch_code);
+    if (!rc) rc = upload(t, species, &T.ch_species);
+    if (!rc) rc = upload(t, chap, &T.ch_ap);
+    if (!rc) rc = upload(t, chab, &T.ch_ab);
+  }
   if (rc) {
     cb_free(t);
     return rc;
   }
   // Packed state and control layouts: each field padded to 32 doubles (256-byte aligned).
+  const long long nch = desc_nch;
   const long long sizes[CB_STATE_FIELDS] = {3 * C, 3 * C, C, C, C, C, 3 * E, E, E, 3 * (long long)W,
-                                            W, W, W};
+                                            W, W, W, 2 * nch * C, nch * C, nch * C};
   long long off = 0;
   for (int f = 0; f < CB_STATE_FIELDS; ++f) {
     t->layout.s[f] = off;
     off += pad32(sizes[f]);
   }
   t->state_total = off;
-  const long long csz[CB_CONTROL_FIELDS] = {C, E, C};
+  const long long csz[CB_CONTROL_FIELDS] = {C, E, C, nch * C};
   off = 0;
   for (int f = 0; f < CB_CONTROL_FIELDS; ++f) {
     t->layout.c[f] = off;
@@ -1020,6 +1294,10 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
   k.omdelta_dt = (1.0 - delta) * dt;
   k.delta = delta;
   k.omdelta = 1.0 - delta;
+  // The gates' advance fractions: each tableau row's sum, in numpy's order (gamma + 0 + 0 and
+  // (delta + (1 - delta)) + 0), times dt (surface_pump_v3.py:3700, entity_sum).
+  k.frac1_dt = ((gamma + 0.0) + 0.0) * dt;
+  k.frac2_dt = ((delta + (1.0 - delta)) + 0.0) * dt;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   CB_DISPATCH(launch_step, state_in, state_out, control, k, n_steps, world_status,
               accepted_steps, s);

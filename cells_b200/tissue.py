@@ -27,6 +27,7 @@ from . import _lib
 
 SPECIES_FIELDS = {"amount_increment", "membrane_transferred", "junction_transferred",
                   "reservoir_supplied"}
+CHANNEL = ("channel_gate", "channel_transferred", "channel_dissipated")
 CELL = ("amount_increment", "membrane_transferred", "membrane_dissipated", "pump_cycles",
         "pump_dissipated", "metabolic_work")
 EDGE = ("junction_transferred", "junction_dissipated", "junction_gate")
@@ -68,11 +69,17 @@ class Tissue:
                                                           dtype=np.float64),
             "gate_threshold": np.ascontiguousarray(b.gate_threshold, dtype=np.float64),
             "gate_minimum": np.ascontiguousarray(b.gate_minimum, dtype=np.float64),
+            "channel_code": np.ascontiguousarray(b.channel_code, dtype=np.int32),
+            "channel_species": np.ascontiguousarray(b.channel_species, dtype=np.int32),
+            "channel_permeability": np.ascontiguousarray(b.channel_permeability,
+                                                         dtype=np.float64),
+            "channel_abundance": np.ascontiguousarray(b.channel_abundance, dtype=np.float64),
         }
         desc = _lib.TissueDesc()
         desc.n_worlds = b.worlds
         desc.n_cells = b.cells
         desc.n_edges = b.edges
+        desc.channel_slots = b.channel_slots
         for name, arr in keep.items():
             ctype = {np.int64: ctypes.c_int64, np.int32: ctypes.c_int32}.get(arr.dtype.type,
                                                                             ctypes.c_double)
@@ -106,6 +113,10 @@ class Tissue:
     # ---------------------------------------------------------------- packing (host)
     def _shape(self, name):
         b = self.batch
+        if name == "channel_gate":
+            return (2, b.channel_slots, b.cells)
+        if name in CHANNEL:
+            return (b.channel_slots, b.cells)
         n = b.cells if name in CELL else b.edges if name in EDGE else b.worlds
         return (3, n) if name in SPECIES_FIELDS else (n,)
 
@@ -129,19 +140,25 @@ class Tissue:
             out[name] = flat[o:o + int(np.prod(shape))].reshape(shape).copy()
         return out
 
-    def pack_control(self, membrane=1.0, junction=1.0, pump=1.0):
+    def pack_control(self, membrane=1.0, junction=1.0, pump=1.0, channel=1.0):
         b = self.batch
         flat = np.zeros(self.control_size)
-        for name, value, n in (("membrane", membrane, b.cells), ("junction", junction, b.edges),
-                               ("pump", pump, b.cells)):
+        nch = b.channel_slots * b.cells
+        for name, value, shape in (("membrane", membrane, (b.cells,)),
+                                   ("junction", junction, (b.edges,)),
+                                   ("pump", pump, (b.cells,)),
+                                   ("channel", channel, (b.channel_slots, b.cells))):
             o = self.control_offsets[name]
-            flat[o:o + n] = np.broadcast_to(np.asarray(value, dtype=np.float64), (n,))
+            n = int(np.prod(shape))
+            flat[o:o + n] = np.broadcast_to(np.asarray(value, dtype=np.float64), shape).reshape(-1)
+        del nch
         return flat
 
     def initial_state(self):
         b = self.batch
         state = {name: np.zeros(self._shape(name)) for name in _lib.STATE_FIELDS}
         state["junction_gate"] = np.asarray(b.gate_initial, dtype=np.float64).copy()
+        state["channel_gate"] = np.asarray(b.channel_gate_initial, dtype=np.float64).copy()
         return state
 
     # ---------------------------------------------------------------- device entry points

@@ -47,6 +47,10 @@ typedef struct cb_tissue cb_tissue;
 #define CB_WORLD_CONTROL 8u        /* an availability outside [0, 1] or non-finite */
 #define CB_WORLD_RESIDUAL 16u      /* stage charge residual above 3e-25 C + 2e-12 |q| */
 #define CB_WORLD_DOMAIN 32u        /* accepted-state domain: amounts, gates, finite ledgers */
+#define CB_WORLD_STIFF 64u         /* dt x membrane charge-relaxation rate > 1 at a stage
+                                      (surface_pump_v3.membrane_rate, :4588) */
+#define CB_WORLD_CHANNEL_DOMAIN 128u /* a channel population off its law's -120..60 mV domain
+                                        or with non-finite kinetics (:848-858) */
 
 /* Return codes. */
 #define CB_OK 0
@@ -84,6 +88,15 @@ typedef struct cb_tissue_desc {
   const double *junction_permeability; /* [3*E] m/s */
   const double *gate_threshold; /* [E] V */
   const double *gate_minimum;   /* [E] minimum open fraction */
+  /* Voltage-gated channel populations (surface_pump_v3.channel_rates, :909-970): NCH slots per
+   * cell, NCH = 0 (none) or 2. Slot arrays are [NCH*C], slot-major. Law codes: 0 Kv1.5 (m h),
+   * 2 NaV1.2 (m^3 h) - the reference's catalogue codes - and 100 the Hodgkin-Huxley K n^4 law
+   * of this library (no counterpart in the reference). One permeant species per population. */
+  int32_t channel_slots;
+  const int32_t *channel_code;        /* [NCH*C] */
+  const int32_t *channel_species;     /* [NCH*C] 0 Na, 1 K, 2 Cl */
+  const double *channel_permeability; /* [NCH*C] m/s, maximum permeability x relative */
+  const double *channel_abundance;    /* [NCH*C] */
 } cb_tissue_desc;
 
 /* State fields in a packed state buffer, in this order (cb_state_layout gives each offset). */
@@ -101,6 +114,9 @@ enum cb_state_field {
   CB_ELECTRODE_CHARGE,          /* [W] C */
   CB_RESERVOIR_WORK,            /* [W] pJ */
   CB_ELECTRODE_WORK,            /* [W] pJ */
+  CB_CHANNEL_GATE,              /* [2][NCH][C] gate rows (m, h) of each population */
+  CB_CHANNEL_TRANSFERRED,       /* [NCH][C] fmol of each population's permeant species */
+  CB_CHANNEL_DISSIPATED,        /* [NCH][C] pJ */
   CB_STATE_FIELDS
 };
 
@@ -109,6 +125,7 @@ enum cb_control_field {
   CB_CONTROL_MEMBRANE = 0, /* [C] */
   CB_CONTROL_JUNCTION,     /* [E] */
   CB_CONTROL_PUMP,         /* [C] */
+  CB_CONTROL_CHANNEL,      /* [NCH][C] */
   CB_CONTROL_FIELDS
 };
 
