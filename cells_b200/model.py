@@ -12,9 +12,10 @@ are never mutated) and ``valid``, the unchanged state when the step is refused, 
 reference (surface_pump.py:362).
 
 Scope: the held-bath pump-leak tissue — every active cell has exactly one active membrane
-patch, every patch faces its world's held bath (a reservoir outside node), no faces, no channel
-population, species Na/K/Cl (+1/+1/-1), the Na/K-ATPase with one set of pump constants per
-world. Other worlds raise ``Unsupported`` at bind; nothing falls back to the CPU.
+patch, every patch faces its world's held bath (a reservoir outside node), no faces, species
+Na/K/Cl (+1/+1/-1), the Na/K-ATPase with one set of pump constants per world, and either no
+channel population or two per cell (Kv1.5 and/or NaV1.2 of @3's catalogue, one permeant species
+each). Other worlds raise ``Unsupported`` at bind; nothing falls back to the CPU.
 """
 
 from __future__ import annotations
@@ -69,9 +70,32 @@ class Mapping:
             raise Unsupported("finite (unheld) outside nodes need the field solve")
         if hasattr(p, "face_active") and np.any(_a(p, "face_active")):
             raise Unsupported("extracellular faces need the field solve")
-        if hasattr(p, "channel_active") and np.any(_a(p, "channel_active")):
-            raise Unsupported("channel populations are not in the device step yet")
         self.bath = int(self.baths[0])
+        # Channel populations: the same number per active cell (0 or 2), each with one permeant
+        # species; slot q of a cell is its q-th population in the reference's channel order.
+        self.nch = 0
+        self.channel_index = np.zeros((0, self.cells.size), dtype=np.int64)
+        self.channel_species = np.zeros((0, self.cells.size), dtype=np.int64)
+        if hasattr(p, "channel_active") and np.any(_a(p, "channel_active")):
+            if not all(hasattr(p, f) for f in ("channel_membranes", "channel_laws",
+                                               "channel_relative_permeability")):
+                raise Unsupported("channel populations need @3's catalogue layout")
+            active = np.flatnonzero(_a(p, "channel_active").astype(bool))
+            patch = _a(p, "channel_membranes")[active]
+            cell_of_patch = _a(p, "membrane_cell")
+            owner = cell_of_patch[patch]
+            counts = np.bincount(owner, minlength=cell_active.size)[self.cells]
+            if np.any(counts != counts[0]) or counts[0] not in (0, 2):
+                raise Unsupported("every cell needs the same number (0 or 2) of channel "
+                                  "populations")
+            self.nch = int(counts[0])
+            index = np.zeros((self.nch, self.cells.size), dtype=np.int64)
+            slot = np.zeros(cell_active.size, dtype=np.int64)
+            local = {int(c): k for k, c in enumerate(self.cells)}
+            for j, c in zip(active, owner, strict=True):
+                index[slot[c], local[int(c)]] = j
+                slot[c] += 1
+            self.channel_index = index
         local = -np.ones(cell_active.size, dtype=np.int64)
         local[self.cells] = np.arange(self.cells.size)
         self.sender = local[_a(p, "junction_sender")[self.junctions]]
@@ -85,6 +109,26 @@ def world_from_layout(p):
     if not np.array_equal(valence, worlds.VALENCE):
         raise Unsupported("species must be Na, K, Cl with valences +1, +1, -1")
     patch = m.patch_of_cell
+    nch = m.nch
+    channel = {}
+    if nch:
+        j = m.channel_index
+        laws = _a(p, "channel_laws")[j]
+        if np.any(~np.isin(laws, (0, 2))):
+            raise Unsupported("channel laws must be Kv1.5 (0) or NaV1.2 (2)")
+        rel = _a(p, "channel_relative_permeability")[:, j]  # [S, NCH, C]
+        if np.any(np.count_nonzero(rel, axis=0) != 1):
+            raise Unsupported("each channel population needs exactly one permeant species")
+        species = np.argmax(rel != 0, axis=0)
+        m.channel_species = species
+        channel = dict(
+            channel_code=laws.astype(np.int32),
+            channel_species=species.astype(np.int32),
+            channel_permeability=(_a(p, "channel_permeability")[j]
+                                  * np.take_along_axis(rel, species[None], 0)[0]),
+            channel_abundance=_a(p, "channel_abundance")[j].astype(float),
+            channel_gate_initial=np.zeros((2, nch, m.cells.size)),
+        )
     if hasattr(p, "pump_present"):
         present = _a(p, "pump_present")[patch].astype(bool)
         stoich = _a(p, "stoichiometry")[:, patch]
@@ -127,6 +171,7 @@ def world_from_layout(p):
         bath_volume=bath_volume,
         bath_potential=float(_a(p, "boundary_V")[m.bath]),
         pump=tuple(constants),
+        **channel,
     )
     return world, m
 
@@ -152,8 +197,7 @@ _BATH_MAP = (
     ("electrode_work_pJ", "electrode_work"),
 )
 _ZERO_FIELDS = ("extracellular_amount_increment", "face_transferred",
-                "face_dissipated_energy_pJ", "channel_transferred",
-                "channel_dissipated_energy_pJ")
+                "face_dissipated_energy_pJ")
 
 
 def packed_state(state, m):
@@ -167,6 +211,17 @@ def packed_state(state, m):
         out[name] = np.asarray(getattr(state, ref))[..., m.junctions].astype(float)
     for ref, name in _BATH_MAP:
         out[name] = np.asarray(getattr(state, ref))[..., m.bath:m.bath + 1].astype(float)
+    j, sp = m.channel_index, m.channel_species
+    if m.nch:
+        out["channel_gate"] = np.asarray(state.channel_gate)[:, j].astype(float)
+        out["channel_transferred"] = np.asarray(state.channel_transferred)[sp, j].astype(float)
+        out["channel_dissipated"] = np.asarray(
+            state.channel_dissipated_energy_pJ)[sp, j].astype(float)
+    else:
+        c = m.cells.size
+        out["channel_gate"] = np.zeros((2, 0, c))
+        out["channel_transferred"] = np.zeros((0, c))
+        out["channel_dissipated"] = np.zeros((0, c))
     return out
 
 
@@ -180,6 +235,11 @@ def reference_state(packed, like, m):
         fields[ref][..., m.junctions] = packed[name]
     for ref, name in _BATH_MAP:
         fields[ref][..., m.bath:m.bath + 1] = packed[name]
+    if m.nch:
+        j, sp = m.channel_index, m.channel_species
+        fields["channel_gate"][:, j] = packed["channel_gate"]
+        fields["channel_transferred"][sp, j] = packed["channel_transferred"]
+        fields["channel_dissipated_energy_pJ"][sp, j] = packed["channel_dissipated"]
     return type(like)(**fields)
 
 
@@ -204,11 +264,17 @@ class DeviceStep:
             if hasattr(state, name) and np.any(np.asarray(getattr(state, name)) != 0):
                 raise Unsupported(f"{name} must stay zero in a held-bath tissue")
         m = self.mapping
+        if m.nch:
+            moved = np.array(state.channel_transferred, copy=True)
+            moved[m.channel_species, m.channel_index] = 0.0
+            if np.any(moved != 0):
+                raise Unsupported("channel transfer of a non-permeant species must stay zero")
         packed = packed_state(state, m)
         ctl = self.tissue.pack_control(
             membrane=np.asarray(control.membrane)[m.patch_of_cell],
             junction=np.asarray(control.junction)[m.junctions],
             pump=np.asarray(control.pump)[m.patch_of_cell],
+            channel=(np.asarray(control.channel)[m.channel_index] if m.nch else 1.0),
         )
         out, status, _ = self.tissue.step_host(self.tissue.pack_state(packed), ctl, float(dt), 1)
         valid = bool(status[0] == 0)

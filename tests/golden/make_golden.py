@@ -26,6 +26,8 @@ Fixtures:
                          population per cell, partial channel availabilities, @3, 300 steps.
   ars222_v3_channels_delaunay.npz  A 40-cell Delaunay world with both populations, gated
                          junctions, partial controls, a -4 mV bath, @3, 200 steps.
+  pytrees_v3_channels_padded.npz  That world's @3 pytrees with every capacity 2 above its count
+                         (layout, controls, padded states over 40 steps), for the drop-in step.
   laws.npz               Point laws on grids of inputs: bernoulli, the pump kinetics and the
                          junction gate rate.
 """
@@ -100,6 +102,12 @@ LAYOUT_FIELDS = (
 )
 
 
+CHANNEL_LAYOUT_FIELDS = (
+    "channel_membranes", "channel_laws", "channel_relative_permeability",
+    "channel_permeability", "channel_abundance", "channel_gate_active",
+)
+
+
 def _run_reference_pytrees(world, *, model_id, dt, steps, keep, padding, controls):
     """The reference's own pytrees: layout fields, controls and full states (padded slots)."""
     from cells.definitions.specs import parse_spec
@@ -112,11 +120,15 @@ def _run_reference_pytrees(world, *, model_id, dt, steps, keep, padding, control
     spec = parse_spec(raw)
     model = get_model(spec.model)
     state, p = model.initial_values(spec)
-    from cells.execution.schedule import control_values
+    if model_id.endswith("@3"):
+        from cells.definitions.surface_pump_v3_spec import control_values
+    else:
+        from cells.execution.schedule import control_values
 
     cv = control_values(spec, [0.0])
     control = type(cv)(*(v[0] for v in cv))
-    out = {"layout_" + f: np.asarray(getattr(p, f)) for f in LAYOUT_FIELDS}
+    fields = LAYOUT_FIELDS + tuple(f for f in CHANNEL_LAYOUT_FIELDS if hasattr(p, f))
+    out = {"layout_" + f: np.asarray(getattr(p, f)) for f in fields}
     out.update({"control_ref_" + f: np.asarray(v) for f, v in control._asdict().items()})
     snaps = []
     for k in range(0, steps + 1):
@@ -265,6 +277,12 @@ def make_channel_trajectories():
         pump_control=rng.uniform(0.5, 1.0, dworld.cells),
         channel_control=rng.uniform(0.3, 1.0, (2, dworld.cells)),
     )
+    # @3's own padded channel pytrees for the drop-in step.
+    out = _run_reference_pytrees(dworld, model_id=v3, dt=1e-3, steps=40, keep={0, 1, 20, 40},
+                                 padding=2, controls=controls)
+    np.savez_compressed(os.path.join(HERE, "pytrees_v3_channels_padded.npz"), **out)
+    print("pytrees_v3_channels_padded.npz written")
+
     keep = {0, 1, 2, 10, 100, 200}
     stacked, kept, el = _run(dworld, model_id=v3, dt=1e-3, steps=200, keep=keep, solver=ars,
                              controls=controls, channels=True)

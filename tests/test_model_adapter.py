@@ -26,8 +26,20 @@ def test_layout_maps_to_the_same_world():
     assert world.pump == ref.pump
 
 
-def test_state_round_trip_keeps_padding():
-    _, p, _, states = load_pytrees()
+def test_channel_layout_maps_to_the_same_world():
+    _, p, _, _ = load_pytrees("pytrees_v3_channels_padded.npz")
+    world, m = model.world_from_layout(p)
+    _, b = load_golden("ars222_v3_channels_delaunay.npz")
+    ref = b.world(0)
+    assert m.nch == 2
+    for name in ("channel_code", "channel_species", "channel_permeability",
+                 "channel_abundance", "permeability", "junction_permeability", "sender"):
+        assert np.array_equal(getattr(world, name), getattr(ref, name)), name
+
+
+@pytest.mark.parametrize("name", ["pytrees_gated_padded.npz", "pytrees_v3_channels_padded.npz"])
+def test_state_round_trip_keeps_padding(name):
+    _, p, _, states = load_pytrees(name)
     _, m = model.world_from_layout(p)
     for st in states:
         packed = model.packed_state(st, m)
