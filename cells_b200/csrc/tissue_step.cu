@@ -811,61 +811,61 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   }
 }
 
-// Ledger residuals per world (the reference's balances(), held-bath worlds).
-template <int BLOCK, int EPT>
-__global__ void __launch_bounds__(BLOCK) balances_kernel(const Tissue T, const Layout L,
-                                                         const double *__restrict__ st,
-                                                         double *__restrict__ out) {
-  extern __shared__ double smem[];
-  double *sJ = smem;                    // [3][EPT*BLOCK]
-  double *sRed = sJ + 3 * EPT * BLOCK;  // [BLOCK/32][8]
-  __shared__ double sW[WC_STRIDE];
+#include "packed_step.cuh"
+
+// Ledger residuals per world (the reference's balances(), held-bath worlds): one 256-thread CTA
+// per world, looping over its cells; junction transfers read through each cell's adjacency.
+constexpr int kBalanceBlock = 256;
+
+__global__ void __launch_bounds__(kBalanceBlock) balances_kernel(const Tissue T, const Layout L,
+                                                                 const double *__restrict__ st,
+                                                                 double *__restrict__ out) {
+  __shared__ double sRed[(kBalanceBlock / 32) * 8];
   const int w = blockIdx.x, tid = threadIdx.x;
   const int c0 = T.cell_offset[w], nc = T.cell_offset[w + 1] - c0;
-  const int e0 = T.edge_offset[w], ne = T.edge_offset[w + 1] - e0;
-  if (tid < WC_STRIDE) sW[tid] = T.world[(size_t)w * WC_STRIDE + tid];
-  for (int q = 0; q < EPT; ++q) {
-    const int e = tid + q * BLOCK;
-    if (e < ne)
-      for (int s = 0; s < 3; ++s)
-        sJ[s * EPT * BLOCK + e] = st[L.s[CB_JUNCTION_TRANSFERRED] + (long long)s * T.E + e0 + e];
-  }
-  __syncthreads();
-  double local = 0.0, metabolic = 0.0, moved[3] = {0, 0, 0}, di[3] = {0, 0, 0}, pl = 0.0;
-  if (tid < nc) {
-    const int gi = c0 + tid;
+  const int e0 = T.edge_offset[w];
+  const long long C = T.C, E = T.E;
+  const int nch = T.nch;
+  const double *wc = T.world + (size_t)w * WC_STRIDE;
+  double local = 0.0, metabolic = 0.0;
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};  // moved[3], amounts[3], plate
+  for (int cl = tid; cl < nc; cl += kBalanceBlock) {
+    const long long gi = c0 + cl;
     const double stoich[3] = {-3.0, 2.0, 0.0};
     const double pc = st[L.s[CB_PUMP_CYCLES] + gi];
     double send[3] = {0, 0, 0}, recv[3] = {0, 0, 0};
     for (int a = T.adj_ptr[gi]; a < T.adj_ptr[gi + 1]; ++a) {
-      const int code = T.adj_idx[a], e = code >> 1;
+      const int code = T.adj_idx[a];
+      const long long ge = e0 + (code >> 1);
       for (int s = 0; s < 3; ++s) {
-        if (code & 1) recv[s] += sJ[s * EPT * BLOCK + e];
-        else send[s] += sJ[s * EPT * BLOCK + e];
+        const double j = st[L.s[CB_JUNCTION_TRANSFERRED] + s * E + ge];
+        if (code & 1) recv[s] += j;
+        else send[s] += j;
       }
     }
-    double n[3];
+    double n[3], moved[3];
     for (int s = 0; s < 3; ++s) {
-      n[s] = st[L.s[CB_AMOUNT_INCREMENT] + (long long)s * T.C + gi];
-      const double total_m = st[L.s[CB_MEMBRANE_TRANSFERRED] + (long long)s * T.C + gi] -
-                             stoich[s] * pc;
-      local = fmax(local, fabs(((n[s] + total_m) + send[s]) - recv[s]));
-      moved[s] = total_m;
-      di[s] = n[s];
+      n[s] = st[L.s[CB_AMOUNT_INCREMENT] + s * C + gi];
+      moved[s] = st[L.s[CB_MEMBRANE_TRANSFERRED] + s * C + gi];
     }
-    metabolic = fabs(st[L.s[CB_METABOLIC_WORK] + gi] + 1e-3 * sW[WC_DRIVE] * pc);
-    pl = -(kChargePerFmol * ((n[0] + n[1]) + (-n[2])));
+    for (int q = 0; q < nch; ++q) {  // channel_to_membrane
+      const int sp = T.ch_species[q * C + gi];
+      moved[sp] += st[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi];
+    }
+    for (int s = 0; s < 3; ++s) {
+      const double total_m = moved[s] - stoich[s] * pc;
+      local = fmax(local, fabs(((n[s] + total_m) + send[s]) - recv[s]));
+      v[s] += total_m;
+      v[3 + s] += n[s];
+    }
+    metabolic = fmax(metabolic, fabs(st[L.s[CB_METABOLIC_WORK] + gi] + 1e-3 * wc[WC_DRIVE] * pc));
+    v[6] += -(kChargePerFmol * ((n[0] + n[1]) + (-n[2])));
   }
-  double v[7] = {moved[0], moved[1], moved[2], di[0], di[1], di[2], pl};
-  block_sum<BLOCK, 7>(v, sRed);
+  block_sum<kBalanceBlock, 7>(v, sRed);
   double mx[2] = {local, metabolic};
-  // max-reduce through shared memory (fixed order)
+  for (int q = 0; q < 2; ++q)
+    for (int o = 16; o > 0; o >>= 1) mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], o));
   __syncthreads();
-  for (int k2 = 0; k2 < 2; ++k2) {
-    double m = mx[k2];
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    mx[k2] = m;
-  }
   if ((tid & 31) == 0) {
     sRed[(tid >> 5) * 8 + 0] = mx[0];
     sRed[(tid >> 5) * 8 + 1] = mx[1];
@@ -873,32 +873,28 @@ __global__ void __launch_bounds__(BLOCK) balances_kernel(const Tissue T, const L
   __syncthreads();
   if (tid == 0) {
     double ml = 0.0, mm = 0.0;
-    for (int q = 0; q < BLOCK / 32; ++q) {
+    for (int q = 0; q < kBalanceBlock / 32; ++q) {
       ml = fmax(ml, sRed[q * 8]);
       mm = fmax(mm, sRed[q * 8 + 1]);
     }
-    double outside = 0.0, total = 0.0, supply_charge_terms[3];
+    double outside = 0.0, total = 0.0, sup[3];
     for (int s = 0; s < 3; ++s) {
-      const double sup = st[L.s[CB_RESERVOIR_SUPPLIED] + (long long)s * T.W + w];
-      outside = fmax(outside, fabs(-v[s] - sup));
-      total = fmax(total, fabs(v[3 + s] - sup));
-      supply_charge_terms[s] = sup;
+      sup[s] = st[L.s[CB_RESERVOIR_SUPPLIED] + s * (long long)T.W + w];
+      outside = fmax(outside, fabs(-v[s] - sup[s]));
+      total = fmax(total, fabs(v[3 + s] - sup[s]));
     }
     const double ec = st[L.s[CB_ELECTRODE_CHARGE] + w];
     const double rw = st[L.s[CB_RESERVOIR_WORK] + w];
     const double ew = st[L.s[CB_ELECTRODE_WORK] + w];
-    const double supply_charge =
-        kChargePerFmol * ((supply_charge_terms[0] + supply_charge_terms[1]) - supply_charge_terms[2]);
-    const double Vb = sW[WC_VB];
-    double* o = out + (size_t)w * 8;
+    const double supply_charge = kChargePerFmol * ((sup[0] + sup[1]) - sup[2]);
+    double *o = out + (size_t)w * 8;
     o[0] = ml;
     o[1] = outside;
     o[2] = total;
     o[3] = fabs(ec - v[6]);
     o[4] = fabs(ec + supply_charge);
-    o[5] = fabs(rw - 1e-3 * ((sW[WC_MUB] * supply_charge_terms[0] + sW[WC_MUB + 1] * supply_charge_terms[1]) +
-                             sW[WC_MUB + 2] * supply_charge_terms[2]));
-    o[6] = fabs(ew - 1e12 * Vb * ec);
+    o[5] = fabs(rw - 1e-3 * ((wc[WC_MUB] * sup[0] + wc[WC_MUB + 1] * sup[1]) + wc[WC_MUB + 2] * sup[2]));
+    o[6] = fabs(ew - 1e12 * wc[WC_VB] * ec);
     o[7] = mm;
   }
 }
@@ -937,6 +933,13 @@ struct cb_tissue {
   Layout layout{};
   long long state_total = 0, control_total = 0;
   std::vector<void *> owned;  // device allocations
+  // The packed persistent kernel (uneven or large worlds): work items, scratch, ticket counter.
+  bool packed = false;
+  int packed_block = 512;
+  int grid_ctas = 0;
+  Packed pk{};
+  double *scratch = nullptr;
+  size_t scratch_bytes = 0;
   // Buffers of the host-pointer entry point, allocated on first use.
   double *h_state = nullptr, *h_control = nullptr;
   uint32_t *h_status = nullptr;
@@ -965,10 +968,6 @@ size_t step_smem(int block, int ept, int nch) {
 }
 constexpr size_t kMaxSmemPerBlock = 227 * 1024;
 
-size_t balances_smem(int block, int ept) {
-  return sizeof(double) * (size_t)(3 * ept * block + (block / 32) * 8);
-}
-
 template <int BLOCK, int EPT>
 int launch_step(cb_tissue *t, const double *in, double *out, const double *control,
                 const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
@@ -995,17 +994,44 @@ int launch_step(cb_tissue *t, const double *in, double *out, const double *contr
   return CB_OK;
 }
 
-template <int BLOCK, int EPT>
 int launch_balances(cb_tissue *t, const double *st, double *out, cudaStream_t stream) {
-  const size_t smem = balances_smem(BLOCK, EPT);
-  auto kern = balances_kernel<BLOCK, EPT>;
+  balances_kernel<<<t->W, kBalanceBlock, 0, stream>>>(t->t, t->layout, st, out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "balances launch");
+  return CB_OK;
+}
+
+template <int BLOCK, int NCH>
+int launch_packed_bn(cb_tissue *t, const double *in, double *out, const double *control,
+                     const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
+                     cudaStream_t stream) {
+  const size_t smem = packed_smem_bytes(t->pk.cap);
+  auto kern = packed_kernel<BLOCK, NCH>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-  kern<<<t->W, BLOCK, smem, stream>>>(t->t, t->layout, st, out);
+  e = cudaMemsetAsync(t->pk.queue, 0, sizeof(unsigned int), stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  kern<<<t->grid_ctas, BLOCK, smem, stream>>>(t->t, t->layout, t->pk, in, out, control, k,
+                                              n_steps, status, taken);
   e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "balances launch");
+  if (e != cudaSuccess) return cuda_fail(e, "packed launch");
   return CB_OK;
+}
+
+int launch_packed(cb_tissue *t, const double *in, double *out, const double *control,
+                  const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
+                  cudaStream_t stream) {
+  const int key = t->packed_block * 10 + t->t.nch;
+  switch (key) {
+    case 2560: return launch_packed_bn<256, 0>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 2562: return launch_packed_bn<256, 2>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 5120: return launch_packed_bn<512, 0>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 5122: return launch_packed_bn<512, 2>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 10240: return launch_packed_bn<1024, 0>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 10242: return launch_packed_bn<1024, 2>(t, in, out, control, k, n_steps, status, taken, stream);
+    default: return fail(CB_ERR_UNSUPPORTED, "no packed kernel for this block size");
+  }
 }
 
 #define CB_DISPATCH(FN, ...)                                                     \
@@ -1061,23 +1087,37 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
     const long long ne = d->edge_offset[w + 1] - d->edge_offset[w];
     if (nc < 1) return fail(CB_ERR_LAYOUT, "every world needs at least one cell");
     if (ne < 0) return fail(CB_ERR_LAYOUT, "junction offsets must not decrease");
-    if (nc > 1024) return fail(CB_ERR_UNSUPPORTED, "worlds of more than 1024 cells");
+    if (nc > 4096) return fail(CB_ERR_UNSUPPORTED, "worlds of more than 4096 cells");
     max_cells = std::max<int>(max_cells, (int)nc);
     max_edges = std::max(max_edges, ne);
   }
   int block = 128;
   while (block < max_cells) block *= 2;
   const int ept = (int)std::max<long long>(1, (max_edges + block - 1) / block);
-  if (ept > 4) return fail(CB_ERR_UNSUPPORTED, "more than 4 junctions per thread");
   const int desc_nch = d->channel_slots;
+  // Kernel path: one world per CTA in shared memory (uniform worlds of up to 1024 cells), or the
+  // packed persistent kernel (uneven or large worlds, up to 4096 cells).
+  bool min_eq_max = true;
+  for (int w = 1; w < W; ++w)
+    min_eq_max = min_eq_max && (d->cell_offset[w + 1] - d->cell_offset[w] ==
+                                d->cell_offset[1] - d->cell_offset[0]);
+  const bool shared_ok = block <= 1024 && ept <= 4 && desc_nch >= 0 && desc_nch <= 2 &&
+                         step_smem(block, ept, desc_nch) <= kMaxSmemPerBlock;
+  bool use_packed = !shared_ok || !(min_eq_max || max_cells <= 256);
+  if (const char *env = std::getenv("CELLS_B200_KERNEL")) {
+    if (!std::strcmp(env, "packed")) use_packed = true;
+    if (!std::strcmp(env, "shared") && shared_ok) use_packed = false;
+  }
+  int cap = 1024;
+  while (cap < max_cells) cap *= 2;
+  if (use_packed && packed_smem_bytes(cap) > kMaxSmemPerBlock)
+    return fail(CB_ERR_UNSUPPORTED, "world too large for the packed step");
   if (desc_nch != 0 && desc_nch != 2)
     return fail(CB_ERR_UNSUPPORTED, "channel slots per cell must be 0 or 2");
   if (desc_nch && (!d->channel_code || !d->channel_species || !d->channel_permeability ||
                    !d->channel_abundance))
     return fail(CB_ERR_ARGUMENT, "null channel array in the tissue description");
-  if (step_smem(block, ept, desc_nch) > kMaxSmemPerBlock)
-    return fail(CB_ERR_UNSUPPORTED, "world too large for the shared-memory step (cells x "
-                                    "junctions per world)");
+
   for (long long q = 0; q < (long long)desc_nch * C; ++q) {
     const int code = d->channel_code[q], sp = d->channel_species[q];
     if (code != 0 && code != 2 && code != 100)
@@ -1175,6 +1215,11 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
   t->E = (int)E;
   t->block = block;
   t->ept = ept;
+  t->packed = use_packed;
+  if (const char *env = std::getenv("CELLS_B200_PACKED_BLOCK")) {
+    const int b = std::atoi(env);
+    if (b == 256 || b == 512 || b == 1024) t->packed_block = b;
+  }
   if (const char *env = std::getenv("CELLS_B200_OCCUPANCY")) t->occupancy = std::atoi(env) == 2 ? 2 : 3;
   std::vector<int> co32(W + 1), eo32(W + 1), snd(E), rcv(E);
   for (int w = 0; w <= W; ++w) {
@@ -1223,6 +1268,81 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
     if (!rc) rc = upload(t, species, &T.ch_species);
     if (!rc) rc = upload(t, chap, &T.ch_ap);
     if (!rc) rc = upload(t, chab, &T.ch_ab);
+  }
+  if (!rc && use_packed) {
+    // Work items: runs of consecutive worlds of at most `cap` cells and kPackedMaxWorlds worlds,
+    // queued largest first.
+    std::vector<int> item_world0{0}, cell_world(C), isnd(E), ircv(E), iadj(adj_idx.size());
+    long long cells_in = 0;
+    int worlds_in = 0;
+    for (int w = 0; w < W; ++w) {
+      const long long nc = d->cell_offset[w + 1] - d->cell_offset[w];
+      if (worlds_in > 0 && (cells_in + nc > cap || worlds_in == kPackedMaxWorlds)) {
+        item_world0.push_back(w);
+        cells_in = 0;
+        worlds_in = 0;
+      }
+      cells_in += nc;
+      ++worlds_in;
+    }
+    item_world0.push_back(W);
+    const int n_items = (int)item_world0.size() - 1;
+    std::vector<long long> item_cells(n_items);
+    for (int it = 0; it < n_items; ++it) {
+      const int a = item_world0[it], b = item_world0[it + 1];
+      const long long ic0 = d->cell_offset[a], ie0 = d->edge_offset[a];
+      item_cells[it] = d->cell_offset[b] - ic0;
+      for (int w = a; w < b; ++w) {
+        for (long long c = d->cell_offset[w]; c < d->cell_offset[w + 1]; ++c) {
+          cell_world[c] = w - a;
+          for (int q = adj_ptr[c]; q < adj_ptr[c + 1]; ++q) {
+            const int code = adj_idx[q];
+            const long long item_edge = d->edge_offset[w] + (code >> 1) - ie0;
+            iadj[q] = (int)((item_edge << 1) | (code & 1));
+          }
+        }
+        for (long long e = d->edge_offset[w]; e < d->edge_offset[w + 1]; ++e) {
+          isnd[e] = (int)(d->cell_offset[w] - ic0 + d->sender[e]);
+          ircv[e] = (int)(d->cell_offset[w] - ic0 + d->receiver[e]);
+        }
+      }
+    }
+    std::vector<int> order(n_items);
+    for (int it = 0; it < n_items; ++it) order[it] = it;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return item_cells[a] > item_cells[b]; });
+    Packed &P = t->pk;
+    P.n_items = n_items;
+    P.cap = cap;
+    rc = upload(t, order, &P.order);
+    if (!rc) rc = upload(t, item_world0, &P.item_world0);
+    if (!rc) rc = upload(t, cell_world, &P.cell_world);
+    if (!rc) rc = upload(t, isnd, &P.isnd);
+    if (!rc) rc = upload(t, ircv, &P.ircv);
+    if (!rc) rc = upload(t, iadj, &P.iadj);
+    if (!rc) {
+      void *q = nullptr;
+      cudaError_t e = cudaMalloc(&q, sizeof(unsigned int));
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc");
+      else {
+        t->owned.push_back(q);
+        P.queue = static_cast<unsigned int *>(q);
+      }
+    }
+    if (!rc) {
+      t->scratch_bytes = sizeof(double) * ((size_t)packed_cell_fields(desc_nch) * C +
+                                           (size_t)SE_FIELDS * std::max<long long>(E, 1));
+      void *sc = nullptr;
+      cudaError_t e = cudaMalloc(&sc, t->scratch_bytes);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc scratch");
+      else {
+        t->owned.push_back(sc);
+        P.sc = static_cast<double *>(sc);
+      }
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    t->grid_ctas = std::max(1, std::min(sms, n_items));
   }
   if (rc) {
     cb_free(t);
@@ -1299,6 +1419,9 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
   k.frac1_dt = ((gamma + 0.0) + 0.0) * dt;
   k.frac2_dt = ((delta + (1.0 - delta)) + 0.0) * dt;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (t->packed)
+    return launch_packed(t, state_in, state_out, control, k, n_steps, world_status,
+                         accepted_steps, s);
   CB_DISPATCH(launch_step, state_in, state_out, control, k, n_steps, world_status,
               accepted_steps, s);
 }
@@ -1339,7 +1462,7 @@ int cb_balances(cb_tissue *t, const double *state, double *out, void *stream) {
   cudaError_t ce = cudaSetDevice(t->device);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  CB_DISPATCH(launch_balances, state, out, s);
+  return launch_balances(t, state, out, s);
 }
 
 }  // extern "C"
