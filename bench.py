@@ -1,10 +1,15 @@
 #!/usr/bin/env python
 """Benchmark: world·cell-steps/s of the batched FP64 tissue step on B200 (one JSON line).
 
-Workload (the batched plain step): 4096 independent worlds per GPU, each a 16x16-grid pump-leak
-tissue (256 cells, 480 gap junctions, Na/K/Cl, GHK leaks, Na/K-ATPase, held bath), per-world
-parameters drawn from one seed; ARS(2,2,2) IMEX step in FP64 at dt = 1 ms
-(cells.solver.imex_ars222_face_electromigration@1). A bench step is one time step of every world.
+Workloads (``--workload``):
+  grid    (default) the batched plain step: 4096 independent worlds per GPU, each a 16x16-grid
+          pump-leak tissue (256 cells, 480 gap junctions, Na/K/Cl, GHK leaks, Na/K-ATPase, held
+          bath), per-world parameters drawn from one seed; ARS(2,2,2) IMEX step in FP64 at
+          dt = 1 ms (cells.solver.imex_ars222_face_electromigration@1);
+  uneven  1024 worlds of 32-4096 cells (log-uniform), Delaunay contact graphs, NaV1.2 (m^3 h)
+          and Hodgkin-Huxley K (n^4) populations on every cell, FP64, through the packed
+          persistent kernel.
+A bench step is one time step of every world.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -33,10 +38,18 @@ sys.path.insert(0, ROOT)
 METRIC = "world·cell-steps/s"
 UNIT = "world·cell-steps/s"
 METHOD = "cells.solver.imex_ars222_face_electromigration@1"
-# Algorithmic bytes per world·cell·step of the plain FP64 step: the state read and written once
-# and the parameters read once per step (per cell: 2*8*(2S+4) state + 8*(4+S) parameters; per
-# junction: 2*8*(S+2) state + 8 + 8*(1+S) parameters; S = 3, 1.875 junctions per cell).
-BYTES_PER_CELL_STEP = 441.0
+
+
+def bytes_per_cell_step(batch):
+    """Algorithmic bytes per world·cell·step: the state read and written once and the parameters
+    read once per step. Per cell 2*8*(2S+4) state + 8*(4+S) parameters; per channel population
+    2*8*4 state (two gate rows, transferred, dissipated) + 2*8 parameters; per junction
+    2*8*(S+2) state + 8 + 8*(1+S) parameters; S = 3. The 16x16 grid (1.875 junctions per cell)
+    gives 441 B."""
+    s = 3
+    per_cell = 2 * 8 * (2 * s + 4) + 8 * (4 + s) + batch.channel_slots * (2 * 8 * 4 + 2 * 8)
+    per_edge = 2 * 8 * (s + 2) + 8 + 8 * (1 + s)
+    return per_cell + per_edge * batch.edges / batch.cells
 
 
 def parse():
@@ -45,7 +58,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=100)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--workload", choices=("grid", "uneven"), default="grid")
+    ap.add_argument("--worlds", type=int, default=None,
+                    help="worlds per GPU (default 4096 for grid, 1024 for uneven)")
     ap.add_argument("--side", type=int, default=16)
     ap.add_argument("--dt", type=float, default=1e-3)
     ap.add_argument("--fuse", type=int, default=100,
@@ -129,13 +144,37 @@ class Clocks:
         }
 
 
-def build_batch(n_worlds, side, rank):
+def build_batch(args, rank):
     from cells_b200 import worlds
 
+    if args.workload == "uneven":  # each rank its own seed
+        return worlds.pack(worlds.delaunay_tissues(args.worlds, seed=2 + rank,
+                                                   channels=worlds.UNEVEN_CHANNELS))
     # Each rank its own worlds: world ids rank*n .. rank*n + n - 1 of seed 1.
-    ws = [worlds.grid_world(side, side, worlds.world_rng(1, rank * n_worlds + w))
-          for w in range(n_worlds)]
+    ws = [worlds.grid_world(args.side, args.side, worlds.world_rng(1, rank * args.worlds + w))
+          for w in range(args.worlds)]
     return worlds.pack(ws)
+
+
+def sample_tasks(args, n, steps):
+    """A strided sample of n of the workload's worlds, as CPU-baseline tasks."""
+    from cells_b200 import worlds
+
+    stride = max(1, args.worlds // n)
+    if args.workload == "uneven":
+        sizes = np.sort(worlds.uneven_sizes(args.worlds, seed=2))[::-1]
+        return [("uneven", w * stride, 2, int(sizes[w * stride]), steps, args.dt)
+                for w in range(n)], stride
+    return [("grid", w * stride, 1, args.side, steps, args.dt) for w in range(n)], stride
+
+
+def workload_name(args):
+    if args.workload == "uneven":
+        return (f"uneven batch: {args.worlds} worlds per GPU of 32-4096 cells (log-uniform), "
+                "Delaunay contacts, NaV1.2 m^3 h + HH K n^4 populations, FP64, "
+                f"dt {args.dt:g} s")
+    return (f"batched plain step: {args.worlds} worlds per GPU x {args.side}x{args.side} grid "
+            f"tissues, FP64, dt {args.dt:g} s")
 
 
 def cpu_baseline(args, samples_per_core=2, steps=100):
@@ -145,17 +184,17 @@ def cpu_baseline(args, samples_per_core=2, steps=100):
 
     cores = os.cpu_count() or 1
     n = cores * samples_per_core
-    stride = max(1, args.worlds // n)
-    tasks = [("grid", w * stride, 1, args.side, steps, args.dt) for w in range(n)]
+    if args.workload == "uneven":
+        steps = max(2, steps // 10)
+    tasks, stride = sample_tasks(args, n, steps)
     cell_steps, wall, procs = cb.measure(tasks, cores)
     return {
         "value": cell_steps / wall,
         "unit": UNIT,
         "cores": procs,
         "kind": "port",
-        "sample": (f"{n} of the {args.worlds} worlds (every {stride}th, {args.side}x{args.side} "
-                   f"grid), {steps} ARS(2,2,2) steps each, one world per process, 1 BLAS thread, "
-                   f"{wall:.1f} s wall"),
+        "sample": (f"{n} of the {args.worlds} worlds (every {stride}th), {steps} ARS(2,2,2) "
+                   f"steps each, one world per process, 1 BLAS thread, {wall:.1f} s wall"),
     }
 
 
@@ -168,9 +207,8 @@ def run_reference(args, rank):
 
     cores = os.cpu_count() or 1
     n = cores * 2
-    stride = max(1, args.worlds // n)
-    per_task = 10
-    tasks = [("grid", w * stride, 1, args.side, per_task, args.dt) for w in range(n)]
+    per_task = 10 if args.workload == "grid" else 1
+    tasks, stride = sample_tasks(args, n, per_task)
     with cb.pool(cores) as pool:
         pool.map(cb.prepare, tasks, chunksize=1)
         for _ in range(max(args.warmup, 0)):
@@ -182,17 +220,15 @@ def run_reference(args, rank):
             done += sum(r[0] for r in res)
         wall = time.perf_counter() - t0
     value = done / wall
-    sample = (f"{n} of the {args.worlds} worlds (every {stride}th, {args.side}x{args.side} grid) "
-              f"advanced {per_task} ARS(2,2,2) steps per bench step, one world per process, "
-              "1 BLAS thread")
+    sample = (f"{n} of the {args.worlds} worlds (every {stride}th) advanced {per_task} "
+              "ARS(2,2,2) steps per bench step, one world per process, 1 BLAS thread")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded 16x16-grid pump-leak tissues)", "impl": "reference",
-        "config": {"workload": (f"batched plain step: {args.worlds} worlds x {args.side}x"
-                                f"{args.side} grid tissues, FP64, dt {args.dt:g} s (sampled)"),
-                   "method": METHOD, "sample": sample},
+        "data": "synthetic (seeded pump-leak tissues)", "impl": "reference",
+        "config": {"workload": workload_name(args) + " (sampled)", "method": METHOD,
+                   "sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -203,6 +239,8 @@ def run_reference(args, rank):
 
 def main():
     args = parse()
+    if args.worlds is None:
+        args.worlds = 1024 if args.workload == "uneven" else 4096
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -229,7 +267,7 @@ def main():
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
 
-    batch = build_batch(args.worlds, args.side, rank)
+    batch = build_batch(args, rank)
     tissue = Tissue(batch, device=local_rank)
     cells = batch.cells
     fuse = max(d for d in range(1, max(1, min(args.fuse, args.steps)) + 1) if args.steps % d == 0)
@@ -312,20 +350,19 @@ def main():
     if rank == 0:
         peak, peak_kind = peaks()
         per_launch_s = ms * 1e-3 / launches
-        algorithmic = BYTES_PER_CELL_STEP * cells * fuse
+        algorithmic = bytes_per_cell_step(batch) * cells * fuse
         achieved = algorithmic / per_launch_s / 1e9
-        traffic = traffic_per_cell_launch()
+        traffic = traffic_per_cell_launch() if args.workload == "grid" else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded 16x16-grid pump-leak tissues)",
+            "data": "synthetic (seeded pump-leak tissues)",
             "config": {
-                "workload": (f"batched plain step: {args.worlds} worlds per GPU x "
-                             f"{args.side}x{args.side} grid tissues ({batch.cells // batch.worlds}"
-                             f" cells, {batch.edges // batch.worlds} junctions), FP64, "
-                             f"dt {args.dt:g} s"),
+                "workload": workload_name(args),
                 "method": METHOD, "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
+                "cells_per_gpu": cells, "junctions_per_gpu": batch.edges,
+                "bytes_per_cell_step": bytes_per_cell_step(batch),
                 "parallelism": f"independent worlds x{world_size} (no collective)",
                 "l2": (f"inputs larger than L2: state {tissue.state_size * 8 / 1e6:.0f} MB + "
                        "parameters per GPU"),

@@ -32,6 +32,8 @@ def _world(kind, w, seed, size):
 
         if kind == "grid":
             world = worlds.grid_world(size, size, worlds.world_rng(seed, w))
+        elif kind == "uneven":  # the uneven batch's world w (size given), with its channels
+            world = worlds.uneven_world(w, size, seed, worlds.UNEVEN_CHANNELS)
         else:
             world = worlds.delaunay_world(size, worlds.world_rng(seed, w))
         b = worlds.pack([world])
