@@ -51,6 +51,7 @@ EXPORTS = (
     "cb_control_layout",
     "cb_step",
     "cb_step_host",
+    "cb_step_packed_static",
     "cb_balances",
     "cb_last_error",
     "cb_version",
@@ -131,6 +132,9 @@ def load(path=LIBRARY):
     lib.cb_step_host.argtypes = [_p, ctypes.c_int, _p, _p, ctypes.c_double, _p, ctypes.c_int,
                                  _p, _p]
     lib.cb_step_host.restype = ctypes.c_int
+    lib.cb_step_packed_static.argtypes = [_p, _p, _p, ctypes.c_double, _p, ctypes.c_int, _p,
+                                          _p, _p]
+    lib.cb_step_packed_static.restype = ctypes.c_int
     lib.cb_balances.argtypes = [_p, _p, _p, _p]
     lib.cb_balances.restype = ctypes.c_int
     lib.cb_last_error.argtypes = []

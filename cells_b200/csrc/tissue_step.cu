@@ -35,6 +35,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1466,3 +1467,111 @@ int cb_balances(cb_tissue *t, const double *state, double *out, void *stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// The packed step on library-held scratch (cb_step_packed_static).
+//
+// The packed kernel needs scratch beyond its inputs and outputs: stage accumulators, junction
+// fluxes, world-sum terms and its work-queue ticket counter. cb_step takes that from memory the
+// handle allocated at bind. This entry point takes it instead from one array that every process
+// loading the library holds on each GPU it uses, so the call itself allocates nothing. The
+// counter lives in the array's first 256 bytes and is cleared before every launch; the rest is
+// written before it is read, so what a previous call left there does no harm. Two calls whose
+// kernels overlap on a GPU (different streams, or different threads) share the array and race.
+
+// 2^21 doubles = 16 MiB per GPU, held until the process exits.
+constexpr size_t kStaticScratchDoubles = size_t(1) << 21;
+constexpr size_t kStaticCounterDoubles = 32;  // 256 bytes: the ticket counter
+static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+double *g_static_ptr[kStaticMaxDevices] = {};
+std::mutex g_static_mutex;
+
+// The device address of g_static_scratch on the current device (host code may not use the
+// symbol itself: on the host it names a stand-in, not device memory). Looked up once per device.
+int static_scratch(int device, double **out) {
+  if (device < 0 || device >= kStaticMaxDevices)
+    return fail(CB_ERR_UNSUPPORTED, "device ordinal beyond the static scratch table");
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_ptr[device]) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+    g_static_ptr[device] = static_cast<double *>(ptr);
+  }
+  *out = g_static_ptr[device];
+  return CB_OK;
+}
+
+template <int BLOCK, int NCH>
+int launch_packed_with(cb_tissue *t, const Packed &P, const double *in, double *out,
+                       const double *control, const StepCoef &k, int n_steps, uint32_t *status,
+                       int32_t *taken, cudaStream_t stream) {
+  const size_t smem = packed_smem_bytes(P.cap);
+  auto kern = packed_kernel<BLOCK, NCH>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  e = cudaMemsetAsync(P.queue, 0, sizeof(unsigned int), stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  kern<<<t->grid_ctas, BLOCK, smem, stream>>>(t->t, t->layout, P, in, out, control, k, n_steps,
+                                              status, taken);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "packed launch (static scratch)");
+  return CB_OK;
+}
+
+}  // namespace
+
+extern "C" int cb_step_packed_static(cb_tissue *t, const double *state_in, double *state_out,
+                                     double dt, const double *control, int n_steps,
+                                     uint32_t *world_status, int32_t *accepted_steps,
+                                     void *stream) {
+  if (!t || !state_in || !state_out || !control || !world_status)
+    return fail(CB_ERR_ARGUMENT, "null argument");
+  if (!t->packed || !t->pk.order)
+    return fail(CB_ERR_UNSUPPORTED,
+                "the handle was not bound for the packed kernel (bind with CELLS_B200_KERNEL="
+                "packed, or worlds that need it)");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
+  if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
+  const size_t need = (size_t)packed_cell_fields(t->t.nch) * (size_t)t->C +
+                      (size_t)SE_FIELDS * (size_t)std::max(t->E, 1);
+  if (need > kStaticScratchDoubles - kStaticCounterDoubles)
+    return fail(CB_ERR_UNSUPPORTED,
+                "batch needs " + std::to_string(need) + " scratch doubles; the static scratch "
+                "holds " + std::to_string(kStaticScratchDoubles - kStaticCounterDoubles) +
+                " (16 MiB): use cb_step");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  double *base = nullptr;
+  int rc = static_scratch(t->device, &base);
+  if (rc) return rc;
+  Packed P = t->pk;
+  P.queue = reinterpret_cast<unsigned int *>(base);
+  P.sc = base + kStaticCounterDoubles;
+  const double gamma = 1.0 - 1.0 / std::sqrt(2.0);
+  const double delta = 1.0 - 1.0 / (2.0 * gamma);
+  StepCoef k;
+  k.dt = dt;
+  k.gamma_dt = gamma * dt;
+  k.delta_dt = delta * dt;
+  k.omdelta_dt = (1.0 - delta) * dt;
+  k.delta = delta;
+  k.omdelta = 1.0 - delta;
+  k.frac1_dt = ((gamma + 0.0) + 0.0) * dt;
+  k.frac2_dt = ((delta + (1.0 - delta)) + 0.0) * dt;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (t->packed_block * 10 + t->t.nch) {
+    case 2560: return launch_packed_with<256, 0>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
+    case 2562: return launch_packed_with<256, 2>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
+    case 5120: return launch_packed_with<512, 0>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
+    case 5122: return launch_packed_with<512, 2>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
+    case 10240: return launch_packed_with<1024, 0>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
+    case 10242: return launch_packed_with<1024, 2>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
+    default: return fail(CB_ERR_UNSUPPORTED, "no packed kernel for this block size");
+  }
+}

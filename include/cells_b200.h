@@ -167,6 +167,23 @@ int cb_step_host(cb_tissue *t, int method, const double *state_in, double *state
  */
 int cb_balances(cb_tissue *t, const double *state, double *out, void *stream);
 
+/*
+ * cb_step for a handle bound for the packed kernel, with the kernel's scratch (stage
+ * accumulators, junction fluxes, world-sum terms, the work-queue counter) taken from a 16 MiB
+ * array that the library holds on every GPU it is loaded on, so the call allocates nothing. No
+ * counterpart in the reference: it exists for callers that may not allocate device memory
+ * while a step runs, such as a plugin inside a host runtime (an XLA/JAX custom call, a captured
+ * CUDA graph) that hands it only its input and output buffers, or a process whose device memory
+ * another allocator has already reserved. A batch needs (26 + 12 NCH) C + 9 E doubles of
+ * scratch and must fit 2^21 - 32 doubles; a larger batch is refused (CB_ERR_UNSUPPORTED) and
+ * should use cb_step. The first call on a device looks up the array's device address; make that
+ * call before any stream capture. Every call shares the array: calls whose kernels overlap on a
+ * GPU race and must be serialised by the caller. DEVICE pointers, as cb_step.
+ */
+int cb_step_packed_static(cb_tissue *t, const double *state_in, double *state_out, double dt,
+                          const double *control, int n_steps, uint32_t *world_status,
+                          int32_t *accepted_steps, void *stream);
+
 /* Message of the last error on this thread. */
 const char *cb_last_error(void);
 /* Library version string. */
