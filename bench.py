@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--fuse", type=int, default=100,
                     help="time steps per kernel launch (the largest divisor of --steps up to it)")
     ap.add_argument("--e2e-calls", type=int, default=3)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the bind's launch configuration instead of the autotuner's")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="issue the timed launches directly instead of replaying a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -281,20 +285,37 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    tuned = None
+    if not args.no_autotune:
+        from cells_b200 import autotune
+
+        best, timings = autotune.tune(tissue, state, control, args.dt,
+                                      steps=min(20, fuse), repeats=2)
+        tuned = {"selected": list(best),
+                 "ms_per_step": {f"{k[0]}/{k[1]}/{k[2]}": round(v, 5) for k, v in timings.items()}}
     left = max(args.warmup, 1)
     while left > 0:  # warm-up steps, in launches of at most `fuse` steps
         tissue.step(state, state, control, args.dt, min(fuse, left), status, stream=handle)
         left -= fuse
+    torch.cuda.synchronize(dev)
+    launches = args.steps // fuse
+    graph = None
+    if not args.no_graph:  # the timed launches as one CUDA graph
+        graph = tissue.capture(state, state, control, args.dt, fuse, status, launches=launches)
+        stream = torch.cuda.current_stream(dev)
+        handle = stream.cuda_stream
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
     clocks = Clocks(local_rank)
     clocks.start()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches = args.steps // fuse
     start.record(stream)
-    for _ in range(launches):
-        tissue.step(state, state, control, args.dt, fuse, status, stream=handle)
+    if graph is not None:
+        graph.replay()
+    else:
+        for _ in range(launches):
+            tissue.step(state, state, control, args.dt, fuse, status, stream=handle)
     stop.record(stream)
     torch.cuda.synchronize(dev)
     clock = clocks.stop()
@@ -361,6 +382,8 @@ def main():
             "config": {
                 "workload": workload_name(args),
                 "method": METHOD, "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
+                "launch": dict(zip(("kernel", "block", "occupancy"), tissue.get_launch())),
+                "autotune": tuned, "cuda_graph": graph is not None,
                 "cells_per_gpu": cells, "junctions_per_gpu": batch.edges,
                 "bytes_per_cell_step": bytes_per_cell_step(batch),
                 "parallelism": f"independent worlds x{world_size} (no collective)",
@@ -383,6 +406,7 @@ def main():
         if base is not None:
             line["cpu_baseline"] = base
         print(json.dumps(line), flush=True)
+    del graph
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

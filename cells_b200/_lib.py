@@ -34,6 +34,7 @@ STATE_FIELDS = (
 )
 CONTROL_FIELDS = ("membrane", "junction", "pump", "channel")
 METHOD_ARS222 = 0
+KERNEL_SHARED, KERNEL_PACKED = 0, 1
 WORLD_BITS = {
     1: "transport",
     2: "pump_domain",
@@ -52,6 +53,8 @@ EXPORTS = (
     "cb_step",
     "cb_step_host",
     "cb_step_packed_static",
+    "cb_set_launch",
+    "cb_get_launch",
     "cb_balances",
     "cb_last_error",
     "cb_version",
@@ -135,6 +138,11 @@ def load(path=LIBRARY):
     lib.cb_step_packed_static.argtypes = [_p, _p, _p, ctypes.c_double, _p, ctypes.c_int, _p,
                                           _p, _p]
     lib.cb_step_packed_static.restype = ctypes.c_int
+    lib.cb_set_launch.argtypes = [_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.cb_set_launch.restype = ctypes.c_int
+    _ip = ctypes.POINTER(ctypes.c_int)
+    lib.cb_get_launch.argtypes = [_p, _ip, _ip, _ip]
+    lib.cb_get_launch.restype = ctypes.c_int
     lib.cb_balances.argtypes = [_p, _p, _p, _p]
     lib.cb_balances.restype = ctypes.c_int
     lib.cb_last_error.argtypes = []

@@ -936,7 +936,8 @@ struct cb_tissue {
   std::vector<void *> owned;  // device allocations
   // The packed persistent kernel (uneven or large worlds): work items, scratch, ticket counter.
   bool packed = false;
-  int packed_block = 512;
+  bool shared_ok = false;
+  int packed_block = 1024;
   int grid_ctas = 0;
   Packed pk{};
   double *scratch = nullptr;
@@ -1058,9 +1059,56 @@ int launch_packed(cb_tissue *t, const double *in, double *out, const double *con
 
 }  // namespace
 
+namespace {
+
+int alloc_packed_scratch(cb_tissue *t) {
+  if (t->pk.sc) return CB_OK;
+  void *sc = nullptr;
+  cudaError_t e = cudaMalloc(&sc, t->scratch_bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc scratch");
+  t->owned.push_back(sc);
+  t->pk.sc = static_cast<double *>(sc);
+  return CB_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *cb_last_error(void) { return g_error.c_str(); }
+
+int cb_set_launch(cb_tissue *t, int kernel, int block, int occupancy) {
+  if (!t) return fail(CB_ERR_ARGUMENT, "null argument");
+  if (kernel == CB_KERNEL_SHARED) {
+    if (!t->shared_ok) return fail(CB_ERR_UNSUPPORTED, "the one-world-per-CTA kernel cannot hold "
+                                                       "these worlds");
+    if (occupancy != 2 && occupancy != 3) return fail(CB_ERR_ARGUMENT, "occupancy must be 2 or 3");
+    t->packed = false;
+    t->occupancy = occupancy;
+    return CB_OK;
+  }
+  if (kernel == CB_KERNEL_PACKED) {
+    if (!t->pk.order) return fail(CB_ERR_UNSUPPORTED, "worlds too large for the packed kernel");
+    if (block != 256 && block != 512 && block != 1024)
+      return fail(CB_ERR_ARGUMENT, "packed block must be 256, 512 or 1024");
+    cudaError_t ce = cudaSetDevice(t->device);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+    const int rc = alloc_packed_scratch(t);
+    if (rc) return rc;
+    t->packed = true;
+    t->packed_block = block;
+    return CB_OK;
+  }
+  return fail(CB_ERR_ARGUMENT, "kernel must be CB_KERNEL_SHARED or CB_KERNEL_PACKED");
+}
+
+int cb_get_launch(const cb_tissue *t, int *kernel, int *block, int *occupancy) {
+  if (!t || !kernel || !block || !occupancy) return fail(CB_ERR_ARGUMENT, "null argument");
+  *kernel = t->packed ? CB_KERNEL_PACKED : CB_KERNEL_SHARED;
+  *block = t->packed ? t->packed_block : t->block;
+  *occupancy = t->packed ? 1 : t->occupancy;
+  return CB_OK;
+}
 
 const char *cb_version(void) { return "cells_b200 0.1 (sm_100a, fp64 ARS(2,2,2))"; }
 
@@ -1270,7 +1318,9 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
     if (!rc) rc = upload(t, chap, &T.ch_ap);
     if (!rc) rc = upload(t, chab, &T.ch_ab);
   }
-  if (!rc && use_packed) {
+  const bool packed_ok = packed_smem_bytes(cap) <= kMaxSmemPerBlock;
+  t->shared_ok = shared_ok;
+  if (!rc && packed_ok) {
     // Work items: runs of consecutive worlds of at most `cap` cells and kPackedMaxWorlds worlds,
     // queued largest first.
     std::vector<int> item_world0{0}, cell_world(C), isnd(E), ircv(E), iadj(adj_idx.size());
@@ -1330,17 +1380,9 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
         P.queue = static_cast<unsigned int *>(q);
       }
     }
-    if (!rc) {
-      t->scratch_bytes = sizeof(double) * ((size_t)packed_cell_fields(desc_nch) * C +
-                                           (size_t)SE_FIELDS * std::max<long long>(E, 1));
-      void *sc = nullptr;
-      cudaError_t e = cudaMalloc(&sc, t->scratch_bytes);
-      if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc scratch");
-      else {
-        t->owned.push_back(sc);
-        P.sc = static_cast<double *>(sc);
-      }
-    }
+    t->scratch_bytes = sizeof(double) * ((size_t)packed_cell_fields(desc_nch) * C +
+                                         (size_t)SE_FIELDS * std::max<long long>(E, 1));
+    if (!rc && use_packed) rc = alloc_packed_scratch(t);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     t->grid_ctas = std::max(1, std::min(sms, n_items));

@@ -174,6 +174,38 @@ class Tissue:
             None if stream is None else ctypes.c_void_p(stream),
         ))  # fmt: skip
 
+    def set_launch(self, kernel, block=1024, occupancy=3):
+        """cb_set_launch: the kernel path (_lib.KERNEL_SHARED / KERNEL_PACKED) and CTA shape."""
+        _lib.check(self.lib.cb_set_launch(self.handle, int(kernel), int(block), int(occupancy)))
+
+    def get_launch(self):
+        k, b, o = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self.lib.cb_get_launch(self.handle, ctypes.byref(k), ctypes.byref(b),
+                                          ctypes.byref(o)))
+        return k.value, b.value, o.value
+
+    def capture(self, state_in, state_out, control, dt, n_steps, status, launches=1,
+                accepted=None):
+        """A CUDA graph of ``launches`` cb_step launches of ``n_steps`` steps each (device
+        tensors, as step). Replay it with graph.replay(); the tensors must stay alive. Launches
+        alternate state_in -> state_out -> state_in ... (in place when they are the same)."""
+        import torch
+
+        graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(device=state_in.device)
+        side.wait_stream(torch.cuda.current_stream(state_in.device))
+        with torch.cuda.stream(side):  # first launch outside the capture sets kernel attributes
+            self.step(state_in, state_out, control, dt, 0, status, accepted,
+                      stream=side.cuda_stream)
+        torch.cuda.current_stream(state_in.device).wait_stream(side)
+        with torch.cuda.graph(graph):
+            stream = torch.cuda.current_stream(state_in.device).cuda_stream
+            src, dst = state_in, state_out
+            for _ in range(launches):
+                self.step(src, dst, control, dt, n_steps, status, accepted, stream=stream)
+                src, dst = dst, src
+        return graph
+
     def step_host(self, state_in, control, dt, n_steps, method=_lib.METHOD_ARS222):
         """cb_step_host on packed host arrays; returns (state, status[W], accepted[W])."""
         src = np.ascontiguousarray(state_in, dtype=np.float64)

@@ -140,6 +140,16 @@ enum cb_control_field {
 int cb_bind(const cb_tissue_desc *desc, int device, cb_tissue **out);
 void cb_free(cb_tissue *t);
 
+/* Kernel paths of cb_step: one world per CTA in shared memory (uniform worlds of up to 1024
+ * cells), or the packed persistent kernel (work items of several worlds, up to 4096 cells each,
+ * taken from a device queue; scratch allocated on first selection). cb_bind picks one; an
+ * autotuner may override it. Block: CTA threads of the packed kernel (256, 512, 1024);
+ * occupancy: resident 256-thread CTAs per SM the shared kernel's registers target (2 or 3). */
+#define CB_KERNEL_SHARED 0
+#define CB_KERNEL_PACKED 1
+int cb_set_launch(cb_tissue *t, int kernel, int block, int occupancy);
+int cb_get_launch(const cb_tissue *t, int *kernel, int *block, int *occupancy);
+
 /* Offsets (in doubles) of each state field in a packed state buffer, and its total length. */
 int cb_state_layout(const cb_tissue *t, int64_t offsets[CB_STATE_FIELDS], int64_t *total);
 /* Offsets (in doubles) of each control field in a packed control buffer, and its total length. */

@@ -108,3 +108,49 @@ def test_packed_repeat_runs_are_bit_identical(cuda, packed):
     c, _, _ = run_device(cuda, tissue, tissue.initial_state(), tissue.pack_control(), 1e-3, 20)
     for f in a:
         assert np.array_equal(a[f], c[f]), f
+
+
+def test_graph_replay_equals_direct_launches(cuda):
+    """The step captured in a CUDA graph (three fused launches) replays the same bits as the same
+    launches issued directly, on both kernel paths."""
+    torch = cuda
+    from cells_b200 import _lib
+
+    b = worlds.pack(worlds.grid_tissues(6, side=16, seed=6))
+    tissue = Tissue(b)
+    dev = torch.device("cuda")
+    ctl = torch.from_numpy(tissue.pack_control()).to(dev)
+    for kernel, block, occ in ((_lib.KERNEL_SHARED, 256, 3), (_lib.KERNEL_PACKED, 512, 1)):
+        tissue.set_launch(kernel, block, occ)
+        start = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+        direct = start.clone()
+        status = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
+        for _ in range(3):
+            tissue.step(direct, direct, ctl, 1e-3, 7, status)
+        graphed = start.clone()
+        gstatus = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
+        graph = tissue.capture(graphed, graphed, ctl, 1e-3, 7, gstatus, launches=3)
+        graphed.copy_(start)
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(direct, graphed)
+        assert int(gstatus.abs().max()) == 0
+        del graph
+
+
+def test_autotune_selects_a_feasible_configuration(cuda):
+    torch = cuda
+    from cells_b200 import _lib, autotune
+
+    ws = worlds.delaunay_tissues(12, lo=32, hi=900, seed=8)
+    tissue = Tissue(worlds.pack(ws))
+    dev = torch.device("cuda")
+    state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    ctl = torch.from_numpy(tissue.pack_control()).to(dev)
+    best, timings = autotune.tune(tissue, state, ctl, 1e-3, steps=5, repeats=1)
+    assert best in timings and timings[best] == min(timings.values())
+    assert tissue.get_launch()[0] == best[0]
+    assert any(k[0] == _lib.KERNEL_PACKED for k in timings)
+    got, status, _ = run_device(cuda, tissue, tissue.initial_state(), tissue.pack_control(),
+                                1e-3, 10)
+    assert np.all(status == 0)
