@@ -38,6 +38,7 @@ sys.path.insert(0, ROOT)
 METRIC = "world·cell-steps/s"
 UNIT = "world·cell-steps/s"
 METHOD = "cells.solver.imex_ars222_face_electromigration@1"
+METHOD_MIXED = "cells_b200.solver.imex_ars222_mixed_fp32@1"
 
 
 def bytes_per_cell_step(batch):
@@ -66,6 +67,8 @@ def parse():
     ap.add_argument("--fuse", type=int, default=100,
                     help="time steps per kernel launch (the largest divisor of --steps up to it)")
     ap.add_argument("--e2e-calls", type=int, default=3)
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
+                    help="mixed: the ARS(2,2,2) step with FP32 rates and FP64 accumulation")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the bind's launch configuration instead of the autotuner's")
     ap.add_argument("--no-graph", action="store_true",
@@ -271,6 +274,10 @@ def main():
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
 
+    from cells_b200 import _lib as _lib_methods
+
+    method = (_lib_methods.METHOD_ARS222_MIXED if args.precision == "mixed"
+              else _lib_methods.METHOD_ARS222)
     batch = build_batch(args, rank)
     tissue = Tissue(batch, device=local_rank)
     cells = batch.cells
@@ -290,18 +297,20 @@ def main():
         from cells_b200 import autotune
 
         best, timings = autotune.tune(tissue, state, control, args.dt,
-                                      steps=min(20, fuse), repeats=2)
+                                      steps=min(20, fuse), repeats=2, method=method)
         tuned = {"selected": list(best),
                  "ms_per_step": {f"{k[0]}/{k[1]}/{k[2]}": round(v, 5) for k, v in timings.items()}}
     left = max(args.warmup, 1)
     while left > 0:  # warm-up steps, in launches of at most `fuse` steps
-        tissue.step(state, state, control, args.dt, min(fuse, left), status, stream=handle)
+        tissue.step(state, state, control, args.dt, min(fuse, left), status, stream=handle,
+                    method=method)
         left -= fuse
     torch.cuda.synchronize(dev)
     launches = args.steps // fuse
     graph = None
     if not args.no_graph:  # the timed launches as one CUDA graph
-        graph = tissue.capture(state, state, control, args.dt, fuse, status, launches=launches)
+        graph = tissue.capture(state, state, control, args.dt, fuse, status, launches=launches,
+                               method=method)
         stream = torch.cuda.current_stream(dev)
         handle = stream.cuda_stream
     torch.cuda.synchronize(dev)
@@ -315,7 +324,8 @@ def main():
         graph.replay()
     else:
         for _ in range(launches):
-            tissue.step(state, state, control, args.dt, fuse, status, stream=handle)
+            tissue.step(state, state, control, args.dt, fuse, status, stream=handle,
+                        method=method)
     stop.record(stream)
     torch.cuda.synchronize(dev)
     clock = clocks.stop()
@@ -347,7 +357,7 @@ def main():
 
     def host_call():
         _lib.check(tissue.lib.cb_step_host(
-            tissue.handle, _lib.METHOD_ARS222, ctypes.c_void_p(host_state.data_ptr()),
+            tissue.handle, method, ctypes.c_void_p(host_state.data_ptr()),
             ctypes.c_void_p(host_out.data_ptr()), float(args.dt),
             ctypes.c_void_p(host_ctl.data_ptr()), fuse, ctypes.c_void_p(status_h.data_ptr()),
             ctypes.c_void_p(taken_h.data_ptr())))
@@ -377,11 +387,12 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 rates / f64 accumulation",
             "data": "synthetic (seeded pump-leak tissues)",
             "config": {
                 "workload": workload_name(args),
-                "method": METHOD, "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
+                "method": METHOD if args.precision == "fp64" else METHOD_MIXED, "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
                 "launch": dict(zip(("kernel", "block", "occupancy"), tissue.get_launch())),
                 "autotune": tuned, "cuda_graph": graph is not None,
                 "cells_per_gpu": cells, "junctions_per_gpu": batch.edges,

@@ -34,6 +34,7 @@ STATE_FIELDS = (
 )
 CONTROL_FIELDS = ("membrane", "junction", "pump", "channel")
 METHOD_ARS222 = 0
+METHOD_ARS222_MIXED = 1
 KERNEL_SHARED, KERNEL_PACKED = 0, 1
 WORLD_BITS = {
     1: "transport",

@@ -30,14 +30,15 @@ def signature(tissue):
             int(sizes.min()))
 
 
-def tune(tissue, state, control, dt, steps=20, repeats=2, torch=None):
+def tune(tissue, state, control, dt, steps=20, repeats=2, torch=None,
+         method=_lib.METHOD_ARS222):
     """Time every feasible launch configuration and select the fastest. ``state`` and ``control``
     are device tensors (packed layout); ``state`` is not modified. Returns (best, timings), the
     timings in ms per step."""
     import torch as _torch
 
     torch = torch or _torch
-    key = signature(tissue)
+    key = signature(tissue) + (method,)
     if key in _CACHE:
         best = _CACHE[key][0]
         tissue.set_launch(*best)
@@ -53,11 +54,16 @@ def tune(tissue, state, control, dt, steps=20, repeats=2, torch=None):
         except RuntimeError:
             continue  # infeasible for these worlds
         work.copy_(state)
-        tissue.step(work, work, control, dt, steps, status, stream=stream.cuda_stream)
+        try:
+            tissue.step(work, work, control, dt, steps, status, stream=stream.cuda_stream,
+                        method=method)
+        except RuntimeError:
+            continue  # this method does not run on this kernel path
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
         for _ in range(repeats):
-            tissue.step(work, work, control, dt, steps, status, stream=stream.cuda_stream)
+            tissue.step(work, work, control, dt, steps, status, stream=stream.cuda_stream,
+                        method=method)
         stop.record(stream)
         torch.cuda.synchronize(dev)
         timings[cand] = start.elapsed_time(stop) / (repeats * steps)

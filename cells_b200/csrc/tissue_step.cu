@@ -120,39 +120,56 @@ struct StepCoef {
   double omdelta;
 };
 
-__device__ __forceinline__ void bernoulli_pair(double x, double &bp, double &bm) {
+template <typename R>
+__device__ __forceinline__ void bernoulli_pair(R x, R &bp, R &bm) {
   // bp = B(x) = x/expm1(x), bm = B(-x), with the reference's series for |x| < 1e-4.
-  const double ax = fabs(x);
-  if (ax < 1e-4) {
-    const double x2 = x * x;
-    const double x4 = x2 * x2;
-    bp = ((1.0 - x / 2.0) + x2 / 12.0) - x4 / 720.0;
-    bm = ((1.0 + x / 2.0) + x2 / 12.0) - x4 / 720.0;
+  const R ax = fabs(x);
+  if (ax < R(1e-4)) {
+    const R x2 = x * x;
+    const R x4 = x2 * x2;
+    bp = ((R(1) - x / R(2)) + x2 / R(12)) - x4 / R(720);
+    bm = ((R(1) + x / R(2)) + x2 / R(12)) - x4 / R(720);
   } else {
-    const double e = expm1(ax);
-    const double small = ax / e;     // B(|x|), in (0, 1)
-    const double large = ax + small; // B(-|x|) = |x| + B(|x|)
-    bp = x >= 0.0 ? small : large;
-    bm = x >= 0.0 ? large : small;
+    const R e = expm1(ax);
+    const R small = ax / e;     // B(|x|), in (0, 1)
+    const R large = ax + small; // B(-|x|) = |x| + B(|x|)
+    bp = x >= R(0) ? small : large;
+    bm = x >= R(0) ? large : small;
+  }
+}
+
+// The mixed-precision pair: the series near x = 0 in FP64 (where the GHK term is a difference of
+// nearly equal concentrations), the exponential form in FP32.
+template <bool MIX>
+__device__ __forceinline__ void bernoulli_pair_at(double x, double &bp, double &bm) {
+  if (!MIX || fabs(x) < 1e-4) {
+    bernoulli_pair<double>(x, bp, bm);
+  } else {
+    float fp, fm;
+    bernoulli_pair<float>((float)x, fp, fm);
+    bp = fp;
+    bm = fm;
   }
 }
 
 // numpy's logaddexp(0, y).
-__device__ __forceinline__ double logaddexp0(double y) {
-  if (y == 0.0) return 0.6931471805599453;  // 0 + ln 2
-  const double tmp = -y;
-  if (tmp > 0.0) return log1p(exp(-tmp));
-  if (tmp <= 0.0) return y + log1p(exp(tmp));
+template <typename R>
+__device__ __forceinline__ R logaddexp0(R y) {
+  if (y == R(0)) return R(0.6931471805599453);  // 0 + ln 2
+  const R tmp = -y;
+  if (tmp > R(0)) return log1p(exp(-tmp));
+  if (tmp <= R(0)) return y + log1p(exp(tmp));
   return tmp;  // NaN
 }
 
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
 // B(x) alone (laws/electrochemistry.py:25-32).
-__device__ __forceinline__ double bernoulli(double x) {
-  if (fabs(x) < 1e-4) {
-    const double x2 = x * x;
-    return ((1.0 - x / 2.0) + x2 / 12.0) - (x2 * x2) / 720.0;
+template <typename R>
+__device__ __forceinline__ R bernoulli(R x) {
+  if (fabs(x) < R(1e-4)) {
+    const R x2 = x * x;
+    return ((R(1) - x / R(2)) + x2 / R(12)) - (x2 * x2) / R(720);
   }
   return x / expm1(x);
 }
@@ -164,38 +181,55 @@ __device__ __forceinline__ double bernoulli(double x) {
 // Vm in mV, alpha_n = 0.1 B(-(Vm+55)/10); one gate, row 1 unused).
 constexpr int kKv1p5 = 0, kNav1p2 = 2, kHhKn4 = 100;
 
-__device__ __forceinline__ double kv_sigmoid(double value) {
-  const double e = exp(-fabs(value));
-  return value >= 0.0 ? 1.0 / (1.0 + e) : e / (1.0 + e);
+template <typename R>
+__device__ __forceinline__ R kv_sigmoid(R value) {
+  const R e = exp(-fabs(value));
+  return value >= R(0) ? R(1) / (R(1) + e) : e / (R(1) + e);
 }
 
+template <typename R>
+__device__ __forceinline__ void channel_kinetics_r(int code, R v, R (&t)[2], R (&tau)[2]) {
+  if (code == kNav1p2) {
+    const R shifted = (v + R(0.025)) / R(0.009);
+    R bp, bm;
+    bernoulli_pair<R>(shifted, bp, bm);
+    const R activation = R(0.182 * 9) * bm;
+    const R deactivation = R(0.124 * 9) * bp;
+    const R recovery = R(0.024 * 5) * bernoulli<R>(-(v + R(0.040)) / R(0.005));
+    const R inactivation = R(0.0091 * 5) * bernoulli<R>((v + R(0.065000123)) / R(0.005));
+    t[0] = activation / (activation + deactivation);
+    t[1] = R(1) / (R(1) + exp((v + R(0.055)) / R(0.0062)));
+    tau[0] = R(0.001) / (activation + deactivation);
+    tau[1] = R(0.001) / (recovery + inactivation);
+  } else if (code == kHhKn4) {
+    const R vm = R(1000) * v;
+    const R alpha = R(100) * bernoulli<R>(-(vm + R(55)) / R(10));
+    const R beta = R(125) * exp(-(vm + R(65)) / R(80));
+    t[0] = alpha / (alpha + beta);
+    t[1] = R(0);
+    tau[0] = R(1) / (alpha + beta);
+    tau[1] = R(1);
+  } else {  // Kv1.5
+    t[0] = kv_sigmoid<R>((v + R(0.0060)) / R(0.0064));
+    t[1] = kv_sigmoid<R>(-(v + R(0.0253)) / R(0.0035));
+    tau[0] = R(0.008330) - R(0.1163) * v;
+    tau[1] = R(1.620000) - R(15.500) * v;
+  }
+}
+
+// The kinetics in FP64, or in FP32 for the mixed-precision step, returned in FP64.
+template <bool MIX = false>
 __device__ __forceinline__ void channel_kinetics(int code, double v, double (&t)[2],
                                                  double (&tau)[2]) {
-  if (code == kNav1p2) {
-    const double shifted = (v + 0.025) / 0.009;
-    double bp, bm;
-    bernoulli_pair(shifted, bp, bm);
-    const double activation = (0.182 * 9) * bm;
-    const double deactivation = (0.124 * 9) * bp;
-    const double recovery = (0.024 * 5) * bernoulli(-(v + 0.040) / 0.005);
-    const double inactivation = (0.0091 * 5) * bernoulli((v + 0.065000123) / 0.005);
-    t[0] = activation / (activation + deactivation);
-    t[1] = 1.0 / (1.0 + exp((v + 0.055) / 0.0062));
-    tau[0] = 0.001 / (activation + deactivation);
-    tau[1] = 0.001 / (recovery + inactivation);
-  } else if (code == kHhKn4) {
-    const double vm = 1000.0 * v;
-    const double alpha = 100.0 * bernoulli(-(vm + 55.0) / 10.0);
-    const double beta = 125.0 * exp(-(vm + 65.0) / 80.0);
-    t[0] = alpha / (alpha + beta);
-    t[1] = 0.0;
-    tau[0] = 1.0 / (alpha + beta);
-    tau[1] = 1.0;
-  } else {  // Kv1.5
-    t[0] = kv_sigmoid((v + 0.0060) / 0.0064);
-    t[1] = kv_sigmoid(-(v + 0.0253) / 0.0035);
-    tau[0] = 0.008330 - 0.1163 * v;
-    tau[1] = 1.620000 - 15.500 * v;
+  if constexpr (MIX) {
+    float tf[2], tauf[2];
+    channel_kinetics_r<float>(code, (float)v, tf, tauf);
+    t[0] = tf[0];
+    t[1] = tf[1];
+    tau[0] = tauf[0];
+    tau[1] = tauf[1];
+  } else {
+    channel_kinetics_r<double>(code, v, t, tau);
   }
 }
 
@@ -216,13 +250,23 @@ __device__ __forceinline__ double channel_opening(int code, double m, double h) 
 }
 
 // Exponential gate update with a linearly varying target (numerics/exponential_gates.py:36-51).
+template <typename R>
+__device__ __forceinline__ R advance_gate_r(R g, R ts, R taus, R te, R taue, R h) {
+  const R z = R(0.5) * h * (R(1) / taus + R(1) / taue);
+  const R em = expm1(-z);
+  const R lag = z < R(1e-3) ? z * (R(0.5) - z * (R(1.0 / 6.0) - z * (R(1.0 / 24.0) - z / R(120))))
+                            : (em + z) / z;
+  return g + (ts - g) * (-em) + (te - ts) * lag;
+}
+
+template <bool MIX = false>
 __device__ __forceinline__ double advance_gate(double g, double ts, double taus, double te,
                                                double taue, double h) {
-  const double z = 0.5 * h * (1.0 / taus + 1.0 / taue);
-  const double em = expm1(-z);
-  const double lag = z < 1e-3 ? z * (0.5 - z * (1.0 / 6.0 - z * (1.0 / 24.0 - z / 120.0)))
-                              : (em + z) / z;
-  return g + (ts - g) * (-em) + (te - ts) * lag;
+  if constexpr (MIX)
+    return advance_gate_r<float>((float)g, (float)ts, (float)taus, (float)te, (float)taue,
+                                 (float)h);
+  else
+    return advance_gate_r<double>(g, ts, taus, te, taue, h);
 }
 
 // Block-wide sum of NV values per thread, fixed tree order: xor-shuffle within warps, then the
@@ -259,7 +303,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *red) {
 // n, g: the stage's amounts and gates; V: this thread's cell potential. sA/sE hold the cell and
 // junction accumulators in slots private to each thread. inflow: this cell's patch flux plus pump
 // transfer (the held bath's inflow terms).
-template <int BLOCK, int EPT, int NCH, bool FIRST>
+template <int BLOCK, int EPT, int NCH, bool FIRST, bool MIX>
 __device__ __forceinline__ void stage(
     const Tissue &T, const Layout &L, const double *__restrict__ wc, const StepCoef &k,
     const double *cur, int c0, int e0, int ne, int i, bool has_cell, const double (&n)[3],
@@ -289,10 +333,12 @@ __device__ __forceinline__ void stage(
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
       c[s] = (__ldg(T.ref + s * C + gi) + n[s]) * ivol;
-      lc[s] = log(c[s]);
+      if (!MIX) {
+        lc[s] = log(c[s]);
+        sL[s * BLOCK + i] = lc[s];
+      }
       if (!(finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
       sC[s * BLOCK + i] = c[s];
-      sL[s * BLOCK + i] = lc[s];
     }
     sV[i] = V;
     if (!finite(V)) bits |= CB_WORLD_TRANSPORT;
@@ -301,16 +347,27 @@ __device__ __forceinline__ void stage(
     const double x = dv * wc[WC_FRT];
     if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
     double bp, bm;
-    bernoulli_pair(x, bp, bm);
+    bernoulli_pair_at<MIX>(x, bp, bm);
     double mu[3];
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
       const double gs = __ldg(T.ap + s * C + gi) * mc;
       const double co = wc[WC_CO + s];
-      // Na, K: z = +1 -> (c_in B(-x) - c_out B(x)); Cl: z = -1 swaps the pair.
-      jm[s] = (s < 2) ? gs * (c[s] * bm - co * bp) : gs * (c[s] * bp - co * bm);
       const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
-      mu[s] = RT * (lc[s] - wc[WC_LOGCO + s]) + zfdv;
+      if constexpr (MIX) {
+        // FP32 with the concentration difference formed in FP64: c_in B(-x) - c_out B(x) =
+        // (c_in - c_out) B(x) + c_in x for z = +1, (c_in - c_out) B(x) - c_out x for z = -1.
+        const float d = (float)(c[s] - co);
+        const float fb = (float)bp, fx = (float)x;
+        const float J = (float)gs * ((s < 2) ? d * fb + (float)c[s] * fx
+                                             : d * fb - (float)co * fx);
+        jm[s] = J;
+        mu[s] = (float)RT * logf((float)c[s] / (float)co) + (float)zfdv;
+      } else {
+        // Na, K: z = +1 -> (c_in B(-x) - c_out B(x)); Cl: z = -1 swaps the pair.
+        jm[s] = (s < 2) ? gs * (c[s] * bm - co * bp) : gs * (c[s] * bp - co * bm);
+        mu[s] = RT * (lc[s] - wc[WC_LOGCO + s]) + zfdv;
+      }
       cell_acc(3 + s, L.s[CB_MEMBRANE_TRANSFERRED] + s * C, jm[s]);
     }
     const double md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
@@ -345,8 +402,16 @@ __device__ __forceinline__ void stage(
         const double cs = sp == 0 ? c[0] : sp == 1 ? c[1] : c[2];
         const double cos_ = wc[WC_CO + sp];
         const double musp = sp == 0 ? mu[0] : sp == 1 ? mu[1] : mu[2];
-        const double J = sp < 2 ? gq * (cs * bm - cos_ * bp) : gq * (cs * bp - cos_ * bm);
-        const double Jd = 1e-3 * J * musp;
+        double J, Jd;
+        if constexpr (MIX) {
+          const float d = (float)(cs - cos_), fb = (float)bp, fx = (float)x;
+          const float Jf = (float)gq * (sp < 2 ? d * fb + (float)cs * fx : d * fb - (float)cos_ * fx);
+          J = Jf;
+          Jd = (float)1e-3 * Jf * (float)musp;
+        } else {
+          J = sp < 2 ? gq * (cs * bm - cos_ * bp) : gq * (cs * bp - cos_ * bm);
+          Jd = 1e-3 * J * musp;
+        }
         chm[sp] += J;
         membrane += ((__ldg(T.ch_ap + q * C + gi) * 1e-15) * (sp == 0 ? largest[0]
                      : sp == 1 ? largest[1] : largest[2])) * available;
@@ -368,11 +433,20 @@ __device__ __forceinline__ void stage(
     const double a = energy * wc[WC_INVRT];
     double cycles = 0.0;
     if (__ldg(T.pcap + gi) > 0.0 && pc_ctl > 0.0) {
-      const double ls =
-          ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
-      const double mag = exp((log_drive_cap + ls) + fmax(a, 0.0));
-      const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
-      cycles = mag * dep;
+      if constexpr (MIX) {
+        const float af = (float)a;
+        const float ls = ((-logaddexp0<float>(3.f * ((float)wc[WC_LOGKMNA] - logf((float)c[0])))) -
+                          (float)wc[WC_LK]) - (float)wc[WC_LATP];
+        const float mag = expf(((float)log_drive_cap + ls) + fmaxf(af, 0.f));
+        const float dep = af >= 0.f ? expm1f(-af) : -expm1f(af);
+        cycles = mag * dep;
+      } else {
+        const double ls =
+            ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
+        const double mag = exp((log_drive_cap + ls) + fmax(a, 0.0));
+        const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
+        cycles = mag * dep;
+      }
     }
     const double pd = (-1e-3 * cycles) * energy;
     const double mw = (-1e-3 * cycles) * drive;
@@ -409,15 +483,22 @@ __device__ __forceinline__ void stage(
       const double x = dv * wc[WC_FRT];
       if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
       double bp, bm;
-      bernoulli_pair(x, bp, bm);
+      bernoulli_pair_at<MIX>(x, bp, bm);
       double jj[3], mu[3];
 #pragma unroll
       for (int s = 0; s < 3; ++s) {
         const double gs = __ldg(T.jap + s * E + ge) * opening;
         const double cs = sC[s * BLOCK + s_], cr = sC[s * BLOCK + r_];
-        jj[s] = (s < 2) ? gs * (cs * bm - cr * bp) : gs * (cs * bp - cr * bm);
         const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
-        mu[s] = RT * (sL[s * BLOCK + s_] - sL[s * BLOCK + r_]) + zfdv;
+        if constexpr (MIX) {
+          // FP32 on the FP64 difference c_s - c_r (as the patch); ln(c_s/c_r) = log1p(d / c_r).
+          const float d = (float)(cs - cr), fb = (float)bp, fx = (float)x;
+          jj[s] = (float)gs * ((s < 2) ? d * fb + (float)cs * fx : d * fb - (float)cr * fx);
+          mu[s] = (float)RT * log1pf(d / (float)cr) + (float)zfdv;
+        } else {
+          jj[s] = (s < 2) ? gs * (cs * bm - cr * bp) : gs * (cs * bp - cr * bm);
+          mu[s] = RT * (sL[s * BLOCK + s_] - sL[s * BLOCK + r_]) + zfdv;
+        }
         sJ[s * EB + e] = jj[s];
       }
       const double jd = 1e-3 * ((jj[0] * mu[0] + jj[1] * mu[1]) + jj[2] * mu[2]);
@@ -425,11 +506,19 @@ __device__ __forceinline__ void stage(
       const double thr = __ldg(T.thr + ge), mn = __ldg(T.jmin + ge);
       double gr = 0.0;
       if (mn < 1.0) {
-        const double shift = fabs(dv) - thr;
-        const double alpha = 1.3 * exp(-77.0 * shift);
-        const double log_beta = kLog0065 + 140.0 * shift;
-        const double beta = 20.0 * exp(-logaddexp0(-log_beta));
-        gr = alpha * (1.0 - g[q]) - beta * (g[q] - mn);
+        if constexpr (MIX) {
+          const float shift = (float)(fabs(dv) - thr);
+          const float alpha = 1.3f * expf(-77.f * shift);
+          const float log_beta = (float)kLog0065 + 140.f * shift;
+          const float beta = 20.f * expf(-logaddexp0<float>(-log_beta));
+          gr = alpha * (1.f - (float)g[q]) - beta * (float)(g[q] - mn);
+        } else {
+          const double shift = fabs(dv) - thr;
+          const double alpha = 1.3 * exp(-77.0 * shift);
+          const double log_beta = kLog0065 + 140.0 * shift;
+          const double beta = 20.0 * exp(-logaddexp0(-log_beta));
+          gr = alpha * (1.0 - g[q]) - beta * (g[q] - mn);
+        }
       }
       if (FIRST) {
 #pragma unroll
@@ -502,7 +591,7 @@ __host__ __device__ constexpr size_t step_smem_words(int block, int ept, int nch
 // global memory (the launch's input, then this CTA's own last accepted state, which stays in L2
 // across fused steps), and the accumulator y + delta dt k0 + (1 - delta) dt k1 lives in shared
 // memory, in slots private to each thread.
-template <int BLOCK, int EPT, int NCH, int MINB>
+template <int BLOCK, int EPT, int NCH, int MINB, bool MIX>
 __global__ void __launch_bounds__(BLOCK, MINB)
     ars222_kernel(const Tissue T, const Layout L, const double *state_in, double *state_out,
                   const double *__restrict__ control, const StepCoef k, int n_steps,
@@ -576,7 +665,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
 #pragma unroll
       for (int q = 0; q < NCH; ++q) {
         double t[2], tau[2];
-        channel_kinetics(__ldg(T.ch_code + q * C + gi), V - Vb, t, tau);
+        channel_kinetics<MIX>(__ldg(T.ch_code + q * C + gi), V - Vb, t, tau);
         k0_ok = k0_ok && channel_kinetics_ok(V - Vb, t, tau);
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
@@ -615,7 +704,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         chg0[r][q] = (NCH > 0 && has_cell) ? cur[L.s[CB_CHANNEL_GATE] + (r * NCH + q) * C + gi]
                                            : 0.0;
     double n1[3], g1[EPT], in0[3], in1[3];
-    stage<BLOCK, EPT, NCH, true>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n0, V0, g0, chg0, mc,
+    stage<BLOCK, EPT, NCH, true, MIX>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n0, V0, g0, chg0, mc,
                                  pctl, log_drive_cap, jctl, chctl, sV, sC, sL, sJ, sA, sE, sH, n1,
                                  g1, in0, bits);
     // Stage 1 potential: the IMEX operator (capacitor only, no faces) solve. The operator is
@@ -632,19 +721,19 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       if (NCH > 0 && has_cell) {
         const int code = __ldg(T.ch_code + q * C + gi);
         double t[2], tau[2];
-        channel_kinetics(code, V1 - Vb, t, tau);
+        channel_kinetics<MIX>(code, V1 - Vb, t, tau);
         if (!channel_kinetics_ok(V1 - Vb, t, tau)) bits |= CB_WORLD_CHANNEL_DOMAIN;
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
           if (r == 1 && code == kHhKn4) continue;
-          chg1[r][q] = advance_gate(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
+          chg1[r][q] = advance_gate<MIX>(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
                                     sK[((2 + r) * NCH + q) * BLOCK + i], t[r], tau[r], k.frac1_dt);
         }
       }
     }
     {
       double nd[3], gd[EPT];
-      stage<BLOCK, EPT, NCH, false>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n1, V1, g1, chg1,
+      stage<BLOCK, EPT, NCH, false, MIX>(T, L, sW, k, cur, c0, e0, ne, i, has_cell, n1, V1, g1, chg1,
                                     mc, pctl, log_drive_cap, jctl, chctl, sV, sC, sL, sJ, sA, sE,
                                     sH, nd, gd, in1, bits);
     }
@@ -667,7 +756,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         for (int q = 0; q < NCH; ++q) {
           const int code = __ldg(T.ch_code + q * C + gi);
           double t[2], tau[2];
-          channel_kinetics(code, V2 - Vb, t, tau);
+          channel_kinetics<MIX>(code, V2 - Vb, t, tau);
           k2_ok = k2_ok && channel_kinetics_ok(V2 - Vb, t, tau);
 #pragma unroll
           for (int r = 0; r < 2; ++r) {
@@ -675,7 +764,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
             k2tau[r][q] = tau[r];
             double g = chg0[r][q];
             if (!(r == 1 && code == kHhKn4))
-              g = advance_gate(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
+              g = advance_gate<MIX>(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
                                sK[((2 + r) * NCH + q) * BLOCK + i], t[r], tau[r], k.frac2_dt);
             sG[(r * NCH + q) * BLOCK + i] = g;
             ok = ok && finite(g) && g >= 0.0 && g <= 1.0;
@@ -973,18 +1062,23 @@ constexpr size_t kMaxSmemPerBlock = 227 * 1024;
 template <int BLOCK, int EPT>
 int launch_step(cb_tissue *t, const double *in, double *out, const double *control,
                 const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
-                cudaStream_t stream) {
+                cudaStream_t stream, bool mix) {
   const int nch = t->t.nch;
   const size_t smem = step_smem(BLOCK, EPT, nch);
   // Resident CTAs per SM that the register budget targets: 128-thread CTAs at 2 (no spills),
   // 256-thread CTAs at 2 (no spills) or 3 (a few spilled words; worlds without channels), larger
   // CTAs at 1.
   constexpr int kMin = BLOCK <= 256 ? 2 : 1;
-  auto kern = ars222_kernel<BLOCK, EPT, 0, kMin>;
+  auto kern = ars222_kernel<BLOCK, EPT, 0, kMin, false>;
   if (nch == 2) {
-    kern = ars222_kernel<BLOCK, EPT, 2, kMin>;
+    kern = mix ? ars222_kernel<BLOCK, EPT, 2, kMin, true> : ars222_kernel<BLOCK, EPT, 2, kMin, false>;
+  } else if (mix) {
+    kern = ars222_kernel<BLOCK, EPT, 0, kMin, true>;
+    if constexpr (BLOCK == 256) {
+      if (t->occupancy == 3) kern = ars222_kernel<BLOCK, EPT, 0, 3, true>;
+    }
   } else if constexpr (BLOCK == 256) {
-    if (t->occupancy == 3) kern = ars222_kernel<BLOCK, EPT, 0, 3>;
+    if (t->occupancy == 3) kern = ars222_kernel<BLOCK, EPT, 0, 3, false>;
   }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
@@ -1442,7 +1536,12 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
             void *stream) {
   if (!t || !state_in || !state_out || !control || !world_status)
     return fail(CB_ERR_ARGUMENT, "null argument");
-  if (method != CB_METHOD_ARS222) return fail(CB_ERR_UNSUPPORTED, "unknown step method");
+  if (method != CB_METHOD_ARS222 && method != CB_METHOD_ARS222_MIXED)
+    return fail(CB_ERR_UNSUPPORTED, "unknown step method");
+  const bool mix = method == CB_METHOD_ARS222_MIXED;
+  if (mix && t->packed)
+    return fail(CB_ERR_UNSUPPORTED, "the mixed-precision step runs on the one-world-per-CTA "
+                                    "kernel only");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
   if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
   cudaError_t ce = cudaSetDevice(t->device);
@@ -1466,7 +1565,7 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
     return launch_packed(t, state_in, state_out, control, k, n_steps, world_status,
                          accepted_steps, s);
   CB_DISPATCH(launch_step, state_in, state_out, control, k, n_steps, world_status,
-              accepted_steps, s);
+              accepted_steps, s, mix);
 }
 
 int cb_step_host(cb_tissue *t, int method, const double *state_in, double *state_out, double dt,

@@ -185,7 +185,7 @@ class Tissue:
         return k.value, b.value, o.value
 
     def capture(self, state_in, state_out, control, dt, n_steps, status, launches=1,
-                accepted=None):
+                accepted=None, method=_lib.METHOD_ARS222):
         """A CUDA graph of ``launches`` cb_step launches of ``n_steps`` steps each (device
         tensors, as step). Replay it with graph.replay(); the tensors must stay alive. Launches
         alternate state_in -> state_out -> state_in ... (in place when they are the same)."""
@@ -196,13 +196,14 @@ class Tissue:
         side.wait_stream(torch.cuda.current_stream(state_in.device))
         with torch.cuda.stream(side):  # first launch outside the capture sets kernel attributes
             self.step(state_in, state_out, control, dt, 0, status, accepted,
-                      stream=side.cuda_stream)
+                      stream=side.cuda_stream, method=method)
         torch.cuda.current_stream(state_in.device).wait_stream(side)
         with torch.cuda.graph(graph):
             stream = torch.cuda.current_stream(state_in.device).cuda_stream
             src, dst = state_in, state_out
             for _ in range(launches):
-                self.step(src, dst, control, dt, n_steps, status, accepted, stream=stream)
+                self.step(src, dst, control, dt, n_steps, status, accepted, stream=stream,
+                          method=method)
                 src, dst = dst, src
         return graph
 

@@ -131,6 +131,12 @@ enum cb_control_field {
 
 /* Step methods. */
 #define CB_METHOD_ARS222 0 /* cells.solver.imex_ars222_face_electromigration@1 */
+/* The same ARS(2,2,2) step with its rates in FP32 (this library's
+ * cells_b200.solver.imex_ars222_mixed_fp32@1; no reference method): transcendentals, fluxes,
+ * the pump and channel kinetics in FP32 on FP64 concentration and potential differences; the
+ * near-zero Bernoulli series, concentrations, potentials, world sums and every state and ledger
+ * accumulation in FP64. One-world-per-CTA kernel only. */
+#define CB_METHOD_ARS222_MIXED 1
 
 /*
  * Host symbolic bind (replaces initial_values' layout binding, surface_tissue.py:135-257 and
