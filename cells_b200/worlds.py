@@ -47,9 +47,11 @@ LEAK_SIGMA = 0.3
 JUNCTION_M_S = 1e-9  # 1e-7 cm/s
 JUNCTION_AREA_M2 = 1e-11  # Not given by the benchmark: declared here.
 INITIAL_mM_RANGES = np.array([[10.0, 15.0], [130.0, 145.0], [5.0, 20.0]])
-# Pump declaration of the reference's configs/resolved_pump_tissue.json, capacity scaled by area
-# (0.02 fmol/s on 4e-10 m^2).
-PUMP_CAPACITY_PER_M2 = 0.02 / 4e-10
+# Pump constants of the reference's configs/resolved_pump_tissue.json. The benchmark gives no pump
+# capacity; that file's density (0.02 fmol/s on 4e-10 m^2) is about 300 times the Na leak of the
+# benchmark's permeabilities and drives its tissues toward -150 mV. Declared here: a density
+# that balances those leaks, resting the tissues at -70 to -80 mV.
+PUMP_CAPACITY_PER_M2 = 5e5
 PUMP_KM_NA, PUMP_KM_K, PUMP_KM_ATP = 12.0, 0.2, 0.5
 PUMP_ATP, PUMP_ADP, PUMP_PI = 1.5, 0.1, 0.1
 PUMP_DG0 = -37000.0
@@ -286,7 +288,7 @@ def delaunay_tissues(worlds, lo=32, hi=4096, seed=2, channels=None):
 
 # The uneven batch's channel populations: NaV1.2 (m^3 h) and Hodgkin-Huxley K (n^4), log-normal
 # permeabilities (sigma 0.3); values declared here (the benchmark names the laws, not densities).
-UNEVEN_CHANNELS = dict(na=("nav", 3e-10, 0.5), k=("hh", 6e-10, 0.5), sigma=0.3)
+UNEVEN_CHANNELS = dict(na=("nav", 1e-9, 0.5), k=("hh", 5e-10, 0.5), sigma=0.3)
 
 
 # --------------------------------------------------------------------------------------------
