@@ -86,6 +86,9 @@ class World:
     channel_abundance: np.ndarray = field(default_factory=lambda: np.zeros((0, 0)))
     channel_gate_initial: np.ndarray = field(default_factory=lambda: np.zeros((2, 0, 0)))
     bath_mM: np.ndarray = field(default_factory=lambda: BATH_mM.copy())
+    # Cell centres in the unit square ([2, N]), for spatial patterns over the tissue (the
+    # adjoint benchmark's voltage target); empty when the builder has no geometry.
+    position: np.ndarray = field(default_factory=lambda: np.zeros((2, 0)))
     bath_volume: float = BATH_VOLUME_PL
     bath_potential: float = 0.0
     pump: tuple = (PUMP_ATP, PUMP_ADP, PUMP_PI, PUMP_KM_NA, PUMP_KM_K, PUMP_KM_ATP, PUMP_DG0)
@@ -176,10 +179,13 @@ def grid_world(nx, ny, rng, *, junction_sigma=0.0, gate=None):
     n = nx * ny
     volume, area, capacitance, permeability, amount, fixed = _cells(rng, n)
     sender, receiver = grid_edges(nx, ny)
-    return _assemble(
+    world = _assemble(
         volume, area, capacitance, permeability, amount, fixed, sender, receiver, rng,
         junction_sigma=junction_sigma, gate=gate,
     )  # fmt: skip
+    ix, iy = np.arange(n) % nx, np.arange(n) // nx
+    world.position = np.stack(((ix + 0.5) / nx, (iy + 0.5) / ny))
+    return world
 
 
 def _assemble(
@@ -242,11 +248,14 @@ def delaunay_world(n, rng, *, junction_sigma=0.3, gate=None):
     """A pump-leak tissue whose contact graph is the Delaunay triangulation of Poisson-disk
     points (mean degree about 6), junction permeabilities log-normal."""
     volume, area, capacitance, permeability, amount, fixed = _cells(rng, n)
-    sender, receiver = delaunay_edges(poisson_disk(rng, n))
-    return _assemble(
+    points = poisson_disk(rng, n)
+    sender, receiver = delaunay_edges(points)
+    world = _assemble(
         volume, area, capacitance, permeability, amount, fixed, sender, receiver, rng,
         junction_sigma=junction_sigma, gate=gate,
     )  # fmt: skip
+    world.position = points.T.copy()
+    return world
 
 
 def world_rng(seed, world):
@@ -325,6 +334,7 @@ class Batch:
     channel_permeability: np.ndarray = None  # [NCH, C] m/s (max permeability x relative)
     channel_abundance: np.ndarray = None  # [NCH, C]
     channel_gate_initial: np.ndarray = None  # [2, NCH, C]
+    position: np.ndarray = None  # [2, C] cell centres in each world's unit square (zeros: none)
 
     def __post_init__(self):
         c = self.cells
@@ -334,6 +344,8 @@ class Batch:
             self.channel_permeability = np.zeros((0, c))
             self.channel_abundance = np.zeros((0, c))
             self.channel_gate_initial = np.zeros((2, 0, c))
+        if self.position is None:
+            self.position = np.zeros((2, c))
 
     @property
     def channel_slots(self):
@@ -377,6 +389,7 @@ class Batch:
             channel_permeability=self.channel_permeability[:, c0:c1],
             channel_abundance=self.channel_abundance[:, c0:c1],
             channel_gate_initial=self.channel_gate_initial[:, :, c0:c1],
+            position=self.position[:, c0:c1],
             bath_mM=self.bath_amount[:, w] / self.bath_volume[w],
             bath_volume=float(self.bath_volume[w]),
             bath_potential=float(self.bath_potential[w]),
@@ -429,7 +442,34 @@ def pack(worlds):
                            else np.zeros((0, int(cells.sum())))),
         channel_gate_initial=(cells_of("channel_gate_initial") if nch
                               else np.zeros((2, 0, int(cells.sum())))),
+        position=cat([w.position if w.position.shape == (2, w.cells) else np.zeros((2, w.cells))
+                      for w in worlds], axis=1),
     )
+
+
+# --------------------------------------------------------------------------------------------
+# The adjoint benchmark's voltage target
+
+TARGET_BASELINE_V = -0.050
+TARGET_BUMP_V = 0.020
+TARGET_BUMPS = 3
+TARGET_WIDTH = 0.15  # Gaussian sigma in units of the tissue's side (not given: declared here)
+
+
+def voltage_target(batch, seed=4):
+    """A smooth membrane-voltage pattern per cell (V): -50 mV plus three Gaussian bumps of
+    20 mV over each world's unit square, bump centres uniform in [0.2, 0.8]^2 from a per-world
+    stream."""
+    out = np.full(batch.cells, TARGET_BASELINE_V)
+    for w in range(batch.worlds):
+        c0, c1 = batch.cell_offset[w], batch.cell_offset[w + 1]
+        rng = np.random.default_rng([int(seed), int(w), 7])
+        centres = rng.uniform(0.2, 0.8, (TARGET_BUMPS, 2))
+        xy = batch.position[:, c0:c1]
+        for cx, cy in centres:
+            r2 = (xy[0] - cx) ** 2 + (xy[1] - cy) ** 2
+            out[c0:c1] += TARGET_BUMP_V * np.exp(-r2 / (2 * TARGET_WIDTH**2))
+    return out
 
 
 # --------------------------------------------------------------------------------------------
