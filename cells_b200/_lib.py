@@ -45,6 +45,7 @@ WORLD_BITS = {
     32: "domain",
     64: "stiff",
     128: "channel_domain",
+    256: "ledger_cotangent",
 }
 EXPORTS = (
     "cb_bind",
@@ -57,6 +58,9 @@ EXPORTS = (
     "cb_set_launch",
     "cb_get_launch",
     "cb_balances",
+    "cb_step_vjp",
+    "cb_vjp_workspace",
+    "cb_set_permeability",
     "cb_last_error",
     "cb_version",
 )
@@ -146,6 +150,13 @@ def load(path=LIBRARY):
     lib.cb_get_launch.restype = ctypes.c_int
     lib.cb_balances.argtypes = [_p, _p, _p, _p]
     lib.cb_balances.restype = ctypes.c_int
+    lib.cb_step_vjp.argtypes = [_p, _p, ctypes.c_double, _p, ctypes.c_int, _p, _p, _p, _p, _p,
+                                _p, ctypes.c_size_t, _p, _p]
+    lib.cb_step_vjp.restype = ctypes.c_int
+    lib.cb_vjp_workspace.argtypes = [_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+    lib.cb_vjp_workspace.restype = ctypes.c_int
+    lib.cb_set_permeability.argtypes = [_p, _p, _p, _p, _p]
+    lib.cb_set_permeability.restype = ctypes.c_int
     lib.cb_last_error.argtypes = []
     lib.cb_last_error.restype = ctypes.c_char_p
     lib.cb_version.argtypes = []

@@ -1,25 +1,34 @@
 """Build libcellsb200.so in-tree with nvcc for sm_100a (the only target).
 
     python -m cells_b200.build [--force]
+
+Each translation unit of csrc/ compiles to an object under csrc/_build/ (in parallel); the
+objects link into cells_b200/libcellsb200.so. A unit recompiles when it, a csrc header or the
+public header is newer than its object.
 """
 
 from __future__ import annotations
 
 import argparse
+import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = [os.path.join(HERE, "csrc", "tissue_step.cu")]
-HEADERS = [os.path.join(ROOT, "include", "cells_b200.h")]
+CSRC = os.path.join(HERE, "csrc")
+SOURCES = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+OBJDIR = os.path.join(CSRC, "_build")
 OUTPUT = os.path.join(HERE, "libcellsb200.so")
-NVCC_FLAGS = [
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "-lineinfo", "-O3", "-std=c++17",
-    "-shared", "-Xcompiler", "-fPIC",
-]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMPILE_FLAGS = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
+
+
+def headers():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+                  + [os.path.join(ROOT, "include", "cells_b200.h")])
 
 
 def nvcc():
@@ -29,20 +38,47 @@ def nvcc():
     return "nvcc"
 
 
+def _object(src):
+    return os.path.join(OBJDIR, os.path.splitext(os.path.basename(src))[0] + ".o")
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    built = os.path.getmtime(target)
+    return any(os.path.getmtime(p) > built for p in deps)
+
+
 def up_to_date():
-    if not os.path.exists(OUTPUT):
-        return False
-    built = os.path.getmtime(OUTPUT)
-    return all(os.path.getmtime(p) <= built for p in SOURCES + HEADERS)
+    objs = [_object(s) for s in SOURCES]
+    return not any(_stale(o, [s, *headers()]) for s, o in zip(SOURCES, objs)) and not _stale(
+        OUTPUT, objs)
 
 
 def build(force=False, verbose=False):
-    if not force and up_to_date():
-        return OUTPUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUTPUT, *SOURCES]
+    os.makedirs(OBJDIR, exist_ok=True)
+    deps = headers()
+    jobs = []
+    for src in SOURCES:
+        obj = _object(src)
+        if force or _stale(obj, [src, *deps]):
+            jobs.append([nvcc(), *COMPILE_FLAGS, "-c", "-o", obj, src])
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        for cmd in jobs:
+            print(" ".join(cmd))
+    with ThreadPoolExecutor(max(1, len(jobs))) as pool:
+        results = list(pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), jobs))
+    for cmd, res in zip(jobs, results):
+        if res.stdout or res.stderr:
+            sys.stderr.write(res.stdout + res.stderr)
+        if res.returncode:
+            raise subprocess.CalledProcessError(res.returncode, cmd)
+    objs = [_object(s) for s in SOURCES]
+    if force or jobs or _stale(OUTPUT, objs):
+        link = [nvcc(), *ARCH, "-shared", "-o", OUTPUT, *objs]
+        if verbose:
+            print(" ".join(link))
+        subprocess.run(link, check=True)
     return OUTPUT
 
 

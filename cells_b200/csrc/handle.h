@@ -1,0 +1,61 @@
+// handle.h - the bound batch (cb_tissue) as the library's translation units share it: its
+// device views, launch choices, packed work items and owned allocations, and the error helpers
+// behind cb_last_error.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "laws.cuh"
+
+namespace cbk {
+
+constexpr int kPackedMaxWorlds = 32;  // worlds per work item of the packed kernel
+
+struct Packed {
+  int n_items;
+  int cap;                      // cells per item (shared exchange arrays)
+  const int *order;             // [n_items] queue order, largest item first
+  const int *item_world0;       // [n_items + 1] first world of each item
+  const int *cell_world;        // [C] item-local world of each cell
+  const int *isnd, *ircv;       // [E] item-local junction endpoints
+  const int *iadj;              // [2E] item-local junction codes (edge << 1 | receiver)
+  unsigned int *queue;          // ticket counter, zero at launch
+  double *sc;                   // scratch: cell fields [SC_FIELDS][C], then edge fields [SE_][E]
+};
+
+// Set the calling thread's error text (cb_last_error) and return `code`.
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+const char *last_error();
+
+}  // namespace cbk
+
+struct cb_tissue {
+  int device = 0;
+  int W = 0, C = 0, E = 0;
+  int block = 0, ept = 0;
+  int occupancy = 3;  // target resident 256-thread CTAs per SM (3, measured faster, or 2)
+  cbk::Tissue t{};
+  cbk::Layout layout{};
+  long long state_total = 0, control_total = 0;
+  std::vector<void *> owned;  // device allocations
+  // The packed persistent kernel (uneven or large worlds): work items, scratch, ticket counter.
+  bool packed = false;
+  bool shared_ok = false;
+  int packed_block = 1024;
+  int grid_ctas = 0;
+  cbk::Packed pk{};
+  double *scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // Buffers of the host-pointer entry point, allocated on first use.
+  double *h_state = nullptr, *h_control = nullptr;
+  uint32_t *h_status = nullptr;
+  int32_t *h_taken = nullptr;
+  // Patch and junction areas (m^2): the permeability prefactors and the adjoint's gradients.
+  const double *area = nullptr;   // [C]
+  const double *jarea = nullptr;  // [E]
+};

@@ -1,0 +1,294 @@
+// laws.cuh - what the tissue step's kernels share: the reference's constants, the per-world
+// constant table, the device views of a bound batch, the ARS(2,2,2) coefficients, and the point
+// laws in device code (constant-field Bernoulli pair, logaddexp, channel kinetics, exponential
+// gate update) with the fixed-order block sum.
+//
+// Arithmetic follows the reference expressions (Cells src/cells):
+//   laws/electrochemistry.py:25-48           bernoulli, ghk route flux
+//   laws/pumps/nak_atp_mass_action_positive.py:55-148  pump kinetics and domain
+//   laws/junctions/junction_voltage_relaxation.py:43-97 gate rate and domain
+//   laws/channels/kv1p5_mh.py:29-41, laws/channels/nav1p2_m3h_regularized.py:22-44
+//   numerics/exponential_gates.py:36-51      exponential stage gates
+//   numerics/surface_imex.py:47-69            the ARS(2,2,2) tableau
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <cmath>
+
+#include "../../include/cells_b200.h"
+
+namespace cbk {
+
+// Constants of laws/electrochemistry.py:11-15, formed by the same products.
+constexpr double kAvogadro = 6.02214076e23;
+constexpr double kF = kAvogadro * 1.602176634e-19;
+constexpr double kR = kAvogadro * 1.380649e-23;
+constexpr double kChargePerFmol = kF * 1e-15;
+constexpr double kMaxAbsX = 50.0;
+constexpr double kMaxAbsJunctionV = 0.120;
+constexpr double kMaxAbsIonPotentialOverRT = 1600.0;
+constexpr double kMaxAbsAffinityOverRT = 80.0;
+constexpr double kLog0065 = -2.7333680090865;  // log(0.065), the gate law's closing constant
+
+// Per-world constants (host-computed with the reference's expressions), stride in doubles.
+enum WorldConst {
+  WC_T = 0,
+  WC_RT,
+  WC_VB,
+  WC_CO,      // 3: bath concentrations
+  WC_LOGCO = WC_CO + 3,   // 3
+  WC_DRIVE = WC_LOGCO + 3,
+  WC_LK,      // logaddexp(0, 2 (log km_k - log k_o))
+  WC_LATP,    // logaddexp(0, log km_atp - log atp)
+  WC_LOGKMNA,
+  WC_AFF0,    // dG0/rt + log adp + log pi - log atp - log 1000 (pump domain affinity)
+  WC_RTDOM,   // rt of the pump domain predicate
+  WC_PUMPOK,  // 1 when temperature and pump parameters lie in the law's domain
+  WC_MUB,     // 3: bath mu (RT log co + z F Vb)
+  WC_FRT = WC_MUB + 3,  // F / RT
+  WC_INVRT,   // 1 / RT
+  WC_INVRTD,  // 1 / rt of the pump domain predicate
+  WC_SLOPE,   // F^2 / RT, the constant-field slope of the explicit-stability rate
+  WC_STRIDE
+};
+
+struct Tissue {
+  int W;
+  int C;
+  int E;
+  const int *cell_offset;  // [W+1]
+  const int *edge_offset;  // [W+1]
+  const int *adj_ptr;      // [C+1], global cell -> adjacency entries
+  const int *adj_idx;      // local edge index << 1 | (1 if the cell is the receiver)
+  const double *world;     // [W * WC_STRIDE]
+  const double *ivol;      // [C] 1 / volume
+  const double *ref;       // [3][C]
+  const double *ap;        // [3][C]  area * permeability / 1e-15 (fmol/s per mM)
+  const double *icap;      // [C] 1 / capacitance
+  const double *q0;        // [C]
+  const double *pcap;      // [C]
+  const double *logpcap;   // [C] log of the pump capacity where positive, else 0
+  const int *snd;          // [E] local
+  const int *rcv;          // [E] local
+  const double *jap;       // [3][E]  junction area * permeability / 1e-15
+  const double *thr;       // [E]
+  const double *jmin;      // [E]
+  int nch;                 // channel slots per cell (0 or 2)
+  const int *ch_code;      // [NCH][C] law code
+  const int *ch_species;   // [NCH][C] permeant species
+  const double *ch_ap;     // [NCH][C] area * permeability / 1e-15
+  const double *ch_ab;     // [NCH][C] abundance
+};
+
+struct Layout {  // offsets in doubles
+  long long s[CB_STATE_FIELDS];
+  long long c[CB_CONTROL_FIELDS];
+};
+
+struct StepCoef {
+  double dt;
+  double frac1_dt;      // the gates' stage-1 and final advance: sum of the tableau row times dt
+  double frac2_dt;
+  double gamma_dt;      // ARS(2,2,2) stage 1 weight times dt
+  double delta_dt;      // final weights times dt
+  double omdelta_dt;
+  double delta;         // for the applied reservoir flux
+  double omdelta;
+};
+
+template <typename R>
+__device__ __forceinline__ void bernoulli_pair(R x, R &bp, R &bm) {
+  // bp = B(x) = x/expm1(x), bm = B(-x), with the reference's series for |x| < 1e-4.
+  const R ax = fabs(x);
+  if (ax < R(1e-4)) {
+    const R x2 = x * x;
+    const R x4 = x2 * x2;
+    bp = ((R(1) - x / R(2)) + x2 / R(12)) - x4 / R(720);
+    bm = ((R(1) + x / R(2)) + x2 / R(12)) - x4 / R(720);
+  } else {
+    const R e = expm1(ax);
+    const R small = ax / e;     // B(|x|), in (0, 1)
+    const R large = ax + small; // B(-|x|) = |x| + B(|x|)
+    bp = x >= R(0) ? small : large;
+    bm = x >= R(0) ? large : small;
+  }
+}
+
+// The mixed-precision pair: the series near x = 0 in FP64 (where the GHK term is a difference of
+// nearly equal concentrations), the exponential form in FP32.
+template <bool MIX>
+__device__ __forceinline__ void bernoulli_pair_at(double x, double &bp, double &bm) {
+  if (!MIX || fabs(x) < 1e-4) {
+    bernoulli_pair<double>(x, bp, bm);
+  } else {
+    float fp, fm;
+    bernoulli_pair<float>((float)x, fp, fm);
+    bp = fp;
+    bm = fm;
+  }
+}
+
+// numpy's logaddexp(0, y).
+template <typename R>
+__device__ __forceinline__ R logaddexp0(R y) {
+  if (y == R(0)) return R(0.6931471805599453);  // 0 + ln 2
+  const R tmp = -y;
+  if (tmp > R(0)) return log1p(exp(-tmp));
+  if (tmp <= R(0)) return y + log1p(exp(tmp));
+  return tmp;  // NaN
+}
+
+__device__ __forceinline__ bool is_finite(double v) { return isfinite(v); }
+
+// B(x) alone (laws/electrochemistry.py:25-32).
+template <typename R>
+__device__ __forceinline__ R bernoulli(R x) {
+  if (fabs(x) < R(1e-4)) {
+    const R x2 = x * x;
+    return ((R(1) - x / R(2)) + x2 / R(12)) - (x2 * x2) / R(720);
+  }
+  return x / expm1(x);
+}
+
+// Voltage-gated channel laws: gate targets t[2] and time constants tau[2] (s) at membrane
+// voltage v (V). Codes: 0 Kv1.5 (laws/channels/kv1p5_mh.py:29-41), 2 NaV1.2
+// (laws/channels/nav1p2_m3h_regularized.py:22-44), 100 Hodgkin-Huxley K n (Hodgkin and Huxley
+// 1952: alpha_n = 0.01 (Vm+55)/(1 - exp(-(Vm+55)/10)), beta_n = 0.125 exp(-(Vm+65)/80) per ms,
+// Vm in mV, alpha_n = 0.1 B(-(Vm+55)/10); one gate, row 1 unused).
+constexpr int kKv1p5 = 0, kNav1p2 = 2, kHhKn4 = 100;
+
+template <typename R>
+__device__ __forceinline__ R kv_sigmoid(R value) {
+  const R e = exp(-fabs(value));
+  return value >= R(0) ? R(1) / (R(1) + e) : e / (R(1) + e);
+}
+
+template <typename R>
+__device__ __forceinline__ void channel_kinetics_r(int code, R v, R (&t)[2], R (&tau)[2]) {
+  if (code == kNav1p2) {
+    const R shifted = (v + R(0.025)) / R(0.009);
+    R bp, bm;
+    bernoulli_pair<R>(shifted, bp, bm);
+    const R activation = R(0.182 * 9) * bm;
+    const R deactivation = R(0.124 * 9) * bp;
+    const R recovery = R(0.024 * 5) * bernoulli<R>(-(v + R(0.040)) / R(0.005));
+    const R inactivation = R(0.0091 * 5) * bernoulli<R>((v + R(0.065000123)) / R(0.005));
+    t[0] = activation / (activation + deactivation);
+    t[1] = R(1) / (R(1) + exp((v + R(0.055)) / R(0.0062)));
+    tau[0] = R(0.001) / (activation + deactivation);
+    tau[1] = R(0.001) / (recovery + inactivation);
+  } else if (code == kHhKn4) {
+    const R vm = R(1000) * v;
+    const R alpha = R(100) * bernoulli<R>(-(vm + R(55)) / R(10));
+    const R beta = R(125) * exp(-(vm + R(65)) / R(80));
+    t[0] = alpha / (alpha + beta);
+    t[1] = R(0);
+    tau[0] = R(1) / (alpha + beta);
+    tau[1] = R(1);
+  } else {  // Kv1.5
+    t[0] = kv_sigmoid<R>((v + R(0.0060)) / R(0.0064));
+    t[1] = kv_sigmoid<R>(-(v + R(0.0253)) / R(0.0035));
+    tau[0] = R(0.008330) - R(0.1163) * v;
+    tau[1] = R(1.620000) - R(15.500) * v;
+  }
+}
+
+// The kinetics in FP64, or in FP32 for the mixed-precision step, returned in FP64.
+template <bool MIX = false>
+__device__ __forceinline__ void channel_kinetics(int code, double v, double (&t)[2],
+                                                 double (&tau)[2]) {
+  if constexpr (MIX) {
+    float tf[2], tauf[2];
+    channel_kinetics_r<float>(code, (float)v, tf, tauf);
+    t[0] = tf[0];
+    t[1] = tf[1];
+    tau[0] = tauf[0];
+    tau[1] = tauf[1];
+  } else {
+    channel_kinetics_r<double>(code, v, t, tau);
+  }
+}
+
+// channel_domain_valid (surface_pump_v3.py:848-858): the -120..60 mV domain, finite kinetics.
+__device__ __forceinline__ bool channel_kinetics_ok(double v, const double (&t)[2],
+                                                    const double (&tau)[2]) {
+  bool ok = v >= -0.120 && v <= 0.060;
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+    ok = ok && is_finite(t[r]) && t[r] >= 0.0 && t[r] <= 1.0 && is_finite(tau[r]) && tau[r] > 0.0;
+  return ok;
+}
+
+__device__ __forceinline__ double channel_opening(int code, double m, double h) {
+  if (code == kNav1p2) return ((m * m) * m) * h;
+  if (code == kHhKn4) return (m * m) * (m * m);
+  return m * h;
+}
+
+// Exponential gate update with a linearly varying target (numerics/exponential_gates.py:36-51).
+template <typename R>
+__device__ __forceinline__ R advance_gate_r(R g, R ts, R taus, R te, R taue, R h) {
+  const R z = R(0.5) * h * (R(1) / taus + R(1) / taue);
+  const R em = expm1(-z);
+  const R lag = z < R(1e-3) ? z * (R(0.5) - z * (R(1.0 / 6.0) - z * (R(1.0 / 24.0) - z / R(120))))
+                            : (em + z) / z;
+  return g + (ts - g) * (-em) + (te - ts) * lag;
+}
+
+template <bool MIX = false>
+__device__ __forceinline__ double advance_gate(double g, double ts, double taus, double te,
+                                               double taue, double h) {
+  if constexpr (MIX)
+    return advance_gate_r<float>((float)g, (float)ts, (float)taus, (float)te, (float)taue,
+                                 (float)h);
+  else
+    return advance_gate_r<double>(g, ts, taus, te, taue, h);
+}
+
+// Block-wide sum of NV values per thread, fixed tree order: xor-shuffle within warps, then the
+// warp partials in warp order. Every thread receives the totals.
+template <int BLOCK, int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *red) {
+  constexpr int WARPS = BLOCK / 32;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();  // red may still be read from a previous reduction
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) red[warp * NV + k] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = red[k];
+    for (int q = 1; q < WARPS; ++q) s += red[q * NV + k];
+    v[k] = s;
+  }
+}
+
+// The ARS(2,2,2) coefficients of one step of size dt (numerics/surface_imex.py:47-48, :63-66).
+inline StepCoef step_coef(double dt) {
+  const double gamma = 1.0 - 1.0 / std::sqrt(2.0);
+  const double delta = 1.0 - 1.0 / (2.0 * gamma);
+  StepCoef k;
+  k.dt = dt;
+  k.gamma_dt = gamma * dt;
+  k.delta_dt = delta * dt;
+  k.omdelta_dt = (1.0 - delta) * dt;
+  k.delta = delta;
+  k.omdelta = 1.0 - delta;
+  // The gates' advance fractions: each tableau row's sum, in numpy's order (gamma + 0 + 0 and
+  // (delta + (1 - delta)) + 0), times dt (surface_pump_v3.py:3700, entity_sum).
+  k.frac1_dt = ((gamma + 0.0) + 0.0) * dt;
+  k.frac2_dt = ((delta + (1.0 - delta)) + 0.0) * dt;
+  return k;
+}
+
+}  // namespace cbk

@@ -14,19 +14,6 @@
 // the rest of its item continues. Arithmetic per cell and junction is the shared-memory
 // kernel's (tissue_step.cu), in the same order.
 
-constexpr int kPackedMaxWorlds = 32;  // worlds per work item
-
-struct Packed {
-  int n_items;
-  int cap;                      // cells per item (shared exchange arrays)
-  const int *order;             // [n_items] queue order, largest item first
-  const int *item_world0;       // [n_items + 1] first world of each item
-  const int *cell_world;        // [C] item-local world of each cell
-  const int *isnd, *ircv;       // [E] item-local junction endpoints
-  const int *iadj;              // [2E] item-local junction codes (edge << 1 | receiver)
-  unsigned int *queue;          // ticket counter, zero at launch
-  double *sc;                   // scratch: cell fields [SC_FIELDS][C], then edge fields [SE_][E]
-};
 
 // Scratch fields (cells): the accumulator (n[3], mt[3], md, pc, pd, mw), the stage-1 amounts,
 // the patch flux and outward extra transfer of the current stage, the world-sum terms (stage-0
@@ -175,7 +162,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
             n[s] = first ? cur[L.s[CB_AMOUNT_INCREMENT] + s * C + gi] : SCc(SC_N1 + s, gi);
           const double q0 = __ldg(T.q0 + gi), icap = __ldg(T.icap + gi);
           const double V = (q0 + kChargePerFmol * ((n[0] + n[1]) + (-n[2]))) * icap + Vb;
-          if (!first && !finite(V)) bits |= CB_WORLD_RESIDUAL;
+          if (!first && !is_finite(V)) bits |= CB_WORLD_RESIDUAL;
           // Stage gates: the start's (stage 0), or the exponential update to the stage-1
           // potential (surface_pump_v3.stage_gates).
           double chg[2][NQ];
@@ -202,12 +189,12 @@ __global__ void __launch_bounds__(BLOCK, 1)
           for (int s = 0; s < 3; ++s) {
             c[s] = (__ldg(T.ref + s * C + gi) + n[s]) * ivol;
             lc[s] = log(c[s]);
-            if (!(finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
+            if (!(is_finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
             sC[s * CAP + cl] = c[s];
             sL[s * CAP + cl] = lc[s];
           }
           sV[cl] = V;
-          if (!finite(V)) bits |= CB_WORLD_TRANSPORT;
+          if (!is_finite(V)) bits |= CB_WORLD_TRANSPORT;
           const double mc = control[L.c[CB_CONTROL_MEMBRANE] + gi];
           const double pctl = control[L.c[CB_CONTROL_PUMP] + gi];
           const double dv = V - Vb;
@@ -224,9 +211,9 @@ __global__ void __launch_bounds__(BLOCK, 1)
             mu[s] = RT * (lc[s] - __ldg(wc + WC_LOGCO + s)) + zfdv;
           }
           const double md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
-          if (!(finite(jm[0]) && finite(jm[1]) && finite(jm[2]) && finite(md)))
+          if (!(is_finite(jm[0]) && is_finite(jm[1]) && is_finite(jm[2]) && is_finite(md)))
             bits |= CB_WORLD_TRANSPORT;
-          if (!(finite(mc) && mc >= 0.0 && mc <= 1.0 && finite(pctl) && pctl >= 0.0 &&
+          if (!(is_finite(mc) && mc >= 0.0 && mc <= 1.0 && is_finite(pctl) && pctl >= 0.0 &&
                 pctl <= 1.0))
             bits |= CB_WORLD_CONTROL;
           double largest[3];
@@ -240,7 +227,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
               const int code = __ldg(T.ch_code + q * C + gi);
               const int sp = __ldg(T.ch_species + q * C + gi);
               const double ctl = control[L.c[CB_CONTROL_CHANNEL] + q * C + gi];
-              if (!(finite(ctl) && ctl >= 0.0 && ctl <= 1.0)) bits |= CB_WORLD_CONTROL;
+              if (!(is_finite(ctl) && ctl >= 0.0 && ctl <= 1.0)) bits |= CB_WORLD_CONTROL;
               const double open = channel_opening(code, chg[0][q], chg[1][q]);
               const double available = (open * ctl) * __ldg(T.ch_ab + q * C + gi);
               const double gq = __ldg(T.ch_ap + q * C + gi) * available;
@@ -256,7 +243,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
                 CH(q, 0, gi) = CH(q, 0, gi) + w_acc * J;
                 CH(q, 1, gi) = CH(q, 1, gi) + w_acc * Jd;
               }
-              if (!(finite(J) && finite(Jd))) bits |= CB_WORLD_TRANSPORT;
+              if (!(is_finite(J) && is_finite(Jd))) bits |= CB_WORLD_TRANSPORT;
             }
           }
           if (!(k.dt * (__ldg(wc + WC_SLOPE) * membrane * icap) <= 1.0)) bits |= CB_WORLD_STIFF;
@@ -278,12 +265,12 @@ __global__ void __launch_bounds__(BLOCK, 1)
           const double mw = (-1e-3 * cycles) * drive;
           const double sna = mu[0] * __ldg(wc + WC_INVRTD), sk = mu[1] * __ldg(wc + WC_INVRTD);
           const double aff = (__ldg(wc + WC_AFF0) + (-3.0) * sna) + 2.0 * sk;
-          if (!(__ldg(wc + WC_PUMPOK) != 0.0 && finite(capacity) && capacity >= 0.0 &&
-                finite(sna) && fabs(sna) <= kMaxAbsIonPotentialOverRT && finite(sk) &&
-                fabs(sk) <= kMaxAbsIonPotentialOverRT && finite(aff) &&
+          if (!(__ldg(wc + WC_PUMPOK) != 0.0 && is_finite(capacity) && capacity >= 0.0 &&
+                is_finite(sna) && fabs(sna) <= kMaxAbsIonPotentialOverRT && is_finite(sk) &&
+                fabs(sk) <= kMaxAbsIonPotentialOverRT && is_finite(aff) &&
                 fabs(aff) <= kMaxAbsAffinityOverRT))
             bits |= CB_WORLD_PUMP_DOMAIN;
-          if (!(finite(cycles) && finite(pd) && finite(mw))) bits |= CB_WORLD_TRANSPORT;
+          if (!(is_finite(cycles) && is_finite(pd) && is_finite(mw))) bits |= CB_WORLD_TRANSPORT;
           const double ex[3] = {(3.0 * cycles - 0.0) + chm[0], (-2.0 * cycles - 0.0) + chm[1],
                                 (-0.0 * cycles - 0.0) + chm[2]};
           const double led[7] = {jm[0], jm[1], jm[2], md, cycles, pd, mw};
@@ -350,11 +337,11 @@ __global__ void __launch_bounds__(BLOCK, 1)
             SCe(SE_ACC + f, ge) = y + w_acc * led[f];
           }
           if (first) SCe(SE_G1, ge) = g + k.gamma_dt * gr;
-          if (!(finite(jj[0]) && finite(jj[1]) && finite(jj[2]) && finite(jd) && finite(gr)))
+          if (!(is_finite(jj[0]) && is_finite(jj[1]) && is_finite(jj[2]) && is_finite(jd) && is_finite(gr)))
             bits |= CB_WORLD_TRANSPORT;
-          if (!(finite(thr) && thr >= 0.0 && thr <= kMaxAbsJunctionV && finite(mn) && mn >= 0.0 &&
-                mn <= 1.0 && finite(dv) && fabs(dv) <= kMaxAbsJunctionV && finite(g) && g >= mn &&
-                g <= 1.0 && finite(jc) && jc >= 0.0 && jc <= 1.0))
+          if (!(is_finite(thr) && thr >= 0.0 && thr <= kMaxAbsJunctionV && is_finite(mn) && mn >= 0.0 &&
+                mn <= 1.0 && is_finite(dv) && fabs(dv) <= kMaxAbsJunctionV && is_finite(g) && g >= mn &&
+                g <= 1.0 && is_finite(jc) && jc >= 0.0 && jc <= 1.0))
             bits |= CB_WORLD_GATE_DOMAIN;
           if (bits) atomicOr(&sBits[wl], bits);
         }
@@ -380,7 +367,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
             const double jm = SCc(SC_JM + s, gi), ex = SCc(SC_EX + s, gi);
             const double rate = ((-jm + send[s]) + recv[s]) - ex;
             SCc(SC_RED + 3 * st + s, gi) = jm + ex;
-            if (!finite(rate)) bits |= CB_WORLD_TRANSPORT;
+            if (!is_finite(rate)) bits |= CB_WORLD_TRANSPORT;
             if (first) {
               const double n = cur[L.s[CB_AMOUNT_INCREMENT] + s * C + gi];
               SCc(SC_N1 + s, gi) = n + k.gamma_dt * rate;
@@ -392,7 +379,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
           if (!first) {
             // The new state: its potential, final channel gates and domain; the end plate charge.
             bool ok = true;
-            for (int f = 0; f < 10; ++f) ok = ok && finite(SCc(SC_ACC + f, gi));
+            for (int f = 0; f < 10; ++f) ok = ok && is_finite(SCc(SC_ACC + f, gi));
             for (int s = 0; s < 3; ++s)
               ok = ok && (__ldg(T.ref + s * C + gi) + SCc(SC_ACC + s, gi)) > 0.0;
             const double *wc = T.world + (size_t)(w0 + wl) * WC_STRIDE;
@@ -400,7 +387,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
             const double qn = kChargePerFmol *
                               ((SCc(SC_ACC, gi) + SCc(SC_ACC + 1, gi)) + (-SCc(SC_ACC + 2, gi)));
             const double V2 = (__ldg(T.q0 + gi) + qn) * __ldg(T.icap + gi) + Vb;
-            if (!finite(V2)) bits |= CB_WORLD_RESIDUAL;
+            if (!is_finite(V2)) bits |= CB_WORLD_RESIDUAL;
             SCc(SC_RED + 6, gi) = -qn;
             if constexpr (NCH > 0) {
               bool k2 = true;
@@ -419,9 +406,9 @@ __global__ void __launch_bounds__(BLOCK, 1)
                   // The end kinetics: the next step's start once this step is accepted.
                   CH(q, 4 + r, gi) = t[r];
                   CH(q, 10 + r, gi) = tau[r];
-                  ok = ok && finite(g) && g >= 0.0 && g <= 1.0;
+                  ok = ok && is_finite(g) && g >= 0.0 && g <= 1.0;
                 }
-                ok = ok && finite(CH(q, 0, gi)) && finite(CH(q, 1, gi));
+                ok = ok && is_finite(CH(q, 0, gi)) && is_finite(CH(q, 1, gi));
               }
               if (!k2) bits |= CB_WORLD_CHANNEL_DOMAIN;
             }
@@ -456,8 +443,8 @@ __global__ void __launch_bounds__(BLOCK, 1)
                                             __ldg(wc + WC_MUB + 2) * (k.dt * applied[2]));
           const double ew2 = r[5] + (1e12 * __ldg(wc + WC_VB)) * electrode;
           unsigned int bits = sBits[wl];
-          if (!(finite(res2[0]) && finite(res2[1]) && finite(res2[2]) && finite(ec2) &&
-                finite(rw2) && finite(ew2)))
+          if (!(is_finite(res2[0]) && is_finite(res2[1]) && is_finite(res2[2]) && is_finite(ec2) &&
+                is_finite(rw2) && is_finite(ew2)))
             bits |= CB_WORLD_DOMAIN;
           if (bits) {
             sRef[wl] = bits;

@@ -39,260 +39,29 @@
 #include <string>
 #include <vector>
 
-#include "../../include/cells_b200.h"
+#include "handle.h"
+
+namespace cbk {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  g_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return CB_ERR_CUDA;
+}
+
+const char *last_error() { return g_error.c_str(); }
+
+}  // namespace cbk
 
 namespace {
 
-// Constants of laws/electrochemistry.py:11-15, formed by the same products.
-constexpr double kAvogadro = 6.02214076e23;
-constexpr double kF = kAvogadro * 1.602176634e-19;
-constexpr double kR = kAvogadro * 1.380649e-23;
-constexpr double kChargePerFmol = kF * 1e-15;
-constexpr double kMaxAbsX = 50.0;
-constexpr double kMaxAbsJunctionV = 0.120;
-constexpr double kMaxAbsIonPotentialOverRT = 1600.0;
-constexpr double kMaxAbsAffinityOverRT = 80.0;
-constexpr double kLog0065 = -2.7333680090865;  // log(0.065), the gate law's closing constant
-
-// Per-world constants (host-computed with the reference's expressions), stride in doubles.
-enum WorldConst {
-  WC_T = 0,
-  WC_RT,
-  WC_VB,
-  WC_CO,      // 3: bath concentrations
-  WC_LOGCO = WC_CO + 3,   // 3
-  WC_DRIVE = WC_LOGCO + 3,
-  WC_LK,      // logaddexp(0, 2 (log km_k - log k_o))
-  WC_LATP,    // logaddexp(0, log km_atp - log atp)
-  WC_LOGKMNA,
-  WC_AFF0,    // dG0/rt + log adp + log pi - log atp - log 1000 (pump domain affinity)
-  WC_RTDOM,   // rt of the pump domain predicate
-  WC_PUMPOK,  // 1 when temperature and pump parameters lie in the law's domain
-  WC_MUB,     // 3: bath mu (RT log co + z F Vb)
-  WC_FRT = WC_MUB + 3,  // F / RT
-  WC_INVRT,   // 1 / RT
-  WC_INVRTD,  // 1 / rt of the pump domain predicate
-  WC_SLOPE,   // F^2 / RT, the constant-field slope of the explicit-stability rate
-  WC_STRIDE
-};
-
-struct Tissue {
-  int W;
-  int C;
-  int E;
-  const int *cell_offset;  // [W+1]
-  const int *edge_offset;  // [W+1]
-  const int *adj_ptr;      // [C+1], global cell -> adjacency entries
-  const int *adj_idx;      // local edge index << 1 | (1 if the cell is the receiver)
-  const double *world;     // [W * WC_STRIDE]
-  const double *ivol;      // [C] 1 / volume
-  const double *ref;       // [3][C]
-  const double *ap;        // [3][C]  area * permeability / 1e-15 (fmol/s per mM)
-  const double *icap;      // [C] 1 / capacitance
-  const double *q0;        // [C]
-  const double *pcap;      // [C]
-  const double *logpcap;   // [C] log of the pump capacity where positive, else 0
-  const int *snd;          // [E] local
-  const int *rcv;          // [E] local
-  const double *jap;       // [3][E]  junction area * permeability / 1e-15
-  const double *thr;       // [E]
-  const double *jmin;      // [E]
-  int nch;                 // channel slots per cell (0 or 2)
-  const int *ch_code;      // [NCH][C] law code
-  const int *ch_species;   // [NCH][C] permeant species
-  const double *ch_ap;     // [NCH][C] area * permeability / 1e-15
-  const double *ch_ab;     // [NCH][C] abundance
-};
-
-struct Layout {  // offsets in doubles
-  long long s[CB_STATE_FIELDS];
-  long long c[CB_CONTROL_FIELDS];
-};
-
-struct StepCoef {
-  double dt;
-  double frac1_dt;      // the gates' stage-1 and final advance: sum of the tableau row times dt
-  double frac2_dt;
-  double gamma_dt;      // ARS(2,2,2) stage 1 weight times dt
-  double delta_dt;      // final weights times dt
-  double omdelta_dt;
-  double delta;         // for the applied reservoir flux
-  double omdelta;
-};
-
-template <typename R>
-__device__ __forceinline__ void bernoulli_pair(R x, R &bp, R &bm) {
-  // bp = B(x) = x/expm1(x), bm = B(-x), with the reference's series for |x| < 1e-4.
-  const R ax = fabs(x);
-  if (ax < R(1e-4)) {
-    const R x2 = x * x;
-    const R x4 = x2 * x2;
-    bp = ((R(1) - x / R(2)) + x2 / R(12)) - x4 / R(720);
-    bm = ((R(1) + x / R(2)) + x2 / R(12)) - x4 / R(720);
-  } else {
-    const R e = expm1(ax);
-    const R small = ax / e;     // B(|x|), in (0, 1)
-    const R large = ax + small; // B(-|x|) = |x| + B(|x|)
-    bp = x >= R(0) ? small : large;
-    bm = x >= R(0) ? large : small;
-  }
-}
-
-// The mixed-precision pair: the series near x = 0 in FP64 (where the GHK term is a difference of
-// nearly equal concentrations), the exponential form in FP32.
-template <bool MIX>
-__device__ __forceinline__ void bernoulli_pair_at(double x, double &bp, double &bm) {
-  if (!MIX || fabs(x) < 1e-4) {
-    bernoulli_pair<double>(x, bp, bm);
-  } else {
-    float fp, fm;
-    bernoulli_pair<float>((float)x, fp, fm);
-    bp = fp;
-    bm = fm;
-  }
-}
-
-// numpy's logaddexp(0, y).
-template <typename R>
-__device__ __forceinline__ R logaddexp0(R y) {
-  if (y == R(0)) return R(0.6931471805599453);  // 0 + ln 2
-  const R tmp = -y;
-  if (tmp > R(0)) return log1p(exp(-tmp));
-  if (tmp <= R(0)) return y + log1p(exp(tmp));
-  return tmp;  // NaN
-}
-
-__device__ __forceinline__ bool finite(double v) { return isfinite(v); }
-
-// B(x) alone (laws/electrochemistry.py:25-32).
-template <typename R>
-__device__ __forceinline__ R bernoulli(R x) {
-  if (fabs(x) < R(1e-4)) {
-    const R x2 = x * x;
-    return ((R(1) - x / R(2)) + x2 / R(12)) - (x2 * x2) / R(720);
-  }
-  return x / expm1(x);
-}
-
-// Voltage-gated channel laws: gate targets t[2] and time constants tau[2] (s) at membrane
-// voltage v (V). Codes: 0 Kv1.5 (laws/channels/kv1p5_mh.py:29-41), 2 NaV1.2
-// (laws/channels/nav1p2_m3h_regularized.py:22-44), 100 Hodgkin-Huxley K n (Hodgkin and Huxley
-// 1952: alpha_n = 0.01 (Vm+55)/(1 - exp(-(Vm+55)/10)), beta_n = 0.125 exp(-(Vm+65)/80) per ms,
-// Vm in mV, alpha_n = 0.1 B(-(Vm+55)/10); one gate, row 1 unused).
-constexpr int kKv1p5 = 0, kNav1p2 = 2, kHhKn4 = 100;
-
-template <typename R>
-__device__ __forceinline__ R kv_sigmoid(R value) {
-  const R e = exp(-fabs(value));
-  return value >= R(0) ? R(1) / (R(1) + e) : e / (R(1) + e);
-}
-
-template <typename R>
-__device__ __forceinline__ void channel_kinetics_r(int code, R v, R (&t)[2], R (&tau)[2]) {
-  if (code == kNav1p2) {
-    const R shifted = (v + R(0.025)) / R(0.009);
-    R bp, bm;
-    bernoulli_pair<R>(shifted, bp, bm);
-    const R activation = R(0.182 * 9) * bm;
-    const R deactivation = R(0.124 * 9) * bp;
-    const R recovery = R(0.024 * 5) * bernoulli<R>(-(v + R(0.040)) / R(0.005));
-    const R inactivation = R(0.0091 * 5) * bernoulli<R>((v + R(0.065000123)) / R(0.005));
-    t[0] = activation / (activation + deactivation);
-    t[1] = R(1) / (R(1) + exp((v + R(0.055)) / R(0.0062)));
-    tau[0] = R(0.001) / (activation + deactivation);
-    tau[1] = R(0.001) / (recovery + inactivation);
-  } else if (code == kHhKn4) {
-    const R vm = R(1000) * v;
-    const R alpha = R(100) * bernoulli<R>(-(vm + R(55)) / R(10));
-    const R beta = R(125) * exp(-(vm + R(65)) / R(80));
-    t[0] = alpha / (alpha + beta);
-    t[1] = R(0);
-    tau[0] = R(1) / (alpha + beta);
-    tau[1] = R(1);
-  } else {  // Kv1.5
-    t[0] = kv_sigmoid<R>((v + R(0.0060)) / R(0.0064));
-    t[1] = kv_sigmoid<R>(-(v + R(0.0253)) / R(0.0035));
-    tau[0] = R(0.008330) - R(0.1163) * v;
-    tau[1] = R(1.620000) - R(15.500) * v;
-  }
-}
-
-// The kinetics in FP64, or in FP32 for the mixed-precision step, returned in FP64.
-template <bool MIX = false>
-__device__ __forceinline__ void channel_kinetics(int code, double v, double (&t)[2],
-                                                 double (&tau)[2]) {
-  if constexpr (MIX) {
-    float tf[2], tauf[2];
-    channel_kinetics_r<float>(code, (float)v, tf, tauf);
-    t[0] = tf[0];
-    t[1] = tf[1];
-    tau[0] = tauf[0];
-    tau[1] = tauf[1];
-  } else {
-    channel_kinetics_r<double>(code, v, t, tau);
-  }
-}
-
-// channel_domain_valid (surface_pump_v3.py:848-858): the -120..60 mV domain, finite kinetics.
-__device__ __forceinline__ bool channel_kinetics_ok(double v, const double (&t)[2],
-                                                    const double (&tau)[2]) {
-  bool ok = v >= -0.120 && v <= 0.060;
-#pragma unroll
-  for (int r = 0; r < 2; ++r)
-    ok = ok && finite(t[r]) && t[r] >= 0.0 && t[r] <= 1.0 && finite(tau[r]) && tau[r] > 0.0;
-  return ok;
-}
-
-__device__ __forceinline__ double channel_opening(int code, double m, double h) {
-  if (code == kNav1p2) return ((m * m) * m) * h;
-  if (code == kHhKn4) return (m * m) * (m * m);
-  return m * h;
-}
-
-// Exponential gate update with a linearly varying target (numerics/exponential_gates.py:36-51).
-template <typename R>
-__device__ __forceinline__ R advance_gate_r(R g, R ts, R taus, R te, R taue, R h) {
-  const R z = R(0.5) * h * (R(1) / taus + R(1) / taue);
-  const R em = expm1(-z);
-  const R lag = z < R(1e-3) ? z * (R(0.5) - z * (R(1.0 / 6.0) - z * (R(1.0 / 24.0) - z / R(120))))
-                            : (em + z) / z;
-  return g + (ts - g) * (-em) + (te - ts) * lag;
-}
-
-template <bool MIX = false>
-__device__ __forceinline__ double advance_gate(double g, double ts, double taus, double te,
-                                               double taue, double h) {
-  if constexpr (MIX)
-    return advance_gate_r<float>((float)g, (float)ts, (float)taus, (float)te, (float)taue,
-                                 (float)h);
-  else
-    return advance_gate_r<double>(g, ts, taus, te, taue, h);
-}
-
-// Block-wide sum of NV values per thread, fixed tree order: xor-shuffle within warps, then the
-// warp partials in warp order. Every thread receives the totals.
-template <int BLOCK, int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double *red) {
-  constexpr int WARPS = BLOCK / 32;
-#pragma unroll
-  for (int k = 0; k < NV; ++k) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __syncthreads();  // red may still be read from a previous reduction
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) red[warp * NV + k] = v[k];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < NV; ++k) {
-    double s = red[k];
-    for (int q = 1; q < WARPS; ++q) s += red[q * NV + k];
-    v[k] = s;
-  }
-}
+using namespace cbk;
 
 // One explicit stage (surface_pump.explicit_rates, surface_pump.py:158-240) for this thread's
 // cell and junction slots, each rate folded into the step accumulator as soon as it is formed
@@ -337,11 +106,11 @@ __device__ __forceinline__ void stage(
         lc[s] = log(c[s]);
         sL[s * BLOCK + i] = lc[s];
       }
-      if (!(finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
+      if (!(is_finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
       sC[s * BLOCK + i] = c[s];
     }
     sV[i] = V;
-    if (!finite(V)) bits |= CB_WORLD_TRANSPORT;
+    if (!is_finite(V)) bits |= CB_WORLD_TRANSPORT;
     // Patch: constant-field flux per species (selective_flux with residual 0, gate 1).
     const double dv = V - Vb;
     const double x = dv * wc[WC_FRT];
@@ -372,9 +141,9 @@ __device__ __forceinline__ void stage(
     }
     const double md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
     cell_acc(6, L.s[CB_MEMBRANE_DISSIPATED], md);
-    if (!(finite(jm[0]) && finite(jm[1]) && finite(jm[2]) && finite(md)))
+    if (!(is_finite(jm[0]) && is_finite(jm[1]) && is_finite(jm[2]) && is_finite(md)))
       bits |= CB_WORLD_TRANSPORT;
-    if (!(finite(mc) && mc >= 0.0 && mc <= 1.0 && finite(pc_ctl) && pc_ctl >= 0.0 &&
+    if (!(is_finite(mc) && mc >= 0.0 && mc <= 1.0 && is_finite(pc_ctl) && pc_ctl >= 0.0 &&
           pc_ctl <= 1.0))
       bits |= CB_WORLD_CONTROL;
     // Explicit-stability refusal (surface_pump_v3.membrane_rate, :4588-4660): dt times the
@@ -395,7 +164,7 @@ __device__ __forceinline__ void stage(
         const int code = __ldg(T.ch_code + q * C + gi);
         const int sp = __ldg(T.ch_species + q * C + gi);
         const double ctl = __ldg(chctl + q * C);
-        if (!(finite(ctl) && ctl >= 0.0 && ctl <= 1.0)) bits |= CB_WORLD_CONTROL;
+        if (!(is_finite(ctl) && ctl >= 0.0 && ctl <= 1.0)) bits |= CB_WORLD_CONTROL;
         const double open = channel_opening(code, chg[0][q], chg[1][q]);
         const double available = (open * ctl) * __ldg(T.ch_ab + q * C + gi);
         const double gq = __ldg(T.ch_ap + q * C + gi) * available;
@@ -423,7 +192,7 @@ __device__ __forceinline__ void stage(
           *tr = *tr + w * J;
           *dd = *dd + w * Jd;
         }
-        if (!(finite(J) && finite(Jd))) bits |= CB_WORLD_TRANSPORT;
+        if (!(is_finite(J) && is_finite(Jd))) bits |= CB_WORLD_TRANSPORT;
       }
     }
     if (!(k.dt * (wc[WC_SLOPE] * membrane * __ldg(T.icap + gi)) <= 1.0)) bits |= CB_WORLD_STIFF;
@@ -461,12 +230,12 @@ __device__ __forceinline__ void stage(
     const double sna = mu[0] * wc[WC_INVRTD], sk = mu[1] * wc[WC_INVRTD];
     const double aff = (wc[WC_AFF0] + (-3.0) * sna) + 2.0 * sk;
     const double capacity = __ldg(T.pcap + gi);
-    const bool pump_ok = wc[WC_PUMPOK] != 0.0 && finite(capacity) && capacity >= 0.0 &&
-                         finite(sna) && fabs(sna) <= kMaxAbsIonPotentialOverRT && finite(sk) &&
-                         fabs(sk) <= kMaxAbsIonPotentialOverRT && finite(aff) &&
+    const bool pump_ok = wc[WC_PUMPOK] != 0.0 && is_finite(capacity) && capacity >= 0.0 &&
+                         is_finite(sna) && fabs(sna) <= kMaxAbsIonPotentialOverRT && is_finite(sk) &&
+                         fabs(sk) <= kMaxAbsIonPotentialOverRT && is_finite(aff) &&
                          fabs(aff) <= kMaxAbsAffinityOverRT;
     if (!pump_ok) bits |= CB_WORLD_PUMP_DOMAIN;
-    if (!(finite(cycles) && finite(pd) && finite(mw))) bits |= CB_WORLD_TRANSPORT;
+    if (!(is_finite(cycles) && is_finite(pd) && is_finite(mw))) bits |= CB_WORLD_TRANSPORT;
   }
   __syncthreads();
   // Edge phase: each junction once, its fluxes to shared memory for the gather.
@@ -533,11 +302,11 @@ __device__ __forceinline__ void stage(
         sE[3 * EB + e] = sE[3 * EB + e] + w * jd;
         sE[4 * EB + e] = sE[4 * EB + e] + w * gr;
       }
-      if (!(finite(jj[0]) && finite(jj[1]) && finite(jj[2]) && finite(jd) && finite(gr)))
+      if (!(is_finite(jj[0]) && is_finite(jj[1]) && is_finite(jj[2]) && is_finite(jd) && is_finite(gr)))
         bits |= CB_WORLD_TRANSPORT;
-      const bool gate_ok = finite(thr) && thr >= 0.0 && thr <= kMaxAbsJunctionV && finite(mn) &&
-                           mn >= 0.0 && mn <= 1.0 && finite(dv) && fabs(dv) <= kMaxAbsJunctionV &&
-                           finite(g[q]) && g[q] >= mn && g[q] <= 1.0 && finite(jc) &&
+      const bool gate_ok = is_finite(thr) && thr >= 0.0 && thr <= kMaxAbsJunctionV && is_finite(mn) &&
+                           mn >= 0.0 && mn <= 1.0 && is_finite(dv) && fabs(dv) <= kMaxAbsJunctionV &&
+                           is_finite(g[q]) && g[q] >= mn && g[q] <= 1.0 && is_finite(jc) &&
                            jc >= 0.0 && jc <= 1.0;
       if (!gate_ok) bits |= CB_WORLD_GATE_DOMAIN;
     }
@@ -562,7 +331,7 @@ __device__ __forceinline__ void stage(
     for (int s = 0; s < 3; ++s) {
       const double rate = ((-jm[s] + send[s]) + recv[s]) - extra[s];
       inflow[s] = jm[s] + extra[s];
-      if (!finite(rate)) bits |= CB_WORLD_TRANSPORT;
+      if (!is_finite(rate)) bits |= CB_WORLD_TRANSPORT;
       if (FIRST) {
         n1[s] = n[s] + k.gamma_dt * rate;
         sA[s * BLOCK + i] = n[s] + w * rate;
@@ -711,7 +480,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     // diagonal on the cells, so Q/C leaves a charge residual within an ulp of Q and only a
     // non-finite potential exceeds 3e-25 C + 2e-12 |Q| (surface_imex.solve_operator).
     const double V1 = (q0 + kChargePerFmol * ((n1[0] + n1[1]) + (-n1[2]))) * icap + Vb;
-    if (has_cell && !finite(V1)) bits |= CB_WORLD_RESIDUAL;
+    if (has_cell && !is_finite(V1)) bits |= CB_WORLD_RESIDUAL;
     // Stage-1 channel gates: the exponential update from the step start to the stage potential
     // (surface_pump_v3.stage_gates, :3061-3070; rows without a law keep their value).
 #pragma unroll
@@ -744,12 +513,12 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     if (has_cell) {
       bool ok = true;
 #pragma unroll
-      for (int f = 0; f < 10; ++f) ok = ok && finite(sA[f * BLOCK + i]);
+      for (int f = 0; f < 10; ++f) ok = ok && is_finite(sA[f * BLOCK + i]);
 #pragma unroll
       for (int s = 0; s < 3; ++s) ok = ok && (__ldg(T.ref + s * C + gi) + sA[s * BLOCK + i]) > 0.0;
       const double q2 = q0 + kChargePerFmol * ((sA[i] + sA[BLOCK + i]) + (-sA[2 * BLOCK + i]));
       const double V2 = q2 * icap + Vb;
-      if (!finite(V2)) bits |= CB_WORLD_RESIDUAL;
+      if (!is_finite(V2)) bits |= CB_WORLD_RESIDUAL;
       // Final channel gates from the step start to the final potential; channel ledgers finite.
       if constexpr (NCH > 0) {
 #pragma unroll
@@ -767,9 +536,9 @@ __global__ void __launch_bounds__(BLOCK, MINB)
               g = advance_gate<MIX>(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
                                sK[((2 + r) * NCH + q) * BLOCK + i], t[r], tau[r], k.frac2_dt);
             sG[(r * NCH + q) * BLOCK + i] = g;
-            ok = ok && finite(g) && g >= 0.0 && g <= 1.0;
+            ok = ok && is_finite(g) && g >= 0.0 && g <= 1.0;
           }
-          ok = ok && finite(sH[q * BLOCK + i]) && finite(sH[(NCH + q) * BLOCK + i]);
+          ok = ok && is_finite(sH[q * BLOCK + i]) && is_finite(sH[(NCH + q) * BLOCK + i]);
         }
         if (!k2_ok) bits |= CB_WORLD_CHANNEL_DOMAIN;
       }
@@ -781,7 +550,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       if (e < ne) {
         bool ok = true;
 #pragma unroll
-        for (int f = 0; f < 5; ++f) ok = ok && finite(sE[f * EB + e]);
+        for (int f = 0; f < 5; ++f) ok = ok && is_finite(sE[f * EB + e]);
         const double g = sE[4 * EB + e];
         ok = ok && g >= __ldg(T.jmin + e0 + e) && g <= 1.0;
         if (!ok) bits |= CB_WORLD_DOMAIN;
@@ -805,8 +574,8 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         rw + 1e-3 * ((sW[WC_MUB] * (k.dt * applied[0]) + sW[WC_MUB + 1] * (k.dt * applied[1])) +
                      sW[WC_MUB + 2] * (k.dt * applied[2]));
     const double ew2 = ew + (1e12 * Vb) * electrode;
-    if (!(finite(res2[0]) && finite(res2[1]) && finite(res2[2]) && finite(ec2) && finite(rw2) &&
-          finite(ew2)))
+    if (!(is_finite(res2[0]) && is_finite(res2[1]) && is_finite(res2[2]) && is_finite(ec2) && is_finite(rw2) &&
+          is_finite(ew2)))
       bits |= CB_WORLD_DOMAIN;
     // The step is accepted or refused for the whole world.
     if (bits) atomicOr(&sBits, bits);
@@ -989,18 +758,6 @@ __global__ void __launch_bounds__(kBalanceBlock) balances_kernel(const Tissue T,
   }
 }
 
-thread_local std::string g_error;
-
-int fail(int code, const std::string &msg) {
-  g_error = msg;
-  return code;
-}
-
-int cuda_fail(cudaError_t e, const char *what) {
-  g_error = std::string(what) + ": " + cudaGetErrorString(e);
-  return CB_ERR_CUDA;
-}
-
 // numpy's logaddexp(0, y) on the host (libm), for the per-world pump constants.
 double host_logaddexp0(double y) {
   if (y == 0.0) return 0.6931471805599453;
@@ -1014,28 +771,6 @@ long long pad32(long long n) { return (n + 31) / 32 * 32; }
 
 }  // namespace
 
-struct cb_tissue {
-  int device = 0;
-  int W = 0, C = 0, E = 0;
-  int block = 0, ept = 0;
-  int occupancy = 3;  // target resident 256-thread CTAs per SM (3, measured faster, or 2)
-  Tissue t{};
-  Layout layout{};
-  long long state_total = 0, control_total = 0;
-  std::vector<void *> owned;  // device allocations
-  // The packed persistent kernel (uneven or large worlds): work items, scratch, ticket counter.
-  bool packed = false;
-  bool shared_ok = false;
-  int packed_block = 1024;
-  int grid_ctas = 0;
-  Packed pk{};
-  double *scratch = nullptr;
-  size_t scratch_bytes = 0;
-  // Buffers of the host-pointer entry point, allocated on first use.
-  double *h_state = nullptr, *h_control = nullptr;
-  uint32_t *h_status = nullptr;
-  int32_t *h_taken = nullptr;
-};
 
 namespace {
 
@@ -1087,6 +822,47 @@ int launch_step(cb_tissue *t, const double *in, double *out, const double *contr
                                       taken);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "ars222 launch");
+  return CB_OK;
+}
+
+// The route prefactors A P / 1e-15 (selective_flux's conductance per mM, fmol/s) from
+// permeabilities P on the device: cb_bind and cb_set_permeability both form them here, so a
+// rebound handle steps bit for bit like a handle bound with the same permeabilities. In place
+// (P read from the prefactor array itself) when pm/pj/pch alias T.ap/T.jap/T.ch_ap.
+__global__ void set_permeability_kernel(const Tissue T, const double *__restrict__ area,
+                                        const double *__restrict__ jarea, const double *pm,
+                                        const double *pj, const double *pch) {
+  const long long C = T.C, E = T.E, NQ = (long long)T.nch * C;
+  const long long n = (pm ? 3 * C : 0) + (pj ? 3 * E : 0) + (pch ? NQ : 0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    long long j = i;
+    if (pm) {
+      if (j < 3 * C) {
+        const_cast<double *>(T.ap)[j] = area[j % C] * pm[j] / 1e-15;
+        continue;
+      }
+      j -= 3 * C;
+    }
+    if (pj) {
+      if (j < 3 * E) {
+        const_cast<double *>(T.jap)[j] = jarea[j % E] * pj[j] / 1e-15;
+        continue;
+      }
+      j -= 3 * E;
+    }
+    const_cast<double *>(T.ch_ap)[j] = area[j % C] * pch[j] / 1e-15;
+  }
+}
+
+int launch_set_permeability(const cb_tissue *t, const double *pm, const double *pj,
+                            const double *pch, cudaStream_t stream) {
+  const long long n = 3LL * t->C + 3LL * t->E + (long long)t->t.nch * t->C;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+  set_permeability_kernel<<<blocks, 256, 0, stream>>>(t->t, t->area, t->jarea, pm,
+                                                      t->E ? pj : nullptr, pch);
+  cudaError_t ce = cudaGetLastError();
+  if (ce != cudaSuccess) return cuda_fail(ce, "set_permeability launch");
   return CB_OK;
 }
 
@@ -1169,7 +945,7 @@ int alloc_packed_scratch(cb_tissue *t) {
 
 extern "C" {
 
-const char *cb_last_error(void) { return g_error.c_str(); }
+const char *cb_last_error(void) { return cbk::last_error(); }
 
 int cb_set_launch(cb_tissue *t, int kernel, int block, int occupancy) {
   if (!t) return fail(CB_ERR_ARGUMENT, "null argument");
@@ -1335,14 +1111,9 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
     c[WC_INVRTD] = 1.0 / rtd;
     c[WC_SLOPE] = kF * kF / RT;
   }
-  // Route conductance prefactors A P / (1e-15 mol/fmol) (selective_flux's), and reciprocals.
-  std::vector<double> ap(3 * C), jap(3 * E), logpcap(C), ivol(C), icap(C);
-  for (int s = 0; s < 3; ++s) {
-    for (long long c = 0; c < C; ++c)
-      ap[s * C + c] = d->area[c] * d->permeability[s * C + c] / 1e-15;
-    for (long long e = 0; e < E; ++e)
-      jap[s * E + e] = d->junction_area[e] * d->junction_permeability[s * E + e] / 1e-15;
-  }
+  // Reciprocals. The route prefactors A P / 1e-15 are formed on the device once the
+  // permeabilities are uploaded (set_permeability_kernel).
+  std::vector<double> logpcap(C), ivol(C), icap(C);
   for (long long c = 0; c < C; ++c) {
     logpcap[c] = d->pump_capacity[c] > 0 ? std::log(d->pump_capacity[c]) : 0.0;
     ivol[c] = 1.0 / d->volume[c];
@@ -1386,16 +1157,19 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
   if (!rc) rc = upload(t, world, &T.world);
   if (!rc) rc = upload(t, ivol, &T.ivol);
   if (!rc) rc = upload(t, vec(d->amount_reference, 3 * C), &T.ref);
-  if (!rc) rc = upload(t, ap, &T.ap);
+  if (!rc) rc = upload(t, vec(d->permeability, 3 * C), &T.ap);
   if (!rc) rc = upload(t, icap, &T.icap);
   if (!rc) rc = upload(t, vec(d->initial_charge, C), &T.q0);
   if (!rc) rc = upload(t, vec(d->pump_capacity, C), &T.pcap);
   if (!rc) rc = upload(t, logpcap, &T.logpcap);
   if (!rc) rc = upload(t, snd, &T.snd);
   if (!rc) rc = upload(t, rcv, &T.rcv);
-  if (!rc) rc = upload(t, jap, &T.jap);
+  if (!rc) rc = upload(t, E ? vec(d->junction_permeability, 3 * E) : std::vector<double>(),
+                       &T.jap);
   if (!rc) rc = upload(t, E ? vec(d->gate_threshold, E) : std::vector<double>(), &T.thr);
   if (!rc) rc = upload(t, E ? vec(d->gate_minimum, E) : std::vector<double>(), &T.jmin);
+  if (!rc) rc = upload(t, vec(d->area, C), &t->area);
+  if (!rc) rc = upload(t, E ? vec(d->junction_area, E) : std::vector<double>(), &t->jarea);
   T.nch = desc_nch;
   {
     const long long nq = (long long)desc_nch * C;
@@ -1404,13 +1178,19 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
     for (long long q = 0; q < nq; ++q) {
       code[q] = d->channel_code[q];
       species[q] = d->channel_species[q];
-      chap[q] = d->area[q % C] * d->channel_permeability[q] / 1e-15;
+      chap[q] = d->channel_permeability[q];
       chab[q] = d->channel_abundance[q];
     }
     if (!rc) rc = upload(t, code, &T.ch_code);
     if (!rc) rc = upload(t, species, &T.ch_species);
     if (!rc) rc = upload(t, chap, &T.ch_ap);
     if (!rc) rc = upload(t, chab, &T.ch_ab);
+  }
+  // A P / 1e-15 in place over the uploaded permeabilities.
+  if (!rc) rc = launch_set_permeability(t, T.ap, T.jap, desc_nch ? T.ch_ap : nullptr, nullptr);
+  if (!rc) {
+    const cudaError_t se = cudaDeviceSynchronize();
+    if (se != cudaSuccess) rc = cuda_fail(se, "permeability prefactors");
   }
   const bool packed_ok = packed_smem_bytes(cap) <= kMaxSmemPerBlock;
   t->shared_ok = shared_ok;
@@ -1546,20 +1326,7 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
   if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
   cudaError_t ce = cudaSetDevice(t->device);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
-  // ARS(2,2,2) (numerics/surface_imex.py:47-48, :63-66).
-  const double gamma = 1.0 - 1.0 / std::sqrt(2.0);
-  const double delta = 1.0 - 1.0 / (2.0 * gamma);
-  StepCoef k;
-  k.dt = dt;
-  k.gamma_dt = gamma * dt;
-  k.delta_dt = delta * dt;
-  k.omdelta_dt = (1.0 - delta) * dt;
-  k.delta = delta;
-  k.omdelta = 1.0 - delta;
-  // The gates' advance fractions: each tableau row's sum, in numpy's order (gamma + 0 + 0 and
-  // (delta + (1 - delta)) + 0), times dt (surface_pump_v3.py:3700, entity_sum).
-  k.frac1_dt = ((gamma + 0.0) + 0.0) * dt;
-  k.frac2_dt = ((delta + (1.0 - delta)) + 0.0) * dt;
+  const StepCoef k = step_coef(dt);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (t->packed)
     return launch_packed(t, state_in, state_out, control, k, n_steps, world_status,
@@ -1597,6 +1364,17 @@ int cb_step_host(cb_tissue *t, int method, const double *state_in, double *state
     ce = cudaMemcpy(accepted_steps, t->h_taken, sizeof(int32_t) * t->W, cudaMemcpyDeviceToHost);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy to host");
   return CB_OK;
+}
+
+int cb_set_permeability(cb_tissue *t, const double *membrane, const double *junction,
+                        const double *channel, void *stream) {
+  if (!t) return fail(CB_ERR_ARGUMENT, "null argument");
+  if (channel && t->t.nch == 0) return fail(CB_ERR_ARGUMENT, "the batch has no channel slots");
+  if (!membrane && !(junction && t->E) && !channel) return CB_OK;
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  return launch_set_permeability(t, membrane, junction, channel,
+                                 static_cast<cudaStream_t>(stream));
 }
 
 int cb_balances(cb_tissue *t, const double *state, double *out, void *stream) {
@@ -1694,17 +1472,7 @@ extern "C" int cb_step_packed_static(cb_tissue *t, const double *state_in, doubl
   Packed P = t->pk;
   P.queue = reinterpret_cast<unsigned int *>(base);
   P.sc = base + kStaticCounterDoubles;
-  const double gamma = 1.0 - 1.0 / std::sqrt(2.0);
-  const double delta = 1.0 - 1.0 / (2.0 * gamma);
-  StepCoef k;
-  k.dt = dt;
-  k.gamma_dt = gamma * dt;
-  k.delta_dt = delta * dt;
-  k.omdelta_dt = (1.0 - delta) * dt;
-  k.delta = delta;
-  k.omdelta = 1.0 - delta;
-  k.frac1_dt = ((gamma + 0.0) + 0.0) * dt;
-  k.frac2_dt = ((delta + (1.0 - delta)) + 0.0) * dt;
+  const StepCoef k = step_coef(dt);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (t->packed_block * 10 + t->t.nch) {
     case 2560: return launch_packed_with<256, 0>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);

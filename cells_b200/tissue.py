@@ -11,6 +11,8 @@ This mirrors the reference's model-module protocol for the resolved pump-leak ti
 * ``checked_step(...)``        ~ ``checked_step(state, dt, control, p, active) -> (state, valid)``
   with host arrays (cb_step_host), one step.
 * ``Tissue.balances(...)``     ~ ``balances(state, p)``'s residuals (cb_balances).
+* ``Tissue.step_vjp(...)``     ~ ``jax.vjp`` of ``checked_step`` repeated ``n_steps`` times
+  (cb_step_vjp); ``Tissue.set_permeability`` rebinds the permeabilities on the device.
 
 State is a dict of NumPy arrays in the packed layout (``_lib.STATE_FIELDS``; cell fields [3, C]
 or [C], junction fields [3, E] or [E], world fields [3, W] or [W]). Device buffers are torch
@@ -225,6 +227,42 @@ class Tissue:
         _lib.check(self.lib.cb_balances(
             self.handle, ctypes.c_void_p(state_dev.data_ptr()),
             ctypes.c_void_p(out_dev.data_ptr()),
+            None if stream is None else ctypes.c_void_p(stream),
+        ))  # fmt: skip
+
+    def set_permeability(self, membrane=None, junction=None, channel=None, stream=None):
+        """cb_set_permeability from float64 device tensors (m/s): membrane [3, C], junction
+        [3, E], channel [NCH, C]; None keeps the bound values."""
+
+        def ptr(t):
+            return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+        for t in (membrane, junction, channel):
+            if t is not None and not t.is_contiguous():
+                raise ValueError("permeability tensors must be contiguous")
+        _lib.check(self.lib.cb_set_permeability(
+            self.handle, ptr(membrane), ptr(junction), ptr(channel),
+            None if stream is None else ctypes.c_void_p(stream),
+        ))  # fmt: skip
+
+    def vjp_workspace_bytes(self, n_steps):
+        out = ctypes.c_size_t()
+        _lib.check(self.lib.cb_vjp_workspace(self.handle, int(n_steps), ctypes.byref(out)))
+        return int(out.value)
+
+    def step_vjp(self, state_in, control, dt, n_steps, cot_out, cot_in, grad_membrane,
+                 grad_junction, grad_channel, workspace, status, stream=None):
+        """cb_step_vjp on device tensors: cotangent of the state after n_steps steps in, of
+        state_in out (may alias); permeability gradients added to grad_* (float64 [3C], [3E],
+        [NCH C]); workspace a uint8 tensor of vjp_workspace_bytes(n_steps); status int32 [W]."""
+
+        def ptr(t):
+            return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+        _lib.check(self.lib.cb_step_vjp(
+            self.handle, ptr(state_in), float(dt), ptr(control), int(n_steps), ptr(cot_out),
+            ptr(cot_in), ptr(grad_membrane), ptr(grad_junction), ptr(grad_channel),
+            ptr(workspace), int(workspace.numel()), ptr(status),
             None if stream is None else ctypes.c_void_p(stream),
         ))  # fmt: skip
 

@@ -51,6 +51,8 @@ typedef struct cb_tissue cb_tissue;
                                       (surface_pump_v3.membrane_rate, :4588) */
 #define CB_WORLD_CHANNEL_DOMAIN 128u /* a channel population off its law's -120..60 mV domain
                                         or with non-finite kinetics (:848-858) */
+#define CB_WORLD_LEDGER_COTANGENT 256u /* cb_step_vjp: a ledger field's cotangent was not zero;
+                                          the gradients leave out the ledgers' dependence */
 
 /* Return codes. */
 #define CB_OK 0
@@ -199,6 +201,44 @@ int cb_balances(cb_tissue *t, const double *state, double *out, void *stream);
 int cb_step_packed_static(cb_tissue *t, const double *state_in, double *state_out, double dt,
                           const double *control, int n_steps, uint32_t *world_status,
                           int32_t *accepted_steps, void *stream);
+
+/*
+ * Reverse-mode derivative of n_steps FP64 ARS(2,2,2) steps (CB_METHOD_ARS222) from state_in.
+ * The reference has no reverse-mode adjoint of its time loop: its loss gradients would be
+ * jax.grad of the composed checked_step (models/surface_pump.py:365, models/surface_pump_v3.py:
+ * 3989), which this computes for the held-bath step by the transposed linearisation of each
+ * stage in reverse order. cot_out is the cotangent of the state after the n_steps steps and
+ * cot_in receives the cotangent of state_in (both in the state layout; they may alias). Only the
+ * amount increments, junction gates and channel gates carry the dynamics: the ledgers never feed
+ * back, so their cotangents pass through unchanged and must be zero for the gradients to be
+ * complete (a world whose ledger cotangents are not zero gets CB_WORLD_LEDGER_COTANGENT). The
+ * gradients of the loss with respect to the permeabilities (m/s) are ADDED to grad_membrane
+ * [3*C], grad_junction [3*E] and grad_channel [NCH*C] (NULL when NCH = 0). A step the forward
+ * refused for a world is the identity for it (the world's state did not move) and adds nothing.
+ * The call recomputes the n_steps steps with cb_step, one step per launch, keeping every state in
+ * `workspace` (cb_vjp_workspace bytes for n_steps, 256-byte aligned, device memory the caller
+ * owns), then runs one reverse launch; callers checkpoint long trajectories by calling it once
+ * per segment, last segment first. world_status[w]: the forward's refusal bits OR-ed over the
+ * steps, plus CB_WORLD_LEDGER_COTANGENT. DEVICE pointers; stream-ordered, no host sync.
+ */
+int cb_step_vjp(cb_tissue *t, const double *state_in, double dt, const double *control,
+                int n_steps, const double *cot_out, double *cot_in, double *grad_membrane,
+                double *grad_junction, double *grad_channel, void *workspace,
+                size_t workspace_bytes, uint32_t *world_status, void *stream);
+/* Bytes of cb_step_vjp's workspace for n_steps steps. */
+int cb_vjp_workspace(const cb_tissue *t, int n_steps, size_t *bytes);
+
+/*
+ * Replace the bound permeabilities (m/s) from DEVICE arrays: membrane [3*C], junction [3*E],
+ * channel [NCH*C]; a NULL array keeps what is bound. The prefactors are formed by the same device
+ * code as cb_bind's (area * P / 1e-15), so a step after this call is bit-identical to a step of a
+ * handle bound with these permeabilities. The reference rebuilds its parameter pytree for new
+ * permeabilities (models/surface_tissue.py:135-257 parses them); this is that rebuild for the
+ * permeabilities alone, without a host round trip. Values must be finite and non-negative (the
+ * bind's checks are not repeated on the device). Stream-ordered.
+ */
+int cb_set_permeability(cb_tissue *t, const double *membrane, const double *junction,
+                        const double *channel, void *stream);
 
 /* Message of the last error on this thread. */
 const char *cb_last_error(void);
