@@ -8,8 +8,14 @@ Workloads (``--workload``):
           dt = 1 ms (cells.solver.imex_ars222_face_electromigration@1);
   uneven  1024 worlds of 32-4096 cells (log-uniform), Delaunay contact graphs, NaV1.2 (m^3 h)
           and Hodgkin-Huxley K (n^4) populations on every cell, FP64, through the packed
-          persistent kernel.
-A bench step is one time step of every world.
+          persistent kernel;
+  adjoint 512 worlds of 1024-cell Delaunay tissues with the uneven batch's laws: the gradient of
+          each world's voltage-pattern loss (squared error of the final membrane voltages against
+          -50 mV plus three 20 mV Gaussian bumps) after 2000 FP64 steps at dt = 1 ms with respect
+          to every cell's P_Na, P_K, P_Cl, every junction's permeabilities and every channel
+          population's permeability, checkpoints every 100 steps with recomputation.
+A bench step is one time step of every world (grid, uneven) or one gradient of every world's
+loss (adjoint: metric world-gradients/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -37,6 +43,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "world·cell-steps/s"
 UNIT = "world·cell-steps/s"
+ADJOINT_METRIC = "adjoint world-gradients/s"
+ADJOINT_UNIT = "world-gradients/s"
 METHOD = "cells.solver.imex_ars222_face_electromigration@1"
 METHOD_MIXED = "cells_b200.solver.imex_ars222_mixed_fp32@1"
 
@@ -56,17 +64,23 @@ def bytes_per_cell_step(batch):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed bench steps (default 1000; adjoint: 3 gradients)")
+    ap.add_argument("--warmup", type=int, default=None,
+                    help="untimed bench steps first (default 100; adjoint: 3 gradients)")
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("grid", "uneven"), default="grid")
+    ap.add_argument("--workload", choices=("grid", "uneven", "adjoint"), default="grid")
     ap.add_argument("--worlds", type=int, default=None,
-                    help="worlds per GPU (default 4096 for grid, 1024 for uneven)")
+                    help="worlds per GPU (default 4096 grid, 1024 uneven, 512 adjoint)")
+    ap.add_argument("--cells", type=int, default=1024, help="adjoint: cells per world")
+    ap.add_argument("--trajectory", type=int, default=2000, help="adjoint: steps per gradient")
+    ap.add_argument("--every", type=int, default=100, help="adjoint: checkpoint interval")
     ap.add_argument("--side", type=int, default=16)
     ap.add_argument("--dt", type=float, default=1e-3)
     ap.add_argument("--fuse", type=int, default=100,
                     help="time steps per kernel launch (the largest divisor of --steps up to it)")
-    ap.add_argument("--e2e-calls", type=int, default=3)
+    ap.add_argument("--e2e-calls", type=int, default=None,
+                    help="end-to-end host calls timed (default 3; adjoint: 1 gradient)")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
                     help="mixed: the ARS(2,2,2) step with FP32 rates and FP64 accumulation")
     ap.add_argument("--no-autotune", action="store_true",
@@ -154,6 +168,10 @@ class Clocks:
 def build_batch(args, rank):
     from cells_b200 import worlds
 
+    if args.workload == "adjoint":  # each rank its own world ids, seed 4
+        return worlds.pack([worlds.uneven_world(rank * args.worlds + w, args.cells, 4,
+                                                worlds.UNEVEN_CHANNELS)
+                            for w in range(args.worlds)])
     if args.workload == "uneven":  # each rank its own seed
         return worlds.pack(worlds.delaunay_tissues(args.worlds, seed=2 + rank,
                                                    channels=worlds.UNEVEN_CHANNELS))
@@ -168,6 +186,8 @@ def sample_tasks(args, n, steps):
     from cells_b200 import worlds
 
     stride = max(1, args.worlds // n)
+    if args.workload == "adjoint":
+        return [("adjoint", w * stride, 4, args.cells, steps, args.dt) for w in range(n)], stride
     if args.workload == "uneven":
         sizes = np.sort(worlds.uneven_sizes(args.worlds, seed=2))[::-1]
         return [("uneven", w * stride, 2, int(sizes[w * stride]), steps, args.dt)
@@ -176,6 +196,12 @@ def sample_tasks(args, n, steps):
 
 
 def workload_name(args):
+    if args.workload == "adjoint":
+        return (f"adjoint sensitivities: {args.worlds} worlds per GPU x {args.cells}-cell "
+                "Delaunay tissues, NaV1.2 m^3 h + HH K n^4 populations, gradient of each world's "
+                "voltage-pattern loss after "
+                f"{args.trajectory} FP64 steps (dt {args.dt:g} s) w.r.t. all membrane, junction "
+                f"and channel permeabilities, checkpoints every {args.every} steps")
     if args.workload == "uneven":
         return (f"uneven batch: {args.worlds} worlds per GPU of 32-4096 cells (log-uniform), "
                 "Delaunay contacts, NaV1.2 m^3 h + HH K n^4 populations, FP64, "
@@ -191,6 +217,19 @@ def cpu_baseline(args, samples_per_core=2, steps=100):
 
     cores = os.cpu_count() or 1
     n = cores * samples_per_core
+    if args.workload == "adjoint":
+        tasks, stride = sample_tasks(args, n, 20)
+        cell_steps, wall, procs = cb.measure(tasks, cores, fn=cb.run_adjoint_world)
+        rate = cell_steps / wall
+        return {
+            "value": rate / (args.cells * args.trajectory), "unit": ADJOINT_UNIT,
+            "cores": procs, "kind": "port",
+            "adjoint_cell_steps_per_s": rate,
+            "sample": (f"{n} of the {args.worlds} worlds (every {stride}th): 20 steps forward "
+                       "then the oracle adjoint back over them, one world per process, 1 BLAS "
+                       f"thread, {wall:.1f} s wall; world-gradients/s = that rate of world-"
+                       f"cell-steps / ({args.cells} cells x {args.trajectory} steps)"),
+        }
     if args.workload == "uneven":
         steps = max(2, steps // 10)
     tasks, stride = sample_tasks(args, n, steps)
@@ -214,40 +253,268 @@ def run_reference(args, rank):
 
     cores = os.cpu_count() or 1
     n = cores * 2
-    per_task = 10 if args.workload == "grid" else 1
+    adjoint = args.workload == "adjoint"
+    per_task = 10 if args.workload == "grid" else 3 if adjoint else 1
+    fn = cb.run_adjoint_world if adjoint else cb.run_world
     tasks, stride = sample_tasks(args, n, per_task)
     with cb.pool(cores) as pool:
         pool.map(cb.prepare, tasks, chunksize=1)
         for _ in range(max(args.warmup, 0)):
-            pool.map(cb.run_world, tasks, chunksize=1)
+            pool.map(fn, tasks, chunksize=1)
         t0 = time.perf_counter()
         done = 0
         for _ in range(args.steps):
-            res = pool.map(cb.run_world, tasks, chunksize=1)
+            res = pool.map(fn, tasks, chunksize=1)
             done += sum(r[0] for r in res)
         wall = time.perf_counter() - t0
     value = done / wall
-    sample = (f"{n} of the {args.worlds} worlds (every {stride}th) advanced {per_task} "
-              "ARS(2,2,2) steps per bench step, one world per process, 1 BLAS thread")
+    metric, unit = METRIC, UNIT
+    if adjoint:  # world-cell-steps of forward + adjoint per second -> world-gradients/s
+        value = value / (args.cells * args.trajectory)
+        metric, unit = ADJOINT_METRIC, ADJOINT_UNIT
+        sample = (f"{n} of the {args.worlds} worlds (every {stride}th), {per_task} steps "
+                  "forward then the oracle adjoint back over them per bench step, one world per "
+                  "process, 1 BLAS thread (the reference has no adjoint; its gradients would "
+                  "come from jax.grad, and jax is not installed)")
+    else:
+        sample = (f"{n} of the {args.worlds} worlds (every {stride}th) advanced {per_task} "
+                  "ARS(2,2,2) steps per bench step, one world per process, 1 BLAS thread")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded pump-leak tissues)", "impl": "reference",
         "config": {"workload": workload_name(args) + " (sampled)", "method": METHOD,
                    "sample": sample},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
                          "sample": sample},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def vjp_bytes_per_cell_step(batch):
+    """Algorithmic bytes per world-cell-step of the reverse (cb_step_vjp's reverse kernel): per
+    cell the step-start dynamic state (3 amounts, 2 NCH gates) and the end amounts read, the
+    parameters read (1/V, 1/C, Q0, 3 references, 3 prefactors, pump capacity and its log, area:
+    12 doubles; per channel population its prefactor, abundance, law and species: 24 B), the
+    controls read (2 + NCH), the dynamic cotangent read and written, the permeability gradients
+    read and written (3 + NCH), and its adjacency offset; per junction its gate, 3 prefactors,
+    area, threshold, minimum and control read, its endpoints and two adjacency entries, its gate
+    cotangent read and written and 3 gradients read and written."""
+    n = batch.channel_slots
+    per_cell = 8 * ((6 + 2 * n) + 12 + (2 + n) + 2 * (3 + 2 * n) + 2 * (3 + n)) + 8 * n + 4
+    per_edge = 8 * 8 + 8 + 8 + 8 * 2 + 8 * 6
+    return per_cell + per_edge * batch.edges / batch.cells
+
+
+def run_adjoint(args, rank, world_size, local_rank, dist, base):
+    """The adjoint workload: each bench step is the gradient of every world's voltage-pattern
+    loss through cells_b200.adjoint (forward in checkpointed segments, cb_step_vjp back)."""
+    import torch
+
+    from cells_b200 import adjoint, worlds
+    from cells_b200.tissue import Tissue
+
+    dev = torch.device("cuda", local_rank)
+    batch = build_batch(args, rank)
+    tissue = Tissue(batch, device=local_rank)
+    cells, w_count = batch.cells, batch.worlds
+    state0 = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    control = torch.from_numpy(tissue.pack_control()).to(dev)
+    target = torch.tensor(worlds.voltage_target(batch), device=dev)
+    params = [t.requires_grad_() for t in adjoint.permeabilities(tissue)]
+    refused = torch.zeros(w_count, dtype=torch.int32, device=dev)
+
+    def gradient(state, perms):
+        final, bits = adjoint.trajectory(tissue, state, control, args.dt, args.trajectory, *perms,
+                                         every=args.every)
+        loss = adjoint.voltage_loss(tissue, final, target)
+        loss.sum().backward()
+        return loss, bits
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        gradient(state0, params)
+        for p in params:
+            p.grad = None
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    clocks = Clocks(local_rank)
+    clocks.start()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        loss, bits = gradient(state0, params)
+        refused |= bits
+        for p in params:
+            p.grad = None
+    stop.record(stream)
+    torch.cuda.synchronize(dev)
+    clock = clocks.stop()
+    ms = start.elapsed_time(stop)
+    n_refused = int((refused != 0).sum().item())
+    barrier()
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = w_count * world_size * args.steps / (ms_max * 1e-3)
+
+    # Kernel durations on the same inputs (CUDA events, this stream): a fused forward segment,
+    # a segment of one-step launches (the recompute), and cb_step_vjp over a segment; the
+    # reverse kernel's time is the last less the recompute.
+    k = min(args.every, args.trajectory)
+    status = torch.zeros(w_count, dtype=torch.int32, device=dev)
+    out = torch.empty_like(state0)
+    ws = torch.empty(tissue.vjp_workspace_bytes(k), dtype=torch.uint8, device=dev)
+    cot = torch.zeros_like(state0)
+    o = tissue.state_offsets["amount_increment"]
+    cot[o:o + 3 * cells] = 1e-3
+    gm = torch.zeros(3 * cells, dtype=torch.float64, device=dev)
+    gj = torch.zeros(max(3 * batch.edges, 1), dtype=torch.float64, device=dev)
+    gch = torch.zeros(max(batch.channel_slots * cells, 1), dtype=torch.float64, device=dev)
+    nch = batch.channel_slots
+
+    def timed(fn, reps=3):
+        fn()
+        times = []
+        for _ in range(reps):
+            a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b_.record(stream)
+            torch.cuda.synchronize(dev)
+            times.append(a.elapsed_time(b_))
+        return statistics.median(times)
+
+    def one_step_segment():
+        src = state0
+        for _ in range(k):
+            tissue.step(src, out, control, args.dt, 1, status)
+            src = out
+
+    fused_ms = timed(lambda: tissue.step(state0, out, control, args.dt, k, status))
+    onestep_ms = timed(one_step_segment)
+    vjp_ms = timed(lambda: tissue.step_vjp(state0, control, args.dt, k, cot, out, gm, gj,
+                                           gch if nch else None, ws, status))
+    reverse_ms = max(vjp_ms - onestep_ms, 1e-6)
+    segments = -(-args.trajectory // args.every)
+    per_gradient = {"packed_kernel (forward, fused)": fused_ms * segments,
+                    "packed_kernel (recompute, one step per launch)": onestep_ms * segments,
+                    "vjp_kernel (reverse)": reverse_ms * segments}
+    total = sum(per_gradient.values())
+    fwd_bytes = bytes_per_cell_step(batch) * cells
+    rev_bytes = vjp_bytes_per_cell_step(batch) * cells
+    peak, peak_kind = peaks()
+    kernels = {
+        "packed_kernel": {"ms_per_gradient": (fused_ms + onestep_ms) * segments,
+                          "share": (fused_ms + onestep_ms) * segments / total,
+                          "achieved_gbs_fused": fwd_bytes * k / (fused_ms * 1e-3) / 1e9,
+                          "achieved_gbs_one_step": fwd_bytes * k / (onestep_ms * 1e-3) / 1e9,
+                          "bytes_per_cell_step": bytes_per_cell_step(batch)},
+        "vjp_kernel": {"ms_per_gradient": reverse_ms * segments,
+                       "share": reverse_ms * segments / total,
+                       "achieved_gbs": rev_bytes * k / (reverse_ms * 1e-3) / 1e9,
+                       "bytes_per_cell_step": vjp_bytes_per_cell_step(batch)},
+    }
+    dominant = max(kernels, key=lambda name: kernels[name]["share"])
+    if dominant == "vjp_kernel":
+        launch_ms, alg = reverse_ms, rev_bytes * k
+    else:
+        launch_ms, alg = fused_ms, fwd_bytes * k
+    achieved = alg / (launch_ms * 1e-3) / 1e9
+
+    # End to end through the public API with host buffers: each call copies the start state and
+    # the permeabilities from pinned host memory, takes the gradient, and copies the gradients
+    # and the losses back.
+    host_state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).pin_memory()
+    host_perm = [p.detach().cpu().pin_memory() for p in params]
+    host_grad = [torch.empty_like(h).pin_memory() for h in host_perm]
+    host_loss = torch.empty(w_count, dtype=torch.float64).pin_memory()
+
+    def host_call():
+        st = host_state.to(dev, non_blocking=True)
+        perms = [h.to(dev, non_blocking=True).requires_grad_() for h in host_perm]
+        loss, _ = gradient(st, perms)
+        for h, p in zip(host_grad, perms, strict=True):
+            h.copy_(p.grad, non_blocking=True)
+        host_loss.copy_(loss.detach(), non_blocking=True)
+        torch.cuda.synchronize(dev)
+
+    e2e_value = None
+    if args.e2e_calls > 0:
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_calls):
+            host_call()
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e_value = w_count * world_size * args.e2e_calls / e2e_s
+    perm_bytes = sum(h.numel() for h in host_perm) * 8
+    launches_per_gradient = 2 + segments + segments * (k + 1)
+    if rank == 0:
+        line = {
+            "metric": ADJOINT_METRIC, "value": value, "unit": ADJOINT_UNIT, "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded pump-leak tissues)",
+            "config": {
+                "workload": workload_name(args), "method": METHOD,
+                "worlds_per_gpu": args.worlds, "cells_per_world": args.cells,
+                "cells_per_gpu": cells, "junctions_per_gpu": batch.edges,
+                "trajectory_steps": args.trajectory, "checkpoint_every": args.every,
+                "parameters_per_gpu": perm_bytes // 8,
+                "launch": dict(zip(("kernel", "block", "occupancy"), tissue.get_launch())),
+                "adjoint_world_cell_steps_per_s": value * cells / w_count * args.trajectory,
+                "parallelism": f"independent worlds x{world_size} (no collective)",
+                "l2": (f"inputs larger than L2: state {tissue.state_size * 8 / 1e6:.0f} MB per "
+                       "GPU, checkpoints and the segment workspace several GB"),
+            },
+            "roofline": {
+                "bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms,
+            },
+            "kernels": kernels,
+            "e2e": {"value": e2e_value, "unit": ADJOINT_UNIT,
+                    "h2d_bytes_per_step": tissue.state_size * 8 + perm_bytes,
+                    "d2h_bytes_per_step": perm_bytes + w_count * 8, "calls": args.e2e_calls},
+            "gpu_launches": launches_per_gradient * args.steps,
+            "refused_worlds": n_refused,
+            "clocks": clock,
+        }
+        if base is not None:
+            line["cpu_baseline"] = base
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    tissue.close()
+    return 0
+
+
 def main():
     args = parse()
+    adjoint = args.workload == "adjoint"
     if args.worlds is None:
-        args.worlds = 1024 if args.workload == "uneven" else 4096
+        args.worlds = {"uneven": 1024, "adjoint": 512}.get(args.workload, 4096)
+    if args.steps is None:
+        args.steps = 3 if adjoint else 1000
+    if args.warmup is None:
+        args.warmup = 3 if adjoint else 100
+    if args.e2e_calls is None:
+        args.e2e_calls = 1 if adjoint else 3
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -273,6 +540,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
+    if adjoint:
+        return run_adjoint(args, rank, world_size, local_rank, dist, base)
 
     from cells_b200 import _lib as _lib_methods
 

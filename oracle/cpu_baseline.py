@@ -16,6 +16,8 @@ from __future__ import annotations
 import os
 import time
 
+import numpy as np
+
 _WORLDS = {}
 
 
@@ -32,7 +34,7 @@ def _world(kind, w, seed, size):
 
         if kind == "grid":
             world = worlds.grid_world(size, size, worlds.world_rng(seed, w))
-        elif kind == "uneven":  # the uneven batch's world w (size given), with its channels
+        elif kind in ("uneven", "adjoint"):  # world w of an uneven or adjoint batch (size given)
             world = worlds.uneven_world(w, size, seed, worlds.UNEVEN_CHANNELS)
         else:
             world = worlds.delaunay_world(size, worlds.world_rng(seed, w))
@@ -57,6 +59,30 @@ def run_world(task):
     return b.cells * steps, elapsed
 
 
+def run_adjoint_world(task):
+    """(kind, world index, seed, size, steps, dt) -> (cell-steps, seconds): steps forward steps
+    of the oracle, each state kept, then the oracle adjoint back over them from the cotangent of
+    the voltage-pattern loss (the gradient a trajectory of that many steps takes)."""
+    _pin_blas()
+    from cells_b200 import worlds
+    from oracle import adjoint as A
+    from oracle import tissue as T
+
+    kind, w, seed, size, steps, dt = task
+    entry = _world(kind, w, seed, size)
+    b, topo, ctl, st = entry
+    target = worlds.voltage_target(b)
+    t0 = time.perf_counter()
+    states = [st]
+    for _ in range(steps):
+        states.append(T.ars222_step(states[-1], dt, ctl, b, topo)[0])
+    _, cot_n = A.voltage_loss(states[-1], b, topo, target)
+    cot = (cot_n, np.zeros(b.edges), np.zeros_like(st.channel_gate))
+    for t in range(steps - 1, -1, -1):
+        cot, _, _, _ = A.step_vjp(states[t], dt, ctl, b, topo, *cot)
+    return b.cells * steps, time.perf_counter() - t0
+
+
 def prepare(task):
     """Build (and keep) a task's world in this worker without stepping it."""
     _pin_blas()
@@ -73,15 +99,17 @@ def pool(processes=None):
     return ctx.Pool(processes or os.cpu_count() or 1)
 
 
-def measure(tasks, processes=None):
+def measure(tasks, processes=None, fn=None):
     """Run the tasks over a spawn pool; returns (cell-steps, wall seconds, processes).
 
     Every task's world is built in a warm-up pass (one step each) before the timed pass, so the
-    wall time covers stepping and the pool's dispatch only."""
+    wall time covers stepping and the pool's dispatch only. ``fn``: run_world (default) or
+    run_adjoint_world."""
     processes = processes or os.cpu_count() or 1
+    fn = fn or run_world
     with pool(processes) as p:
-        p.map(run_world, [t[:4] + (1, t[5]) for t in tasks], chunksize=1)
+        p.map(fn, [t[:4] + (1, t[5]) for t in tasks], chunksize=1)
         t0 = time.perf_counter()
-        results = p.map(run_world, tasks, chunksize=1)
+        results = p.map(fn, tasks, chunksize=1)
         wall = time.perf_counter() - t0
     return sum(r[0] for r in results), wall, processes
