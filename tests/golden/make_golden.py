@@ -28,6 +28,9 @@ Fixtures:
                          junctions, partial controls, a -4 mV bath, @3, 200 steps.
   pytrees_v3_channels_padded.npz  That world's @3 pytrees with every capacity 2 above its count
                          (layout, controls, padded states over 40 steps), for the drop-in step.
+  n2_grid4x4.npz         The 4x4 world under N2 (@3, implicit slope conductances), 300 steps.
+  n2_channels_delaunay.npz  A 40-cell Delaunay world with NaV1.2 and Kv1.5 populations, gated
+                         junctions, partial controls, a -4 mV bath, under N2, 200 steps.
   laws.npz               Point laws on grids of inputs: bernoulli, the pump kinetics and the
                          junction gate rate.
 """
@@ -291,6 +294,39 @@ def make_channel_trajectories():
           extra={"control_" + k.split("_")[0]: v for k, v in controls.items()})
 
 
+def make_n2_trajectories():
+    """@3 under N2 (cells.solver.imex_ars222_implicit_conductances@1): the membranes', channels'
+    and junctions' slope conductances implicit, junction gates by their exponential update."""
+    from cells_b200 import worlds
+
+    n2 = "cells.solver.imex_ars222_implicit_conductances@1"
+    v3 = "cells.model.resolved_pump_tissue@3"
+    world = worlds.single_grid_tissue(0)
+    keep = {0, 1, 2, 10, 100, 300}
+    stacked, kept, el = _run(world, model_id=v3, dt=1e-3, steps=300, keep=keep, solver=n2)
+    _save("n2_grid4x4.npz", worlds.pack([world]), stacked, kept, dt=1e-3, model_id=v3,
+          solver=n2, elapsed=el)
+
+    rng = np.random.default_rng(31)
+    dworld = worlds.with_channels(
+        worlds.delaunay_world(40, worlds.world_rng(5, 0), junction_sigma=0.3,
+                              gate=(0.02, 0.1, 0.8)), rng,
+        na=("nav", 4e-10, 0.4), k=("kv", 5e-10, 0.6), sigma=0.3)
+    dworld.bath_potential = -0.004
+    controls = dict(
+        membrane_control=rng.uniform(0.5, 1.0, dworld.cells),
+        junction_control=rng.uniform(0.5, 1.0, dworld.edges),
+        pump_control=rng.uniform(0.5, 1.0, dworld.cells),
+        channel_control=rng.uniform(0.3, 1.0, (2, dworld.cells)),
+    )
+    keep = {0, 1, 2, 10, 100, 200}
+    stacked, kept, el = _run(dworld, model_id=v3, dt=1e-3, steps=200, keep=keep, solver=n2,
+                             controls=controls, channels=True)
+    _save("n2_channels_delaunay.npz", worlds.pack([dworld]), stacked, kept, dt=1e-3,
+          model_id=v3, solver=n2, elapsed=el,
+          extra={"control_" + k.split("_")[0]: v for k, v in controls.items()})
+
+
 def make_laws():
     from cells.laws import electrochemistry as ec
     from cells.laws.junctions import junction_voltage_relaxation as jg
@@ -329,7 +365,7 @@ def make_laws():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("laws", "trajectories", "channels"))
+    ap.add_argument("--only", choices=("laws", "trajectories", "channels", "n2"))
     args = ap.parse_args()
     _setup(args.reference)
     if args.only in (None, "laws"):
@@ -338,6 +374,8 @@ def main():
         make_trajectories()
     if args.only in (None, "channels"):
         make_channel_trajectories()
+    if args.only in (None, "n2"):
+        make_n2_trajectories()
 
 
 if __name__ == "__main__":
