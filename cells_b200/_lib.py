@@ -35,6 +35,7 @@ STATE_FIELDS = (
 CONTROL_FIELDS = ("membrane", "junction", "pump", "channel")
 METHOD_ARS222 = 0
 METHOD_ARS222_MIXED = 1
+METHOD_N2 = 2
 KERNEL_SHARED, KERNEL_PACKED = 0, 1
 WORLD_BITS = {
     1: "transport",
@@ -46,6 +47,7 @@ WORLD_BITS = {
     64: "stiff",
     128: "channel_domain",
     256: "ledger_cotangent",
+    512: "operator",
 }
 EXPORTS = (
     "cb_bind",

@@ -32,6 +32,18 @@ int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 const char *last_error();
 
+struct N2Plan;  // n2_step.cu
+
+}  // namespace cbk
+
+struct cb_tissue;
+
+namespace cbk {
+// The N2 method (n2_step.cu): n_steps steps of every world, device buffers (cb_step's contract).
+int n2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
+            const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
+            cudaStream_t stream);
+void n2_release(cb_tissue *t);
 }  // namespace cbk
 
 struct cb_tissue {
@@ -58,4 +70,10 @@ struct cb_tissue {
   // Patch and junction areas (m^2): the permeability prefactors and the adjoint's gradients.
   const double *area = nullptr;   // [C]
   const double *jarea = nullptr;  // [E]
+  // Host copies of the contact graph for plans built after bind: world offsets and the
+  // world-local junction endpoints.
+  std::vector<long long> h_cell_offset, h_edge_offset;
+  std::vector<int> h_snd, h_rcv;
+  // The N2 method's sparse-factor plan and workspace, built at its first step.
+  cbk::N2Plan *n2 = nullptr;
 };

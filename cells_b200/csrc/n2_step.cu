@@ -1,0 +1,1247 @@
+// n2_step.cu - the N2 step (CB_METHOD_N2): ARS(2,2,2) with the routes' slope conductances in the
+// implicit operator, for held-bath worlds, and the batched sparse Cholesky it factors each step.
+//
+// Reference: models/surface_pump_v3.py:3547-3955 (imex_step under
+// cells.solver.imex_ars222_implicit_conductances@1): operator_time_conductances :2961-3029,
+// conductance_weights / route_slope :2741-2813 (bernoulli_slope of
+// laws/routes/patch_electrodiffusion.py:43-54), conductance_laplacian :2816-2841,
+// explicit_remainder :2925-2946, implicit_rates :2659-2700, implicit_route_heat :2949-2958,
+// stage_junction_gates :3130-3156; the operator factor and solve of numerics/surface_imex.py
+// :207-225, :269-278; the sparse factor's plan of numerics/sparse_cholesky.py:137-215 (a
+// minimum-degree order, the elimination tree's union rule, levels).
+//
+// One CTA advances one world n_steps steps; threads loop over the world's cells and junctions.
+// Per step, for each world:
+//   stage 0   whole rates at the start potentials (cells, then junctions, then each cell's gather
+//             of its junction fluxes in edge order);
+//   predict   amounts, channel gates and junction gates half a step ahead, their potentials; the
+//             slopes W = dJ/d(dv) of every patch, channel population and junction there; the
+//             conductances G = F/1e15 sum_s z_s W_s;
+//   operator  M = C + gamma dt L on the cells (the held bath clamped), Jacobi scaled, assembled
+//             into the world's factor pattern and factored left-looking, level by level of the
+//             elimination tree (a warp per column; each update term's destination precomputed on
+//             the host, so no atomics);
+//   stage i   the stage's charges, forward and back substitution by levels, the potentials; the
+//             routes' linear fluxes W dv there (the implicit drift), their heat at the stage; the
+//             remainders J - W dv of the explicit rates; channel and junction gates by their
+//             exponential updates from the step start;
+//   book      ledgers as the plain step; accept or refuse the world's step as a whole.
+// Stage values live in a global scratch that stays in L2 while the world's CTA runs.
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <queue>
+#include <set>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "handle.h"
+
+namespace cbk {
+
+struct N2Dev {
+  int *rank;      // [C] cell -> position (world base + minimum-degree rank)
+  int *colp;      // [C+1] position -> first factor entry (global)
+  int *lrow;      // [F] factor entry -> row position
+  int *uk_ptr;    // [C+1] position j -> its update list (the columns k < j with L_jk != 0)
+  int *uk_col;    // [U] column position k
+  int *uk_pos;    // [U] factor entry of L_jk
+  int *uk_rel;    // [U] offset into rel of the pair's relative indices
+  int *rel;       // [R] entry of column k at or below row j -> offset in column j
+  int *lv_world;  // [W+1] first level of each world
+  int *lv_ptr;    // [levels+1] first column of each level in lv_cols
+  int *lv_cols;   // [C] positions, level by level
+  int *edge_pos;  // [E] factor entry of the junction's off-diagonal
+  double *lval;   // [F] factor values
+  double *cs;     // cell scratch [NC_FIELDS][C]
+  double *es;     // junction scratch [NE_FIELDS][E]
+};
+
+struct N2Plan {
+  N2Dev d{};
+  std::vector<void *> owned;
+  long long factor_entries = 0, update_terms = 0;
+  int levels = 0, max_level = 0;
+};
+
+}  // namespace cbk
+
+namespace {
+
+using namespace cbk;
+
+// The stage solve's acceptance (surface_field.CHARGE_ATOL_C, CHARGE_RTOL).
+constexpr double kChargeAtol = 3e-25;
+constexpr double kChargeRtol = 2e-12;
+
+// Cell scratch fields ([field][C]).
+enum N2Cell {
+  NC_CX = 0,    // 3: the current stage's concentrations
+  NC_LX = 3,    // 3: their logs
+  NC_VX = 6,    // the current stage's potential
+  NC_CP = 7,    // 3: predicted concentrations
+  NC_VP = 10,   // predicted potential
+  NC_WM = 11,   // 3: patch slopes W (fmol/s per V)
+  NC_GP = 14,   // patch conductance (its channels' included)
+  NC_S = 15,    // Jacobi scale 1/sqrt(M_ii)
+  NC_MD = 16,   // M_ii
+  NC_MB = 17,   // M_i,bath
+  NC_A = 18,    // 10: accumulators n[3], mt[3], md, pc, pd, mw
+  NC_K1 = 28,   // 3: stage-1 known amounts
+  NC_KN = 31,   // 3: the stage-0 whole amount rate, then the stage-1 drift's amount rate
+  NC_JM = 34,   // 3: the stage's patch flux J_m
+  NC_EX = 37,   // 3: the stage's outward pump + channel transfer ("extra")
+  NC_R = 40,    // 4: the stage's md, cycles, pd, mw
+  NC_Y = 44,    // forward solve (position-indexed)
+  NC_X = 45,    // back solve (position-indexed)
+  NC_CH = 46    // per channel slot q: W, t0[2], tau0[2], gate[2], acc transferred, acc heat,
+                //   J, J heat: 11 fields
+};
+constexpr int kN2ChFields = 11;
+enum N2ChField {
+  CH_W = 0, CH_T0 = 1, CH_TAU0 = 3, CH_G = 5, CH_AT = 7, CH_AD = 8, CH_J = 9, CH_JD = 10
+};
+__host__ __device__ constexpr int n2_cell_fields(int nch) { return NC_CH + kN2ChFields * nch; }
+// Junction scratch fields ([field][E]).
+enum N2Edge {
+  NE_J = 0,     // 3: flux for the cells' gather
+  NE_W = 3,     // 3: slopes W
+  NE_G = 6,     // conductance
+  NE_T0 = 7,    // start target of the gate law
+  NE_R0 = 8,    // start relaxation rate
+  NE_GX = 9,    // predicted gate, then the stage gate
+  NE_A = 10,    // 4: accumulators jt[3], jd
+  NE_JJ = 14,   // 3: the stage's whole flux
+  NE_JD = 17,   // the stage's whole heat
+  NE_FIELDS = 18
+};
+
+// B'(x), the reference's form (patch_electrodiffusion.bernoulli_slope): the series
+// -1/2 + x/6 - x^3/180 below |x| < 1e-3, otherwise with em = e^-|x|:
+// x > 0: (em (1 - x) - em^2) / (1 - em)^2; x < 0: (em - 1 - x em) / (em - 1)^2.
+__device__ __forceinline__ double ref_bernoulli_slope(double x) {
+  if (fabs(x) < 1e-3) return (-0.5 + x / 6.0) - ((x * x) * x) / 180.0;
+  const double em = exp(-fabs(x));
+  if (x > 0.0) {
+    const double d = 1.0 - em;
+    return (em * (1.0 - x) - em * em) / (d * d);
+  }
+  const double d = em - 1.0;
+  return ((em - 1.0) - x * em) / (d * d);
+}
+
+// dJ/d(dv) of a route with prefactor g (fmol/s per mM) between c_from and c_to, valence z.
+__device__ __forceinline__ double route_slope(double g, double c_from, double c_to, double dv,
+                                              double zfrt) {
+  const double x = zfrt * dv;
+  return g * zfrt * (-c_from * ref_bernoulli_slope(-x) - c_to * ref_bernoulli_slope(x));
+}
+
+__device__ __forceinline__ void junction_law(double dv, double thr, double mn, double &target,
+                                             double &relaxation) {
+  const double shift = fabs(dv) - thr;
+  const double alpha = 1.3 * exp(-77.0 * shift);
+  const double log_beta = kLog0065 + 140.0 * shift;
+  const double beta = 20.0 * exp(-logaddexp0(-log_beta));
+  relaxation = alpha + beta;
+  target = (alpha + beta * mn) / relaxation;
+}
+
+__device__ __forceinline__ bool gate_domain(double g, double dv, double thr, double mn,
+                                            double jc) {
+  return is_finite(thr) && thr >= 0.0 && thr <= kMaxAbsJunctionV && is_finite(mn) && mn >= 0.0 &&
+         mn <= 1.0 && is_finite(dv) && fabs(dv) <= kMaxAbsJunctionV && is_finite(g) && g >= mn &&
+         g <= 1.0 && is_finite(jc) && jc >= 0.0 && jc <= 1.0;
+}
+
+// A cell's own whole rates at a stage (patch flux, pump, channel populations), the plain step's
+// arithmetic: J_m[3], extra[3] (outward pump + channel transfer), md, cycles, pd, mw, each
+// population's J and heat; validity bits. Gate m of slot q at gate[q slot_stride], h at
+// gate[q slot_stride + row_stride].
+template <int NCH>
+__device__ __forceinline__ uint32_t own_rates(const Tissue &T, const double *__restrict__ wc,
+                                              long long gi, const double (&c)[3],
+                                              const double (&lc)[3], double V, const double *gate,
+                                              long long slot_stride, long long row_stride,
+                                              double mc, double pctl,
+                                              double ldc, const double *chctl, double (&jm)[3],
+                                              double (&extra)[3], double (&r4)[4],
+                                              double (&chj)[NCH > 0 ? NCH : 1],
+                                              double (&chd)[NCH > 0 ? NCH : 1]) {
+  const long long C = T.C;
+  uint32_t bits = 0;
+  const double RT = wc[WC_RT], dv = V - wc[WC_VB];
+  const double x = dv * wc[WC_FRT];
+  if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
+  if (!is_finite(V)) bits |= CB_WORLD_TRANSPORT;
+  double bp, bm;
+  bernoulli_pair<double>(x, bp, bm);
+  double mu[3];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    if (!(is_finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
+    const double gs = __ldg(T.ap + s * C + gi) * mc;
+    const double co = wc[WC_CO + s];
+    jm[s] = (s < 2) ? gs * (c[s] * bm - co * bp) : gs * (c[s] * bp - co * bm);
+    mu[s] = RT * (lc[s] - wc[WC_LOGCO + s]) + ((s < 2) ? kF * dv : (-kF) * dv);
+  }
+  const double md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
+  if (!(is_finite(jm[0]) && is_finite(jm[1]) && is_finite(jm[2]) && is_finite(md)))
+    bits |= CB_WORLD_TRANSPORT;
+  if (!(is_finite(mc) && mc >= 0.0 && mc <= 1.0 && is_finite(pctl) && pctl >= 0.0 && pctl <= 1.0))
+    bits |= CB_WORLD_CONTROL;
+  double chm[3] = {0.0, 0.0, 0.0};
+  if constexpr (NCH > 0) {
+#pragma unroll
+    for (int q = 0; q < NCH; ++q) {
+      const int code = __ldg(T.ch_code + q * C + gi);
+      const int sp = __ldg(T.ch_species + q * C + gi);
+      const double ctl = __ldg(chctl + q * C);
+      if (!(is_finite(ctl) && ctl >= 0.0 && ctl <= 1.0)) bits |= CB_WORLD_CONTROL;
+      const double open =
+          channel_opening(code, gate[q * slot_stride], gate[q * slot_stride + row_stride]);
+      const double gq = __ldg(T.ch_ap + q * C + gi) * ((open * ctl) * __ldg(T.ch_ab + q * C + gi));
+      const double cs_ = sp == 0 ? c[0] : sp == 1 ? c[1] : c[2];
+      const double co = wc[WC_CO + sp];
+      const double J = sp < 2 ? gq * (cs_ * bm - co * bp) : gq * (cs_ * bp - co * bm);
+      const double Jd = 1e-3 * J * (sp == 0 ? mu[0] : sp == 1 ? mu[1] : mu[2]);
+      chj[q] = J;
+      chd[q] = Jd;
+      chm[sp] += J;
+      if (!(is_finite(J) && is_finite(Jd))) bits |= CB_WORLD_TRANSPORT;
+    }
+  }
+  const double energy = (wc[WC_DRIVE] + (-3.0) * mu[0]) + 2.0 * mu[1];
+  const double a = energy * wc[WC_INVRT];
+  double cycles = 0.0;
+  if (__ldg(T.pcap + gi) > 0.0 && pctl > 0.0) {
+    const double ls = ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
+    const double mag = exp((ldc + ls) + fmax(a, 0.0));
+    cycles = mag * (a >= 0.0 ? expm1(-a) : -expm1(a));
+  }
+  r4[0] = md;
+  r4[1] = cycles;
+  r4[2] = (-1e-3 * cycles) * energy;
+  r4[3] = (-1e-3 * cycles) * wc[WC_DRIVE];
+  extra[0] = (3.0 * cycles - 0.0) + chm[0];
+  extra[1] = (-2.0 * cycles - 0.0) + chm[1];
+  extra[2] = (-0.0 * cycles - 0.0) + chm[2];
+  const double sna = mu[0] * wc[WC_INVRTD], sk = mu[1] * wc[WC_INVRTD];
+  const double aff = (wc[WC_AFF0] + (-3.0) * sna) + 2.0 * sk;
+  const double capacity = __ldg(T.pcap + gi);
+  const bool pump_ok = wc[WC_PUMPOK] != 0.0 && is_finite(capacity) && capacity >= 0.0 &&
+                       is_finite(sna) && fabs(sna) <= kMaxAbsIonPotentialOverRT && is_finite(sk) &&
+                       fabs(sk) <= kMaxAbsIonPotentialOverRT && is_finite(aff) &&
+                       fabs(aff) <= kMaxAbsAffinityOverRT;
+  if (!pump_ok) bits |= CB_WORLD_PUMP_DOMAIN;
+  if (!(is_finite(cycles) && is_finite(r4[2]) && is_finite(r4[3]))) bits |= CB_WORLD_TRANSPORT;
+  return bits;
+}
+
+// A junction's whole flux at a stage: jj[3], its heat; validity bits.
+__device__ __forceinline__ uint32_t junction_flux(const Tissue &T, const double *__restrict__ wc,
+                                                  long long ge, const double (&ca)[3],
+                                                  const double (&cb)[3], const double (&la)[3],
+                                                  const double (&lb)[3], double dv,
+                                                  double opening, double (&jj)[3], double &jd) {
+  const long long E = T.E;
+  uint32_t bits = 0;
+  const double x = dv * wc[WC_FRT];
+  if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
+  double bp, bm, mu[3];
+  bernoulli_pair<double>(x, bp, bm);
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const double gs = __ldg(T.jap + s * E + ge) * opening;
+    jj[s] = (s < 2) ? gs * (ca[s] * bm - cb[s] * bp) : gs * (ca[s] * bp - cb[s] * bm);
+    mu[s] = wc[WC_RT] * (la[s] - lb[s]) + ((s < 2) ? kF * dv : (-kF) * dv);
+  }
+  jd = 1e-3 * ((jj[0] * mu[0] + jj[1] * mu[1]) + jj[2] * mu[2]);
+  if (!(is_finite(jj[0]) && is_finite(jj[1]) && is_finite(jj[2]) && is_finite(jd)))
+    bits |= CB_WORLD_TRANSPORT;
+  return bits;
+}
+
+// The electrochemical differences of a junction (sender minus receiver) and of a patch.
+__device__ __forceinline__ void junction_mu(const double *__restrict__ wc, const double (&la)[3],
+                                            const double (&lb)[3], double dv, double (&mu)[3]) {
+#pragma unroll
+  for (int s = 0; s < 3; ++s)
+    mu[s] = wc[WC_RT] * (la[s] - lb[s]) + ((s < 2) ? kF * dv : (-kF) * dv);
+}
+__device__ __forceinline__ void patch_mu(const double *__restrict__ wc, const double (&lc)[3],
+                                         double dv, double (&mu)[3]) {
+#pragma unroll
+  for (int s = 0; s < 3; ++s)
+    mu[s] = wc[WC_RT] * (lc[s] - wc[WC_LOGCO + s]) + ((s < 2) ? kF * dv : (-kF) * dv);
+}
+
+template <int BLOCK, int NCH>
+__global__ void __launch_bounds__(BLOCK)
+    n2_kernel(const Tissue T, const Layout L, const N2Dev D, const double *state_in,
+              double *state_out, const double *__restrict__ control, const StepCoef k,
+              int n_steps, uint32_t *__restrict__ world_status,
+              int32_t *__restrict__ accepted_steps) {
+  constexpr int NQ = NCH > 0 ? NCH : 1;
+  __shared__ double sW[WC_STRIDE];
+  __shared__ double sRed[(BLOCK / 32) * 16];
+  __shared__ unsigned int sBits;
+  const int w = blockIdx.x, tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  constexpr int WARPS = BLOCK / 32;
+  const int c0 = T.cell_offset[w], nc = T.cell_offset[w + 1] - c0;
+  const int e0 = T.edge_offset[w], ne = T.edge_offset[w + 1] - e0;
+  const long long C = T.C, E = T.E, W = T.W;
+  if (tid < WC_STRIDE) sW[tid] = T.world[(size_t)w * WC_STRIDE + tid];
+  if (tid == 0) sBits = 0u;
+  double *cs = D.cs;
+  double *es = D.es;
+  double *lval = D.lval;
+  const long long oN = L.s[CB_AMOUNT_INCREMENT], oG = L.s[CB_JUNCTION_GATE];
+  const long long oH = L.s[CB_CHANNEL_GATE];
+  const double *mctl = control + L.c[CB_CONTROL_MEMBRANE];
+  const double *pctlp = control + L.c[CB_CONTROL_PUMP];
+  const double *jctl = control + L.c[CB_CONTROL_JUNCTION];
+  const double *chctl0 = control + L.c[CB_CONTROL_CHANNEL];
+  const double K = kChargePerFmol;
+  const double gdt = k.gamma_dt;               // the implicit diagonal gamma dt (the operator's)
+  const double theta = 0.5 * k.dt;             // the routes' operator time
+  const double w1 = (1.0 - (1.0 - 1.0 / sqrt(2.0))) * k.dt;  // (1 - gamma) dt
+  const int lv0 = D.lv_world[w], lv1 = D.lv_world[w + 1];
+  auto CF = [&](int f, long long gi) -> double & { return cs[(long long)f * C + gi]; };
+  auto EF = [&](int f, long long ge) -> double & { return es[(long long)f * E + ge]; };
+  auto CH = [&](int q, int f, long long gi) -> double & {
+    return cs[(long long)(NC_CH + q * kN2ChFields + f) * C + gi];
+  };
+  __syncthreads();
+  const double Vb = sW[WC_VB];
+  double res[3], ec, rw, ew;
+  for (int s = 0; s < 3; ++s) res[s] = state_in[L.s[CB_RESERVOIR_SUPPLIED] + s * W + w];
+  ec = state_in[L.s[CB_ELECTRODE_CHARGE] + w];
+  rw = state_in[L.s[CB_RESERVOIR_WORK] + w];
+  ew = state_in[L.s[CB_ELECTRODE_WORK] + w];
+  const double *cur = state_in;
+  int taken = 0;
+  uint32_t refused = 0u;
+
+  // Left-looking factor of the world's pattern, level by level; a warp per column.
+  auto factor = [&]() {
+    uint32_t bad = 0;
+    for (int lv = lv0; lv < lv1; ++lv) {
+      const int a0 = D.lv_ptr[lv], a1 = D.lv_ptr[lv + 1];
+      for (int a = a0 + warp; a < a1; a += WARPS) {
+        const int j = D.lv_cols[a];
+        const int cj = D.colp[j];
+        for (int u = D.uk_ptr[j]; u < D.uk_ptr[j + 1]; ++u) {
+          const int kk = D.uk_col[u], p = D.uk_pos[u], r0 = D.uk_rel[u];
+          const int cnt = D.colp[kk + 1] - p;
+          const double ljk = lval[p];
+          for (int t = lane; t < cnt; t += 32) lval[cj + D.rel[r0 + t]] -= lval[p + t] * ljk;
+          __syncwarp();
+        }
+        double piv = 0.0;
+        if (lane == 0) {
+          const double d = lval[cj];
+          if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+          piv = sqrt(d);
+          lval[cj] = piv;
+        }
+        piv = __shfl_sync(0xffffffffu, piv, 0);
+        const double inv = 1.0 / piv;
+        const int len = D.colp[j + 1] - cj;
+        for (int t = 1 + lane; t < len; t += 32) lval[cj + t] *= inv;
+        __syncwarp();
+      }
+      __syncthreads();
+    }
+    return bad;
+  };
+  // Forward and back substitution of L L^T x = b (b in NC_Y, position-indexed; x to NC_X).
+  auto solve = [&]() {
+    for (int lv = lv0; lv < lv1; ++lv) {
+      for (int a = D.lv_ptr[lv] + tid; a < D.lv_ptr[lv + 1]; a += BLOCK) {
+        const int j = D.lv_cols[a];
+        double b = CF(NC_Y, j);
+        for (int u = D.uk_ptr[j]; u < D.uk_ptr[j + 1]; ++u)
+          b -= lval[D.uk_pos[u]] * CF(NC_Y, D.uk_col[u]);
+        CF(NC_Y, j) = b / lval[D.colp[j]];
+      }
+      __syncthreads();
+    }
+    for (int lv = lv1 - 1; lv >= lv0; --lv) {
+      for (int a = D.lv_ptr[lv] + tid; a < D.lv_ptr[lv + 1]; a += BLOCK) {
+        const int j = D.lv_cols[a];
+        const int cj = D.colp[j], len = D.colp[j + 1] - cj;
+        double x = CF(NC_Y, j);
+        for (int t = 1; t < len; ++t) x -= lval[cj + t] * CF(NC_X, D.lrow[cj + t]);
+        CF(NC_X, j) = x / lval[cj];
+      }
+      __syncthreads();
+    }
+  };
+  // A cell's gather over its junctions (senders first, then receivers, edge order) of field f.
+  auto gather = [&](long long gi, int f, double (&send)[3], double (&recv)[3]) {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) send[s] = recv[s] = 0.0;
+    for (int a = __ldg(T.adj_ptr + gi); a < __ldg(T.adj_ptr + gi + 1); ++a) {
+      const int code = __ldg(T.adj_idx + a);
+      const long long ge = e0 + (code >> 1);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        if (code & 1) recv[s] += EF(f + s, ge);
+        else send[s] += EF(f + s, ge);
+      }
+    }
+  };
+  // Concentrations and logs of amounts n, into the current-stage fields.
+  auto set_stage = [&](long long gi, const double (&n)[3], double V) {
+    const double ivol = __ldg(T.ivol + gi);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const double c = (__ldg(T.ref + s * C + gi) + n[s]) * ivol;
+      CF(NC_CX + s, gi) = c;
+      CF(NC_LX + s, gi) = log(c);
+    }
+    CF(NC_VX, gi) = V;
+  };
+  auto potential_of = [&](long long gi, const double (&n)[3]) {
+    return (__ldg(T.q0 + gi) + K * ((n[0] + n[1]) + (-n[2]))) * __ldg(T.icap + gi) + Vb;
+  };
+  // The operator's row product (M phi)_i (neighbours' potentials in NC_VX) less the charge q.
+  auto row_residual = [&](long long gi, double q, double &product) {
+    double sum = CF(NC_MD, gi) * CF(NC_VX, gi);
+    for (int a = __ldg(T.adj_ptr + gi); a < __ldg(T.adj_ptr + gi + 1); ++a) {
+      const int code = __ldg(T.adj_idx + a);
+      const long long ge = e0 + (code >> 1);
+      const long long nb = c0 + ((code & 1) ? __ldg(T.snd + ge) : __ldg(T.rcv + ge));
+      sum += (gdt * (-EF(NE_G, ge))) * CF(NC_VX, nb);
+    }
+    product = sum + CF(NC_MB, gi) * Vb;
+    return product - q;
+  };
+
+  for (int step = 0; step < n_steps; ++step) {
+    uint32_t bits = 0;
+    double inflow0[3] = {0, 0, 0}, outlin0[3] = {0, 0, 0}, plate0 = 0.0;
+    // P1 (cells): the start: concentrations, potentials, own whole rates, start kinetics.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      double n[3], c[3], lc[3];
+      for (int s = 0; s < 3; ++s) n[s] = cur[oN + s * C + gi];
+      const double V0 = potential_of(gi, n);
+      set_stage(gi, n, V0);
+      for (int s = 0; s < 3; ++s) {
+        c[s] = CF(NC_CX + s, gi);
+        lc[s] = CF(NC_LX + s, gi);
+      }
+      plate0 += -(K * ((n[0] + n[1]) + (-n[2])));
+      const double pctl = pctlp[gi];
+      const double ldc = pctl > 0.0 ? __ldg(T.logpcap + gi) + log(pctl) : 0.0;
+      double jm[3], ex[3], r4[4], chj[NQ], chd[NQ];
+      bits |= own_rates<NCH>(T, sW, gi, c, lc, V0, cur + oH + gi, C, NCH * C, mctl[gi], pctl,
+                             ldc, chctl0 + gi, jm, ex, r4, chj, chd);
+      for (int s = 0; s < 3; ++s) {
+        CF(NC_JM + s, gi) = jm[s];
+        CF(NC_EX + s, gi) = ex[s];
+        inflow0[s] += jm[s] + ex[s];
+      }
+      for (int f = 0; f < 4; ++f) CF(NC_R + f, gi) = r4[f];
+      if constexpr (NCH > 0) {
+        for (int q = 0; q < NCH; ++q) {
+          CH(q, CH_J, gi) = chj[q];
+          CH(q, CH_JD, gi) = chd[q];
+          double t[2], tau[2];
+          channel_kinetics<false>(__ldg(T.ch_code + q * C + gi), V0 - Vb, t, tau);
+          if (!channel_kinetics_ok(V0 - Vb, t, tau)) bits |= CB_WORLD_CHANNEL_DOMAIN;
+          for (int r = 0; r < 2; ++r) {
+            CH(q, CH_T0 + r, gi) = t[r];
+            CH(q, CH_TAU0 + r, gi) = tau[r];
+          }
+        }
+      }
+      // Zero the world's factor columns held by this thread's cells.
+      const int P = __ldg(D.rank + gi);
+      for (int f = D.colp[P]; f < D.colp[P + 1]; ++f) lval[f] = 0.0;
+    }
+    __syncthreads();
+    // E1 (junctions): stage-0 whole fluxes, the gate law at the start, the predicted gate.
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      const long long ga = c0 + __ldg(T.snd + ge), gb = c0 + __ldg(T.rcv + ge);
+      double ca[3], cb[3], la[3], lb[3], jj[3], jd;
+      for (int s = 0; s < 3; ++s) {
+        ca[s] = CF(NC_CX + s, ga);
+        cb[s] = CF(NC_CX + s, gb);
+        la[s] = CF(NC_LX + s, ga);
+        lb[s] = CF(NC_LX + s, gb);
+      }
+      const double dv = CF(NC_VX, ga) - CF(NC_VX, gb);
+      const double g = cur[oG + ge], jc = jctl[ge];
+      bits |= junction_flux(T, sW, ge, ca, cb, la, lb, dv, jc * g, jj, jd);
+      for (int s = 0; s < 3; ++s) {
+        EF(NE_J + s, ge) = jj[s];
+        EF(NE_JJ + s, ge) = jj[s];
+      }
+      EF(NE_JD, ge) = jd;
+      const double thr = __ldg(T.thr + ge), mn = __ldg(T.jmin + ge);
+      if (!gate_domain(g, dv, thr, mn, jc)) bits |= CB_WORLD_GATE_DOMAIN;
+      double t0, r0;
+      junction_law(dv, thr, mn, t0, r0);
+      EF(NE_T0, ge) = t0;
+      EF(NE_R0, ge) = r0;
+      EF(NE_GX, ge) = g + (t0 - g) * -expm1(-r0 * theta);
+    }
+    __syncthreads();
+    // P2 (cells): the whole stage-0 amount rate, the prediction, the patch slopes.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      double send[3], recv[3], np_[3], cp[3];
+      gather(gi, NE_J, send, recv);
+      const double ivol = __ldg(T.ivol + gi);
+      for (int s = 0; s < 3; ++s) {
+        const double rate = ((-CF(NC_JM + s, gi) + (-send[s])) + recv[s]) - CF(NC_EX + s, gi);
+        CF(NC_KN + s, gi) = rate;
+        np_[s] = cur[oN + s * C + gi] + theta * rate;
+        cp[s] = (__ldg(T.ref + s * C + gi) + np_[s]) * ivol;
+        CF(NC_CP + s, gi) = cp[s];
+        if (!(is_finite(cp[s]) && cp[s] > 0.0)) bits |= CB_WORLD_OPERATOR;
+      }
+      const double Vp = potential_of(gi, np_);
+      CF(NC_VP, gi) = Vp;
+      if (!is_finite(Vp)) bits |= CB_WORLD_OPERATOR;
+      const double dv = Vp - Vb, mc = mctl[gi];
+      double gp = 0.0;
+      double zw[3];
+      for (int s = 0; s < 3; ++s) {
+        const double zfrt = (s < 2 ? 1.0 : -1.0) * sW[WC_FRT];
+        const double W_ = route_slope(__ldg(T.ap + s * C + gi) * mc, cp[s], sW[WC_CO + s], dv,
+                                      zfrt);
+        CF(NC_WM + s, gi) = W_;
+        zw[s] = (s < 2 ? 1.0 : -1.0) * W_;
+        if (!is_finite(W_)) bits |= CB_WORLD_OPERATOR;
+      }
+      gp = K * ((zw[0] + zw[1]) + zw[2]);
+      if constexpr (NCH > 0) {
+        double extra = 0.0;
+        for (int q = 0; q < NCH; ++q) {
+          const int code = __ldg(T.ch_code + q * C + gi);
+          const int sp = __ldg(T.ch_species + q * C + gi);
+          double gq[2];
+          for (int r = 0; r < 2; ++r) {
+            const double g0 = cur[oH + (r * NCH + q) * C + gi];
+            gq[r] = (r == 1 && code == kHhKn4)
+                        ? g0
+                        : advance_gate<false>(g0, CH(q, CH_T0 + r, gi), CH(q, CH_TAU0 + r, gi),
+                                              CH(q, CH_T0 + r, gi), CH(q, CH_TAU0 + r, gi), theta);
+          }
+          const double available = (__ldg(T.ch_ab + q * C + gi) * channel_opening(code, gq[0], gq[1])) *
+                                   __ldg(chctl0 + q * C + gi);
+          const double zfrt = (sp < 2 ? 1.0 : -1.0) * sW[WC_FRT];
+          const double W_ = route_slope(__ldg(T.ch_ap + q * C + gi) * available, cp[sp],
+                                        sW[WC_CO + sp], dv, zfrt);
+          CH(q, CH_W, gi) = W_;
+          if (!is_finite(W_)) bits |= CB_WORLD_OPERATOR;
+          extra = extra + K * ((sp < 2 ? 1.0 : -1.0) * W_);
+        }
+        gp = gp + extra;
+      }
+      CF(NC_GP, gi) = gp;
+    }
+    __syncthreads();
+    // E2 (junctions): slopes and conductances at the prediction; the stage-0 linear part and its
+    // heat; the junction accumulators y + delta dt (J - W dv).
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      const long long ga = c0 + __ldg(T.snd + ge), gb = c0 + __ldg(T.rcv + ge);
+      const double dvp = CF(NC_VP, ga) - CF(NC_VP, gb);
+      const double opening = jctl[ge] * EF(NE_GX, ge);
+      double zw[3], la[3], lb[3], mu[3];
+      for (int s = 0; s < 3; ++s) {
+        const double zfrt = (s < 2 ? 1.0 : -1.0) * sW[WC_FRT];
+        const double W_ = route_slope(__ldg(T.jap + s * E + ge) * opening, CF(NC_CP + s, ga),
+                                      CF(NC_CP + s, gb), dvp, zfrt);
+        EF(NE_W + s, ge) = W_;
+        zw[s] = (s < 2 ? 1.0 : -1.0) * W_;
+        if (!is_finite(W_)) bits |= CB_WORLD_OPERATOR;
+        la[s] = CF(NC_LX + s, ga);
+        lb[s] = CF(NC_LX + s, gb);
+      }
+      EF(NE_G, ge) = K * ((zw[0] + zw[1]) + zw[2]);
+      const double dv0 = CF(NC_VX, ga) - CF(NC_VX, gb);
+      junction_mu(sW, la, lb, dv0, mu);
+      double lin[3], hm[3];
+      for (int s = 0; s < 3; ++s) {
+        lin[s] = EF(NE_W + s, ge) * dv0;
+        hm[s] = lin[s] * mu[s];
+        EF(NE_J + s, ge) = lin[s];
+        EF(NE_A + s, ge) =
+            cur[L.s[CB_JUNCTION_TRANSFERRED] + s * E + ge] + k.delta_dt * (EF(NE_JJ + s, ge) - lin[s]);
+      }
+      const double heat = 1e-3 * ((hm[0] + hm[1]) + hm[2]);
+      EF(NE_A + 3, ge) = cur[L.s[CB_JUNCTION_DISSIPATED] + ge] + k.delta_dt * (EF(NE_JD, ge) - heat);
+    }
+    __syncthreads();
+    // P4 (cells): the stage-0 remainder, the accumulators, the operator's diagonal.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      double send[3], recv[3], lc[3], mu[3];
+      gather(gi, NE_J, send, recv);
+      const double dv0 = CF(NC_VX, gi) - Vb;
+      for (int s = 0; s < 3; ++s) lc[s] = CF(NC_LX + s, gi);
+      patch_mu(sW, lc, dv0, mu);
+      double lm[3], patches[3], hm[3];
+      for (int s = 0; s < 3; ++s) {
+        lm[s] = CF(NC_WM + s, gi) * dv0;
+        patches[s] = lm[s];
+        hm[s] = lm[s] * mu[s];
+      }
+      double lch[NQ], hch[NQ];
+      if constexpr (NCH > 0) {
+        for (int q = 0; q < NCH; ++q) {
+          const int sp = __ldg(T.ch_species + q * C + gi);
+          lch[q] = CH(q, CH_W, gi) * dv0;
+          hch[q] = 1e-3 * lch[q] * mu[sp];
+          patches[sp] = patches[sp] + lch[q];
+        }
+      }
+      const double hmem = 1e-3 * ((hm[0] + hm[1]) + hm[2]);
+      for (int s = 0; s < 3; ++s) {
+        const double cells_lin = (recv[s] - send[s]) - patches[s];
+        const double k0n = CF(NC_KN + s, gi) - cells_lin;
+        const double n0 = cur[oN + s * C + gi];
+        CF(NC_A + s, gi) = n0 + k.delta_dt * k0n;
+        CF(NC_K1 + s, gi) = n0 + k.gamma_dt * k0n;
+        CF(NC_A + 3 + s, gi) = cur[L.s[CB_MEMBRANE_TRANSFERRED] + s * C + gi] +
+                               k.delta_dt * (CF(NC_JM + s, gi) - lm[s]);
+        outlin0[s] += patches[s];
+      }
+      CF(NC_A + 6, gi) = cur[L.s[CB_MEMBRANE_DISSIPATED] + gi] + k.delta_dt * (CF(NC_R, gi) - hmem);
+      CF(NC_A + 7, gi) = cur[L.s[CB_PUMP_CYCLES] + gi] + k.delta_dt * CF(NC_R + 1, gi);
+      CF(NC_A + 8, gi) = cur[L.s[CB_PUMP_DISSIPATED] + gi] + k.delta_dt * CF(NC_R + 2, gi);
+      CF(NC_A + 9, gi) = cur[L.s[CB_METABOLIC_WORK] + gi] + k.delta_dt * CF(NC_R + 3, gi);
+      if constexpr (NCH > 0) {
+        for (int q = 0; q < NCH; ++q) {
+          CH(q, CH_AT, gi) = cur[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi] +
+                             k.delta_dt * (CH(q, CH_J, gi) - lch[q]);
+          CH(q, CH_AD, gi) = cur[L.s[CB_CHANNEL_DISSIPATED] + q * C + gi] +
+                             k.delta_dt * (CH(q, CH_JD, gi) - hch[q]);
+        }
+      }
+      // M_ii = C_i + gamma dt (G_patch + sum of its junctions' G), the junctions as the
+      // Laplacian's scatter orders them (senders, then receivers).
+      double gs = 0.0, gr = 0.0;
+      for (int a = __ldg(T.adj_ptr + gi); a < __ldg(T.adj_ptr + gi + 1); ++a) {
+        const int code = __ldg(T.adj_idx + a);
+        const double g = EF(NE_G, e0 + (code >> 1));
+        if (code & 1) gr += g;
+        else gs += g;
+      }
+      const double cap = 1.0 / __ldg(T.icap + gi);
+      const double gp = CF(NC_GP, gi);
+      const double mii = cap + gdt * (gp + (gs + gr));
+      CF(NC_MD, gi) = mii;
+      CF(NC_MB, gi) = (-cap) + gdt * (-gp);
+      if (!(mii > 0.0)) bits |= CB_WORLD_OPERATOR;
+      const double sc = 1.0 / sqrt(mii > 0.0 ? mii : 1.0);
+      CF(NC_S, gi) = sc;
+      lval[D.colp[__ldg(D.rank + gi)]] = (mii * sc) * sc;
+    }
+    __syncthreads();
+    // E3 (junctions): the operator's off-diagonal entries, scaled (row then column).
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      const long long ga = c0 + __ldg(T.snd + ge), gb = c0 + __ldg(T.rcv + ge);
+      const int ra = __ldg(D.rank + ga), rb = __ldg(D.rank + gb);
+      const double m = 0.0 + gdt * (-EF(NE_G, ge));
+      const double s_row = ra > rb ? CF(NC_S, ga) : CF(NC_S, gb);
+      const double s_col = ra > rb ? CF(NC_S, gb) : CF(NC_S, ga);
+      lval[__ldg(D.edge_pos + ge)] = (m * s_row) * s_col;
+    }
+    __syncthreads();
+    if (factor()) bits |= CB_WORLD_OPERATOR;
+    // Two stages: i = 1 (known K1) and i = 2 (known: the accumulators).
+    double inflow1[3] = {0, 0, 0}, outlin1[3] = {0, 0, 0}, outlin2[3] = {0, 0, 0};
+    double plate2 = 0.0;
+    for (int st = 1; st <= 2; ++st) {
+      const int kf = st == 1 ? NC_K1 : NC_A;
+      // Charges and the scaled right-hand side (charge - M held) s.
+      for (int i = tid; i < nc; i += BLOCK) {
+        const long long gi = c0 + i;
+        const double q = __ldg(T.q0 + gi) +
+                         K * ((CF(kf, gi) + CF(kf + 1, gi)) + (-CF(kf + 2, gi)));
+        CF(NC_Y, __ldg(D.rank + gi)) = (q - CF(NC_MB, gi) * Vb) * CF(NC_S, gi);
+      }
+      __syncthreads();
+      solve();
+      for (int i = tid; i < nc; i += BLOCK) {
+        const long long gi = c0 + i;
+        CF(NC_VX, gi) = CF(NC_X, __ldg(D.rank + gi)) * CF(NC_S, gi);
+      }
+      __syncthreads();
+      // Junctions: the linear flux at the stage potentials, the stage gate.
+      const double frac_dt = st == 1 ? k.frac1_dt : k.frac2_dt;
+      for (int e = tid; e < ne; e += BLOCK) {
+        const long long ge = e0 + e;
+        const long long ga = c0 + __ldg(T.snd + ge), gb = c0 + __ldg(T.rcv + ge);
+        const double dv = CF(NC_VX, ga) - CF(NC_VX, gb);
+        for (int s = 0; s < 3; ++s) EF(NE_J + s, ge) = EF(NE_W + s, ge) * dv;
+        const double thr = __ldg(T.thr + ge), mn = __ldg(T.jmin + ge);
+        double t1, r1;
+        junction_law(dv, thr, mn, t1, r1);
+        const double g = advance_gate<false>(cur[oG + ge], EF(NE_T0, ge), 1.0 / EF(NE_R0, ge), t1,
+                                             1.0 / r1, frac_dt);
+        EF(NE_GX, ge) = g;
+        if (!gate_domain(g, dv, thr, mn, jctl[ge])) bits |= CB_WORLD_GATE_DOMAIN;
+      }
+      __syncthreads();
+      // Cells: the residual, the drift's amounts, the stage state, its gates, its own rates.
+      for (int i = tid; i < nc; i += BLOCK) {
+        const long long gi = c0 + i;
+        const double q = __ldg(T.q0 + gi) +
+                         K * ((CF(kf, gi) + CF(kf + 1, gi)) + (-CF(kf + 2, gi)));
+        double product;
+        const double r = row_residual(gi, q, product);
+        const double V = CF(NC_VX, gi);
+        if (!is_finite(V) || !(fabs(r) <= kChargeAtol + kChargeRtol * fmax(fabs(q), fabs(product))))
+          bits |= CB_WORLD_RESIDUAL;
+        double send[3], recv[3], patches[3], n[3];
+        gather(gi, NE_J, send, recv);
+        const double dv = V - Vb;
+        for (int s = 0; s < 3; ++s) patches[s] = CF(NC_WM + s, gi) * dv;
+        if constexpr (NCH > 0) {
+          for (int q_ = 0; q_ < NCH; ++q_) {
+            const int sp = __ldg(T.ch_species + q_ * C + gi);
+            patches[sp] = patches[sp] + CH(q_, CH_W, gi) * dv;
+          }
+        }
+        for (int s = 0; s < 3; ++s) {
+          const double d = (recv[s] - send[s]) - patches[s];
+          n[s] = CF(kf + s, gi) + k.gamma_dt * d;  // the stage state's amounts
+          if (st == 1) {
+            CF(NC_KN + s, gi) = d;
+            outlin1[s] += patches[s];
+          } else {
+            CF(NC_A + s, gi) = n[s];  // the step's new amounts
+            outlin2[s] += patches[s];
+          }
+        }
+        if (st == 2) plate2 += -(K * ((n[0] + n[1]) + (-n[2])));
+        const double ivol = __ldg(T.ivol + gi);
+        double c[3], lc[3];
+        for (int s = 0; s < 3; ++s) {
+          c[s] = (__ldg(T.ref + s * C + gi) + n[s]) * ivol;
+          lc[s] = log(c[s]);
+          CF(NC_CX + s, gi) = c[s];
+          CF(NC_LX + s, gi) = lc[s];
+        }
+        // Channel gates: the exponential update from the start to this stage's potential.
+        if constexpr (NCH > 0) {
+          for (int q_ = 0; q_ < NCH; ++q_) {
+            const int code = __ldg(T.ch_code + q_ * C + gi);
+            double t[2], tau[2];
+            channel_kinetics<false>(code, dv, t, tau);
+            if (!channel_kinetics_ok(dv, t, tau)) bits |= CB_WORLD_CHANNEL_DOMAIN;
+            for (int r2 = 0; r2 < 2; ++r2) {
+              const double g0 = cur[oH + (r2 * NCH + q_) * C + gi];
+              CH(q_, CH_G + r2, gi) =
+                  (r2 == 1 && code == kHhKn4)
+                      ? g0
+                      : advance_gate<false>(g0, CH(q_, CH_T0 + r2, gi), CH(q_, CH_TAU0 + r2, gi),
+                                            t[r2], tau[r2], frac_dt);
+            }
+          }
+        }
+        // The linear parts' heat at the stage state and potential.
+        double mu[3];
+        patch_mu(sW, lc, dv, mu);
+        double lm[3], hm[3];
+        for (int s = 0; s < 3; ++s) {
+          lm[s] = CF(NC_WM + s, gi) * dv;
+          hm[s] = lm[s] * mu[s];
+        }
+        const double hmem = 1e-3 * ((hm[0] + hm[1]) + hm[2]);
+        double lch[NQ], hch[NQ];
+        if constexpr (NCH > 0) {
+          for (int q_ = 0; q_ < NCH; ++q_) {
+            const int sp = __ldg(T.ch_species + q_ * C + gi);
+            lch[q_] = CH(q_, CH_W, gi) * dv;
+            hch[q_] = 1e-3 * lch[q_] * mu[sp];
+          }
+        }
+        if (st == 1) {
+          // The stage-1 whole rates (own parts; the junctions' after their pass), the remainder
+          // k1 = whole - linear and the drift d1 into the accumulators, as _combine orders them.
+          const double pctl = pctlp[gi];
+          const double ldc = pctl > 0.0 ? __ldg(T.logpcap + gi) + log(pctl) : 0.0;
+          double jm[3], ex[3], r4[4], chj[NQ], chd[NQ];
+          bits |= own_rates<NCH>(T, sW, gi, c, lc, V, cs + (long long)(NC_CH + CH_G) * C + gi,
+                                 (long long)kN2ChFields * C, C, mctl[gi], pctl, ldc,
+                                 chctl0 + gi, jm, ex, r4, chj, chd);
+          for (int s = 0; s < 3; ++s) {
+            CF(NC_JM + s, gi) = jm[s];
+            CF(NC_EX + s, gi) = ex[s];
+            inflow1[s] += jm[s] + ex[s];
+            CF(NC_A + 3 + s, gi) = (CF(NC_A + 3 + s, gi) + k.omdelta_dt * (jm[s] - lm[s])) +
+                                   w1 * lm[s];
+          }
+          CF(NC_A + 6, gi) = (CF(NC_A + 6, gi) + k.omdelta_dt * (r4[0] - hmem)) + w1 * hmem;
+          CF(NC_A + 7, gi) = (CF(NC_A + 7, gi) + k.omdelta_dt * r4[1]) + w1 * 0.0;
+          CF(NC_A + 8, gi) = (CF(NC_A + 8, gi) + k.omdelta_dt * r4[2]) + w1 * 0.0;
+          CF(NC_A + 9, gi) = (CF(NC_A + 9, gi) + k.omdelta_dt * r4[3]) + w1 * 0.0;
+          if constexpr (NCH > 0) {
+            for (int q_ = 0; q_ < NCH; ++q_) {
+              CH(q_, CH_AT, gi) = (CH(q_, CH_AT, gi) + k.omdelta_dt * (chj[q_] - lch[q_])) +
+                                  w1 * lch[q_];
+              CH(q_, CH_AD, gi) = (CH(q_, CH_AD, gi) + k.omdelta_dt * (chd[q_] - hch[q_])) +
+                                  w1 * hch[q_];
+            }
+          }
+        } else {
+          // The new state's ledgers: the accumulators plus gamma dt of the stage-2 drift.
+          for (int s = 0; s < 3; ++s)
+            CF(NC_A + 3 + s, gi) = CF(NC_A + 3 + s, gi) + k.gamma_dt * lm[s];
+          CF(NC_A + 6, gi) = CF(NC_A + 6, gi) + k.gamma_dt * hmem;
+          CF(NC_A + 7, gi) = CF(NC_A + 7, gi) + k.gamma_dt * 0.0;
+          CF(NC_A + 8, gi) = CF(NC_A + 8, gi) + k.gamma_dt * 0.0;
+          CF(NC_A + 9, gi) = CF(NC_A + 9, gi) + k.gamma_dt * 0.0;
+          bool ok = true;
+          for (int f = 0; f < 10; ++f) ok = ok && is_finite(CF(NC_A + f, gi));
+          for (int s = 0; s < 3; ++s) ok = ok && (__ldg(T.ref + s * C + gi) + n[s]) > 0.0;
+          if constexpr (NCH > 0) {
+            for (int q_ = 0; q_ < NCH; ++q_) {
+              CH(q_, CH_AT, gi) = CH(q_, CH_AT, gi) + k.gamma_dt * lch[q_];
+              CH(q_, CH_AD, gi) = CH(q_, CH_AD, gi) + k.gamma_dt * hch[q_];
+              ok = ok && is_finite(CH(q_, CH_AT, gi)) && is_finite(CH(q_, CH_AD, gi));
+              for (int r2 = 0; r2 < 2; ++r2) {
+                const double g = CH(q_, CH_G + r2, gi);
+                ok = ok && is_finite(g) && g >= 0.0 && g <= 1.0;
+              }
+            }
+          }
+          if (!ok) bits |= CB_WORLD_DOMAIN;
+        }
+      }
+      __syncthreads();
+      // Junctions: the linear part's heat at the stage; at stage 1 the whole flux too.
+      for (int e = tid; e < ne; e += BLOCK) {
+        const long long ge = e0 + e;
+        const long long ga = c0 + __ldg(T.snd + ge), gb = c0 + __ldg(T.rcv + ge);
+        double ca[3], cb[3], la[3], lb[3], mu[3], lin[3], hm[3];
+        for (int s = 0; s < 3; ++s) {
+          ca[s] = CF(NC_CX + s, ga);
+          cb[s] = CF(NC_CX + s, gb);
+          la[s] = CF(NC_LX + s, ga);
+          lb[s] = CF(NC_LX + s, gb);
+        }
+        const double dv = CF(NC_VX, ga) - CF(NC_VX, gb);
+        junction_mu(sW, la, lb, dv, mu);
+        for (int s = 0; s < 3; ++s) {
+          lin[s] = EF(NE_W + s, ge) * dv;
+          hm[s] = lin[s] * mu[s];
+        }
+        const double heat = 1e-3 * ((hm[0] + hm[1]) + hm[2]);
+        const double g = EF(NE_GX, ge), jc = jctl[ge];
+        if (st == 1) {
+          double jj[3], jd;
+          bits |= junction_flux(T, sW, ge, ca, cb, la, lb, dv, jc * g, jj, jd);
+          if (!gate_domain(g, dv, __ldg(T.thr + ge), __ldg(T.jmin + ge), jc))
+            bits |= CB_WORLD_GATE_DOMAIN;
+          for (int s = 0; s < 3; ++s) {
+            EF(NE_J + s, ge) = jj[s];
+            EF(NE_A + s, ge) = (EF(NE_A + s, ge) + k.omdelta_dt * (jj[s] - lin[s])) + w1 * lin[s];
+          }
+          EF(NE_A + 3, ge) = (EF(NE_A + 3, ge) + k.omdelta_dt * (jd - heat)) + w1 * heat;
+        } else {
+          bool ok = true;
+          for (int s = 0; s < 3; ++s) {
+            EF(NE_A + s, ge) = EF(NE_A + s, ge) + k.gamma_dt * lin[s];
+            ok = ok && is_finite(EF(NE_A + s, ge));
+          }
+          EF(NE_A + 3, ge) = EF(NE_A + 3, ge) + k.gamma_dt * heat;
+          ok = ok && is_finite(EF(NE_A + 3, ge)) && is_finite(g) && g >= __ldg(T.jmin + ge) &&
+               g <= 1.0;
+          if (!ok) bits |= CB_WORLD_DOMAIN;
+        }
+      }
+      __syncthreads();
+      if (st == 1) {
+        // Cells: the stage-1 whole amount rate (own + junctions) less the drift, into the
+        // accumulators: A += (1 - delta) dt k1 + (1 - gamma) dt d1.
+        for (int i = tid; i < nc; i += BLOCK) {
+          const long long gi = c0 + i;
+          double send[3], recv[3];
+          gather(gi, NE_J, send, recv);
+          for (int s = 0; s < 3; ++s) {
+            const double whole =
+                ((-CF(NC_JM + s, gi) + (-send[s])) + recv[s]) - CF(NC_EX + s, gi);
+            const double d1 = CF(NC_KN + s, gi);
+            CF(NC_A + s, gi) = (CF(NC_A + s, gi) + k.omdelta_dt * (whole - d1)) + w1 * d1;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // World sums: the bath's inflow terms of both stages' rates and drifts, the end plate.
+    double v[14] = {inflow0[0], inflow0[1], inflow0[2], outlin0[0], outlin0[1], outlin0[2],
+                    inflow1[0], inflow1[1], inflow1[2], outlin1[0], outlin1[1], outlin1[2],
+                    plate0, plate2};
+    block_sum<BLOCK, 14>(v, sRed);
+    double v2[3] = {outlin2[0], outlin2[1], outlin2[2]};
+    block_sum<BLOCK, 3>(v2, sRed);
+    double res2[3], applied[3];
+    // The bath's supply rates: a whole stage rate supplies -inflow; the routes' linear parts
+    // carry +outlin out through the patches, so a remainder supplies -inflow + outlin and a
+    // drift -outlin.
+    for (int s = 0; s < 3; ++s) {
+      const double k0r = -v[s] + v[3 + s];
+      const double k1r = -v[6 + s] + v[9 + s];
+      const double d1r = -v[9 + s];
+      const double d2r = -v2[s];
+      res2[s] = (((res[s] + k.delta_dt * k0r) + k.omdelta_dt * k1r) + w1 * d1r) + k.gamma_dt * d2r;
+      applied[s] = ((0.0 + k.delta * k0r) + k.omdelta * k1r) +
+                   ((0.0 + (1.0 - (1.0 - 1.0 / sqrt(2.0))) * d1r) + (1.0 - 1.0 / sqrt(2.0)) * d2r);
+    }
+    const double electrode = v[13] - v[12];
+    const double ec2 = ec + electrode;
+    const double rw2 = rw + 1e-3 * ((sW[WC_MUB] * (k.dt * applied[0]) +
+                                     sW[WC_MUB + 1] * (k.dt * applied[1])) +
+                                    sW[WC_MUB + 2] * (k.dt * applied[2]));
+    const double ew2 = ew + (1e12 * Vb) * electrode;
+    if (!(is_finite(res2[0]) && is_finite(res2[1]) && is_finite(res2[2]) && is_finite(ec2) &&
+          is_finite(rw2) && is_finite(ew2)))
+      bits |= CB_WORLD_DOMAIN;
+    if (bits) atomicOr(&sBits, bits);
+    __syncthreads();
+    const uint32_t world_bits = sBits;
+    if (world_bits) {
+      refused = world_bits;
+      break;
+    }
+    // Commit the accepted state.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      for (int s = 0; s < 3; ++s) {
+        state_out[oN + s * C + gi] = CF(NC_A + s, gi);
+        state_out[L.s[CB_MEMBRANE_TRANSFERRED] + s * C + gi] = CF(NC_A + 3 + s, gi);
+      }
+      state_out[L.s[CB_MEMBRANE_DISSIPATED] + gi] = CF(NC_A + 6, gi);
+      state_out[L.s[CB_PUMP_CYCLES] + gi] = CF(NC_A + 7, gi);
+      state_out[L.s[CB_PUMP_DISSIPATED] + gi] = CF(NC_A + 8, gi);
+      state_out[L.s[CB_METABOLIC_WORK] + gi] = CF(NC_A + 9, gi);
+      if constexpr (NCH > 0) {
+        for (int q = 0; q < NCH; ++q) {
+          state_out[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi] = CH(q, CH_AT, gi);
+          state_out[L.s[CB_CHANNEL_DISSIPATED] + q * C + gi] = CH(q, CH_AD, gi);
+          for (int r = 0; r < 2; ++r)
+            state_out[oH + (r * NCH + q) * C + gi] = CH(q, CH_G + r, gi);
+        }
+      }
+    }
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      for (int s = 0; s < 3; ++s)
+        state_out[L.s[CB_JUNCTION_TRANSFERRED] + s * E + ge] = EF(NE_A + s, ge);
+      state_out[L.s[CB_JUNCTION_DISSIPATED] + ge] = EF(NE_A + 3, ge);
+      state_out[oG + ge] = EF(NE_GX, ge);
+    }
+    for (int s = 0; s < 3; ++s) res[s] = res2[s];
+    ec = ec2;
+    rw = rw2;
+    ew = ew2;
+    ++taken;
+    cur = state_out;
+    __syncthreads();
+  }
+  // A world refused at its first step keeps its input state.
+  if (taken == 0 && state_in != state_out) {
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      for (int f = CB_AMOUNT_INCREMENT; f <= CB_METABOLIC_WORK; ++f) {
+        const int reps = (f <= CB_MEMBRANE_TRANSFERRED) ? 3 : 1;
+        for (int s = 0; s < reps; ++s)
+          state_out[L.s[f] + s * C + gi] = state_in[L.s[f] + s * C + gi];
+      }
+      for (int f = CB_CHANNEL_GATE; f <= CB_CHANNEL_DISSIPATED; ++f) {
+        const int reps = (f == CB_CHANNEL_GATE) ? 2 * NCH : NCH;
+        for (int s = 0; s < reps; ++s)
+          state_out[L.s[f] + s * C + gi] = state_in[L.s[f] + s * C + gi];
+      }
+    }
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      for (int f = CB_JUNCTION_TRANSFERRED; f <= CB_JUNCTION_GATE; ++f) {
+        const int reps = (f == CB_JUNCTION_TRANSFERRED) ? 3 : 1;
+        for (int s = 0; s < reps; ++s)
+          state_out[L.s[f] + s * E + ge] = state_in[L.s[f] + s * E + ge];
+      }
+    }
+  }
+  if (tid == 0) {
+    for (int s = 0; s < 3; ++s) state_out[L.s[CB_RESERVOIR_SUPPLIED] + s * W + w] = res[s];
+    state_out[L.s[CB_ELECTRODE_CHARGE] + w] = ec;
+    state_out[L.s[CB_RESERVOIR_WORK] + w] = rw;
+    state_out[L.s[CB_ELECTRODE_WORK] + w] = ew;
+    world_status[w] = refused;
+    if (accepted_steps) accepted_steps[w] = taken;
+  }
+}
+
+constexpr int kN2Block = 256;
+
+// ---------------------------------------------------------------------------------------------
+// Host: the sparse factor's plan (numerics/sparse_cholesky.py's bind, restated): a
+// minimum-degree order (least current degree, ties by the least original degree, then the
+// smallest index; the eliminated node's neighbours form a clique), the filled pattern by the
+// elimination tree's union rule, the tree's levels, each column's update list and the relative
+// positions of its update terms, and each junction's off-diagonal entry.
+
+struct WorldPlan {
+  std::vector<int> order, rank, colp, lrow, uk_ptr, uk_col, uk_pos, uk_rel, rel, level_cols,
+      level_ptr, edge_pos;
+};
+
+int plan_world(int n, const int *snd, const int *rcv, int ne, WorldPlan &p) {
+  std::vector<std::set<int>> adj(n);
+  for (int e = 0; e < ne; ++e) {
+    const int a = snd[e], b = rcv[e];
+    if (a == b) return fail(CB_ERR_LAYOUT, "N2: a junction joins a cell to itself");
+    if (!adj[a].insert(b).second)
+      return fail(CB_ERR_LAYOUT, "N2: two junctions join the same pair of cells");
+    adj[b].insert(a);
+  }
+  // Minimum degree.
+  std::vector<int> original(n);
+  for (int i = 0; i < n; ++i) original[i] = (int)adj[i].size();
+  std::vector<std::set<int>> g = adj;
+  using Key = std::tuple<int, int, int>;
+  std::priority_queue<Key, std::vector<Key>, std::greater<Key>> heap;
+  for (int i = 0; i < n; ++i) heap.push(Key(original[i], original[i], i));
+  std::vector<char> alive(n, 1);
+  p.order.clear();
+  while (!heap.empty()) {
+    const auto [degree, orig, node] = heap.top();
+    heap.pop();
+    if (!alive[node] || degree != (int)g[node].size()) continue;
+    alive[node] = 0;
+    p.order.push_back(node);
+    const std::set<int> nb = g[node];
+    for (int a : nb) {
+      g[a].erase(node);
+      for (int b : nb)
+        if (b != a) g[a].insert(b);
+      heap.push(Key((int)g[a].size(), original[a], a));
+    }
+    g[node].clear();
+  }
+  p.rank.assign(n, 0);
+  for (int r = 0; r < n; ++r) p.rank[p.order[r]] = r;
+  // Symbolic factorisation (union rule) and the elimination tree.
+  std::vector<std::set<int>> below(n);
+  for (int i = 0; i < n; ++i) {
+    const int r = p.rank[i];
+    for (int a : adj[i])
+      if (p.rank[a] > r) below[r].insert(p.rank[a]);
+  }
+  std::vector<int> parent(n, -1), level(n, 0);
+  for (int kk = 0; kk < n; ++kk) {
+    if (!below[kk].empty()) {
+      const int par = *below[kk].begin();
+      parent[kk] = par;
+      for (int r : below[kk])
+        if (r != par) below[par].insert(r);
+    }
+  }
+  for (int kk = 0; kk < n; ++kk)
+    if (parent[kk] >= 0) level[parent[kk]] = std::max(level[parent[kk]], level[kk] + 1);
+  p.colp.assign(n + 1, 0);
+  for (int kk = 0; kk < n; ++kk) p.colp[kk + 1] = p.colp[kk] + 1 + (int)below[kk].size();
+  p.lrow.assign(p.colp[n], 0);
+  for (int kk = 0; kk < n; ++kk) {
+    int f = p.colp[kk];
+    p.lrow[f++] = kk;
+    for (int r : below[kk]) p.lrow[f++] = r;
+  }
+  // Update lists: for column j, every k < j whose column holds row j, ascending k; the
+  // relative positions in column j of column k's rows at or below j.
+  std::vector<std::vector<std::pair<int, int>>> rowlist(n);  // j -> (k, entry of L_jk)
+  for (int kk = 0; kk < n; ++kk)
+    for (int f = p.colp[kk] + 1; f < p.colp[kk + 1]; ++f) rowlist[p.lrow[f]].push_back({kk, f});
+  std::vector<int> where(n, -1);
+  p.uk_ptr.assign(n + 1, 0);
+  p.uk_col.clear();
+  p.uk_pos.clear();
+  p.uk_rel.clear();
+  p.rel.clear();
+  for (int j = 0; j < n; ++j) {
+    for (int f = p.colp[j]; f < p.colp[j + 1]; ++f) where[p.lrow[f]] = f - p.colp[j];
+    for (const auto &[kk, f] : rowlist[j]) {
+      p.uk_col.push_back(kk);
+      p.uk_pos.push_back(f);
+      p.uk_rel.push_back((int)p.rel.size());
+      for (int t = f; t < p.colp[kk + 1]; ++t) {
+        const int off = where[p.lrow[t]];
+        if (off < 0) return fail(CB_ERR_LAYOUT, "N2: inconsistent factor pattern");
+        p.rel.push_back(off);
+      }
+    }
+    for (int f = p.colp[j]; f < p.colp[j + 1]; ++f) where[p.lrow[f]] = -1;
+    p.uk_ptr[j + 1] = (int)p.uk_col.size();
+  }
+  // Levels.
+  const int levels = n ? 1 + *std::max_element(level.begin(), level.end()) : 0;
+  p.level_ptr.assign(levels + 1, 0);
+  for (int kk = 0; kk < n; ++kk) p.level_ptr[level[kk] + 1]++;
+  for (int l = 0; l < levels; ++l) p.level_ptr[l + 1] += p.level_ptr[l];
+  p.level_cols.assign(n, 0);
+  std::vector<int> fill(p.level_ptr.begin(), p.level_ptr.end() - 1);
+  for (int kk = 0; kk < n; ++kk) p.level_cols[fill[level[kk]]++] = kk;
+  // Junctions' off-diagonal entries (row = the later rank, column = the earlier).
+  p.edge_pos.assign(ne, 0);
+  for (int e = 0; e < ne; ++e) {
+    const int ra = p.rank[snd[e]], rb = p.rank[rcv[e]];
+    const int col = std::min(ra, rb), row = std::max(ra, rb);
+    int found = -1;
+    for (int f = p.colp[col]; f < p.colp[col + 1]; ++f)
+      if (p.lrow[f] == row) found = f;
+    if (found < 0) return fail(CB_ERR_LAYOUT, "N2: junction outside the factor pattern");
+    p.edge_pos[e] = found;
+  }
+  return CB_OK;
+}
+
+template <typename V>
+int upload_vec(N2Plan *plan, const std::vector<V> &host, V **dst) {
+  void *ptr = nullptr;
+  const size_t bytes = std::max<size_t>(host.size() * sizeof(V), 16);
+  cudaError_t e = cudaMalloc(&ptr, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (N2 plan)");
+  plan->owned.push_back(ptr);
+  if (!host.empty()) {
+    e = cudaMemcpy(ptr, host.data(), host.size() * sizeof(V), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy (N2 plan)");
+  }
+  *dst = static_cast<V *>(ptr);
+  return CB_OK;
+}
+
+int build_plan(cb_tissue *t) {
+  if (t->n2) return CB_OK;
+  auto *plan = new N2Plan();
+  const int W = t->W;
+  const long long C = t->C, E = t->E;
+  std::vector<int> rank(C), colp(C + 1, 0), lrow, uk_ptr(C + 1, 0), uk_col, uk_pos, uk_rel, rel,
+      lv_world(W + 1, 0), lv_ptr{0}, lv_cols(C), edge_pos(E);
+  long long fbase = 0, ubase = 0, rbase = 0;
+  int rc = CB_OK;
+  for (int w = 0; w < W && !rc; ++w) {
+    const long long c0 = t->h_cell_offset[w], n = t->h_cell_offset[w + 1] - c0;
+    const long long e0 = t->h_edge_offset[w], ne = t->h_edge_offset[w + 1] - e0;
+    WorldPlan p;
+    rc = plan_world((int)n, t->h_snd.data() + e0, t->h_rcv.data() + e0, (int)ne, p);
+    if (rc) break;
+    if (fbase + p.colp[n] >= (1LL << 31) || ubase + (long long)p.uk_col.size() >= (1LL << 31) ||
+        rbase + (long long)p.rel.size() >= (1LL << 31)) {
+      rc = fail(CB_ERR_UNSUPPORTED, "N2: the batch's factor plan exceeds 2^31 entries");
+      break;
+    }
+    for (long long i = 0; i < n; ++i) rank[c0 + i] = (int)(c0 + p.rank[i]);
+    for (long long r = 0; r < n; ++r) {
+      colp[c0 + r] = (int)(fbase + p.colp[r]);
+      uk_ptr[c0 + r] = (int)(ubase + p.uk_ptr[r]);
+    }
+    for (int r : p.lrow) lrow.push_back((int)(c0 + r));
+    for (size_t u = 0; u < p.uk_col.size(); ++u) {
+      uk_col.push_back((int)(c0 + p.uk_col[u]));
+      uk_pos.push_back((int)(fbase + p.uk_pos[u]));
+      uk_rel.push_back((int)(rbase + p.uk_rel[u]));
+    }
+    rel.insert(rel.end(), p.rel.begin(), p.rel.end());
+    lv_world[w] = (int)lv_ptr.size() - 1;
+    for (size_t l = 0; l + 1 < p.level_ptr.size(); ++l)
+      lv_ptr.push_back(lv_ptr.back() + (p.level_ptr[l + 1] - p.level_ptr[l]));
+    for (long long r = 0; r < n; ++r) lv_cols[c0 + r] = (int)(c0 + p.level_cols[r]);
+    for (long long e = 0; e < ne; ++e) edge_pos[e0 + e] = (int)(fbase + p.edge_pos[e]);
+    plan->max_level = std::max(plan->max_level, (int)p.level_ptr.size() - 1);
+    fbase += p.colp[n];
+    ubase += (long long)p.uk_col.size();
+    rbase += (long long)p.rel.size();
+  }
+  if (rc) {
+    delete plan;
+    return rc;
+  }
+  lv_world[W] = (int)lv_ptr.size() - 1;
+  colp[C] = (int)fbase;
+  uk_ptr[C] = (int)ubase;
+  plan->factor_entries = fbase;
+  plan->update_terms = rbase;
+  plan->levels = (int)lv_ptr.size() - 1;
+  N2Dev &d = plan->d;
+  if (!rc) rc = upload_vec(plan, rank, &d.rank);
+  if (!rc) rc = upload_vec(plan, colp, &d.colp);
+  if (!rc) rc = upload_vec(plan, lrow, &d.lrow);
+  if (!rc) rc = upload_vec(plan, uk_ptr, &d.uk_ptr);
+  if (!rc) rc = upload_vec(plan, uk_col, &d.uk_col);
+  if (!rc) rc = upload_vec(plan, uk_pos, &d.uk_pos);
+  if (!rc) rc = upload_vec(plan, uk_rel, &d.uk_rel);
+  if (!rc) rc = upload_vec(plan, rel, &d.rel);
+  if (!rc) rc = upload_vec(plan, lv_world, &d.lv_world);
+  if (!rc) rc = upload_vec(plan, lv_ptr, &d.lv_ptr);
+  if (!rc) rc = upload_vec(plan, lv_cols, &d.lv_cols);
+  if (!rc) rc = upload_vec(plan, edge_pos, &d.edge_pos);
+  if (!rc) rc = upload_vec(plan, std::vector<double>(fbase), &d.lval);
+  if (!rc)
+    rc = upload_vec(plan, std::vector<double>((size_t)n2_cell_fields(t->t.nch) * C), &d.cs);
+  if (!rc) rc = upload_vec(plan, std::vector<double>((size_t)NE_FIELDS * std::max(E, 1LL)), &d.es);
+  if (rc) {
+    for (void *ptr : plan->owned) cudaFree(ptr);
+    delete plan;
+    return rc;
+  }
+  t->n2 = plan;
+  return CB_OK;
+}
+
+template <int NCH>
+int launch_n2(cb_tissue *t, const double *in, double *out, const double *control,
+              const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
+              cudaStream_t stream) {
+  n2_kernel<kN2Block, NCH><<<t->W, kN2Block, 0, stream>>>(t->t, t->layout, t->n2->d, in, out,
+                                                          control, k, n_steps, status, taken);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "n2 launch");
+  return CB_OK;
+}
+
+}  // namespace
+
+namespace cbk {
+
+int n2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
+            const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
+            cudaStream_t stream) {
+  int rc = build_plan(t);
+  if (rc) return rc;
+  const StepCoef k = step_coef(dt);
+  if (t->t.nch == 2)
+    return launch_n2<2>(t, state_in, state_out, control, k, n_steps, world_status,
+                        accepted_steps, stream);
+  if (t->t.nch == 0)
+    return launch_n2<0>(t, state_in, state_out, control, k, n_steps, world_status,
+                        accepted_steps, stream);
+  return fail(CB_ERR_UNSUPPORTED, "channel slots must be 0 or 2");
+}
+
+void n2_release(cb_tissue *t) {
+  if (!t->n2) return;
+  for (void *ptr : t->n2->owned) cudaFree(ptr);
+  delete t->n2;
+  t->n2 = nullptr;
+}
+
+}  // namespace cbk

@@ -1144,6 +1144,10 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
     snd[e] = d->sender[e];
     rcv[e] = d->receiver[e];
   }
+  t->h_cell_offset.assign(d->cell_offset, d->cell_offset + W + 1);
+  t->h_edge_offset.assign(d->edge_offset, d->edge_offset + W + 1);
+  t->h_snd = snd;
+  t->h_rcv = rcv;
   auto vec = [](const double *p, long long n) { return std::vector<double>(p, p + n); };
   int rc = CB_OK;
   Tissue &T = t->t;
@@ -1289,6 +1293,7 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
 void cb_free(cb_tissue *t) {
   if (!t) return;
   cudaSetDevice(t->device);
+  n2_release(t);
   for (void *p : t->owned) cudaFree(p);
   if (t->h_state) cudaFree(t->h_state);
   if (t->h_control) cudaFree(t->h_control);
@@ -1316,6 +1321,14 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
             void *stream) {
   if (!t || !state_in || !state_out || !control || !world_status)
     return fail(CB_ERR_ARGUMENT, "null argument");
+  if (method == CB_METHOD_N2) {
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
+    if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
+    cudaError_t ce = cudaSetDevice(t->device);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+    return n2_step(t, state_in, state_out, dt, control, n_steps, world_status, accepted_steps,
+                   static_cast<cudaStream_t>(stream));
+  }
   if (method != CB_METHOD_ARS222 && method != CB_METHOD_ARS222_MIXED)
     return fail(CB_ERR_UNSUPPORTED, "unknown step method");
   const bool mix = method == CB_METHOD_ARS222_MIXED;

@@ -53,6 +53,8 @@ typedef struct cb_tissue cb_tissue;
                                         or with non-finite kinetics (:848-858) */
 #define CB_WORLD_LEDGER_COTANGENT 256u /* cb_step_vjp: a ledger field's cotangent was not zero;
                                           the gradients leave out the ledgers' dependence */
+#define CB_WORLD_OPERATOR 512u     /* N2: the half-step prediction (non-positive concentration,
+                                      non-finite slopes) or the operator (a non-positive pivot) */
 
 /* Return codes. */
 #define CB_OK 0
@@ -139,6 +141,15 @@ enum cb_control_field {
  * near-zero Bernoulli series, concentrations, potentials, world sums and every state and ledger
  * accumulation in FP64. One-world-per-CTA kernel only. */
 #define CB_METHOD_ARS222_MIXED 1
+/* N2 (cells.solver.imex_ars222_implicit_conductances@1, models/surface_pump_v3.py:3547-3955 under
+ * an N2 ID): ARS(2,2,2) with every patch's, channel population's and junction's slope
+ * conductance dJ/d(dv), frozen at the step's half-way prediction (operator_time_conductances,
+ * :2961-3029), in the implicit operator C + gamma dt L beside the capacitors; the remainders
+ * J - W dv explicit; junction gates by their exponential update at the stages. The operator of
+ * each world is factored every step by a sparse Cholesky on its contact graph (a minimum-degree
+ * order and elimination-tree levels bound on the host at the first N2 step; left-looking by
+ * levels on the device, one CTA per world). FP64. */
+#define CB_METHOD_N2 2
 
 /*
  * Host symbolic bind (replaces initial_values' layout binding, surface_tissue.py:135-257 and
