@@ -47,6 +47,7 @@ ADJOINT_METRIC = "adjoint world-gradients/s"
 ADJOINT_UNIT = "world-gradients/s"
 METHOD = "cells.solver.imex_ars222_face_electromigration@1"
 METHOD_MIXED = "cells_b200.solver.imex_ars222_mixed_fp32@1"
+METHOD_N2 = "cells.solver.imex_ars222_implicit_conductances@1"
 
 
 def bytes_per_cell_step(batch):
@@ -83,6 +84,8 @@ def parse():
                     help="end-to-end host calls timed (default 3; adjoint: 1 gradient)")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
                     help="mixed: the ARS(2,2,2) step with FP32 rates and FP64 accumulation")
+    ap.add_argument("--method", choices=("ars222", "n2"), default="ars222",
+                    help="n2: slope conductances implicit, a sparse Cholesky per world per step")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the bind's launch configuration instead of the autotuner's")
     ap.add_argument("--no-graph", action="store_true",
@@ -545,7 +548,10 @@ def main():
 
     from cells_b200 import _lib as _lib_methods
 
-    method = (_lib_methods.METHOD_ARS222_MIXED if args.precision == "mixed"
+    if args.method == "n2" and args.precision == "mixed":
+        raise SystemExit("--method n2 runs in FP64 only")
+    method = (_lib_methods.METHOD_N2 if args.method == "n2"
+              else _lib_methods.METHOD_ARS222_MIXED if args.precision == "mixed"
               else _lib_methods.METHOD_ARS222)
     batch = build_batch(args, rank)
     tissue = Tissue(batch, device=local_rank)
@@ -562,7 +568,7 @@ def main():
             dist.barrier()
 
     tuned = None
-    if not args.no_autotune:
+    if not args.no_autotune and args.method != "n2":
         from cells_b200 import autotune
 
         best, timings = autotune.tune(tissue, state, control, args.dt,
@@ -661,8 +667,12 @@ def main():
             "data": "synthetic (seeded pump-leak tissues)",
             "config": {
                 "workload": workload_name(args),
-                "method": METHOD if args.precision == "fp64" else METHOD_MIXED, "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
-                "launch": dict(zip(("kernel", "block", "occupancy"), tissue.get_launch())),
+                "method": (METHOD_N2 if args.method == "n2" else
+                           METHOD if args.precision == "fp64" else METHOD_MIXED),
+                "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
+                "launch": ({"kernel": "n2 (one world per CTA)", "block": 256}
+                           if args.method == "n2" else
+                           dict(zip(("kernel", "block", "occupancy"), tissue.get_launch()))),
                 "autotune": tuned, "cuda_graph": graph is not None,
                 "cells_per_gpu": cells, "junctions_per_gpu": batch.edges,
                 "bytes_per_cell_step": bytes_per_cell_step(batch),

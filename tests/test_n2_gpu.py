@@ -104,9 +104,13 @@ def test_n2_fused_launch_equals_one_step_launches_and_keeps_ledgers(cuda):
     tissue.balances(st, out)
     torch.cuda.synchronize(dev)
     res = out.cpu().numpy().reshape(b.worlds, 8)
-    scale = np.max(np.abs(fused["amount_increment"]))
-    assert np.max(res[:, :3]) <= 1e-12 * scale
-    assert np.max(res[:, 3:5]) <= 1e-26
+    # The plain step's ledger bounds (tests/test_step_gpu.py): material against the reference
+    # amounts, electrode and global charge against the electrode charge, 1e-12 relative.
+    assert np.max(res[:, :3]) <= 1e-12 * np.max(np.abs(b.amount_reference))
+    ec = np.max(np.abs(fused["electrode_charge"]))
+    assert np.max(res[:, 3:5]) <= 1e-12 * ec
+    for k, f in ((5, "reservoir_work"), (7, "metabolic_work")):
+        assert np.max(res[:, k]) <= 1e-12 * np.max(np.abs(fused[f])), f
 
 
 def test_n2_refuses_a_world_and_keeps_its_state(cuda):
