@@ -67,6 +67,7 @@ struct N2Plan {
   std::vector<void *> owned;
   long long factor_entries = 0, update_terms = 0;
   int levels = 0, max_level = 0;
+  size_t smem_bytes = 0;  // dynamic shared memory of the shared-memory kernel; 0: global mode
 };
 
 }  // namespace cbk
@@ -281,12 +282,15 @@ __device__ __forceinline__ void patch_mu(const double *__restrict__ wc, const do
     mu[s] = wc[WC_RT] * (lc[s] - wc[WC_LOGCO + s]) + ((s < 2) ? kF * dv : (-kF) * dv);
 }
 
-template <int BLOCK, int NCH>
+// SHARED: the world's factor values and solve vectors in dynamic shared memory (when every
+// world's fit), else in the global scratch.
+template <int BLOCK, int NCH, bool SHARED>
 __global__ void __launch_bounds__(BLOCK)
     n2_kernel(const Tissue T, const Layout L, const N2Dev D, const double *state_in,
               double *state_out, const double *__restrict__ control, const StepCoef k,
               int n_steps, uint32_t *__restrict__ world_status,
               int32_t *__restrict__ accepted_steps) {
+  extern __shared__ double n2_smem[];
   constexpr int NQ = NCH > 0 ? NCH : 1;
   __shared__ double sW[WC_STRIDE];
   __shared__ double sRed[(BLOCK / 32) * 16];
@@ -301,7 +305,13 @@ __global__ void __launch_bounds__(BLOCK)
   if (tid == 0) sBits = 0u;
   double *cs = D.cs;
   double *es = D.es;
-  double *lval = D.lval;
+  // Factor values and solve vectors, addressed by global factor entry / global position.
+  const int fbase = D.colp[T.cell_offset[blockIdx.x]];
+  const int fcount = D.colp[T.cell_offset[blockIdx.x + 1]] - fbase;
+  double *lval = SHARED ? n2_smem - fbase : D.lval;
+  double *Yv = SHARED ? n2_smem + fcount - T.cell_offset[blockIdx.x] : cs + (long long)NC_Y * T.C;
+  double *Xv = SHARED ? Yv + (T.cell_offset[blockIdx.x + 1] - T.cell_offset[blockIdx.x])
+                      : cs + (long long)NC_X * T.C;
   const long long oN = L.s[CB_AMOUNT_INCREMENT], oG = L.s[CB_JUNCTION_GATE];
   const long long oH = L.s[CB_CHANNEL_GATE];
   const double *mctl = control + L.c[CB_CONTROL_MEMBRANE];
@@ -329,57 +339,118 @@ __global__ void __launch_bounds__(BLOCK)
   int taken = 0;
   uint32_t refused = 0u;
 
-  // Left-looking factor of the world's pattern, level by level; a warp per column.
+  // One column of the left-looking factor, by one warp: its update terms in ascending k (each
+  // term's rows at their precomputed offsets in the column), the pivot, the scaling.
+  auto factor_column = [&](int j) -> uint32_t {
+    uint32_t bad = 0;
+    const int cj = D.colp[j];
+    for (int u = D.uk_ptr[j]; u < D.uk_ptr[j + 1]; ++u) {
+      const int kk = D.uk_col[u], p = D.uk_pos[u], r0 = D.uk_rel[u];
+      const int cnt = D.colp[kk + 1] - p;
+      const double ljk = lval[p];
+      for (int t = lane; t < cnt; t += 32) lval[cj + D.rel[r0 + t]] -= lval[p + t] * ljk;
+      __syncwarp();
+    }
+    double piv = 0.0;
+    if (lane == 0) {
+      const double d = lval[cj];
+      if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+      piv = sqrt(d);
+      lval[cj] = piv;
+    }
+    piv = __shfl_sync(0xffffffffu, piv, 0);
+    const double inv = 1.0 / piv;
+    const int len = D.colp[j + 1] - cj;
+    for (int t = 1 + lane; t < len; t += 32) lval[cj + t] *= inv;
+    __syncwarp();
+    return bad;
+  };
+  // The end of the run of one-column levels starting at lv (uniform across the CTA).
+  auto single_run_end = [&](int lv) {
+    int end = lv;
+    while (end < lv1 && D.lv_ptr[end + 1] - D.lv_ptr[end] == 1) ++end;
+    return end;
+  };
+  // Left-looking factor of the world's pattern, level by level; a warp per column; a run of
+  // one-column levels (the top separator's chain) by warp 0 alone, with warp syncs only.
   auto factor = [&]() {
     uint32_t bad = 0;
-    for (int lv = lv0; lv < lv1; ++lv) {
+    for (int lv = lv0; lv < lv1;) {
       const int a0 = D.lv_ptr[lv], a1 = D.lv_ptr[lv + 1];
-      for (int a = a0 + warp; a < a1; a += WARPS) {
-        const int j = D.lv_cols[a];
-        const int cj = D.colp[j];
-        for (int u = D.uk_ptr[j]; u < D.uk_ptr[j + 1]; ++u) {
-          const int kk = D.uk_col[u], p = D.uk_pos[u], r0 = D.uk_rel[u];
-          const int cnt = D.colp[kk + 1] - p;
-          const double ljk = lval[p];
-          for (int t = lane; t < cnt; t += 32) lval[cj + D.rel[r0 + t]] -= lval[p + t] * ljk;
-          __syncwarp();
-        }
-        double piv = 0.0;
-        if (lane == 0) {
-          const double d = lval[cj];
-          if (!(d > 0.0) || !is_finite(d)) bad = 1u;
-          piv = sqrt(d);
-          lval[cj] = piv;
-        }
-        piv = __shfl_sync(0xffffffffu, piv, 0);
-        const double inv = 1.0 / piv;
-        const int len = D.colp[j + 1] - cj;
-        for (int t = 1 + lane; t < len; t += 32) lval[cj + t] *= inv;
-        __syncwarp();
+      if (a1 - a0 == 1) {
+        const int end = single_run_end(lv);
+        if (warp == 0)
+          for (int l = lv; l < end; ++l) bad |= factor_column(D.lv_cols[D.lv_ptr[l]]);
+        lv = end;
+      } else {
+        for (int a = a0 + warp; a < a1; a += WARPS) bad |= factor_column(D.lv_cols[a]);
+        ++lv;
       }
       __syncthreads();
     }
     return bad;
   };
-  // Forward and back substitution of L L^T x = b (b in NC_Y, position-indexed; x to NC_X).
+  // Forward and back substitution of L L^T x = b (b in Yv, x to Xv, position-indexed): a thread
+  // per column, or for a run of one-column levels warp 0 with the dot products across its lanes
+  // (a fixed xor tree).
+  auto warp_sum = [&](double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  };
   auto solve = [&]() {
-    for (int lv = lv0; lv < lv1; ++lv) {
-      for (int a = D.lv_ptr[lv] + tid; a < D.lv_ptr[lv + 1]; a += BLOCK) {
-        const int j = D.lv_cols[a];
-        double b = CF(NC_Y, j);
-        for (int u = D.uk_ptr[j]; u < D.uk_ptr[j + 1]; ++u)
-          b -= lval[D.uk_pos[u]] * CF(NC_Y, D.uk_col[u]);
-        CF(NC_Y, j) = b / lval[D.colp[j]];
+    for (int lv = lv0; lv < lv1;) {
+      const int a0 = D.lv_ptr[lv], a1 = D.lv_ptr[lv + 1];
+      if (a1 - a0 == 1) {
+        const int end = single_run_end(lv);
+        if (warp == 0) {
+          for (int l = lv; l < end; ++l) {
+            const int j = D.lv_cols[D.lv_ptr[l]];
+            double part = 0.0;
+            for (int u = D.uk_ptr[j] + lane; u < D.uk_ptr[j + 1]; u += 32)
+              part += lval[D.uk_pos[u]] * Yv[D.uk_col[u]];
+            part = warp_sum(part);
+            if (lane == 0) Yv[j] = (Yv[j] - part) / lval[D.colp[j]];
+            __syncwarp();
+          }
+        }
+        lv = end;
+      } else {
+        for (int a = a0 + tid; a < a1; a += BLOCK) {
+          const int j = D.lv_cols[a];
+          double b = Yv[j];
+          for (int u = D.uk_ptr[j]; u < D.uk_ptr[j + 1]; ++u) b -= lval[D.uk_pos[u]] * Yv[D.uk_col[u]];
+          Yv[j] = b / lval[D.colp[j]];
+        }
+        ++lv;
       }
       __syncthreads();
     }
-    for (int lv = lv1 - 1; lv >= lv0; --lv) {
-      for (int a = D.lv_ptr[lv] + tid; a < D.lv_ptr[lv + 1]; a += BLOCK) {
-        const int j = D.lv_cols[a];
-        const int cj = D.colp[j], len = D.colp[j + 1] - cj;
-        double x = CF(NC_Y, j);
-        for (int t = 1; t < len; ++t) x -= lval[cj + t] * CF(NC_X, D.lrow[cj + t]);
-        CF(NC_X, j) = x / lval[cj];
+    for (int lv = lv1 - 1; lv >= lv0;) {
+      const int a0 = D.lv_ptr[lv], a1 = D.lv_ptr[lv + 1];
+      if (a1 - a0 == 1) {
+        int begin = lv;  // the run of one-column levels ending at lv
+        while (begin > lv0 && D.lv_ptr[begin] - D.lv_ptr[begin - 1] == 1) --begin;
+        if (warp == 0) {
+          for (int l = lv; l >= begin; --l) {
+            const int j = D.lv_cols[D.lv_ptr[l]];
+            const int cj = D.colp[j], len = D.colp[j + 1] - cj;
+            double part = 0.0;
+            for (int t = 1 + lane; t < len; t += 32) part += lval[cj + t] * Xv[D.lrow[cj + t]];
+            part = warp_sum(part);
+            if (lane == 0) Xv[j] = (Yv[j] - part) / lval[cj];
+            __syncwarp();
+          }
+        }
+        lv = begin - 1;
+      } else {
+        for (int a = a0 + tid; a < a1; a += BLOCK) {
+          const int j = D.lv_cols[a];
+          const int cj = D.colp[j], len = D.colp[j + 1] - cj;
+          double x = Yv[j];
+          for (int t = 1; t < len; ++t) x -= lval[cj + t] * Xv[D.lrow[cj + t]];
+          Xv[j] = x / lval[cj];
+        }
+        --lv;
       }
       __syncthreads();
     }
@@ -674,13 +745,13 @@ __global__ void __launch_bounds__(BLOCK)
         const long long gi = c0 + i;
         const double q = __ldg(T.q0 + gi) +
                          K * ((CF(kf, gi) + CF(kf + 1, gi)) + (-CF(kf + 2, gi)));
-        CF(NC_Y, __ldg(D.rank + gi)) = (q - CF(NC_MB, gi) * Vb) * CF(NC_S, gi);
+        Yv[__ldg(D.rank + gi)] = (q - CF(NC_MB, gi) * Vb) * CF(NC_S, gi);
       }
       __syncthreads();
       solve();
       for (int i = tid; i < nc; i += BLOCK) {
         const long long gi = c0 + i;
-        CF(NC_VX, gi) = CF(NC_X, __ldg(D.rank + gi)) * CF(NC_S, gi);
+        CF(NC_VX, gi) = Xv[__ldg(D.rank + gi)] * CF(NC_S, gi);
       }
       __syncthreads();
       // Junctions: the linear flux at the stage potentials, the stage gate.
@@ -1167,6 +1238,8 @@ int build_plan(cb_tissue *t) {
     for (long long r = 0; r < n; ++r) lv_cols[c0 + r] = (int)(c0 + p.level_cols[r]);
     for (long long e = 0; e < ne; ++e) edge_pos[e0 + e] = (int)(fbase + p.edge_pos[e]);
     plan->max_level = std::max(plan->max_level, (int)p.level_ptr.size() - 1);
+    plan->smem_bytes = std::max(plan->smem_bytes,
+                                sizeof(double) * (size_t)(p.colp[n] + 2 * n));
     fbase += p.colp[n];
     ubase += (long long)p.uk_col.size();
     rbase += (long long)p.rel.size();
@@ -1203,6 +1276,8 @@ int build_plan(cb_tissue *t) {
     delete plan;
     return rc;
   }
+  // Shared-memory mode when every world's factor and vectors fit beside the kernel's own arrays.
+  if (plan->smem_bytes > 200 * 1024) plan->smem_bytes = 0;
   t->n2 = plan;
   return CB_OK;
 }
@@ -1211,9 +1286,19 @@ template <int NCH>
 int launch_n2(cb_tissue *t, const double *in, double *out, const double *control,
               const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
               cudaStream_t stream) {
-  n2_kernel<kN2Block, NCH><<<t->W, kN2Block, 0, stream>>>(t->t, t->layout, t->n2->d, in, out,
-                                                          control, k, n_steps, status, taken);
-  cudaError_t e = cudaGetLastError();
+  const size_t smem = t->n2->smem_bytes;
+  cudaError_t e;
+  if (smem) {
+    auto kern = n2_kernel<kN2Block, NCH, true>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (n2)");
+    kern<<<t->W, kN2Block, smem, stream>>>(t->t, t->layout, t->n2->d, in, out, control, k,
+                                           n_steps, status, taken);
+  } else {
+    n2_kernel<kN2Block, NCH, false><<<t->W, kN2Block, 0, stream>>>(
+        t->t, t->layout, t->n2->d, in, out, control, k, n_steps, status, taken);
+  }
+  e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "n2 launch");
   return CB_OK;
 }
