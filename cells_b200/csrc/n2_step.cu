@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <queue>
 #include <set>
 #include <string>
@@ -45,19 +46,20 @@
 namespace cbk {
 
 struct N2Dev {
-  int *rank;      // [C] cell -> position (world base + minimum-degree rank)
-  int *colp;      // [C+1] position -> first factor entry (global)
-  int *lrow;      // [F] factor entry -> row position
-  int *uk_ptr;    // [C+1] position j -> its update list (the columns k < j with L_jk != 0)
-  int *uk_col;    // [U] column position k
-  int *uk_pos;    // [U] factor entry of L_jk
-  int *uk_rel;    // [U] offset into rel of the pair's relative indices
-  int *rel;       // [R] entry of column k at or below row j -> offset in column j
-  int *lv_world;  // [W+1] first level of each world
-  int *lv_ptr;    // [levels+1] first column of each level in lv_cols
-  int *lv_cols;   // [C] positions, level by level
-  int *edge_pos;  // [E] factor entry of the junction's off-diagonal
-  double *lval;   // [F] factor values
+  // World-local plan arrays; world w's entries start at the bases below.
+  int *rank;      // [C] each cell's position (its minimum-degree rank in its world)
+  int *colp;      // [C+W] per world n+1 first factor entries of its columns (world w at c0 + w)
+  int *lrow;      // [F] each factor entry's row
+  int *uk_ptr;    // [C+W] per world n+1: column j's update list (the k < j with L_jk != 0)
+  int *uk_col;    // [U] k
+  int *uk_pos;    // [U] the factor entry of L_jk
+  int *uk_rel;    // [U] offset into rel of the pair's relative positions
+  int *rel;       // [R] each entry of column k at or below row j -> its offset in column j
+  int *lv_ptr;    // [levels+W] per world L+1 first columns of its levels (world w at lb[w] + w)
+  int *lv_cols;   // [C] columns level by level (world w at c0)
+  int *edge_pos;  // [E] each junction's off-diagonal factor entry
+  int *fb, *ub, *rb, *lb;  // [W+1] bases: factor entries, update terms, rel, levels
+  double *lval;   // [F] factor values (global mode)
   double *cs;     // cell scratch [NC_FIELDS][C]
   double *es;     // junction scratch [NE_FIELDS][E]
 };
@@ -67,7 +69,10 @@ struct N2Plan {
   std::vector<void *> owned;
   long long factor_entries = 0, update_terms = 0;
   int levels = 0, max_level = 0;
-  size_t smem_bytes = 0;  // dynamic shared memory of the shared-memory kernel; 0: global mode
+  size_t smem_bytes = 0;  // dynamic shared memory per CTA (worlds that fit stage into it)
+  int block = 256;        // CTA threads (256, or 128 for small worlds)
+  int min_blocks = 2;     // the register budget's target CTAs per SM (2: capped at 128
+                          // registers, measured fastest on 16x16 grids; 1: uncapped)
 };
 
 }  // namespace cbk
@@ -282,14 +287,15 @@ __device__ __forceinline__ void patch_mu(const double *__restrict__ wc, const do
     mu[s] = wc[WC_RT] * (lc[s] - wc[WC_LOGCO + s]) + ((s < 2) ? kF * dv : (-kF) * dv);
 }
 
-// SHARED: the world's factor values and solve vectors in dynamic shared memory (when every
-// world's fit), else in the global scratch.
-template <int BLOCK, int NCH, bool SHARED>
-__global__ void __launch_bounds__(BLOCK)
+// Each world's factor values, solve vectors and plan are copied to dynamic shared memory once per
+// launch when they fit (`smem_bytes`): all of it, or all but the relative positions; otherwise the
+// world works from global memory. The choice is per world (uniform within its CTA).
+template <int BLOCK, int NCH, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
     n2_kernel(const Tissue T, const Layout L, const N2Dev D, const double *state_in,
               double *state_out, const double *__restrict__ control, const StepCoef k,
               int n_steps, uint32_t *__restrict__ world_status,
-              int32_t *__restrict__ accepted_steps) {
+              int32_t *__restrict__ accepted_steps, size_t smem_bytes) {
   extern __shared__ double n2_smem[];
   constexpr int NQ = NCH > 0 ? NCH : 1;
   __shared__ double sW[WC_STRIDE];
@@ -305,13 +311,46 @@ __global__ void __launch_bounds__(BLOCK)
   if (tid == 0) sBits = 0u;
   double *cs = D.cs;
   double *es = D.es;
-  // Factor values and solve vectors, addressed by global factor entry / global position.
-  const int fbase = D.colp[T.cell_offset[blockIdx.x]];
-  const int fcount = D.colp[T.cell_offset[blockIdx.x + 1]] - fbase;
-  double *lval = SHARED ? n2_smem - fbase : D.lval;
-  double *Yv = SHARED ? n2_smem + fcount - T.cell_offset[blockIdx.x] : cs + (long long)NC_Y * T.C;
-  double *Xv = SHARED ? Yv + (T.cell_offset[blockIdx.x + 1] - T.cell_offset[blockIdx.x])
-                      : cs + (long long)NC_X * T.C;
+  // The world's factor plan (local indices), factor values and solve vectors (by position).
+  const int wF = D.fb[blockIdx.x + 1] - D.fb[blockIdx.x];
+  const int wU = D.ub[blockIdx.x + 1] - D.ub[blockIdx.x];
+  const int wR = D.rb[blockIdx.x + 1] - D.rb[blockIdx.x];
+  const int wL = D.lb[blockIdx.x + 1] - D.lb[blockIdx.x];
+  const int wc0 = T.cell_offset[blockIdx.x], wn = T.cell_offset[blockIdx.x + 1] - wc0;
+  const int *colp = D.colp + wc0 + blockIdx.x, *lrow = D.lrow + D.fb[blockIdx.x];
+  const int *ukp = D.uk_ptr + wc0 + blockIdx.x, *ukc = D.uk_col + D.ub[blockIdx.x];
+  const int *ukpos = D.uk_pos + D.ub[blockIdx.x], *ukrel = D.uk_rel + D.ub[blockIdx.x];
+  const int *rel = D.rel + D.rb[blockIdx.x];
+  const int *lvp = D.lv_ptr + D.lb[blockIdx.x] + blockIdx.x, *lvc = D.lv_cols + wc0;
+  double *lval = D.lval + D.fb[blockIdx.x];
+  double *Yv = cs + (long long)NC_Y * T.C + wc0;
+  double *Xv = cs + (long long)NC_X * T.C + wc0;
+  const size_t values = sizeof(double) * (size_t)(wF + 2 * wn);
+  const size_t plan_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wF + 3 * wU + wL + 1 + wn);
+  const int mode = values + plan_ints + sizeof(int) * (size_t)wR <= smem_bytes ? 2
+                   : values + plan_ints <= smem_bytes                           ? 1
+                                                                                : 0;
+  if (mode > 0) {
+    lval = n2_smem;
+    Yv = lval + wF;
+    Xv = Yv + wn;
+    int *si = reinterpret_cast<int *>(Xv + wn);
+    auto stage_ints = [&](const int *src, int count) {
+      for (int i = threadIdx.x; i < count; i += BLOCK) si[i] = src[i];
+      const int *out = si;
+      si += count;
+      return out;
+    };
+    colp = stage_ints(colp, wn + 1);
+    lrow = stage_ints(lrow, wF);
+    ukp = stage_ints(ukp, wn + 1);
+    ukc = stage_ints(ukc, wU);
+    ukpos = stage_ints(ukpos, wU);
+    ukrel = stage_ints(ukrel, wU);
+    lvp = stage_ints(lvp, wL + 1);
+    lvc = stage_ints(lvc, wn);
+    if (mode == 2) rel = stage_ints(rel, wR);
+  }
   const long long oN = L.s[CB_AMOUNT_INCREMENT], oG = L.s[CB_JUNCTION_GATE];
   const long long oH = L.s[CB_CHANNEL_GATE];
   const double *mctl = control + L.c[CB_CONTROL_MEMBRANE];
@@ -322,7 +361,7 @@ __global__ void __launch_bounds__(BLOCK)
   const double gdt = k.gamma_dt;               // the implicit diagonal gamma dt (the operator's)
   const double theta = 0.5 * k.dt;             // the routes' operator time
   const double w1 = (1.0 - (1.0 - 1.0 / sqrt(2.0))) * k.dt;  // (1 - gamma) dt
-  const int lv0 = D.lv_world[w], lv1 = D.lv_world[w + 1];
+  const int lv0 = 0, lv1 = wL;
   auto CF = [&](int f, long long gi) -> double & { return cs[(long long)f * C + gi]; };
   auto EF = [&](int f, long long ge) -> double & { return es[(long long)f * E + ge]; };
   auto CH = [&](int q, int f, long long gi) -> double & {
@@ -343,12 +382,12 @@ __global__ void __launch_bounds__(BLOCK)
   // term's rows at their precomputed offsets in the column), the pivot, the scaling.
   auto factor_column = [&](int j) -> uint32_t {
     uint32_t bad = 0;
-    const int cj = D.colp[j];
-    for (int u = D.uk_ptr[j]; u < D.uk_ptr[j + 1]; ++u) {
-      const int kk = D.uk_col[u], p = D.uk_pos[u], r0 = D.uk_rel[u];
-      const int cnt = D.colp[kk + 1] - p;
+    const int cj = colp[j];
+    for (int u = ukp[j]; u < ukp[j + 1]; ++u) {
+      const int kk = ukc[u], p = ukpos[u], r0 = ukrel[u];
+      const int cnt = colp[kk + 1] - p;
       const double ljk = lval[p];
-      for (int t = lane; t < cnt; t += 32) lval[cj + D.rel[r0 + t]] -= lval[p + t] * ljk;
+      for (int t = lane; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
       __syncwarp();
     }
     double piv = 0.0;
@@ -360,7 +399,7 @@ __global__ void __launch_bounds__(BLOCK)
     }
     piv = __shfl_sync(0xffffffffu, piv, 0);
     const double inv = 1.0 / piv;
-    const int len = D.colp[j + 1] - cj;
+    const int len = colp[j + 1] - cj;
     for (int t = 1 + lane; t < len; t += 32) lval[cj + t] *= inv;
     __syncwarp();
     return bad;
@@ -368,7 +407,7 @@ __global__ void __launch_bounds__(BLOCK)
   // The end of the run of one-column levels starting at lv (uniform across the CTA).
   auto single_run_end = [&](int lv) {
     int end = lv;
-    while (end < lv1 && D.lv_ptr[end + 1] - D.lv_ptr[end] == 1) ++end;
+    while (end < lv1 && lvp[end + 1] - lvp[end] == 1) ++end;
     return end;
   };
   // Left-looking factor of the world's pattern, level by level; a warp per column; a run of
@@ -376,14 +415,14 @@ __global__ void __launch_bounds__(BLOCK)
   auto factor = [&]() {
     uint32_t bad = 0;
     for (int lv = lv0; lv < lv1;) {
-      const int a0 = D.lv_ptr[lv], a1 = D.lv_ptr[lv + 1];
+      const int a0 = lvp[lv], a1 = lvp[lv + 1];
       if (a1 - a0 == 1) {
         const int end = single_run_end(lv);
         if (warp == 0)
-          for (int l = lv; l < end; ++l) bad |= factor_column(D.lv_cols[D.lv_ptr[l]]);
+          for (int l = lv; l < end; ++l) bad |= factor_column(lvc[lvp[l]]);
         lv = end;
       } else {
-        for (int a = a0 + warp; a < a1; a += WARPS) bad |= factor_column(D.lv_cols[a]);
+        for (int a = a0 + warp; a < a1; a += WARPS) bad |= factor_column(lvc[a]);
         ++lv;
       }
       __syncthreads();
@@ -399,43 +438,43 @@ __global__ void __launch_bounds__(BLOCK)
   };
   auto solve = [&]() {
     for (int lv = lv0; lv < lv1;) {
-      const int a0 = D.lv_ptr[lv], a1 = D.lv_ptr[lv + 1];
+      const int a0 = lvp[lv], a1 = lvp[lv + 1];
       if (a1 - a0 == 1) {
         const int end = single_run_end(lv);
         if (warp == 0) {
           for (int l = lv; l < end; ++l) {
-            const int j = D.lv_cols[D.lv_ptr[l]];
+            const int j = lvc[lvp[l]];
             double part = 0.0;
-            for (int u = D.uk_ptr[j] + lane; u < D.uk_ptr[j + 1]; u += 32)
-              part += lval[D.uk_pos[u]] * Yv[D.uk_col[u]];
+            for (int u = ukp[j] + lane; u < ukp[j + 1]; u += 32)
+              part += lval[ukpos[u]] * Yv[ukc[u]];
             part = warp_sum(part);
-            if (lane == 0) Yv[j] = (Yv[j] - part) / lval[D.colp[j]];
+            if (lane == 0) Yv[j] = (Yv[j] - part) / lval[colp[j]];
             __syncwarp();
           }
         }
         lv = end;
       } else {
         for (int a = a0 + tid; a < a1; a += BLOCK) {
-          const int j = D.lv_cols[a];
+          const int j = lvc[a];
           double b = Yv[j];
-          for (int u = D.uk_ptr[j]; u < D.uk_ptr[j + 1]; ++u) b -= lval[D.uk_pos[u]] * Yv[D.uk_col[u]];
-          Yv[j] = b / lval[D.colp[j]];
+          for (int u = ukp[j]; u < ukp[j + 1]; ++u) b -= lval[ukpos[u]] * Yv[ukc[u]];
+          Yv[j] = b / lval[colp[j]];
         }
         ++lv;
       }
       __syncthreads();
     }
     for (int lv = lv1 - 1; lv >= lv0;) {
-      const int a0 = D.lv_ptr[lv], a1 = D.lv_ptr[lv + 1];
+      const int a0 = lvp[lv], a1 = lvp[lv + 1];
       if (a1 - a0 == 1) {
         int begin = lv;  // the run of one-column levels ending at lv
-        while (begin > lv0 && D.lv_ptr[begin] - D.lv_ptr[begin - 1] == 1) --begin;
+        while (begin > lv0 && lvp[begin] - lvp[begin - 1] == 1) --begin;
         if (warp == 0) {
           for (int l = lv; l >= begin; --l) {
-            const int j = D.lv_cols[D.lv_ptr[l]];
-            const int cj = D.colp[j], len = D.colp[j + 1] - cj;
+            const int j = lvc[lvp[l]];
+            const int cj = colp[j], len = colp[j + 1] - cj;
             double part = 0.0;
-            for (int t = 1 + lane; t < len; t += 32) part += lval[cj + t] * Xv[D.lrow[cj + t]];
+            for (int t = 1 + lane; t < len; t += 32) part += lval[cj + t] * Xv[lrow[cj + t]];
             part = warp_sum(part);
             if (lane == 0) Xv[j] = (Yv[j] - part) / lval[cj];
             __syncwarp();
@@ -444,10 +483,10 @@ __global__ void __launch_bounds__(BLOCK)
         lv = begin - 1;
       } else {
         for (int a = a0 + tid; a < a1; a += BLOCK) {
-          const int j = D.lv_cols[a];
-          const int cj = D.colp[j], len = D.colp[j + 1] - cj;
+          const int j = lvc[a];
+          const int cj = colp[j], len = colp[j + 1] - cj;
           double x = Yv[j];
-          for (int t = 1; t < len; ++t) x -= lval[cj + t] * Xv[D.lrow[cj + t]];
+          for (int t = 1; t < len; ++t) x -= lval[cj + t] * Xv[lrow[cj + t]];
           Xv[j] = x / lval[cj];
         }
         --lv;
@@ -537,7 +576,7 @@ __global__ void __launch_bounds__(BLOCK)
       }
       // Zero the world's factor columns held by this thread's cells.
       const int P = __ldg(D.rank + gi);
-      for (int f = D.colp[P]; f < D.colp[P + 1]; ++f) lval[f] = 0.0;
+      for (int f = colp[P]; f < colp[P + 1]; ++f) lval[f] = 0.0;
     }
     __syncthreads();
     // E1 (junctions): stage-0 whole fluxes, the gate law at the start, the predicted gate.
@@ -720,7 +759,7 @@ __global__ void __launch_bounds__(BLOCK)
       if (!(mii > 0.0)) bits |= CB_WORLD_OPERATOR;
       const double sc = 1.0 / sqrt(mii > 0.0 ? mii : 1.0);
       CF(NC_S, gi) = sc;
-      lval[D.colp[__ldg(D.rank + gi)]] = (mii * sc) * sc;
+      lval[colp[__ldg(D.rank + gi)]] = (mii * sc) * sc;
     }
     __syncthreads();
     // E3 (junctions): the operator's off-diagonal entries, scaled (row then column).
@@ -1062,8 +1101,6 @@ __global__ void __launch_bounds__(BLOCK)
   }
 }
 
-constexpr int kN2Block = 256;
-
 // ---------------------------------------------------------------------------------------------
 // Host: the sparse factor's plan (numerics/sparse_cholesky.py's bind, restated): a
 // minimum-degree order (least current degree, ties by the least original degree, then the
@@ -1205,9 +1242,9 @@ int build_plan(cb_tissue *t) {
   auto *plan = new N2Plan();
   const int W = t->W;
   const long long C = t->C, E = t->E;
-  std::vector<int> rank(C), colp(C + 1, 0), lrow, uk_ptr(C + 1, 0), uk_col, uk_pos, uk_rel, rel,
-      lv_world(W + 1, 0), lv_ptr{0}, lv_cols(C), edge_pos(E);
-  long long fbase = 0, ubase = 0, rbase = 0;
+  std::vector<int> rank(C), colp, lrow, uk_ptr, uk_col, uk_pos, uk_rel, rel, lv_ptr, lv_cols(C),
+      edge_pos(E), fb{0}, ub{0}, rb{0}, lb{0};
+  size_t shared_all = 0, shared_plan = 0;
   int rc = CB_OK;
   for (int w = 0; w < W && !rc; ++w) {
     const long long c0 = t->h_cell_offset[w], n = t->h_cell_offset[w + 1] - c0;
@@ -1215,45 +1252,53 @@ int build_plan(cb_tissue *t) {
     WorldPlan p;
     rc = plan_world((int)n, t->h_snd.data() + e0, t->h_rcv.data() + e0, (int)ne, p);
     if (rc) break;
-    if (fbase + p.colp[n] >= (1LL << 31) || ubase + (long long)p.uk_col.size() >= (1LL << 31) ||
-        rbase + (long long)p.rel.size() >= (1LL << 31)) {
+    const long long F = p.colp[n], U = (long long)p.uk_col.size(), R = (long long)p.rel.size();
+    const long long L = (long long)p.level_ptr.size() - 1;
+    if (fb.back() + F >= (1LL << 31) || ub.back() + U >= (1LL << 31) ||
+        rb.back() + R >= (1LL << 31)) {
       rc = fail(CB_ERR_UNSUPPORTED, "N2: the batch's factor plan exceeds 2^31 entries");
       break;
     }
-    for (long long i = 0; i < n; ++i) rank[c0 + i] = (int)(c0 + p.rank[i]);
-    for (long long r = 0; r < n; ++r) {
-      colp[c0 + r] = (int)(fbase + p.colp[r]);
-      uk_ptr[c0 + r] = (int)(ubase + p.uk_ptr[r]);
-    }
-    for (int r : p.lrow) lrow.push_back((int)(c0 + r));
-    for (size_t u = 0; u < p.uk_col.size(); ++u) {
-      uk_col.push_back((int)(c0 + p.uk_col[u]));
-      uk_pos.push_back((int)(fbase + p.uk_pos[u]));
-      uk_rel.push_back((int)(rbase + p.uk_rel[u]));
-    }
+    for (long long i = 0; i < n; ++i) rank[c0 + i] = p.rank[i];
+    colp.insert(colp.end(), p.colp.begin(), p.colp.end());
+    lrow.insert(lrow.end(), p.lrow.begin(), p.lrow.end());
+    uk_ptr.insert(uk_ptr.end(), p.uk_ptr.begin(), p.uk_ptr.end());
+    uk_col.insert(uk_col.end(), p.uk_col.begin(), p.uk_col.end());
+    uk_pos.insert(uk_pos.end(), p.uk_pos.begin(), p.uk_pos.end());
+    uk_rel.insert(uk_rel.end(), p.uk_rel.begin(), p.uk_rel.end());
     rel.insert(rel.end(), p.rel.begin(), p.rel.end());
-    lv_world[w] = (int)lv_ptr.size() - 1;
-    for (size_t l = 0; l + 1 < p.level_ptr.size(); ++l)
-      lv_ptr.push_back(lv_ptr.back() + (p.level_ptr[l + 1] - p.level_ptr[l]));
-    for (long long r = 0; r < n; ++r) lv_cols[c0 + r] = (int)(c0 + p.level_cols[r]);
-    for (long long e = 0; e < ne; ++e) edge_pos[e0 + e] = (int)(fbase + p.edge_pos[e]);
-    plan->max_level = std::max(plan->max_level, (int)p.level_ptr.size() - 1);
-    plan->smem_bytes = std::max(plan->smem_bytes,
-                                sizeof(double) * (size_t)(p.colp[n] + 2 * n));
-    fbase += p.colp[n];
-    ubase += (long long)p.uk_col.size();
-    rbase += (long long)p.rel.size();
+    lv_ptr.insert(lv_ptr.end(), p.level_ptr.begin(), p.level_ptr.end());
+    for (long long r = 0; r < n; ++r) lv_cols[c0 + r] = p.level_cols[r];
+    for (long long e = 0; e < ne; ++e) edge_pos[e0 + e] = p.edge_pos[e];
+    fb.push_back((int)(fb.back() + F));
+    ub.push_back((int)(ub.back() + U));
+    rb.push_back((int)(rb.back() + R));
+    lb.push_back((int)(lb.back() + L));
+    plan->max_level = std::max(plan->max_level, (int)L);
+    // Shared-memory footprint: values and vectors, then the plan's integers.
+    const size_t values = sizeof(double) * (size_t)(F + 2 * n);
+    const size_t ints = sizeof(int) * (size_t)(2 * (n + 1) + F + 3 * U + L + 1 + n);
+    shared_plan = std::max(shared_plan, values + ints);
+    shared_all = std::max(shared_all, values + ints + sizeof(int) * (size_t)R);
   }
   if (rc) {
     delete plan;
     return rc;
   }
-  lv_world[W] = (int)lv_ptr.size() - 1;
-  colp[C] = (int)fbase;
-  uk_ptr[C] = (int)ubase;
-  plan->factor_entries = fbase;
-  plan->update_terms = rbase;
-  plan->levels = (int)lv_ptr.size() - 1;
+  plan->factor_entries = fb.back();
+  plan->update_terms = rb.back();
+  plan->levels = lb.back();
+  // Shared memory per CTA: the largest world's whole footprint, at most 200 KB (larger worlds
+  // stage less or work from global memory). Overrides for sweeps: CELLS_B200_N2_SMEM (KB),
+  // CELLS_B200_N2_BLOCK (128 or 256), CELLS_B200_N2_MINB (1, or 2: registers capped for more
+  // resident CTAs).
+  size_t cap = 200 * 1024;
+  if (const char *env = std::getenv("CELLS_B200_N2_SMEM")) cap = (size_t)std::atoi(env) * 1024;
+  plan->smem_bytes = std::min(std::max(shared_all, shared_plan), cap);
+  if (const char *env = std::getenv("CELLS_B200_N2_BLOCK"))
+    plan->block = std::atoi(env) == 128 ? 128 : 256;
+  if (const char *env = std::getenv("CELLS_B200_N2_MINB"))
+    plan->min_blocks = std::atoi(env) >= 2 ? 2 : 1;
   N2Dev &d = plan->d;
   if (!rc) rc = upload_vec(plan, rank, &d.rank);
   if (!rc) rc = upload_vec(plan, colp, &d.colp);
@@ -1263,11 +1308,14 @@ int build_plan(cb_tissue *t) {
   if (!rc) rc = upload_vec(plan, uk_pos, &d.uk_pos);
   if (!rc) rc = upload_vec(plan, uk_rel, &d.uk_rel);
   if (!rc) rc = upload_vec(plan, rel, &d.rel);
-  if (!rc) rc = upload_vec(plan, lv_world, &d.lv_world);
   if (!rc) rc = upload_vec(plan, lv_ptr, &d.lv_ptr);
   if (!rc) rc = upload_vec(plan, lv_cols, &d.lv_cols);
   if (!rc) rc = upload_vec(plan, edge_pos, &d.edge_pos);
-  if (!rc) rc = upload_vec(plan, std::vector<double>(fbase), &d.lval);
+  if (!rc) rc = upload_vec(plan, fb, &d.fb);
+  if (!rc) rc = upload_vec(plan, ub, &d.ub);
+  if (!rc) rc = upload_vec(plan, rb, &d.rb);
+  if (!rc) rc = upload_vec(plan, lb, &d.lb);
+  if (!rc) rc = upload_vec(plan, std::vector<double>((size_t)fb.back()), &d.lval);
   if (!rc)
     rc = upload_vec(plan, std::vector<double>((size_t)n2_cell_fields(t->t.nch) * C), &d.cs);
   if (!rc) rc = upload_vec(plan, std::vector<double>((size_t)NE_FIELDS * std::max(E, 1LL)), &d.es);
@@ -1276,8 +1324,6 @@ int build_plan(cb_tissue *t) {
     delete plan;
     return rc;
   }
-  // Shared-memory mode when every world's factor and vectors fit beside the kernel's own arrays.
-  if (plan->smem_bytes > 200 * 1024) plan->smem_bytes = 0;
   t->n2 = plan;
   return CB_OK;
 }
@@ -1287,17 +1333,15 @@ int launch_n2(cb_tissue *t, const double *in, double *out, const double *control
               const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
               cudaStream_t stream) {
   const size_t smem = t->n2->smem_bytes;
-  cudaError_t e;
-  if (smem) {
-    auto kern = n2_kernel<kN2Block, NCH, true>;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (n2)");
-    kern<<<t->W, kN2Block, smem, stream>>>(t->t, t->layout, t->n2->d, in, out, control, k,
-                                           n_steps, status, taken);
-  } else {
-    n2_kernel<kN2Block, NCH, false><<<t->W, kN2Block, 0, stream>>>(
-        t->t, t->layout, t->n2->d, in, out, control, k, n_steps, status, taken);
-  }
+  const int block = t->n2->block, minb = t->n2->min_blocks;
+  auto kern = n2_kernel<256, NCH, 1>;
+  if (block == 128) kern = minb >= 2 ? n2_kernel<128, NCH, 4> : n2_kernel<128, NCH, 1>;
+  else if (minb >= 2) kern = n2_kernel<256, NCH, 2>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (n2)");
+  kern<<<t->W, block, smem, stream>>>(t->t, t->layout, t->n2->d, in, out, control, k, n_steps,
+                                      status, taken, smem);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "n2 launch");
   return CB_OK;
