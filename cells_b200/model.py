@@ -26,6 +26,7 @@ from . import worlds
 from .tissue import Tissue
 
 ARS222_ID = "cells.solver.imex_ars222_face_electromigration@1"
+N2_ID = "cells.solver.imex_ars222_implicit_conductances@1"
 PUMP_FIELDS = ("atp_mM", "adp_mM", "pi_mM", "km_na_mM", "km_k_mM", "km_atp_mM",
                "delta_g0_J_mol")
 
@@ -243,18 +244,32 @@ def reference_state(packed, like, m):
     return type(like)(**fields)
 
 
+def layout_solver(p):
+    """The IMEX method a bound layout declares: N2 (imex_ars222_implicit_conductances@1) when its
+    operator time is a vector (one entry per frozen block, the reference's own static switch,
+    numerics/surface_imex.py:94-107), else the plain ARS(2,2,2)."""
+    time = getattr(p, "imex_operator_time", None)
+    return N2_ID if time is not None and np.shape(time) == (2,) else ARS222_ID
+
+
 class DeviceStep:
     """checked_step(state, dt, control, p, active) of the held-bath pump tissue on the device.
 
     Bind once per layout: ``step = DeviceStep(p)``; then ``state, valid = step(state, dt,
     control, p, active)`` as the reference's checked_step. ``solver`` is the layout's IMEX
-    method; only ARS(2,2,2) (the reference's imex_ars222_face_electromigration@1) runs here."""
+    method (by default the one the layout declares, layout_solver): ARS(2,2,2)
+    (imex_ars222_face_electromigration@1, CB_METHOD_ARS222) or N2
+    (imex_ars222_implicit_conductances@1, CB_METHOD_N2)."""
 
-    def __init__(self, p, device=0, solver=ARS222_ID):
-        if solver != ARS222_ID:
+    def __init__(self, p, device=0, solver=None):
+        from . import _lib
+
+        solver = layout_solver(p) if solver is None else solver
+        if solver not in (ARS222_ID, N2_ID):
             raise Unsupported(f"solver {solver} is not in the device step")
         if hasattr(p, "imex_explicit") and np.asarray(p.imex_explicit).shape[0] != 3:
             raise Unsupported("the layout's tableau is not ARS(2,2,2)")
+        self.method = _lib.METHOD_N2 if solver == N2_ID else _lib.METHOD_ARS222
         world, self.mapping = world_from_layout(p)
         self.batch = worlds.pack([world])
         self.tissue = Tissue(self.batch, device=device)
@@ -276,7 +291,8 @@ class DeviceStep:
             pump=np.asarray(control.pump)[m.patch_of_cell],
             channel=(np.asarray(control.channel)[m.channel_index] if m.nch else 1.0),
         )
-        out, status, _ = self.tissue.step_host(self.tissue.pack_state(packed), ctl, float(dt), 1)
+        out, status, _ = self.tissue.step_host(self.tissue.pack_state(packed), ctl, float(dt), 1,
+                                               method=self.method)
         valid = bool(status[0] == 0)
         new = reference_state(self.tissue.unpack_state(out), state, m)
         return new, np.asarray(valid)

@@ -31,6 +31,8 @@ Fixtures:
   n2_grid4x4.npz         The 4x4 world under N2 (@3, implicit slope conductances), 300 steps.
   n2_channels_delaunay.npz  A 40-cell Delaunay world with NaV1.2 and Kv1.5 populations, gated
                          junctions, partial controls, a -4 mV bath, under N2, 200 steps.
+  pytrees_n2_padded.npz  That world's @3 pytrees under N2 (capacities 2 above the counts, 40
+                         steps), for the drop-in step.
   laws.npz               Point laws on grids of inputs: bernoulli, the pump kinetics and the
                          junction gate rate.
 """
@@ -102,6 +104,7 @@ LAYOUT_FIELDS = (
     "membrane_area", "membrane_capacitance", "membrane_permeability", "amount_reference",
     "initial_cell_charge_C", "junction_area", "junction_permeability",
     "junction_threshold_voltage", "junction_minimum", "boundary_V", "imex_explicit",
+    "imex_operator_time",
 )
 
 
@@ -111,15 +114,16 @@ CHANNEL_LAYOUT_FIELDS = (
 )
 
 
-def _run_reference_pytrees(world, *, model_id, dt, steps, keep, padding, controls):
+def _run_reference_pytrees(world, *, model_id, dt, steps, keep, padding, controls, solver=None):
     """The reference's own pytrees: layout fields, controls and full states (padded slots)."""
     from cells.definitions.specs import parse_spec
     from cells.registry.models import get_model
 
     from cells_b200 import worlds
 
+    extra = {} if solver is None else {"solver": solver}
     raw = worlds.reference_definition(world, dt=dt, steps=steps, model=model_id,
-                                      padding=padding, **controls)
+                                      padding=padding, **controls, **extra)
     spec = parse_spec(raw)
     model = get_model(spec.model)
     state, p = model.initial_values(spec)
@@ -325,6 +329,11 @@ def make_n2_trajectories():
     _save("n2_channels_delaunay.npz", worlds.pack([dworld]), stacked, kept, dt=1e-3,
           model_id=v3, solver=n2, elapsed=el,
           extra={"control_" + k.split("_")[0]: v for k, v in controls.items()})
+    # @3's own padded pytrees under N2, for the drop-in step.
+    out = _run_reference_pytrees(dworld, model_id=v3, dt=1e-3, steps=40, keep={0, 1, 20, 40},
+                                 padding=2, controls=controls, solver=n2)
+    np.savez_compressed(os.path.join(HERE, "pytrees_n2_padded.npz"), **out)
+    print("pytrees_n2_padded.npz written")
 
 
 def make_laws():

@@ -61,3 +61,12 @@ def test_out_of_scope_layouts_are_refused():
     outside[1] = True  # a finite, unheld outside node
     with pytest.raises(model.Unsupported):
         model.world_from_layout(p._replace(outside_active=outside))
+
+
+def test_layout_declares_its_solver():
+    _, p, _, _ = load_pytrees("pytrees_n2_padded.npz")
+    assert model.layout_solver(p) == model.N2_ID
+    world, m = model.world_from_layout(p)
+    assert m.nch == 2
+    _, p1, _, _ = load_pytrees()
+    assert model.layout_solver(p1) == model.ARS222_ID
