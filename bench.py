@@ -48,6 +48,7 @@ ADJOINT_UNIT = "world-gradients/s"
 METHOD = "cells.solver.imex_ars222_face_electromigration@1"
 METHOD_MIXED = "cells_b200.solver.imex_ars222_mixed_fp32@1"
 METHOD_N2 = "cells.solver.imex_ars222_implicit_conductances@1"
+METHOD_N2_MIXED = "cells_b200.solver.imex_ars222_implicit_conductances_mixed@1"
 
 
 def bytes_per_cell_step(batch):
@@ -548,11 +549,12 @@ def main():
 
     from cells_b200 import _lib as _lib_methods
 
-    if args.method == "n2" and args.precision == "mixed":
-        raise SystemExit("--method n2 runs in FP64 only")
-    method = (_lib_methods.METHOD_N2 if args.method == "n2"
-              else _lib_methods.METHOD_ARS222_MIXED if args.precision == "mixed"
-              else _lib_methods.METHOD_ARS222)
+    if args.method == "n2":
+        method = (_lib_methods.METHOD_N2_MIXED if args.precision == "mixed"
+                  else _lib_methods.METHOD_N2)
+    else:
+        method = (_lib_methods.METHOD_ARS222_MIXED if args.precision == "mixed"
+                  else _lib_methods.METHOD_ARS222)
     batch = build_batch(args, rank)
     tissue = Tissue(batch, device=local_rank)
     cells = batch.cells
@@ -663,11 +665,14 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32 rates / f64 accumulation",
+            "dtype": ("f64" if args.precision == "fp64" else
+                      "f32 factor / f64 refinement" if args.method == "n2" else
+                      "f32 rates / f64 accumulation"),
             "data": "synthetic (seeded pump-leak tissues)",
             "config": {
                 "workload": workload_name(args),
-                "method": (METHOD_N2 if args.method == "n2" else
+                "method": ((METHOD_N2 if args.precision == "fp64" else METHOD_N2_MIXED)
+                           if args.method == "n2" else
                            METHOD if args.precision == "fp64" else METHOD_MIXED),
                 "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
                 "launch": ({"kernel": "n2 (one world per CTA)", "block": 256}

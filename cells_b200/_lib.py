@@ -36,6 +36,7 @@ CONTROL_FIELDS = ("membrane", "junction", "pump", "channel")
 METHOD_ARS222 = 0
 METHOD_ARS222_MIXED = 1
 METHOD_N2 = 2
+METHOD_N2_MIXED = 3
 KERNEL_SHARED, KERNEL_PACKED = 0, 1
 WORLD_BITS = {
     1: "transport",

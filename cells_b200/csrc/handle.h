@@ -42,7 +42,7 @@ namespace cbk {
 // The N2 method (n2_step.cu): n_steps steps of every world, device buffers (cb_step's contract).
 int n2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
             const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
-            cudaStream_t stream);
+            cudaStream_t stream, bool mix);
 void n2_release(cb_tissue *t);
 }  // namespace cbk
 

@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 #include <queue>
 #include <set>
 #include <string>
@@ -84,6 +85,8 @@ using namespace cbk;
 // The stage solve's acceptance (surface_field.CHARGE_ATOL_C, CHARGE_RTOL).
 constexpr double kChargeAtol = 3e-25;
 constexpr double kChargeRtol = 2e-12;
+// The mixed form's refinement bound (corrections per stage solve).
+constexpr int kRefine = 6;
 
 // Cell scratch fields ([field][C]).
 enum N2Cell {
@@ -290,7 +293,9 @@ __device__ __forceinline__ void patch_mu(const double *__restrict__ wc, const do
 // Each world's factor values, solve vectors and plan are copied to dynamic shared memory once per
 // launch when they fit (`smem_bytes`): all of it, or all but the relative positions; otherwise the
 // world works from global memory. The choice is per world (uniform within its CTA).
-template <int BLOCK, int NCH, int MINB>
+// MIX: the factor and its substitutions in FP32, the stage potentials recovered by FP64
+// iterative refinement of the charge residual against the FP64 operator.
+template <int BLOCK, int NCH, int MINB, bool MIX>
 __global__ void __launch_bounds__(BLOCK, MINB)
     n2_kernel(const Tissue T, const Layout L, const N2Dev D, const double *state_in,
               double *state_out, const double *__restrict__ control, const StepCoef k,
@@ -322,16 +327,17 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   const int *ukpos = D.uk_pos + D.ub[blockIdx.x], *ukrel = D.uk_rel + D.ub[blockIdx.x];
   const int *rel = D.rel + D.rb[blockIdx.x];
   const int *lvp = D.lv_ptr + D.lb[blockIdx.x] + blockIdx.x, *lvc = D.lv_cols + wc0;
-  double *lval = D.lval + D.fb[blockIdx.x];
-  double *Yv = cs + (long long)NC_Y * T.C + wc0;
-  double *Xv = cs + (long long)NC_X * T.C + wc0;
-  const size_t values = sizeof(double) * (size_t)(wF + 2 * wn);
+  using FT = typename std::conditional<MIX, float, double>::type;
+  FT *lval = reinterpret_cast<FT *>(D.lval) + D.fb[blockIdx.x];
+  FT *Yv = reinterpret_cast<FT *>(cs + (long long)NC_Y * T.C) + wc0;
+  FT *Xv = reinterpret_cast<FT *>(cs + (long long)NC_X * T.C) + wc0;
+  const size_t values = sizeof(FT) * (size_t)(wF + 2 * wn);
   const size_t plan_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wF + 3 * wU + wL + 1 + wn);
   const int mode = values + plan_ints + sizeof(int) * (size_t)wR <= smem_bytes ? 2
                    : values + plan_ints <= smem_bytes                           ? 1
                                                                                 : 0;
   if (mode > 0) {
-    lval = n2_smem;
+    lval = reinterpret_cast<FT *>(n2_smem);
     Yv = lval + wF;
     Xv = Yv + wn;
     int *si = reinterpret_cast<int *>(Xv + wn);
@@ -386,19 +392,19 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     for (int u = ukp[j]; u < ukp[j + 1]; ++u) {
       const int kk = ukc[u], p = ukpos[u], r0 = ukrel[u];
       const int cnt = colp[kk + 1] - p;
-      const double ljk = lval[p];
+      const FT ljk = lval[p];
       for (int t = lane; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
       __syncwarp();
     }
-    double piv = 0.0;
+    FT piv = 0;
     if (lane == 0) {
-      const double d = lval[cj];
+      const FT d = lval[cj];
       if (!(d > 0.0) || !is_finite(d)) bad = 1u;
       piv = sqrt(d);
       lval[cj] = piv;
     }
     piv = __shfl_sync(0xffffffffu, piv, 0);
-    const double inv = 1.0 / piv;
+    const FT inv = FT(1) / piv;
     const int len = colp[j + 1] - cj;
     for (int t = 1 + lane; t < len; t += 32) lval[cj + t] *= inv;
     __syncwarp();
@@ -432,7 +438,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   // Forward and back substitution of L L^T x = b (b in Yv, x to Xv, position-indexed): a thread
   // per column, or for a run of one-column levels warp 0 with the dot products across its lanes
   // (a fixed xor tree).
-  auto warp_sum = [&](double v) {
+  auto warp_sum = [&](FT v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
   };
@@ -444,7 +450,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         if (warp == 0) {
           for (int l = lv; l < end; ++l) {
             const int j = lvc[lvp[l]];
-            double part = 0.0;
+            FT part = 0;
             for (int u = ukp[j] + lane; u < ukp[j + 1]; u += 32)
               part += lval[ukpos[u]] * Yv[ukc[u]];
             part = warp_sum(part);
@@ -456,7 +462,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       } else {
         for (int a = a0 + tid; a < a1; a += BLOCK) {
           const int j = lvc[a];
-          double b = Yv[j];
+          FT b = Yv[j];
           for (int u = ukp[j]; u < ukp[j + 1]; ++u) b -= lval[ukpos[u]] * Yv[ukc[u]];
           Yv[j] = b / lval[colp[j]];
         }
@@ -473,7 +479,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
           for (int l = lv; l >= begin; --l) {
             const int j = lvc[lvp[l]];
             const int cj = colp[j], len = colp[j + 1] - cj;
-            double part = 0.0;
+            FT part = 0;
             for (int t = 1 + lane; t < len; t += 32) part += lval[cj + t] * Xv[lrow[cj + t]];
             part = warp_sum(part);
             if (lane == 0) Xv[j] = (Yv[j] - part) / lval[cj];
@@ -485,7 +491,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         for (int a = a0 + tid; a < a1; a += BLOCK) {
           const int j = lvc[a];
           const int cj = colp[j], len = colp[j + 1] - cj;
-          double x = Yv[j];
+          FT x = Yv[j];
           for (int t = 1; t < len; ++t) x -= lval[cj + t] * Xv[lrow[cj + t]];
           Xv[j] = x / lval[cj];
         }
@@ -759,7 +765,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       if (!(mii > 0.0)) bits |= CB_WORLD_OPERATOR;
       const double sc = 1.0 / sqrt(mii > 0.0 ? mii : 1.0);
       CF(NC_S, gi) = sc;
-      lval[colp[__ldg(D.rank + gi)]] = (mii * sc) * sc;
+      lval[colp[__ldg(D.rank + gi)]] = FT((mii * sc) * sc);
     }
     __syncthreads();
     // E3 (junctions): the operator's off-diagonal entries, scaled (row then column).
@@ -770,7 +776,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       const double m = 0.0 + gdt * (-EF(NE_G, ge));
       const double s_row = ra > rb ? CF(NC_S, ga) : CF(NC_S, gb);
       const double s_col = ra > rb ? CF(NC_S, gb) : CF(NC_S, ga);
-      lval[__ldg(D.edge_pos + ge)] = (m * s_row) * s_col;
+      lval[__ldg(D.edge_pos + ge)] = FT((m * s_row) * s_col);
     }
     __syncthreads();
     if (factor()) bits |= CB_WORLD_OPERATOR;
@@ -779,20 +785,48 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     double plate2 = 0.0;
     for (int st = 1; st <= 2; ++st) {
       const int kf = st == 1 ? NC_K1 : NC_A;
-      // Charges and the scaled right-hand side (charge - M held) s.
-      for (int i = tid; i < nc; i += BLOCK) {
-        const long long gi = c0 + i;
-        const double q = __ldg(T.q0 + gi) +
-                         K * ((CF(kf, gi) + CF(kf + 1, gi)) + (-CF(kf + 2, gi)));
-        Yv[__ldg(D.rank + gi)] = (q - CF(NC_MB, gi) * Vb) * CF(NC_S, gi);
+      if constexpr (!MIX) {
+        // Charges and the scaled right-hand side (charge - M held) s; the FP64 solve.
+        for (int i = tid; i < nc; i += BLOCK) {
+          const long long gi = c0 + i;
+          const double q = __ldg(T.q0 + gi) +
+                           K * ((CF(kf, gi) + CF(kf + 1, gi)) + (-CF(kf + 2, gi)));
+          Yv[__ldg(D.rank + gi)] = (q - CF(NC_MB, gi) * Vb) * CF(NC_S, gi);
+        }
+        __syncthreads();
+        solve();
+        for (int i = tid; i < nc; i += BLOCK) {
+          const long long gi = c0 + i;
+          CF(NC_VX, gi) = Xv[__ldg(D.rank + gi)] * CF(NC_S, gi);
+        }
+        __syncthreads();
+      } else {
+        // Iterative refinement from V = 0: the FP64 residual r = q - M V, its FP32 correction
+        // (scaled), V += correction; until every row is within 1e-3 of the stage's acceptance
+        // bound (3e-25 C + 2e-12 max(|q|, |M V|)), at most kRefine corrections.
+        for (int i = tid; i < nc; i += BLOCK) CF(NC_VX, c0 + i) = 0.0;
+        __syncthreads();
+        for (int it = 0; it < kRefine; ++it) {
+          int pending = 0;
+          for (int i = tid; i < nc; i += BLOCK) {
+            const long long gi = c0 + i;
+            const double q = __ldg(T.q0 + gi) +
+                             K * ((CF(kf, gi) + CF(kf + 1, gi)) + (-CF(kf + 2, gi)));
+            double product;
+            const double r = -row_residual(gi, q, product);
+            const double bound = kChargeAtol + kChargeRtol * fmax(fabs(q), fabs(product));
+            if (!(fabs(r) <= 1e-3 * bound)) pending = 1;
+            Yv[__ldg(D.rank + gi)] = FT(r * CF(NC_S, gi));
+          }
+          if (!__syncthreads_or(pending)) break;
+          solve();
+          for (int i = tid; i < nc; i += BLOCK) {
+            const long long gi = c0 + i;
+            CF(NC_VX, gi) = CF(NC_VX, gi) + double(Xv[__ldg(D.rank + gi)]) * CF(NC_S, gi);
+          }
+          __syncthreads();
+        }
       }
-      __syncthreads();
-      solve();
-      for (int i = tid; i < nc; i += BLOCK) {
-        const long long gi = c0 + i;
-        CF(NC_VX, gi) = Xv[__ldg(D.rank + gi)] * CF(NC_S, gi);
-      }
-      __syncthreads();
       // Junctions: the linear flux at the stage potentials, the stage gate.
       const double frac_dt = st == 1 ? k.frac1_dt : k.frac2_dt;
       for (int e = tid; e < ne; e += BLOCK) {
@@ -1331,12 +1365,15 @@ int build_plan(cb_tissue *t) {
 template <int NCH>
 int launch_n2(cb_tissue *t, const double *in, double *out, const double *control,
               const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
-              cudaStream_t stream) {
+              cudaStream_t stream, bool mix) {
   const size_t smem = t->n2->smem_bytes;
   const int block = t->n2->block, minb = t->n2->min_blocks;
-  auto kern = n2_kernel<256, NCH, 1>;
-  if (block == 128) kern = minb >= 2 ? n2_kernel<128, NCH, 4> : n2_kernel<128, NCH, 1>;
-  else if (minb >= 2) kern = n2_kernel<256, NCH, 2>;
+  auto kern = mix ? n2_kernel<256, NCH, 1, true> : n2_kernel<256, NCH, 1, false>;
+  if (block == 128)
+    kern = minb >= 2 ? (mix ? n2_kernel<128, NCH, 4, true> : n2_kernel<128, NCH, 4, false>)
+                     : (mix ? n2_kernel<128, NCH, 1, true> : n2_kernel<128, NCH, 1, false>);
+  else if (minb >= 2)
+    kern = mix ? n2_kernel<256, NCH, 2, true> : n2_kernel<256, NCH, 2, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (n2)");
@@ -1353,16 +1390,16 @@ namespace cbk {
 
 int n2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
             const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
-            cudaStream_t stream) {
+            cudaStream_t stream, bool mix) {
   int rc = build_plan(t);
   if (rc) return rc;
   const StepCoef k = step_coef(dt);
   if (t->t.nch == 2)
     return launch_n2<2>(t, state_in, state_out, control, k, n_steps, world_status,
-                        accepted_steps, stream);
+                        accepted_steps, stream, mix);
   if (t->t.nch == 0)
     return launch_n2<0>(t, state_in, state_out, control, k, n_steps, world_status,
-                        accepted_steps, stream);
+                        accepted_steps, stream, mix);
   return fail(CB_ERR_UNSUPPORTED, "channel slots must be 0 or 2");
 }
 

@@ -150,6 +150,12 @@ enum cb_control_field {
  * order and elimination-tree levels bound on the host at the first N2 step; left-looking by
  * levels on the device, one CTA per world). FP64. */
 #define CB_METHOD_N2 2
+/* N2 with its operator factored and substituted in FP32, the stage potentials recovered by FP64
+ * iterative refinement of the charge residual against the FP64 operator (corrections until every
+ * row is within 1e-3 of the stage's acceptance bound, at most 6); rates, slopes and every
+ * accumulation in FP64 (this library's cells_b200.solver.imex_ars222_implicit_conductances_
+ * mixed@1; no reference method). */
+#define CB_METHOD_N2_MIXED 3
 
 /*
  * Host symbolic bind (replaces initial_values' layout binding, surface_tissue.py:135-257 and

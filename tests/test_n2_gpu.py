@@ -148,3 +148,39 @@ def test_n2_steps_where_the_explicit_step_is_refused_as_stiff(cuda):
         assert ok.all()
     for f, ref in oracle_state(st).items():
         assert scaled_difference(got[f], ref) <= TOL, f
+
+
+@pytest.mark.parametrize("name", ["n2_grid4x4.npz", "n2_channels_delaunay.npz"])
+def test_mixed_n2_matches_the_reference_trajectory(cuda, name):
+    """CB_METHOD_N2_MIXED (FP32 factor and substitutions, FP64 refinement of the stage charge
+    residual): the reference's N2 trajectories within the FP64 tolerance."""
+    z, b = load_golden(name)
+    tissue = Tissue(b)
+    control = tissue.pack_control(**{f: z["control_" + f] for f in
+                                     ("membrane", "junction", "pump", "channel")
+                                     if "control_" + f in z.files})
+    state, done, worst = tissue.initial_state(), 0, {}
+    for idx, target in enumerate(z["steps"]):
+        if target > done:
+            state, status, _ = run_n2(cuda, tissue, state, control, float(z["dt"]),
+                                      [int(target - done)], method=_lib.METHOD_N2_MIXED)
+            assert np.all(status == 0), decode_status(status[0])
+            done = int(target)
+        for f in T.State._fields:
+            if "ref_" + f in z.files:
+                worst[f] = max(worst.get(f, 0.0), scaled_difference(state[f], z["ref_" + f][idx]))
+    bad = {k: v for k, v in worst.items() if v > TOL}
+    assert not bad, bad
+
+
+def test_mixed_n2_matches_fp64_n2_on_uneven_worlds(cuda):
+    b, rng = uneven_batch(45)
+    tissue = Tissue(b)
+    control = tissue.pack_control(rng.uniform(0.6, 1, b.cells), rng.uniform(0.6, 1, b.edges),
+                                  rng.uniform(0.6, 1, b.cells), rng.uniform(0.4, 1, (2, b.cells)))
+    fp64, s1, _ = run_n2(cuda, tissue, tissue.initial_state(), control, 1e-3, [60])
+    mixed, s2, _ = run_n2(cuda, tissue, tissue.initial_state(), control, 1e-3, [60],
+                          method=_lib.METHOD_N2_MIXED)
+    assert np.all(s1 == 0) and np.all(s2 == 0)
+    bad = {f: d for f in fp64 if (d := scaled_difference(mixed[f], fp64[f])) > TOL}
+    assert not bad, bad
