@@ -1199,14 +1199,18 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
   const bool packed_ok = packed_smem_bytes(cap) <= kMaxSmemPerBlock;
   t->shared_ok = shared_ok;
   if (!rc && packed_ok) {
-    // Work items: runs of consecutive worlds of at most `cap` cells and kPackedMaxWorlds worlds,
-    // queued largest first.
+    // Work items: runs of consecutive worlds of at most `target` cells (a larger world is an item
+    // of its own, up to `cap`) and kPackedMaxWorlds worlds, queued largest first. The target sets
+    // how many cells the running items hold at once, and so whether their scratch stays in L2.
+    long long target = std::min<long long>(cap, 1024);  // measured best of 512..4096
+    if (const char *env = std::getenv("CELLS_B200_ITEM_CELLS"))
+      target = std::max(32LL, std::min<long long>(cap, std::atoll(env)));
     std::vector<int> item_world0{0}, cell_world(C), isnd(E), ircv(E), iadj(adj_idx.size());
     long long cells_in = 0;
     int worlds_in = 0;
     for (int w = 0; w < W; ++w) {
       const long long nc = d->cell_offset[w + 1] - d->cell_offset[w];
-      if (worlds_in > 0 && (cells_in + nc > cap || worlds_in == kPackedMaxWorlds)) {
+      if (worlds_in > 0 && (cells_in + nc > target || worlds_in == kPackedMaxWorlds)) {
         item_world0.push_back(w);
         cells_in = 0;
         worlds_in = 0;
