@@ -33,6 +33,9 @@ Fixtures:
                          junctions, partial controls, a -4 mV bath, under N2, 200 steps.
   pytrees_n2_padded.npz  That world's @3 pytrees under N2 (capacities 2 above the counts, 40
                          steps), for the drop-in step.
+  device_checks.npz      The reference's accepted-row device checks (@3) on rows of its own
+                         trajectory of a 36-cell gated Delaunay world with channels: accepted
+                         rows after 1-120 steps and two planted faults (failed bits, values).
   laws.npz               Point laws on grids of inputs: bernoulli, the pump kinetics and the
                          junction gate rate.
 """
@@ -336,6 +339,68 @@ def make_n2_trajectories():
     print("pytrees_n2_padded.npz written")
 
 
+def make_checks():
+    """The reference's accepted-row device checks (@3's device_checks: surface_pump_checks
+    .row_checks with its balances, magnitudes and ledger limits) on rows of its own trajectory
+    of a gated Delaunay world with NaV1.2 and Kv1.5 populations: accepted rows at several step
+    counts, and rows with planted faults (a material error, a heat that decreases)."""
+    from cells.definitions.specs import parse_spec
+    from cells.definitions.surface_pump_v3_spec import control_values
+    from cells.registry.models import get_model
+
+    from cells_b200 import worlds
+
+    ars = "cells.solver.imex_ars222_face_electromigration@1"
+    v3 = "cells.model.resolved_pump_tissue@3"
+    rng = np.random.default_rng(41)
+    world = worlds.with_channels(
+        worlds.delaunay_world(36, worlds.world_rng(6, 0), junction_sigma=0.3,
+                              gate=(0.02, 0.1, 0.8)), rng,
+        na=("nav", 4e-10, 0.4), k=("kv", 5e-10, 0.6), sigma=0.3)
+    world.bath_potential = -0.004
+    raw = worlds.reference_definition(world, dt=1e-3, steps=120, model=v3, solver=ars)
+    spec = parse_spec(raw)
+    model = get_model(spec.model)
+    state, p = model.initial_values(spec)
+    cv = control_values(spec, [0.0])
+    control = type(cv)(*(v[0] for v in cv))
+    constants = model.device_check_constants(spec)
+    rows = {0: state}
+    for k in range(1, 121):
+        state, ok = model.imex_step(state, 1e-3, control, p, xp=np)[:2]
+        assert bool(ok)
+        rows[k] = state
+    cases = []
+    for k in (1, 2, 10, 60, 120):
+        cases.append((rows[k - 1], rows[k], k, "accepted"))
+    bad = rows[60]._replace(amount_increment=np.asarray(rows[60].amount_increment).copy())
+    bad.amount_increment[1, 3] += 1e-8  # 500 x the 2e-11 fmol material tolerance
+    cases.append((rows[59], bad, 60, "material"))
+    heat = rows[60]._replace(
+        junction_dissipated_energy_pJ=np.asarray(rows[59].junction_dissipated_energy_pJ) - 1e-9)
+    cases.append((rows[59], heat, 60, "dissipation"))
+    out = {}
+    for i, (prev, row, k, label) in enumerate(cases):
+        failed, values = model.device_checks(prev, row, p, constants, k)
+        for tag, st in (("prev", prev), ("row", row)):
+            packed = _state_to_packed(st)
+            packed.update(_channels_to_packed(st, world))
+            for f, v in packed.items():
+                out[f"case{i}_{tag}_{f}"] = v
+        out[f"case{i}_steps"] = np.asarray(k)
+        out[f"case{i}_label"] = np.asarray(label)
+        out[f"case{i}_failed"] = np.asarray(failed)
+        out[f"case{i}_values"] = np.asarray(values)
+    out["cases"] = np.asarray(len(cases))
+    out["material_atol"] = np.asarray(constants.material_atol)
+    out["energy_rtol"] = np.asarray(constants.energy_rtol)
+    out["checks"] = np.asarray(model.DEVICE_CHECKS)
+    out["diagnostics"] = np.asarray(model.DEVICE_DIAGNOSTICS)
+    np.savez_compressed(os.path.join(HERE, "device_checks.npz"), **_batch_arrays(
+        worlds.pack([world])), **out)
+    print("device_checks.npz written:", [c[3] for c in cases])
+
+
 def make_laws():
     from cells.laws import electrochemistry as ec
     from cells.laws.junctions import junction_voltage_relaxation as jg
@@ -374,7 +439,7 @@ def make_laws():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("laws", "trajectories", "channels", "n2"))
+    ap.add_argument("--only", choices=("laws", "trajectories", "channels", "n2", "checks"))
     args = ap.parse_args()
     _setup(args.reference)
     if args.only in (None, "laws"):
@@ -385,6 +450,8 @@ def main():
         make_channel_trajectories()
     if args.only in (None, "n2"):
         make_n2_trajectories()
+    if args.only in (None, "checks"):
+        make_checks()
 
 
 if __name__ == "__main__":
