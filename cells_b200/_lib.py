@@ -64,6 +64,7 @@ EXPORTS = (
     "cb_step_vjp",
     "cb_vjp_workspace",
     "cb_set_permeability",
+    "cb_device_checks",
     "cb_last_error",
     "cb_version",
 )
@@ -160,6 +161,8 @@ def load(path=LIBRARY):
     lib.cb_vjp_workspace.restype = ctypes.c_int
     lib.cb_set_permeability.argtypes = [_p, _p, _p, _p, _p]
     lib.cb_set_permeability.restype = ctypes.c_int
+    lib.cb_device_checks.argtypes = [_p, _p, _p, ctypes.c_int64, _d, ctypes.c_double, _p, _p, _p]
+    lib.cb_device_checks.restype = ctypes.c_int
     lib.cb_last_error.argtypes = []
     lib.cb_last_error.restype = ctypes.c_char_p
     lib.cb_version.argtypes = []

@@ -11,6 +11,8 @@ This mirrors the reference's model-module protocol for the resolved pump-leak ti
 * ``checked_step(...)``        ~ ``checked_step(state, dt, control, p, active) -> (state, valid)``
   with host arrays (cb_step_host), one step.
 * ``Tissue.balances(...)``     ~ ``balances(state, p)``'s residuals (cb_balances).
+* ``Tissue.device_checks(...)`` ~ @3's ``device_checks(previous, row, p, constants, steps)``
+  (surface_pump_v3.py:5572-5597): the accepted-row checks, bitmask and diagnostics per world.
 * ``Tissue.step_vjp(...)``     ~ ``jax.vjp`` of ``checked_step`` repeated ``n_steps`` times
   (cb_step_vjp); ``Tissue.set_permeability`` rebinds the permeabilities on the device.
 
@@ -34,6 +36,15 @@ CELL = ("amount_increment", "membrane_transferred", "membrane_dissipated", "pump
         "pump_dissipated", "metabolic_work")
 EDGE = ("junction_transferred", "junction_dissipated", "junction_gate")
 WORLD = ("reservoir_supplied", "electrode_charge", "reservoir_work", "electrode_work")
+# cb_device_checks' bits and diagnostics, in the reference's DEVICE_CHECKS and DEVICE_DIAGNOSTICS
+# order (models/surface_pump_v3.py, device_checks).
+CHECKS = ("domain", "local", "outside", "total", "charge", "electrode", "global_charge", "energy",
+          "reservoir_work", "electrode_work", "metabolic_work", "dissipation")
+DIAGNOSTICS = tuple("max_" + k for k in (
+    "balance_error_fmol", "extracellular_balance_error_fmol", "global_balance_error_fmol",
+    "capacitor_charge_error_C", "electrode_charge_error_C", "global_charge_error_C",
+    "energy_balance_error_pJ", "reservoir_work_error_pJ", "electrode_work_error_pJ",
+    "metabolic_work_error_pJ", "energy_balance_relative", "global_charge_bound_ratio"))
 
 
 def _ptr(a, ctype=ctypes.c_double):
@@ -227,6 +238,19 @@ class Tissue:
         _lib.check(self.lib.cb_balances(
             self.handle, ctypes.c_void_p(state_dev.data_ptr()),
             ctypes.c_void_p(out_dev.data_ptr()),
+            None if stream is None else ctypes.c_void_p(stream),
+        ))  # fmt: skip
+
+    def device_checks(self, previous_dev, row_dev, steps, material_atol, energy_rtol, failed_dev,
+                      values_dev, stream=None):
+        """cb_device_checks: the accepted-row checks of row_dev against previous_dev (packed
+        float64 device states); failed_dev [W] int32 receives each world's bitmask (bit k:
+        CHECKS[k] failed), values_dev [W*12] float64 the diagnostics."""
+        atol = (ctypes.c_double * 3)(*np.broadcast_to(np.asarray(material_atol, float), 3))
+        _lib.check(self.lib.cb_device_checks(
+            self.handle, ctypes.c_void_p(previous_dev.data_ptr()),
+            ctypes.c_void_p(row_dev.data_ptr()), int(steps), atol, float(energy_rtol),
+            ctypes.c_void_p(failed_dev.data_ptr()), ctypes.c_void_p(values_dev.data_ptr()),
             None if stream is None else ctypes.c_void_p(stream),
         ))  # fmt: skip
 

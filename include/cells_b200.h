@@ -11,6 +11,8 @@
  *                                                   surface_pump_v3.py:3989 -> imex_step :3547)
  *   balances(state, p)                            ~ cb_balances       (surface_tissue.py:536-611,
  *                                                                      surface_kinetic.py:470-482)
+ *   device_checks(prev, row, p, constants, steps) ~ cb_device_checks (surface_pump_v3.py:5572,
+ *                                                                      surface_pump_checks.py:101)
  *
  * Worlds are packed back to back (see cells_b200/worlds.py): world w owns cells
  * cell_offset[w] .. cell_offset[w+1]-1 and junctions edge_offset[w] .. edge_offset[w+1]-1.
@@ -201,6 +203,24 @@ int cb_step_host(cb_tissue *t, int method, const double *state_in, double *state
  * 5 reservoir work (pJ), 6 electrode work (pJ), 7 metabolic work (pJ).
  */
 int cb_balances(cb_tissue *t, const double *state, double *out, void *stream);
+
+/*
+ * The accepted-row checks of one row against its predecessor (DEVICE pointers; replaces @3's
+ * device_checks, models/surface_pump_v3.py:5572-5597, which evaluates
+ * models/surface_pump_checks.row_checks :101-192 on the device). steps is the number of steps
+ * accepted up to row (the rounding allowance of every ledger is 2.5 eps x steps x the magnitudes
+ * rounded into it, surface_pump.ledger_limits :752-800); material_atol [3] (HOST, fmol per
+ * species) and energy_rtol are the solver's tolerances (@3's device_check_constants).
+ * failed [W]: bit k set when check k failed, in the order 0 domain, 1 local material,
+ * 2 bath material, 3 world total material, 4 capacitor charge, 5 electrode charge,
+ * 6 global charge, 7 energy, 8 reservoir work, 9 electrode work, 10 metabolic work,
+ * 11 dissipation (negative, or decreasing since previous). values [W*12]: the max |residual| of
+ * the ten ledgers in that order (fmol, C, pJ), then the energy residual over its flows and the
+ * global-charge residual over its bound (DEVICE_DIAGNOSTICS).
+ */
+int cb_device_checks(cb_tissue *t, const double *previous, const double *row, int64_t steps,
+                     const double *material_atol, double energy_rtol, uint32_t *failed,
+                     double *values, void *stream);
 
 /*
  * cb_step for a handle bound for the packed kernel, with the kernel's scratch (stage
