@@ -30,6 +30,24 @@ def load_golden(name):
     return z, batch
 
 
+def load_field_golden(name):
+    """(npz, FieldWorld) of one field fixture (tests/golden/make_golden.py, field_*.npz)."""
+    from cells_b200 import field_worlds
+
+    z = np.load(os.path.join(GOLDEN, name))
+    values = {}
+    for f in fields(field_worlds.FieldWorld):
+        v = z["fw_" + f.name]
+        if f.name in ("side", "cells_side", "stride"):
+            v = int(v)
+        elif f.name in ("face_area", "face_length", "temperature"):
+            v = float(v)
+        elif f.name == "pump":
+            v = tuple(float(x) for x in v)
+        values[f.name] = v
+    return z, field_worlds.FieldWorld(**values)
+
+
 def scaled_difference(a, b):
     """max |a - b| / max(|a|, |b|) over a field: the reference's own trajectory comparison
     (tests/unit/test_surface_pump_v3_imex.py:45-48)."""

@@ -36,6 +36,11 @@ Fixtures:
   device_checks.npz      The reference's accepted-row device checks (@3) on rows of its own
                          trajectory of a 36-cell gated Delaunay world with channels: accepted
                          rows after 1-120 steps and two planted faults (failed bits, values).
+  field_grid10.npz       A 10x10 extracellular grid (held ring) with a 3x3 tissue, @1 ARS(2,2,2)
+                         with face electromigration and the factored field, 400 steps at 0.5 ms.
+  field_gated14.npz      A 14x14 grid with a 4x4 gated tissue (log-normal junctions), partial
+                         controls, 200 steps.
+  field_grid24.npz       A 24x24 grid with a 6x6 tissue, 60 steps.
   laws.npz               Point laws on grids of inputs: bernoulli, the pump kinetics and the
                          junction gate rate.
 """
@@ -436,10 +441,88 @@ def make_laws():
     print("laws.npz written")
 
 
+FIELD_NAMES = dict(
+    amount_increment="amount_increment", extracellular_increment="extracellular_amount_increment",
+    membrane_transferred="membrane_transferred", junction_transferred="junction_transferred",
+    face_transferred="face_transferred", reservoir_supplied="reservoir_supplied",
+    membrane_dissipated="membrane_dissipated_energy_pJ",
+    junction_dissipated="junction_dissipated_energy_pJ",
+    face_dissipated="face_dissipated_energy_pJ", electrode_charge="electrode_charge_transferred_C",
+    reservoir_work="reservoir_work_pJ", electrode_work="electrode_work_pJ",
+    junction_gate="junction_gate", pump_cycles="pump_cycles",
+    pump_dissipated="pump_dissipated_energy_pJ", metabolic_work="metabolic_work_pJ",
+)
+
+
+def _field_world_arrays(world):
+    from dataclasses import fields
+
+    return {"fw_" + f.name: np.asarray(getattr(world, f.name)) for f in fields(world)
+            if f.name != "pump"} | {"fw_pump": np.asarray(world.pump)}
+
+
+def _run_field(name, world, *, dt, steps, keep, controls=None):
+    """The reference's own step (@1, ARS(2,2,2) face electromigration, factored field) on one
+    field world, its states at the keep steps in the oracle's field names."""
+    from cells.definitions.specs import parse_spec
+    from cells.execution.schedule import control_values
+    from cells.registry.models import get_model
+
+    from cells_b200 import field_worlds
+
+    controls = controls or {}
+    raw = field_worlds.reference_definition(world, dt=dt, steps=steps, **controls)
+    spec = parse_spec(raw)
+    model = get_model(spec.model)
+    state, p = model.initial_values(spec)
+    cv = control_values(spec, [0.0])
+    control = type(cv)(*(v[0] for v in cv))
+    assert np.array_equal(np.asarray(p.face_factor), world.face_factor)
+    snaps = []
+    t0 = time.time()
+    for k in range(steps + 1):
+        if k:
+            state, ok = model.imex_step(state, dt, control, p, xp=np)[:2]
+            if not bool(ok):
+                raise RuntimeError(f"reference refused step {k}")
+        if k in keep:
+            snaps.append({f: np.asarray(getattr(state, r)) for f, r in FIELD_NAMES.items()})
+    out = _field_world_arrays(world)
+    out.update({"control_" + k: np.asarray(v) for k, v in
+                (("membrane", control.membrane), ("junction", control.junction),
+                 ("pump", control.pump))})
+    out["dt"], out["steps"] = np.asarray(dt), np.asarray(sorted(keep))
+    for f in FIELD_NAMES:
+        out["ref_" + f] = np.stack([s[f] for s in snaps])
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(f"{name} written ({steps} steps, {time.time() - t0:.1f} s)")
+
+
+def make_field_trajectories():
+    """Field worlds (cells facing a resolved extracellular grid with a held ring)."""
+    from cells_b200 import field_worlds as FW
+    from cells_b200 import worlds
+
+    w = FW.field_world(10, 3, 2, worlds.world_rng(11, 0))
+    _run_field("field_grid10.npz", w, dt=5e-4, steps=400,
+               keep={0, 1, 2, 5, 10, 50, 100, 200, 400})
+    rng = np.random.default_rng(12)
+    w = FW.field_world(14, 4, 3, worlds.world_rng(12, 0), gate=(0.015, 0.2, 1.0),
+                       junction_sigma=0.3)
+    controls = dict(membrane_control=rng.uniform(0.6, 1.0, w.cells),
+                    junction_control=rng.uniform(0.6, 1.0, w.edges),
+                    pump_control=rng.uniform(0.6, 1.0, w.cells))
+    _run_field("field_gated14.npz", w, dt=5e-4, steps=200, keep={0, 1, 3, 20, 100, 200},
+               controls=controls)
+    w = FW.field_world(24, 6, 3, worlds.world_rng(13, 0))
+    _run_field("field_grid24.npz", w, dt=5e-4, steps=60, keep={0, 1, 10, 60})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("laws", "trajectories", "channels", "n2", "checks"))
+    ap.add_argument("--only", choices=("laws", "trajectories", "channels", "n2", "checks",
+                                       "field"))
     args = ap.parse_args()
     _setup(args.reference)
     if args.only in (None, "laws"):
@@ -452,6 +535,8 @@ def main():
         make_n2_trajectories()
     if args.only in (None, "checks"):
         make_checks()
+    if args.only in (None, "field"):
+        make_field_trajectories()
 
 
 if __name__ == "__main__":
