@@ -49,7 +49,15 @@ WORLD_BITS = {
     128: "channel_domain",
     256: "ledger_cotangent",
     512: "operator",
+    1024: "field",
 }
+# Field worlds (cb_field_*): state fields in CB_FIELD_* order.
+FIELD_STATE_FIELDS = (
+    "amount_increment", "extracellular_increment", "membrane_transferred",
+    "junction_transferred", "face_transferred", "reservoir_supplied", "membrane_dissipated",
+    "junction_dissipated", "face_dissipated", "electrode_charge", "reservoir_work",
+    "electrode_work", "junction_gate", "pump_cycles", "pump_dissipated", "metabolic_work",
+)
 EXPORTS = (
     "cb_bind",
     "cb_free",
@@ -65,6 +73,12 @@ EXPORTS = (
     "cb_vjp_workspace",
     "cb_set_permeability",
     "cb_device_checks",
+    "cb_field_bind",
+    "cb_field_free",
+    "cb_field_state_layout",
+    "cb_field_control_length",
+    "cb_field_step",
+    "cb_field_step_host",
     "cb_last_error",
     "cb_version",
 )
@@ -107,6 +121,42 @@ class TissueDesc(ctypes.Structure):
         ("channel_species", _i32),
         ("channel_permeability", _d),
         ("channel_abundance", _d),
+    ]
+
+
+class FieldDesc(ctypes.Structure):
+    """cb_field_desc (include/cells_b200.h)."""
+
+    _fields_ = [
+        ("worlds", ctypes.c_int32),
+        ("cells", ctypes.c_int32),
+        ("nodes", ctypes.c_int32),
+        ("junctions", ctypes.c_int32),
+        ("faces", ctypes.c_int32),
+        ("cell_node", _i64),
+        ("junction_sender", _i64),
+        ("junction_receiver", _i64),
+        ("face_sender", _i64),
+        ("face_receiver", _i64),
+        ("reservoir", ctypes.POINTER(ctypes.c_uint8)),
+        ("temperature", _d),
+        ("pump", _d),
+        ("volume", _d),
+        ("area", _d),
+        ("capacitance", _d),
+        ("permeability", _d),
+        ("pump_capacity", _d),
+        ("amount", _d),
+        ("initial_charge", _d),
+        ("junction_area", _d),
+        ("junction_permeability", _d),
+        ("gate_threshold", _d),
+        ("gate_minimum", _d),
+        ("outside_volume", _d),
+        ("outside_amount", _d),
+        ("outside_charge", _d),
+        ("boundary_V", _d),
+        ("face_factor", _d),
     ]
 
 
@@ -163,6 +213,19 @@ def load(path=LIBRARY):
     lib.cb_set_permeability.restype = ctypes.c_int
     lib.cb_device_checks.argtypes = [_p, _p, _p, ctypes.c_int64, _d, ctypes.c_double, _p, _p, _p]
     lib.cb_device_checks.restype = ctypes.c_int
+    lib.cb_field_bind.argtypes = [ctypes.POINTER(FieldDesc), ctypes.c_int, ctypes.POINTER(_p)]
+    lib.cb_field_bind.restype = ctypes.c_int
+    lib.cb_field_free.argtypes = [_p]
+    lib.cb_field_free.restype = None
+    lib.cb_field_state_layout.argtypes = [_p, _i64, _i64]
+    lib.cb_field_state_layout.restype = ctypes.c_int
+    lib.cb_field_control_length.argtypes = [_p]
+    lib.cb_field_control_length.restype = ctypes.c_int64
+    lib.cb_field_step.argtypes = [_p, _p, _p, ctypes.c_double, _p, ctypes.c_int, _p, _p, _p]
+    lib.cb_field_step.restype = ctypes.c_int
+    lib.cb_field_step_host.argtypes = [_p, _d, _d, ctypes.c_double, _d, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_uint32), _i32]
+    lib.cb_field_step_host.restype = ctypes.c_int
     lib.cb_last_error.argtypes = []
     lib.cb_last_error.restype = ctypes.c_char_p
     lib.cb_version.argtypes = []

@@ -1,0 +1,1317 @@
+// field_step.cu - the resolved-field step (cb_field_*): tissues whose cells face a resolved
+// extracellular grid with held boundary nodes, ARS(2,2,2) with implicit face electromigration.
+//
+// Reference: models/surface_pump.py:158-369 (explicit_rates, implicit_rates, imex_step) with the
+// field closure numerics/surface_field.py:253-855 (bind, _capacitor_solve, the damped Newton on
+// the floating offsets) and the face operator numerics/surface_imex.py:123-278 (face_weights,
+// drift_flux, face_laplacian, factor_operator, solve_operator); transport and logmean of
+// numerics/surface_transport.py:298-386 and numerics/extracellular_field.py:48-62.
+//
+// Algebra. Each cell's one membrane faces a free outside node, so a cell and its node form one
+// capacitor component and every other free node is a component of its own. Eliminating each cell
+// into its node (C (phi_c - phi_m) = q_c) leaves, on the free nodes:
+//   start field   currents balance: sum of face and junction currents out of each component = 0,
+//                 with phi_c = phi_m + q_c / C_c. Face currents are affine in the potentials at
+//                 the step start's concentrations; junction currents are the constant-field law.
+//                 Solved as the reference's Newton (initial solve with the face conductances, then
+//                 corrections with a backtracking line search and its acceptance: max residual
+//                 down, or within NEWTON_TARGET of the current scale), with the face Laplacian as
+//                 the Newton matrix throughout (a chord: the junction slopes, five orders below the
+//                 face conductances, are left out of the matrix, not out of the residual).
+//   stage solve   gamma dt L(W) phi = q_m + q_c on the free nodes, the held nodes' potentials on
+//                 the right, W the face weights at the half-step prediction.
+// Both matrices are the face conductance Laplacian of the free nodes: one sparse pattern for
+// every world, ordered by nested dissection of the grid (or minimum degree for other graphs),
+// factored left-looking by the elimination tree's levels (a warp per column).
+//
+// One CTA advances one world n_steps steps; its vectors, rates and factor live in a global scratch
+// slice of its own.
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cells_b200.h"
+#include "handle.h"
+#include "sparse_plan.h"
+
+namespace {
+
+using namespace cbk;
+
+constexpr double kNewtonTarget = 0.01;   // surface_field.NEWTON_TARGET
+constexpr double kCurrentAtol = 1e-23;   // CURRENT_ATOL_A
+constexpr double kCurrentRtol = 2e-12;   // CURRENT_RTOL
+constexpr int kMaxIterations = 16;       // solve's max_iterations
+constexpr int kMaxBacktracks = 12;       // max_backtracks
+constexpr int kFieldBlock = 512;
+constexpr int kRefineRounds = 1;         // FP64 refinement rounds of each stage solve
+constexpr double kChargeAtol = 3e-25;    // surface_field.CHARGE_ATOL_C
+constexpr double kChargeRtol = 2e-12;    // CHARGE_RTOL
+
+enum FieldWorldConst {
+  FW_T = 0, FW_RT, FW_FRT, FW_INVRT, FW_DRIVE, FW_LOGKMK, FW_LATP, FW_LOGKMNA, FW_AFF0,
+  FW_PUMPOK, FW_INVRTD, FW_STRIDE
+};
+
+struct Topo {  // shared by every world
+  int N, O, E, F, U, levels;
+  const int *cell_node;  // [N]
+  const int *ncell;      // [O] the cell facing the node, or -1
+  const int *upos;       // [O] the node's unknown (factor column), or -1 when held
+  const int *nf_ptr, *nf_idx;  // node -> faces, face order: f << 1 | (1 when the receiver)
+  const int *cj_ptr, *cj_idx;  // cell -> junctions, edge order: e << 1 | (1 when the receiver)
+  const int *fs, *fr;    // [F]
+  const int *js, *jr;    // [E]
+  const int *face_pos;   // [F] off-diagonal factor entry of a face between free nodes, or -1
+  const int *colp, *lrow, *ukp, *ukc, *ukpos, *ukrel, *rel, *lvp, *lvc;
+};
+
+struct Params {  // per world, world-major
+  const double *wc;      // [W][FW_STRIDE]
+  const double *vol, *icap, *q0, *pcap, *logpcap;  // [W*N]
+  const double *ref, *ap;                          // [3][W*N]
+  const double *jap;                               // [3][W*E]
+  const double *thr, *jmin;                        // [W*E]
+  const double *ovol, *q0o, *vb;                   // [W*O]
+  const double *oref;                              // [3][W*O]
+  const double *ff;                                // [3][W*F] D A / L
+  long long WN, WO, WE, WF;
+};
+
+struct FLayout {
+  long long s[CB_FIELD_STATE_FIELDS];
+};
+
+// Scratch fields of one world, in doubles (offsets from the world's slice).
+struct Scratch {
+  long long lval, x, xt, dx, r, rt, y, phi, pc, co, lco, ci, lci, fm, ld, wp, ifc, ijc, k0, k1,
+      d1, d2, n1, o1, g1, cp, stride;
+  // a rate block: cell amount [3N], membrane transferred [3N], md, cycles, pd, mw [N each],
+  // junction transferred [3E], jd, gate [E each], face diffusion [3F], node extracellular [3O],
+  // node supply [3O], the outward pump transfer "extra" [3N]
+  long long rk_n, rk_mt, rk_md, rk_cy, rk_pd, rk_mw, rk_jt, rk_jd, rk_g, rk_fd, rk_x, rk_s, rk_ex,
+      rk_size;
+};
+
+__device__ __forceinline__ void logmean(double l, double r, double &mean, double &lg) {
+  // extracellular_field.logmean (:48-62)
+  const double middle = 0.5 * l + 0.5 * r;
+  const double difference = l - r;
+  const double ratio = (0.5 * difference) / middle;
+  const bool near = fabs(ratio) < 0.5;
+  lg = near ? 2.0 * atanh(ratio) : log(l) - log(r);
+  if (fabs(ratio) < 1e-4) {
+    const double sq = ratio * ratio;
+    mean = middle * ((1.0 - sq / 3.0) - 4.0 * sq * sq / 45.0);
+  } else {
+    mean = difference / lg;
+  }
+}
+
+template <int BLOCK>
+__device__ __forceinline__ double block_max_abs(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double m = red[0];
+  for (int q = 1; q < BLOCK / 32; ++q) m = fmax(m, red[q]);
+  return m;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ unsigned block_or(unsigned v, unsigned *red) {
+  for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  unsigned m = 0;
+  for (int q = 0; q < BLOCK / 32; ++q) m |= red[q];
+  return m;
+}
+
+// Constant-field route flux of species s (z = +1 for Na, K; -1 for Cl), selective_flux with
+// residual 0 and gate 1: g (c_from B(-x) - c_to B(x)) for z = +1, the pair swapped for z = -1.
+__device__ __forceinline__ double ghk(int s, double g, double cf, double ct, double bp,
+                                      double bm) {
+  return s < 2 ? g * (cf * bm - ct * bp) : g * (cf * bp - ct * bm);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1)
+    field_kernel(const Topo T, const Params P, const FLayout L, const Scratch S,
+                 double *__restrict__ state, const double *__restrict__ control, const StepCoef k,
+                 int n_steps, uint32_t *__restrict__ status, int32_t *__restrict__ taken_out,
+                 double *__restrict__ scratch) {
+  __shared__ double sRed[BLOCK / 32];
+  __shared__ unsigned sBits[BLOCK / 32];
+  constexpr int WARPS = BLOCK / 32;
+  const int w = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int N = T.N, O = T.O, E = T.E, F = T.F, U = T.U;
+  const long long WN = P.WN, WO = P.WO, WE = P.WE, WF = P.WF;
+  const long long c0 = (long long)w * N, o0 = (long long)w * O, e0 = (long long)w * E,
+                  f0 = (long long)w * F;
+  const double *wc = P.wc + (size_t)w * FW_STRIDE;
+  const double RT = wc[FW_RT], FRT = wc[FW_FRT], temp = wc[FW_T];
+  double *base = scratch + (size_t)w * S.stride;
+  double *lval = base + S.lval;
+  double *X = base + S.x, *XT = base + S.xt, *DX = base + S.dx, *Rv = base + S.r,
+         *RTv = base + S.rt, *Y = base + S.y;
+  double *PHI = base + S.phi, *PC = base + S.pc;
+  double *CO = base + S.co, *LCO = base + S.lco, *CI = base + S.ci, *LCI = base + S.lci;
+  double *FM = base + S.fm, *LD = base + S.ld, *WP = base + S.wp;
+  double *IFC = base + S.ifc, *IJC = base + S.ijc;
+  double *K0 = base + S.k0, *K1 = base + S.k1, *D1 = base + S.d1, *D2 = base + S.d2;
+  double *N1 = base + S.n1, *O1 = base + S.o1, *G1 = base + S.g1, *CP = base + S.cp;
+  const double *cm = control, *cj = control + WN, *cpmp = control + WN + WE;
+  auto st = [&](int f) { return state + L.s[f]; };
+  const double dt = k.dt;
+  const double omgamma_dt = (1.0 - (1.0 - 1.0 / sqrt(2.0))) * dt;  // (1 - gamma) dt
+  int taken = 0;
+  uint32_t refused = 0u;
+
+  // ---- sparse factor and substitutions on the shared plan --------------------------------
+  auto factor_column = [&](int j) -> unsigned {
+    unsigned bad = 0;
+    const int cjp = T.colp[j];
+    for (int u = T.ukp[j]; u < T.ukp[j + 1]; ++u) {
+      const int kk = T.ukc[u], p = T.ukpos[u], r0 = T.ukrel[u];
+      const int cnt = T.colp[kk + 1] - p;
+      const double ljk = lval[p];
+      for (int t = lane; t < cnt; t += 32) lval[cjp + T.rel[r0 + t]] -= lval[p + t] * ljk;
+      __syncwarp();
+    }
+    double piv = 0.0;
+    if (lane == 0) {
+      const double d = lval[cjp];
+      if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+      piv = sqrt(d);
+      lval[cjp] = piv;
+    }
+    piv = __shfl_sync(0xffffffffu, piv, 0);
+    const double inv = 1.0 / piv;
+    const int len = T.colp[j + 1] - cjp;
+    for (int t = 1 + lane; t < len; t += 32) lval[cjp + t] *= inv;
+    __syncwarp();
+    return bad;
+  };
+  auto factor = [&]() -> unsigned {
+    unsigned bad = 0;
+    for (int lv = 0; lv < T.levels; ++lv) {
+      const int a0 = T.lvp[lv], a1 = T.lvp[lv + 1];
+      for (int a = a0 + warp; a < a1; a += WARPS) bad |= factor_column(T.lvc[a]);
+      __syncthreads();
+    }
+    return block_or<BLOCK>(bad, sBits);
+  };
+  auto warp_sum = [&](double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  };
+  // L L^T x = y (y in Y by factor column, overwritten; x to the out vector by factor column).
+  auto solve = [&](double *out) {
+    for (int lv = 0; lv < T.levels; ++lv) {
+      const int a0 = T.lvp[lv], a1 = T.lvp[lv + 1];
+      for (int a = a0 + warp; a < a1; a += WARPS) {
+        const int j = T.lvc[a];
+        double part = 0.0;
+        for (int u = T.ukp[j] + lane; u < T.ukp[j + 1]; u += 32)
+          part += lval[T.ukpos[u]] * Y[T.ukc[u]];
+        part = warp_sum(part);
+        if (lane == 0) Y[j] = (Y[j] - part) / lval[T.colp[j]];
+      }
+      __syncthreads();
+    }
+    for (int lv = T.levels - 1; lv >= 0; --lv) {
+      const int a0 = T.lvp[lv], a1 = T.lvp[lv + 1];
+      for (int a = a0 + warp; a < a1; a += WARPS) {
+        const int j = T.lvc[a];
+        const int cjp = T.colp[j], len = T.colp[j + 1] - cjp;
+        double part = 0.0;
+        for (int t = 1 + lane; t < len; t += 32) part += lval[cjp + t] * out[T.lrow[cjp + t]];
+        part = warp_sum(part);
+        if (lane == 0) out[j] = (Y[j] - part) / lval[cjp];
+      }
+      __syncthreads();
+    }
+  };
+  // The face Laplacian with conductances g (a per-face functor) into the factor's storage.
+  auto assemble = [&](auto g) {
+    const long long nnz = T.colp[U];
+    for (long long a = tid; a < nnz; a += BLOCK) lval[a] = 0.0;
+    __syncthreads();
+    for (int m = tid; m < O; m += BLOCK) {
+      const int u = T.upos[m];
+      if (u < 0) continue;
+      double d = 0.0;
+      for (int a = T.nf_ptr[m]; a < T.nf_ptr[m + 1]; ++a) d += g(T.nf_idx[a] >> 1);
+      lval[T.colp[u]] = d;
+    }
+    for (int f = tid; f < F; f += BLOCK) {
+      const int p = T.face_pos[f];
+      if (p >= 0) lval[p] = -g(f);
+    }
+    __syncthreads();
+  };
+
+  // ---- transport pieces --------------------------------------------------------------------
+  // Concentrations and logs of a stage: cells from amounts n (functor (s, i)), nodes from o.
+  auto set_conc = [&](auto n, auto o) -> unsigned {
+    unsigned bits = 0;
+    for (int i = tid; i < N; i += BLOCK) {
+      const double v = P.vol[c0 + i];
+      for (int s = 0; s < 3; ++s) {
+        const double c = (P.ref[s * WN + c0 + i] + n(s, i)) / v;
+        if (!(is_finite(c) && c > 0.0)) bits |= CB_WORLD_TRANSPORT;
+        CI[s * N + i] = c;
+        LCI[s * N + i] = log(c);
+      }
+    }
+    for (int m = tid; m < O; m += BLOCK) {
+      const double v = P.ovol[o0 + m];
+      for (int s = 0; s < 3; ++s) {
+        const double c = (P.oref[s * WO + o0 + m] + o(s, m)) / v;
+        if (!(is_finite(c) && c > 0.0)) bits |= CB_WORLD_TRANSPORT;
+        CO[s * O + m] = c;
+        LCO[s * O + m] = log(c);
+      }
+    }
+    return bits;
+  };
+  // A junction's constant-field fluxes at voltage dv (opening = availability x gate).
+  auto junction_flux = [&](int e, double dv, double opening, double (&jj)[3], double (&mu)[3],
+                           unsigned &bits) {
+    const int a = T.js[e], b = T.jr[e];
+    const double x = dv * FRT;
+    if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
+    double bp, bm;
+    bernoulli_pair<double>(x, bp, bm);
+    for (int s = 0; s < 3; ++s) {
+      const double g = P.jap[s * WE + e0 + e] * opening;
+      jj[s] = ghk(s, g, CI[s * N + a], CI[s * N + b], bp, bm);
+      mu[s] = RT * (LCI[s * N + a] - LCI[s * N + b]) + ((s < 2) ? kF * dv : (-kF) * dv);
+    }
+  };
+  // A face's current (A) at potentials PHI with the step start's weights (transport's face
+  // expression: flux = factor mean mu / (RT 1e-15)).
+  auto face_current = [&](int f) {
+    const double dv = PHI[T.fs[f]] - PHI[T.fr[f]];
+    double cur = 0.0;
+    for (int s = 0; s < 3; ++s) {
+      const double z = s < 2 ? 1.0 : -1.0;
+      const double mu = RT * LD[s * F + f] + z * kF * dv;
+      const double flux = FM[s * F + f] * mu / (RT * 1e-15);
+      cur += z * flux;
+    }
+    return kChargePerFmol * cur;
+  };
+  // Explicit rates at a stage (surface_pump.explicit_rates): concentrations in CI/CO, cell
+  // potentials PC, node potentials PHI, gates g(e), into rate block K. Face diffusion uses the
+  // stage's own weights (W ln(a/b)).
+  auto explicit_rates = [&](double *Kb, auto gate) -> unsigned {
+    unsigned bits = 0;
+    double *kn = Kb + S.rk_n, *kmt = Kb + S.rk_mt, *kmd = Kb + S.rk_md, *kcy = Kb + S.rk_cy,
+           *kpd = Kb + S.rk_pd, *kmw = Kb + S.rk_mw, *kjt = Kb + S.rk_jt, *kjd = Kb + S.rk_jd,
+           *kg = Kb + S.rk_g, *kfd = Kb + S.rk_fd, *kx = Kb + S.rk_x, *ks = Kb + S.rk_s,
+           *kex = Kb + S.rk_ex;
+    for (int i = tid; i < N; i += BLOCK) {
+      const int m = T.cell_node[i];
+      const double dv = PC[i] - PHI[m];
+      const double x = dv * FRT;
+      if (!(fabs(x) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
+      double bp, bm;
+      bernoulli_pair<double>(x, bp, bm);
+      const double mc = cm[c0 + i], pcc = cpmp[c0 + i];
+      if (!(is_finite(mc) && mc >= 0.0 && mc <= 1.0 && is_finite(pcc) && pcc >= 0.0 &&
+            pcc <= 1.0))
+        bits |= CB_WORLD_CONTROL;
+      double jm[3], mu[3];
+      for (int s = 0; s < 3; ++s) {
+        const double g = P.ap[s * WN + c0 + i] * mc;
+        jm[s] = ghk(s, g, CI[s * N + i], CO[s * O + m], bp, bm);
+        mu[s] = RT * (LCI[s * N + i] - LCO[s * O + m]) + ((s < 2) ? kF * dv : (-kF) * dv);
+        kmt[s * N + i] = jm[s];
+      }
+      const double md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
+      kmd[i] = md;
+      if (!(is_finite(jm[0]) && is_finite(jm[1]) && is_finite(jm[2]) && is_finite(md)))
+        bits |= CB_WORLD_TRANSPORT;
+      // Na/K-ATPase: Na inside, K at the cell's node.
+      const double drive = wc[FW_DRIVE];
+      const double energy = (drive + (-3.0) * mu[0]) + 2.0 * mu[1];
+      const double a = energy * wc[FW_INVRT];
+      double cycles = 0.0;
+      const double cap = P.pcap[c0 + i];
+      if (cap > 0.0 && pcc > 0.0) {
+        const double lk = logaddexp0(2.0 * (wc[FW_LOGKMK] - LCO[O + m]));
+        const double ls = ((-logaddexp0(3.0 * (wc[FW_LOGKMNA] - LCI[i]))) - lk) - wc[FW_LATP];
+        const double mag = exp(((P.logpcap[c0 + i] + log(pcc)) + ls) + fmax(a, 0.0));
+        const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
+        cycles = mag * dep;
+      }
+      const double pd = (-1e-3 * cycles) * energy, mw = (-1e-3 * cycles) * drive;
+      kcy[i] = cycles;
+      kpd[i] = pd;
+      kmw[i] = mw;
+      kex[i] = 3.0 * cycles;
+      kex[N + i] = -2.0 * cycles;
+      kex[2 * N + i] = -0.0 * cycles;
+      const double sna = mu[0] * wc[FW_INVRTD], sk = mu[1] * wc[FW_INVRTD];
+      const double aff = (wc[FW_AFF0] + (-3.0) * sna) + 2.0 * sk;
+      if (!(wc[FW_PUMPOK] != 0.0 && is_finite(cap) && cap >= 0.0 && is_finite(sna) &&
+            fabs(sna) <= kMaxAbsIonPotentialOverRT && is_finite(sk) &&
+            fabs(sk) <= kMaxAbsIonPotentialOverRT && is_finite(aff) &&
+            fabs(aff) <= kMaxAbsAffinityOverRT))
+        bits |= CB_WORLD_PUMP_DOMAIN;
+      if (!(is_finite(cycles) && is_finite(pd) && is_finite(mw))) bits |= CB_WORLD_TRANSPORT;
+    }
+    for (int e = tid; e < E; e += BLOCK) {
+      const double g = gate(e);
+      const double dv = PC[T.js[e]] - PC[T.jr[e]];
+      const double jc = cj[e0 + e];
+      double jj[3], mu[3];
+      junction_flux(e, dv, jc * g, jj, mu, bits);
+      for (int s = 0; s < 3; ++s) kjt[s * E + e] = jj[s];
+      const double jd = 1e-3 * ((jj[0] * mu[0] + jj[1] * mu[1]) + jj[2] * mu[2]);
+      kjd[e] = jd;
+      const double thr = P.thr[e0 + e], mn = P.jmin[e0 + e];
+      double gr = 0.0;
+      if (mn < 1.0) {
+        const double shift = fabs(dv) - thr;
+        const double alpha = 1.3 * exp(-77.0 * shift);
+        const double log_beta = kLog0065 + 140.0 * shift;
+        const double beta = 20.0 * exp(-logaddexp0(-log_beta));
+        gr = alpha * (1.0 - g) - beta * (g - mn);
+      }
+      kg[e] = gr;
+      const bool gate_ok = is_finite(thr) && thr >= 0.0 && thr <= kMaxAbsJunctionV &&
+                           is_finite(mn) && mn >= 0.0 && mn <= 1.0 && is_finite(dv) &&
+                           fabs(dv) <= kMaxAbsJunctionV && is_finite(g) && g >= mn && g <= 1.0 &&
+                           is_finite(jc) && jc >= 0.0 && jc <= 1.0;
+      if (!gate_ok) bits |= CB_WORLD_GATE_DOMAIN;
+      if (!(is_finite(jj[0]) && is_finite(jj[1]) && is_finite(jj[2]) && is_finite(jd) &&
+            is_finite(gr)))
+        bits |= CB_WORLD_TRANSPORT;
+    }
+    for (int f = tid; f < F; f += BLOCK) {
+      const int a = T.fs[f], b = T.fr[f];
+      const double dv = PHI[a] - PHI[b];
+      if (!(fabs(dv * FRT) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
+      for (int s = 0; s < 3; ++s) {
+        double mean, lg;
+        logmean(CO[s * O + a], CO[s * O + b], mean, lg);
+        const double wgt = P.ff[s * WF + f0 + f] * mean / 1e-15;
+        const double d = wgt * (LCO[s * O + a] - LCO[s * O + b]);
+        kfd[s * F + f] = d;
+        if (!is_finite(d)) bits |= CB_WORLD_TRANSPORT;
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < N; i += BLOCK) {
+      double snd[3] = {0.0, 0.0, 0.0}, rcv[3] = {0.0, 0.0, 0.0};
+      for (int a = T.cj_ptr[i]; a < T.cj_ptr[i + 1]; ++a) {
+        const int code = T.cj_idx[a], e = code >> 1;
+        for (int s = 0; s < 3; ++s) {
+          if (code & 1) rcv[s] += kjt[s * E + e];
+          else snd[s] += -kjt[s * E + e];
+        }
+      }
+      for (int s = 0; s < 3; ++s) {
+        const double cell = ((-kmt[s * N + i]) + snd[s]) + rcv[s];
+        kn[s * N + i] = cell - kex[s * N + i];
+        if (!is_finite(kn[s * N + i])) bits |= CB_WORLD_TRANSPORT;
+      }
+    }
+    for (int m = tid; m < O; m += BLOCK) {
+      const int i = T.ncell[m];
+      const bool held = T.upos[m] < 0;
+      for (int s = 0; s < 3; ++s) {
+        double a = 0.0, out = 0.0, in = 0.0;
+        if (i >= 0) a = 0.0 + (kmt[s * N + i] + kex[s * N + i]);
+        for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
+          const int code = T.nf_idx[q];
+          if (code & 1) in += kfd[s * F + (code >> 1)];
+          else out += kfd[s * F + (code >> 1)];
+        }
+        const double inflow = (a - out) + in;
+        kx[s * O + m] = held ? 0.0 : inflow;
+        ks[s * O + m] = held ? -inflow : 0.0;
+      }
+    }
+    __syncthreads();
+    return bits;
+  };
+
+  for (int step = 0; step < n_steps && refused == 0u; ++step) {
+    unsigned bits = 0;
+    // ---- start concentrations, cell potentials relative to their nodes, face weights -------
+    bits |= set_conc([&](int s, int i) { return st(CB_FIELD_AMOUNT_INCREMENT)[s * WN + c0 + i]; },
+                     [&](int s, int m) {
+                       return st(CB_FIELD_EXTRACELLULAR_INCREMENT)[s * WO + o0 + m];
+                     });
+    __syncthreads();
+    for (int f = tid; f < F; f += BLOCK) {
+      const int a = T.fs[f], b = T.fr[f];
+      for (int s = 0; s < 3; ++s) {
+        double mean, lg;
+        logmean(CO[s * O + a], CO[s * O + b], mean, lg);
+        FM[s * F + f] = P.ff[s * WF + f0 + f] * mean;
+        LD[s * F + f] = LCO[s * O + a] - LCO[s * O + b];
+      }
+    }
+    // Base potentials: free nodes 0, held nodes their boundary; cells q_c / C_c above their node.
+    for (int m = tid; m < O; m += BLOCK) PHI[m] = T.upos[m] < 0 ? P.vb[o0 + m] : 0.0;
+    __syncthreads();
+    // The face conductance Laplacian (F^2/RT sum z^2 factor mean) and its factor.
+    assemble([&](int f) {
+      return kF * kF / RT * ((FM[f] + FM[F + f]) + FM[2 * F + f]);
+    });
+    if (factor()) bits |= CB_WORLD_FIELD;
+    // ---- the start field: Newton on the free nodes' potentials (the floating offsets) -----
+    // residual at potentials PHI (cells PC = node + relative): face currents, then junctions.
+    auto cell_potentials = [&](double *dst) {
+      for (int i = tid; i < N; i += BLOCK) {
+        const double *n = st(CB_FIELD_AMOUNT_INCREMENT);
+        const double q = P.q0[c0 + i] +
+                         kChargePerFmol * ((n[c0 + i] + n[WN + c0 + i]) + (-n[2 * WN + c0 + i]));
+        dst[i] = q * P.icap[c0 + i] + PHI[T.cell_node[i]];
+      }
+    };
+    // evaluate: residual into res (by factor column), returns (max |residual|, norm, valid).
+    auto evaluate = [&](double *res, bool junctions, double &rmax, double &norm) -> bool {
+      unsigned b = 0;
+      cell_potentials(PC);
+      for (int f = tid; f < F; f += BLOCK) {
+        IFC[f] = face_current(f);
+        if (!(fabs((PHI[T.fs[f]] - PHI[T.fr[f]]) * FRT) <= kMaxAbsX) || !is_finite(IFC[f]))
+          b |= 1u;
+      }
+      __syncthreads();
+      for (int e = tid; e < E; e += BLOCK) {
+        double jj[3], mu[3];
+        unsigned jb = 0;
+        const double opening = cj[e0 + e] * st(CB_FIELD_JUNCTION_GATE)[e0 + e];
+        junction_flux(e, PC[T.js[e]] - PC[T.jr[e]], opening, jj, mu, jb);
+        IJC[e] = junctions ? kChargePerFmol * ((jj[0] + jj[1]) + (-jj[2])) : 0.0;
+        if (jb || !is_finite(IJC[e])) b |= 1u;
+      }
+      __syncthreads();
+      double mr = 0.0, sc = 0.0;
+      for (int f = tid; f < F; f += BLOCK) sc = fmax(sc, fabs(IFC[f]));
+      for (int e = tid; e < E; e += BLOCK) sc = fmax(sc, fabs(IJC[e]));
+      for (int m = tid; m < O; m += BLOCK) {
+        const int u = T.upos[m];
+        if (u < 0) continue;
+        double r = 0.0;
+        for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
+          const int code = T.nf_idx[q];
+          r += (code & 1) ? -IFC[code >> 1] : IFC[code >> 1];
+        }
+        const int i = T.ncell[m];
+        if (i >= 0)
+          for (int q = T.cj_ptr[i]; q < T.cj_ptr[i + 1]; ++q) {
+            const int code = T.cj_idx[q];
+            r += (code & 1) ? -IJC[code >> 1] : IJC[code >> 1];
+          }
+        res[u] = r;
+        mr = fmax(mr, fabs(r));
+        if (!is_finite(r)) b |= 1u;
+      }
+      for (int i = tid; i < N; i += BLOCK)
+        if (!(fabs((PC[i] - PHI[T.cell_node[i]]) * FRT) <= kMaxAbsX)) b |= 1u;
+      rmax = block_max_abs<BLOCK>(mr, sRed);
+      const double scale = block_max_abs<BLOCK>(sc, sRed);
+      norm = rmax / (kCurrentAtol + kCurrentRtol * scale);
+      return block_or<BLOCK>(b, sBits) == 0u && is_finite(norm);
+    };
+    auto set_phi = [&](const double *x) {
+      for (int m = tid; m < O; m += BLOCK) {
+        const int u = T.upos[m];
+        PHI[m] = u < 0 ? P.vb[o0 + m] : x[u];
+      }
+      __syncthreads();
+    };
+    // The initial offsets: the face currents' balance at the base potentials.
+    double rmax, norm;
+    evaluate(Rv, false, rmax, norm);
+    for (int u = tid; u < U; u += BLOCK) Y[u] = -Rv[u];
+    __syncthreads();
+    solve(X);
+    set_phi(X);
+    bool accepted = evaluate(Rv, true, rmax, norm);
+    int count = 0;
+    while (count < kMaxIterations && norm > kNewtonTarget && accepted) {
+      const double before = rmax;
+      for (int u = tid; u < U; u += BLOCK) Y[u] = -Rv[u];
+      __syncthreads();
+      solve(DX);
+      bool ok = false;
+      double tmax = 0.0, tnorm = norm;
+      for (int bt = 0; bt < kMaxBacktracks && !ok; ++bt) {
+        const double h = ldexp(1.0, -bt);
+        for (int u = tid; u < U; u += BLOCK) XT[u] = X[u] + DX[u] * h;
+        __syncthreads();
+        set_phi(XT);
+        const bool valid = evaluate(RTv, true, tmax, tnorm);
+        ok = valid && (tmax < before || tnorm <= kNewtonTarget);
+      }
+      norm = tnorm;
+      accepted = ok;
+      if (ok) {
+        for (int u = tid; u < U; u += BLOCK) {
+          X[u] = XT[u];
+          Rv[u] = RTv[u];
+        }
+        rmax = tmax;
+      }
+      ++count;
+      __syncthreads();
+    }
+    set_phi(X);
+    {
+      double rm2, n2;
+      const bool valid = evaluate(Rv, true, rm2, n2);
+      if (!(valid && accepted && n2 <= kNewtonTarget)) bits |= CB_WORLD_FIELD;
+    }
+    // ---- stage 0: explicit rates at the start potentials ---------------------------------
+    const double *g0 = st(CB_FIELD_JUNCTION_GATE) + e0;
+    bits |= explicit_rates(K0, [&](int e) { return g0[e]; });
+    // The readouts' extracellular rate (membrane flux, whole face flux at the start field, the
+    // pump's transfer) and the half-step prediction of the node concentrations.
+    for (int m = tid; m < O; m += BLOCK) {
+      const int i = T.ncell[m];
+      const bool held = T.upos[m] < 0;
+      for (int s = 0; s < 3; ++s) {
+        const double z = s < 2 ? 1.0 : -1.0;
+        double a = 0.0, out = 0.0, in = 0.0;
+        if (i >= 0) a = 0.0 + K0[S.rk_mt + s * N + i];
+        for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
+          const int code = T.nf_idx[q], f = code >> 1;
+          const double mu = RT * LD[s * F + f] + z * kF * (PHI[T.fs[f]] - PHI[T.fr[f]]);
+          const double flux = FM[s * F + f] * mu / (RT * 1e-15);
+          if (code & 1) in += flux;
+          else out += flux;
+        }
+        double rate = held ? 0.0 : (a - out) + in;
+        if (!held && i >= 0) rate = rate + K0[S.rk_ex + s * N + i];
+        const double amount = P.oref[s * WO + o0 + m] +
+                              st(CB_FIELD_EXTRACELLULAR_INCREMENT)[s * WO + o0 + m];
+        const double pred = (amount + (0.5 * dt) * rate) / P.ovol[o0 + m];
+        if (!(is_finite(pred) && pred > 0.0)) bits |= CB_WORLD_OPERATOR;
+        CP[s * O + m] = pred > 0.0 ? pred : 1.0;
+      }
+    }
+    __syncthreads();
+    // Frozen face weights at the prediction, and the operator gamma dt L(W).
+    for (int f = tid; f < F; f += BLOCK) {
+      const int a = T.fs[f], b = T.fr[f];
+      for (int s = 0; s < 3; ++s) {
+        double mean, lg;
+        logmean(CP[s * O + a], CP[s * O + b], mean, lg);
+        WP[s * F + f] = P.ff[s * WF + f0 + f] * mean / 1e-15;
+      }
+    }
+    __syncthreads();
+    const double cond = kChargePerFmol * kF / (kR * temp);
+    auto gface = [&](int f) {
+      return k.gamma_dt * (cond * ((WP[f] + WP[F + f]) + WP[2 * F + f]));
+    };
+    assemble(gface);
+    if (factor()) bits |= CB_WORLD_OPERATOR;
+    // ---- stages 1 and 2 ---------------------------------------------------------------------
+    // The stage solve on known amounts (cells n(s,i), nodes o(s,m)): potentials into PHI, PC.
+    auto stage_solve = [&](auto n, auto o) {
+      for (int m = tid; m < O; m += BLOCK) {
+        const int u = T.upos[m];
+        if (u < 0) continue;
+        double q = P.q0o[o0 + m] + kChargePerFmol * ((o(0, m) + o(1, m)) + (-o(2, m)));
+        const int i = T.ncell[m];
+        if (i >= 0)
+          q = q + (P.q0[c0 + i] + kChargePerFmol * ((n(0, i) + n(1, i)) + (-n(2, i))));
+        for (int a = T.nf_ptr[m]; a < T.nf_ptr[m + 1]; ++a) {
+          const int f = T.nf_idx[a] >> 1;
+          const int other = T.fs[f] == m ? T.fr[f] : T.fs[f];
+          if (T.upos[other] < 0) q += gface(f) * P.vb[o0 + other];
+        }
+        Y[u] = q;
+        RTv[u] = q;  // the right-hand side, kept for the refinement
+      }
+      __syncthreads();
+      solve(X);
+      // FP64 iterative refinement: r = b - L x on the free rows (the held nodes' terms are in b),
+      // one correction per round. The last round's residual is the stage solve's acceptance
+      // (|r| <= CHARGE_ATOL + CHARGE_RTOL max(|b|, |L x|), numerics/surface_imex.py).
+      unsigned rb = 0;
+      for (int round = 0; round <= kRefineRounds; ++round) {
+        for (int m = tid; m < O; m += BLOCK) {
+          const int u = T.upos[m];
+          if (u < 0) continue;
+          double diag = 0.0, off = 0.0;
+          for (int a = T.nf_ptr[m]; a < T.nf_ptr[m + 1]; ++a) {
+            const int f = T.nf_idx[a] >> 1;
+            const double g = gface(f);
+            diag += g;
+            const int other = T.fs[f] == m ? T.fr[f] : T.fs[f];
+            const int v = T.upos[other];
+            if (v >= 0) off += g * X[v];
+          }
+          const double lx = diag * X[u] - off;
+          const double r = RTv[u] - lx;
+          Y[u] = r;
+          if (round == kRefineRounds &&
+              !(fabs(r) <= kChargeAtol + kChargeRtol * fmax(fabs(RTv[u]), fabs(lx))))
+            rb = 1u;
+        }
+        __syncthreads();
+        if (round == kRefineRounds) break;
+        solve(XT);
+        for (int u = tid; u < U; u += BLOCK) X[u] += XT[u];
+        __syncthreads();
+      }
+      for (int m = tid; m < O; m += BLOCK) {
+        const int u = T.upos[m];
+        PHI[m] = u < 0 ? P.vb[o0 + m] : X[u];
+      }
+      __syncthreads();
+      unsigned b = 0;
+      for (int i = tid; i < N; i += BLOCK) {
+        const double q = P.q0[c0 + i] + kChargePerFmol * ((n(0, i) + n(1, i)) + (-n(2, i)));
+        PC[i] = PHI[T.cell_node[i]] + q * P.icap[c0 + i];
+        if (!is_finite(PC[i])) b = 1u;
+      }
+      for (int m = tid; m < O; m += BLOCK)
+        if (!is_finite(PHI[m])) b = 1u;
+      __syncthreads();
+      return (b | rb) ? (unsigned)CB_WORLD_RESIDUAL : 0u;
+    };
+    // The implicit drift W z F/RT dv at the stage potentials into D.
+    auto drift = [&](double *D) {
+      for (int f = tid; f < F; f += BLOCK) {
+        const double dv = PHI[T.fs[f]] - PHI[T.fr[f]];
+        for (int s = 0; s < 3; ++s) {
+          const double z = s < 2 ? 1.0 : -1.0;
+          D[s * F + f] = WP[s * F + f] * (z * FRT) * dv;
+        }
+      }
+      __syncthreads();
+    };
+    // A node's drift inflow of species s (scatter to receivers less scatter from senders).
+    auto drift_inflow = [&](const double *D, int s, int m) {
+      double in = 0.0, out = 0.0;
+      for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
+        const int code = T.nf_idx[q];
+        if (code & 1) in += D[s * F + (code >> 1)];
+        else out += D[s * F + (code >> 1)];
+      }
+      return in - out;
+    };
+    const double *n0 = st(CB_FIELD_AMOUNT_INCREMENT), *x0 = st(CB_FIELD_EXTRACELLULAR_INCREMENT);
+    // Stage 1: known = y + (gamma dt) k0.
+    bits |= stage_solve(
+        [&](int s, int i) { return n0[s * WN + c0 + i] + k.gamma_dt * K0[S.rk_n + s * N + i]; },
+        [&](int s, int m) { return x0[s * WO + o0 + m] + k.gamma_dt * K0[S.rk_x + s * O + m]; });
+    drift(D1);
+    for (int i = tid; i < N; i += BLOCK)
+      for (int s = 0; s < 3; ++s)
+        N1[s * N + i] = n0[s * WN + c0 + i] + k.gamma_dt * K0[S.rk_n + s * N + i];
+    for (int m = tid; m < O; m += BLOCK) {
+      const bool held = T.upos[m] < 0;
+      for (int s = 0; s < 3; ++s) {
+        const double known = x0[s * WO + o0 + m] + k.gamma_dt * K0[S.rk_x + s * O + m];
+        O1[s * O + m] = known + k.gamma_dt * (held ? 0.0 : drift_inflow(D1, s, m));
+      }
+    }
+    for (int e = tid; e < E; e += BLOCK) G1[e] = g0[e] + k.gamma_dt * K0[S.rk_g + e];
+    __syncthreads();
+    bits |= set_conc([&](int s, int i) { return N1[s * N + i]; },
+                     [&](int s, int m) { return O1[s * O + m]; });
+    __syncthreads();
+    bits |= explicit_rates(K1, [&](int e) { return G1[e]; });
+    // Stage 2: known = y + (delta dt) k0 + ((1 - delta) dt) k1 + ((1 - gamma) dt) d1.
+    auto known2_cell = [&](int s, int i) {
+      return (n0[s * WN + c0 + i] + k.delta_dt * K0[S.rk_n + s * N + i]) +
+             k.omdelta_dt * K1[S.rk_n + s * N + i];
+    };
+    auto known2_node = [&](int s, int m) {
+      const bool held = T.upos[m] < 0;
+      return ((x0[s * WO + o0 + m] + k.delta_dt * K0[S.rk_x + s * O + m]) +
+              k.omdelta_dt * K1[S.rk_x + s * O + m]) +
+             omgamma_dt * (held ? 0.0 : drift_inflow(D1, s, m));
+    };
+    bits |= stage_solve(known2_cell, known2_node);
+    drift(D2);
+    // ---- the step's end: ledgers, heat, domain; write or refuse ---------------------------
+    unsigned dom = 0;
+    const double gdt = k.gamma_dt, ddt = k.delta_dt, odt = k.omdelta_dt;
+    const double dl = k.delta, od = k.omdelta, gm = 1.0 - 1.0 / sqrt(2.0), og = 1.0 - gm;
+    // Cells.
+    for (int i = tid; i < N; i += BLOCK) {
+      for (int s = 0; s < 3; ++s) {
+        const double v = known2_cell(s, i);
+        if (!(is_finite(v) && P.ref[s * WN + c0 + i] + v > 0.0)) dom = 1u;
+      }
+      for (int s = 0; s < 3; ++s) {
+        const double v = (st(CB_FIELD_MEMBRANE_TRANSFERRED)[s * WN + c0 + i] +
+                          ddt * K0[S.rk_mt + s * N + i]) + odt * K1[S.rk_mt + s * N + i];
+        if (!is_finite(v)) dom = 1u;
+      }
+      const int f4[4] = {CB_FIELD_MEMBRANE_DISSIPATED, CB_FIELD_PUMP_CYCLES,
+                         CB_FIELD_PUMP_DISSIPATED, CB_FIELD_METABOLIC_WORK};
+      const long long r4[4] = {S.rk_md, S.rk_cy, S.rk_pd, S.rk_mw};
+      for (int q = 0; q < 4; ++q) {
+        const double v = (st(f4[q])[c0 + i] + ddt * K0[r4[q] + i]) + odt * K1[r4[q] + i];
+        if (!is_finite(v)) dom = 1u;
+      }
+    }
+    for (int e = tid; e < E; e += BLOCK) {
+      for (int s = 0; s < 3; ++s) {
+        const double v = (st(CB_FIELD_JUNCTION_TRANSFERRED)[s * WE + e0 + e] +
+                          ddt * K0[S.rk_jt + s * E + e]) + odt * K1[S.rk_jt + s * E + e];
+        if (!is_finite(v)) dom = 1u;
+      }
+      const double jd = (st(CB_FIELD_JUNCTION_DISSIPATED)[e0 + e] + ddt * K0[S.rk_jd + e]) +
+                        odt * K1[S.rk_jd + e];
+      const double g = (g0[e] + ddt * K0[S.rk_g + e]) + odt * K1[S.rk_g + e];
+      if (!(is_finite(jd) && is_finite(g))) dom = 1u;
+    }
+    for (int m = tid; m < O; m += BLOCK)
+      for (int s = 0; s < 3; ++s) {
+        const double v = known2_node(s, m) + gdt * (T.upos[m] < 0 ? 0.0 : drift_inflow(D2, s, m));
+        if (!(is_finite(v) && P.oref[s * WO + o0 + m] + v > 0.0)) dom = 1u;
+      }
+    if (block_or<BLOCK>(dom, sBits)) bits |= CB_WORLD_DOMAIN;
+    bits = block_or<BLOCK>(bits, sBits);
+    if (bits) {
+      refused = bits;
+      break;
+    }
+    // Accepted: write the step in place, field by field (each from its own start value).
+    for (int i = tid; i < N; i += BLOCK) {
+      double nv[3];
+      for (int s = 0; s < 3; ++s) nv[s] = known2_cell(s, i);
+      for (int s = 0; s < 3; ++s) {
+        st(CB_FIELD_AMOUNT_INCREMENT)[s * WN + c0 + i] = nv[s];
+        double *mt = st(CB_FIELD_MEMBRANE_TRANSFERRED) + s * WN + c0 + i;
+        *mt = (*mt + ddt * K0[S.rk_mt + s * N + i]) + odt * K1[S.rk_mt + s * N + i];
+      }
+      const int f4[4] = {CB_FIELD_MEMBRANE_DISSIPATED, CB_FIELD_PUMP_CYCLES,
+                         CB_FIELD_PUMP_DISSIPATED, CB_FIELD_METABOLIC_WORK};
+      const long long r4[4] = {S.rk_md, S.rk_cy, S.rk_pd, S.rk_mw};
+      for (int q = 0; q < 4; ++q) {
+        double *v = st(f4[q]) + c0 + i;
+        *v = (*v + ddt * K0[r4[q] + i]) + odt * K1[r4[q] + i];
+      }
+    }
+    for (int e = tid; e < E; e += BLOCK) {
+      for (int s = 0; s < 3; ++s) {
+        double *v = st(CB_FIELD_JUNCTION_TRANSFERRED) + s * WE + e0 + e;
+        *v = (*v + ddt * K0[S.rk_jt + s * E + e]) + odt * K1[S.rk_jt + s * E + e];
+      }
+      double *jd = st(CB_FIELD_JUNCTION_DISSIPATED) + e0 + e;
+      *jd = (*jd + ddt * K0[S.rk_jd + e]) + odt * K1[S.rk_jd + e];
+      double *g = st(CB_FIELD_JUNCTION_GATE) + e0 + e;
+      *g = (*g + ddt * K0[S.rk_g + e]) + odt * K1[S.rk_g + e];
+    }
+    // Faces: transferred (explicit diffusion, both drifts), heat of the applied flux.
+    for (int f = tid; f < F; f += BLOCK) {
+      double heat = 0.0;
+      for (int s = 0; s < 3; ++s) {
+        const double k0d = K0[S.rk_fd + s * F + f], k1d = K1[S.rk_fd + s * F + f];
+        const double d1 = D1[s * F + f], d2 = D2[s * F + f];
+        double *v = st(CB_FIELD_FACE_TRANSFERRED) + s * WF + f0 + f;
+        *v = (((*v + ddt * k0d) + odt * k1d) + omgamma_dt * d1) + gdt * d2;
+        const double applied = ((0.0 + dl * k0d) + od * k1d) + ((0.0 + og * d1) + gm * d2);
+        const double wgt = WP[s * F + f];
+        heat += wgt > 0.0 ? applied * applied / wgt : 0.0;
+      }
+      double *fd = st(CB_FIELD_FACE_DISSIPATED) + f0 + f;
+      *fd = *fd + dt * (1e-3 * kR * temp * heat);
+    }
+    // Nodes: amounts (free), supply and reservoir work (held); the held nodes face no capacitor,
+    // so their electrodes deliver nothing (electrode charge and work unchanged).
+    for (int m = tid; m < O; m += BLOCK) {
+      const bool held = T.upos[m] < 0;
+      double nv[3], sup[3];
+      for (int s = 0; s < 3; ++s) {
+        nv[s] = known2_node(s, m) + gdt * (held ? 0.0 : drift_inflow(D2, s, m));
+        const double i1 = held ? -drift_inflow(D1, s, m) : 0.0;
+        const double i2 = held ? -drift_inflow(D2, s, m) : 0.0;
+        const double k0s = K0[S.rk_s + s * O + m], k1s = K1[S.rk_s + s * O + m];
+        double *v = st(CB_FIELD_RESERVOIR_SUPPLIED) + s * WO + o0 + m;
+        *v = (((*v + ddt * k0s) + odt * k1s) + omgamma_dt * i1) + gdt * i2;
+        sup[s] = ((0.0 + dl * k0s) + od * k1s) + ((0.0 + og * i1) + gm * i2);
+      }
+      for (int s = 0; s < 3; ++s) st(CB_FIELD_EXTRACELLULAR_INCREMENT)[s * WO + o0 + m] = nv[s];
+      if (held) {
+        const double vb = P.vb[o0 + m];
+        double work = 0.0;
+        for (int s = 0; s < 3; ++s) {
+          const double z = s < 2 ? 1.0 : -1.0;
+          const double co = P.oref[s * WO + o0 + m] / P.ovol[o0 + m];
+          const double mu = kR * temp * log(co) + z * kF * vb;
+          work += mu * (dt * sup[s]);
+        }
+        double *rw = st(CB_FIELD_RESERVOIR_WORK) + o0 + m;
+        *rw = *rw + 1e-3 * work;
+      }
+    }
+    __syncthreads();
+    ++taken;
+  }
+  if (tid == 0) {
+    status[w] = refused;
+    if (taken_out) taken_out[w] = taken;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Host
+
+struct cb_field {
+  int device = 0;
+  int W = 0, N = 0, O = 0, E = 0, F = 0, U = 0, levels = 0;
+  long long nnz = 0;
+  Topo topo{};
+  Params params{};
+  FLayout layout{};
+  Scratch scratch{};
+  long long state_total = 0;
+  double *scratch_buf = nullptr;
+  std::vector<void *> owned;
+};
+
+namespace {
+
+template <typename V>
+int upload(cb_field *f, const V *host, size_t count, V **dst) {
+  void *p = nullptr;
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(V);
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+  f->owned.push_back(p);
+  if (count) {
+    e = cudaMemcpy(p, host, count * sizeof(V), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy");
+  }
+  *dst = static_cast<V *>(p);
+  return CB_OK;
+}
+
+template <typename V>
+int upload(cb_field *f, const std::vector<V> &host, const V **dst) {
+  V *p = nullptr;
+  const int rc = upload(f, host.data(), host.size(), &p);
+  *dst = p;
+  return rc;
+}
+
+double host_logaddexp0(double y) {
+  if (y == 0.0) return 0.6931471805599453;
+  if (-y > 0) return std::log1p(std::exp(y));
+  return y + std::log1p(std::exp(-y));
+}
+
+// Nested dissection of the free nodes of a side x side grid whose held nodes are its ring: the
+// free box (side - 2)^2, split across its longer side by a middle line, the line last.
+void nested_dissection(int x0, int x1, int y0, int y1, int width, std::vector<int> &order) {
+  const int w = x1 - x0, h = y1 - y0;
+  if (w <= 0 || h <= 0) return;
+  if (w * h <= 16) {
+    for (int y = y0; y < y1; ++y)
+      for (int x = x0; x < x1; ++x) order.push_back(y * width + x);
+    return;
+  }
+  if (w >= h) {
+    const int mid = x0 + w / 2;
+    nested_dissection(x0, mid, y0, y1, width, order);
+    nested_dissection(mid + 1, x1, y0, y1, width, order);
+    for (int y = y0; y < y1; ++y) order.push_back(y * width + mid);
+  } else {
+    const int mid = y0 + h / 2;
+    nested_dissection(x0, x1, y0, mid, width, order);
+    nested_dissection(x0, x1, mid + 1, y1, width, order);
+    for (int x = x0; x < x1; ++x) order.push_back(mid * width + x);
+  }
+}
+
+}  // namespace
+
+extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out) {
+  if (!d || !out) return fail(CB_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  const int W = d->worlds, N = d->cells, O = d->nodes, E = d->junctions, F = d->faces;
+  if (W <= 0 || N < 0 || O <= 0 || E < 0 || F < 0)
+    return fail(CB_ERR_ARGUMENT, "field: sizes must be positive");
+  for (const void *p : {(const void *)d->cell_node, (const void *)d->face_sender,
+                        (const void *)d->face_receiver, (const void *)d->reservoir,
+                        (const void *)d->temperature, (const void *)d->pump,
+                        (const void *)d->volume, (const void *)d->capacitance,
+                        (const void *)d->permeability, (const void *)d->pump_capacity,
+                        (const void *)d->amount, (const void *)d->initial_charge,
+                        (const void *)d->outside_volume, (const void *)d->outside_amount,
+                        (const void *)d->outside_charge, (const void *)d->boundary_V,
+                        (const void *)d->face_factor, (const void *)d->area})
+    if (!p) return fail(CB_ERR_ARGUMENT, "field: null array");
+  if (E && (!d->junction_sender || !d->junction_receiver || !d->junction_area ||
+            !d->junction_permeability || !d->gate_threshold || !d->gate_minimum))
+    return fail(CB_ERR_ARGUMENT, "field: null junction array");
+  // Topology checks: the contract the eliminated algebra rests on.
+  std::vector<int> ncell(O, -1), cell_node(N);
+  for (int i = 0; i < N; ++i) {
+    const long long m = d->cell_node[i];
+    if (m < 0 || m >= O) return fail(CB_ERR_LAYOUT, "field: cell_node out of range");
+    if (d->reservoir[m]) return fail(CB_ERR_LAYOUT, "field: a cell faces a held node");
+    if (ncell[m] >= 0) return fail(CB_ERR_LAYOUT, "field: two cells face one node");
+    ncell[m] = i;
+    cell_node[i] = (int)m;
+  }
+  std::vector<int> fs(F), fr(F), js(E), jr(E);
+  for (int f = 0; f < F; ++f) {
+    const long long a = d->face_sender[f], b = d->face_receiver[f];
+    if (a < 0 || a >= O || b < 0 || b >= O || a == b)
+      return fail(CB_ERR_LAYOUT, "field: a face's nodes are out of range or equal");
+    fs[f] = (int)a;
+    fr[f] = (int)b;
+  }
+  for (int e = 0; e < E; ++e) {
+    const long long a = d->junction_sender[e], b = d->junction_receiver[e];
+    if (a < 0 || a >= N || b < 0 || b >= N || a == b)
+      return fail(CB_ERR_LAYOUT, "field: a junction's cells are out of range or equal");
+    js[e] = (int)a;
+    jr[e] = (int)b;
+  }
+  // Free nodes, the Laplacian's graph (faces between free nodes), its order.
+  std::vector<int> free_index(O, -1), free_nodes;
+  for (int m = 0; m < O; ++m)
+    if (!d->reservoir[m]) {
+      free_index[m] = (int)free_nodes.size();
+      free_nodes.push_back(m);
+    }
+  const int U = (int)free_nodes.size();
+  if (U == 0) return fail(CB_ERR_LAYOUT, "field: no free node");
+  std::vector<int> ga, gb, gface;
+  std::vector<char> touches_held(U, 0);
+  for (int f = 0; f < F; ++f) {
+    const int a = free_index[fs[f]], b = free_index[fr[f]];
+    if (a >= 0 && b >= 0) {
+      ga.push_back(a);
+      gb.push_back(b);
+      gface.push_back(f);
+    } else if (a >= 0) {
+      touches_held[a] = 1;
+    } else if (b >= 0) {
+      touches_held[b] = 1;
+    }
+  }
+  // Every free node must reach a held node through faces (the reference's return-path rule),
+  // or the Laplacian is singular.
+  {
+    std::vector<std::vector<int>> adj(U);
+    for (size_t q = 0; q < ga.size(); ++q) {
+      adj[ga[q]].push_back(gb[q]);
+      adj[gb[q]].push_back(ga[q]);
+    }
+    std::vector<char> seen(U, 0);
+    std::vector<int> stack;
+    for (int u = 0; u < U; ++u)
+      if (touches_held[u]) {
+        seen[u] = 1;
+        stack.push_back(u);
+      }
+    while (!stack.empty()) {
+      const int u = stack.back();
+      stack.pop_back();
+      for (int v : adj[u])
+        if (!seen[v]) {
+          seen[v] = 1;
+          stack.push_back(v);
+        }
+    }
+    for (int u = 0; u < U; ++u)
+      if (!seen[u])
+        return fail(CB_ERR_LAYOUT,
+                    "field: a floating component has no face path to a held node");
+  }
+  // Grid detection: O = side^2 with the ring held and 4-neighbour faces -> nested dissection.
+  std::vector<int> order;
+  const int side = (int)std::lround(std::sqrt((double)O));
+  bool grid = side * side == O && side >= 3 && F == 2 * side * (side - 1);
+  if (grid) {
+    for (int m = 0; m < O && grid; ++m) {
+      const int x = m % side, y = m / side;
+      const bool ring = x == 0 || y == 0 || x == side - 1 || y == side - 1;
+      grid = (d->reservoir[m] != 0) == ring;
+    }
+    for (int f = 0; f < F && grid; ++f) {
+      const int a = fs[f], b = fr[f];
+      const int dx = std::abs(a % side - b % side), dy = std::abs(a / side - b / side);
+      grid = dx + dy == 1;
+    }
+  }
+  if (grid) {
+    std::vector<int> cells;
+    nested_dissection(0, side - 2, 0, side - 2, side - 2, cells);
+    // cells index the free box row-major; map to free-node indices.
+    for (int c : cells) {
+      const int x = c % (side - 2) + 1, y = c / (side - 2) + 1;
+      order.push_back(free_index[y * side + x]);
+    }
+  }
+  WorldPlan plan;
+  int rc = plan_world(U, ga.data(), gb.data(), (int)ga.size(), plan,
+                      grid ? order.data() : nullptr, "field");
+  if (rc) return rc;
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  auto *f = new cb_field();
+  f->device = device;
+  f->W = W, f->N = N, f->O = O, f->E = E, f->F = F, f->U = U;
+  f->levels = (int)plan.level_ptr.size() - 1;
+  f->nnz = plan.colp[U];
+  auto bail = [&](int code) {
+    cb_field_free(f);
+    return code;
+  };
+  // Shared topology.
+  std::vector<int> upos(O, -1);
+  for (int u = 0; u < U; ++u) upos[free_nodes[u]] = plan.rank[u];
+  std::vector<int> nf_ptr(O + 1, 0), nf_idx;
+  {
+    std::vector<std::vector<int>> lists(O);
+    for (int q = 0; q < F; ++q) {
+      lists[fs[q]].push_back(q << 1);
+      lists[fr[q]].push_back((q << 1) | 1);
+    }
+    for (int m = 0; m < O; ++m) {
+      nf_ptr[m + 1] = nf_ptr[m] + (int)lists[m].size();
+      nf_idx.insert(nf_idx.end(), lists[m].begin(), lists[m].end());
+    }
+  }
+  std::vector<int> cj_ptr(N + 1, 0), cj_idx;
+  {
+    std::vector<std::vector<int>> lists(N);
+    for (int e = 0; e < E; ++e) {
+      lists[js[e]].push_back(e << 1);
+      lists[jr[e]].push_back((e << 1) | 1);
+    }
+    for (int i = 0; i < N; ++i) {
+      cj_ptr[i + 1] = cj_ptr[i] + (int)lists[i].size();
+      cj_idx.insert(cj_idx.end(), lists[i].begin(), lists[i].end());
+    }
+  }
+  std::vector<int> face_pos(F, -1);
+  for (size_t q = 0; q < gface.size(); ++q) face_pos[gface[q]] = plan.edge_pos[q];
+  Topo &T = f->topo;
+  T.N = N, T.O = O, T.E = E, T.F = F, T.U = U, T.levels = f->levels;
+  if ((rc = upload(f, cell_node, &T.cell_node)) || (rc = upload(f, ncell, &T.ncell)) ||
+      (rc = upload(f, upos, &T.upos)) || (rc = upload(f, nf_ptr, &T.nf_ptr)) ||
+      (rc = upload(f, nf_idx, &T.nf_idx)) || (rc = upload(f, cj_ptr, &T.cj_ptr)) ||
+      (rc = upload(f, cj_idx, &T.cj_idx)) || (rc = upload(f, fs, &T.fs)) ||
+      (rc = upload(f, fr, &T.fr)) || (rc = upload(f, js, &T.js)) ||
+      (rc = upload(f, jr, &T.jr)) || (rc = upload(f, face_pos, &T.face_pos)) ||
+      (rc = upload(f, plan.colp, &T.colp)) || (rc = upload(f, plan.lrow, &T.lrow)) ||
+      (rc = upload(f, plan.uk_ptr, &T.ukp)) || (rc = upload(f, plan.uk_col, &T.ukc)) ||
+      (rc = upload(f, plan.uk_pos, &T.ukpos)) || (rc = upload(f, plan.uk_rel, &T.ukrel)) ||
+      (rc = upload(f, plan.rel, &T.rel)) || (rc = upload(f, plan.level_ptr, &T.lvp)) ||
+      (rc = upload(f, plan.level_cols, &T.lvc)))
+    return bail(rc);
+  // Per-world parameters.
+  const long long WN = (long long)W * N, WO = (long long)W * O, WE = (long long)W * E,
+                  WF = (long long)W * F;
+  Params &P = f->params;
+  P.WN = WN, P.WO = WO, P.WE = WE, P.WF = WF;
+  std::vector<double> wcv((size_t)W * FW_STRIDE);
+  const double ln1000 = std::log(1000.0);
+  for (int w = 0; w < W; ++w) {
+    double *c = wcv.data() + (size_t)w * FW_STRIDE;
+    const double Tk = d->temperature[w], RT = kR * Tk;
+    c[FW_T] = Tk;
+    c[FW_RT] = RT;
+    c[FW_FRT] = kF / RT;
+    c[FW_INVRT] = 1.0 / RT;
+    const double atp = d->pump[0 * W + w], adp = d->pump[1 * W + w], pi = d->pump[2 * W + w];
+    const double km_na = d->pump[3 * W + w], km_k = d->pump[4 * W + w];
+    const double km_atp = d->pump[5 * W + w], dg0 = d->pump[6 * W + w];
+    c[FW_DRIVE] = dg0 + RT * (((std::log(adp) + std::log(pi)) - std::log(atp)) - ln1000);
+    c[FW_LOGKMK] = std::log(km_k);
+    c[FW_LATP] = host_logaddexp0(std::log(km_atp) - std::log(atp));
+    c[FW_LOGKMNA] = std::log(km_na);
+    const bool t_ok = std::isfinite(Tk) && Tk >= 200.0 && Tk <= 400.0;
+    const double rtd = kR * (t_ok ? Tk : 298.15);
+    bool ok = t_ok;
+    for (double v : {atp, adp, pi, km_na, km_k, km_atp}) ok = ok && std::isfinite(v) && v > 0;
+    ok = ok && std::isfinite(dg0);
+    const double s_atp = ok ? atp : 1.0, s_adp = ok ? adp : 1.0, s_pi = ok ? pi : 1.0;
+    c[FW_AFF0] = (((dg0 / rtd + std::log(s_adp)) + std::log(s_pi)) - std::log(s_atp)) - ln1000;
+    c[FW_PUMPOK] = ok ? 1.0 : 0.0;
+    c[FW_INVRTD] = 1.0 / rtd;
+  }
+  std::vector<double> icap(WN), logpcap(WN), ap(3 * WN), jap(3 * WE);
+  for (long long i = 0; i < WN; ++i) {
+    icap[i] = 1.0 / d->capacitance[i];
+    logpcap[i] = d->pump_capacity[i] > 0 ? std::log(d->pump_capacity[i]) : 0.0;
+    for (int s = 0; s < 3; ++s)
+      ap[s * WN + i] = d->area[i] * d->permeability[s * WN + i] / 1e-15;
+  }
+  for (long long e = 0; e < WE; ++e)
+    for (int s = 0; s < 3; ++s)
+      jap[s * WE + e] = d->junction_area[e] * d->junction_permeability[s * WE + e] / 1e-15;
+  double *tmp = nullptr;
+  auto put = [&](const double *src, size_t count, const double **dst) {
+    int r = upload(f, src, count, &tmp);
+    *dst = tmp;
+    return r;
+  };
+  if ((rc = upload(f, wcv, &P.wc)) || (rc = put(d->volume, WN, &P.vol)) ||
+      (rc = upload(f, icap, &P.icap)) || (rc = put(d->initial_charge, WN, &P.q0)) ||
+      (rc = put(d->pump_capacity, WN, &P.pcap)) || (rc = upload(f, logpcap, &P.logpcap)) ||
+      (rc = put(d->amount, 3 * WN, &P.ref)) || (rc = upload(f, ap, &P.ap)) ||
+      (rc = upload(f, jap, &P.jap)) || (rc = put(E ? d->gate_threshold : nullptr, WE, &P.thr)) ||
+      (rc = put(E ? d->gate_minimum : nullptr, WE, &P.jmin)) ||
+      (rc = put(d->outside_volume, WO, &P.ovol)) || (rc = put(d->outside_charge, WO, &P.q0o)) ||
+      (rc = put(d->boundary_V, WO, &P.vb)) || (rc = put(d->outside_amount, 3 * WO, &P.oref)) ||
+      (rc = put(d->face_factor, 3 * WF, &P.ff)))
+    return bail(rc);
+  // State layout.
+  const long long sizes[CB_FIELD_STATE_FIELDS] = {3 * WN, 3 * WO, 3 * WN, 3 * WE, 3 * WF, 3 * WO,
+                                                  WN, WE, WF, WO, WO, WO, WE, WN, WN, WN};
+  long long off = 0;
+  for (int q = 0; q < CB_FIELD_STATE_FIELDS; ++q) {
+    f->layout.s[q] = off;
+    off += sizes[q];
+  }
+  f->state_total = off;
+  // Scratch slices.
+  Scratch &S = f->scratch;
+  long long o = 0;
+  auto take = [&](long long n) {
+    const long long at = o;
+    o += (n + 31) / 32 * 32;  // 256-byte aligned sub-arrays
+    return at;
+  };
+  S.rk_n = 0;
+  S.rk_mt = 3LL * N;
+  S.rk_md = 6LL * N;
+  S.rk_cy = 7LL * N;
+  S.rk_pd = 8LL * N;
+  S.rk_mw = 9LL * N;
+  S.rk_jt = 10LL * N;
+  S.rk_jd = S.rk_jt + 3LL * E;
+  S.rk_g = S.rk_jd + E;
+  S.rk_fd = S.rk_g + E;
+  S.rk_x = S.rk_fd + 3LL * F;
+  S.rk_s = S.rk_x + 3LL * O;
+  S.rk_ex = S.rk_s + 3LL * O;
+  S.rk_size = S.rk_ex + 3LL * N;
+  S.lval = take(f->nnz);
+  S.x = take(U), S.xt = take(U), S.dx = take(U), S.r = take(U), S.rt = take(U), S.y = take(U);
+  S.phi = take(O), S.pc = take(N);
+  S.co = take(3LL * O), S.lco = take(3LL * O), S.ci = take(3LL * N), S.lci = take(3LL * N);
+  S.fm = take(3LL * F), S.ld = take(3LL * F), S.wp = take(3LL * F);
+  S.ifc = take(F), S.ijc = take(std::max(E, 1));
+  S.k0 = take(S.rk_size), S.k1 = take(S.rk_size);
+  S.d1 = take(3LL * F), S.d2 = take(3LL * F);
+  S.n1 = take(3LL * N), S.o1 = take(3LL * O), S.g1 = take(std::max(E, 1));
+  S.cp = take(3LL * O);
+  S.stride = o;
+  {
+    void *p = nullptr;
+    ce = cudaMalloc(&p, (size_t)S.stride * W * sizeof(double));
+    if (ce != cudaSuccess) {
+      cuda_fail(ce, "cudaMalloc field scratch");
+      return bail(CB_ERR_CUDA);
+    }
+    f->owned.push_back(p);
+    f->scratch_buf = static_cast<double *>(p);
+  }
+  *out = f;
+  return CB_OK;
+}
+
+extern "C" void cb_field_free(cb_field *f) {
+  if (!f) return;
+  cudaSetDevice(f->device);
+  for (void *p : f->owned) cudaFree(p);
+  delete f;
+}
+
+extern "C" int cb_field_state_layout(const cb_field *f, int64_t offsets[CB_FIELD_STATE_FIELDS],
+                                     int64_t *total) {
+  if (!f || !offsets || !total) return fail(CB_ERR_ARGUMENT, "null argument");
+  for (int q = 0; q < CB_FIELD_STATE_FIELDS; ++q) offsets[q] = f->layout.s[q];
+  *total = f->state_total;
+  return CB_OK;
+}
+
+extern "C" int64_t cb_field_control_length(const cb_field *f) {
+  if (!f) return -1;
+  return (long long)f->W * (2LL * f->N + f->E);
+}
+
+extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_out, double dt,
+                             const double *control, int n_steps, uint32_t *world_status,
+                             int32_t *accepted_steps, void *stream) {
+  if (!f || !state_in || !state_out || !control || !world_status)
+    return fail(CB_ERR_ARGUMENT, "null argument");
+  if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
+  cudaError_t ce = cudaSetDevice(f->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  auto s = static_cast<cudaStream_t>(stream);
+  if (state_out != state_in) {
+    ce = cudaMemcpyAsync(state_out, state_in, (size_t)f->state_total * sizeof(double),
+                         cudaMemcpyDeviceToDevice, s);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpyAsync");
+  }
+  field_kernel<kFieldBlock><<<f->W, kFieldBlock, 0, s>>>(
+      f->topo, f->params, f->layout, f->scratch, state_out, control, step_coef(dt), n_steps,
+      world_status,
+      accepted_steps, f->scratch_buf);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return cuda_fail(ce, "field launch");
+  return CB_OK;
+}
+
+extern "C" int cb_field_step_host(cb_field *f, const double *state_in, double *state_out,
+                                  double dt, const double *control, int n_steps,
+                                  uint32_t *world_status, int32_t *accepted_steps) {
+  if (!f || !state_in || !state_out || !control || !world_status)
+    return fail(CB_ERR_ARGUMENT, "null argument");
+  cudaError_t ce = cudaSetDevice(f->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  const size_t sb = (size_t)f->state_total * sizeof(double);
+  const size_t cb = (size_t)cb_field_control_length(f) * sizeof(double);
+  double *ds = nullptr, *dc = nullptr;
+  uint32_t *dst = nullptr;
+  int32_t *dacc = nullptr;
+  int rc = CB_OK;
+  if ((ce = cudaMalloc(&ds, sb)) != cudaSuccess || (ce = cudaMalloc(&dc, cb)) != cudaSuccess ||
+      (ce = cudaMalloc(&dst, f->W * sizeof(uint32_t))) != cudaSuccess ||
+      (ce = cudaMalloc(&dacc, f->W * sizeof(int32_t))) != cudaSuccess) {
+    rc = cuda_fail(ce, "cudaMalloc");
+  } else if ((ce = cudaMemcpy(ds, state_in, sb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+             (ce = cudaMemcpy(dc, control, cb, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    rc = cuda_fail(ce, "cudaMemcpy");
+  } else if ((rc = cb_field_step(f, ds, ds, dt, dc, n_steps, dst, dacc, nullptr)) == CB_OK) {
+    if ((ce = cudaMemcpy(state_out, ds, sb, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (ce = cudaMemcpy(world_status, dst, f->W * sizeof(uint32_t), cudaMemcpyDeviceToHost)) !=
+            cudaSuccess ||
+        (accepted_steps && (ce = cudaMemcpy(accepted_steps, dacc, f->W * sizeof(int32_t),
+                                            cudaMemcpyDeviceToHost)) != cudaSuccess))
+      rc = cuda_fail(ce, "cudaMemcpy");
+  }
+  cudaFree(ds);
+  cudaFree(dc);
+  cudaFree(dst);
+  cudaFree(dacc);
+  return rc;
+}

@@ -56,7 +56,10 @@ typedef struct cb_tissue cb_tissue;
 #define CB_WORLD_LEDGER_COTANGENT 256u /* cb_step_vjp: a ledger field's cotangent was not zero;
                                           the gradients leave out the ledgers' dependence */
 #define CB_WORLD_OPERATOR 512u     /* N2: the half-step prediction (non-positive concentration,
-                                      non-finite slopes) or the operator (a non-positive pivot) */
+                                      non-finite slopes) or the operator (a non-positive pivot);
+                                      field worlds: the same for the face-drift operator */
+#define CB_WORLD_FIELD 1024u       /* field worlds: the start field's Newton on the floating
+                                      offsets found no root within its bounds */
 
 /* Return codes. */
 #define CB_OK 0
@@ -281,6 +284,82 @@ int cb_set_permeability(cb_tissue *t, const double *membrane, const double *junc
 const char *cb_last_error(void);
 /* Library version string. */
 const char *cb_version(void);
+
+/*
+ * Field worlds: tissues whose cells face a resolved extracellular grid (cells_b200/field_worlds.py)
+ * instead of one held bath. Replaces the reference's model-module protocol for
+ * cells.model.resolved_pump_tissue@1 with outside nodes and faces under
+ * cells.solver.imex_ars222_face_electromigration@1 (models/surface_pump.py:158-369, the field
+ * closure of numerics/surface_field.py:253-855, the face operator of numerics/surface_imex.py).
+ *
+ * Every world of a batch shares one topology: N cells, O outside nodes, E junctions, F faces;
+ * cell i's one membrane faces outside node cell_node[i]; at most one cell per node and none on a
+ * held node; held (reservoir) nodes have no membrane. Per-world parameters are world-major
+ * ([W*N] etc.; species arrays [3][W*X]). The start field is the reference's capacitor reduction
+ * with a damped Newton on the floating offsets (one per capacitor component: a cell with its node,
+ * or a lone node), here a chord Newton whose matrix is the face conductance Laplacian; the stage
+ * potentials solve (C + gamma dt L) phi = q with each cell eliminated into its node. Both
+ * matrices are the face Laplacian on the free nodes: one nested-dissection plan, one sparse
+ * Cholesky per matrix per world per step.
+ */
+typedef struct cb_field cb_field;
+typedef struct {
+  int32_t worlds, cells, nodes, junctions, faces;
+  const int64_t *cell_node;        /* [N] */
+  const int64_t *junction_sender;  /* [E] cells */
+  const int64_t *junction_receiver;
+  const int64_t *face_sender;      /* [F] outside nodes */
+  const int64_t *face_receiver;
+  const uint8_t *reservoir;        /* [O] held nodes */
+  const double *temperature;       /* [W] K */
+  const double *pump;              /* [7][W] atp, adp, pi (mM), km_na, km_k, km_atp (mM), dG0 */
+  const double *volume;            /* [W*N] pL */
+  const double *area;              /* [W*N] m^2 */
+  const double *capacitance;       /* [W*N] F */
+  const double *permeability;      /* [3][W*N] m/s */
+  const double *pump_capacity;     /* [W*N] fmol/s */
+  const double *amount;            /* [3][W*N] reference amounts, fmol */
+  const double *initial_charge;    /* [W*N] C */
+  const double *junction_area;     /* [W*E] */
+  const double *junction_permeability; /* [3][W*E] */
+  const double *gate_threshold;    /* [W*E] V */
+  const double *gate_minimum;      /* [W*E] */
+  const double *outside_volume;    /* [W*O] pL */
+  const double *outside_amount;    /* [3][W*O] fmol */
+  const double *outside_charge;    /* [W*O] C */
+  const double *boundary_V;        /* [W*O] held potentials (0 on free nodes) */
+  const double *face_factor;       /* [3][W*F] D A / L, m^3/s */
+} cb_field_desc;
+
+/* State fields of a field batch (offsets from cb_field_state_layout), the reference's STATE_TYPE
+ * without channels: cell fields [3][W*N] or [W*N], node fields [3][W*O] or [W*O], junction
+ * fields [3][W*E] or [W*E], face fields [3][W*F] or [W*F]. */
+enum {
+  CB_FIELD_AMOUNT_INCREMENT = 0, CB_FIELD_EXTRACELLULAR_INCREMENT, CB_FIELD_MEMBRANE_TRANSFERRED,
+  CB_FIELD_JUNCTION_TRANSFERRED, CB_FIELD_FACE_TRANSFERRED, CB_FIELD_RESERVOIR_SUPPLIED,
+  CB_FIELD_MEMBRANE_DISSIPATED, CB_FIELD_JUNCTION_DISSIPATED, CB_FIELD_FACE_DISSIPATED,
+  CB_FIELD_ELECTRODE_CHARGE, CB_FIELD_RESERVOIR_WORK, CB_FIELD_ELECTRODE_WORK,
+  CB_FIELD_JUNCTION_GATE, CB_FIELD_PUMP_CYCLES, CB_FIELD_PUMP_DISSIPATED, CB_FIELD_METABOLIC_WORK,
+  CB_FIELD_STATE_FIELDS
+};
+
+/* Bind (host analysis: components, the nested-dissection plan of the free nodes' Laplacian;
+ * uploads) on `device`. Refuses (CB_ERR_LAYOUT) a topology outside the contract above. */
+int cb_field_bind(const cb_field_desc *desc, int device, cb_field **out);
+void cb_field_free(cb_field *f);
+int cb_field_state_layout(const cb_field *f, int64_t offsets[CB_FIELD_STATE_FIELDS],
+                          int64_t *total);
+/* Control: membrane [W*N], junction [W*E], pump [W*N] availabilities, back to back. */
+int64_t cb_field_control_length(const cb_field *f);
+/* n_steps ARS(2,2,2) steps of every world (checked_step repeated; a refused world keeps its
+ * last accepted state and stops). DEVICE pointers; state_in and state_out may alias. */
+int cb_field_step(cb_field *f, const double *state_in, double *state_out, double dt,
+                  const double *control, int n_steps, uint32_t *world_status,
+                  int32_t *accepted_steps, void *stream);
+/* cb_field_step with HOST buffers: copies in, steps, copies out, synchronizes. */
+int cb_field_step_host(cb_field *f, const double *state_in, double *state_out, double dt,
+                       const double *control, int n_steps, uint32_t *world_status,
+                       int32_t *accepted_steps);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,163 @@
+"""The device field step (cb_field_step: cells facing a resolved extracellular grid) against the
+reference's own trajectories (tests/golden/field_*.npz) and the field oracle (oracle/field.py).
+
+Tolerances, as the plain step's: every state field within 1e-10 scaled difference of the
+reference over the whole run, with one exception written out here. The held ring's supplies and
+reservoir work are small nets of the face fluxes into the ring, and the reference forms each
+face's diffusion as log(a) - log(b) of nearly equal concentrations next to the ring: one ulp of a
+logarithm (CUDA's and glibc's may differ by one) moves them by up to 5e-8 (supplies) and 1e-6
+(work) of their own maxima (measured by nudging the oracle's logs by one ulp). Those two fields
+are compared against the scale of the flows they net: the supplies against the largest face
+transfer, the work against 1e-3 x the largest |mu| x that transfer.
+
+The device solves the same equations by other means (a chord Newton on the floating offsets with
+the face Laplacian as its matrix, each cell eliminated into its node in the stage solves,
+nested-dissection sparse Cholesky), so agreement is to rounding, not bit for bit. A fused launch equals one-step launches bit for bit; a world's result does not depend
+on its batch position; the host entry point equals the device one bit for bit.
+"""
+
+import numpy as np
+import pytest
+import threadpoolctl
+
+from cells_b200 import field_worlds as FW
+from cells_b200 import worlds
+from cells_b200.field import FieldTissue
+from conftest import load_field_golden, scaled_difference
+from oracle import field as OF
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def run(torch, tissue, state, control, dt, chunks):
+    dev = torch.device("cuda", tissue.device)
+    buf = torch.from_numpy(tissue.pack_state(state)).to(dev)
+    ctl = torch.from_numpy(np.asarray(control, dtype=np.float64)).to(dev)
+    status = torch.zeros(tissue.W, dtype=torch.int32, device=dev)
+    taken = torch.zeros(tissue.W, dtype=torch.int32, device=dev)
+    total = np.zeros(tissue.W, dtype=np.int64)
+    for k in chunks:
+        tissue.step(buf, buf, ctl, dt, k, status, taken)
+        torch.cuda.synchronize(dev)
+        total += taken.cpu().numpy()
+    return tissue.unpack_state(buf.cpu().numpy()), status.cpu().numpy(), total
+
+
+@pytest.mark.parametrize("name", ["field_grid10.npz", "field_gated14.npz", "field_grid24.npz"])
+def test_field_step_matches_the_reference_trajectory(cuda, name):
+    z, w = load_field_golden(name)
+    tissue = FieldTissue([w])
+    control = tissue.pack_control(z["control_membrane"], z["control_junction"],
+                                  z["control_pump"])
+    dt = float(z["dt"])
+    state, done, worst = tissue.initial_state(), 0, {}
+    for idx, target in enumerate(z["steps"]):
+        if target > done:
+            state, status, taken = run(cuda, tissue, state, control, dt, [int(target - done)])
+            assert status[0] == 0, status
+            assert taken[0] == target - done
+            done = int(target)
+        for f in OF.FieldState._fields:
+            worst[f] = max(worst.get(f, 0.0), field_difference(
+                state[f][0], z["ref_" + f][idx], z["ref_face_transferred"][idx], w, f))
+    bad = {k: v for k, v in worst.items() if v > TOL}
+    assert not bad, (bad, worst)
+
+
+def field_difference(got, ref, face, w, f):
+    """scaled_difference, or for the ring's supplies and work the difference over the flows they
+    net (see the module's docstring); face: the reference's face transfers at that point."""
+    if f not in ("reservoir_supplied", "reservoir_work"):
+        return scaled_difference(got, ref)
+    flow = np.max(np.abs(face))
+    if f == "reservoir_work":
+        co = w.outside_amount / w.outside_volume
+        mu = OF.R * w.temperature * np.log(co) + OF.Z * OF.F * w.boundary_V
+        flow = 1e-3 * np.max(np.abs(mu)) * flow
+    return 0.0 if flow == 0 else float(np.max(np.abs(got - ref)) / flow)
+
+
+def small_batch(n=3, seed=21):
+    ws = [FW.field_world(16, 4, 3, worlds.world_rng(seed, k), gate=(0.015, 0.2, 1.0),
+                         junction_sigma=0.3) for k in range(n)]
+    return ws
+
+
+def test_field_batch_matches_the_oracle_per_world(cuda):
+    ws = small_batch()
+    rng = np.random.default_rng(5)
+    mem = rng.uniform(0.6, 1.0, (len(ws), ws[0].cells))
+    jun = rng.uniform(0.6, 1.0, (len(ws), ws[0].edges))
+    pmp = rng.uniform(0.6, 1.0, (len(ws), ws[0].cells))
+    tissue = FieldTissue(ws)
+    got, status, taken = run(cuda, tissue, tissue.initial_state(),
+                             tissue.pack_control(mem, jun, pmp), 5e-4, [12, 18])
+    assert np.all(status == 0) and np.all(taken == 30)
+    with threadpoolctl.threadpool_limits(limits=1, user_api="blas"):
+        for k, w in enumerate(ws):
+            tp = OF.bind(w)
+            st = OF.initial_state(w)
+            ctl = OF.Control(mem[k], jun[k], pmp[k])
+            for _ in range(30):
+                st, ok = OF.imex_step(st, 5e-4, ctl, w, tp)
+                assert ok
+            bad = {f: d for f in OF.FieldState._fields
+                   if (d := field_difference(got[f][k], getattr(st, f), st.face_transferred, w,
+                                             f)) > TOL}
+            assert not bad, (k, bad)
+
+
+def test_field_fused_launch_position_and_host_entry_are_bitwise(cuda):
+    ws = small_batch(3, seed=22)
+    tissue = FieldTissue(ws)
+    control = tissue.pack_control()
+    fused, s1, _ = run(cuda, tissue, tissue.initial_state(), control, 5e-4, [20])
+    single, s2, _ = run(cuda, tissue, tissue.initial_state(), control, 5e-4, [1] * 20)
+    assert np.all(s1 == 0) and np.all(s2 == 0)
+    for f in fused:
+        assert np.array_equal(fused[f], single[f]), f
+    # World 2 alone, and the batch reversed: the same bits.
+    alone = FieldTissue([ws[2]])
+    a, _, _ = run(cuda, alone, alone.initial_state(), alone.pack_control(), 5e-4, [20])
+    rev = FieldTissue(ws[::-1])
+    r, _, _ = run(cuda, rev, rev.initial_state(), rev.pack_control(), 5e-4, [20])
+    for f in fused:
+        assert np.array_equal(fused[f][2], a[f][0]), f
+        assert np.array_equal(fused[f][2], r[f][0]), f
+    host, status, taken = tissue.step_host(tissue.initial_state(), control, 5e-4, 20)
+    assert np.all(status == 0) and np.all(taken == 20)
+    for f in fused:
+        assert np.array_equal(fused[f], host[f]), f
+
+
+def test_field_refuses_a_world_and_keeps_its_state(cuda):
+    ws = small_batch(3, seed=23)
+    tissue = FieldTissue(ws)
+    membrane = np.ones((3, ws[0].cells))
+    membrane[1, 4] = 1.2  # world 1: an availability above 1
+    start = tissue.initial_state()
+    got, status, taken = run(cuda, tissue, start, tissue.pack_control(membrane=membrane), 5e-4,
+                             [5])
+    assert status[0] == 0 and status[2] == 0 and status[1] & 8
+    assert taken[1] == 0 and taken[0] == 5
+    for f in got:
+        assert np.array_equal(got[f][1], start[f][1]), f
+
+
+def test_field_ledgers_hold(cuda):
+    """Material per species: cells + free nodes - supplied = 0 (the total ledger), and every
+    held node's increment and every free node's supply stay exactly zero."""
+    ws = small_batch(2, seed=24)
+    tissue = FieldTissue(ws)
+    got, status, _ = run(cuda, tissue, tissue.initial_state(), tissue.pack_control(), 5e-4, [200])
+    assert np.all(status == 0)
+    held = ws[0].reservoir
+    for k, w in enumerate(ws):
+        total = (got["amount_increment"][k].sum(axis=1)
+                 + got["extracellular_increment"][k].sum(axis=1)
+                 - got["reservoir_supplied"][k].sum(axis=1))
+        scale = np.abs(w.amount).sum(axis=1) + np.abs(w.outside_amount).sum(axis=1)
+        assert np.all(np.abs(total) <= 1e-12 * scale), total
+        assert np.all(got["extracellular_increment"][k][:, held] == 0)
+        assert np.all(got["reservoir_supplied"][k][:, ~held] == 0)
