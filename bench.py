@@ -14,8 +14,12 @@ Workloads (``--workload``):
           -50 mV plus three 20 mV Gaussian bumps) after 2000 FP64 steps at dt = 1 ms with respect
           to every cell's P_Na, P_K, P_Cl, every junction's permeabilities and every channel
           population's permeability, checkpoints every 100 steps with recomputation.
-A bench step is one time step of every world (grid, uneven) or one gradient of every world's
-loss (adjoint: metric world-gradients/s).
+  field   256 worlds of 1024 cells in a 128x128 extracellular grid (10 um spacing, the boundary
+          ring held at the bath), 4-neighbour faces with log-normal conductivity (sigma 0.5),
+          ARS(2,2,2) with implicit face electromigration at dt = 0.5 ms, the start field by the
+          Newton on the floating offsets, the stage fields by sparse Cholesky, FP64.
+A bench step is one time step of every world (grid, uneven, field) or one gradient of every
+world's loss (adjoint: metric world-gradients/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -71,14 +75,16 @@ def parse():
     ap.add_argument("--warmup", type=int, default=None,
                     help="untimed bench steps first (default 100; adjoint: 3 gradients)")
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("grid", "uneven", "adjoint"), default="grid")
+    ap.add_argument("--workload", choices=("grid", "uneven", "adjoint", "field"), default="grid")
     ap.add_argument("--worlds", type=int, default=None,
                     help="worlds per GPU (default 4096 grid, 1024 uneven, 512 adjoint)")
     ap.add_argument("--cells", type=int, default=1024, help="adjoint: cells per world")
     ap.add_argument("--trajectory", type=int, default=2000, help="adjoint: steps per gradient")
     ap.add_argument("--every", type=int, default=100, help="adjoint: checkpoint interval")
-    ap.add_argument("--side", type=int, default=16)
-    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--side", type=int, default=None,
+                    help="grid tissues' side (16), or the field grid's (128)")
+    ap.add_argument("--field-cells", type=int, default=32, help="field: tissue side (cells)")
+    ap.add_argument("--dt", type=float, default=None, help="1 ms (0.5 ms for field)")
     ap.add_argument("--fuse", type=int, default=100,
                     help="time steps per kernel launch (the largest divisor of --steps up to it)")
     ap.add_argument("--e2e-calls", type=int, default=None,
@@ -200,6 +206,11 @@ def sample_tasks(args, n, steps):
 
 
 def workload_name(args):
+    if args.workload == "field":
+        return (f"spatial extracellular field: {args.worlds} worlds per GPU x "
+                f"{args.field_cells ** 2} cells in a {args.side}x{args.side} extracellular grid "
+                "(10 um, held ring), log-normal face conductivity (sigma 0.5), ARS(2,2,2) with "
+                f"implicit face electromigration, FP64, dt {args.dt:g} s")
     if args.workload == "adjoint":
         return (f"adjoint sensitivities: {args.worlds} worlds per GPU x {args.cells}-cell "
                 "Delaunay tissues, NaV1.2 m^3 h + HH K n^4 populations, gradient of each world's "
@@ -234,6 +245,11 @@ def cpu_baseline(args, samples_per_core=2, steps=100):
                        f"thread, {wall:.1f} s wall; world-gradients/s = that rate of world-"
                        f"cell-steps / ({args.cells} cells x {args.trajectory} steps)"),
         }
+    if args.workload == "field":
+        tasks = [("field", w, 7, FIELD_SAMPLE_SIDE, 10, args.dt) for w in range(n)]
+        cell_steps, wall, procs = cb.measure(tasks, cores, fn=cb.run_field_world)
+        return {"value": cell_steps / wall, "unit": UNIT, "cores": procs, "kind": "port",
+                "sample": field_sample(n, 10, wall)}
     if args.workload == "uneven":
         steps = max(2, steps // 10)
     tasks, stride = sample_tasks(args, n, steps)
@@ -248,6 +264,18 @@ def cpu_baseline(args, samples_per_core=2, steps=100):
     }
 
 
+FIELD_SAMPLE_SIDE = 24
+
+
+def field_sample(n, steps, wall=None):
+    text = (f"{n} field worlds of a {FIELD_SAMPLE_SIDE}x{FIELD_SAMPLE_SIDE} grid with a 6x6 "
+            f"tissue (the same laws), {steps} ARS(2,2,2) steps each, one world per process, "
+            "1 BLAS thread: the reference's field solver is dense in the floating offsets (a "
+            "15876 x 15876 solve per Newton iteration on the 128x128 grid), so the CPU sample "
+            "runs the largest grid of its golden runs; world·cell-steps/s of that world")
+    return text + (f", {wall:.1f} s wall" if wall is not None else "")
+
+
 def run_reference(args, rank):
     """The reference's CPU step (its oracle restatement) on the host cores: each bench step
     advances a strided sample of the workload's worlds (two per core) by ten time steps."""
@@ -258,9 +286,15 @@ def run_reference(args, rank):
     cores = os.cpu_count() or 1
     n = cores * 2
     adjoint = args.workload == "adjoint"
+    field = args.workload == "field"
     per_task = 10 if args.workload == "grid" else 3 if adjoint else 1
-    fn = cb.run_adjoint_world if adjoint else cb.run_world
-    tasks, stride = sample_tasks(args, n, per_task)
+    fn = cb.run_adjoint_world if adjoint else cb.run_field_world if field else cb.run_world
+    if field:
+        per_task = 2
+        tasks, stride = [("field", w, 7, FIELD_SAMPLE_SIDE, per_task, args.dt)
+                         for w in range(n)], 1
+    else:
+        tasks, stride = sample_tasks(args, n, per_task)
     with cb.pool(cores) as pool:
         pool.map(cb.prepare, tasks, chunksize=1)
         for _ in range(max(args.warmup, 0)):
@@ -280,6 +314,8 @@ def run_reference(args, rank):
                   "forward then the oracle adjoint back over them per bench step, one world per "
                   "process, 1 BLAS thread (the reference has no adjoint; its gradients would "
                   "come from jax.grad, and jax is not installed)")
+    elif field:
+        sample = field_sample(n, per_task) + " (per bench step)"
     else:
         sample = (f"{n} of the {args.worlds} worlds (every {stride}th) advanced {per_task} "
                   "ARS(2,2,2) steps per bench step, one world per process, 1 BLAS thread")
@@ -508,17 +544,146 @@ def run_adjoint(args, rank, world_size, local_rank, dist, base):
     return 0
 
 
+def field_bytes_per_world_step(tissue, info, solves=6):
+    """Algorithmic bytes per world per step of the field step: the state read and written once,
+    the parameters read once (per cell 11 doubles, per junction 5, per node 6, per face 3), each
+    of the step's two factors written once and read by each of its solves (the start field's
+    initial solve and chord corrections, the two stage solves: six on the benchmark's worlds),
+    and each factorisation's update matrices written and read once."""
+    state = tissue.state_total // tissue.W
+    params = 11 * tissue.N + 5 * tissue.E + 6 * tissue.O + 3 * tissue.F
+    factor = info["factor_doubles"] * (2 + solves)
+    updates = 2 * 2 * info["update_doubles"]
+    return 8 * (2 * state + params + factor + updates)
+
+
+def run_field(args, rank, world_size, local_rank, dist, base):
+    """The spatial-field workload: each bench step is one ARS(2,2,2) step of every world."""
+    import torch
+
+    from cells_b200 import field_worlds, worlds
+    from cells_b200.field import FieldTissue
+
+    dev = torch.device("cuda", local_rank)
+    ws = [field_worlds.field_world(args.side, args.field_cells, 3,
+                                   worlds.world_rng(7, rank * args.worlds + w))
+          for w in range(args.worlds)]
+    tissue = FieldTissue(ws, device=local_rank)
+    info = tissue.info()
+    cells = tissue.N * tissue.W
+    state0 = tissue.pack_state(tissue.initial_state())
+    state = torch.from_numpy(state0).to(dev)
+    control_np = tissue.pack_control()
+    control = torch.from_numpy(control_np).to(dev)
+    status = torch.zeros(tissue.W, dtype=torch.int32, device=dev)
+    taken = torch.zeros(tissue.W, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        tissue.step(state, state, control, args.dt, 1, status, taken,
+                    stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(local_rank)
+    clocks.start()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        tissue.step(state, state, control, args.dt, 1, status, taken,
+                    stream=stream.cuda_stream)
+    stop.record(stream)
+    torch.cuda.synchronize(dev)
+    clock = clocks.stop()
+    ms = start.elapsed_time(stop)
+    n_refused = int((status != 0).sum().item())
+    barrier()
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = cells * world_size * args.steps / (ms_max * 1e-3)
+    launch_ms = ms / args.steps
+    alg = field_bytes_per_world_step(tissue, info) * tissue.W
+    achieved = alg / (launch_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    # End to end through the C ABI with host buffers (cb_field_step_host: the state and control
+    # copied in, one step, the state and status copied out, every call).
+    host_state = tissue.unpack_state(state0)
+    e2e_value = None
+    if args.e2e_calls > 0:
+        tissue.step_host(host_state, control_np, args.dt, 1)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_calls):
+            tissue.step_host(host_state, control_np, args.dt, 1)
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e_value = cells * world_size * args.e2e_calls / e2e_s
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded field worlds)",
+            "config": {
+                "workload": workload_name(args), "method": METHOD,
+                "field_solver": "capacitive reduction, Newton on the floating offsets (chord, "
+                                "face Laplacian), nested-dissection multifrontal Cholesky",
+                "worlds_per_gpu": args.worlds, "cells_per_world": tissue.N,
+                "outside_nodes_per_world": tissue.O, "faces_per_world": tissue.F,
+                "junctions_per_world": tissue.E, "solver": info,
+                "parallelism": f"independent worlds x{world_size} (no collective)",
+                "l2": (f"inputs larger than L2: state {tissue.state_total * 8 / 1e6:.0f} MB, "
+                       f"scratch {info['scratch_bytes'] / 1e9:.1f} GB per GPU"),
+            },
+            "roofline": {
+                "bound": "hbm", "kernel": "field_kernel", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms,
+                "bytes_per_world_step": alg / tissue.W,
+            },
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * (tissue.state_total + tissue.control_total),
+                    "d2h_bytes_per_step": 8 * tissue.state_total + 8 * tissue.W,
+                    "calls": args.e2e_calls},
+            "gpu_launches": args.steps,
+            "refused_worlds": n_refused,
+            "clocks": clock,
+        }
+        if base is not None:
+            line["cpu_baseline"] = base
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     adjoint = args.workload == "adjoint"
+    field = args.workload == "field"
     if args.worlds is None:
-        args.worlds = {"uneven": 1024, "adjoint": 512}.get(args.workload, 4096)
+        args.worlds = {"uneven": 1024, "adjoint": 512, "field": 256}.get(args.workload, 4096)
+    if args.side is None:
+        args.side = 128 if field else 16
+    if args.dt is None:
+        args.dt = 5e-4 if field else 1e-3
     if args.steps is None:
-        args.steps = 3 if adjoint else 1000
+        args.steps = 3 if adjoint else 10 if field else 1000
     if args.warmup is None:
-        args.warmup = 3 if adjoint else 100
+        args.warmup = 3 if adjoint or field else 100
     if args.e2e_calls is None:
-        args.e2e_calls = 1 if adjoint else 3
+        args.e2e_calls = 1 if adjoint else 2 if field else 3
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -546,6 +711,8 @@ def main():
     torch.cuda.set_device(dev)
     if adjoint:
         return run_adjoint(args, rank, world_size, local_rank, dist, base)
+    if field:
+        return run_field(args, rank, world_size, local_rank, dist, base)
 
     from cells_b200 import _lib as _lib_methods
 

@@ -77,6 +77,7 @@ EXPORTS = (
     "cb_field_free",
     "cb_field_state_layout",
     "cb_field_control_length",
+    "cb_field_info",
     "cb_field_step",
     "cb_field_step_host",
     "cb_last_error",
@@ -219,6 +220,8 @@ def load(path=LIBRARY):
     lib.cb_field_free.restype = None
     lib.cb_field_state_layout.argtypes = [_p, _i64, _i64]
     lib.cb_field_state_layout.restype = ctypes.c_int
+    lib.cb_field_info.argtypes = [_p, _i64]
+    lib.cb_field_info.restype = ctypes.c_int
     lib.cb_field_control_length.argtypes = [_p]
     lib.cb_field_control_length.restype = ctypes.c_int64
     lib.cb_field_step.argtypes = [_p, _p, _p, ctypes.c_double, _p, ctypes.c_int, _p, _p, _p]

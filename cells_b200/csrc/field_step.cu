@@ -51,7 +51,10 @@ constexpr double kCurrentRtol = 2e-12;   // CURRENT_RTOL
 constexpr int kMaxIterations = 16;       // solve's max_iterations
 constexpr int kMaxBacktracks = 12;       // max_backtracks
 constexpr int kFieldBlock = 512;
-constexpr int kRefineRounds = 1;         // FP64 refinement rounds of each stage solve
+constexpr int kWarpSlice = 1536;  // doubles of shared memory per warp for small fronts:
+constexpr int kWarpBlock = 1280;  // the front's block, then its vector (m <= kWarpSlice - kWarpBlock)
+constexpr long long kMaxSmemBytes = 227 * 1024;
+constexpr int kRefineRounds = 0;         // FP64 refinement rounds of each stage solve
 constexpr double kChargeAtol = 3e-25;    // surface_field.CHARGE_ATOL_C
 constexpr double kChargeRtol = 2e-12;    // CHARGE_RTOL
 
@@ -69,10 +72,18 @@ struct Topo {  // shared by every world
   const int *cj_ptr, *cj_idx;  // cell -> junctions, edge order: e << 1 | (1 when the receiver)
   const int *fs, *fr;    // [F]
   const int *js, *jr;    // [E]
-  const int *face_pos;   // [F] off-diagonal factor entry of a face between free nodes, or -1
-  const int *colp, *lrow, *ukp, *ukc, *ukpos, *ukrel, *rel, *lvp, *lvc;
+  const int *col_node;   // [U] each factor column's node
+  // Supernodes (the multifrontal factor): first column, columns, front rows; offsets of each
+  // front's factor block (m x s, column-major), update matrix (b x b) and update vector (b);
+  // front rows; children; a child's boundary rows' positions in its parent's front; levels and
+  // whether a level's fronts are small enough for one warp each; each front's face entries.
+  const int *sn_c0, *sn_s, *sn_m;
+  const long long *sn_loff, *sn_uoff, *sn_voff;
+  const int *rows_ptr, *rows, *ch_ptr, *ch, *map_ptr, *map, *lv_ptr, *lv_sn, *lv_group;
+  const int *lv_block;     // a group level's region offset of the solve vector (its largest m x s)
+  long long smem_doubles;  // dynamic shared memory of the CTA
+  const int *af_ptr, *af_face, *af_pos;
 };
-
 struct Params {  // per world, world-major
   const double *wc;      // [W][FW_STRIDE]
   const double *vol, *icap, *q0, *pcap, *logpcap;  // [W*N]
@@ -91,7 +102,7 @@ struct FLayout {
 
 // Scratch fields of one world, in doubles (offsets from the world's slice).
 struct Scratch {
-  long long lval, x, xt, dx, r, rt, y, phi, pc, co, lco, ci, lci, fm, ld, wp, ifc, ijc, k0, k1,
+  long long lval, uf, wv, x, xt, dx, r, rt, y, phi, pc, co, lco, ci, lci, fm, ld, wp, ifc, ijc, k0, k1,
       d1, d2, n1, o1, g1, cp, stride;
   // a rate block: cell amount [3N], membrane transferred [3N], md, cycles, pd, mw [N each],
   // junction transferred [3E], jd, gate [E each], face diffusion [3F], node extracellular [3O],
@@ -161,7 +172,8 @@ __global__ void __launch_bounds__(BLOCK, 1)
   const double *wc = P.wc + (size_t)w * FW_STRIDE;
   const double RT = wc[FW_RT], FRT = wc[FW_FRT], temp = wc[FW_T];
   double *base = scratch + (size_t)w * S.stride;
-  double *lval = base + S.lval;
+  double *LF = base + S.lval, *UF = base + S.uf, *WV = base + S.wv;
+  extern __shared__ double dsm[];
   double *X = base + S.x, *XT = base + S.xt, *DX = base + S.dx, *Rv = base + S.r,
          *RTv = base + S.rt, *Y = base + S.y;
   double *PHI = base + S.phi, *PC = base + S.pc;
@@ -177,88 +189,181 @@ __global__ void __launch_bounds__(BLOCK, 1)
   int taken = 0;
   uint32_t refused = 0u;
 
-  // ---- sparse factor and substitutions on the shared plan --------------------------------
-  auto factor_column = [&](int j) -> unsigned {
+  // ---- the multifrontal factor and substitutions on the shared supernodes ------------------
+  // A level's fronts run on groups of threads: one warp per front (lv_group 0: small fronts, a
+  // warp's slice of shared memory each), or G groups of BLOCK / G threads (lv_group G), each with
+  // its own region and named barrier; each group takes the level's fronts in turn.
+  //
+  // One front q by a group (gid in [0, gsize)) with region A: assemble the face Laplacian's
+  // entries of its columns (conductances g), add its children's update matrices (ascending),
+  // factor its m x s panel right-looking with one barrier per column (the trailing update uses
+  // the unscaled pivot column over the pivot; the column is scaled in the same pass and the
+  // pivots kept apart), subtract the panel's product from its update matrix, store the panel.
+  auto front = [&](int q, auto g, double *A, double *piv, int gid, int gsize, auto sync)
+      -> unsigned {
+    const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q], b = m - sc;
+    double *Uq = UF + T.sn_uoff[q];
     unsigned bad = 0;
-    const int cjp = T.colp[j];
-    for (int u = T.ukp[j]; u < T.ukp[j + 1]; ++u) {
-      const int kk = T.ukc[u], p = T.ukpos[u], r0 = T.ukrel[u];
-      const int cnt = T.colp[kk + 1] - p;
-      const double ljk = lval[p];
-      for (int t = lane; t < cnt; t += 32) lval[cjp + T.rel[r0 + t]] -= lval[p + t] * ljk;
-      __syncwarp();
+    for (int a = gid; a < m * sc; a += gsize) A[a] = 0.0;
+    for (int a = gid; a < b * b; a += gsize) Uq[a] = 0.0;
+    sync();
+    for (int k = gid; k < sc; k += gsize) {
+      const int node = T.col_node[c0 + k];
+      double d = 0.0;
+      for (int a = T.nf_ptr[node]; a < T.nf_ptr[node + 1]; ++a) d += g(T.nf_idx[a] >> 1);
+      A[k + k * m] = d;
     }
-    double piv = 0.0;
-    if (lane == 0) {
-      const double d = lval[cjp];
-      if (!(d > 0.0) || !is_finite(d)) bad = 1u;
-      piv = sqrt(d);
-      lval[cjp] = piv;
+    for (int a = T.af_ptr[q] + gid; a < T.af_ptr[q + 1]; a += gsize) A[T.af_pos[a]] = -g(T.af_face[a]);
+    sync();
+    for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
+      const int c = T.ch[t];
+      const int bc = T.sn_m[c] - T.sn_s[c];
+      const double *Uc = UF + T.sn_uoff[c];
+      const int *mp = T.map + T.map_ptr[c];
+      for (int a = gid; a < bc * bc; a += gsize) {
+        const int i = a % bc, j = a / bc;
+        if (i < j) continue;
+        const int pr = mp[i], pc = mp[j];
+        if (pc < sc) A[pr + pc * m] += Uc[a];
+        else Uq[(pr - sc) + (pc - sc) * b] += Uc[a];
+      }
+      sync();
     }
-    piv = __shfl_sync(0xffffffffu, piv, 0);
-    const double inv = 1.0 / piv;
-    const int len = T.colp[j + 1] - cjp;
-    for (int t = 1 + lane; t < len; t += 32) lval[cjp + t] *= inv;
-    __syncwarp();
+    for (int k = 0; k < sc; ++k) {
+      const double d = A[k + k * m];
+      if (gid == 0) {
+        if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+        piv[k] = sqrt(d);
+      }
+      const double inv_d = 1.0 / d, inv_p = 1.0 / sqrt(d);
+      const int rows_left = m - k - 1, cols_left = sc - k - 1;
+      // trailing entries (i >= j > k) and the pivot column's own scaling (j == k), one pass
+      for (int a = gid; a < rows_left * (cols_left + 1); a += gsize) {
+        const int i = k + 1 + a % rows_left, j = k + a / rows_left;
+        if (j == k) continue;
+        if (i >= j) A[i + j * m] -= A[i + k * m] * (A[j + k * m] * inv_d);
+      }
+      sync();
+      for (int i = k + 1 + gid; i < m; i += gsize) A[i + k * m] *= inv_p;
+      // the next column's trailing pass reads column k + 1 only, never column k
+    }
+    sync();
+    for (int k = gid; k < sc; k += gsize) A[k + k * m] = piv[k];
+    sync();
+    for (int a = gid; a < b * b; a += gsize) {
+      const int i = a % b, j = a / b;
+      if (i < j) continue;
+      double acc = Uq[a];
+      for (int k = 0; k < sc; ++k) acc -= A[sc + i + k * m] * A[sc + j + k * m];
+      Uq[a] = acc;
+    }
+    double *Lq = LF + T.sn_loff[q];
+    for (int a = gid; a < m * sc; a += gsize) Lq[a] = A[a];
+    sync();
     return bad;
   };
-  auto factor = [&]() -> unsigned {
-    unsigned bad = 0;
-    for (int lv = 0; lv < T.levels; ++lv) {
-      const int a0 = T.lvp[lv], a1 = T.lvp[lv + 1];
-      for (int a = a0 + warp; a < a1; a += WARPS) bad |= factor_column(T.lvc[a]);
-      __syncthreads();
+  // Run body(q, A, v, gid, gsize, sync, reduce) for every front of level lv on its groups.
+  auto level = [&](int lv, auto body) {
+    const int a0 = T.lv_ptr[lv], a1 = T.lv_ptr[lv + 1], G = T.lv_group[lv];
+    if (G == 0) {
+      double *A = dsm + (size_t)warp * kWarpSlice;
+      double *v = A + kWarpBlock;
+      auto sync = [] { __syncwarp(); };
+      auto reduce = [&](double x) {
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        return x;
+      };
+      for (int a = a0 + warp; a < a1; a += WARPS) body(T.lv_sn[a], A, v, lane, 32, sync, reduce);
+    } else {
+      const int gsize = BLOCK / G, grp = tid / gsize, gid = tid % gsize;
+      const int gw = gsize / 32, w0 = grp * gw;
+      double *A = dsm + (size_t)grp * (T.smem_doubles / G);
+      double *v = A + T.lv_block[lv];
+      auto sync = [&] { asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(gsize) : "memory"); };
+      auto reduce = [&](double x) {
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        sync();
+        if (lane == 0) sRed[warp] = x;
+        sync();
+        double t = 0.0;
+        for (int q = 0; q < gw; ++q) t += sRed[w0 + q];
+        return t;
+      };
+      for (int a = a0 + grp; a < a1; a += G) body(T.lv_sn[a], A, v, gid, gsize, sync, reduce);
     }
+    __syncthreads();
+  };
+  auto factor = [&](auto g) -> unsigned {
+    unsigned bad = 0;
+    for (int lv = 0; lv < T.levels; ++lv)
+      level(lv, [&](int q, double *A, double *v, int gid, int gsize, auto sync, auto) {
+        bad |= front(q, g, A, v, gid, gsize, sync);
+      });
     return block_or<BLOCK>(bad, sBits);
   };
-  auto warp_sum = [&](double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+  // Stage front q's factor block into A (one pipelined copy).
+  auto stage_block = [&](int q, double *A, int gid, int gsize) {
+    const int n = T.sn_m[q] * T.sn_s[q];
+    const double *Lq = LF + T.sn_loff[q];
+    for (int a = gid; a < n; a += gsize) A[a] = Lq[a];
   };
-  // L L^T x = y (y in Y by factor column, overwritten; x to the out vector by factor column).
+  // Forward substitution of front q: its columns' right-hand side plus its children's update
+  // vectors, the dense triangular solve, the update vector for its parent.
+  auto forward = [&](int q, double *A, double *v, int gid, int gsize, auto sync) {
+    const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
+    stage_block(q, A, gid, gsize);
+    for (int i = gid; i < m; i += gsize) v[i] = i < sc ? Y[c0 + i] : 0.0;
+    sync();
+    for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
+      const int c = T.ch[t];
+      const int bc = T.sn_m[c] - T.sn_s[c];
+      const double *vc = WV + T.sn_voff[c];
+      const int *mp = T.map + T.map_ptr[c];
+      for (int i = gid; i < bc; i += gsize) v[mp[i]] += vc[i];
+      sync();
+    }
+    for (int k = 0; k < sc; ++k) {
+      const double vk = v[k] / A[k + k * m];
+      for (int i = k + 1 + gid; i < m; i += gsize) v[i] -= A[i + k * m] * vk;
+      sync();
+      if (gid == 0) v[k] = vk;
+    }
+    sync();
+    double *vq = WV + T.sn_voff[q];
+    for (int i = gid; i < m; i += gsize) {
+      if (i < sc) Y[c0 + i] = v[i];
+      else vq[i - sc] = v[i];
+    }
+    sync();
+  };
+  // Back substitution of front q: x_S = L_SS^-T (y_S - L_BS^T x_B), x_B from its ancestors.
+  auto backward = [&](int q, double *A, double *v, double *out, int gid, int gsize, auto sync,
+                      auto reduce) {
+    const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
+    const int *rq = T.rows + T.rows_ptr[q];
+    stage_block(q, A, gid, gsize);
+    for (int i = sc + gid; i < m; i += gsize) v[i] = out[rq[i]];
+    sync();
+    for (int k = sc - 1; k >= 0; --k) {
+      double part = 0.0;
+      for (int i = k + 1 + gid; i < m; i += gsize) part += A[i + k * m] * v[i];
+      part = reduce(part);
+      if (gid == 0) v[k] = (Y[c0 + k] - part) / A[k + k * m];
+      sync();
+    }
+    for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k];
+    sync();
+  };
+  // L L^T x = y (y in Y by factor column, overwritten; x to out by factor column).
   auto solve = [&](double *out) {
-    for (int lv = 0; lv < T.levels; ++lv) {
-      const int a0 = T.lvp[lv], a1 = T.lvp[lv + 1];
-      for (int a = a0 + warp; a < a1; a += WARPS) {
-        const int j = T.lvc[a];
-        double part = 0.0;
-        for (int u = T.ukp[j] + lane; u < T.ukp[j + 1]; u += 32)
-          part += lval[T.ukpos[u]] * Y[T.ukc[u]];
-        part = warp_sum(part);
-        if (lane == 0) Y[j] = (Y[j] - part) / lval[T.colp[j]];
-      }
-      __syncthreads();
-    }
-    for (int lv = T.levels - 1; lv >= 0; --lv) {
-      const int a0 = T.lvp[lv], a1 = T.lvp[lv + 1];
-      for (int a = a0 + warp; a < a1; a += WARPS) {
-        const int j = T.lvc[a];
-        const int cjp = T.colp[j], len = T.colp[j + 1] - cjp;
-        double part = 0.0;
-        for (int t = 1 + lane; t < len; t += 32) part += lval[cjp + t] * out[T.lrow[cjp + t]];
-        part = warp_sum(part);
-        if (lane == 0) out[j] = (Y[j] - part) / lval[cjp];
-      }
-      __syncthreads();
-    }
-  };
-  // The face Laplacian with conductances g (a per-face functor) into the factor's storage.
-  auto assemble = [&](auto g) {
-    const long long nnz = T.colp[U];
-    for (long long a = tid; a < nnz; a += BLOCK) lval[a] = 0.0;
-    __syncthreads();
-    for (int m = tid; m < O; m += BLOCK) {
-      const int u = T.upos[m];
-      if (u < 0) continue;
-      double d = 0.0;
-      for (int a = T.nf_ptr[m]; a < T.nf_ptr[m + 1]; ++a) d += g(T.nf_idx[a] >> 1);
-      lval[T.colp[u]] = d;
-    }
-    for (int f = tid; f < F; f += BLOCK) {
-      const int p = T.face_pos[f];
-      if (p >= 0) lval[p] = -g(f);
-    }
-    __syncthreads();
+    for (int lv = 0; lv < T.levels; ++lv)
+      level(lv, [&](int q, double *A, double *v, int gid, int gsize, auto sync, auto) {
+        forward(q, A, v, gid, gsize, sync);
+      });
+    for (int lv = T.levels - 1; lv >= 0; --lv)
+      level(lv, [&](int q, double *A, double *v, int gid, int gsize, auto sync, auto reduce) {
+        backward(q, A, v, out, gid, gsize, sync, reduce);
+      });
   };
 
   // ---- transport pieces --------------------------------------------------------------------
@@ -470,10 +575,8 @@ __global__ void __launch_bounds__(BLOCK, 1)
     for (int m = tid; m < O; m += BLOCK) PHI[m] = T.upos[m] < 0 ? P.vb[o0 + m] : 0.0;
     __syncthreads();
     // The face conductance Laplacian (F^2/RT sum z^2 factor mean) and its factor.
-    assemble([&](int f) {
-      return kF * kF / RT * ((FM[f] + FM[F + f]) + FM[2 * F + f]);
-    });
-    if (factor()) bits |= CB_WORLD_FIELD;
+    if (factor([&](int f) { return kF * kF / RT * ((FM[f] + FM[F + f]) + FM[2 * F + f]); }))
+      bits |= CB_WORLD_FIELD;
     // ---- the start field: Newton on the free nodes' potentials (the floating offsets) -----
     // residual at potentials PHI (cells PC = node + relative): face currents, then junctions.
     auto cell_potentials = [&](double *dst) {
@@ -623,8 +726,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
     auto gface = [&](int f) {
       return k.gamma_dt * (cond * ((WP[f] + WP[F + f]) + WP[2 * F + f]));
     };
-    assemble(gface);
-    if (factor()) bits |= CB_WORLD_OPERATOR;
+    if (factor(gface)) bits |= CB_WORLD_OPERATOR;
     // ---- stages 1 and 2 ---------------------------------------------------------------------
     // The stage solve on known amounts (cells n(s,i), nodes o(s,m)): potentials into PHI, PC.
     auto stage_solve = [&](auto n, auto o) {
@@ -879,7 +981,8 @@ __global__ void __launch_bounds__(BLOCK, 1)
 struct cb_field {
   int device = 0;
   int W = 0, N = 0, O = 0, E = 0, F = 0, U = 0, levels = 0;
-  long long nnz = 0;
+  long long lsize = 0, usize = 0, vsize = 0, smem_doubles = 0;
+  int supernodes = 0;
   Topo topo{};
   Params params{};
   FLayout layout{};
@@ -922,24 +1025,38 @@ double host_logaddexp0(double y) {
 
 // Nested dissection of the free nodes of a side x side grid whose held nodes are its ring: the
 // free box (side - 2)^2, split across its longer side by a middle line, the line last.
-void nested_dissection(int x0, int x1, int y0, int y1, int width, std::vector<int> &order) {
+// Each leaf block (at most kLeafNodes nodes) becomes one relaxed supernode: group gets its id for
+// the block's columns, -1 for separator columns.
+constexpr int kLeafNodes = 16;
+void nested_dissection(int x0, int x1, int y0, int y1, int width, std::vector<int> &order,
+                       std::vector<int> &group, int &groups) {
   const int w = x1 - x0, h = y1 - y0;
   if (w <= 0 || h <= 0) return;
-  if (w * h <= 16) {
+  if (w * h <= kLeafNodes) {
     for (int y = y0; y < y1; ++y)
-      for (int x = x0; x < x1; ++x) order.push_back(y * width + x);
+      for (int x = x0; x < x1; ++x) {
+        order.push_back(y * width + x);
+        group.push_back(groups);
+      }
+    ++groups;
     return;
   }
   if (w >= h) {
     const int mid = x0 + w / 2;
-    nested_dissection(x0, mid, y0, y1, width, order);
-    nested_dissection(mid + 1, x1, y0, y1, width, order);
-    for (int y = y0; y < y1; ++y) order.push_back(y * width + mid);
+    nested_dissection(x0, mid, y0, y1, width, order, group, groups);
+    nested_dissection(mid + 1, x1, y0, y1, width, order, group, groups);
+    for (int y = y0; y < y1; ++y) {
+      order.push_back(y * width + mid);
+      group.push_back(-1);
+    }
   } else {
     const int mid = y0 + h / 2;
-    nested_dissection(x0, x1, y0, mid, width, order);
-    nested_dissection(x0, x1, mid + 1, y1, width, order);
-    for (int x = x0; x < x1; ++x) order.push_back(mid * width + x);
+    nested_dissection(x0, x1, y0, mid, width, order, group, groups);
+    nested_dissection(x0, x1, mid + 1, y1, width, order, group, groups);
+    for (int x = x0; x < x1; ++x) {
+      order.push_back(mid * width + x);
+      group.push_back(-1);
+    }
   }
 }
 
@@ -1057,9 +1174,11 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
       grid = dx + dy == 1;
     }
   }
+  std::vector<int> group;
   if (grid) {
     std::vector<int> cells;
-    nested_dissection(0, side - 2, 0, side - 2, side - 2, cells);
+    int groups = 0;
+    nested_dissection(0, side - 2, 0, side - 2, side - 2, cells, group, groups);
     // cells index the free box row-major; map to free-node indices.
     for (int c : cells) {
       const int x = c % (side - 2) + 1, y = c / (side - 2) + 1;
@@ -1075,8 +1194,6 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
   auto *f = new cb_field();
   f->device = device;
   f->W = W, f->N = N, f->O = O, f->E = E, f->F = F, f->U = U;
-  f->levels = (int)plan.level_ptr.size() - 1;
-  f->nnz = plan.colp[U];
   auto bail = [&](int code) {
     cb_field_free(f);
     return code;
@@ -1108,21 +1225,76 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
       cj_idx.insert(cj_idx.end(), lists[i].begin(), lists[i].end());
     }
   }
-  std::vector<int> face_pos(F, -1);
-  for (size_t q = 0; q < gface.size(); ++q) face_pos[gface[q]] = plan.edge_pos[q];
+  // Supernodes and each front's face entries (row = the later column, column = the earlier).
+  SuperPlan sp;
+  if ((rc = build_supernodes(plan, sp, grid ? &group : nullptr))) return bail(rc);
+  std::vector<int> col_node(U), af_ptr(sp.count + 1, 0), af_face, af_pos;
+  for (int u = 0; u < U; ++u) col_node[plan.rank[u]] = free_nodes[u];
+  {
+    std::vector<std::vector<std::pair<int, int>>> lists(sp.count);
+    for (size_t q = 0; q < gface.size(); ++q) {
+      const int ra = plan.rank[ga[q]], rb = plan.rank[gb[q]];
+      const int col = std::min(ra, rb), row = std::max(ra, rb);
+      const int sn = sp.sn_of[col];
+      const int *rq = sp.rows.data() + sp.rows_ptr[sn];
+      const int *at = std::lower_bound(rq, rq + sp.m[sn], row);
+      if (at == rq + sp.m[sn] || *at != row) return bail(fail(CB_ERR_LAYOUT, "field: face outside its front"));
+      lists[sn].push_back({gface[q], (int)(at - rq) + (col - sp.c0[sn]) * sp.m[sn]});
+    }
+    for (int q = 0; q < sp.count; ++q) {
+      for (auto &pr : lists[q]) {
+        af_face.push_back(pr.first);
+        af_pos.push_back(pr.second);
+      }
+      af_ptr[q + 1] = (int)af_face.size();
+    }
+  }
+  // A level's fronts go one per warp when each fits a warp's slice of shared memory, else to
+  // the most groups (a power of two, at most the level's fronts) whose regions hold its block and
+  // vector.
+  const long long smem_doubles = kMaxSmemBytes / (long long)sizeof(double) - 64;
+  std::vector<int> lv_group(sp.levels, 0), lv_block(sp.levels, 0);
+  for (int l = 0; l < sp.levels; ++l) {
+    long long mb = 0;
+    int mm = 0;
+    for (int a = sp.lv_ptr[l]; a < sp.lv_ptr[l + 1]; ++a) {
+      const int q = sp.lv_sn[a];
+      mb = std::max(mb, (long long)sp.m[q] * sp.s[q]);
+      mm = std::max(mm, sp.m[q]);
+    }
+    lv_block[l] = (int)mb;
+    if (mb <= kWarpBlock && mm <= kWarpSlice - kWarpBlock) continue;
+    const int fronts = sp.lv_ptr[l + 1] - sp.lv_ptr[l];
+    int G = 1;
+    while (G * 2 <= fronts && G * 2 <= kFieldBlock / 64 && (G * 2) * (mb + mm) <= smem_doubles)
+      G *= 2;
+    if (G * (mb + mm) > smem_doubles)
+      return bail(fail(CB_ERR_UNSUPPORTED, "field: a front exceeds shared memory"));
+    lv_group[l] = G;
+  }
+  f->smem_doubles = smem_doubles;
+  f->levels = sp.levels;
+  f->supernodes = sp.count;
+  f->lsize = sp.lsize, f->usize = sp.usize, f->vsize = sp.vsize;
   Topo &T = f->topo;
-  T.N = N, T.O = O, T.E = E, T.F = F, T.U = U, T.levels = f->levels;
+  T.N = N, T.O = O, T.E = E, T.F = F, T.U = U, T.levels = sp.levels;
+  T.smem_doubles = f->smem_doubles;
+  std::vector<int> sn_c0 = sp.c0, sn_s = sp.s, sn_m = sp.m;
   if ((rc = upload(f, cell_node, &T.cell_node)) || (rc = upload(f, ncell, &T.ncell)) ||
       (rc = upload(f, upos, &T.upos)) || (rc = upload(f, nf_ptr, &T.nf_ptr)) ||
       (rc = upload(f, nf_idx, &T.nf_idx)) || (rc = upload(f, cj_ptr, &T.cj_ptr)) ||
       (rc = upload(f, cj_idx, &T.cj_idx)) || (rc = upload(f, fs, &T.fs)) ||
       (rc = upload(f, fr, &T.fr)) || (rc = upload(f, js, &T.js)) ||
-      (rc = upload(f, jr, &T.jr)) || (rc = upload(f, face_pos, &T.face_pos)) ||
-      (rc = upload(f, plan.colp, &T.colp)) || (rc = upload(f, plan.lrow, &T.lrow)) ||
-      (rc = upload(f, plan.uk_ptr, &T.ukp)) || (rc = upload(f, plan.uk_col, &T.ukc)) ||
-      (rc = upload(f, plan.uk_pos, &T.ukpos)) || (rc = upload(f, plan.uk_rel, &T.ukrel)) ||
-      (rc = upload(f, plan.rel, &T.rel)) || (rc = upload(f, plan.level_ptr, &T.lvp)) ||
-      (rc = upload(f, plan.level_cols, &T.lvc)))
+      (rc = upload(f, jr, &T.jr)) || (rc = upload(f, col_node, &T.col_node)) ||
+      (rc = upload(f, sn_c0, &T.sn_c0)) || (rc = upload(f, sn_s, &T.sn_s)) ||
+      (rc = upload(f, sn_m, &T.sn_m)) || (rc = upload(f, sp.loff, &T.sn_loff)) ||
+      (rc = upload(f, sp.uoff, &T.sn_uoff)) || (rc = upload(f, sp.voff, &T.sn_voff)) ||
+      (rc = upload(f, sp.rows_ptr, &T.rows_ptr)) || (rc = upload(f, sp.rows, &T.rows)) ||
+      (rc = upload(f, sp.ch_ptr, &T.ch_ptr)) || (rc = upload(f, sp.ch, &T.ch)) ||
+      (rc = upload(f, sp.map_ptr, &T.map_ptr)) || (rc = upload(f, sp.map, &T.map)) ||
+      (rc = upload(f, sp.lv_ptr, &T.lv_ptr)) || (rc = upload(f, sp.lv_sn, &T.lv_sn)) ||
+      (rc = upload(f, lv_group, &T.lv_group)) || (rc = upload(f, lv_block, &T.lv_block)) || (rc = upload(f, af_ptr, &T.af_ptr)) ||
+      (rc = upload(f, af_face, &T.af_face)) || (rc = upload(f, af_pos, &T.af_pos)))
     return bail(rc);
   // Per-world parameters.
   const long long WN = (long long)W * N, WO = (long long)W * O, WE = (long long)W * E,
@@ -1212,7 +1384,7 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
   S.rk_s = S.rk_x + 3LL * O;
   S.rk_ex = S.rk_s + 3LL * O;
   S.rk_size = S.rk_ex + 3LL * N;
-  S.lval = take(f->nnz);
+  S.lval = take(f->lsize), S.uf = take(f->usize), S.wv = take(std::max(f->vsize, 1LL));
   S.x = take(U), S.xt = take(U), S.dx = take(U), S.r = take(U), S.rt = take(U), S.y = take(U);
   S.phi = take(O), S.pc = take(N);
   S.co = take(3LL * O), S.lco = take(3LL * O), S.ci = take(3LL * N), S.lci = take(3LL * N);
@@ -1252,6 +1424,19 @@ extern "C" int cb_field_state_layout(const cb_field *f, int64_t offsets[CB_FIELD
   return CB_OK;
 }
 
+extern "C" int cb_field_info(const cb_field *f, int64_t info[8]) {
+  if (!f || !info) return fail(CB_ERR_ARGUMENT, "null argument");
+  info[0] = f->U;
+  info[1] = f->supernodes;
+  info[2] = f->levels;
+  info[3] = f->lsize;
+  info[4] = f->usize;
+  info[5] = f->vsize;
+  info[6] = f->smem_doubles * (int64_t)sizeof(double);
+  info[7] = f->scratch.stride * (int64_t)f->W * (int64_t)sizeof(double);
+  return CB_OK;
+}
+
 extern "C" int64_t cb_field_control_length(const cb_field *f) {
   if (!f) return -1;
   return (long long)f->W * (2LL * f->N + f->E);
@@ -1272,7 +1457,11 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
                          cudaMemcpyDeviceToDevice, s);
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpyAsync");
   }
-  field_kernel<kFieldBlock><<<f->W, kFieldBlock, 0, s>>>(
+  const size_t smem = (size_t)f->smem_doubles * sizeof(double);
+  ce = cudaFuncSetAttribute(field_kernel<kFieldBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaFuncSetAttribute");
+  field_kernel<kFieldBlock><<<f->W, kFieldBlock, smem, s>>>(
       f->topo, f->params, f->layout, f->scratch, state_out, control, step_coef(dt), n_steps,
       world_status,
       accepted_steps, f->scratch_buf);

@@ -140,4 +140,133 @@ inline int plan_world(int n, const int *snd, const int *rcv, int ne, WorldPlan &
   return CB_OK;
 }
 
+// Supernodes of a plan's factor (the multifrontal form of its factorisation): column j joins the
+// supernode of column j - 1 when j - 1 is j's only child and struct(j - 1) = {j - 1} + struct(j), so a
+// supernode's columns share one dense front: rows c0 .. c1 - 1 (its columns) then its boundary B
+// (rows of later supernodes). Each front is factored densely (its s x s diagonal block, the b x s
+// block below), leaving the update matrix B x B for its parent; the parent adds its children's
+// update matrices into its own front (extend-add) in ascending child order. Levels: a
+// supernode's level is one above its highest child's.
+struct SuperPlan {
+  int count = 0, levels = 0;
+  std::vector<int> c0, s, m;                // first column, columns, front rows
+  std::vector<long long> loff, uoff, voff;  // factor block (m x s), update matrix (b x b), vector
+  std::vector<int> rows_ptr, rows;          // each front's rows (factor columns, ascending)
+  std::vector<int> ch_ptr, ch;              // each supernode's children, ascending
+  std::vector<int> map_ptr, map;            // a child's boundary rows' positions in its parent
+  std::vector<int> parent;                  // -1 at a root
+  std::vector<int> lv_ptr, lv_sn;           // supernodes level by level
+  std::vector<int> sn_of;                   // column -> supernode
+  long long lsize = 0, usize = 0, vsize = 0;
+  long long max_block = 0;                  // largest m x s
+  int max_m = 0;
+};
+
+// group (optional, by column): consecutive columns with the same non-negative id form one
+// supernode (a relaxed supernode: a connected subtree of the elimination tree, its front rows the
+// union of its columns' structures, its diagonal block dense); columns with id -1 follow the
+// fundamental rule.
+inline int build_supernodes(const WorldPlan &p, SuperPlan &sp,
+                            const std::vector<int> *group = nullptr) {
+  const int n = (int)p.colp.size() - 1;
+  auto len = [&](int j) { return p.colp[j + 1] - p.colp[j]; };
+  auto par = [&](int j) { return len(j) > 1 ? p.lrow[p.colp[j] + 1] : -1; };
+  sp = SuperPlan();
+  sp.sn_of.assign(n, -1);
+  std::vector<int> children(n, 0);
+  for (int j = 0; j < n; ++j)
+    if (par(j) >= 0) children[par(j)]++;
+  for (int j = 0; j < n; ++j) {
+    // fundamental supernodes: j - 1 is j's only child
+    bool join = j > 0 && par(j - 1) == j && children[j] == 1 && len(j - 1) == len(j) + 1;
+    if (group) {
+      const int gj = (*group)[j], gp = j > 0 ? (*group)[j - 1] : -2;
+      if (gj >= 0 || gp >= 0) join = j > 0 && gj >= 0 && gj == gp;
+    }
+    if (!join) {
+      sp.c0.push_back(j);
+      sp.s.push_back(0);
+    }
+    sp.s.back() += 1;
+    sp.sn_of[j] = (int)sp.c0.size() - 1;
+  }
+  const int S = sp.count = (int)sp.c0.size();
+  sp.m.resize(S);
+  sp.parent.assign(S, -1);
+  sp.rows_ptr.assign(S + 1, 0);
+  for (int q = 0; q < S; ++q) {
+    const int c = sp.c0[q], c1 = c + sp.s[q];
+    // Rows: the supernode's columns, then the union of its columns' rows beyond it.
+    std::set<int> beyond;
+    for (int k = c; k < c1; ++k)
+      for (int t = p.colp[k]; t < p.colp[k + 1]; ++t)
+        if (p.lrow[t] >= c1) beyond.insert(p.lrow[t]);
+    for (int k = c; k < c1; ++k) sp.rows.push_back(k);
+    sp.rows.insert(sp.rows.end(), beyond.begin(), beyond.end());
+    sp.rows_ptr[q + 1] = (int)sp.rows.size();
+    sp.m[q] = sp.rows_ptr[q + 1] - sp.rows_ptr[q];
+    if (!beyond.empty()) sp.parent[q] = sp.sn_of[*beyond.begin()];
+    for (int k = c; k < c1; ++k)  // a relaxed supernode must be one subtree
+      if (par(k) >= 0 && par(k) >= c1 && par(k) != *beyond.begin())
+        return fail(CB_ERR_LAYOUT, "supernodes: a group is not one subtree");
+    // the supernode's columns are its first rows
+    for (int k = 0; k < sp.s[q]; ++k)
+      if (sp.rows[sp.rows_ptr[q] + k] != c + k)
+        return fail(CB_ERR_LAYOUT, "supernodes: inconsistent front rows");
+  }
+  std::vector<std::vector<int>> kids(S);
+  for (int q = 0; q < S; ++q)
+    if (sp.parent[q] >= 0) kids[sp.parent[q]].push_back(q);
+  sp.ch_ptr.assign(S + 1, 0);
+  for (int q = 0; q < S; ++q) {
+    sp.ch.insert(sp.ch.end(), kids[q].begin(), kids[q].end());
+    sp.ch_ptr[q + 1] = (int)sp.ch.size();
+  }
+  sp.map_ptr.assign(S + 1, 0);
+  for (int q = 0; q < S; ++q) {
+    const int b = sp.m[q] - sp.s[q];
+    if (sp.parent[q] >= 0) {
+      const int pq = sp.parent[q];
+      const int *pr = sp.rows.data() + sp.rows_ptr[pq];
+      const int pm = sp.m[pq];
+      for (int i = 0; i < b; ++i) {
+        const int r = sp.rows[sp.rows_ptr[q] + sp.s[q] + i];
+        const int *at = std::lower_bound(pr, pr + pm, r);
+        if (at == pr + pm || *at != r)
+          return fail(CB_ERR_LAYOUT, "supernodes: a boundary row is not in the parent's front");
+        sp.map.push_back((int)(at - pr));
+      }
+    } else if (b != 0) {
+      return fail(CB_ERR_LAYOUT, "supernodes: a root front has boundary rows");
+    }
+    sp.map_ptr[q + 1] = (int)sp.map.size();
+  }
+  // Levels (children precede parents: supernodes are numbered in column order).
+  std::vector<int> level(S, 0);
+  for (int q = 0; q < S; ++q)
+    if (sp.parent[q] >= 0) level[sp.parent[q]] = std::max(level[sp.parent[q]], level[q] + 1);
+  sp.levels = S ? 1 + *std::max_element(level.begin(), level.end()) : 0;
+  sp.lv_ptr.assign(sp.levels + 1, 0);
+  for (int q = 0; q < S; ++q) sp.lv_ptr[level[q] + 1]++;
+  for (int l = 0; l < sp.levels; ++l) sp.lv_ptr[l + 1] += sp.lv_ptr[l];
+  sp.lv_sn.assign(S, 0);
+  std::vector<int> fill(sp.lv_ptr.begin(), sp.lv_ptr.end() - 1);
+  for (int q = 0; q < S; ++q) sp.lv_sn[fill[level[q]]++] = q;
+  sp.loff.resize(S);
+  sp.uoff.resize(S);
+  sp.voff.resize(S);
+  for (int q = 0; q < S; ++q) {
+    const long long mm = sp.m[q], ss = sp.s[q], b = mm - ss;
+    sp.loff[q] = sp.lsize;
+    sp.lsize += mm * ss;
+    sp.uoff[q] = sp.usize;
+    sp.usize += b * b;
+    sp.voff[q] = sp.vsize;
+    sp.vsize += b;
+    sp.max_block = std::max(sp.max_block, mm * ss);
+    sp.max_m = std::max(sp.max_m, (int)mm);
+  }
+  return CB_OK;
+}
+
 }  // namespace cbk

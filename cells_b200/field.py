@@ -111,6 +111,15 @@ class FieldTissue:
         self.state_total = int(total.value)
         self.control_total = int(self.lib.cb_field_control_length(self.handle))
 
+    def info(self):
+        """cb_field_info: the solver's sizes (free nodes, fronts, levels, factor / update doubles
+        per world, shared memory per CTA, scratch bytes)."""
+        out = (ctypes.c_int64 * 8)()
+        _lib.check(self.lib.cb_field_info(self.handle, out))
+        keys = ("unknowns", "supernodes", "levels", "factor_doubles", "update_doubles",
+                "vector_doubles", "smem_bytes", "scratch_bytes")
+        return dict(zip(keys, (int(v) for v in out), strict=True))
+
     def __del__(self):
         handle = getattr(self, "handle", None)
         if handle is not None and handle.value:

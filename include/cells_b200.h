@@ -349,6 +349,10 @@ int cb_field_bind(const cb_field_desc *desc, int device, cb_field **out);
 void cb_field_free(cb_field *f);
 int cb_field_state_layout(const cb_field *f, int64_t offsets[CB_FIELD_STATE_FIELDS],
                           int64_t *total);
+/* The bound solver's sizes: info[0] free nodes (unknowns), [1] supernodes (fronts), [2] their
+ * levels, [3] factor doubles per world, [4] update-matrix doubles per world, [5] update-vector
+ * doubles per world, [6] shared memory bytes per CTA, [7] scratch bytes (all worlds). */
+int cb_field_info(const cb_field *f, int64_t info[8]);
 /* Control: membrane [W*N], junction [W*E], pump [W*N] availabilities, back to back. */
 int64_t cb_field_control_length(const cb_field *f);
 /* n_steps ARS(2,2,2) steps of every world (checked_step repeated; a refused world keeps its

@@ -59,6 +59,33 @@ def run_world(task):
     return b.cells * steps, elapsed
 
 
+FIELD_CELLS_SIDE, FIELD_STRIDE = 6, 3  # the sampled field world: a 6 x 6 tissue, stride 3
+
+
+def run_field_world(task):
+    """("field", world index, seed, grid side, steps, dt) -> (cell-steps, seconds): the field
+    oracle's ARS(2,2,2) step (the reference's face-electromigration step with its dense factored
+    field, bit for bit) on one field world."""
+    _pin_blas()
+    from cells_b200 import field_worlds, worlds
+    from oracle import field as OF
+
+    kind, w, seed, side, steps, dt = task
+    key = (kind, w, seed, side)
+    if key not in _WORLDS:
+        world = field_worlds.field_world(side, FIELD_CELLS_SIDE, FIELD_STRIDE,
+                                         worlds.world_rng(seed, w))
+        _WORLDS[key] = [world, OF.bind(world), OF.full_control(world), OF.initial_state(world)]
+    entry = _WORLDS[key]
+    world, tp, ctl, st = entry
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st, _ = OF.imex_step(st, dt, ctl, world, tp)
+    elapsed = time.perf_counter() - t0
+    entry[3] = st
+    return world.cells * steps, elapsed
+
+
 def run_adjoint_world(task):
     """(kind, world index, seed, size, steps, dt) -> (cell-steps, seconds): steps forward steps
     of the oracle, each state kept, then the oracle adjoint back over them from the cotangent of
@@ -86,8 +113,11 @@ def run_adjoint_world(task):
 def prepare(task):
     """Build (and keep) a task's world in this worker without stepping it."""
     _pin_blas()
-    kind, w, seed, size, _, _ = task
-    _world(kind, w, seed, size)
+    kind, w, seed, size, _, dt = task
+    if kind == "field":
+        run_field_world((kind, w, seed, size, 0, dt))
+    else:
+        _world(kind, w, seed, size)
     return os.getpid()
 
 
