@@ -51,9 +51,11 @@ constexpr double kCurrentRtol = 2e-12;   // CURRENT_RTOL
 constexpr int kMaxIterations = 16;       // solve's max_iterations
 constexpr int kMaxBacktracks = 12;       // max_backtracks
 constexpr int kFieldBlock = 512;
-constexpr int kWarpSlice = 1536;  // doubles of shared memory per warp for small fronts:
-constexpr int kWarpBlock = 1280;  // the front's block, then its vector (m <= kWarpSlice - kWarpBlock)
-constexpr long long kMaxSmemBytes = 227 * 1024;
+constexpr int kWarpBlock = 1280;  // a level's fronts go one per warp when their blocks fit this
+constexpr int kWarpVector = 256;  // ... and their fronts' rows this
+// Dynamic shared memory a level kernel may ask for: the 227 KB per CTA less room for its static
+// shared memory.
+constexpr long long kMaxSmemBytes = 227 * 1024 - 1024;
 constexpr int kRefineRounds = 0;         // FP64 refinement rounds of each stage solve
 constexpr double kChargeAtol = 3e-25;    // surface_field.CHARGE_ATOL_C
 constexpr double kChargeRtol = 2e-12;    // CHARGE_RTOL
@@ -79,9 +81,7 @@ struct Topo {  // shared by every world
   // whether a level's fronts are small enough for one warp each; each front's face entries.
   const int *sn_c0, *sn_s, *sn_m;
   const long long *sn_loff, *sn_uoff, *sn_voff;
-  const int *rows_ptr, *rows, *ch_ptr, *ch, *map_ptr, *map, *lv_ptr, *lv_sn, *lv_group;
-  const int *lv_block;     // a group level's region offset of the solve vector (its largest m x s)
-  long long smem_doubles;  // dynamic shared memory of the CTA
+  const int *rows_ptr, *rows, *ch_ptr, *ch, *map_ptr, *map, *lv_ptr, *lv_sn;
   const int *af_ptr, *af_face, *af_pos;
 };
 struct Params {  // per world, world-major
@@ -102,7 +102,7 @@ struct FLayout {
 
 // Scratch fields of one world, in doubles (offsets from the world's slice).
 struct Scratch {
-  long long lval, uf, wv, x, xt, dx, r, rt, y, phi, pc, co, lco, ci, lci, fm, ld, wp, ifc, ijc, k0, k1,
+  long long lval, uf, wv, ctl, x, xt, dx, r, rt, y, phi, pc, co, lco, ci, lci, fm, ld, wp, ifc, ijc, k0, k1,
       d1, d2, n1, o1, g1, cp, stride;
   // a rate block: cell amount [3N], membrane transferred [3N], md, cycles, pd, mw [N each],
   // junction transferred [3E], jd, gate [E each], face diffusion [3F], node extracellular [3O],
@@ -155,12 +155,267 @@ __device__ __forceinline__ double ghk(int s, double g, double cf, double ct, dou
   return s < 2 ? g * (cf * bm - ct * bp) : g * (cf * bp - ct * bm);
 }
 
+// The step's phases, launched in order by cb_field_step around the factor and solve levels.
+enum Phase { PH_START = 0, PH_NEWTON_INIT, PH_NEWTON_SEARCH, PH_AFTER_NEWTON, PH_STAGE1, PH_FINISH };
+
+// A factorisation's face conductances: a (b sum_s W_s(f)) over the faces' weights W.
+struct Conductance {
+  const double *w;
+  int F;
+  double a, b;
+  __device__ double operator()(int f) const {
+    return a * (b * ((w[f] + w[F + f]) + w[2 * F + f]));
+  }
+};
+
+// kind 0: the start field's Newton matrix (F^2/RT sum factor mean); kind 1: the stage operator
+// (gamma dt K F/(R T) sum W at the prediction).
+__device__ __forceinline__ Conductance conductance(const Params &P, const Scratch &S, double *base,
+                                                   int w, int F, int kind, double gamma_dt) {
+  const double *wc = P.wc + (size_t)w * FW_STRIDE;
+  if (kind == 0) return Conductance{base + S.fm, F, 1.0, kF * kF / wc[FW_RT]};
+  return Conductance{base + S.wp, F, gamma_dt, kChargePerFmol * kF / (kR * wc[FW_T])};
+}
+
+// One front q of one world by a group of gsize threads (gid in [0, gsize)) with shared region A
+// (its m x s block) and piv (s doubles): assemble the face Laplacian's entries of its columns,
+// add its children's update matrices (ascending), factor its m x s panel right-looking with one
+// barrier per column (the trailing update uses the unscaled pivot column over the pivot; the
+// column is scaled after the barrier, the pivots kept apart), subtract the panel's product from
+// its update matrix, store the panel. Returns nonzero (at gid 0) on a pivot that is not positive.
+template <class Sync>
+__device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
+                                 const Conductance &g, double *A, double *piv, int gid,
+                                 int gsize, Sync sync) {
+  const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q], b = m - sc;
+  double *Uq = UF + T.sn_uoff[q];
+  unsigned bad = 0;
+  for (int a = gid; a < m * sc; a += gsize) A[a] = 0.0;
+  for (int a = gid; a < b * b; a += gsize) Uq[a] = 0.0;
+  sync();
+  for (int k = gid; k < sc; k += gsize) {
+    const int node = T.col_node[c0 + k];
+    double d = 0.0;
+    for (int a = T.nf_ptr[node]; a < T.nf_ptr[node + 1]; ++a) d += g(T.nf_idx[a] >> 1);
+    A[k + k * m] = d;
+  }
+  for (int a = T.af_ptr[q] + gid; a < T.af_ptr[q + 1]; a += gsize) A[T.af_pos[a]] = -g(T.af_face[a]);
+  sync();
+  for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
+    const int c = T.ch[t];
+    const int bc = T.sn_m[c] - T.sn_s[c];
+    const double *Uc = UF + T.sn_uoff[c];
+    const int *mp = T.map + T.map_ptr[c];
+    for (int a = gid; a < bc * bc; a += gsize) {
+      const int i = a % bc, j = a / bc;
+      if (i < j) continue;
+      const int pr = mp[i], pc = mp[j];
+      if (pc < sc) A[pr + pc * m] += Uc[a];
+      else Uq[(pr - sc) + (pc - sc) * b] += Uc[a];
+    }
+    sync();
+  }
+  for (int k = 0; k < sc; ++k) {
+    const double d = A[k + k * m];
+    if (gid == 0) {
+      if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+      piv[k] = sqrt(d);
+    }
+    const double inv_d = 1.0 / d, inv_p = 1.0 / sqrt(d);
+    const int rows_left = m - k - 1, cols_left = sc - k - 1;
+    for (int a = gid; a < rows_left * (cols_left + 1); a += gsize) {
+      const int i = k + 1 + a % rows_left, j = k + a / rows_left;
+      if (j == k) continue;
+      if (i >= j) A[i + j * m] -= A[i + k * m] * (A[j + k * m] * inv_d);
+    }
+    sync();
+    for (int i = k + 1 + gid; i < m; i += gsize) A[i + k * m] *= inv_p;
+  }
+  sync();
+  for (int k = gid; k < sc; k += gsize) A[k + k * m] = piv[k];
+  sync();
+  for (int a = gid; a < b * b; a += gsize) {
+    const int i = a % b, j = a / b;
+    if (i < j) continue;
+    double acc = Uq[a];
+    for (int k = 0; k < sc; ++k) acc -= A[sc + i + k * m] * A[sc + j + k * m];
+    Uq[a] = acc;
+  }
+  double *Lq = LF + T.sn_loff[q];
+  for (int a = gid; a < m * sc; a += gsize) Lq[a] = A[a];
+  sync();
+  return bad;
+}
+
+// Forward substitution of front q: its columns' right-hand side (Y) plus its children's update
+// vectors, the dense triangular solve on the staged block, the update vector for its parent.
+template <class Sync>
+__device__ void front_forward(const Topo &T, const double *LF, double *WV, double *Y, int q,
+                              double *A, double *v, int gid, int gsize, Sync sync) {
+  const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
+  const double *Lq = LF + T.sn_loff[q];
+  for (int a = gid; a < m * sc; a += gsize) A[a] = Lq[a];
+  for (int i = gid; i < m; i += gsize) v[i] = i < sc ? Y[c0 + i] : 0.0;
+  sync();
+  for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
+    const int c = T.ch[t];
+    const int bc = T.sn_m[c] - T.sn_s[c];
+    const double *vc = WV + T.sn_voff[c];
+    const int *mp = T.map + T.map_ptr[c];
+    for (int i = gid; i < bc; i += gsize) v[mp[i]] += vc[i];
+    sync();
+  }
+  for (int k = 0; k < sc; ++k) {
+    const double vk = v[k] / A[k + k * m];
+    for (int i = k + 1 + gid; i < m; i += gsize) v[i] -= A[i + k * m] * vk;
+    sync();
+    if (gid == 0) v[k] = vk;
+  }
+  sync();
+  double *vq = WV + T.sn_voff[q];
+  for (int i = gid; i < m; i += gsize) {
+    if (i < sc) Y[c0 + i] = v[i];
+    else vq[i - sc] = v[i];
+  }
+}
+
+// Back substitution of front q: x_S = L_SS^-T (y_S - L_BS^T x_B), x_B from its ancestors (out).
+template <class Sync, class Reduce>
+__device__ void front_backward(const Topo &T, const double *LF, const double *Y, double *out,
+                               int q, double *A, double *v, int gid, int gsize, Sync sync,
+                               Reduce reduce) {
+  const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
+  const double *Lq = LF + T.sn_loff[q];
+  const int *rq = T.rows + T.rows_ptr[q];
+  for (int a = gid; a < m * sc; a += gsize) A[a] = Lq[a];
+  for (int i = sc + gid; i < m; i += gsize) v[i] = out[rq[i]];
+  sync();
+  for (int k = sc - 1; k >= 0; --k) {
+    double part = 0.0;
+    for (int i = k + 1 + gid; i < m; i += gsize) part += A[i + k * m] * v[i];
+    part = reduce(part);
+    if (gid == 0) v[k] = (Y[c0 + k] - part) / A[k + k * m];
+    sync();
+  }
+  for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k];
+}
+
+// Level kernels. Warp form: each warp one (front, world) task of the level, world-major, with a
+// slice of shared memory (the level's largest block, then its largest front's vector). CTA form:
+// one CTA of kGroupThreads per (front, world). Refused worlds are skipped.
+constexpr int kWarpsPerCta = 8;
+constexpr int kGroupThreads = 256;
+
+struct LevelTask {
+  int q, w;
+  bool ok;
+};
+
+__device__ __forceinline__ LevelTask warp_task(const Topo &T, const uint32_t *status, int a0,
+                                               int fronts, int W) {
+  const long long task = (long long)blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
+  if (task >= (long long)fronts * W) return {0, 0, false};
+  const int w = (int)(task / fronts);
+  return {T.lv_sn[a0 + (int)(task % fronts)], w, status[w] == 0u};
+}
+
+__device__ __forceinline__ double warp_reduce(double x) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
+    factor_warps(const Topo T, const Params P, const Scratch S, double *scratch,
+                 const uint32_t *status, int kind, double gamma_dt, int a0, int fronts, int W,
+                 int slice, int vec) {
+  extern __shared__ double sm[];
+  const LevelTask t = warp_task(T, status, a0, fronts, W);
+  if (!t.ok) return;
+  double *base = scratch + (size_t)t.w * S.stride;
+  double *A = sm + (size_t)(threadIdx.x >> 5) * slice;
+  const unsigned bad = front_factor(T, base + S.lval, base + S.uf, t.q,
+                                    conductance(P, S, base, t.w, T.F, kind, gamma_dt), A, A + vec,
+                                    threadIdx.x & 31, 32, [] { __syncwarp(); });
+  if (bad) base[S.ctl + 7] = 1.0;
+}
+
+__global__ void __launch_bounds__(kGroupThreads)
+    factor_group(const Topo T, const Params P, const Scratch S, double *scratch,
+                 const uint32_t *status, int kind, double gamma_dt, int a0, int vec) {
+  extern __shared__ double sm[];
+  const int w = blockIdx.y;
+  if (status[w] != 0u) return;
+  double *base = scratch + (size_t)w * S.stride;
+  const unsigned bad = front_factor(T, base + S.lval, base + S.uf, T.lv_sn[a0 + blockIdx.x],
+                                    conductance(P, S, base, w, T.F, kind, gamma_dt), sm, sm + vec,
+                                    threadIdx.x, kGroupThreads, [] { __syncthreads(); });
+  if (bad) base[S.ctl + 7] = 1.0;
+}
+
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
+    forward_warps(const Topo T, const Scratch S, double *scratch, const uint32_t *status, int a0,
+                  int fronts, int W, int slice, int vec) {
+  extern __shared__ double sm[];
+  const LevelTask t = warp_task(T, status, a0, fronts, W);
+  if (!t.ok) return;
+  double *base = scratch + (size_t)t.w * S.stride;
+  double *A = sm + (size_t)(threadIdx.x >> 5) * slice;
+  front_forward(T, base + S.lval, base + S.wv, base + S.y, t.q, A, A + vec, threadIdx.x & 31, 32,
+                [] { __syncwarp(); });
+}
+
+__global__ void __launch_bounds__(kGroupThreads)
+    forward_group(const Topo T, const Scratch S, double *scratch, const uint32_t *status, int a0,
+                  int vec) {
+  extern __shared__ double sm[];
+  const int w = blockIdx.y;
+  if (status[w] != 0u) return;
+  double *base = scratch + (size_t)w * S.stride;
+  front_forward(T, base + S.lval, base + S.wv, base + S.y, T.lv_sn[a0 + blockIdx.x], sm, sm + vec,
+                threadIdx.x, kGroupThreads, [] { __syncthreads(); });
+}
+
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
+    backward_warps(const Topo T, const Scratch S, double *scratch, const uint32_t *status,
+                   long long out_off, int a0, int fronts, int W, int slice, int vec) {
+  extern __shared__ double sm[];
+  const LevelTask t = warp_task(T, status, a0, fronts, W);
+  if (!t.ok) return;
+  double *base = scratch + (size_t)t.w * S.stride;
+  double *A = sm + (size_t)(threadIdx.x >> 5) * slice;
+  front_backward(T, base + S.lval, base + S.y, base + out_off, t.q, A, A + vec, threadIdx.x & 31,
+                 32, [] { __syncwarp(); }, warp_reduce);
+}
+
+__global__ void __launch_bounds__(kGroupThreads)
+    backward_group(const Topo T, const Scratch S, double *scratch, const uint32_t *status,
+                   long long out_off, int a0, int vec) {
+  extern __shared__ double sm[];
+  __shared__ double red[kGroupThreads / 32];
+  const int w = blockIdx.y;
+  if (status[w] != 0u) return;
+  double *base = scratch + (size_t)w * S.stride;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  auto reduce = [&](double x) {
+    x = warp_reduce(x);
+    __syncthreads();
+    if (lane == 0) red[warp] = x;
+    __syncthreads();
+    double t = 0.0;
+    for (int q = 0; q < kGroupThreads / 32; ++q) t += red[q];
+    return t;
+  };
+  front_backward(T, base + S.lval, base + S.y, base + out_off, T.lv_sn[a0 + blockIdx.x], sm,
+                 sm + vec, threadIdx.x, kGroupThreads, [] { __syncthreads(); }, reduce);
+}
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1)
-    field_kernel(const Topo T, const Params P, const FLayout L, const Scratch S,
-                 double *__restrict__ state, const double *__restrict__ control, const StepCoef k,
-                 int n_steps, uint32_t *__restrict__ status, int32_t *__restrict__ taken_out,
-                 double *__restrict__ scratch) {
+    field_phase(const Topo T, const Params P, const FLayout L, const Scratch S,
+                double *__restrict__ state, const double *__restrict__ control, const StepCoef k,
+                int phase, int first, uint32_t *__restrict__ status,
+                int32_t *__restrict__ taken_out, double *__restrict__ scratch,
+                int *__restrict__ any_active) {
   __shared__ double sRed[BLOCK / 32];
   __shared__ unsigned sBits[BLOCK / 32];
   constexpr int WARPS = BLOCK / 32;
@@ -172,8 +427,8 @@ __global__ void __launch_bounds__(BLOCK, 1)
   const double *wc = P.wc + (size_t)w * FW_STRIDE;
   const double RT = wc[FW_RT], FRT = wc[FW_FRT], temp = wc[FW_T];
   double *base = scratch + (size_t)w * S.stride;
-  double *LF = base + S.lval, *UF = base + S.uf, *WV = base + S.wv;
-  extern __shared__ double dsm[];
+  double *ctl = base + S.ctl;  // per world: bits, count, accepted, active, norm, rmax, taken, bad
+  if (status[w] != 0u) return;  // refused earlier in this call
   double *X = base + S.x, *XT = base + S.xt, *DX = base + S.dx, *Rv = base + S.r,
          *RTv = base + S.rt, *Y = base + S.y;
   double *PHI = base + S.phi, *PC = base + S.pc;
@@ -186,185 +441,6 @@ __global__ void __launch_bounds__(BLOCK, 1)
   auto st = [&](int f) { return state + L.s[f]; };
   const double dt = k.dt;
   const double omgamma_dt = (1.0 - (1.0 - 1.0 / sqrt(2.0))) * dt;  // (1 - gamma) dt
-  int taken = 0;
-  uint32_t refused = 0u;
-
-  // ---- the multifrontal factor and substitutions on the shared supernodes ------------------
-  // A level's fronts run on groups of threads: one warp per front (lv_group 0: small fronts, a
-  // warp's slice of shared memory each), or G groups of BLOCK / G threads (lv_group G), each with
-  // its own region and named barrier; each group takes the level's fronts in turn.
-  //
-  // One front q by a group (gid in [0, gsize)) with region A: assemble the face Laplacian's
-  // entries of its columns (conductances g), add its children's update matrices (ascending),
-  // factor its m x s panel right-looking with one barrier per column (the trailing update uses
-  // the unscaled pivot column over the pivot; the column is scaled in the same pass and the
-  // pivots kept apart), subtract the panel's product from its update matrix, store the panel.
-  auto front = [&](int q, auto g, double *A, double *piv, int gid, int gsize, auto sync)
-      -> unsigned {
-    const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q], b = m - sc;
-    double *Uq = UF + T.sn_uoff[q];
-    unsigned bad = 0;
-    for (int a = gid; a < m * sc; a += gsize) A[a] = 0.0;
-    for (int a = gid; a < b * b; a += gsize) Uq[a] = 0.0;
-    sync();
-    for (int k = gid; k < sc; k += gsize) {
-      const int node = T.col_node[c0 + k];
-      double d = 0.0;
-      for (int a = T.nf_ptr[node]; a < T.nf_ptr[node + 1]; ++a) d += g(T.nf_idx[a] >> 1);
-      A[k + k * m] = d;
-    }
-    for (int a = T.af_ptr[q] + gid; a < T.af_ptr[q + 1]; a += gsize) A[T.af_pos[a]] = -g(T.af_face[a]);
-    sync();
-    for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
-      const int c = T.ch[t];
-      const int bc = T.sn_m[c] - T.sn_s[c];
-      const double *Uc = UF + T.sn_uoff[c];
-      const int *mp = T.map + T.map_ptr[c];
-      for (int a = gid; a < bc * bc; a += gsize) {
-        const int i = a % bc, j = a / bc;
-        if (i < j) continue;
-        const int pr = mp[i], pc = mp[j];
-        if (pc < sc) A[pr + pc * m] += Uc[a];
-        else Uq[(pr - sc) + (pc - sc) * b] += Uc[a];
-      }
-      sync();
-    }
-    for (int k = 0; k < sc; ++k) {
-      const double d = A[k + k * m];
-      if (gid == 0) {
-        if (!(d > 0.0) || !is_finite(d)) bad = 1u;
-        piv[k] = sqrt(d);
-      }
-      const double inv_d = 1.0 / d, inv_p = 1.0 / sqrt(d);
-      const int rows_left = m - k - 1, cols_left = sc - k - 1;
-      // trailing entries (i >= j > k) and the pivot column's own scaling (j == k), one pass
-      for (int a = gid; a < rows_left * (cols_left + 1); a += gsize) {
-        const int i = k + 1 + a % rows_left, j = k + a / rows_left;
-        if (j == k) continue;
-        if (i >= j) A[i + j * m] -= A[i + k * m] * (A[j + k * m] * inv_d);
-      }
-      sync();
-      for (int i = k + 1 + gid; i < m; i += gsize) A[i + k * m] *= inv_p;
-      // the next column's trailing pass reads column k + 1 only, never column k
-    }
-    sync();
-    for (int k = gid; k < sc; k += gsize) A[k + k * m] = piv[k];
-    sync();
-    for (int a = gid; a < b * b; a += gsize) {
-      const int i = a % b, j = a / b;
-      if (i < j) continue;
-      double acc = Uq[a];
-      for (int k = 0; k < sc; ++k) acc -= A[sc + i + k * m] * A[sc + j + k * m];
-      Uq[a] = acc;
-    }
-    double *Lq = LF + T.sn_loff[q];
-    for (int a = gid; a < m * sc; a += gsize) Lq[a] = A[a];
-    sync();
-    return bad;
-  };
-  // Run body(q, A, v, gid, gsize, sync, reduce) for every front of level lv on its groups.
-  auto level = [&](int lv, auto body) {
-    const int a0 = T.lv_ptr[lv], a1 = T.lv_ptr[lv + 1], G = T.lv_group[lv];
-    if (G == 0) {
-      double *A = dsm + (size_t)warp * kWarpSlice;
-      double *v = A + kWarpBlock;
-      auto sync = [] { __syncwarp(); };
-      auto reduce = [&](double x) {
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        return x;
-      };
-      for (int a = a0 + warp; a < a1; a += WARPS) body(T.lv_sn[a], A, v, lane, 32, sync, reduce);
-    } else {
-      const int gsize = BLOCK / G, grp = tid / gsize, gid = tid % gsize;
-      const int gw = gsize / 32, w0 = grp * gw;
-      double *A = dsm + (size_t)grp * (T.smem_doubles / G);
-      double *v = A + T.lv_block[lv];
-      auto sync = [&] { asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(gsize) : "memory"); };
-      auto reduce = [&](double x) {
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        sync();
-        if (lane == 0) sRed[warp] = x;
-        sync();
-        double t = 0.0;
-        for (int q = 0; q < gw; ++q) t += sRed[w0 + q];
-        return t;
-      };
-      for (int a = a0 + grp; a < a1; a += G) body(T.lv_sn[a], A, v, gid, gsize, sync, reduce);
-    }
-    __syncthreads();
-  };
-  auto factor = [&](auto g) -> unsigned {
-    unsigned bad = 0;
-    for (int lv = 0; lv < T.levels; ++lv)
-      level(lv, [&](int q, double *A, double *v, int gid, int gsize, auto sync, auto) {
-        bad |= front(q, g, A, v, gid, gsize, sync);
-      });
-    return block_or<BLOCK>(bad, sBits);
-  };
-  // Stage front q's factor block into A (one pipelined copy).
-  auto stage_block = [&](int q, double *A, int gid, int gsize) {
-    const int n = T.sn_m[q] * T.sn_s[q];
-    const double *Lq = LF + T.sn_loff[q];
-    for (int a = gid; a < n; a += gsize) A[a] = Lq[a];
-  };
-  // Forward substitution of front q: its columns' right-hand side plus its children's update
-  // vectors, the dense triangular solve, the update vector for its parent.
-  auto forward = [&](int q, double *A, double *v, int gid, int gsize, auto sync) {
-    const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
-    stage_block(q, A, gid, gsize);
-    for (int i = gid; i < m; i += gsize) v[i] = i < sc ? Y[c0 + i] : 0.0;
-    sync();
-    for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
-      const int c = T.ch[t];
-      const int bc = T.sn_m[c] - T.sn_s[c];
-      const double *vc = WV + T.sn_voff[c];
-      const int *mp = T.map + T.map_ptr[c];
-      for (int i = gid; i < bc; i += gsize) v[mp[i]] += vc[i];
-      sync();
-    }
-    for (int k = 0; k < sc; ++k) {
-      const double vk = v[k] / A[k + k * m];
-      for (int i = k + 1 + gid; i < m; i += gsize) v[i] -= A[i + k * m] * vk;
-      sync();
-      if (gid == 0) v[k] = vk;
-    }
-    sync();
-    double *vq = WV + T.sn_voff[q];
-    for (int i = gid; i < m; i += gsize) {
-      if (i < sc) Y[c0 + i] = v[i];
-      else vq[i - sc] = v[i];
-    }
-    sync();
-  };
-  // Back substitution of front q: x_S = L_SS^-T (y_S - L_BS^T x_B), x_B from its ancestors.
-  auto backward = [&](int q, double *A, double *v, double *out, int gid, int gsize, auto sync,
-                      auto reduce) {
-    const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
-    const int *rq = T.rows + T.rows_ptr[q];
-    stage_block(q, A, gid, gsize);
-    for (int i = sc + gid; i < m; i += gsize) v[i] = out[rq[i]];
-    sync();
-    for (int k = sc - 1; k >= 0; --k) {
-      double part = 0.0;
-      for (int i = k + 1 + gid; i < m; i += gsize) part += A[i + k * m] * v[i];
-      part = reduce(part);
-      if (gid == 0) v[k] = (Y[c0 + k] - part) / A[k + k * m];
-      sync();
-    }
-    for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k];
-    sync();
-  };
-  // L L^T x = y (y in Y by factor column, overwritten; x to out by factor column).
-  auto solve = [&](double *out) {
-    for (int lv = 0; lv < T.levels; ++lv)
-      level(lv, [&](int q, double *A, double *v, int gid, int gsize, auto sync, auto) {
-        forward(q, A, v, gid, gsize, sync);
-      });
-    for (int lv = T.levels - 1; lv >= 0; --lv)
-      level(lv, [&](int q, double *A, double *v, int gid, int gsize, auto sync, auto reduce) {
-        backward(q, A, v, out, gid, gsize, sync, reduce);
-      });
-  };
 
   // ---- transport pieces --------------------------------------------------------------------
   // Concentrations and logs of a stage: cells from amounts n (functor (s, i)), nodes from o.
@@ -554,30 +630,19 @@ __global__ void __launch_bounds__(BLOCK, 1)
     return bits;
   };
 
-  for (int step = 0; step < n_steps && refused == 0u; ++step) {
-    unsigned bits = 0;
-    // ---- start concentrations, cell potentials relative to their nodes, face weights -------
-    bits |= set_conc([&](int s, int i) { return st(CB_FIELD_AMOUNT_INCREMENT)[s * WN + c0 + i]; },
-                     [&](int s, int m) {
-                       return st(CB_FIELD_EXTRACELLULAR_INCREMENT)[s * WO + o0 + m];
-                     });
+  // Per-world control words across the phases (doubles holding small integers and flags).
+  auto bits_in = [&]() { return (unsigned)ctl[0]; };
+  auto bits_out = [&](unsigned b) {
+    b = block_or<BLOCK>(b, sBits);
+    if (tid == 0) ctl[0] = (double)b;
     __syncthreads();
-    for (int f = tid; f < F; f += BLOCK) {
-      const int a = T.fs[f], b = T.fr[f];
-      for (int s = 0; s < 3; ++s) {
-        double mean, lg;
-        logmean(CO[s * O + a], CO[s * O + b], mean, lg);
-        FM[s * F + f] = P.ff[s * WF + f0 + f] * mean;
-        LD[s * F + f] = LCO[s * O + a] - LCO[s * O + b];
-      }
-    }
-    // Base potentials: free nodes 0, held nodes their boundary; cells q_c / C_c above their node.
-    for (int m = tid; m < O; m += BLOCK) PHI[m] = T.upos[m] < 0 ? P.vb[o0 + m] : 0.0;
-    __syncthreads();
-    // The face conductance Laplacian (F^2/RT sum z^2 factor mean) and its factor.
-    if (factor([&](int f) { return kF * kF / RT * ((FM[f] + FM[F + f]) + FM[2 * F + f]); }))
-      bits |= CB_WORLD_FIELD;
-    // ---- the start field: Newton on the free nodes' potentials (the floating offsets) -----
+  };
+  const double *n0 = st(CB_FIELD_AMOUNT_INCREMENT), *x0 = st(CB_FIELD_EXTRACELLULAR_INCREMENT);
+  const double *g0 = st(CB_FIELD_JUNCTION_GATE) + e0;
+  const double cond = kChargePerFmol * kF / (kR * temp);
+  auto gface = [&](int f) {
+    return k.gamma_dt * (cond * ((WP[f] + WP[F + f]) + WP[2 * F + f]));
+  };
     // residual at potentials PHI (cells PC = node + relative): face currents, then junctions.
     auto cell_potentials = [&](double *dst) {
       for (int i = tid; i < N; i += BLOCK) {
@@ -641,50 +706,199 @@ __global__ void __launch_bounds__(BLOCK, 1)
       }
       __syncthreads();
     };
-    // The initial offsets: the face currents' balance at the base potentials.
+  // The stage solve's right-hand side on known amounts (cells n(s,i), nodes o(s,m)), into Y (and
+  // RTv, kept for the residual check).
+  auto stage_rhs = [&](auto n, auto o) {
+    for (int m = tid; m < O; m += BLOCK) {
+      const int u = T.upos[m];
+      if (u < 0) continue;
+      double q = P.q0o[o0 + m] + kChargePerFmol * ((o(0, m) + o(1, m)) + (-o(2, m)));
+      const int i = T.ncell[m];
+      if (i >= 0)
+        q = q + (P.q0[c0 + i] + kChargePerFmol * ((n(0, i) + n(1, i)) + (-n(2, i))));
+      for (int a = T.nf_ptr[m]; a < T.nf_ptr[m + 1]; ++a) {
+        const int f = T.nf_idx[a] >> 1;
+        const int other = T.fs[f] == m ? T.fr[f] : T.fs[f];
+        if (T.upos[other] < 0) q += gface(f) * P.vb[o0 + other];
+      }
+      Y[u] = q;
+      RTv[u] = q;
+    }
+    __syncthreads();
+  };
+  // The stage solution X: potentials into PHI, PC, and the stage solve's acceptance (the
+  // residual r = b - L x on the free rows within CHARGE_ATOL + CHARGE_RTOL max(|b|, |L x|),
+  // numerics/surface_imex.py).
+  auto stage_post = [&](auto n) -> unsigned {
+    unsigned b = 0;
+    for (int m = tid; m < O; m += BLOCK) {
+      const int u = T.upos[m];
+      PHI[m] = u < 0 ? P.vb[o0 + m] : X[u];
+      if (u < 0) continue;
+      double diag = 0.0, off = 0.0;
+      for (int a = T.nf_ptr[m]; a < T.nf_ptr[m + 1]; ++a) {
+        const int f = T.nf_idx[a] >> 1;
+        const double g = gface(f);
+        diag += g;
+        const int other = T.fs[f] == m ? T.fr[f] : T.fs[f];
+        const int v = T.upos[other];
+        if (v >= 0) off += g * X[v];
+      }
+      const double lx = diag * X[u] - off;
+      const double r = RTv[u] - lx;
+      if (!(fabs(r) <= kChargeAtol + kChargeRtol * fmax(fabs(RTv[u]), fabs(lx)))) b = 1u;
+    }
+    __syncthreads();
+    for (int i = tid; i < N; i += BLOCK) {
+      const double q = P.q0[c0 + i] + kChargePerFmol * ((n(0, i) + n(1, i)) + (-n(2, i)));
+      PC[i] = PHI[T.cell_node[i]] + q * P.icap[c0 + i];
+      if (!is_finite(PC[i])) b = 1u;
+    }
+    for (int m = tid; m < O; m += BLOCK)
+      if (!is_finite(PHI[m])) b = 1u;
+    __syncthreads();
+    return b ? (unsigned)CB_WORLD_RESIDUAL : 0u;
+  };
+    // The implicit drift W z F/RT dv at the stage potentials into D.
+    auto drift = [&](double *D) {
+      for (int f = tid; f < F; f += BLOCK) {
+        const double dv = PHI[T.fs[f]] - PHI[T.fr[f]];
+        for (int s = 0; s < 3; ++s) {
+          const double z = s < 2 ? 1.0 : -1.0;
+          D[s * F + f] = WP[s * F + f] * (z * FRT) * dv;
+        }
+      }
+      __syncthreads();
+    };
+    // A node's drift inflow of species s (scatter to receivers less scatter from senders).
+    auto drift_inflow = [&](const double *D, int s, int m) {
+      double in = 0.0, out = 0.0;
+      for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
+        const int code = T.nf_idx[q];
+        if (code & 1) in += D[s * F + (code >> 1)];
+        else out += D[s * F + (code >> 1)];
+      }
+      return in - out;
+    };
+  auto known1_cell = [&](int s, int i) {
+    return n0[s * WN + c0 + i] + k.gamma_dt * K0[S.rk_n + s * N + i];
+  };
+  auto known1_node = [&](int s, int m) {
+    return x0[s * WO + o0 + m] + k.gamma_dt * K0[S.rk_x + s * O + m];
+  };
+  auto known2_cell = [&](int s, int i) {
+    return (n0[s * WN + c0 + i] + k.delta_dt * K0[S.rk_n + s * N + i]) +
+           k.omdelta_dt * K1[S.rk_n + s * N + i];
+  };
+  auto known2_node = [&](int s, int m) {
+    const bool held = T.upos[m] < 0;
+    return ((x0[s * WO + o0 + m] + k.delta_dt * K0[S.rk_x + s * O + m]) +
+            k.omdelta_dt * K1[S.rk_x + s * O + m]) +
+           omgamma_dt * (held ? 0.0 : drift_inflow(D1, s, m));
+  };
+  // The Newton's next right-hand side: -R for an active world, 0 otherwise.
+  auto newton_rhs = [&](bool active) {
+    for (int u = tid; u < U; u += BLOCK) Y[u] = active ? -Rv[u] : 0.0;
+    if (active && tid == 0) atomicOr(any_active, 1);
+    __syncthreads();
+  };
+
+  if (phase == PH_START) {
+    // ---- start concentrations, face weights, base potentials, the initial offsets' rhs --------
+    if (tid == 0) {
+      if (first) ctl[6] = 0.0;
+      ctl[0] = 0.0;
+      ctl[7] = 0.0;
+    }
+    unsigned bits = set_conc([&](int s, int i) { return n0[s * WN + c0 + i]; },
+                             [&](int s, int m) { return x0[s * WO + o0 + m]; });
+    __syncthreads();
+    for (int f = tid; f < F; f += BLOCK) {
+      const int a = T.fs[f], b = T.fr[f];
+      for (int s = 0; s < 3; ++s) {
+        double mean, lg;
+        logmean(CO[s * O + a], CO[s * O + b], mean, lg);
+        FM[s * F + f] = P.ff[s * WF + f0 + f] * mean;
+        LD[s * F + f] = LCO[s * O + a] - LCO[s * O + b];
+      }
+    }
+    // Base potentials: free nodes 0, held nodes their boundary; cells q_c / C_c above their node.
+    for (int m = tid; m < O; m += BLOCK) PHI[m] = T.upos[m] < 0 ? P.vb[o0 + m] : 0.0;
+    __syncthreads();
     double rmax, norm;
     evaluate(Rv, false, rmax, norm);
     for (int u = tid; u < U; u += BLOCK) Y[u] = -Rv[u];
-    __syncthreads();
-    solve(X);
-    set_phi(X);
-    bool accepted = evaluate(Rv, true, rmax, norm);
-    int count = 0;
-    while (count < kMaxIterations && norm > kNewtonTarget && accepted) {
-      const double before = rmax;
-      for (int u = tid; u < U; u += BLOCK) Y[u] = -Rv[u];
+    bits_out(bits);
+    return;
+  }
+  if (phase == PH_NEWTON_INIT || phase == PH_NEWTON_SEARCH) {
+    // ---- the start field: Newton on the free nodes' potentials (the floating offsets) -------
+    if (phase == PH_NEWTON_INIT) {
+      unsigned bits = bits_in() | (ctl[7] != 0.0 ? (unsigned)CB_WORLD_FIELD : 0u);
+      set_phi(X);
+      double rmax, norm;
+      const bool accepted = evaluate(Rv, true, rmax, norm);
+      const bool active = accepted && norm > kNewtonTarget;
       __syncthreads();
-      solve(DX);
-      bool ok = false;
-      double tmax = 0.0, tnorm = norm;
-      for (int bt = 0; bt < kMaxBacktracks && !ok; ++bt) {
-        const double h = ldexp(1.0, -bt);
-        for (int u = tid; u < U; u += BLOCK) XT[u] = X[u] + DX[u] * h;
-        __syncthreads();
-        set_phi(XT);
-        const bool valid = evaluate(RTv, true, tmax, tnorm);
-        ok = valid && (tmax < before || tnorm <= kNewtonTarget);
+      if (tid == 0) {
+        ctl[1] = 0.0;
+        ctl[2] = accepted ? 1.0 : 0.0;
+        ctl[3] = active ? 1.0 : 0.0;
+        ctl[4] = norm;
+        ctl[5] = rmax;
       }
-      norm = tnorm;
-      accepted = ok;
-      if (ok) {
-        for (int u = tid; u < U; u += BLOCK) {
-          X[u] = XT[u];
-          Rv[u] = RTv[u];
-        }
-        rmax = tmax;
-      }
-      ++count;
-      __syncthreads();
+      newton_rhs(active);
+      bits_out(bits);
+      return;
     }
+    if (ctl[3] == 0.0) {  // converged or stopped: keep the next solve's rhs at zero
+      newton_rhs(false);
+      return;
+    }
+    // One correction (DX, solved by the host's level launches) with its backtracking line search.
+    const double before = ctl[5];
+    double norm = ctl[4], tmax = 0.0, tnorm = norm;
+    bool ok = false;
+    for (int bt = 0; bt < kMaxBacktracks && !ok; ++bt) {
+      const double h = ldexp(1.0, -bt);
+      for (int u = tid; u < U; u += BLOCK) XT[u] = X[u] + DX[u] * h;
+      __syncthreads();
+      set_phi(XT);
+      const bool valid = evaluate(RTv, true, tmax, tnorm);
+      ok = valid && (tmax < before || tnorm <= kNewtonTarget);
+    }
+    norm = tnorm;
+    double rmax = before;
+    if (ok) {
+      for (int u = tid; u < U; u += BLOCK) {
+        X[u] = XT[u];
+        Rv[u] = RTv[u];
+      }
+      rmax = tmax;
+    }
+    __syncthreads();
+    const int count = (int)ctl[1] + 1;
+    const bool active = count < kMaxIterations && norm > kNewtonTarget && ok;
+    __syncthreads();
+    if (tid == 0) {
+      ctl[1] = (double)count;
+      ctl[2] = ok ? 1.0 : 0.0;
+      ctl[3] = active ? 1.0 : 0.0;
+      ctl[4] = norm;
+      ctl[5] = rmax;
+    }
+    newton_rhs(active);
+    return;
+  }
+  if (phase == PH_AFTER_NEWTON) {
+    unsigned bits = bits_in();
     set_phi(X);
     {
       double rm2, n2;
       const bool valid = evaluate(Rv, true, rm2, n2);
-      if (!(valid && accepted && n2 <= kNewtonTarget)) bits |= CB_WORLD_FIELD;
+      if (!(valid && ctl[2] != 0.0 && n2 <= kNewtonTarget)) bits |= CB_WORLD_FIELD;
     }
     // ---- stage 0: explicit rates at the start potentials ---------------------------------
-    const double *g0 = st(CB_FIELD_JUNCTION_GATE) + e0;
     bits |= explicit_rates(K0, [&](int e) { return g0[e]; });
     // The readouts' extracellular rate (membrane flux, whole face flux at the start field, the
     // pump's transfer) and the half-step prediction of the node concentrations.
@@ -722,113 +936,22 @@ __global__ void __launch_bounds__(BLOCK, 1)
       }
     }
     __syncthreads();
-    const double cond = kChargePerFmol * kF / (kR * temp);
-    auto gface = [&](int f) {
-      return k.gamma_dt * (cond * ((WP[f] + WP[F + f]) + WP[2 * F + f]));
-    };
-    if (factor(gface)) bits |= CB_WORLD_OPERATOR;
-    // ---- stages 1 and 2 ---------------------------------------------------------------------
-    // The stage solve on known amounts (cells n(s,i), nodes o(s,m)): potentials into PHI, PC.
-    auto stage_solve = [&](auto n, auto o) {
-      for (int m = tid; m < O; m += BLOCK) {
-        const int u = T.upos[m];
-        if (u < 0) continue;
-        double q = P.q0o[o0 + m] + kChargePerFmol * ((o(0, m) + o(1, m)) + (-o(2, m)));
-        const int i = T.ncell[m];
-        if (i >= 0)
-          q = q + (P.q0[c0 + i] + kChargePerFmol * ((n(0, i) + n(1, i)) + (-n(2, i))));
-        for (int a = T.nf_ptr[m]; a < T.nf_ptr[m + 1]; ++a) {
-          const int f = T.nf_idx[a] >> 1;
-          const int other = T.fs[f] == m ? T.fr[f] : T.fs[f];
-          if (T.upos[other] < 0) q += gface(f) * P.vb[o0 + other];
-        }
-        Y[u] = q;
-        RTv[u] = q;  // the right-hand side, kept for the refinement
-      }
-      __syncthreads();
-      solve(X);
-      // FP64 iterative refinement: r = b - L x on the free rows (the held nodes' terms are in b),
-      // one correction per round. The last round's residual is the stage solve's acceptance
-      // (|r| <= CHARGE_ATOL + CHARGE_RTOL max(|b|, |L x|), numerics/surface_imex.py).
-      unsigned rb = 0;
-      for (int round = 0; round <= kRefineRounds; ++round) {
-        for (int m = tid; m < O; m += BLOCK) {
-          const int u = T.upos[m];
-          if (u < 0) continue;
-          double diag = 0.0, off = 0.0;
-          for (int a = T.nf_ptr[m]; a < T.nf_ptr[m + 1]; ++a) {
-            const int f = T.nf_idx[a] >> 1;
-            const double g = gface(f);
-            diag += g;
-            const int other = T.fs[f] == m ? T.fr[f] : T.fs[f];
-            const int v = T.upos[other];
-            if (v >= 0) off += g * X[v];
-          }
-          const double lx = diag * X[u] - off;
-          const double r = RTv[u] - lx;
-          Y[u] = r;
-          if (round == kRefineRounds &&
-              !(fabs(r) <= kChargeAtol + kChargeRtol * fmax(fabs(RTv[u]), fabs(lx))))
-            rb = 1u;
-        }
-        __syncthreads();
-        if (round == kRefineRounds) break;
-        solve(XT);
-        for (int u = tid; u < U; u += BLOCK) X[u] += XT[u];
-        __syncthreads();
-      }
-      for (int m = tid; m < O; m += BLOCK) {
-        const int u = T.upos[m];
-        PHI[m] = u < 0 ? P.vb[o0 + m] : X[u];
-      }
-      __syncthreads();
-      unsigned b = 0;
-      for (int i = tid; i < N; i += BLOCK) {
-        const double q = P.q0[c0 + i] + kChargePerFmol * ((n(0, i) + n(1, i)) + (-n(2, i)));
-        PC[i] = PHI[T.cell_node[i]] + q * P.icap[c0 + i];
-        if (!is_finite(PC[i])) b = 1u;
-      }
-      for (int m = tid; m < O; m += BLOCK)
-        if (!is_finite(PHI[m])) b = 1u;
-      __syncthreads();
-      return (b | rb) ? (unsigned)CB_WORLD_RESIDUAL : 0u;
-    };
-    // The implicit drift W z F/RT dv at the stage potentials into D.
-    auto drift = [&](double *D) {
-      for (int f = tid; f < F; f += BLOCK) {
-        const double dv = PHI[T.fs[f]] - PHI[T.fr[f]];
-        for (int s = 0; s < 3; ++s) {
-          const double z = s < 2 ? 1.0 : -1.0;
-          D[s * F + f] = WP[s * F + f] * (z * FRT) * dv;
-        }
-      }
-      __syncthreads();
-    };
-    // A node's drift inflow of species s (scatter to receivers less scatter from senders).
-    auto drift_inflow = [&](const double *D, int s, int m) {
-      double in = 0.0, out = 0.0;
-      for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
-        const int code = T.nf_idx[q];
-        if (code & 1) in += D[s * F + (code >> 1)];
-        else out += D[s * F + (code >> 1)];
-      }
-      return in - out;
-    };
-    const double *n0 = st(CB_FIELD_AMOUNT_INCREMENT), *x0 = st(CB_FIELD_EXTRACELLULAR_INCREMENT);
-    // Stage 1: known = y + (gamma dt) k0.
-    bits |= stage_solve(
-        [&](int s, int i) { return n0[s * WN + c0 + i] + k.gamma_dt * K0[S.rk_n + s * N + i]; },
-        [&](int s, int m) { return x0[s * WO + o0 + m] + k.gamma_dt * K0[S.rk_x + s * O + m]; });
+    __syncthreads();
+    if (tid == 0) ctl[7] = 0.0;  // the operator factor's pivot flag
+    stage_rhs(known1_cell, known1_node);
+    bits_out(bits);
+    return;
+  }
+  if (phase == PH_STAGE1) {
+    unsigned bits = bits_in() | (ctl[7] != 0.0 ? (unsigned)CB_WORLD_OPERATOR : 0u);
+    bits |= stage_post(known1_cell);
     drift(D1);
     for (int i = tid; i < N; i += BLOCK)
-      for (int s = 0; s < 3; ++s)
-        N1[s * N + i] = n0[s * WN + c0 + i] + k.gamma_dt * K0[S.rk_n + s * N + i];
+      for (int s = 0; s < 3; ++s) N1[s * N + i] = known1_cell(s, i);
     for (int m = tid; m < O; m += BLOCK) {
       const bool held = T.upos[m] < 0;
-      for (int s = 0; s < 3; ++s) {
-        const double known = x0[s * WO + o0 + m] + k.gamma_dt * K0[S.rk_x + s * O + m];
-        O1[s * O + m] = known + k.gamma_dt * (held ? 0.0 : drift_inflow(D1, s, m));
-      }
+      for (int s = 0; s < 3; ++s)
+        O1[s * O + m] = known1_node(s, m) + k.gamma_dt * (held ? 0.0 : drift_inflow(D1, s, m));
     }
     for (int e = tid; e < E; e += BLOCK) G1[e] = g0[e] + k.gamma_dt * K0[S.rk_g + e];
     __syncthreads();
@@ -836,18 +959,14 @@ __global__ void __launch_bounds__(BLOCK, 1)
                      [&](int s, int m) { return O1[s * O + m]; });
     __syncthreads();
     bits |= explicit_rates(K1, [&](int e) { return G1[e]; });
-    // Stage 2: known = y + (delta dt) k0 + ((1 - delta) dt) k1 + ((1 - gamma) dt) d1.
-    auto known2_cell = [&](int s, int i) {
-      return (n0[s * WN + c0 + i] + k.delta_dt * K0[S.rk_n + s * N + i]) +
-             k.omdelta_dt * K1[S.rk_n + s * N + i];
-    };
-    auto known2_node = [&](int s, int m) {
-      const bool held = T.upos[m] < 0;
-      return ((x0[s * WO + o0 + m] + k.delta_dt * K0[S.rk_x + s * O + m]) +
-              k.omdelta_dt * K1[S.rk_x + s * O + m]) +
-             omgamma_dt * (held ? 0.0 : drift_inflow(D1, s, m));
-    };
-    bits |= stage_solve(known2_cell, known2_node);
+    stage_rhs(known2_cell, known2_node);
+    bits_out(bits);
+    return;
+  }
+  // PH_FINISH: the stage-2 solution, its drift, the step's end.
+  {
+    unsigned bits = bits_in();
+    bits |= stage_post(known2_cell);
     drift(D2);
     // ---- the step's end: ledgers, heat, domain; write or refuse ---------------------------
     unsigned dom = 0;
@@ -891,8 +1010,8 @@ __global__ void __launch_bounds__(BLOCK, 1)
     if (block_or<BLOCK>(dom, sBits)) bits |= CB_WORLD_DOMAIN;
     bits = block_or<BLOCK>(bits, sBits);
     if (bits) {
-      refused = bits;
-      break;
+      if (tid == 0) status[w] = bits;
+      return;
     }
     // Accepted: write the step in place, field by field (each from its own start value).
     for (int i = tid; i < N; i += BLOCK) {
@@ -965,11 +1084,10 @@ __global__ void __launch_bounds__(BLOCK, 1)
       }
     }
     __syncthreads();
-    ++taken;
-  }
-  if (tid == 0) {
-    status[w] = refused;
-    if (taken_out) taken_out[w] = taken;
+    if (tid == 0) {
+      ctl[6] = ctl[6] + 1.0;
+      if (taken_out) taken_out[w] = (int32_t)ctl[6];
+    }
   }
 }
 
@@ -983,6 +1101,11 @@ struct cb_field {
   int W = 0, N = 0, O = 0, E = 0, F = 0, U = 0, levels = 0;
   long long lsize = 0, usize = 0, vsize = 0, smem_doubles = 0;
   int supernodes = 0;
+  // Levels of the fronts (host copies): first entry in lv_sn, one warp per front, the largest
+  // block (m x s) and front rows.
+  std::vector<int> lv_ptr, lv_warp, lv_block, lv_m;
+  int *any = nullptr;       // device: some world's Newton goes on
+  int *any_host = nullptr;  // pinned copy
   Topo topo{};
   Params params{};
   FLayout layout{};
@@ -1249,11 +1372,11 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
       af_ptr[q + 1] = (int)af_face.size();
     }
   }
-  // A level's fronts go one per warp when each fits a warp's slice of shared memory, else to
-  // the most groups (a power of two, at most the level's fronts) whose regions hold its block and
-  // vector.
-  const long long smem_doubles = kMaxSmemBytes / (long long)sizeof(double) - 64;
-  std::vector<int> lv_group(sp.levels, 0), lv_block(sp.levels, 0);
+  // A level's fronts go one per warp (their blocks and rows small) or one per CTA.
+  f->lv_ptr = sp.lv_ptr;
+  f->lv_warp.assign(sp.levels, 0);
+  f->lv_block.assign(sp.levels, 0);
+  f->lv_m.assign(sp.levels, 0);
   for (int l = 0; l < sp.levels; ++l) {
     long long mb = 0;
     int mm = 0;
@@ -1262,23 +1385,19 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
       mb = std::max(mb, (long long)sp.m[q] * sp.s[q]);
       mm = std::max(mm, sp.m[q]);
     }
-    lv_block[l] = (int)mb;
-    if (mb <= kWarpBlock && mm <= kWarpSlice - kWarpBlock) continue;
-    const int fronts = sp.lv_ptr[l + 1] - sp.lv_ptr[l];
-    int G = 1;
-    while (G * 2 <= fronts && G * 2 <= kFieldBlock / 64 && (G * 2) * (mb + mm) <= smem_doubles)
-      G *= 2;
-    if (G * (mb + mm) > smem_doubles)
-      return bail(fail(CB_ERR_UNSUPPORTED, "field: a front exceeds shared memory"));
-    lv_group[l] = G;
+    f->lv_block[l] = (int)mb;
+    f->lv_m[l] = mm;
+    f->lv_warp[l] = (mb <= kWarpBlock && mm <= kWarpVector) ? 1 : 0;
+    const long long need = f->lv_warp[l] ? (long long)kWarpsPerCta * (mb + mm) : mb + mm;
+    f->smem_doubles = std::max(f->smem_doubles, need);
   }
-  f->smem_doubles = smem_doubles;
+  if (f->smem_doubles * (long long)sizeof(double) > kMaxSmemBytes)
+    return bail(fail(CB_ERR_UNSUPPORTED, "field: a front exceeds shared memory"));
   f->levels = sp.levels;
   f->supernodes = sp.count;
   f->lsize = sp.lsize, f->usize = sp.usize, f->vsize = sp.vsize;
   Topo &T = f->topo;
   T.N = N, T.O = O, T.E = E, T.F = F, T.U = U, T.levels = sp.levels;
-  T.smem_doubles = f->smem_doubles;
   std::vector<int> sn_c0 = sp.c0, sn_s = sp.s, sn_m = sp.m;
   if ((rc = upload(f, cell_node, &T.cell_node)) || (rc = upload(f, ncell, &T.ncell)) ||
       (rc = upload(f, upos, &T.upos)) || (rc = upload(f, nf_ptr, &T.nf_ptr)) ||
@@ -1293,7 +1412,7 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
       (rc = upload(f, sp.ch_ptr, &T.ch_ptr)) || (rc = upload(f, sp.ch, &T.ch)) ||
       (rc = upload(f, sp.map_ptr, &T.map_ptr)) || (rc = upload(f, sp.map, &T.map)) ||
       (rc = upload(f, sp.lv_ptr, &T.lv_ptr)) || (rc = upload(f, sp.lv_sn, &T.lv_sn)) ||
-      (rc = upload(f, lv_group, &T.lv_group)) || (rc = upload(f, lv_block, &T.lv_block)) || (rc = upload(f, af_ptr, &T.af_ptr)) ||
+      (rc = upload(f, af_ptr, &T.af_ptr)) ||
       (rc = upload(f, af_face, &T.af_face)) || (rc = upload(f, af_pos, &T.af_pos)))
     return bail(rc);
   // Per-world parameters.
@@ -1385,6 +1504,7 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
   S.rk_ex = S.rk_s + 3LL * O;
   S.rk_size = S.rk_ex + 3LL * N;
   S.lval = take(f->lsize), S.uf = take(f->usize), S.wv = take(std::max(f->vsize, 1LL));
+  S.ctl = take(8);
   S.x = take(U), S.xt = take(U), S.dx = take(U), S.r = take(U), S.rt = take(U), S.y = take(U);
   S.phi = take(O), S.pc = take(N);
   S.co = take(3LL * O), S.lco = take(3LL * O), S.ci = take(3LL * N), S.lci = take(3LL * N);
@@ -1405,6 +1525,28 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
     f->owned.push_back(p);
     f->scratch_buf = static_cast<double *>(p);
   }
+  {
+    void *p = nullptr;
+    if ((ce = cudaMalloc(&p, sizeof(int))) != cudaSuccess) {
+      cuda_fail(ce, "cudaMalloc");
+      return bail(CB_ERR_CUDA);
+    }
+    f->owned.push_back(p);
+    f->any = static_cast<int *>(p);
+    if ((ce = cudaMallocHost(&p, sizeof(int))) != cudaSuccess) {
+      cuda_fail(ce, "cudaMallocHost");
+      return bail(CB_ERR_CUDA);
+    }
+    f->any_host = static_cast<int *>(p);
+  }
+  for (const void *fn : {(const void *)factor_warps, (const void *)factor_group,
+                         (const void *)forward_warps, (const void *)forward_group,
+                         (const void *)backward_warps, (const void *)backward_group})
+    if ((ce = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kMaxSmemBytes)) != cudaSuccess) {
+      cuda_fail(ce, "cudaFuncSetAttribute");
+      return bail(CB_ERR_CUDA);
+    }
   *out = f;
   return CB_OK;
 }
@@ -1413,6 +1555,7 @@ extern "C" void cb_field_free(cb_field *f) {
   if (!f) return;
   cudaSetDevice(f->device);
   for (void *p : f->owned) cudaFree(p);
+  if (f->any_host) cudaFreeHost(f->any_host);
   delete f;
 }
 
@@ -1457,17 +1600,109 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
                          cudaMemcpyDeviceToDevice, s);
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpyAsync");
   }
-  const size_t smem = (size_t)f->smem_doubles * sizeof(double);
-  ce = cudaFuncSetAttribute(field_kernel<kFieldBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)smem);
-  if (ce != cudaSuccess) return cuda_fail(ce, "cudaFuncSetAttribute");
-  field_kernel<kFieldBlock><<<f->W, kFieldBlock, smem, s>>>(
-      f->topo, f->params, f->layout, f->scratch, state_out, control, step_coef(dt), n_steps,
-      world_status,
-      accepted_steps, f->scratch_buf);
-  ce = cudaGetLastError();
-  if (ce != cudaSuccess) return cuda_fail(ce, "field launch");
-  return CB_OK;
+  if ((ce = cudaMemsetAsync(world_status, 0, f->W * sizeof(uint32_t), s)) != cudaSuccess ||
+      (accepted_steps &&
+       (ce = cudaMemsetAsync(accepted_steps, 0, f->W * sizeof(int32_t), s)) != cudaSuccess))
+    return cuda_fail(ce, "cudaMemsetAsync");
+  const StepCoef k = step_coef(dt);
+  const Topo &T = f->topo;
+  const Scratch &S = f->scratch;
+  double *sc = f->scratch_buf;
+  auto phase = [&](int ph, int first) {
+    field_phase<kFieldBlock><<<f->W, kFieldBlock, 0, s>>>(T, f->params, f->layout, S, state_out,
+                                                         control, k, ph, first, world_status,
+                                                         accepted_steps, sc, f->any);
+    return cudaGetLastError();
+  };
+  auto level_launch = [&](int l, auto warps, auto group) {
+    const int a0 = f->lv_ptr[l], fronts = f->lv_ptr[l + 1] - a0;
+    const int vec = f->lv_block[l];
+    if (f->lv_warp[l]) {
+      const int slice = f->lv_block[l] + f->lv_m[l];
+      const long long tasks = (long long)fronts * f->W;
+      const int ctas = (int)((tasks + kWarpsPerCta - 1) / kWarpsPerCta);
+      warps(ctas, (size_t)kWarpsPerCta * slice * sizeof(double), a0, fronts, slice, vec);
+    } else {
+      group(dim3(fronts, f->W), (size_t)(f->lv_block[l] + f->lv_m[l]) * sizeof(double), a0, vec);
+    }
+    return cudaGetLastError();
+  };
+  auto factor = [&](int kind) {
+    for (int l = 0; l < f->levels; ++l) {
+      ce = level_launch(
+          l,
+          [&](int ctas, size_t smem, int a0, int fronts, int slice, int vec) {
+            factor_warps<<<ctas, kWarpsPerCta * 32, smem, s>>>(T, f->params, S, sc, world_status,
+                                                               kind, k.gamma_dt, a0, fronts, f->W,
+                                                               slice, vec);
+          },
+          [&](dim3 grid, size_t smem, int a0, int vec) {
+            factor_group<<<grid, kGroupThreads, smem, s>>>(T, f->params, S, sc, world_status, kind,
+                                                            k.gamma_dt, a0, vec);
+          });
+      if (ce != cudaSuccess) return ce;
+    }
+    return cudaSuccess;
+  };
+  auto solve = [&](long long out_off) {
+    for (int l = 0; l < f->levels; ++l) {
+      ce = level_launch(
+          l,
+          [&](int ctas, size_t smem, int a0, int fronts, int slice, int vec) {
+            forward_warps<<<ctas, kWarpsPerCta * 32, smem, s>>>(T, S, sc, world_status, a0,
+                                                                fronts, f->W, slice, vec);
+          },
+          [&](dim3 grid, size_t smem, int a0, int vec) {
+            forward_group<<<grid, kGroupThreads, smem, s>>>(T, S, sc, world_status, a0, vec);
+          });
+      if (ce != cudaSuccess) return ce;
+    }
+    for (int l = f->levels - 1; l >= 0; --l) {
+      ce = level_launch(
+          l,
+          [&](int ctas, size_t smem, int a0, int fronts, int slice, int vec) {
+            backward_warps<<<ctas, kWarpsPerCta * 32, smem, s>>>(T, S, sc, world_status, out_off,
+                                                                 a0, fronts, f->W, slice, vec);
+          },
+          [&](dim3 grid, size_t smem, int a0, int vec) {
+            backward_group<<<grid, kGroupThreads, smem, s>>>(T, S, sc, world_status, out_off, a0,
+                                                             vec);
+          });
+      if (ce != cudaSuccess) return ce;
+    }
+    return cudaSuccess;
+  };
+  auto check = [&](cudaError_t e, const char *what) {
+    return e == cudaSuccess ? CB_OK : cuda_fail(e, what);
+  };
+  int rc = CB_OK;
+  for (int step = 0; step < n_steps && rc == CB_OK; ++step) {
+    if ((rc = check(phase(PH_START, step == 0), "field start")) ||
+        (rc = check(factor(0), "field factor")) || (rc = check(solve(S.x), "field solve")) ||
+        (rc = check(cudaMemsetAsync(f->any, 0, sizeof(int), s), "cudaMemsetAsync")) ||
+        (rc = check(phase(PH_NEWTON_INIT, 0), "field newton")))
+      break;
+    // The Newton's corrections while some world's goes on (one flag read back per correction).
+    for (int it = 0; it < kMaxIterations && rc == CB_OK; ++it) {
+      if ((rc = check(cudaMemcpyAsync(f->any_host, f->any, sizeof(int), cudaMemcpyDeviceToHost,
+                                      s), "cudaMemcpyAsync")) ||
+          (rc = check(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+        break;
+      if (*f->any_host == 0) break;
+      if ((rc = check(solve(S.dx), "field solve")) ||
+          (rc = check(cudaMemsetAsync(f->any, 0, sizeof(int), s), "cudaMemsetAsync")) ||
+          (rc = check(phase(PH_NEWTON_SEARCH, 0), "field newton")))
+        break;
+    }
+    if (rc) break;
+    if ((rc = check(phase(PH_AFTER_NEWTON, 0), "field stage 0")) ||
+        (rc = check(factor(1), "field factor")) || (rc = check(solve(S.x), "field solve")) ||
+        (rc = check(phase(PH_STAGE1, 0), "field stage 1")) ||
+        (rc = check(solve(S.x), "field solve")) ||
+        (rc = check(phase(PH_FINISH, 0), "field finish")))
+      break;
+  }
+  return rc;
 }
 
 extern "C" int cb_field_step_host(cb_field *f, const double *state_in, double *state_out,
