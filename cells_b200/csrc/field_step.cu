@@ -81,7 +81,7 @@ struct Topo {  // shared by every world
   // whether a level's fronts are small enough for one warp each; each front's face entries.
   const int *sn_c0, *sn_s, *sn_m;
   const long long *sn_loff, *sn_uoff, *sn_voff;
-  const int *rows_ptr, *rows, *ch_ptr, *ch, *map_ptr, *map, *lv_ptr, *lv_sn;
+  const int *rows_ptr, *rows, *ch_ptr, *ch, *map_ptr, *map, *split, *lv_ptr, *lv_sn;
   const int *af_ptr, *af_face, *af_pos;
 };
 struct Params {  // per world, world-major
@@ -177,12 +177,33 @@ __device__ __forceinline__ Conductance conductance(const Params &P, const Scratc
   return Conductance{base + S.wp, F, gamma_dt, kChargePerFmol * kF / (kR * wc[FW_T])};
 }
 
+// Visit entries [a0, a1) of the lower triangle (i >= j) of an n x n matrix packed by columns
+// (column j's entries at j n - j (j - 1) / 2 + (i - j)): fn(i, j, packed index), strided by group.
+template <class Fn>
+__device__ __forceinline__ void packed_lower(int n, long long a0, long long a1, int gid,
+                                             int gsize, Fn fn) {
+  int j = 0;
+  long long start = 0;
+  for (long long a = a0 + gid; a < a1; a += gsize) {
+    while (a >= start + (n - j)) {
+      start += n - j;
+      ++j;
+    }
+    fn(j + (int)(a - start), j, a);
+  }
+}
+__device__ __forceinline__ long long packed_start(int n, int j) {
+  return (long long)j * n - (long long)j * (j - 1) / 2;
+}
+
 // One front q of one world by a group of gsize threads (gid in [0, gsize)) with shared region A
-// (its m x s block) and piv (s doubles): assemble the face Laplacian's entries of its columns,
-// add its children's update matrices (ascending), factor its m x s panel right-looking with one
-// barrier per column (the trailing update uses the unscaled pivot column over the pivot; the
-// column is scaled after the barrier, the pivots kept apart), subtract the panel's product from
-// its update matrix, store the panel. Returns nonzero (at gid 0) on a pivot that is not positive.
+// (its m x s block) and piv (s doubles): assemble the face Laplacian's entries of its columns and
+// the entries of its children's update matrices that fall in its columns (children ascending);
+// factor its m x s panel right-looking with one barrier per column (the trailing update uses the
+// unscaled pivot column over the pivot; the column is scaled after the barrier, the pivots kept
+// apart); write its update matrix as minus the panel's product, then add the children's entries
+// that fall in it (children ascending); store the panel. Update matrices are packed lower
+// triangles. Returns nonzero (at gid 0) on a pivot that is not positive.
 template <class Sync>
 __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
                                  const Conductance &g, double *A, double *piv, int gid,
@@ -191,7 +212,6 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
   double *Uq = UF + T.sn_uoff[q];
   unsigned bad = 0;
   for (int a = gid; a < m * sc; a += gsize) A[a] = 0.0;
-  for (int a = gid; a < b * b; a += gsize) Uq[a] = 0.0;
   sync();
   for (int k = gid; k < sc; k += gsize) {
     const int node = T.col_node[c0 + k];
@@ -206,13 +226,9 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
     const int bc = T.sn_m[c] - T.sn_s[c];
     const double *Uc = UF + T.sn_uoff[c];
     const int *mp = T.map + T.map_ptr[c];
-    for (int a = gid; a < bc * bc; a += gsize) {
-      const int i = a % bc, j = a / bc;
-      if (i < j) continue;
-      const int pr = mp[i], pc = mp[j];
-      if (pc < sc) A[pr + pc * m] += Uc[a];
-      else Uq[(pr - sc) + (pc - sc) * b] += Uc[a];
-    }
+    packed_lower(bc, 0, packed_start(bc, T.split[c]), gid, gsize, [&](int i, int j, long long a) {
+      A[mp[i] + mp[j] * m] += Uc[a];
+    });
     sync();
   }
   for (int k = 0; k < sc; ++k) {
@@ -234,12 +250,23 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
   sync();
   for (int k = gid; k < sc; k += gsize) A[k + k * m] = piv[k];
   sync();
-  for (int a = gid; a < b * b; a += gsize) {
-    const int i = a % b, j = a / b;
-    if (i < j) continue;
-    double acc = Uq[a];
+  packed_lower(b, 0, packed_start(b, b), gid, gsize, [&](int i, int j, long long a) {
+    double acc = 0.0;
     for (int k = 0; k < sc; ++k) acc -= A[sc + i + k * m] * A[sc + j + k * m];
     Uq[a] = acc;
+  });
+  sync();
+  for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
+    const int c = T.ch[t];
+    const int bc = T.sn_m[c] - T.sn_s[c];
+    const double *Uc = UF + T.sn_uoff[c];
+    const int *mp = T.map + T.map_ptr[c];
+    packed_lower(bc, packed_start(bc, T.split[c]), packed_start(bc, bc), gid, gsize,
+                 [&](int i, int j, long long a) {
+                   const int pr = mp[i] - sc, pc = mp[j] - sc;
+                   Uq[packed_start(b, pc) + (pr - pc)] += Uc[a];
+                 });
+    sync();
   }
   double *Lq = LF + T.sn_loff[q];
   for (int a = gid; a < m * sc; a += gsize) Lq[a] = A[a];
@@ -1411,6 +1438,7 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
       (rc = upload(f, sp.rows_ptr, &T.rows_ptr)) || (rc = upload(f, sp.rows, &T.rows)) ||
       (rc = upload(f, sp.ch_ptr, &T.ch_ptr)) || (rc = upload(f, sp.ch, &T.ch)) ||
       (rc = upload(f, sp.map_ptr, &T.map_ptr)) || (rc = upload(f, sp.map, &T.map)) ||
+      (rc = upload(f, sp.split, &T.split)) ||
       (rc = upload(f, sp.lv_ptr, &T.lv_ptr)) || (rc = upload(f, sp.lv_sn, &T.lv_sn)) ||
       (rc = upload(f, af_ptr, &T.af_ptr)) ||
       (rc = upload(f, af_face, &T.af_face)) || (rc = upload(f, af_pos, &T.af_pos)))

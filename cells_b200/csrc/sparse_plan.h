@@ -150,10 +150,13 @@ inline int plan_world(int n, const int *snd, const int *rcv, int ne, WorldPlan &
 struct SuperPlan {
   int count = 0, levels = 0;
   std::vector<int> c0, s, m;                // first column, columns, front rows
-  std::vector<long long> loff, uoff, voff;  // factor block (m x s), update matrix (b x b), vector
+  std::vector<long long> loff, uoff, voff;  // factor block (m x s), update matrix (packed
+                                            // lower b x b), vector
   std::vector<int> rows_ptr, rows;          // each front's rows (factor columns, ascending)
   std::vector<int> ch_ptr, ch;              // each supernode's children, ascending
   std::vector<int> map_ptr, map;            // a child's boundary rows' positions in its parent
+  std::vector<int> split;                   // a child's boundary rows that fall in its parent's
+                                            // columns (the first `split`, as its map ascends)
   std::vector<int> parent;                  // -1 at a root
   std::vector<int> lv_ptr, lv_sn;           // supernodes level by level
   std::vector<int> sn_of;                   // column -> supernode
@@ -241,6 +244,11 @@ inline int build_supernodes(const WorldPlan &p, SuperPlan &sp,
     }
     sp.map_ptr[q + 1] = (int)sp.map.size();
   }
+  sp.split.assign(S, 0);
+  for (int q = 0; q < S; ++q)
+    if (sp.parent[q] >= 0)
+      for (int t = sp.map_ptr[q]; t < sp.map_ptr[q + 1]; ++t)
+        if (sp.map[t] < sp.s[sp.parent[q]]) sp.split[q]++;
   // Levels (children precede parents: supernodes are numbered in column order).
   std::vector<int> level(S, 0);
   for (int q = 0; q < S; ++q)
@@ -260,7 +268,7 @@ inline int build_supernodes(const WorldPlan &p, SuperPlan &sp,
     sp.loff[q] = sp.lsize;
     sp.lsize += mm * ss;
     sp.uoff[q] = sp.usize;
-    sp.usize += b * b;
+    sp.usize += b * (b + 1) / 2;  // the update matrix's lower triangle, packed by columns
     sp.voff[q] = sp.vsize;
     sp.vsize += b;
     sp.max_block = std::max(sp.max_block, mm * ss);
