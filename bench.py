@@ -592,10 +592,12 @@ def run_field(args, rank, world_size, local_rank, dist, base):
     clocks = Clocks(local_rank)
     clocks.start()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
     start.record(stream)
     for _ in range(args.steps):
         tissue.step(state, state, control, args.dt, 1, status, taken,
                     stream=stream.cuda_stream)
+        launches += tissue.launches()
     stop.record(stream)
     torch.cuda.synchronize(dev)
     clock = clocks.stop()
@@ -646,7 +648,9 @@ def run_field(args, rank, world_size, local_rank, dist, base):
                        f"scratch {info['scratch_bytes'] / 1e9:.1f} GB per GPU"),
             },
             "roofline": {
-                "bound": "hbm", "kernel": "field_kernel", "achieved": achieved, "peak": peak,
+                "bound": "hbm",
+                "kernel": "field step (field_phase, factor_*, forward_*, backward_* launches)",
+                "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms,
                 "bytes_per_world_step": alg / tissue.W,
@@ -655,7 +659,7 @@ def run_field(args, rank, world_size, local_rank, dist, base):
                     "h2d_bytes_per_step": 8 * (tissue.state_total + tissue.control_total),
                     "d2h_bytes_per_step": 8 * tissue.state_total + 8 * tissue.W,
                     "calls": args.e2e_calls},
-            "gpu_launches": args.steps,
+            "gpu_launches": launches,
             "refused_worlds": n_refused,
             "clocks": clock,
         }

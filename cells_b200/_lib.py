@@ -78,6 +78,7 @@ EXPORTS = (
     "cb_field_state_layout",
     "cb_field_control_length",
     "cb_field_info",
+    "cb_field_launches",
     "cb_field_step",
     "cb_field_step_host",
     "cb_last_error",
@@ -220,6 +221,8 @@ def load(path=LIBRARY):
     lib.cb_field_free.restype = None
     lib.cb_field_state_layout.argtypes = [_p, _i64, _i64]
     lib.cb_field_state_layout.restype = ctypes.c_int
+    lib.cb_field_launches.argtypes = [_p]
+    lib.cb_field_launches.restype = ctypes.c_int64
     lib.cb_field_info.argtypes = [_p, _i64]
     lib.cb_field_info.restype = ctypes.c_int
     lib.cb_field_control_length.argtypes = [_p]

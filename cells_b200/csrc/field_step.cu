@@ -1131,6 +1131,7 @@ struct cb_field {
   // Levels of the fronts (host copies): first entry in lv_sn, one warp per front, the largest
   // block (m x s) and front rows.
   std::vector<int> lv_ptr, lv_warp, lv_block, lv_m;
+  long long launches = 0;   // kernels launched by the last cb_field_step
   int *any = nullptr;       // device: some world's Newton goes on
   int *any_host = nullptr;  // pinned copy
   Topo topo{};
@@ -1608,6 +1609,8 @@ extern "C" int cb_field_info(const cb_field *f, int64_t info[8]) {
   return CB_OK;
 }
 
+extern "C" int64_t cb_field_launches(const cb_field *f) { return f ? f->launches : -1; }
+
 extern "C" int64_t cb_field_control_length(const cb_field *f) {
   if (!f) return -1;
   return (long long)f->W * (2LL * f->N + f->E);
@@ -1636,7 +1639,9 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
   const Topo &T = f->topo;
   const Scratch &S = f->scratch;
   double *sc = f->scratch_buf;
+  f->launches = 0;
   auto phase = [&](int ph, int first) {
+    ++f->launches;
     field_phase<kFieldBlock><<<f->W, kFieldBlock, 0, s>>>(T, f->params, f->layout, S, state_out,
                                                          control, k, ph, first, world_status,
                                                          accepted_steps, sc, f->any);
@@ -1645,6 +1650,7 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
   auto level_launch = [&](int l, auto warps, auto group) {
     const int a0 = f->lv_ptr[l], fronts = f->lv_ptr[l + 1] - a0;
     const int vec = f->lv_block[l];
+    ++f->launches;
     if (f->lv_warp[l]) {
       const int slice = f->lv_block[l] + f->lv_m[l];
       const long long tasks = (long long)fronts * f->W;

@@ -120,6 +120,10 @@ class FieldTissue:
                 "vector_doubles", "smem_bytes", "scratch_bytes")
         return dict(zip(keys, (int(v) for v in out), strict=True))
 
+    def launches(self):
+        """Kernels launched by the last step call (cb_field_launches)."""
+        return int(self.lib.cb_field_launches(self.handle))
+
     def __del__(self):
         handle = getattr(self, "handle", None)
         if handle is not None and handle.value:

@@ -356,10 +356,15 @@ int cb_field_info(const cb_field *f, int64_t info[8]);
 /* Control: membrane [W*N], junction [W*E], pump [W*N] availabilities, back to back. */
 int64_t cb_field_control_length(const cb_field *f);
 /* n_steps ARS(2,2,2) steps of every world (checked_step repeated; a refused world keeps its
- * last accepted state and stops). DEVICE pointers; state_in and state_out may alias. */
+ * last accepted state and stops). DEVICE pointers; state_in and state_out may alias. Each step is
+ * a sequence of launches on `stream` (per-world phases around the factor and substitution levels);
+ * the Newton's corrections continue while some world's does, which the call reads back, so it
+ * synchronizes `stream` once per correction. */
 int cb_field_step(cb_field *f, const double *state_in, double *state_out, double dt,
                   const double *control, int n_steps, uint32_t *world_status,
                   int32_t *accepted_steps, void *stream);
+/* Kernels launched by the handle's last cb_field_step call. */
+int64_t cb_field_launches(const cb_field *f);
 /* cb_field_step with HOST buffers: copies in, steps, copies out, synchronizes. */
 int cb_field_step_host(cb_field *f, const double *state_in, double *state_out, double dt,
                        const double *control, int n_steps, uint32_t *world_status,
