@@ -231,6 +231,8 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
     });
     sync();
   }
+  // Warps of the group over columns, lanes over rows.
+  const int nw = gsize >> 5, wid = gid >> 5, ln = gid & 31;
   for (int k = 0; k < sc; ++k) {
     const double d = A[k + k * m];
     if (gid == 0) {
@@ -238,11 +240,9 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
       piv[k] = sqrt(d);
     }
     const double inv_d = 1.0 / d, inv_p = 1.0 / sqrt(d);
-    const int rows_left = m - k - 1, cols_left = sc - k - 1;
-    for (int a = gid; a < rows_left * (cols_left + 1); a += gsize) {
-      const int i = k + 1 + a % rows_left, j = k + a / rows_left;
-      if (j == k) continue;
-      if (i >= j) A[i + j * m] -= A[i + k * m] * (A[j + k * m] * inv_d);
+    for (int j = k + 1 + wid; j < sc; j += nw) {
+      const double ljk = A[j + k * m] * inv_d;
+      for (int i = j + ln; i < m; i += 32) A[i + j * m] -= A[i + k * m] * ljk;
     }
     sync();
     for (int i = k + 1 + gid; i < m; i += gsize) A[i + k * m] *= inv_p;
@@ -250,11 +250,14 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
   sync();
   for (int k = gid; k < sc; k += gsize) A[k + k * m] = piv[k];
   sync();
-  packed_lower(b, 0, packed_start(b, b), gid, gsize, [&](int i, int j, long long a) {
-    double acc = 0.0;
-    for (int k = 0; k < sc; ++k) acc -= A[sc + i + k * m] * A[sc + j + k * m];
-    Uq[a] = acc;
-  });
+  for (int j = wid; j < b; j += nw) {
+    double *Uj = Uq + packed_start(b, j) - j;
+    for (int i = j + ln; i < b; i += 32) {
+      double acc = 0.0;
+      for (int k = 0; k < sc; ++k) acc -= A[sc + i + k * m] * A[sc + j + k * m];
+      Uj[i] = acc;
+    }
+  }
   sync();
   for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
     const int c = T.ch[t];
