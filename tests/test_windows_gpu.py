@@ -1,0 +1,97 @@
+"""The window runner (cells_b200/windows.py: steps with per-row device checks, the reference's
+vector window, src/cells/execution/vector_windows.py:348-410) against the same window built from
+the oracle's step and checks (oracle/tissue.py, oracle/checks.py).
+
+Three gated worlds, six rows of 1 ms under a two-entry held-control table; world 1's second
+control has an availability above 1 (its step is refused at the first row that holds it, row 3),
+world 2 takes only four rows. Failing rows and bits equal; final states and stored rows within
+1e-10 scaled difference; the energy diagnostics' maxima to 1e-8.
+"""
+
+import numpy as np
+import pytest
+
+from cells_b200 import windows, worlds
+from cells_b200.tissue import Tissue
+from conftest import scaled_difference
+from gpu_util import oracle_state
+from oracle import checks as CK
+from oracle import tissue as T
+
+pytestmark = pytest.mark.gpu
+DT = [1e-3] * 6
+HELD = [0, 0, 1, 1, 0, 1]
+SLOTS = [0, -1, 1, -1, -1, 2]
+COUNTS = [6, 6, 4]
+ATOL, RTOL = np.full(3, 2e-11), 2e-3
+
+
+def batch():
+    rng = np.random.default_rng(31)
+    ws = [worlds.grid_world(4, 4, worlds.world_rng(31, k), gate=(0.015, 0.2, 1.0)) for k in
+          range(3)]
+    b = worlds.pack(ws)
+    c0 = T.Control(rng.uniform(0.6, 1, b.cells), rng.uniform(0.6, 1, b.edges),
+                   rng.uniform(0.6, 1, b.cells))
+    m1 = c0.membrane.copy()
+    m1[b.cell_offset[1] + 3] = 1.2  # world 1 refuses every step under control 1
+    c1 = T.Control(m1, c0.junction * 0.9, c0.pump)
+    return b, [c0, c1]
+
+
+def oracle_window(b, controls):
+    topo = T.topology(b)
+    cur = T.initial_state(b)
+    failed0, vals0 = CK.row_checks(cur, cur, b, topo, 0, ATOL, RTOL)
+    pack = (failed0 << (np.arange(12) + 1)).sum(axis=1)
+    ok = pack == 0
+    first = np.where(ok, -1, 0)
+    bits = pack.copy()
+    maxima = np.where(ok[:, None], vals0, 0.0)
+    stored = {}
+    for j in range(1, len(DT) + 1):
+        new, valid = T.ars222_step(cur, DT[j - 1], controls[HELD[j - 1]], b, topo)
+        failed, vals = CK.row_checks(cur, new, b, topo, j, ATOL, RTOL)
+        flags = np.where(valid, (failed << (np.arange(12) + 1)).sum(axis=1), 1)
+        live = (j <= np.asarray(COUNTS)) & ok
+        failing = live & (flags != 0)
+        accept = live & (flags == 0)
+        first = np.where(failing, j, first)
+        bits = np.where(failing, flags, bits)
+        cur = T._select(accept, new, cur, b, topo)
+        maxima = np.where(accept[:, None], np.maximum(maxima, vals), maxima)
+        if SLOTS[j - 1] >= 0:
+            stored[SLOTS[j - 1]] = (accept.copy(), oracle_state(cur))
+        ok = ok & ~failing
+    return cur, first, bits, maxima, stored
+
+
+def test_window_matches_the_oracle_window(cuda):
+    torch = cuda
+    b, controls = batch()
+    tissue = Tissue(b)
+    dev = torch.device("cuda", tissue.device)
+    table = torch.from_numpy(np.stack([tissue.pack_control(c.membrane, c.junction, c.pump)
+                                       for c in controls])).to(dev)
+    state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    win = windows.vector_window(tissue, state, DT, table, HELD, slots=SLOTS, counts=COUNTS,
+                                material_atol=ATOL, energy_rtol=RTOL, rows=3)
+    torch.cuda.synchronize(dev)
+    cur, first, bits, maxima, stored = oracle_window(b, controls)
+    assert np.array_equal(win.first.cpu().numpy(), first)
+    assert np.array_equal(win.bits.cpu().numpy(), bits)
+    assert first.tolist() == [-1, 3, -1] and windows.failure_names(bits[1]) == ("step_refused",)
+    got = tissue.unpack_state(win.state.cpu().numpy())
+    bad = {f: d for f, ref in oracle_state(cur).items()
+           if (d := scaled_difference(got[f], ref)) > 1e-10}
+    assert not bad, bad
+    rows = win.rows.cpu().numpy()
+    for slot, (accept, ref) in stored.items():
+        got_row = tissue.unpack_state(rows[slot])
+        cells = np.repeat(accept, np.diff(b.cell_offset))
+        for f in ("amount_increment", "membrane_transferred", "pump_cycles"):
+            g, r = np.asarray(got_row[f]), np.asarray(ref[f])
+            assert scaled_difference(g[..., cells], r[..., cells]) <= 1e-10, (slot, f)
+    m = win.maxima.cpu().numpy()
+    for k in (6, 10):
+        assert np.all(np.abs(m[:, k] - maxima[:, k]) <= 1e-8 * np.abs(maxima[:, k])), k
