@@ -51,6 +51,7 @@ constexpr double kCurrentRtol = 2e-12;   // CURRENT_RTOL
 constexpr int kMaxIterations = 16;       // solve's max_iterations
 constexpr int kMaxBacktracks = 12;       // max_backtracks
 constexpr int kFieldBlock = 512;
+constexpr int kPhaseMinBlocks = 2;  // phase CTAs per SM the register budget aims for
 constexpr int kWarpBlock = 1280;  // a level's fronts go one per warp when their blocks fit this
 constexpr int kWarpVector = 256;  // ... and their fronts' rows this
 // Dynamic shared memory a level kernel may ask for: the 227 KB per CTA less room for its static
@@ -439,11 +440,12 @@ __global__ void __launch_bounds__(kGroupThreads)
                  sm + vec, threadIdx.x, kGroupThreads, [] { __syncthreads(); }, reduce);
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1)
+// One instantiation per phase, so each gets its own register allocation (MINB: CTAs per SM).
+template <int BLOCK, int phase, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
     field_phase(const Topo T, const Params P, const FLayout L, const Scratch S,
                 double *__restrict__ state, const double *__restrict__ control, const StepCoef k,
-                int phase, int first, uint32_t *__restrict__ status,
+                int first, uint32_t *__restrict__ status,
                 int32_t *__restrict__ taken_out, double *__restrict__ scratch,
                 int *__restrict__ any_active) {
   __shared__ double sRed[BLOCK / 32];
@@ -1645,9 +1647,18 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
   f->launches = 0;
   auto phase = [&](int ph, int first) {
     ++f->launches;
-    field_phase<kFieldBlock><<<f->W, kFieldBlock, 0, s>>>(T, f->params, f->layout, S, state_out,
-                                                         control, k, ph, first, world_status,
-                                                         accepted_steps, sc, f->any);
+    auto go = [&](auto kernel) {
+      kernel<<<f->W, kFieldBlock, 0, s>>>(T, f->params, f->layout, S, state_out, control, k, first,
+                                          world_status, accepted_steps, sc, f->any);
+    };
+    switch (ph) {
+      case PH_START: go(field_phase<kFieldBlock, PH_START, kPhaseMinBlocks>); break;
+      case PH_NEWTON_INIT: go(field_phase<kFieldBlock, PH_NEWTON_INIT, kPhaseMinBlocks>); break;
+      case PH_NEWTON_SEARCH: go(field_phase<kFieldBlock, PH_NEWTON_SEARCH, kPhaseMinBlocks>); break;
+      case PH_AFTER_NEWTON: go(field_phase<kFieldBlock, PH_AFTER_NEWTON, kPhaseMinBlocks>); break;
+      case PH_STAGE1: go(field_phase<kFieldBlock, PH_STAGE1, kPhaseMinBlocks>); break;
+      default: go(field_phase<kFieldBlock, PH_FINISH, kPhaseMinBlocks>); break;
+    }
     return cudaGetLastError();
   };
   auto level_launch = [&](int l, auto warps, auto group) {
