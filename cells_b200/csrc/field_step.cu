@@ -1005,9 +1005,11 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     const double gdt = k.gamma_dt, ddt = k.delta_dt, odt = k.omdelta_dt;
     const double dl = k.delta, od = k.omdelta, gm = 1.0 - 1.0 / sqrt(2.0), og = 1.0 - gm;
     // Cells.
+    // The final amounts go to N1 / O1 (no longer needed) for the write below.
     for (int i = tid; i < N; i += BLOCK) {
       for (int s = 0; s < 3; ++s) {
         const double v = known2_cell(s, i);
+        N1[s * N + i] = v;
         if (!(is_finite(v) && P.ref[s * WN + c0 + i] + v > 0.0)) dom = 1u;
       }
       for (int s = 0; s < 3; ++s) {
@@ -1037,6 +1039,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     for (int m = tid; m < O; m += BLOCK)
       for (int s = 0; s < 3; ++s) {
         const double v = known2_node(s, m) + gdt * (T.upos[m] < 0 ? 0.0 : drift_inflow(D2, s, m));
+        O1[s * O + m] = v;
         if (!(is_finite(v) && P.oref[s * WO + o0 + m] + v > 0.0)) dom = 1u;
       }
     if (block_or<BLOCK>(dom, sBits)) bits |= CB_WORLD_DOMAIN;
@@ -1048,7 +1051,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     // Accepted: write the step in place, field by field (each from its own start value).
     for (int i = tid; i < N; i += BLOCK) {
       double nv[3];
-      for (int s = 0; s < 3; ++s) nv[s] = known2_cell(s, i);
+      for (int s = 0; s < 3; ++s) nv[s] = N1[s * N + i];
       for (int s = 0; s < 3; ++s) {
         st(CB_FIELD_AMOUNT_INCREMENT)[s * WN + c0 + i] = nv[s];
         double *mt = st(CB_FIELD_MEMBRANE_TRANSFERRED) + s * WN + c0 + i;
@@ -1093,7 +1096,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       const bool held = T.upos[m] < 0;
       double nv[3], sup[3];
       for (int s = 0; s < 3; ++s) {
-        nv[s] = known2_node(s, m) + gdt * (held ? 0.0 : drift_inflow(D2, s, m));
+        nv[s] = O1[s * O + m];
         const double i1 = held ? -drift_inflow(D1, s, m) : 0.0;
         const double i2 = held ? -drift_inflow(D2, s, m) : 0.0;
         const double k0s = K0[S.rk_s + s * O + m], k1s = K1[S.rk_s + s * O + m];
