@@ -310,25 +310,29 @@ __device__ void front_forward(const Topo &T, const double *LF, double *WV, doubl
   }
 }
 
-// Back substitution of front q: x_S = L_SS^-T (y_S - L_BS^T x_B), x_B from its ancestors (out).
-template <class Sync, class Reduce>
+// Back substitution of front q: t = y_S - L_BS^T x_B (x_B from its ancestors, in out), one
+// column per thread; then L_SS^T x_S = t by a column sweep, one barrier per column.
+template <class Sync>
 __device__ void front_backward(const Topo &T, const double *LF, const double *Y, double *out,
-                               int q, double *A, double *v, int gid, int gsize, Sync sync,
-                               Reduce reduce) {
+                               int q, double *A, double *v, int gid, int gsize, Sync sync) {
   const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
   const double *Lq = LF + T.sn_loff[q];
   const int *rq = T.rows + T.rows_ptr[q];
   for (int a = gid; a < m * sc; a += gsize) A[a] = Lq[a];
   for (int i = sc + gid; i < m; i += gsize) v[i] = out[rq[i]];
   sync();
-  for (int k = sc - 1; k >= 0; --k) {
-    double part = 0.0;
-    for (int i = k + 1 + gid; i < m; i += gsize) part += A[i + k * m] * v[i];
-    part = reduce(part);
-    if (gid == 0) v[k] = (Y[c0 + k] - part) / A[k + k * m];
+  for (int k = gid; k < sc; k += gsize) {
+    double t = Y[c0 + k];
+    for (int i = sc; i < m; ++i) t -= A[i + k * m] * v[i];
+    v[k] = t;
+  }
+  sync();
+  for (int k = sc - 1; k > 0; --k) {
+    const double xk = v[k] / A[k + k * m];
+    for (int j = gid; j < k; j += gsize) v[j] -= A[k + j * m] * xk;
     sync();
   }
-  for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k];
+  for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k] / A[k + k * m];
 }
 
 // Level kernels. Warp form: each warp one (front, world) task of the level, world-major, with a
@@ -350,10 +354,6 @@ __device__ __forceinline__ LevelTask warp_task(const Topo &T, const uint32_t *st
   return {T.lv_sn[a0 + (int)(task % fronts)], w, status[w] == 0u};
 }
 
-__device__ __forceinline__ double warp_reduce(double x) {
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  return x;
-}
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
     factor_warps(const Topo T, const Params P, const Scratch S, double *scratch,
@@ -415,29 +415,18 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
   double *base = scratch + (size_t)t.w * S.stride;
   double *A = sm + (size_t)(threadIdx.x >> 5) * slice;
   front_backward(T, base + S.lval, base + S.y, base + out_off, t.q, A, A + vec, threadIdx.x & 31,
-                 32, [] { __syncwarp(); }, warp_reduce);
+                 32, [] { __syncwarp(); });
 }
 
 __global__ void __launch_bounds__(kGroupThreads)
     backward_group(const Topo T, const Scratch S, double *scratch, const uint32_t *status,
                    long long out_off, int a0, int vec) {
   extern __shared__ double sm[];
-  __shared__ double red[kGroupThreads / 32];
   const int w = blockIdx.y;
   if (status[w] != 0u) return;
   double *base = scratch + (size_t)w * S.stride;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  auto reduce = [&](double x) {
-    x = warp_reduce(x);
-    __syncthreads();
-    if (lane == 0) red[warp] = x;
-    __syncthreads();
-    double t = 0.0;
-    for (int q = 0; q < kGroupThreads / 32; ++q) t += red[q];
-    return t;
-  };
   front_backward(T, base + S.lval, base + S.y, base + out_off, T.lv_sn[a0 + blockIdx.x], sm,
-                 sm + vec, threadIdx.x, kGroupThreads, [] { __syncthreads(); }, reduce);
+                 sm + vec, threadIdx.x, kGroupThreads, [] { __syncthreads(); });
 }
 
 // One instantiation per phase, so each gets its own register allocation (MINB: CTAs per SM).
