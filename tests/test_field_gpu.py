@@ -161,3 +161,22 @@ def test_field_ledgers_hold(cuda):
         assert np.all(np.abs(total) <= 1e-12 * scale), total
         assert np.all(got["extracellular_increment"][k][:, held] == 0)
         assert np.all(got["reservoir_supplied"][k][:, ~held] == 0)
+
+
+def test_field_single_cell_without_junctions(cuda):
+    """A one-cell tissue (no junctions: the C ABI's junction arrays empty) in a 7x7 grid, against
+    the oracle over 20 steps."""
+    w = FW.field_world(7, 1, 2, worlds.world_rng(25, 0))
+    assert w.edges == 0 and w.cells == 1
+    tissue = FieldTissue([w])
+    got, status, taken = run(cuda, tissue, tissue.initial_state(), tissue.pack_control(), 5e-4,
+                             [20])
+    assert status[0] == 0 and taken[0] == 20
+    with threadpoolctl.threadpool_limits(limits=1, user_api="blas"):
+        tp, st = OF.bind(w), OF.initial_state(w)
+        for _ in range(20):
+            st, ok = OF.imex_step(st, 5e-4, OF.full_control(w), w, tp)
+            assert ok
+    bad = {f: d for f in OF.FieldState._fields
+           if (d := field_difference(got[f][0], getattr(st, f), st.face_transferred, w, f)) > TOL}
+    assert not bad, bad
