@@ -614,16 +614,23 @@ def run_field(args, rank, world_size, local_rank, dist, base):
     alg = field_bytes_per_world_step(tissue, info) * tissue.W
     achieved = alg / (launch_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
-    # End to end through the C ABI with host buffers (cb_field_step_host: the state and control
-    # copied in, one step, the state and status copied out, every call).
-    host_state = tissue.unpack_state(state0)
+    # End to end through the C ABI with host buffers (cb_field_step_host on packed, pinned host
+    # buffers: the state and control copied in, one step, the state and status copied out, every
+    # call).
+    pinned_in = torch.from_numpy(state0).pin_memory().numpy()
+    pinned_out = torch.empty(state0.size, dtype=torch.float64).pin_memory().numpy()
+    pinned_ctl = torch.from_numpy(control_np).pin_memory().numpy()
+    host_status = np.zeros(tissue.W, dtype=np.uint32)
+    host_taken = np.zeros(tissue.W, dtype=np.int32)
     e2e_value = None
     if args.e2e_calls > 0:
-        tissue.step_host(host_state, control_np, args.dt, 1)
+        tissue.step_host_packed(pinned_in, pinned_out, pinned_ctl, args.dt, 1, host_status,
+                                host_taken)
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_calls):
-            tissue.step_host(host_state, control_np, args.dt, 1)
+            tissue.step_host_packed(pinned_in, pinned_out, pinned_ctl, args.dt, 1, host_status,
+                                    host_taken)
         e2e_s = time.perf_counter() - t0
         if dist is not None:
             t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)

@@ -1129,6 +1129,9 @@ struct cb_field {
   // block (m x s) and front rows.
   std::vector<int> lv_ptr, lv_warp, lv_block, lv_m;
   long long launches = 0;   // kernels launched by the last cb_field_step
+  double *host_state = nullptr, *host_control = nullptr;  // cb_field_step_host's device copies
+  uint32_t *host_status = nullptr;
+  int32_t *host_taken = nullptr;
   int *any = nullptr;       // device: some world's Newton goes on
   int *any_host = nullptr;  // pinned copy
   Topo topo{};
@@ -1754,16 +1757,25 @@ extern "C" int cb_field_step_host(cb_field *f, const double *state_in, double *s
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
   const size_t sb = (size_t)f->state_total * sizeof(double);
   const size_t cb = (size_t)cb_field_control_length(f) * sizeof(double);
-  double *ds = nullptr, *dc = nullptr;
-  uint32_t *dst = nullptr;
-  int32_t *dacc = nullptr;
+  // The device buffers of host calls: allocated by the handle's first host call, kept until
+  // cb_field_free.
+  if (!f->host_state) {
+    void *p = nullptr;
+    const size_t bytes = sb + cb + f->W * (sizeof(uint32_t) + sizeof(int32_t)) + 256;
+    if ((ce = cudaMalloc(&p, bytes)) != cudaSuccess) return cuda_fail(ce, "cudaMalloc");
+    f->owned.push_back(p);
+    char *c = static_cast<char *>(p);
+    f->host_state = reinterpret_cast<double *>(c);
+    f->host_control = reinterpret_cast<double *>(c + sb);
+    f->host_status = reinterpret_cast<uint32_t *>(c + sb + cb);
+    f->host_taken = reinterpret_cast<int32_t *>(c + sb + cb + f->W * sizeof(uint32_t));
+  }
+  double *ds = f->host_state, *dc = f->host_control;
+  uint32_t *dst = f->host_status;
+  int32_t *dacc = f->host_taken;
   int rc = CB_OK;
-  if ((ce = cudaMalloc(&ds, sb)) != cudaSuccess || (ce = cudaMalloc(&dc, cb)) != cudaSuccess ||
-      (ce = cudaMalloc(&dst, f->W * sizeof(uint32_t))) != cudaSuccess ||
-      (ce = cudaMalloc(&dacc, f->W * sizeof(int32_t))) != cudaSuccess) {
-    rc = cuda_fail(ce, "cudaMalloc");
-  } else if ((ce = cudaMemcpy(ds, state_in, sb, cudaMemcpyHostToDevice)) != cudaSuccess ||
-             (ce = cudaMemcpy(dc, control, cb, cudaMemcpyHostToDevice)) != cudaSuccess) {
+  if ((ce = cudaMemcpy(ds, state_in, sb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (ce = cudaMemcpy(dc, control, cb, cudaMemcpyHostToDevice)) != cudaSuccess) {
     rc = cuda_fail(ce, "cudaMemcpy");
   } else if ((rc = cb_field_step(f, ds, ds, dt, dc, n_steps, dst, dacc, nullptr)) == CB_OK) {
     if ((ce = cudaMemcpy(state_out, ds, sb, cudaMemcpyDeviceToHost)) != cudaSuccess ||
@@ -1773,9 +1785,5 @@ extern "C" int cb_field_step_host(cb_field *f, const double *state_in, double *s
                                             cudaMemcpyDeviceToHost)) != cudaSuccess))
       rc = cuda_fail(ce, "cudaMemcpy");
   }
-  cudaFree(ds);
-  cudaFree(dc);
-  cudaFree(dst);
-  cudaFree(dacc);
   return rc;
 }

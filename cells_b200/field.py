@@ -188,6 +188,16 @@ class FieldTissue:
             None if stream is None else ctypes.c_void_p(stream),
         ))  # fmt: skip
 
+    def step_host_packed(self, state_in, state_out, control, dt, n_steps, status, taken):
+        """cb_field_step_host on packed host buffers (numpy float64 [state_total], control
+        [control_total], uint32 / int32 [W]); pinned memory copies fastest."""
+        _lib.check(self.lib.cb_field_step_host(
+            self.handle, state_in.ctypes.data_as(_lib._d), state_out.ctypes.data_as(_lib._d),
+            float(dt), control.ctypes.data_as(_lib._d), int(n_steps),
+            status.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+            taken.ctypes.data_as(_lib._i32),
+        ))  # fmt: skip
+
     def step_host(self, state, control, dt, n_steps):
         """cb_field_step_host: host arrays in and out. Returns (state dict, status, taken)."""
         src = np.ascontiguousarray(self.pack_state(state))

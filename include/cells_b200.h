@@ -365,7 +365,8 @@ int cb_field_step(cb_field *f, const double *state_in, double *state_out, double
                   int32_t *accepted_steps, void *stream);
 /* Kernels launched by the handle's last cb_field_step call. */
 int64_t cb_field_launches(const cb_field *f);
-/* cb_field_step with HOST buffers: copies in, steps, copies out, synchronizes. */
+/* cb_field_step with HOST buffers: copies in, steps, copies out, synchronizes. The device copies
+ * are allocated by the handle's first host call and kept until cb_field_free. */
 int cb_field_step_host(cb_field *f, const double *state_in, double *state_out, double dt,
                        const double *control, int n_steps, uint32_t *world_status,
                        int32_t *accepted_steps);
