@@ -547,14 +547,24 @@ def run_adjoint(args, rank, world_size, local_rank, dist, base):
 def field_bytes_per_world_step(tissue, info, solves=6):
     """Algorithmic bytes per world per step of the field step: the state read and written once,
     the parameters read once (per cell 11 doubles, per junction 5, per node 6, per face 3), each
-    of the step's two factors written once and read by each of its solves (the start field's
-    initial solve and chord corrections, the two stage solves: six on the benchmark's worlds),
-    and each factorisation's update matrices written and read once."""
+    of the step's two factors written once and read by both passes of each of its solves (the
+    start field's initial solve and chord corrections, the two stage solves: six on the
+    benchmark's worlds), and each factorisation's update matrices written and read once."""
     state = tissue.state_total // tissue.W
     params = 11 * tissue.N + 5 * tissue.E + 6 * tissue.O + 3 * tissue.F
-    factor = info["factor_doubles"] * (2 + solves)
+    factor = info["factor_doubles"] * (2 + 2 * solves)
     updates = 2 * 2 * info["update_doubles"]
     return 8 * (2 * state + params + factor + updates)
+
+
+def field_traffic_per_world_step():
+    """DRAM bytes per world·step of the field step (ncu, committed summary)."""
+    path = os.path.join(ROOT, "profiles", "field_traffic.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["dram_bytes_per_world_step"])
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def run_field(args, rank, world_size, local_rank, dist, base):
@@ -659,7 +669,10 @@ def run_field(args, rank, world_size, local_rank, dist, base):
                 "kernel": "field step (field_phase, factor_*, forward_*, backward_* launches)",
                 "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms,
+                "traffic": (None if field_traffic_per_world_step() is None
+                            else field_traffic_per_world_step() * tissue.W),
+                "traffic_note": "DRAM bytes of one step of 32 worlds (ncu), scaled per world",
+                "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms,
                 "bytes_per_world_step": alg / tissue.W,
             },
             "e2e": {"value": e2e_value, "unit": UNIT,
