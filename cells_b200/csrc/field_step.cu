@@ -57,7 +57,6 @@ constexpr int kWarpVector = 256;  // ... and their fronts' rows this
 // Dynamic shared memory a level kernel may ask for: the 227 KB per CTA less room for its static
 // shared memory.
 constexpr long long kMaxSmemBytes = 227 * 1024 - 1024;
-constexpr int kRefineRounds = 0;         // FP64 refinement rounds of each stage solve
 constexpr double kChargeAtol = 3e-25;    // surface_field.CHARGE_ATOL_C
 constexpr double kChargeRtol = 2e-12;    // CHARGE_RTOL
 
@@ -439,8 +438,9 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                 int *__restrict__ any_active) {
   __shared__ double sRed[BLOCK / 32];
   __shared__ unsigned sBits[BLOCK / 32];
-  constexpr int WARPS = BLOCK / 32;
-  const int w = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  [[maybe_unused]] constexpr int WARPS = BLOCK / 32;
+  const int w = blockIdx.x, tid = threadIdx.x;
+  [[maybe_unused]] const int lane = tid & 31, warp = tid >> 5;
   const int N = T.N, O = T.O, E = T.E, F = T.F, U = T.U;
   const long long WN = P.WN, WO = P.WO, WE = P.WE, WF = P.WF;
   const long long c0 = (long long)w * N, o0 = (long long)w * O, e0 = (long long)w * E,

@@ -12,8 +12,9 @@ transfer, the work against 1e-3 x the largest |mu| x that transfer.
 
 The device solves the same equations by other means (a chord Newton on the floating offsets with
 the face Laplacian as its matrix, each cell eliminated into its node in the stage solves,
-nested-dissection sparse Cholesky), so agreement is to rounding, not bit for bit. A fused launch equals one-step launches bit for bit; a world's result does not depend
-on its batch position; the host entry point equals the device one bit for bit.
+nested-dissection sparse Cholesky), so agreement is to rounding, not bit for bit. A fused launch
+equals one-step launches bit for bit; a world's result does not depend on its batch position; the
+host entry point equals the device one bit for bit.
 """
 
 import numpy as np
