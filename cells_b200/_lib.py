@@ -72,6 +72,7 @@ EXPORTS = (
     "cb_step_vjp",
     "cb_vjp_workspace",
     "cb_set_permeability",
+    "cb_set_channel_block",
     "cb_device_checks",
     "cb_field_bind",
     "cb_field_free",
@@ -213,6 +214,8 @@ def load(path=LIBRARY):
     lib.cb_vjp_workspace.restype = ctypes.c_int
     lib.cb_set_permeability.argtypes = [_p, _p, _p, _p, _p]
     lib.cb_set_permeability.restype = ctypes.c_int
+    lib.cb_set_channel_block.argtypes = [_p, ctypes.c_int32, _d, _d, _d, _d]
+    lib.cb_set_channel_block.restype = ctypes.c_int
     lib.cb_device_checks.argtypes = [_p, _p, _p, ctypes.c_int64, _d, ctypes.c_double, _p, _p, _p]
     lib.cb_device_checks.restype = ctypes.c_int
     lib.cb_field_bind.argtypes = [ctypes.POINTER(FieldDesc), ctypes.c_int, ctypes.POINTER(_p)]

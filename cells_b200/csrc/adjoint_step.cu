@@ -733,6 +733,8 @@ int cb_step_vjp(cb_tissue *t, const double *state_in, double dt, const double *c
   if (!t || !state_in || !control || !cot_out || !cot_in || !grad_membrane || !world_status ||
       (t->E && !grad_junction) || (t->t.nch && !grad_channel) || !workspace)
     return fail(CB_ERR_ARGUMENT, "null argument");
+  if (t->t.blk_modes > 0)
+    return fail(CB_ERR_UNSUPPORTED, "the adjoint step has no open-channel block");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
   if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
   const WorkspacePlan p = plan(t, n_steps);

@@ -74,6 +74,10 @@ struct cb_tissue {
   // world-local junction endpoints.
   std::vector<long long> h_cell_offset, h_edge_offset;
   std::vector<int> h_snd, h_rcv;
+  std::vector<double> h_temperature;  // [W] K
+  // The open-channel block's device table (cb_set_channel_block), or null.
+  double *blk_buf = nullptr;
+  size_t blk_doubles = 0;
   // The N2 method's sparse-factor plan and workspace, built at its first step.
   cbk::N2Plan *n2 = nullptr;
 };

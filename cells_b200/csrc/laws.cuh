@@ -27,6 +27,7 @@ constexpr double kAvogadro = 6.02214076e23;
 constexpr double kF = kAvogadro * 1.602176634e-19;
 constexpr double kR = kAvogadro * 1.380649e-23;
 constexpr double kChargePerFmol = kF * 1e-15;
+constexpr double kNormalMin = 2.2250738585072014e-308;  // the smallest normal binary64
 constexpr double kMaxAbsX = 50.0;
 constexpr double kMaxAbsJunctionV = 0.120;
 constexpr double kMaxAbsIonPotentialOverRT = 1600.0;
@@ -81,6 +82,10 @@ struct Tissue {
   const int *ch_species;   // [NCH][C] permeant species
   const double *ch_ap;     // [NCH][C] area * permeability / 1e-15
   const double *ch_ab;     // [NCH][C] abundance
+  // Open-channel block of the populations (0 modes: none declared).
+  int blk_modes;           // mode slots per population (1..4)
+  const double *blk;       // [3][M][NCH][C]: weight, K(0) (mM), a = steepness F/(R T) (1/V)
+  const double *blk_conc;  // [NCH][C] blocker concentration (mM)
 };
 
 struct Layout {  // offsets in doubles
@@ -226,6 +231,36 @@ __device__ __forceinline__ double channel_opening(int code, double m, double h) 
   if (code == kNav1p2) return ((m * m) * m) * h;
   if (code == kHhKn4) return (m * m) * (m * m);
   return m * h;
+}
+
+// The open-channel block of population q of cell gi at the patch voltage v
+// (laws/channels/open_channel_block.py, the reference's kernels dissociation, fractions,
+// unblocked_fraction, slope and domain_valid): K_k = K_k(0) exp(a_k v); both fractions formed
+// directly, theta_k = c_B / (c_B + K_k), 1 - theta_k = K_k / (c_B + K_k); the unblocked fraction
+// u = (sum_k w_k (1 - theta_k)) / sum_k w_k and u's slope bound
+// (sum_k w_k |a_k| theta_k (1 - theta_k)) / sum_k w_k, each sum left to right over the modes.
+// ok turns false where a K_k or c_B + K_k is not a finite normal number.
+__device__ __forceinline__ void channel_block(const Tissue &T, int q, long long gi, double v,
+                                              double &u, double &slope, bool &ok) {
+  const int M = T.blk_modes;
+  const long long NC = (long long)T.nch * T.C, at = (long long)q * T.C + gi;
+  const double cb = __ldg(T.blk_conc + at);
+  double num = 0.0, den = 0.0, snum = 0.0;
+  for (int k = 0; k < M; ++k) {
+    const double w = __ldg(T.blk + (long long)k * NC + at);
+    const double k0 = __ldg(T.blk + (long long)(M + k) * NC + at);
+    const double a = __ldg(T.blk + (long long)(2 * M + k) * NC + at);
+    const double K = k0 * exp(a * v);
+    const double total = cb + K;
+    const double theta = cb / total, free = K / total;
+    ok = ok && is_finite(K) && K >= kNormalMin && is_finite(total) && total >= kNormalMin;
+    const double wf = w * free, ws = (w * fabs(a)) * (theta * free);
+    num = k == 0 ? wf : num + wf;
+    den = k == 0 ? w : den + w;
+    snum = k == 0 ? ws : snum + ws;
+  }
+  u = num / den;
+  slope = snum / den;
 }
 
 // Exponential gate update with a linearly varying target (numerics/exponential_gates.py:36-51).

@@ -32,7 +32,7 @@ __host__ __device__ constexpr size_t packed_smem_bytes(int cap) {
          sizeof(unsigned int) * 3 * kPackedMaxWorlds;
 }
 
-template <int BLOCK, int NCH>
+template <int BLOCK, int NCH, bool BLK = false>
 __global__ void __launch_bounds__(BLOCK, 1)
     packed_kernel(const Tissue T, const Layout L, const Packed P, const double *state_in,
                   double *state_out, const double *__restrict__ control, const StepCoef k,
@@ -222,6 +222,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
               ((((__ldg(T.ap + gi) * largest[0]) + __ldg(T.ap + C + gi) * largest[1]) +
                 __ldg(T.ap + 2 * C + gi) * largest[2]) * 1e-15) * mc;
           double chm[3] = {0.0, 0.0, 0.0};
+          double blocked_tv = 0.0;  // the blocked populations' T_V (S)
           if constexpr (NCH > 0) {
             for (int q = 0; q < NCH; ++q) {
               const int code = __ldg(T.ch_code + q * C + gi);
@@ -232,10 +233,25 @@ __global__ void __launch_bounds__(BLOCK, 1)
               const double available = (open * ctl) * __ldg(T.ch_ab + q * C + gi);
               const double gq = __ldg(T.ch_ap + q * C + gi) * available;
               const double cs = c[sp], cos_ = __ldg(wc + WC_CO + sp);
-              const double J = sp < 2 ? gq * (cs * bm - cos_ * bp) : gq * (cs * bp - cos_ * bm);
+              double J = sp < 2 ? gq * (cs * bm - cos_ * bp) : gq * (cs * bp - cos_ * bm);
+              const double gterm =
+                  ((__ldg(T.ch_ap + q * C + gi) * 1e-15) * largest[sp]) * available;
+              if constexpr (BLK) {
+                // Open-channel block (surface_pump_v3.channel_rates :958-960, channel_block_terms
+                // :1051-1090): u multiplies the flux; the stability rule takes the population's
+                // T_V = u G_max + |I_free| slope in place of G_max.
+                double u, su;
+                bool bok = true;
+                channel_block(T, q, gi, dv, u, su, bok);
+                if (!bok) bits |= CB_WORLD_CHANNEL_DOMAIN;
+                const double ifree = kChargePerFmol * ((sp < 2 ? 1.0 : -1.0) * J);
+                blocked_tv += u * (__ldg(wc + WC_SLOPE) * gterm) + fabs(ifree) * su;
+                J = J * u;
+              } else {
+                membrane += gterm;
+              }
               const double Jd = 1e-3 * J * mu[sp];
               chm[sp] += J;
-              membrane += ((__ldg(T.ch_ap + q * C + gi) * 1e-15) * largest[sp]) * available;
               if (first) {
                 CH(q, 0, gi) = cur[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi] + w_acc * J;
                 CH(q, 1, gi) = cur[L.s[CB_CHANNEL_DISSIPATED] + q * C + gi] + w_acc * Jd;
@@ -246,7 +262,8 @@ __global__ void __launch_bounds__(BLOCK, 1)
               if (!(is_finite(J) && is_finite(Jd))) bits |= CB_WORLD_TRANSPORT;
             }
           }
-          if (!(k.dt * (__ldg(wc + WC_SLOPE) * membrane * icap) <= 1.0)) bits |= CB_WORLD_STIFF;
+          if (!(k.dt * ((__ldg(wc + WC_SLOPE) * membrane + blocked_tv) * icap) <= 1.0))
+            bits |= CB_WORLD_STIFF;
           // Pump.
           const double drive = __ldg(wc + WC_DRIVE);
           const double energy = (drive + (-3.0) * mu[0]) + 2.0 * mu[1];

@@ -793,6 +793,7 @@ size_t step_smem(int block, int ept, int nch) {
   return sizeof(double) * step_smem_words(block, ept, nch);
 }
 constexpr size_t kMaxSmemPerBlock = 227 * 1024;
+constexpr int kBlockMaxModes = 4;  // open_channel_block.MAX_MODES
 
 template <int BLOCK, int EPT>
 int launch_step(cb_tissue *t, const double *in, double *out, const double *control,
@@ -873,12 +874,12 @@ int launch_balances(cb_tissue *t, const double *st, double *out, cudaStream_t st
   return CB_OK;
 }
 
-template <int BLOCK, int NCH>
+template <int BLOCK, int NCH, bool BLK = false>
 int launch_packed_bn(cb_tissue *t, const double *in, double *out, const double *control,
                      const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
                      cudaStream_t stream) {
   const size_t smem = packed_smem_bytes(t->pk.cap);
-  auto kern = packed_kernel<BLOCK, NCH>;
+  auto kern = packed_kernel<BLOCK, NCH, BLK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
@@ -894,8 +895,11 @@ int launch_packed_bn(cb_tissue *t, const double *in, double *out, const double *
 int launch_packed(cb_tissue *t, const double *in, double *out, const double *control,
                   const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
                   cudaStream_t stream) {
-  const int key = t->packed_block * 10 + t->t.nch;
+  const int key = t->packed_block * 10 + t->t.nch + (t->t.blk_modes > 0 ? 100000 : 0);
   switch (key) {
+    case 102562: return launch_packed_bn<256, 2, true>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 105122: return launch_packed_bn<512, 2, true>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 110242: return launch_packed_bn<1024, 2, true>(t, in, out, control, k, n_steps, status, taken, stream);
     case 2560: return launch_packed_bn<256, 0>(t, in, out, control, k, n_steps, status, taken, stream);
     case 2562: return launch_packed_bn<256, 2>(t, in, out, control, k, n_steps, status, taken, stream);
     case 5120: return launch_packed_bn<512, 0>(t, in, out, control, k, n_steps, status, taken, stream);
@@ -950,6 +954,9 @@ const char *cb_last_error(void) { return cbk::last_error(); }
 int cb_set_launch(cb_tissue *t, int kernel, int block, int occupancy) {
   if (!t) return fail(CB_ERR_ARGUMENT, "null argument");
   if (kernel == CB_KERNEL_SHARED) {
+    if (t->t.blk_modes > 0)
+      return fail(CB_ERR_UNSUPPORTED, "a batch with an open-channel block runs on the packed "
+                                      "kernel only");
     if (!t->shared_ok) return fail(CB_ERR_UNSUPPORTED, "the one-world-per-CTA kernel cannot hold "
                                                        "these worlds");
     if (occupancy != 2 && occupancy != 3) return fail(CB_ERR_ARGUMENT, "occupancy must be 2 or 3");
@@ -1148,6 +1155,7 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
   t->h_edge_offset.assign(d->edge_offset, d->edge_offset + W + 1);
   t->h_snd = snd;
   t->h_rcv = rcv;
+  t->h_temperature.assign(d->temperature, d->temperature + W);
   auto vec = [](const double *p, long long n) { return std::vector<double>(p, p + n); };
   int rc = CB_OK;
   Tissue &T = t->t;
@@ -1303,6 +1311,7 @@ void cb_free(cb_tissue *t) {
   if (t->h_control) cudaFree(t->h_control);
   if (t->h_status) cudaFree(t->h_status);
   if (t->h_taken) cudaFree(t->h_taken);
+  if (t->blk_buf) cudaFree(t->blk_buf);
   delete t;
 }
 
@@ -1325,6 +1334,13 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
             void *stream) {
   if (!t || !state_in || !state_out || !control || !world_status)
     return fail(CB_ERR_ARGUMENT, "null argument");
+  if (t->t.blk_modes > 0 && method != CB_METHOD_ARS222)
+    return fail(CB_ERR_UNSUPPORTED,
+                method == CB_METHOD_N2 || method == CB_METHOD_N2_MIXED
+                    ? "the implicit-conductance step (N2) refuses a blocked channel population: a "
+                      "negative slope in its operator could make it indefinite"
+                    : "a batch with an open-channel block takes the FP64 step (CB_METHOD_ARS222) "
+                      "only");
   if (method == CB_METHOD_N2 || method == CB_METHOD_N2_MIXED) {
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
     if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
@@ -1394,6 +1410,84 @@ int cb_set_permeability(cb_tissue *t, const double *membrane, const double *junc
                                  static_cast<cudaStream_t>(stream));
 }
 
+int cb_set_channel_block(cb_tissue *t, int32_t modes, const double *weight,
+                         const double *k0_mM, const double *steepness,
+                         const double *concentration_mM) {
+  if (!t) return fail(CB_ERR_ARGUMENT, "null argument");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  if (modes == 0) {
+    t->t.blk_modes = 0;
+    t->t.blk = nullptr;
+    t->t.blk_conc = nullptr;
+    return CB_OK;
+  }
+  if (modes < 0 || modes > kBlockMaxModes)
+    return fail(CB_ERR_ARGUMENT, "block modes must be 0 (none) to 4");
+  if (t->t.nch == 0) return fail(CB_ERR_ARGUMENT, "the batch has no channel slots");
+  if (!weight || !k0_mM || !steepness || !concentration_mM)
+    return fail(CB_ERR_ARGUMENT, "null block array");
+  if (!t->pk.order)
+    return fail(CB_ERR_UNSUPPORTED, "a blocked batch runs on the packed kernel, which cannot "
+                                    "hold these worlds");
+  const long long NC = (long long)t->t.nch * t->C;
+  // The admitted domain (surface_pump_v3_spec.parse_block, _block_mode): weights in [0, 1]
+  // summing to 1 within 8 ulps, K(0) in [1e-15, 1e15] mM, |steepness| <= 8, the blocker in
+  // [0, 1e3] mM.
+  for (long long q = 0; q < NC; ++q) {
+    long double sum = 0.0L;
+    for (int k = 0; k < modes; ++k) {
+      const double w = weight[k * NC + q], k0 = k0_mM[k * NC + q], s = steepness[k * NC + q];
+      if (!(w >= 0.0 && w <= 1.0))
+        return fail(CB_ERR_LAYOUT, "block weights must lie in [0, 1]");
+      if (!(k0 >= 1e-15 && k0 <= 1e15))
+        return fail(CB_ERR_LAYOUT, "block K(0) must lie in [1e-15, 1e15] mM");
+      if (!(std::fabs(s) <= 8.0)) return fail(CB_ERR_LAYOUT, "block steepness must be <= 8");
+      sum += w;
+    }
+    if (!(std::fabs((double)(sum - 1.0L)) <= 8.0 * 2.220446049250313e-16))
+      return fail(CB_ERR_LAYOUT, "each population's block weights must sum to 1");
+    const double c = concentration_mM[q];
+    if (!(c >= 0.0 && c <= 1e3))
+      return fail(CB_ERR_LAYOUT, "blocker concentration must lie in [0, 1e3] mM");
+  }
+  // [3][M][NCH][C] (weight, K(0), a = steepness F/(R T) with the cell's world temperature),
+  // then the concentrations [NCH][C].
+  std::vector<double> host((size_t)(3 * modes + 1) * NC);
+  for (int w = 0; w < t->W; ++w) {
+    const double per_volt = kF / (kR * t->h_temperature[w]);
+    for (long long c = t->h_cell_offset[w]; c < t->h_cell_offset[w + 1]; ++c)
+      for (int q = 0; q < t->t.nch; ++q) {
+        const long long at = (long long)q * t->C + c;
+        for (int k = 0; k < modes; ++k) {
+          host[(size_t)k * NC + at] = weight[k * NC + at];
+          host[(size_t)(modes + k) * NC + at] = k0_mM[k * NC + at];
+          host[(size_t)(2 * modes + k) * NC + at] = steepness[k * NC + at] * per_volt;
+        }
+        host[(size_t)3 * modes * NC + at] = concentration_mM[at];
+      }
+  }
+  if (t->blk_doubles < host.size()) {
+    if (t->blk_buf) cudaFree(t->blk_buf);
+    t->blk_buf = nullptr;
+    t->blk_doubles = 0;
+    ce = cudaMalloc(&t->blk_buf, sizeof(double) * host.size());
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaMalloc block table");
+    t->blk_doubles = host.size();
+  }
+  ce = cudaMemcpy(t->blk_buf, host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy block table");
+  if (!t->packed) {
+    const int rc = alloc_packed_scratch(t);
+    if (rc) return rc;
+    t->packed = true;
+  }
+  t->t.blk_modes = modes;
+  t->t.blk = t->blk_buf;
+  t->t.blk_conc = t->blk_buf + (size_t)3 * modes * NC;
+  return CB_OK;
+}
+
 int cb_balances(cb_tissue *t, const double *state, double *out, void *stream) {
   if (!t || !state || !out) return fail(CB_ERR_ARGUMENT, "null argument");
   cudaError_t ce = cudaSetDevice(t->device);
@@ -1442,12 +1536,12 @@ int static_scratch(int device, double **out) {
   return CB_OK;
 }
 
-template <int BLOCK, int NCH>
+template <int BLOCK, int NCH, bool BLK = false>
 int launch_packed_with(cb_tissue *t, const Packed &P, const double *in, double *out,
                        const double *control, const StepCoef &k, int n_steps, uint32_t *status,
                        int32_t *taken, cudaStream_t stream) {
   const size_t smem = packed_smem_bytes(P.cap);
-  auto kern = packed_kernel<BLOCK, NCH>;
+  auto kern = packed_kernel<BLOCK, NCH, BLK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
@@ -1491,7 +1585,10 @@ extern "C" int cb_step_packed_static(cb_tissue *t, const double *state_in, doubl
   P.sc = base + kStaticCounterDoubles;
   const StepCoef k = step_coef(dt);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  switch (t->packed_block * 10 + t->t.nch) {
+  switch (t->packed_block * 10 + t->t.nch + (t->t.blk_modes > 0 ? 100000 : 0)) {
+    case 102562: return launch_packed_with<256, 2, true>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
+    case 105122: return launch_packed_with<512, 2, true>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
+    case 110242: return launch_packed_with<1024, 2, true>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
     case 2560: return launch_packed_with<256, 0>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
     case 2562: return launch_packed_with<256, 2>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);
     case 5120: return launch_packed_with<512, 0>(t, P, state_in, state_out, control, k, n_steps, world_status, accepted_steps, s);

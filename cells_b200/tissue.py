@@ -111,6 +111,8 @@ class Tissue:
                                               _ptr(total, ctypes.c_int64)))
         self.control_offsets = dict(zip(_lib.CONTROL_FIELDS, coff.tolist(), strict=True))
         self.control_size = int(total[0])
+        if b.channel_block is not None:
+            self.set_channel_block(b.channel_block)
 
     def close(self):
         if getattr(self, "handle", None) is not None and self.handle.value:
@@ -268,6 +270,17 @@ class Tissue:
             self.handle, ptr(membrane), ptr(junction), ptr(channel),
             None if stream is None else ctypes.c_void_p(stream),
         ))  # fmt: skip
+
+    def set_channel_block(self, block):
+        """cb_set_channel_block from a worlds.ChannelBlock over the batch's cells (None: remove
+        the block). A blocked batch runs on the packed kernel, FP64 ARS(2,2,2) only."""
+        if block is None:
+            _lib.check(self.lib.cb_set_channel_block(self.handle, 0, None, None, None, None))
+            return
+        arrays = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                  (block.weight, block.k0_mM, block.steepness, block.concentration_mM)]
+        _lib.check(self.lib.cb_set_channel_block(
+            self.handle, block.modes, *(_ptr(a, ctypes.c_double) for a in arrays)))
 
     def vjp_workspace_bytes(self, n_steps):
         out = ctypes.c_size_t()

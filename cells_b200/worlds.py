@@ -86,6 +86,8 @@ class World:
     channel_abundance: np.ndarray = field(default_factory=lambda: np.zeros((0, 0)))
     channel_gate_initial: np.ndarray = field(default_factory=lambda: np.zeros((2, 0, 0)))
     bath_mM: np.ndarray = field(default_factory=lambda: BATH_mM.copy())
+    # The populations' open-channel block ([M, NCH, N] modes), or None for none.
+    channel_block: ChannelBlock | None = None
     # Cell centres in the unit square ([2, N]), for spatial patterns over the tissue (the
     # adjoint benchmark's voltage target); empty when the builder has no geometry.
     position: np.ndarray = field(default_factory=lambda: np.zeros((2, 0)))
@@ -104,6 +106,122 @@ class World:
     @property
     def channel_slots(self):
         return int(self.channel_code.shape[0]) if self.channel_code.size else 0
+
+
+BLOCK_LAW_ID = "cells.channel_block.open_channel_block_weighted_modes@1"
+BLOCK_SIDES = {"outside": 1, "inside": -1}  # s in a_k = s sgn(z_B) m_k F/(R T)
+
+
+@dataclass
+class ChannelBlock:
+    """Open-channel block of the channel populations (the reference's FR-51 block,
+    laws/channels/open_channel_block.py), over the cells of one world or a batch. Arrays
+    [M, NCH, N] per mode slot, [NCH, N] per population. A population that declares no block holds
+    weights (1, 0, ...), K(0) 1, distance 0 and concentration 0, the reference's layout for it
+    (surface_pump_v3.block_initial_values :599-615), so its u is exactly 1; mode slots past a
+    population's own modes hold weight 0, K(0) 1, distance 0."""
+
+    declared: np.ndarray          # [NCH, N] bool: the population declares a block
+    weight: np.ndarray            # [M, NCH, N]
+    k0_mM: np.ndarray             # [M, NCH, N]
+    distance: np.ndarray          # [M, NCH, N] electrical distance delta_k in [0, 1]
+    modes_declared: np.ndarray    # [NCH, N] int: the population's own mode count
+    valence: np.ndarray           # [NCH, N] int: the blocker's valence z_B
+    side: np.ndarray              # [NCH, N] int: +1 outside, -1 inside
+    concentration_mM: np.ndarray  # [NCH, N]
+
+    @property
+    def modes(self):
+        return int(self.weight.shape[0])
+
+    @property
+    def steepness(self):
+        """[M, NCH, N] the signed steepness s sgn(z_B) |z_B| delta_k (ChannelBlock.steepness of
+        definitions/surface_pump_v3_spec.py, in its order of operations)."""
+        sign = self.side * np.where(self.valence > 0, 1, -1)
+        return sign * (np.abs(self.valence) * self.distance)
+
+    def cells(self, a, b):
+        """The block of cells a..b (a view)."""
+        return ChannelBlock(self.declared[:, a:b], self.weight[..., a:b], self.k0_mM[..., a:b],
+                            self.distance[..., a:b], self.modes_declared[:, a:b],
+                            self.valence[:, a:b], self.side[:, a:b],
+                            self.concentration_mM[:, a:b])
+
+    def padded(self, modes):
+        """The same block with ``modes`` mode slots (>= its own)."""
+        extra = modes - self.modes
+        if extra == 0:
+            return self
+        shape = (extra,) + self.weight.shape[1:]
+        return ChannelBlock(self.declared,
+                            np.concatenate([self.weight, np.zeros(shape)]),
+                            np.concatenate([self.k0_mM, np.ones(shape)]),
+                            np.concatenate([self.distance, np.zeros(shape)]),
+                            self.modes_declared, self.valence, self.side, self.concentration_mM)
+
+
+def unblocked(nch, n, modes=1):
+    """The layout of populations that declare no block."""
+    weight = np.zeros((modes, nch, n))
+    weight[0] = 1.0
+    return ChannelBlock(np.zeros((nch, n), dtype=bool), weight, np.ones((modes, nch, n)),
+                        np.zeros((modes, nch, n)), np.zeros((nch, n), dtype=np.int64),
+                        np.ones((nch, n), dtype=np.int64), np.ones((nch, n), dtype=np.int64),
+                        np.zeros((nch, n)))
+
+
+def with_block(world, rng, *, slot=0, fraction=1.0, valence=2, side="outside",
+               concentration_mM=(0.5, 2.0), modes=((0.625, 3.0, 0.8), (0.375, 30.0, 0.4))):
+    """Block the population in ``slot`` of a fraction of the cells by a held blocker of the given
+    valence and side (the default: an outside divalent blocker, Mg2+-like): concentration
+    log-uniform in ``concentration_mM``; ``modes`` as (weight, K(0) mM, electrical distance),
+    each K(0) scaled per cell by a log-uniform factor in [0.5, 2]. The weights must sum to 1."""
+    nch, n = world.channel_slots, world.cells
+    if nch == 0:
+        raise ValueError("the world has no channel populations")
+    m = len(modes)
+    if world.channel_block is None:
+        blk = unblocked(nch, n, m)
+    else:  # another slot's block is kept; the mode axis grows to the larger count
+        old = world.channel_block
+        blk = old.padded(max(m, old.modes))
+        blk = ChannelBlock(*(np.array(getattr(blk, f)) for f in (
+            "declared", "weight", "k0_mM", "distance", "modes_declared", "valence", "side",
+            "concentration_mM")))
+    cells = rng.random(n) < fraction
+    lo, hi = np.log(concentration_mM[0]), np.log(concentration_mM[1])
+    conc = np.exp(rng.uniform(lo, hi, n))
+    scale = np.exp(rng.uniform(np.log(0.5), np.log(2.0), (m, n)))
+    for i in np.flatnonzero(cells):
+        blk.declared[slot, i] = True
+        blk.modes_declared[slot, i] = m
+        blk.valence[slot, i] = valence
+        blk.side[slot, i] = BLOCK_SIDES[side]
+        blk.concentration_mM[slot, i] = conc[i]
+        blk.weight[:, slot, i], blk.k0_mM[:, slot, i], blk.distance[:, slot, i] = 0.0, 1.0, 0.0
+        for k, (w, k0, delta) in enumerate(modes):
+            blk.weight[k, slot, i] = w
+            blk.k0_mM[k, slot, i] = k0 * scale[k, i]
+            blk.distance[k, slot, i] = delta
+    world.channel_block = blk
+    return world
+
+
+def block_declaration(block, k, i):
+    """The reference's declaration of the block of population k of cell i (the channel entry's
+    "block" key, definitions/surface_pump_v3_spec.parse_block), or None."""
+    if block is None or not block.declared[k, i]:
+        return None
+    side = {v: key for key, v in BLOCK_SIDES.items()}[int(block.side[k, i])]
+    return {
+        "law": BLOCK_LAW_ID,
+        "blocker": {"id": f"blocker_{k}_{i}", "valence": int(block.valence[k, i]),
+                    "side": side, "concentration_mM": float(block.concentration_mM[k, i])},
+        "modes": [{"weight": float(block.weight[j, k, i]), "k0_mM": float(block.k0_mM[j, k, i]),
+                   "electrical_distance": float(block.distance[j, k, i])}
+                  for j in range(int(block.modes_declared[k, i]))],
+    }
 
 
 CHANNEL_LAW_IDS = {
@@ -335,6 +453,7 @@ class Batch:
     channel_abundance: np.ndarray = None  # [NCH, C]
     channel_gate_initial: np.ndarray = None  # [2, NCH, C]
     position: np.ndarray = None  # [2, C] cell centres in each world's unit square (zeros: none)
+    channel_block: ChannelBlock | None = None  # over the batch's cells; None: no block
 
     def __post_init__(self):
         c = self.cells
@@ -390,6 +509,8 @@ class Batch:
             channel_abundance=self.channel_abundance[:, c0:c1],
             channel_gate_initial=self.channel_gate_initial[:, :, c0:c1],
             position=self.position[:, c0:c1],
+            channel_block=(None if self.channel_block is None
+                           else self.channel_block.cells(c0, c1)),
             bath_mM=self.bath_amount[:, w] / self.bath_volume[w],
             bath_volume=float(self.bath_volume[w]),
             bath_potential=float(self.bath_potential[w]),
@@ -444,7 +565,23 @@ def pack(worlds):
                               else np.zeros((2, 0, int(cells.sum())))),
         position=cat([w.position if w.position.shape == (2, w.cells) else np.zeros((2, w.cells))
                       for w in worlds], axis=1),
+        channel_block=_pack_blocks(worlds, nch),
     )
+
+
+def _pack_blocks(worlds, nch):
+    """The worlds' blocks over the batch's cells (padded to the most modes), or None where no
+    world declares one."""
+    blocks = [w.channel_block for w in worlds]
+    if all(b is None for b in blocks):
+        return None
+    modes = max(b.modes for b in blocks if b is not None)
+    parts = [(unblocked(nch, w.cells, modes) if b is None else b.padded(modes))
+             for w, b in zip(worlds, blocks, strict=True)]
+    cat = np.concatenate
+    return ChannelBlock(*(cat([getattr(p, f) for p in parts], axis=-1) for f in
+                          ("declared", "weight", "k0_mM", "distance", "modes_declared",
+                           "valence", "side", "concentration_mM")))
 
 
 # --------------------------------------------------------------------------------------------
@@ -627,6 +764,9 @@ def reference_definition(world, *, dt, steps, model="cells.model.resolved_pump_t
                     "permeant_ions": [{"species_id": SPECIES[int(world.channel_species[k, i])],
                                        "relative_permeability": 1.0}],
                 })
+                block = block_declaration(world.channel_block, k, i)
+                if block is not None:
+                    chs[-1]["block"] = block
         out["model"]["channels"] = chs
         out["experiment"]["channel_controls"] = [
             {"channel_id": f"channel_{k}_{i}",

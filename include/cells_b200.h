@@ -280,6 +280,27 @@ int cb_vjp_workspace(const cb_tissue *t, int n_steps, size_t *bytes);
 int cb_set_permeability(cb_tissue *t, const double *membrane, const double *junction,
                         const double *channel, void *stream);
 
+/*
+ * Open-channel block of the channel populations (cells.channel_block.open_channel_block_weighted_modes@1,
+ * laws/channels/open_channel_block.py; @3's channel_rates :958-960, channel_block :1003-1036,
+ * channel_block_terms :1051-1126). Replaces the reference's block layout fields
+ * (surface_pump_v3.block_initial_values :599-615): channel_block_weight, channel_block_k0_mM,
+ * channel_block_steepness [modes][NCH*C] and channel_block_concentration_mM [NCH*C], host
+ * arrays in the channel slots' order. An unblocked population in a blocked batch takes weights
+ * (1, 0, ...), K(0) 1, steepness 0 and concentration 0 (u = 1 exactly), as the reference's layout
+ * gives it. The block reads the patch voltage (no voltage shift). The step multiplies each
+ * population's flux by its unblocked fraction u, takes T_V = u G_max + |I_free| du/dV in place of
+ * G_max in the explicit-stability rule, and refuses a world where a K or c_B + K is not a finite
+ * normal number (bit CB_WORLD_CHANNEL_DOMAIN). A blocked batch runs on the packed kernel (a
+ * shared-kernel handle is switched to it), FP64 ARS(2,2,2) only: N2 (as the reference refuses
+ * it), the mixed step and the adjoint return CB_ERR_UNSUPPORTED. modes = 0 removes the block.
+ * Domain checks as the reference's parse: weights in [0, 1] summing to 1 within 8 ulps, K(0) in
+ * [1e-15, 1e15] mM, |steepness| <= 8, the blocker in [0, 1e3] mM; modes at most 4.
+ */
+int cb_set_channel_block(cb_tissue *t, int32_t modes, const double *weight,
+                         const double *k0_mM, const double *steepness,
+                         const double *concentration_mM);
+
 /* Message of the last error on this thread. */
 const char *cb_last_error(void);
 /* Library version string. */

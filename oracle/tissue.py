@@ -400,6 +400,33 @@ def concentrations(state, b):
     return ci, co
 
 
+NORMAL = float(np.finfo(np.float64).tiny)
+
+
+def channel_block(blk, k, v, temperature):
+    """The open-channel block of slot k's populations at their patch voltages v [C]
+    (laws/channels/open_channel_block.py: dissociation, fractions, unblocked_fraction, slope,
+    domain_valid; surface_pump_v3.channel_block :1003-1036 without a voltage shift).
+    Returns (u, slope, valid) [C]."""
+    steep = blk.steepness[:, k]
+    per_volt = steep * (F / (R * temperature))  # exponent_per_volt
+    K = blk.k0_mM[:, k] * np.exp(per_volt * v)
+    c = blk.concentration_mM[k]
+    total = c + K
+    theta, free = c / total, K / total
+    w = blk.weight[:, k]
+    a = np.abs(per_volt)
+    num, den = w[0] * free[0], w[0]
+    snum = w[0] * a[0] * (theta[0] * free[0])
+    for j in range(1, w.shape[0]):
+        num = num + w[j] * free[j]
+        den = den + w[j]
+        snum = snum + w[j] * a[j] * (theta[j] * free[j])
+    valid = np.all(np.isfinite(K) & (K >= NORMAL) & np.isfinite(total) & (total >= NORMAL),
+                   axis=0)
+    return num / den, snum / den, valid
+
+
 def explicit_rates(state, potential, control, b, topo):
     """surface_pump.explicit_rates (surface_pump.py:158-240) for held-bath worlds."""
     w = topo.cell_world
@@ -439,6 +466,7 @@ def explicit_rates(state, potential, control, b, topo):
     chan, chan_d = np.zeros((nch, b.cells)), np.zeros((nch, b.cells))
     chsum = np.zeros((3, b.cells))
     ch_ok = np.ones(b.cells, dtype=bool)
+    block_ok = np.ones(b.cells, dtype=bool)
     if nch:
         opening = channel_opening(state.channel_gate, b.channel_code)
         with np.errstate(all="ignore"):
@@ -449,11 +477,15 @@ def explicit_rates(state, potential, control, b, topo):
                     0.0 + (1 - 0.0) * b.channel_abundance[k])
                 g = b.area * b.channel_permeability[k] * available / MOL_PER_FMOL
                 flux = g * (ci[sp, idx] * bernoulli(-x) - co_c[sp, idx] * bernoulli(x))
+                if getattr(b, "channel_block", None) is not None:  # surface_pump_v3.channel_rates :958-960
+                    u, _, blk_ok = channel_block(b.channel_block, k, dvm, t_c)
+                    flux = flux * u
+                    block_ok &= blk_ok
                 chan[k] = flux
                 chan_d[k] = 1e-3 * flux * mu_m[sp, idx]
                 chsum[sp, idx] = chsum[sp, idx] + flux
             targets, tau = channel_kinetics(dvm[None, :], b.channel_code)
-        ch_ok = np.all(channel_domain(dvm[None, :], targets, tau), axis=0)
+        ch_ok = np.all(channel_domain(dvm[None, :], targets, tau), axis=0) & block_ok
         ch_ok &= np.all(np.isfinite(control.channel) & (control.channel >= 0)
                         & (control.channel <= 1), axis=0)
         ch_ok &= np.all(np.isfinite(chan) & np.isfinite(chan_d), axis=0)
@@ -505,10 +537,14 @@ def explicit_rates(state, potential, control, b, topo):
     return Rates(rates, valid, dvm)
 
 
-def membrane_rate(state, control, b, topo):
+def membrane_rate(state, control, b, topo, potential=None):
     """Gershgorin rate (1/s) of membrane charge relaxation at a stage's openings, per world
     (surface_pump_v3.membrane_rate, :4588-4660, with _patch_slopes :4534-4585): max over cells of
-    F^2/RT sum z^2 P max(c) A (patch and open populations) over the cell's capacitance."""
+    F^2/RT sum z^2 P max(c) A (patch and open populations) over the cell's capacitance. With an
+    open-channel block every population enters with its T_V = u G_max + |I_free| slope
+    (channel_block_terms :1051-1090) at the stage's potentials, added after the patch's term."""
+    if getattr(b, "channel_block", None) is not None:
+        return _blocked_membrane_rate(state, control, b, topo, potential)
     w = topo.cell_world
     ci, co = concentrations(state, b)
     largest = np.maximum(ci, co[:, w])
@@ -528,6 +564,40 @@ def membrane_rate(state, control, b, topo):
             extra = extra + ch * b.area
     membrane = membrane + extra
     rate = slope * (0.0 + membrane) / (0.0 + b.capacitance)
+    out = np.zeros(b.worlds)
+    np.maximum.at(out, w, rate)
+    return out
+
+
+def _blocked_membrane_rate(state, control, b, topo, potential):
+    w = topo.cell_world
+    ci, co = concentrations(state, b)
+    largest = np.maximum(ci, co[:, w])
+    t_c = b.temperature[w]
+    slope = F * F / (R * t_c)
+    z2 = VALENCE[:, None] ** 2
+    terms = z2 * b.permeability * largest
+    passive = ((terms[0] + terms[1]) + terms[2]) * control.membrane
+    membrane = 0.0 + passive * b.area
+    dvm = potential - b.bath_potential[w]
+    idx = np.arange(b.cells)
+    open_fraction = b.channel_abundance * channel_opening(state.channel_gate, b.channel_code)
+    blocked = np.zeros(b.cells)
+    with np.errstate(all="ignore"):
+        for k in range(b.channel_slots):
+            sp = b.channel_species[k]
+            z = VALENCE[sp]
+            ch = (z ** 2 * b.channel_permeability[k] * 1.0 * largest[sp, idx]) * (
+                open_fraction[k] * control.channel[k])
+            g_max = F * F / (R * t_c) * (ch * b.area)
+            x = z * F * dvm / (R * t_c)
+            available = (channel_opening(state.channel_gate, b.channel_code)[k]
+                         * control.channel[k]) * (0.0 + (1 - 0.0) * b.channel_abundance[k])
+            g = b.area * b.channel_permeability[k] * available / MOL_PER_FMOL
+            free = g * (ci[sp, idx] * bernoulli(-x) - co[sp, w] * bernoulli(x))
+            u, s_u, _ = channel_block(b.channel_block, k, dvm, t_c)
+            blocked = blocked + (u * g_max + np.abs(CHARGE_PER_FMOL * (z * free)) * s_u)
+    rate = (slope * membrane + blocked) / (0.0 + b.capacitance)
     out = np.zeros(b.worlds)
     np.maximum.at(out, w, rate)
     return out
@@ -599,7 +669,7 @@ def ars222_step(state, dt, control, b, topo=None):
     k0 = explicit_rates(state, start, control, b, topo)
     valid = k0.valid.copy()
     # The explicit-stability refusal at each explicit stage (surface_pump_v3.py:3668-3670).
-    valid &= dt * membrane_rate(state, control, b, topo) <= EXPLICIT_STEP_BOUND
+    valid &= dt * membrane_rate(state, control, b, topo, start) <= EXPLICIT_STEP_BOUND
     zero = State(*(np.zeros_like(v) for v in state))
     zero = zero._replace(reservoir_supplied=-zero.reservoir_supplied)  # implicit_rates' -0.0
     rows = gate_rows_active(b.channel_code)
@@ -630,7 +700,7 @@ def ars222_step(state, dt, control, b, topo=None):
         np.logical_and.at(valid, w, ok)
     k1 = explicit_rates(stage, potential, control, b, topo)
     valid &= k1.valid
-    valid &= dt * membrane_rate(stage, control, b, topo) <= EXPLICIT_STEP_BOUND
+    valid &= dt * membrane_rate(stage, control, b, topo, potential) <= EXPLICIT_STEP_BOUND
     # Stage 2 (the last): explicit weights delta, 1 - delta; implicit 1 - gamma, gamma (zeros).
     known = _combine(state, dt, [(e_mat[2, 0], k0.state), (e_mat[2, 1], k1.state),
                                  (1.0 - GAMMA, zero)])

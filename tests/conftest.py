@@ -27,6 +27,9 @@ def load_golden(name):
     z = np.load(os.path.join(GOLDEN, name))
     batch = worlds.Batch(**{f.name: z["batch_" + f.name] for f in fields(worlds.Batch)
                             if "batch_" + f.name in z.files})
+    if "block_weight" in z.files:
+        batch.channel_block = worlds.ChannelBlock(
+            **{f.name: z["block_" + f.name] for f in fields(worlds.ChannelBlock)})
     return z, batch
 
 

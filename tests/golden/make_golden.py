@@ -99,7 +99,12 @@ def _channels_to_packed(state, world):
 def _batch_arrays(batch):
     from dataclasses import fields
 
-    return {"batch_" + f.name: getattr(batch, f.name) for f in fields(batch)}
+    out = {"batch_" + f.name: getattr(batch, f.name) for f in fields(batch)
+           if f.name != "channel_block"}
+    if batch.channel_block is not None:
+        out.update({"block_" + f.name: getattr(batch.channel_block, f.name)
+                    for f in fields(batch.channel_block)})
+    return out
 
 
 LAYOUT_FIELDS = (
@@ -302,6 +307,48 @@ def make_channel_trajectories():
     stacked, kept, el = _run(dworld, model_id=v3, dt=1e-3, steps=200, keep=keep, solver=ars,
                              controls=controls, channels=True)
     _save("ars222_v3_channels_delaunay.npz", worlds.pack([dworld]), stacked, kept, dt=1e-3,
+          model_id=v3, solver=ars, elapsed=el,
+          extra={"control_" + k.split("_")[0]: v for k, v in controls.items()})
+
+
+def make_block_trajectories():
+    """@3 with an open-channel block (cells.channel_block.open_channel_block_weighted_modes@1) on
+    its channel populations, read at the patch voltage."""
+    from cells_b200 import worlds
+
+    ars = "cells.solver.imex_ars222_face_electromigration@1"
+    v3 = "cells.model.resolved_pump_tissue@3"
+    rng = np.random.default_rng(41)
+    world = worlds.with_channels(worlds.grid_world(4, 4, worlds.world_rng(5, 0)), rng,
+                                 na=("nav", 2e-10, 0.5), k=("kv", 3e-10, 0.5), sigma=0.3)
+    worlds.with_block(world, rng, slot=0, fraction=0.75)
+    controls = dict(channel_control=rng.uniform(0.5, 1.0, (2, world.cells)))
+    keep = {0, 1, 2, 5, 50, 100, 200, 300}
+    stacked, kept, el = _run(world, model_id=v3, dt=1e-3, steps=300, keep=keep, solver=ars,
+                             controls=controls, channels=True)
+    _save("ars222_v3_block.npz", worlds.pack([world]), stacked, kept, dt=1e-3,
+          model_id=v3, solver=ars, elapsed=el, extra={"control_channel": controls[
+              "channel_control"]})
+
+    dworld = worlds.with_channels(
+        worlds.delaunay_world(40, worlds.world_rng(6, 0), junction_sigma=0.3,
+                              gate=(0.02, 0.1, 0.8)), rng,
+        na=("nav", 4e-10, 0.4), k=("kv", 5e-10, 0.6), sigma=0.3)
+    dworld.bath_potential = -0.004
+    worlds.with_block(dworld, rng, slot=0, fraction=0.5)
+    worlds.with_block(dworld, rng, slot=1, fraction=0.8, valence=2, side="inside",
+                      concentration_mM=(0.2, 1.0),
+                      modes=((0.5, 0.05, 0.9), (0.25, 0.5, 0.5), (0.25, 5.0, 0.1)))
+    controls = dict(
+        membrane_control=rng.uniform(0.5, 1.0, dworld.cells),
+        junction_control=rng.uniform(0.5, 1.0, dworld.edges),
+        pump_control=rng.uniform(0.5, 1.0, dworld.cells),
+        channel_control=rng.uniform(0.3, 1.0, (2, dworld.cells)),
+    )
+    keep = {0, 1, 2, 10, 100, 200}
+    stacked, kept, el = _run(dworld, model_id=v3, dt=1e-3, steps=200, keep=keep, solver=ars,
+                             controls=controls, channels=True)
+    _save("ars222_v3_block_delaunay.npz", worlds.pack([dworld]), stacked, kept, dt=1e-3,
           model_id=v3, solver=ars, elapsed=el,
           extra={"control_" + k.split("_")[0]: v for k, v in controls.items()})
 
@@ -521,8 +568,8 @@ def make_field_trajectories():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("laws", "trajectories", "channels", "n2", "checks",
-                                       "field"))
+    ap.add_argument("--only", choices=("laws", "trajectories", "channels", "block", "n2",
+                                       "checks", "field"))
     args = ap.parse_args()
     _setup(args.reference)
     if args.only in (None, "laws"):
@@ -531,6 +578,8 @@ def main():
         make_trajectories()
     if args.only in (None, "channels"):
         make_channel_trajectories()
+    if args.only in (None, "block"):
+        make_block_trajectories()
     if args.only in (None, "n2"):
         make_n2_trajectories()
     if args.only in (None, "checks"):
