@@ -103,6 +103,30 @@ class Mapping:
         self.receiver = local[_a(p, "junction_receiver")[self.junctions]]
 
 
+def block_from_layout(p, j):
+    """The layout's open-channel block (surface_pump_v3.block_initial_values' fields
+    channel_block_weight, _k0_mM, _steepness [M, channel] and _concentration_mM [channel]) at the
+    populations j [NCH, C], as a worlds.ChannelBlock. The signed steepness is carried as a
+    unit-valence blocker on the side of its sign, whose m_k is |steepness|, so the block's
+    steepness equals the layout's exactly."""
+    steep = _a(p, "channel_block_steepness")[:, j].astype(float)
+    weight = _a(p, "channel_block_weight")[:, j].astype(float)
+    conc = _a(p, "channel_block_concentration_mM")[j].astype(float)
+    modes = weight.shape[0]
+    neutral = np.zeros_like(weight)
+    neutral[0] = 1.0
+    declared = (conc != 0) | np.any(weight != neutral, axis=0)
+    side = np.where(np.all(steep >= 0, axis=0), 1, -1)
+    if np.any((steep != 0) & (np.sign(steep) != side)):
+        raise Unsupported("one population's modes must share their steepness sign")
+    return worlds.ChannelBlock(
+        declared=declared, weight=weight,
+        k0_mM=_a(p, "channel_block_k0_mM")[:, j].astype(float),
+        distance=np.abs(steep), modes_declared=np.full(conc.shape, modes),
+        valence=np.ones(conc.shape, dtype=np.int64), side=side.astype(np.int64),
+        concentration_mM=conc)
+
+
 def world_from_layout(p):
     """One reference layout -> (worlds.World, Mapping)."""
     m = Mapping(p)
@@ -130,6 +154,8 @@ def world_from_layout(p):
             channel_abundance=_a(p, "channel_abundance")[j].astype(float),
             channel_gate_initial=np.zeros((2, nch, m.cells.size)),
         )
+        if hasattr(p, "channel_block_weight"):
+            channel["channel_block"] = block_from_layout(p, j)
     if hasattr(p, "pump_present"):
         present = _a(p, "pump_present")[patch].astype(bool)
         stoich = _a(p, "stoichiometry")[:, patch]

@@ -124,7 +124,8 @@ class ChannelBlock:
     declared: np.ndarray          # [NCH, N] bool: the population declares a block
     weight: np.ndarray            # [M, NCH, N]
     k0_mM: np.ndarray             # [M, NCH, N]
-    distance: np.ndarray          # [M, NCH, N] electrical distance delta_k in [0, 1]
+    distance: np.ndarray          # [M, NCH, N] electrical distance delta_k (or, for a unit
+                                  # valence, the effective valence m_k)
     modes_declared: np.ndarray    # [NCH, N] int: the population's own mode count
     valence: np.ndarray           # [NCH, N] int: the blocker's valence z_B
     side: np.ndarray              # [NCH, N] int: +1 outside, -1 inside

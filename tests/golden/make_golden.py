@@ -24,6 +24,12 @@ Fixtures:
   rk4_grid4x4.npz        The 4x4 world by RK4 at dt 0.1 ms, 100 steps (@1).
   ars222_v3_channels.npz The 4x4 world (seed 3) with a NaV1.2 (m^3 h) and a Kv1.5 (m h)
                          population per cell, partial channel availabilities, @3, 300 steps.
+  ars222_v3_block.npz    A 4x4 world with both populations; 12 of its Na populations blocked by
+                         an outside divalent blocker in two modes; @3, 300 steps.
+  ars222_v3_block_delaunay.npz  A gated 40-cell Delaunay world with both populations: half the
+                         Na populations blocked (outside, two modes), 80% of the K populations
+                         (inside, three modes); partial controls; 200 steps.
+  pytrees_v3_block_padded.npz  That world's @3 pytrees, capacities 2 above the counts.
   ars222_v3_channels_delaunay.npz  A 40-cell Delaunay world with both populations, gated
                          junctions, partial controls, a -4 mV bath, @3, 200 steps.
   pytrees_v3_channels_padded.npz  That world's @3 pytrees with every capacity 2 above its count
@@ -124,6 +130,8 @@ LAYOUT_FIELDS = (
 CHANNEL_LAYOUT_FIELDS = (
     "channel_membranes", "channel_laws", "channel_relative_permeability",
     "channel_permeability", "channel_abundance", "channel_gate_active",
+    "channel_block_weight", "channel_block_k0_mM", "channel_block_steepness",
+    "channel_block_concentration_mM",
 )
 
 
@@ -345,6 +353,12 @@ def make_block_trajectories():
         pump_control=rng.uniform(0.5, 1.0, dworld.cells),
         channel_control=rng.uniform(0.3, 1.0, (2, dworld.cells)),
     )
+    # @3's own padded pytrees of the blocked world for the drop-in step.
+    out = _run_reference_pytrees(dworld, model_id=v3, dt=1e-3, steps=40, keep={0, 1, 20, 40},
+                                 padding=2, controls=controls)
+    np.savez_compressed(os.path.join(HERE, "pytrees_v3_block_padded.npz"), **out)
+    print("pytrees_v3_block_padded.npz written")
+
     keep = {0, 1, 2, 10, 100, 200}
     stacked, kept, el = _run(dworld, model_id=v3, dt=1e-3, steps=200, keep=keep, solver=ars,
                              controls=controls, channels=True)

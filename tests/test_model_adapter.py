@@ -37,7 +37,21 @@ def test_channel_layout_maps_to_the_same_world():
         assert np.array_equal(getattr(world, name), getattr(ref, name)), name
 
 
-@pytest.mark.parametrize("name", ["pytrees_gated_padded.npz", "pytrees_v3_channels_padded.npz"])
+def test_block_layout_maps_to_the_same_block():
+    """The reference's block layout fields of a padded @3 layout give the block of the world
+    they were made from: the same weights, K(0), concentrations and signed steepness."""
+    _, p, _, _ = load_pytrees("pytrees_v3_block_padded.npz")
+    world, m = model.world_from_layout(p)
+    _, b = load_golden("ars222_v3_block_delaunay.npz")
+    got, want = world.channel_block, b.channel_block
+    assert got is not None and got.modes == want.modes
+    for name in ("weight", "k0_mM", "concentration_mM", "steepness"):
+        assert np.array_equal(getattr(got, name), getattr(want, name)), name
+    assert np.array_equal(got.declared, want.declared)
+
+
+@pytest.mark.parametrize("name", ["pytrees_gated_padded.npz", "pytrees_v3_channels_padded.npz",
+                                  "pytrees_v3_block_padded.npz"])
 def test_state_round_trip_keeps_padding(name):
     _, p, _, states = load_pytrees(name)
     _, m = model.world_from_layout(p)

@@ -199,11 +199,11 @@ def test_device_balances_match_oracle_balances(cuda):
 
 
 @pytest.mark.parametrize("name", ["pytrees_gated_padded.npz", "pytrees_v3_channels_padded.npz",
-                                  "pytrees_n2_padded.npz"])
+                                  "pytrees_n2_padded.npz", "pytrees_v3_block_padded.npz"])
 def test_drop_in_checked_step_on_reference_pytrees(cuda, name):
     """model.DeviceStep called with the reference's own padded state, control and layout, step
     by step, against the reference's trajectory (@1; @3 with channels; @3 under N2, which the
-    layout declares); padded slots stay untouched."""
+    layout declares; @3 with blocked populations); padded slots stay untouched."""
     from cells_b200 import model
     from pytree_util import load_pytrees
 
