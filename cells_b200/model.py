@@ -127,8 +127,31 @@ def block_from_layout(p, j):
         concentration_mM=conc)
 
 
+# @3 options the device step does not carry, by a layout field each adds where it is declared
+# (models/surface_pump_v3.py: FORMS_LAYOUT_FIELDS :179, SHIFT_LAYOUT_FIELDS :210,
+# LOOP_LAYOUT_FIELDS :230, ONE_WAY_LAYOUT_FIELDS :287; series junction gates' parameters :6306).
+OPTION_FIELDS = {
+    "channel_shift_row": "voltage-shifted channel readers (FR-64)",
+    "forms_face_active": "forms faces",
+    "loop_flux_row": "routed loops",
+    "one_way_entity": "one-way flux records",
+    "junction_series_parameters": "series junction gates",
+}
+
+
+def refuse_options(p):
+    """Raise Unsupported for a layout that declares an option outside the device step: one of
+    OPTION_FIELDS, or a present Ca pump (@2's calcium_pump_present, models/surface_pump_v2.py:51)."""
+    for name, what in OPTION_FIELDS.items():
+        if hasattr(p, name):
+            raise Unsupported(f"{what} are not in the device step")
+    if hasattr(p, "calcium_pump_present") and np.any(_a(p, "calcium_pump_present")):
+        raise Unsupported("Ca pumps are not in the device step")
+
+
 def world_from_layout(p):
     """One reference layout -> (worlds.World, Mapping)."""
+    refuse_options(p)
     m = Mapping(p)
     valence = _a(p, "valence").reshape(-1)
     if not np.array_equal(valence, worlds.VALENCE):

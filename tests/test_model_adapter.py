@@ -77,6 +77,23 @@ def test_out_of_scope_layouts_are_refused():
         model.world_from_layout(p._replace(outside_active=outside))
 
 
+def test_layouts_with_other_options_are_refused():
+    """A layout that declares an option outside the device step (a voltage shift, forms faces,
+    loops, one-way records, series junction gates, a present Ca pump) is refused, so the stub
+    keeps the reference's own step for it."""
+    from collections import namedtuple
+
+    _, p, _, _ = load_pytrees("pytrees_v3_block_padded.npz")
+    for field in model.OPTION_FIELDS:
+        With = namedtuple("Layout", (*p._fields, field))
+        with pytest.raises(model.Unsupported):
+            model.world_from_layout(With(*p, np.zeros(1)))
+    With = namedtuple("Layout", (*p._fields, "calcium_pump_present"))
+    model.world_from_layout(With(*p, np.zeros(3, dtype=bool)))  # declared slots, none present
+    with pytest.raises(model.Unsupported, match="Ca pumps"):
+        model.world_from_layout(With(*p, np.array([False, True, False])))
+
+
 def test_layout_declares_its_solver():
     _, p, _, _ = load_pytrees("pytrees_n2_padded.npz")
     assert model.layout_solver(p) == model.N2_ID
