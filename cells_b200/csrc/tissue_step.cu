@@ -874,12 +874,12 @@ int launch_balances(cb_tissue *t, const double *st, double *out, cudaStream_t st
   return CB_OK;
 }
 
-template <int BLOCK, int NCH, bool BLK = false>
+template <int BLOCK, int NCH, bool BLK = false, bool MIX = false>
 int launch_packed_bn(cb_tissue *t, const double *in, double *out, const double *control,
                      const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
                      cudaStream_t stream) {
   const size_t smem = packed_smem_bytes(t->pk.cap);
-  auto kern = packed_kernel<BLOCK, NCH, BLK>;
+  auto kern = packed_kernel<BLOCK, NCH, BLK, MIX>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
@@ -894,9 +894,16 @@ int launch_packed_bn(cb_tissue *t, const double *in, double *out, const double *
 
 int launch_packed(cb_tissue *t, const double *in, double *out, const double *control,
                   const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
-                  cudaStream_t stream) {
-  const int key = t->packed_block * 10 + t->t.nch + (t->t.blk_modes > 0 ? 100000 : 0);
+                  cudaStream_t stream, bool mix = false) {
+  const int key = t->packed_block * 10 + t->t.nch + (t->t.blk_modes > 0 ? 100000 : 0) +
+                  (mix ? 200000 : 0);
   switch (key) {
+    case 202560: return launch_packed_bn<256, 0, false, true>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 202562: return launch_packed_bn<256, 2, false, true>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 205120: return launch_packed_bn<512, 0, false, true>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 205122: return launch_packed_bn<512, 2, false, true>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 210240: return launch_packed_bn<1024, 0, false, true>(t, in, out, control, k, n_steps, status, taken, stream);
+    case 210242: return launch_packed_bn<1024, 2, false, true>(t, in, out, control, k, n_steps, status, taken, stream);
     case 102562: return launch_packed_bn<256, 2, true>(t, in, out, control, k, n_steps, status, taken, stream);
     case 105122: return launch_packed_bn<512, 2, true>(t, in, out, control, k, n_steps, status, taken, stream);
     case 110242: return launch_packed_bn<1024, 2, true>(t, in, out, control, k, n_steps, status, taken, stream);
@@ -1352,9 +1359,6 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
   if (method != CB_METHOD_ARS222 && method != CB_METHOD_ARS222_MIXED)
     return fail(CB_ERR_UNSUPPORTED, "unknown step method");
   const bool mix = method == CB_METHOD_ARS222_MIXED;
-  if (mix && t->packed)
-    return fail(CB_ERR_UNSUPPORTED, "the mixed-precision step runs on the one-world-per-CTA "
-                                    "kernel only");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
   if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
   cudaError_t ce = cudaSetDevice(t->device);
@@ -1363,7 +1367,7 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (t->packed)
     return launch_packed(t, state_in, state_out, control, k, n_steps, world_status,
-                         accepted_steps, s);
+                         accepted_steps, s, mix);
   CB_DISPATCH(launch_step, state_in, state_out, control, k, n_steps, world_status,
               accepted_steps, s, mix);
 }

@@ -144,7 +144,8 @@ enum cb_control_field {
  * cells_b200.solver.imex_ars222_mixed_fp32@1; no reference method): transcendentals, fluxes,
  * the pump and channel kinetics in FP32 on FP64 concentration and potential differences; the
  * near-zero Bernoulli series, concentrations, potentials, world sums and every state and ledger
- * accumulation in FP64. One-world-per-CTA kernel only. */
+ * accumulation in FP64. Both kernels (one world per CTA, and the packed kernel for uneven
+ * batches); not with an open-channel block. */
 #define CB_METHOD_ARS222_MIXED 1
 /* N2 (cells.solver.imex_ars222_implicit_conductances@1, models/surface_pump_v3.py:3547-3955 under
  * an N2 ID): ARS(2,2,2) with every patch's, channel population's and junction's slope

@@ -32,11 +32,19 @@ def _run(torch, tissue, method, steps, chunks):
     return tissue.unpack_state(state.cpu().numpy()), worst
 
 
-@pytest.mark.parametrize("kind", ["grid", "channels"])
+@pytest.mark.parametrize("kind", ["grid", "channels", "packed"])
 def test_mixed_step_error_against_fp64(cuda, kind):
+    """grid and channels on the one-world-per-CTA kernel; packed: uneven Delaunay worlds of
+    40-2500 cells with NaV1.2 + HH K on the packed kernel (both methods)."""
     rng = np.random.default_rng(3)
     if kind == "grid":
         ws = worlds.grid_tissues(64, side=16, seed=12)
+    elif kind == "packed":
+        ws = [worlds.with_channels(worlds.delaunay_world(n, worlds.world_rng(14, k),
+                                                         junction_sigma=0.3,
+                                                         gate=(0.02, 0.2, 0.9)), rng,
+                                   na=("nav", 1e-9, 0.5), k=("hh", 5e-10, 0.5), sigma=0.3)
+              for k, n in enumerate((2500, 1100, 700, 333, 150, 90, 40))]
     else:
         ws = [worlds.with_channels(worlds.delaunay_world(200, worlds.world_rng(13, k),
                                                          junction_sigma=0.3), rng,
@@ -44,6 +52,8 @@ def test_mixed_step_error_against_fp64(cuda, kind):
               for k in range(16)]
     b = worlds.pack(ws)
     tissue = Tissue(b)
+    if kind == "packed":
+        assert tissue.get_launch()[0] == _lib.KERNEL_PACKED
     ref, _ = _run(cuda, tissue, _lib.METHOD_ARS222, 100, 5)
     got, ledgers = _run(cuda, tissue, _lib.METHOD_ARS222_MIXED, 100, 5)
     amounts = np.abs(b.amount_reference + ref["amount_increment"])
