@@ -296,7 +296,9 @@ int cb_set_permeability(cb_tissue *t, const double *membrane, const double *junc
  * shared-kernel handle is switched to it), FP64 ARS(2,2,2) only: N2 (as the reference refuses
  * it), the mixed step and the adjoint return CB_ERR_UNSUPPORTED. modes = 0 removes the block.
  * Domain checks as the reference's parse: weights in [0, 1] summing to 1 within 8 ulps, K(0) in
- * [1e-15, 1e15] mM, |steepness| <= 8, the blocker in [0, 1e3] mM; modes at most 4.
+ * [1e-15, 1e15] mM, |steepness| <= 8, the blocker in [0, 1e3] mM; modes at most 4. Host call
+ * (it may allocate the device table and synchronizes): not inside a stream capture, and not while
+ * a step of this handle runs.
  */
 int cb_set_channel_block(cb_tissue *t, int32_t modes, const double *weight,
                          const double *k0_mM, const double *steepness,
