@@ -74,6 +74,7 @@ EXPORTS = (
     "cb_set_permeability",
     "cb_set_channel_block",
     "cb_device_checks",
+    "cb_device_checks_each",
     "cb_field_bind",
     "cb_field_free",
     "cb_field_state_layout",
@@ -218,6 +219,8 @@ def load(path=LIBRARY):
     lib.cb_set_channel_block.restype = ctypes.c_int
     lib.cb_device_checks.argtypes = [_p, _p, _p, ctypes.c_int64, _d, ctypes.c_double, _p, _p, _p]
     lib.cb_device_checks.restype = ctypes.c_int
+    lib.cb_device_checks_each.argtypes = [_p, _p, _p, _p, _d, ctypes.c_double, _p, _p, _p]
+    lib.cb_device_checks_each.restype = ctypes.c_int
     lib.cb_field_bind.argtypes = [ctypes.POINTER(FieldDesc), ctypes.c_int, ctypes.POINTER(_p)]
     lib.cb_field_bind.restype = ctypes.c_int
     lib.cb_field_free.argtypes = [_p]

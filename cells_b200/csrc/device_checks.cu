@@ -48,6 +48,7 @@ struct CheckArgs {
   double rtol;     // the solver's energy tolerance
   double rounding; // 2.5 eps x accepted steps
   double grounding;  // 2.5 eps x accepted steps (the grounded components' rule)
+  const int64_t *steps;  // per-world accepted steps (device [W]), or null: rounding/grounding
 };
 
 template <int BLOCK>
@@ -74,6 +75,11 @@ __global__ void __launch_bounds__(BLOCK)
   const long long C = T.C, E = T.E, W = T.W;
   const int nch = T.nch;
   const double *wc = T.world + (size_t)w * WC_STRIDE;
+  // The step-scaled rounding allowances: the call's, or this world's own step count.
+  const double rounding =
+      A.steps ? kLedgerStepRounding * kEps * (double)A.steps[w] : A.rounding;
+  const double grounding =
+      A.steps ? kComponentStepRounding * kEps * (double)A.steps[w] : A.grounding;
   if (tid == 0) sFail = 0u;
   __syncthreads();
   uint32_t fail = 0;
@@ -140,7 +146,7 @@ __global__ void __launch_bounds__(BLOCK)
       const double total_m = moved[sp] - stoich[sp] * pc;
       const double local = ((n[sp] + total_m) + send[sp]) - recv[sp];
       const double mag = (fabs(n[sp]) + absmoved[sp]) + abs_j[sp];
-      if (bad(local, A.tol[sp] + A.rounding * mag)) fail |= 1u << K_LOCAL;
+      if (bad(local, A.tol[sp] + rounding * mag)) fail |= 1u << K_LOCAL;
       m_local = fmax(m_local, fabs(local));
       s[sp] += total_m;
       s[3 + sp] += n[sp];
@@ -161,7 +167,7 @@ __global__ void __launch_bounds__(BLOCK)
     // Metabolic work: mw + 1e-3 drive cycles.
     const double mw = row[L.s[CB_METABOLIC_WORK] + gi];
     const double met = mw + 1e-3 * wc[WC_DRIVE] * pc;
-    if (bad(met, kWorkBound + A.rounding * (fabs(mw) + 1e-3 * fabs(wc[WC_DRIVE] * pc))))
+    if (bad(met, kWorkBound + rounding * (fabs(mw) + 1e-3 * fabs(wc[WC_DRIVE] * pc))))
       fail |= 1u << K_METABOLIC;
     m_metab = fmax(m_metab, fabs(met));
     // Energy: chemical free energy, capacitor energy, heat, less metabolic work.
@@ -215,8 +221,8 @@ __global__ void __launch_bounds__(BLOCK)
     abs_sup[sp] = fabs(sup[sp]);
     const double outside = -s[sp] - sup[sp];
     const double total = s[3 + sp] - sup[sp];
-    if (bad(outside, A.tol[sp] + A.rounding * (s[6 + sp] + abs_sup[sp]))) bits |= 1u << K_OUTSIDE;
-    if (bad(total, A.tol[sp] + A.rounding * (s[9 + sp] + abs_sup[sp]))) bits |= 1u << K_TOTAL;
+    if (bad(outside, A.tol[sp] + rounding * (s[6 + sp] + abs_sup[sp]))) bits |= 1u << K_OUTSIDE;
+    if (bad(total, A.tol[sp] + rounding * (s[9 + sp] + abs_sup[sp]))) bits |= 1u << K_TOTAL;
     m_out = fmax(m_out, fabs(outside));
     m_tot = fmax(m_tot, fabs(total));
     moved_charge += fabs(z[sp] * sup[sp]);
@@ -233,7 +239,7 @@ __global__ void __launch_bounds__(BLOCK)
   const double global = ec + kChargePerFmol * ((sup[0] + sup[1]) - sup[2]);
   const double gbound = kGlobalChargeAtol + kGlobalChargeRounding * moved_charge;
   const double glimit =
-      fmax(gbound + A.rounding * moved_charge, gbound + A.grounding * s[13]);
+      fmax(gbound + rounding * moved_charge, gbound + grounding * s[13]);
   if (bad(global, glimit)) bits |= 1u << K_GLOBAL;
   const double energy = (s[14] - rw) - ew;
   const double flows = (s[15] + fabs(rw)) + fabs(ew);
@@ -243,9 +249,9 @@ __global__ void __launch_bounds__(BLOCK)
   const double mag_rw = fabs(rw) + 1e-3 * ((fabs(wc[WC_MUB]) * abs_sup[0] +
                                             fabs(wc[WC_MUB + 1]) * abs_sup[1]) +
                                            fabs(wc[WC_MUB + 2]) * abs_sup[2]);
-  if (bad(res_w, kWorkBound + A.rounding * mag_rw)) bits |= 1u << K_RESERVOIR_WORK;
+  if (bad(res_w, kWorkBound + rounding * mag_rw)) bits |= 1u << K_RESERVOIR_WORK;
   const double res_e = ew - 1e12 * Vb * ec;
-  if (bad(res_e, kWorkBound + A.rounding * (fabs(ew) + 1e12 * fabs(Vb * ec))))
+  if (bad(res_e, kWorkBound + rounding * (fabs(ew) + 1e12 * fabs(Vb * ec))))
     bits |= 1u << K_ELECTRODE_WORK;
   failed_out[w] = bits;
   double *v = values_out + (size_t)w * 12;
@@ -278,6 +284,28 @@ extern "C" int cb_device_checks(cb_tissue *t, const double *previous, const doub
   A.rtol = energy_rtol;
   A.rounding = kLedgerStepRounding * kEps * (double)steps;
   A.grounding = kComponentStepRounding * kEps * (double)steps;
+  A.steps = nullptr;
+  checks_kernel<kChecksBlock><<<t->W, kChecksBlock, 0, static_cast<cudaStream_t>(stream)>>>(
+      t->t, t->layout, previous, row, A, failed, values);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return cuda_fail(ce, "device checks launch");
+  return CB_OK;
+}
+
+extern "C" int cb_device_checks_each(cb_tissue *t, const double *previous, const double *row,
+                                     const int64_t *steps, const double *material_atol,
+                                     double energy_rtol, uint32_t *failed, double *values,
+                                     void *stream) {
+  if (!t || !previous || !row || !steps || !material_atol || !failed || !values)
+    return fail(CB_ERR_ARGUMENT, "null argument");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  CheckArgs A;
+  for (int s = 0; s < 3; ++s) A.tol[s] = material_atol[s];
+  A.rtol = energy_rtol;
+  A.rounding = 0.0;
+  A.grounding = 0.0;
+  A.steps = steps;
   checks_kernel<kChecksBlock><<<t->W, kChecksBlock, 0, static_cast<cudaStream_t>(stream)>>>(
       t->t, t->layout, previous, row, A, failed, values);
   ce = cudaGetLastError();

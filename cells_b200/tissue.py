@@ -47,6 +47,12 @@ DIAGNOSTICS = tuple("max_" + k for k in (
     "metabolic_work_error_pJ", "energy_balance_relative", "global_charge_bound_ratio"))
 
 
+def _torch_int64():
+    import torch
+
+    return torch.int64
+
+
 def _ptr(a, ctype=ctypes.c_double):
     return a.ctypes.data_as(ctypes.POINTER(ctype))
 
@@ -247,14 +253,21 @@ class Tissue:
                       values_dev, stream=None):
         """cb_device_checks: the accepted-row checks of row_dev against previous_dev (packed
         float64 device states); failed_dev [W] int32 receives each world's bitmask (bit k:
-        CHECKS[k] failed), values_dev [W*12] float64 the diagnostics."""
+        CHECKS[k] failed), values_dev [W*12] float64 the diagnostics. steps: the accepted-step
+        count, one number for every world, or an int64 device tensor [W] of each world's own
+        (cb_device_checks_each)."""
         atol = (ctypes.c_double * 3)(*np.broadcast_to(np.asarray(material_atol, float), 3))
-        _lib.check(self.lib.cb_device_checks(
-            self.handle, ctypes.c_void_p(previous_dev.data_ptr()),
-            ctypes.c_void_p(row_dev.data_ptr()), int(steps), atol, float(energy_rtol),
-            ctypes.c_void_p(failed_dev.data_ptr()), ctypes.c_void_p(values_dev.data_ptr()),
-            None if stream is None else ctypes.c_void_p(stream),
-        ))  # fmt: skip
+        args = (ctypes.c_void_p(previous_dev.data_ptr()), ctypes.c_void_p(row_dev.data_ptr()))
+        tail = (atol, float(energy_rtol), ctypes.c_void_p(failed_dev.data_ptr()),
+                ctypes.c_void_p(values_dev.data_ptr()),
+                None if stream is None else ctypes.c_void_p(stream))
+        if hasattr(steps, "data_ptr"):
+            if steps.dtype != _torch_int64() or steps.numel() != self.batch.worlds:
+                raise ValueError("per-world steps must be an int64 tensor of one entry per world")
+            _lib.check(self.lib.cb_device_checks_each(
+                self.handle, *args, ctypes.c_void_p(steps.data_ptr()), *tail))
+        else:
+            _lib.check(self.lib.cb_device_checks(self.handle, *args, int(steps), *tail))
 
     def set_permeability(self, membrane=None, junction=None, channel=None, stream=None):
         """cb_set_permeability from float64 device tensors (m/s): membrane [3, C], junction

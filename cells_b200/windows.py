@@ -13,11 +13,12 @@ accepted steps), and
   DEVICE_DIAGNOSTICS of cb_device_checks) and stores the row in its observation slot;
 * a world stops after its own count of rows (``counts``).
 
-Differences from the reference, by design of the C ABI: the worlds of one batch share their
-accepted-step count at the window start (``first_step`` is one number; cb_device_checks takes one
-step count), and a row's step size and held control are the same for every world. The state
-stays on the device; the host issues two kernels per row (the step, the checks) and a few device
-selects.
+As the reference's, each world has its own step size, held-control index and observation slot
+per row (``[W, width]``; a ``[width]`` row applies to every world) and its own accepted-step count
+at the window start (``first_step``: one number or ``[W]``; cb_device_checks_each). cb_step takes
+one step size per launch, so a row whose worlds take different step sizes runs the step once per
+distinct size and keeps each world's own result. The state stays on the device; the host issues
+two kernels per row (the step, the checks) and a few device selects.
 """
 
 from __future__ import annotations
@@ -64,14 +65,34 @@ def world_of_elements(tissue):
     return tissue.pack_state(ids).astype(np.int64)
 
 
+def world_of_controls(tissue):
+    """[control_total] world index of every element of the packed control (padding: 0)."""
+    b = tissue.batch
+    cell_world = np.repeat(np.arange(b.worlds), np.diff(b.cell_offset)).astype(np.float64)
+    edge_world = np.repeat(np.arange(b.worlds), np.diff(b.edge_offset)).astype(np.float64)
+    return tissue.pack_control(membrane=cell_world, junction=edge_world, pump=cell_world,
+                               channel=cell_world).astype(np.int64)
+
+
+def _per_world(value, n_worlds, width, dtype):
+    """A row table [W, width] from [width] (every world) or [W, width]."""
+    a = np.asarray(value, dtype=dtype)
+    if a.ndim == 1:
+        a = np.broadcast_to(a[None, :], (n_worlds, a.size))
+    if a.shape != (n_worlds, width):
+        raise ValueError(f"expected [{width}] or [{n_worlds}, {width}], got {a.shape}")
+    return np.array(a)  # a writable copy (torch refuses read-only views)
+
+
 def vector_window(tissue, state, dt, controls, held, *, slots=None, counts=None, first_step=0,
                   material_atol=2e-11, energy_rtol=2e-3, rows=0, method=0, world_of=None):
     """One window of every world of a bound batch (torch float64 device tensors).
 
-    state: packed start state [state_total]; dt: [width] step sizes; controls: [n, control_total]
-    the held-control table; held: [width] row -> control index; slots: [width] row -> observation
-    slot (-1 or >= rows: not stored); counts: [W] rows each world takes (default: all);
-    first_step: accepted steps before the window (every world's); material_atol: per species
+    state: packed start state [state_total]; dt: step sizes [width] or [W, width]; controls:
+    [n, control_total] the held-control table (row i packs every world's control i); held: row
+    -> control index, [width] or [W, width]; slots: row -> observation slot (-1 or >= rows: not
+    stored), [width] or [W, width]; counts: [W] rows each world takes (default: all);
+    first_step: accepted steps before the window, one number or [W]; material_atol: per species
     (fmol); energy_rtol; rows: observation slots; method: cb_step's method; world_of: the cached
     world_of_elements(tissue) as a device tensor.
     """
@@ -79,34 +100,63 @@ def vector_window(tissue, state, dt, controls, held, *, slots=None, counts=None,
 
     dev = state.device
     n_worlds = tissue.batch.worlds
-    width = len(dt)
-    held = [int(h) for h in held]
-    slots = [-1] * width if slots is None else [int(s) for s in slots]
+    width = np.asarray(dt).shape[-1]
+    dt_w = _per_world(dt, n_worlds, width, np.float64)
+    held_w = _per_world(held, n_worlds, width, np.int64)
+    slots_w = _per_world(np.full(width, -1) if slots is None else slots, n_worlds, width,
+                         np.int64)
     counts_t = torch.full((n_worlds,), width, dtype=torch.int64, device=dev) if counts is None \
         else torch.as_tensor(np.asarray(counts), dtype=torch.int64, device=dev)
+    per_world_first = np.ndim(first_step) > 0
+    first_t = torch.as_tensor(np.array(np.broadcast_to(np.asarray(first_step, np.int64),
+                                                       (n_worlds,))),
+                              dtype=torch.int64, device=dev)
     if world_of is None:
         world_of = torch.from_numpy(world_of_elements(tissue)).to(dev)
+    ctl_world = None
+    if np.any(held_w != held_w[:1]):
+        ctl_world = torch.from_numpy(world_of_controls(tissue)).to(dev)
+        ctl_index = torch.arange(controls.shape[1], device=dev)
     shift = torch.arange(12, dtype=torch.int64, device=dev) + FAILURE_SHIFT
     failed = torch.zeros(n_worlds, dtype=torch.int32, device=dev)
     values = torch.zeros(n_worlds * 12, dtype=torch.float64, device=dev)
     status = torch.zeros(n_worlds, dtype=torch.int32, device=dev)
 
-    def checks(previous, row, steps):
+    def checks(previous, row, offset):
+        steps = first_t + offset if per_world_first else int(first_step) + offset
         tissue.device_checks(previous, row, steps, material_atol, energy_rtol, failed, values)
         bits = (failed.to(torch.int64)[:, None] >> torch.arange(12, device=dev)) & 1
         return (bits << shift).sum(dim=1), values.view(n_worlds, 12).clone()
 
     current = state.clone()
-    bits, vals = checks(current, current, first_step)
+    bits, vals = checks(current, current, 0)
     ok = bits == 0
     first = torch.where(ok, -1, 0).to(torch.int32)
     maxima = torch.where(ok[:, None], vals, torch.zeros_like(vals))
     stored = torch.zeros((rows, current.numel()), dtype=torch.float64, device=dev)
     updated = torch.empty_like(current)
+    element = torch.arange(current.numel(), device=dev)
     for j in range(1, width + 1):
-        tissue.step(current, updated, controls[held[j - 1]], float(dt[j - 1]), 1, status,
-                    method=method)
-        row_bits, vals = checks(current, updated, first_step + j)
+        col = j - 1
+        if ctl_world is None:
+            control = controls[int(held_w[0, col])]
+        else:
+            held_t = torch.as_tensor(held_w[:, col], device=dev)
+            control = controls[held_t[ctl_world], ctl_index]
+        sizes = np.unique(dt_w[:, col])
+        if sizes.size == 1:
+            tissue.step(current, updated, control, float(sizes[0]), 1, status, method=method)
+        else:  # one launch per distinct step size, each world keeping its own
+            trial = torch.empty_like(current)
+            trial_status = torch.empty_like(status)
+            dt_t = torch.as_tensor(dt_w[:, col], device=dev)
+            for size in sizes:
+                tissue.step(current, trial, control, float(size), 1, trial_status,
+                            method=method)
+                take = dt_t == float(size)
+                updated = torch.where(take[world_of], trial, updated)
+                status = torch.where(take, trial_status, status)
+        row_bits, vals = checks(current, updated, j)
         flags = torch.where(status == 0, row_bits, torch.ones_like(row_bits))
         live = (j <= counts_t) & ok
         failing = live & (flags != 0)
@@ -115,8 +165,14 @@ def vector_window(tissue, state, dt, controls, held, *, slots=None, counts=None,
         bits = torch.where(failing, flags, bits)
         current = torch.where(accept[world_of], updated, current)
         maxima = torch.where(accept[:, None], torch.maximum(maxima, vals), maxima)
-        slot = slots[j - 1]
-        if 0 <= slot < rows:
-            stored[slot] = torch.where(accept[world_of], current, stored[slot])
+        slot_col = slots_w[:, col]
+        if np.all(slot_col == slot_col[0]):
+            slot = int(slot_col[0])
+            if 0 <= slot < rows:
+                stored[slot] = torch.where(accept[world_of], current, stored[slot])
+        else:
+            slot_t = torch.as_tensor(slot_col, device=dev)[world_of]
+            keep = accept[world_of] & (slot_t >= 0) & (slot_t < rows)
+            stored[slot_t[keep], element[keep]] = current[keep]
         ok = ok & ~failing
     return Window(current, first, bits, maxima, stored)

@@ -227,6 +227,17 @@ int cb_device_checks(cb_tissue *t, const double *previous, const double *row, in
                      double *values, void *stream);
 
 /*
+ * cb_device_checks with each world's own accepted-step count (steps: DEVICE int64 [W], each
+ * non-negative), as the reference's vector windows give every world its own first_step
+ * (execution/vector_windows.py:348-410, `checked(current, updated, params, constants,
+ * first_step + row)`). A world's result equals cb_device_checks' at that world's count, bit for
+ * bit.
+ */
+int cb_device_checks_each(cb_tissue *t, const double *previous, const double *row,
+                          const int64_t *steps, const double *material_atol, double energy_rtol,
+                          uint32_t *failed, double *values, void *stream);
+
+/*
  * cb_step for a handle bound for the packed kernel, with the kernel's scratch (stage
  * accumulators, junction fluxes, world-sum terms, the work-queue counter) taken from a 16 MiB
  * array that the library holds on every GPU it is loaded on, so the call allocates nothing. No

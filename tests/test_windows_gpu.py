@@ -95,3 +95,105 @@ def test_window_matches_the_oracle_window(cuda):
     m = win.maxima.cpu().numpy()
     for k in (6, 10):
         assert np.all(np.abs(m[:, k] - maxima[:, k]) <= 1e-8 * np.abs(maxima[:, k])), k
+
+
+# Per-world rows: each world its own step sizes, held-control indices, observation slots and
+# accepted-step count at the window start (the reference's [W, width] tables and [W] first_step).
+DT_W = np.array([[1e-3] * 6, [5e-4] * 6, [1e-3, 2e-3, 1e-3, 2e-3, 1e-3, 2e-3]])
+HELD_W = np.array([[0, 0, 1, 1, 0, 1], [1, 0, 0, 1, 1, 0], [0, 1, 0, 1, 0, 1]])
+SLOTS_W = np.array([[0, -1, 1, -1, -1, 2], [-1, 0, -1, 1, 2, -1], [2, -1, -1, 0, 1, -1]])
+FIRST_W = np.array([0, 7, 3])
+
+
+def _control_of(controls, held_row, b, topo):
+    """The oracle Control whose world w takes controls[held_row[w]]."""
+    cw, ew = topo.cell_world, topo.edge_world
+    cells = np.arange(b.cells)
+    pick = held_row[cw]
+    membrane = np.stack([c.membrane for c in controls])[pick, cells]
+    pump = np.stack([c.pump for c in controls])[pick, cells]
+    junction = np.stack([c.junction for c in controls])[held_row[ew], np.arange(b.edges)]
+    channel = np.stack([np.asarray(c.channel) for c in controls])
+    if channel.ndim == 3:  # [n, NCH, C]
+        channel = channel[pick, :, cells].T
+    else:  # no channel slots: the one (empty) control of every entry
+        channel = np.asarray(controls[0].channel)
+    return T.Control(membrane, junction, pump, channel)
+
+
+def oracle_window_each(b, controls):
+    topo = T.topology(b)
+    cur = T.initial_state(b)
+
+    def checks_each(prev, row, offset):
+        failed = np.zeros((b.worlds, 12), dtype=bool)
+        vals = np.zeros((b.worlds, 12))
+        for steps in np.unique(FIRST_W + offset):
+            f, v = CK.row_checks(prev, row, b, topo, int(steps), ATOL, RTOL)
+            sel = FIRST_W + offset == steps
+            failed[sel], vals[sel] = f[sel], v[sel]
+        return failed, vals
+
+    failed0, vals0 = checks_each(cur, cur, 0)
+    pack = (failed0 << (np.arange(12) + 1)).sum(axis=1)
+    ok = pack == 0
+    first = np.where(ok, -1, 0)
+    bits = pack.copy()
+    maxima = np.where(ok[:, None], vals0, 0.0)
+    stored = {}
+    for j in range(1, DT_W.shape[1] + 1):
+        control = _control_of(controls, HELD_W[:, j - 1], b, topo)
+        new, valid = cur, np.zeros(b.worlds, dtype=bool)
+        for size in np.unique(DT_W[:, j - 1]):
+            trial, v = T.ars222_step(cur, float(size), control, b, topo)
+            take = DT_W[:, j - 1] == size
+            new = T._select(take, trial, new, b, topo)
+            valid = np.where(take, v, valid)
+        failed, vals = checks_each(cur, new, j)
+        flags = np.where(valid, (failed << (np.arange(12) + 1)).sum(axis=1), 1)
+        live = (j <= np.asarray(COUNTS)) & ok
+        failing = live & (flags != 0)
+        accept = live & (flags == 0)
+        first = np.where(failing, j, first)
+        bits = np.where(failing, flags, bits)
+        cur = T._select(accept, new, cur, b, topo)
+        maxima = np.where(accept[:, None], np.maximum(maxima, vals), maxima)
+        for w in range(b.worlds):
+            slot = SLOTS_W[w, j - 1]
+            if slot >= 0 and accept[w]:
+                stored[(slot, w)] = oracle_state(cur)
+        ok = ok & ~failing
+    return cur, first, bits, maxima, stored
+
+
+def test_window_with_per_world_rows_matches_the_oracle(cuda):
+    torch = cuda
+    b, controls = batch()
+    tissue = Tissue(b)
+    dev = torch.device("cuda", tissue.device)
+    table = torch.from_numpy(np.stack([tissue.pack_control(c.membrane, c.junction, c.pump)
+                                       for c in controls])).to(dev)
+    state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    win = windows.vector_window(tissue, state, DT_W, table, HELD_W, slots=SLOTS_W,
+                                counts=COUNTS, first_step=FIRST_W, material_atol=ATOL,
+                                energy_rtol=RTOL, rows=3)
+    torch.cuda.synchronize(dev)
+    cur, first, bits, maxima, stored = oracle_window_each(b, controls)
+    assert np.array_equal(win.first.cpu().numpy(), first)
+    assert np.array_equal(win.bits.cpu().numpy(), bits)
+    assert first[1] > 0 and windows.failure_names(bits[1]) == ("step_refused",)
+    got = tissue.unpack_state(win.state.cpu().numpy())
+    bad = {f: d for f, ref in oracle_state(cur).items()
+           if (d := scaled_difference(got[f], ref)) > 1e-10}
+    assert not bad, bad
+    rows = win.rows.cpu().numpy()
+    topo = T.topology(b)
+    for (slot, w), ref in stored.items():
+        got_row = tissue.unpack_state(rows[slot])
+        cells = topo.cell_world == w
+        for f in ("amount_increment", "membrane_transferred", "pump_cycles"):
+            g, r = np.asarray(got_row[f]), np.asarray(ref[f])
+            assert scaled_difference(g[..., cells], r[..., cells]) <= 1e-10, (slot, w, f)
+    m = win.maxima.cpu().numpy()
+    for k in (6, 10):
+        assert np.all(np.abs(m[:, k] - maxima[:, k]) <= 1e-8 * np.abs(maxima[:, k])), k
