@@ -75,6 +75,9 @@ EXPORTS = (
     "cb_set_channel_block",
     "cb_device_checks",
     "cb_device_checks_each",
+    "cb_copy_worlds",
+    "cb_window_row",
+    "cb_store_worlds",
     "cb_field_bind",
     "cb_field_free",
     "cb_field_state_layout",
@@ -221,6 +224,13 @@ def load(path=LIBRARY):
     lib.cb_device_checks.restype = ctypes.c_int
     lib.cb_device_checks_each.argtypes = [_p, _p, _p, _p, _d, ctypes.c_double, _p, _p, _p]
     lib.cb_device_checks_each.restype = ctypes.c_int
+    lib.cb_copy_worlds.argtypes = [_p, _p, _p, _p, _p]
+    lib.cb_copy_worlds.restype = ctypes.c_int
+    lib.cb_window_row.argtypes = [_p, _p, _p, ctypes.c_int32, _p, ctypes.c_int64, _d,
+                                  ctypes.c_double, _p, _p, _p, _p, _p, _p, _p, _p]
+    lib.cb_window_row.restype = ctypes.c_int
+    lib.cb_store_worlds.argtypes = [_p, _p, _p, _p, _p, ctypes.c_int32, _p]
+    lib.cb_store_worlds.restype = ctypes.c_int
     lib.cb_field_bind.argtypes = [ctypes.POINTER(FieldDesc), ctypes.c_int, ctypes.POINTER(_p)]
     lib.cb_field_bind.restype = ctypes.c_int
     lib.cb_field_free.argtypes = [_p]

@@ -27,6 +27,8 @@ namespace {
 using namespace cbk;
 
 constexpr int kChecksBlock = 256;
+constexpr int kChecksMinBlocks = 4;  // resident CTAs per SM the registers target (64 each)
+constexpr int kFailureShift = 1;  // vector_windows.FAILURE_SHIFT: bit 0 is the refused step
 constexpr double kEps = DBL_EPSILON;
 constexpr double kLedgerStepRounding = 2.5;     // surface_pump.LEDGER_STEP_ROUNDING
 constexpr double kComponentStepRounding = 2.5;  // surface_field.COMPONENT_STEP_ROUNDING
@@ -49,6 +51,19 @@ struct CheckArgs {
   double rounding; // 2.5 eps x accepted steps
   double grounding;  // 2.5 eps x accepted steps (the grounded components' rule)
   const int64_t *steps;  // per-world accepted steps (device [W]), or null: rounding/grounding
+  int64_t step_offset;   // added to steps[w]
+};
+
+// A vector window's per-world bookkeeping of one row (cb_window_row), or row < 0 for none.
+struct WindowRow {
+  int row;                        // 0: the start row; j > 0: the state after slot j
+  const uint32_t *step_status;    // [W] the row's step status (row > 0)
+  const int64_t *counts;          // [W] rows each world takes
+  int32_t *ok;                    // [W] in/out: no failure so far
+  int32_t *first;                 // [W] out: first failing row, -1 if none
+  int64_t *bits;                  // [W] out: its failure bits
+  double *maxima;                 // [W*12] out: diagnostic maxima over accepted rows
+  int32_t *keep;                  // [W] out: 1 where the world stays at its current state
 };
 
 template <int BLOCK>
@@ -63,9 +78,9 @@ __device__ __forceinline__ double block_max(double v, double *red) {
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, kChecksMinBlocks)
     checks_kernel(const Tissue T, const Layout L, const double *__restrict__ prev,
-                  const double *__restrict__ row, const CheckArgs A,
+                  const double *__restrict__ row, const CheckArgs A, const WindowRow R,
                   uint32_t *__restrict__ failed_out, double *__restrict__ values_out) {
   __shared__ double sRed[(BLOCK / 32) * 16];
   __shared__ unsigned int sFail;
@@ -77,9 +92,10 @@ __global__ void __launch_bounds__(BLOCK)
   const double *wc = T.world + (size_t)w * WC_STRIDE;
   // The step-scaled rounding allowances: the call's, or this world's own step count.
   const double rounding =
-      A.steps ? kLedgerStepRounding * kEps * (double)A.steps[w] : A.rounding;
+      A.steps ? kLedgerStepRounding * kEps * (double)(A.steps[w] + A.step_offset) : A.rounding;
   const double grounding =
-      A.steps ? kComponentStepRounding * kEps * (double)A.steps[w] : A.grounding;
+      A.steps ? kComponentStepRounding * kEps * (double)(A.steps[w] + A.step_offset)
+              : A.grounding;
   if (tid == 0) sFail = 0u;
   __syncthreads();
   uint32_t fail = 0;
@@ -253,20 +269,38 @@ __global__ void __launch_bounds__(BLOCK)
   const double res_e = ew - 1e12 * Vb * ec;
   if (bad(res_e, kWorkBound + rounding * (fabs(ew) + 1e12 * fabs(Vb * ec))))
     bits |= 1u << K_ELECTRODE_WORK;
-  failed_out[w] = bits;
-  double *v = values_out + (size_t)w * 12;
-  v[0] = m_local;
-  v[1] = m_out;
-  v[2] = m_tot;
-  v[3] = m_charge;
-  v[4] = fabs(electrode);
-  v[5] = fabs(global);
-  v[6] = fabs(energy);
-  v[7] = fabs(res_w);
-  v[8] = fabs(res_e);
-  v[9] = m_metab;
-  v[10] = fabs(energy) / fmax(flows, kEnergyAtol);
-  v[11] = fabs(global) / glimit;
+  const double v[12] = {m_local,       m_out,          m_tot,         m_charge,
+                        fabs(electrode), fabs(global),   fabs(energy),  fabs(res_w),
+                        fabs(res_e),   m_metab,        fabs(energy) / fmax(flows, kEnergyAtol),
+                        fabs(global) / glimit};
+  if (failed_out) failed_out[w] = bits;
+  if (values_out)
+    for (int k = 0; k < 12; ++k) values_out[(size_t)w * 12 + k] = v[k];
+  if (R.row < 0) return;
+  // The window's row (execution/vector_windows.py:379-404): a refused step is bit 0, failed
+  // checks bits 1 + k; the row counts for a world still live within its own row count.
+  double *mx = R.maxima + (size_t)w * 12;
+  const int64_t flags =
+      (R.row > 0 && R.step_status[w] != 0u) ? 1 : (int64_t)bits << kFailureShift;
+  if (R.row == 0) {
+    const bool ok = flags == 0;
+    R.ok[w] = ok;
+    R.first[w] = ok ? -1 : 0;
+    R.bits[w] = flags;
+    for (int k = 0; k < 12; ++k) mx[k] = ok ? v[k] : 0.0;
+    R.keep[w] = 1;
+    return;
+  }
+  const bool live = R.row <= R.counts[w] && R.ok[w] != 0;
+  const bool failing = live && flags != 0, accept = live && flags == 0;
+  if (failing) {
+    R.first[w] = R.row;
+    R.bits[w] = flags;
+    R.ok[w] = 0;
+  }
+  if (accept)
+    for (int k = 0; k < 12; ++k) mx[k] = fmax(mx[k], v[k]);
+  R.keep[w] = accept ? 0 : 1;
 }
 
 }  // namespace
@@ -285,8 +319,11 @@ extern "C" int cb_device_checks(cb_tissue *t, const double *previous, const doub
   A.rounding = kLedgerStepRounding * kEps * (double)steps;
   A.grounding = kComponentStepRounding * kEps * (double)steps;
   A.steps = nullptr;
+  A.step_offset = 0;
+  WindowRow R{};
+  R.row = -1;
   checks_kernel<kChecksBlock><<<t->W, kChecksBlock, 0, static_cast<cudaStream_t>(stream)>>>(
-      t->t, t->layout, previous, row, A, failed, values);
+      t->t, t->layout, previous, row, A, R, failed, values);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) return cuda_fail(ce, "device checks launch");
   return CB_OK;
@@ -306,9 +343,130 @@ extern "C" int cb_device_checks_each(cb_tissue *t, const double *previous, const
   A.rounding = 0.0;
   A.grounding = 0.0;
   A.steps = steps;
+  A.step_offset = 0;
+  WindowRow R{};
+  R.row = -1;
   checks_kernel<kChecksBlock><<<t->W, kChecksBlock, 0, static_cast<cudaStream_t>(stream)>>>(
-      t->t, t->layout, previous, row, A, failed, values);
+      t->t, t->layout, previous, row, A, R, failed, values);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) return cuda_fail(ce, "device checks launch");
+  return CB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Per-world state copies (cb_copy_worlds): the window's selects, done for the worlds that need
+// them. One CTA per world; a world whose mask entry is zero returns at once.
+
+namespace {
+
+template <int BLOCK>
+__device__ __forceinline__ void copy_world(const Tissue &T, const Layout &L, int w,
+                                           const double *__restrict__ src,
+                                           double *__restrict__ dst) {
+  const int tid = threadIdx.x;
+  const long long C = T.C, E = T.E, W = T.W;
+  const int c0 = T.cell_offset[w], nc = T.cell_offset[w + 1] - c0;
+  const int e0 = T.edge_offset[w], ne = T.edge_offset[w + 1] - e0;
+  const int nch = T.nch;
+  // Cell fields: [reps][C] each.
+  const int cell_field[9] = {CB_AMOUNT_INCREMENT, CB_MEMBRANE_TRANSFERRED, CB_MEMBRANE_DISSIPATED,
+                             CB_PUMP_CYCLES,      CB_PUMP_DISSIPATED,      CB_METABOLIC_WORK,
+                             CB_CHANNEL_GATE,     CB_CHANNEL_TRANSFERRED,  CB_CHANNEL_DISSIPATED};
+  const int cell_reps[9] = {3, 3, 1, 1, 1, 1, 2 * nch, nch, nch};
+  for (int f = 0; f < 9; ++f)
+    for (int r = 0; r < cell_reps[f]; ++r) {
+      const long long base = L.s[cell_field[f]] + (long long)r * C + c0;
+      for (int i = tid; i < nc; i += BLOCK) dst[base + i] = src[base + i];
+    }
+  // Junction fields: [reps][E] each.
+  const int edge_field[3] = {CB_JUNCTION_TRANSFERRED, CB_JUNCTION_DISSIPATED, CB_JUNCTION_GATE};
+  const int edge_reps[3] = {3, 1, 1};
+  for (int f = 0; f < 3; ++f)
+    for (int r = 0; r < edge_reps[f]; ++r) {
+      const long long base = L.s[edge_field[f]] + (long long)r * E + e0;
+      for (int i = tid; i < ne; i += BLOCK) dst[base + i] = src[base + i];
+    }
+  // World fields: [reps][W] each.
+  if (tid < 6) {
+    const int f = tid < 3 ? CB_RESERVOIR_SUPPLIED : CB_ELECTRODE_CHARGE + (tid - 3);
+    const long long at = L.s[f] + (tid < 3 ? (long long)tid * W : 0) + w;
+    dst[at] = src[at];
+  }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+    copy_worlds_kernel(const Tissue T, const Layout L, const int32_t *__restrict__ mask,
+                       const double *__restrict__ src, double *__restrict__ dst) {
+  if (mask[blockIdx.x] == 0) return;
+  copy_world<BLOCK>(T, L, blockIdx.x, src, dst);
+}
+
+// World w's state into stored row slot[w] (rows of `stride` doubles) where keep[w] == 0 and
+// 0 <= slot[w] < n_rows.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+    store_worlds_kernel(const Tissue T, const Layout L, const int32_t *__restrict__ keep,
+                        const int64_t *__restrict__ slot, int n_rows, long long stride,
+                        const double *__restrict__ src, double *__restrict__ rows) {
+  const int w = blockIdx.x;
+  const int64_t s = slot[w];
+  if (keep[w] != 0 || s < 0 || s >= n_rows) return;
+  copy_world<BLOCK>(T, L, w, src, rows + s * stride);
+}
+
+}  // namespace
+
+extern "C" int cb_copy_worlds(cb_tissue *t, const int32_t *mask, const double *src, double *dst,
+                              void *stream) {
+  if (!t || !mask || !src || !dst) return fail(CB_ERR_ARGUMENT, "null argument");
+  if (src == dst) return CB_OK;
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  copy_worlds_kernel<256><<<t->W, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      t->t, t->layout, mask, src, dst);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return cuda_fail(ce, "copy worlds launch");
+  return CB_OK;
+}
+
+extern "C" int cb_window_row(cb_tissue *t, const double *previous, const double *row,
+                             int32_t row_index, const int64_t *first_step, int64_t first_all,
+                             const double *material_atol, double energy_rtol,
+                             const uint32_t *step_status, const int64_t *counts, int32_t *ok,
+                             int32_t *first, int64_t *bits, double *maxima, int32_t *keep,
+                             void *stream) {
+  if (!t || !previous || !row || !material_atol || !counts || !ok || !first || !bits ||
+      !maxima || !keep || (row_index > 0 && !step_status))
+    return fail(CB_ERR_ARGUMENT, "null argument");
+  if (row_index < 0) return fail(CB_ERR_ARGUMENT, "row_index must be non-negative");
+  if (!first_step && first_all < 0) return fail(CB_ERR_ARGUMENT, "steps must be non-negative");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  CheckArgs A;
+  for (int s = 0; s < 3; ++s) A.tol[s] = material_atol[s];
+  A.rtol = energy_rtol;
+  A.rounding = kLedgerStepRounding * kEps * (double)(first_all + row_index);
+  A.grounding = kComponentStepRounding * kEps * (double)(first_all + row_index);
+  A.steps = first_step;
+  A.step_offset = row_index;
+  WindowRow R{row_index, step_status, counts, ok, first, bits, maxima, keep};
+  checks_kernel<kChecksBlock><<<t->W, kChecksBlock, 0, static_cast<cudaStream_t>(stream)>>>(
+      t->t, t->layout, previous, row, A, R, nullptr, nullptr);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return cuda_fail(ce, "window row launch");
+  return CB_OK;
+}
+
+extern "C" int cb_store_worlds(cb_tissue *t, const int32_t *keep, const int64_t *slot,
+                               const double *src, double *rows, int32_t n_rows, void *stream) {
+  if (!t || !keep || !slot || !src || !rows) return fail(CB_ERR_ARGUMENT, "null argument");
+  if (n_rows <= 0) return CB_OK;
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  store_worlds_kernel<256><<<t->W, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      t->t, t->layout, keep, slot, n_rows, t->state_total, src, rows);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return cuda_fail(ce, "store worlds launch");
   return CB_OK;
 }

@@ -269,6 +269,15 @@ class Tissue:
         else:
             _lib.check(self.lib.cb_device_checks(self.handle, *args, int(steps), *tail))
 
+    def copy_worlds(self, mask_dev, src_dev, dst_dev, stream=None):
+        """cb_copy_worlds: every state element of each world with mask_dev[w] != 0 (int32
+        device tensor [W]) from src_dev to dst_dev (packed float64 device states)."""
+        _lib.check(self.lib.cb_copy_worlds(
+            self.handle, ctypes.c_void_p(mask_dev.data_ptr()),
+            ctypes.c_void_p(src_dev.data_ptr()), ctypes.c_void_p(dst_dev.data_ptr()),
+            None if stream is None else ctypes.c_void_p(stream),
+        ))  # fmt: skip
+
     def set_permeability(self, membrane=None, junction=None, channel=None, stream=None):
         """cb_set_permeability from float64 device tensors (m/s): membrane [3, C], junction
         [3, E], channel [NCH, C]; None keeps the bound values."""

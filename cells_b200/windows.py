@@ -17,16 +17,20 @@ As the reference's, each world has its own step size, held-control index and obs
 per row (``[W, width]``; a ``[width]`` row applies to every world) and its own accepted-step count
 at the window start (``first_step``: one number or ``[W]``; cb_device_checks_each). cb_step takes
 one step size per launch, so a row whose worlds take different step sizes runs the step once per
-distinct size and keeps each world's own result. The state stays on the device; the host issues
-two kernels per row (the step, the checks) and a few device selects.
+distinct size and keeps each world's own result. The state stays on the device and a row is
+four launches: the step; the row's checks fused with every world's bookkeeping (cb_window_row);
+the copy back of the worlds that did not advance (cb_copy_worlds, after a buffer swap); and, on a
+row with observation slots, the store of the advanced worlds (cb_store_worlds).
 """
 
 from __future__ import annotations
 
+import ctypes
 from typing import NamedTuple
 
 import numpy as np
 
+from . import _lib
 from . import tissue as _tissue
 
 STEP_REFUSED = "step_refused"
@@ -94,7 +98,10 @@ def vector_window(tissue, state, dt, controls, held, *, slots=None, counts=None,
     stored), [width] or [W, width]; counts: [W] rows each world takes (default: all);
     first_step: accepted steps before the window, one number or [W]; material_atol: per species
     (fmol); energy_rtol; rows: observation slots; method: cb_step's method; world_of: the cached
-    world_of_elements(tissue) as a device tensor.
+    world_of_elements(tissue) as a device tensor (used where a row's worlds take several step
+    sizes). The selects of the reference's window are per-world copies (cb_copy_worlds): the
+    accepted worlds' new rows become current by a buffer swap, the others' states are copied
+    back.
     """
     import torch
 
@@ -111,68 +118,66 @@ def vector_window(tissue, state, dt, controls, held, *, slots=None, counts=None,
     first_t = torch.as_tensor(np.array(np.broadcast_to(np.asarray(first_step, np.int64),
                                                        (n_worlds,))),
                               dtype=torch.int64, device=dev)
-    if world_of is None:
+    if world_of is None and np.any(dt_w != dt_w[:1]):  # only rows of several step sizes use it
         world_of = torch.from_numpy(world_of_elements(tissue)).to(dev)
+    # The per-world row tables on the device once (an upload inside the loop would wait for the
+    # device to drain each row).
+    slots_dev = torch.as_tensor(np.ascontiguousarray(slots_w.T), device=dev)  # [width, W]
+    held_dev = torch.as_tensor(held_w, device=dev)
+    dt_dev = torch.as_tensor(dt_w, device=dev)
     ctl_world = None
     if np.any(held_w != held_w[:1]):
         ctl_world = torch.from_numpy(world_of_controls(tissue)).to(dev)
         ctl_index = torch.arange(controls.shape[1], device=dev)
-    shift = torch.arange(12, dtype=torch.int64, device=dev) + FAILURE_SHIFT
-    failed = torch.zeros(n_worlds, dtype=torch.int32, device=dev)
-    values = torch.zeros(n_worlds * 12, dtype=torch.float64, device=dev)
+    lib = tissue.lib
+    atol = (ctypes.c_double * 3)(*np.broadcast_to(np.asarray(material_atol, float), 3))
+    first_ptr = ctypes.c_void_p(first_t.data_ptr()) if per_world_first else None
+    first_all = 0 if per_world_first else int(first_step)
+    ok = torch.zeros(n_worlds, dtype=torch.int32, device=dev)
+    first = torch.zeros(n_worlds, dtype=torch.int32, device=dev)
+    bits = torch.zeros(n_worlds, dtype=torch.int64, device=dev)
+    maxima = torch.zeros((n_worlds, 12), dtype=torch.float64, device=dev)
+    keep = torch.ones(n_worlds, dtype=torch.int32, device=dev)
     status = torch.zeros(n_worlds, dtype=torch.int32, device=dev)
 
-    def checks(previous, row, offset):
-        steps = first_t + offset if per_world_first else int(first_step) + offset
-        tissue.device_checks(previous, row, steps, material_atol, energy_rtol, failed, values)
-        bits = (failed.to(torch.int64)[:, None] >> torch.arange(12, device=dev)) & 1
-        return (bits << shift).sum(dim=1), values.view(n_worlds, 12).clone()
+    def ptr(x):
+        return ctypes.c_void_p(x.data_ptr())
+
+    def window_row(previous, row, j):
+        """cb_window_row: the row's checks and every world's bookkeeping, one launch."""
+        _lib.check(lib.cb_window_row(
+            tissue.handle, ptr(previous), ptr(row), j, first_ptr, first_all, atol,
+            float(energy_rtol), ptr(status), ptr(counts_t), ptr(ok), ptr(first), ptr(bits),
+            ptr(maxima), ptr(keep), None))  # fmt: skip
 
     current = state.clone()
-    bits, vals = checks(current, current, 0)
-    ok = bits == 0
-    first = torch.where(ok, -1, 0).to(torch.int32)
-    maxima = torch.where(ok[:, None], vals, torch.zeros_like(vals))
+    window_row(current, current, 0)
     stored = torch.zeros((rows, current.numel()), dtype=torch.float64, device=dev)
     updated = torch.empty_like(current)
-    element = torch.arange(current.numel(), device=dev)
     for j in range(1, width + 1):
         col = j - 1
         if ctl_world is None:
             control = controls[int(held_w[0, col])]
         else:
-            held_t = torch.as_tensor(held_w[:, col], device=dev)
-            control = controls[held_t[ctl_world], ctl_index]
+            control = controls[held_dev[:, col][ctl_world], ctl_index]
         sizes = np.unique(dt_w[:, col])
         if sizes.size == 1:
             tissue.step(current, updated, control, float(sizes[0]), 1, status, method=method)
         else:  # one launch per distinct step size, each world keeping its own
             trial = torch.empty_like(current)
             trial_status = torch.empty_like(status)
-            dt_t = torch.as_tensor(dt_w[:, col], device=dev)
+            dt_t = dt_dev[:, col]
             for size in sizes:
                 tissue.step(current, trial, control, float(size), 1, trial_status,
                             method=method)
                 take = dt_t == float(size)
-                updated = torch.where(take[world_of], trial, updated)
-                status = torch.where(take, trial_status, status)
-        row_bits, vals = checks(current, updated, j)
-        flags = torch.where(status == 0, row_bits, torch.ones_like(row_bits))
-        live = (j <= counts_t) & ok
-        failing = live & (flags != 0)
-        accept = live & (flags == 0)
-        first = torch.where(failing, torch.full_like(first, j), first)
-        bits = torch.where(failing, flags, bits)
-        current = torch.where(accept[world_of], updated, current)
-        maxima = torch.where(accept[:, None], torch.maximum(maxima, vals), maxima)
-        slot_col = slots_w[:, col]
-        if np.all(slot_col == slot_col[0]):
-            slot = int(slot_col[0])
-            if 0 <= slot < rows:
-                stored[slot] = torch.where(accept[world_of], current, stored[slot])
-        else:
-            slot_t = torch.as_tensor(slot_col, device=dev)[world_of]
-            keep = accept[world_of] & (slot_t >= 0) & (slot_t < rows)
-            stored[slot_t[keep], element[keep]] = current[keep]
-        ok = ok & ~failing
+                updated.copy_(torch.where(take[world_of], trial, updated))
+                status.copy_(torch.where(take, trial_status, status))
+        window_row(current, updated, j)
+        # The accepted worlds advance: swap the buffers and copy the others' states back.
+        tissue.copy_worlds(keep, current, updated)
+        current, updated = updated, current
+        if rows and np.any((slots_w[:, col] >= 0) & (slots_w[:, col] < rows)):
+            _lib.check(lib.cb_store_worlds(tissue.handle, ptr(keep), ptr(slots_dev[col]),
+                                           ptr(current), ptr(stored), rows, None))
     return Window(current, first, bits, maxima, stored)

@@ -238,6 +238,43 @@ int cb_device_checks_each(cb_tissue *t, const double *previous, const double *ro
                           uint32_t *failed, double *values, void *stream);
 
 /*
+ * Copy every state element of each world w with mask[w] != 0 from src to dst (packed states,
+ * DEVICE pointers; mask DEVICE int32 [W]); other worlds' elements and the layout's padding are
+ * left as they are. One CTA per world, so a copy costs only the masked worlds' bytes. The
+ * vector window's selects (`jnp.where(accept, updated, current)` and the stored rows,
+ * execution/vector_windows.py:393-402) as copies of the worlds that need them.
+ */
+int cb_copy_worlds(cb_tissue *t, const int32_t *mask, const double *src, double *dst,
+                   void *stream);
+
+/*
+ * One row of a vector window (execution/vector_windows.py:379-404) in one launch: the
+ * accepted-row checks of `row` against `previous` (as cb_device_checks, each world at its own
+ * count first_step[w] + row_index, or first_all + row_index where first_step is NULL) and each
+ * world's bookkeeping. Row 0 is the window start (row == previous, step_status unused): ok[w] =
+ * no failure, first[w] = -1 or 0, bits[w] = its failure bits, maxima = its diagnostics (0 where
+ * failing). Row j > 0 (step_status: the row's cb_step status): a world still live (ok[w] and
+ * j <= counts[w]) fails at j with bits = 1 (refused step) or failed << 1 (FAILURE_SHIFT), or is
+ * accepted and raises its maxima; keep[w] = 0 for an accepted world, else 1 (its state stays:
+ * cb_copy_worlds(keep, current, row) then makes `row` the window's next current state).
+ * DEVICE arrays: counts int64 [W], ok int32 [W], first int32 [W], bits int64 [W], maxima
+ * float64 [W*12], keep int32 [W], first_step int64 [W] or NULL.
+ */
+int cb_window_row(cb_tissue *t, const double *previous, const double *row, int32_t row_index,
+                  const int64_t *first_step, int64_t first_all, const double *material_atol,
+                  double energy_rtol, const uint32_t *step_status, const int64_t *counts,
+                  int32_t *ok, int32_t *first, int64_t *bits, double *maxima, int32_t *keep,
+                  void *stream);
+
+/*
+ * Store each world's state from src into observation row slot[w] of `rows` (n_rows rows of the
+ * packed state's length) where keep[w] == 0 and 0 <= slot[w] < n_rows: the window's stored rows
+ * (execution/vector_windows.py:400-402). DEVICE pointers; slot int64 [W].
+ */
+int cb_store_worlds(cb_tissue *t, const int32_t *keep, const int64_t *slot, const double *src,
+                    double *rows, int32_t n_rows, void *stream);
+
+/*
  * cb_step for a handle bound for the packed kernel, with the kernel's scratch (stage
  * accumulators, junction fluxes, world-sum terms, the work-queue counter) taken from a 16 MiB
  * array that the library holds on every GPU it is loaded on, so the call allocates nothing. No

@@ -132,3 +132,28 @@ def test_device_checks_pass_on_device_trajectories(cuda):
         assert not failed.any(), np.argwhere(failed)
         assert np.all(values[:, 10] < 2e-3) and np.all(values[:, 11] <= 1.0)
         prev, done = row, target
+
+
+def test_per_world_step_counts_match_one_count_each(cuda):
+    """cb_device_checks_each at counts [1, 25, 7, 200, 0, 3] gives each world cb_device_checks'
+    bits and diagnostics at that world's count, bit for bit."""
+    torch = cuda
+    b = uneven_batch(52)
+    topo = T.topology(b)
+    prev = T.initial_state(b)
+    row, ok = T.ars222_step(prev, 1e-3, T.full_control(b), b, topo)
+    assert ok.all()
+    tissue = Tissue(b)
+    dev = torch.device("cuda", tissue.device)
+    p = torch.from_numpy(tissue.pack_state(oracle_state(prev))).to(dev)
+    r = torch.from_numpy(tissue.pack_state(oracle_state(row))).to(dev)
+    counts = [1, 25, 7, 200, 0, 3]
+    steps = torch.tensor(counts, dtype=torch.int64, device=dev)
+    failed = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
+    values = torch.zeros(b.worlds * 12, dtype=torch.float64, device=dev)
+    tissue.device_checks(p, r, steps, np.full(3, 2e-11), 2e-3, failed, values)
+    each_f, each_v = failed.clone(), values.clone()
+    for w, n in enumerate(counts):
+        tissue.device_checks(p, r, n, np.full(3, 2e-11), 2e-3, failed, values)
+        assert int(each_f[w]) == int(failed[w])
+        assert torch.equal(each_v[12 * w:12 * w + 12], values[12 * w:12 * w + 12])

@@ -197,3 +197,27 @@ def test_window_with_per_world_rows_matches_the_oracle(cuda):
     m = win.maxima.cpu().numpy()
     for k in (6, 10):
         assert np.all(np.abs(m[:, k] - maxima[:, k]) <= 1e-8 * np.abs(maxima[:, k])), k
+
+
+def test_copy_worlds_is_a_masked_select(cuda):
+    """cb_copy_worlds copies exactly the masked worlds' state elements (channel batch, uneven
+    worlds), bit for bit, and leaves every other element as it was."""
+    torch = cuda
+    rng = np.random.default_rng(8)
+    ws = [worlds.with_channels(worlds.delaunay_world(n, worlds.world_rng(8, k)), rng)
+          for k, n in enumerate((30, 257, 64, 700, 16))]
+    b = worlds.pack(ws)
+    tissue = Tissue(b)
+    dev = torch.device("cuda", tissue.device)
+    n = tissue.state_size
+    src = torch.from_numpy(rng.standard_normal(n)).to(dev)
+    dst = torch.from_numpy(rng.standard_normal(n)).to(dev)
+    mask = torch.tensor([1, 0, 1, 1, 0], dtype=torch.int32, device=dev)
+    real = tissue.pack_state({f: np.ones_like(v, dtype=float)
+                              for f, v in tissue.initial_state().items()}) == 1.0
+    world = windows.world_of_elements(tissue)
+    take = torch.from_numpy(real & mask.cpu().numpy().astype(bool)[world]).to(dev)
+    want = torch.where(take, src, dst)
+    tissue.copy_worlds(mask, src, dst)
+    torch.cuda.synchronize(dev)
+    assert torch.equal(dst, want)
