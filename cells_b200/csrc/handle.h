@@ -67,6 +67,10 @@ struct cb_tissue {
   double *h_state = nullptr, *h_control = nullptr;
   uint32_t *h_status = nullptr;
   int32_t *h_taken = nullptr;
+  // Streams of the host entry point's chunked pipeline (created on first use).
+  cudaStream_t h_streams[4] = {};
+  cudaEvent_t h_event = nullptr;
+  bool h_streams_ready = false;
   // Patch and junction areas (m^2): the permeability prefactors and the adjoint's gradients.
   const double *area = nullptr;   // [C]
   const double *jarea = nullptr;  // [E]

@@ -102,6 +102,10 @@ struct StepCoef {
   double omdelta_dt;
   double delta;         // for the applied reservoir flux
   double omdelta;
+  // The worlds of a launch of the one-world-per-CTA kernel: world0 .. world0 + worlds - 1
+  // (worlds = 0: every world).
+  int world0;
+  int worlds;
 };
 
 template <typename R>
@@ -323,6 +327,8 @@ inline StepCoef step_coef(double dt) {
   // (delta + (1 - delta)) + 0), times dt (surface_pump_v3.py:3700, entity_sum).
   k.frac1_dt = ((gamma + 0.0) + 0.0) * dt;
   k.frac2_dt = ((delta + (1.0 - delta)) + 0.0) * dt;
+  k.world0 = 0;
+  k.worlds = 0;
   return k;
 }
 

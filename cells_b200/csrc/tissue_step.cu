@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   __shared__ double sW[WC_STRIDE];
   __shared__ unsigned int sBits;
 
-  const int w = blockIdx.x;
+  const int w = k.world0 + blockIdx.x;
   const int tid = threadIdx.x;
   const int c0 = T.cell_offset[w], nc = T.cell_offset[w + 1] - c0;
   const int e0 = T.edge_offset[w], ne = T.edge_offset[w + 1] - e0;
@@ -819,7 +819,8 @@ int launch_step(cb_tissue *t, const double *in, double *out, const double *contr
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-  kern<<<t->W, BLOCK, smem, stream>>>(t->t, t->layout, in, out, control, k, n_steps, status,
+  const int grid = k.worlds > 0 ? k.worlds : t->W;
+  kern<<<grid, BLOCK, smem, stream>>>(t->t, t->layout, in, out, control, k, n_steps, status,
                                       taken);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "ars222 launch");
@@ -941,6 +942,103 @@ int launch_packed(cb_tissue *t, const double *in, double *out, const double *con
 }  // namespace
 
 namespace {
+
+// The one-world-per-CTA step over the worlds k.world0 .. k.world0 + k.worlds - 1.
+int launch_shared(cb_tissue *t, const double *in, double *out, const double *control,
+                  const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
+                  cudaStream_t stream, bool mix) {
+  CB_DISPATCH(launch_step, in, out, control, k, n_steps, status, taken, stream, mix);
+}
+
+// The host entry point's pipeline: the worlds in this many chunks, each on a stream of its own,
+// so that one chunk's copies overlap another's steps.
+constexpr int kHostChunks = 4;
+
+// The state elements of worlds wa .. wb-1 between two packed states (one strided copy per
+// field: a field's species or slot rows are C, E or W doubles apart).
+int copy_world_range(const cb_tissue *t, const double *src, double *dst, int wa, int wb,
+                     cudaMemcpyKind kind, cudaStream_t stream) {
+  const long long C = t->C, E = t->E, W = t->W, nch = t->t.nch;
+  const long long ca = t->h_cell_offset[wa], cb = t->h_cell_offset[wb];
+  const long long ea = t->h_edge_offset[wa], eb = t->h_edge_offset[wb];
+  struct Range {
+    int field;
+    long long reps, lo, n, pitch;
+  };
+  const Range ranges[CB_STATE_FIELDS] = {
+      {CB_AMOUNT_INCREMENT, 3, ca, cb - ca, C},     {CB_MEMBRANE_TRANSFERRED, 3, ca, cb - ca, C},
+      {CB_MEMBRANE_DISSIPATED, 1, ca, cb - ca, C},  {CB_PUMP_CYCLES, 1, ca, cb - ca, C},
+      {CB_PUMP_DISSIPATED, 1, ca, cb - ca, C},      {CB_METABOLIC_WORK, 1, ca, cb - ca, C},
+      {CB_JUNCTION_TRANSFERRED, 3, ea, eb - ea, E}, {CB_JUNCTION_DISSIPATED, 1, ea, eb - ea, E},
+      {CB_JUNCTION_GATE, 1, ea, eb - ea, E},        {CB_RESERVOIR_SUPPLIED, 3, wa, wb - wa, W},
+      {CB_ELECTRODE_CHARGE, 1, wa, wb - wa, W},     {CB_RESERVOIR_WORK, 1, wa, wb - wa, W},
+      {CB_ELECTRODE_WORK, 1, wa, wb - wa, W},       {CB_CHANNEL_GATE, 2 * nch, ca, cb - ca, C},
+      {CB_CHANNEL_TRANSFERRED, nch, ca, cb - ca, C}, {CB_CHANNEL_DISSIPATED, nch, ca, cb - ca, C}};
+  for (const Range &r : ranges) {
+    if (r.reps == 0 || r.n == 0) continue;
+    const long long off = t->layout.s[r.field] + r.lo;
+    const size_t pitch = sizeof(double) * (size_t)r.pitch;
+    cudaError_t e = cudaMemcpy2DAsync(dst + off, pitch, src + off, pitch,
+                                      sizeof(double) * (size_t)r.n, (size_t)r.reps, kind, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy2DAsync (world range)");
+  }
+  return CB_OK;
+}
+
+// cb_step_host for the one-world-per-CTA kernel: chunk c's state goes to the device, takes its
+// steps and comes back on stream c, so the copies of one chunk run beside the steps of the
+// others. Every world's arithmetic is that of one launch over all worlds (one CTA per world).
+int step_host_chunked(cb_tissue *t, int method, const double *state_in, double *state_out,
+                      double dt, const double *control, int n_steps, uint32_t *world_status,
+                      int32_t *accepted_steps) {
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
+  if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
+  cudaError_t ce = cudaSuccess;
+  if (!t->h_streams_ready) {
+    for (int c = 0; c < kHostChunks && ce == cudaSuccess; ++c)
+      ce = cudaStreamCreateWithFlags(&t->h_streams[c], cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&t->h_event, cudaEventDisableTiming);
+    if (ce != cudaSuccess) return cuda_fail(ce, "stream creation");
+    t->h_streams_ready = true;
+  }
+  cudaStream_t *st = t->h_streams;
+  int rc = CB_OK;
+  ce = cudaMemcpyAsync(t->h_control, control, sizeof(double) * t->control_total,
+                       cudaMemcpyHostToDevice, st[0]);
+  if (ce == cudaSuccess) ce = cudaEventRecord(t->h_event, st[0]);
+  for (int c = 1; c < kHostChunks && ce == cudaSuccess; ++c)
+    ce = cudaStreamWaitEvent(st[c], t->h_event, 0);
+  if (ce != cudaSuccess) rc = cuda_fail(ce, "control copy");
+  StepCoef k = step_coef(dt);
+  const bool mix = method == CB_METHOD_ARS222_MIXED;
+  for (int c = 0; c < kHostChunks && rc == CB_OK; ++c) {
+    const int wa = (int)((long long)t->W * c / kHostChunks);
+    const int wb = (int)((long long)t->W * (c + 1) / kHostChunks);
+    if (wb == wa) continue;
+    rc = copy_world_range(t, state_in, t->h_state, wa, wb, cudaMemcpyHostToDevice, st[c]);
+    k.world0 = wa;
+    k.worlds = wb - wa;
+    if (!rc)
+      rc = launch_shared(t, t->h_state, t->h_state, t->h_control, k, n_steps, t->h_status,
+                         t->h_taken, st[c], mix);
+    if (!rc) rc = copy_world_range(t, t->h_state, state_out, wa, wb, cudaMemcpyDeviceToHost,
+                                   st[c]);
+    if (!rc) {
+      ce = cudaMemcpyAsync(world_status + wa, t->h_status + wa, sizeof(uint32_t) * (wb - wa),
+                           cudaMemcpyDeviceToHost, st[c]);
+      if (ce == cudaSuccess && accepted_steps)
+        ce = cudaMemcpyAsync(accepted_steps + wa, t->h_taken + wa, sizeof(int32_t) * (wb - wa),
+                             cudaMemcpyDeviceToHost, st[c]);
+      if (ce != cudaSuccess) rc = cuda_fail(ce, "status copy");
+    }
+  }
+  // Every stream drains before the host buffers are handed back, also after an error.
+  for (int c = 0; c < kHostChunks; ++c) {
+    ce = cudaStreamSynchronize(st[c]);
+    if (ce != cudaSuccess && rc == CB_OK) rc = cuda_fail(ce, "cudaStreamSynchronize");
+  }
+  return rc;
+}
 
 int alloc_packed_scratch(cb_tissue *t) {
   if (t->pk.sc) return CB_OK;
@@ -1319,6 +1417,10 @@ void cb_free(cb_tissue *t) {
   if (t->h_status) cudaFree(t->h_status);
   if (t->h_taken) cudaFree(t->h_taken);
   if (t->blk_buf) cudaFree(t->blk_buf);
+  if (t->h_streams_ready) {
+    for (cudaStream_t s : t->h_streams) cudaStreamDestroy(s);
+    cudaEventDestroy(t->h_event);
+  }
   delete t;
 }
 
@@ -1386,6 +1488,10 @@ int cb_step_host(cb_tissue *t, int method, const double *state_in, double *state
     if (ce == cudaSuccess) ce = cudaMalloc(&t->h_taken, sizeof(int32_t) * t->W);
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaMalloc");
   }
+  if (!t->packed && (method == CB_METHOD_ARS222 || method == CB_METHOD_ARS222_MIXED) &&
+      t->W >= 2 * kHostChunks)
+    return step_host_chunked(t, method, state_in, state_out, dt, control, n_steps, world_status,
+                             accepted_steps);
   ce = cudaMemcpy(t->h_state, state_in, sizeof(double) * t->state_total, cudaMemcpyHostToDevice);
   if (ce == cudaSuccess)
     ce = cudaMemcpy(t->h_control, control, sizeof(double) * t->control_total,

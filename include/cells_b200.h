@@ -195,7 +195,13 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
             const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
             void *stream);
 
-/* cb_step with HOST buffers: copies in, steps, copies out, synchronizes (end-to-end call). */
+/*
+ * cb_step with HOST buffers: copies in, steps, copies out, synchronizes (end-to-end call). On the
+ * one-world-per-CTA kernel (ARS(2,2,2), FP64 or mixed, 8 worlds or more) the worlds go in four
+ * chunks on four streams of the handle, so one chunk's copies run beside another's steps; from
+ * pinned host memory the copies then overlap the steps. Results equal cb_step's bit for bit;
+ * the layout's padding in state_out is not written.
+ */
 int cb_step_host(cb_tissue *t, int method, const double *state_in, double *state_out, double dt,
                  const double *control, int n_steps, uint32_t *world_status,
                  int32_t *accepted_steps);

@@ -153,6 +153,38 @@ def test_host_entry_point_equals_device_entry_point(cuda):
         assert np.array_equal(dev[f], host[f]), f
 
 
+@pytest.mark.parametrize("method", [0, 1])
+def test_chunked_host_entry_point_equals_device_entry_point(cuda, method):
+    """cb_step_host on 37 worlds (four uneven chunks on four streams) with NaV1.2 + Kv1.5
+    populations and one world refused (a membrane availability above 1): state, status and
+    accepted steps equal cb_step's bit for bit, FP64 and mixed."""
+    rng = np.random.default_rng(19)
+    ws = [worlds.with_channels(worlds.grid_world(16, 16, worlds.world_rng(19, k)), rng,
+                               sigma=0.3) for k in range(37)]
+    b = worlds.pack(ws)
+    tissue = Tissue(b)
+    membrane = np.ones(b.cells)
+    membrane[b.cell_offset[20] + 5] = 1.3
+    ctl = tissue.pack_control(membrane=membrane)
+    dev = cuda.device("cuda", tissue.device)
+    src = cuda.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    out = cuda.empty_like(src)
+    c = cuda.from_numpy(ctl).to(dev)
+    st = cuda.zeros(b.worlds, dtype=cuda.int32, device=dev)
+    tk = cuda.zeros(b.worlds, dtype=cuda.int32, device=dev)
+    tissue.step(src, out, c, 1e-3, 15, st, tk, method=method)
+    cuda.cuda.synchronize(dev)
+    want = tissue.unpack_state(out.cpu().numpy())
+    got_out, status, taken = tissue.step_host(tissue.pack_state(tissue.initial_state()), ctl,
+                                              1e-3, 15, method=method)
+    got = tissue.unpack_state(got_out)
+    assert np.array_equal(status, st.cpu().numpy().astype(np.uint32))
+    assert np.array_equal(taken, tk.cpu().numpy())
+    assert status[20] != 0 and np.count_nonzero(status) == 1
+    for f in want:
+        assert np.array_equal(want[f], got[f]), f
+
+
 def test_full_size_batched_plain_step_conserves_ledgers(cuda):
     """4096 worlds of 16x16 cells (the batched plain step's full size): every step's ledgers
     within 1e-12 relative (device balances), all worlds accepted."""
