@@ -75,7 +75,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=None,
                     help="untimed bench steps first (default 100; adjoint: 3 gradients)")
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("grid", "uneven", "adjoint", "field"), default="grid")
+    ap.add_argument("--workload", choices=("grid", "uneven", "adjoint", "field"), default="field")
     ap.add_argument("--worlds", type=int, default=None,
                     help="worlds per GPU (default 4096 grid, 1024 uneven, 512 adjoint)")
     ap.add_argument("--cells", type=int, default=1024, help="adjoint: cells per world")
@@ -98,6 +98,8 @@ def parse():
     ap.add_argument("--no-graph", action="store_true",
                     help="issue the timed launches directly instead of replaying a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="field: skip the grid and adjoint sub-records")
     return ap.parse_args()
 
 
@@ -123,18 +125,61 @@ def traffic_per_cell_launch():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clocks, power and throttle reasons sampled DURING the timed region: NVML every 10 ms
+    on a host thread (the device found by its UUID, so CUDA_VISIBLE_DEVICES maps right), else
+    nvidia-smi every 100 ms."""
 
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
+        self.samples = []
+        self.thread = None
         self.proc = None
         self.file = None
+        self.halt = None
+        self.nvml = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+        name = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        return pynvml, pynvml.nvmlDeviceGetHandleByUUID(name)
 
     def start(self):
+        import threading
+
+        try:
+            nvml, handle = self._nvml_handle()
+            self.nvml = (nvml, handle)
+            self.smax = nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM)
+        except Exception:  # noqa: BLE001 - no NVML: the nvidia-smi sampler below
+            self.nvml = None
+        if self.nvml is not None:
+            self.halt = threading.Event()
+
+            def loop():
+                nvml, handle = self.nvml
+                while not self.halt.is_set():
+                    try:
+                        sm = nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)
+                        mask = nvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                        power = nvml.nvmlDeviceGetPowerUsage(handle) / 1e3
+                        self.samples.append((sm, mask, power))
+                    except Exception:  # noqa: BLE001
+                        pass
+                    self.halt.wait(0.01)
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
@@ -145,6 +190,19 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.halt.set()
+            self.thread.join(timeout=5)
+            sm = [x[0] for x in self.samples]
+            reasons = set()
+            for _, mask, _ in self.samples:
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        reasons.add(name)
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": self.smax, "reasons": sorted(reasons), "samples": len(sm),
+                    "power_w_max": max((x[2] for x in self.samples), default=None),
+                    "sampler": "nvml 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -172,6 +230,7 @@ class Clocks:
             "sm_max_mhz": max(smax) if smax else None,
             "reasons": sorted(reasons),
             "samples": len(sm),
+            "sampler": "nvidia-smi 100 ms",
         }
 
 
@@ -246,10 +305,10 @@ def cpu_baseline(args, samples_per_core=2, steps=100):
                        f"cell-steps / ({args.cells} cells x {args.trajectory} steps)"),
         }
     if args.workload == "field":
-        tasks = [("field", w, 7, FIELD_SAMPLE_SIDE, 10, args.dt) for w in range(n)]
+        tasks, stride = field_tasks(args, n, 10)
         cell_steps, wall, procs = cb.measure(tasks, cores, fn=cb.run_field_world)
         return {"value": cell_steps / wall, "unit": UNIT, "cores": procs, "kind": "port",
-                "sample": field_sample(n, 10, wall)}
+                "sample": field_sample(args, n, stride, 10, wall)}
     if args.workload == "uneven":
         steps = max(2, steps // 10)
     tasks, stride = sample_tasks(args, n, steps)
@@ -264,15 +323,20 @@ def cpu_baseline(args, samples_per_core=2, steps=100):
     }
 
 
-FIELD_SAMPLE_SIDE = 24
+def field_tasks(args, n, steps):
+    """A strided sample of n of the field workload's own worlds (same seed, ids and shape) as
+    CPU tasks."""
+    stride = max(1, args.worlds // n)
+    shape = (args.side, args.field_cells, 3)
+    return [("field", w * stride, 7, shape, steps, args.dt) for w in range(n)], stride
 
 
-def field_sample(n, steps, wall=None):
-    text = (f"{n} field worlds of a {FIELD_SAMPLE_SIDE}x{FIELD_SAMPLE_SIDE} grid with a 6x6 "
-            f"tissue (the same laws), {steps} ARS(2,2,2) steps each, one world per process, "
-            "1 BLAS thread: the reference's field solver is dense in the floating offsets (a "
-            "15876 x 15876 solve per Newton iteration on the 128x128 grid), so the CPU sample "
-            "runs the largest grid of its golden runs; world·cell-steps/s of that world")
+def field_sample(args, n, stride, steps, wall=None):
+    text = (f"{n} of the {args.worlds} field worlds (every {stride}th; {args.side}x{args.side} "
+            f"grid, {args.field_cells ** 2} cells), {steps} ARS(2,2,2) steps each, one world per "
+            "process, 1 BLAS thread: the field oracle's restatement of the reference's step in "
+            "sparse containers (the reference's own dense offset solve would be a 15876 x 15876 "
+            "LU per Newton iteration at this grid; its sparse field bind refuses the grid)")
     return text + (f", {wall:.1f} s wall" if wall is not None else "")
 
 
@@ -290,9 +354,8 @@ def run_reference(args, rank):
     per_task = 10 if args.workload == "grid" else 3 if adjoint else 1
     fn = cb.run_adjoint_world if adjoint else cb.run_field_world if field else cb.run_world
     if field:
-        per_task = 2
-        tasks, stride = [("field", w, 7, FIELD_SAMPLE_SIDE, per_task, args.dt)
-                         for w in range(n)], 1
+        per_task = 1
+        tasks, stride = field_tasks(args, n, per_task)
     else:
         tasks, stride = sample_tasks(args, n, per_task)
     with cb.pool(cores) as pool:
@@ -315,7 +378,7 @@ def run_reference(args, rank):
                   "process, 1 BLAS thread (the reference has no adjoint; its gradients would "
                   "come from jax.grad, and jax is not installed)")
     elif field:
-        sample = field_sample(n, per_task) + " (per bench step)"
+        sample = field_sample(args, n, stride, per_task) + " (per bench step)"
     else:
         sample = (f"{n} of the {args.worlds} worlds (every {stride}th) advanced {per_task} "
                   "ARS(2,2,2) steps per bench step, one world per process, 1 BLAS thread")
@@ -536,25 +599,38 @@ def run_adjoint(args, rank, world_size, local_rank, dist, base):
         }
         if base is not None:
             line["cpu_baseline"] = base
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
     tissue.close()
-    return 0
+    return line if rank == 0 else None
 
 
-def field_bytes_per_world_step(tissue, info, solves=6):
-    """Algorithmic bytes per world per step of the field step: the state read and written once,
-    the parameters read once (per cell 11 doubles, per junction 5, per node 6, per face 3), each
-    of the step's two factors written once and read by both passes of each of its solves (the
-    start field's initial solve and chord corrections, the two stage solves: six on the
-    benchmark's worlds), and each factorisation's update matrices written and read once."""
+def field_bytes_per_world_step(tissue, info, factorisations=2, solve_reads=0):
+    """Algorithmic bytes per world per step of the field step, by the minimal-traffic count: the
+    state read and written once, the parameters read once (per cell 11 doubles, per junction 5,
+    per node 6, per face 3), and each factorisation's factor written once and read once
+    (factor_doubles each way). solve_reads > 0 adds that many further reads of the factor (both
+    sweeps of every solve re-read it: 2 x solves), the count that charges every pass."""
     state = tissue.state_total // tissue.W
     params = 11 * tissue.N + 5 * tissue.E + 6 * tissue.O + 3 * tissue.F
-    factor = info["factor_doubles"] * (2 + 2 * solves)
-    updates = 2 * 2 * info["update_doubles"]
-    return 8 * (2 * state + params + factor + updates)
+    factor = info["factor_doubles"] * (2 * factorisations + solve_reads)
+    return 8 * (2 * state + params + factor)
+
+
+_FP64_PEAK = {}
+
+
+def fp64_peak(device):
+    """The device's FP64 FMA rate (FLOP/s, cb_probe_fp64: independent FMA chains on every SM,
+    CUDA events), measured once per process."""
+    if device not in _FP64_PEAK:
+        import ctypes
+
+        from cells_b200 import _lib
+
+        lib = _lib.load()
+        rate, ms = ctypes.c_double(), ctypes.c_double()
+        _lib.check(lib.cb_probe_fp64(device, 1 << 18, ctypes.byref(rate), ctypes.byref(ms)))
+        _FP64_PEAK[device] = (rate.value, ms.value)
+    return _FP64_PEAK[device]
 
 
 def field_traffic_per_world_step():
@@ -602,12 +678,15 @@ def run_field(args, rank, world_size, local_rank, dist, base):
     clocks = Clocks(local_rank)
     clocks.start()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches = 0
+    launches = factorisations = solves = 0
     start.record(stream)
     for _ in range(args.steps):
         tissue.step(state, state, control, args.dt, 1, status, taken,
                     stream=stream.cuda_stream)
-        launches += tissue.launches()
+        c = tissue.counts()
+        launches += c["launches"]
+        factorisations += c["factorisations"]
+        solves += c["solves"]
     stop.record(stream)
     torch.cuda.synchronize(dev)
     clock = clocks.stop()
@@ -621,9 +700,15 @@ def run_field(args, rank, world_size, local_rank, dist, base):
         ms_max = float(t.item())
     value = cells * world_size * args.steps / (ms_max * 1e-3)
     launch_ms = ms / args.steps
-    alg = field_bytes_per_world_step(tissue, info) * tissue.W
+    fact_per_step, solves_per_step = factorisations / args.steps, solves / args.steps
+    alg = field_bytes_per_world_step(tissue, info, fact_per_step) * tissue.W
+    alg_all = field_bytes_per_world_step(tissue, info, fact_per_step,
+                                         2 * solves_per_step) * tissue.W
     achieved = alg / (launch_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
+    fl = tissue.flops()
+    step_flops = (fact_per_step * fl["factor"] + solves_per_step * fl["solve"]) * tissue.W
+    fp64_rate, fp64_ms = fp64_peak(local_rank)
     # End to end through the C ABI with host buffers (cb_field_step_host on packed, pinned host
     # buffers: the state and control copied in, one step, the state and status copied out, every
     # call).
@@ -674,6 +759,22 @@ def run_field(args, rank, world_size, local_rank, dist, base):
                 "traffic_note": "DRAM bytes of one step of 32 worlds (ncu), scaled per world",
                 "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms,
                 "bytes_per_world_step": alg / tissue.W,
+                "count": ("minimal traffic: state read and written once, parameters read once, "
+                          "each factorisation's factor written once and read once"),
+                "achieved_every_pass": alg_all / (launch_ms * 1e-3) / 1e9,
+                "frac_every_pass": alg_all / (launch_ms * 1e-3) / 1e9 / peak,
+                "every_pass_note": ("the same with the factor re-read by both sweeps of each "
+                                    f"solve ({solves_per_step:g} solves per step)"),
+            },
+            "fp64": {
+                "peak_tflops": fp64_rate / 1e12, "peak_kind": "measured (cb_probe_fp64)",
+                "probe_ms": fp64_ms,
+                "achieved_tflops": step_flops / (launch_ms * 1e-3) / 1e12,
+                "frac": step_flops / (launch_ms * 1e-3) / fp64_rate,
+                "flops_per_world_step": step_flops / tissue.W,
+                "note": ("factorisation and substitution arithmetic of the plan only (FMA = 2), "
+                         f"{fact_per_step:g} factorisations and {solves_per_step:g} solves per "
+                         "step; the per-world phases' arithmetic is not counted"),
             },
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": 8 * (tissue.state_total + tissue.control_total),
@@ -685,59 +786,17 @@ def run_field(args, rank, world_size, local_rank, dist, base):
         }
         if base is not None:
             line["cpu_baseline"] = base
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    return 0
+    return line if rank == 0 else None
 
 
-def main():
-    args = parse()
-    adjoint = args.workload == "adjoint"
-    field = args.workload == "field"
-    if args.worlds is None:
-        args.worlds = {"uneven": 1024, "adjoint": 512, "field": 256}.get(args.workload, 4096)
-    if args.side is None:
-        args.side = 128 if field else 16
-    if args.dt is None:
-        args.dt = 5e-4 if field else 1e-3
-    if args.steps is None:
-        args.steps = 3 if adjoint else 10 if field else 1000
-    if args.warmup is None:
-        args.warmup = 3 if adjoint or field else 100
-    if args.e2e_calls is None:
-        args.e2e_calls = 1 if adjoint else 2 if field else 3
-    rank = int(os.environ.get("RANK", "0"))
-    world_size = int(os.environ.get("WORLD_SIZE", "1"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        return run_reference(args, rank)
-
-    # The CPU baseline pool is spawned before any CUDA call.
-    base = None
-    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(args)
-
+def run_grid(args, rank, world_size, local_rank, dist, base):
+    """The held-bath workloads (grid, uneven): each bench step is one time step of every world,
+    the timed launches replayed from one CUDA graph."""
     import torch
 
     from cells_b200.tissue import Tissue
 
-    dist = None
-    if world_size > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    if adjoint:
-        return run_adjoint(args, rank, world_size, local_rank, dist, base)
-    if field:
-        return run_field(args, rank, world_size, local_rank, dist, base)
-
     from cells_b200 import _lib as _lib_methods
 
     if args.method == "n2":
@@ -891,13 +950,82 @@ def main():
         }
         if base is not None:
             line["cpu_baseline"] = base
-        print(json.dumps(line), flush=True)
     del graph
+    tissue.close()
+    return line if rank == 0 else None
+
+
+
+
+def main():
+    args = parse()
+    adjoint = args.workload == "adjoint"
+    field = args.workload == "field"
+    if args.worlds is None:
+        args.worlds = {"uneven": 1024, "adjoint": 512, "field": 256}.get(args.workload, 4096)
+    if args.side is None:
+        args.side = 128 if field else 16
+    if args.dt is None:
+        args.dt = 5e-4 if field else 1e-3
+    if args.steps is None:
+        args.steps = 3 if adjoint else 10 if field else 1000
+    if args.warmup is None:
+        args.warmup = 3 if adjoint or field else 100
+    if args.e2e_calls is None:
+        args.e2e_calls = 1 if adjoint else 2 if field else 3
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    # The CPU baseline pool is spawned before any CUDA call.
+    base = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(args)
+
+    import torch
+
+    from cells_b200.tissue import Tissue
+
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    runner = run_adjoint if adjoint else run_field if field else run_grid
+    line = runner(args, rank, world_size, local_rank, dist, base)
+    if field and not args.no_sub:
+        # The metric's other two numbers, measured in the same run: the batched plain step on
+        # 4096 16x16-grid worlds, and adjoint world-gradients/s on 512 1024-cell Delaunay worlds.
+        subs = {}
+        for name, kw in (("grid", dict(workload="grid", worlds=4096, side=16, dt=1e-3,
+                                       steps=200, warmup=100, e2e_calls=1, fuse=100)),
+                         ("adjoint", dict(workload="adjoint", worlds=512, dt=1e-3, steps=1,
+                                          warmup=1, e2e_calls=0))):
+            sub = argparse.Namespace(**{**vars(args), **kw})
+            fn = run_adjoint if name == "adjoint" else run_grid
+            subs[name] = fn(sub, rank, world_size, local_rank, dist, None)
+        if line is not None:
+            line["sub_records"] = {k: sub_record(v) for k, v in subs.items()}
+    if line is not None:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
-    tissue.close()
     return 0
+
+
+def sub_record(line):
+    """The keys of a workload's line that a sub-record keeps."""
+    keep = ("metric", "value", "unit", "ms_per_step", "dtype", "config", "roofline", "e2e",
+            "gpu_launches", "refused_worlds", "clocks", "kernels")
+    return {k: line[k] for k in keep if k in line}
 
 
 if __name__ == "__main__":

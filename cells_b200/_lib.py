@@ -84,8 +84,12 @@ EXPORTS = (
     "cb_field_control_length",
     "cb_field_info",
     "cb_field_launches",
+    "cb_field_levels",
+    "cb_field_counts",
+    "cb_field_flops",
     "cb_field_step",
     "cb_field_step_host",
+    "cb_probe_fp64",
     "cb_last_error",
     "cb_version",
 )
@@ -239,6 +243,12 @@ def load(path=LIBRARY):
     lib.cb_field_state_layout.restype = ctypes.c_int
     lib.cb_field_launches.argtypes = [_p]
     lib.cb_field_launches.restype = ctypes.c_int64
+    lib.cb_field_counts.argtypes = [_p, _i64]
+    lib.cb_field_counts.restype = ctypes.c_int
+    lib.cb_field_flops.argtypes = [_p, _d]
+    lib.cb_field_flops.restype = ctypes.c_int
+    lib.cb_field_levels.argtypes = [_p, _i32, ctypes.c_int32]
+    lib.cb_field_levels.restype = ctypes.c_int32
     lib.cb_field_info.argtypes = [_p, _i64]
     lib.cb_field_info.restype = ctypes.c_int
     lib.cb_field_control_length.argtypes = [_p]
@@ -248,6 +258,8 @@ def load(path=LIBRARY):
     lib.cb_field_step_host.argtypes = [_p, _d, _d, ctypes.c_double, _d, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_uint32), _i32]
     lib.cb_field_step_host.restype = ctypes.c_int
+    lib.cb_probe_fp64.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d]
+    lib.cb_probe_fp64.restype = ctypes.c_int
     lib.cb_last_error.argtypes = []
     lib.cb_last_error.restype = ctypes.c_char_p
     lib.cb_version.argtypes = []

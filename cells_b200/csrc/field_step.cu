@@ -1128,7 +1128,9 @@ struct cb_field {
   // Levels of the fronts (host copies): first entry in lv_sn, one warp per front, the largest
   // block (m x s) and front rows.
   std::vector<int> lv_ptr, lv_warp, lv_block, lv_m;
+  double factor_flops = 0.0, solve_flops = 0.0;  // per world: one factorisation, one solve
   long long launches = 0;   // kernels launched by the last cb_field_step
+  long long solves = 0, factorisations = 0;  // ... and the solves and factorisations it ran
   double *host_state = nullptr, *host_control = nullptr;  // cb_field_step_host's device copies
   uint32_t *host_status = nullptr;
   int32_t *host_taken = nullptr;
@@ -1421,6 +1423,18 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
   }
   if (f->smem_doubles * (long long)sizeof(double) > kMaxSmemBytes)
     return bail(fail(CB_ERR_UNSUPPORTED, "field: a front exceeds shared memory"));
+  // Arithmetic of the plan per world (FMA = 2 flops): the panel's scaling and right-looking
+  // update, the update matrix (packed lower triangle), and one FMA per factor entry each way of a
+  // solve.
+  for (int q = 0; q < sp.count; ++q) {
+    const double sq = sp.s[q], mq = sp.m[q], bq = mq - sq;
+    for (int k = 0; k < sp.s[q]; ++k) {
+      f->factor_flops += mq - k - 1;
+      for (int j = k + 1; j < sp.s[q]; ++j) f->factor_flops += 2.0 * (mq - j);
+    }
+    f->factor_flops += bq * (bq + 1.0) * sq;
+    f->solve_flops += 4.0 * (mq * sq - sq * (sq - 1.0) / 2.0);
+  }
   f->levels = sp.levels;
   f->supernodes = sp.count;
   f->lsize = sp.lsize, f->usize = sp.usize, f->vsize = sp.vsize;
@@ -1609,7 +1623,28 @@ extern "C" int cb_field_info(const cb_field *f, int64_t info[8]) {
   return CB_OK;
 }
 
+extern "C" int cb_field_flops(const cb_field *f, double out[2]) {
+  if (!f || !out) return fail(CB_ERR_ARGUMENT, "null argument");
+  out[0] = f->factor_flops;
+  out[1] = f->solve_flops;
+  return CB_OK;
+}
+
+extern "C" int32_t cb_field_levels(const cb_field *f, int32_t *kinds, int32_t capacity) {
+  if (!f) return fail(CB_ERR_ARGUMENT, "null argument"), -1;
+  for (int l = 0; l < f->levels && kinds && l < capacity; ++l) kinds[l] = f->lv_warp[l] ? 0 : 1;
+  return f->levels;
+}
+
 extern "C" int64_t cb_field_launches(const cb_field *f) { return f ? f->launches : -1; }
+
+extern "C" int cb_field_counts(const cb_field *f, int64_t out[3]) {
+  if (!f || !out) return fail(CB_ERR_ARGUMENT, "null argument");
+  out[0] = f->launches;
+  out[1] = f->factorisations;
+  out[2] = f->solves;
+  return CB_OK;
+}
 
 extern "C" int64_t cb_field_control_length(const cb_field *f) {
   if (!f) return -1;
@@ -1640,6 +1675,8 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
   const Scratch &S = f->scratch;
   double *sc = f->scratch_buf;
   f->launches = 0;
+  f->solves = 0;
+  f->factorisations = 0;
   auto phase = [&](int ph, int first) {
     ++f->launches;
     auto go = [&](auto kernel) {
@@ -1671,6 +1708,7 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
     return cudaGetLastError();
   };
   auto factor = [&](int kind) {
+    ++f->factorisations;
     for (int l = 0; l < f->levels; ++l) {
       ce = level_launch(
           l,
@@ -1688,6 +1726,7 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
     return cudaSuccess;
   };
   auto solve = [&](long long out_off) {
+    ++f->solves;
     for (int l = 0; l < f->levels; ++l) {
       ce = level_launch(
           l,

@@ -995,10 +995,15 @@ int step_host_chunked(cb_tissue *t, int method, const double *state_in, double *
   if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
   cudaError_t ce = cudaSuccess;
   if (!t->h_streams_ready) {
-    for (int c = 0; c < kHostChunks && ce == cudaSuccess; ++c)
-      ce = cudaStreamCreateWithFlags(&t->h_streams[c], cudaStreamNonBlocking);
+    int made = 0;
+    for (; made < kHostChunks && ce == cudaSuccess; ++made)
+      ce = cudaStreamCreateWithFlags(&t->h_streams[made], cudaStreamNonBlocking);
+    if (ce != cudaSuccess) --made;  // the failed creation made nothing
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&t->h_event, cudaEventDisableTiming);
-    if (ce != cudaSuccess) return cuda_fail(ce, "stream creation");
+    if (ce != cudaSuccess) {  // release what was made, so a later call starts clean
+      for (int c = 0; c < made; ++c) cudaStreamDestroy(t->h_streams[c]);
+      return cuda_fail(ce, "stream creation");
+    }
     t->h_streams_ready = true;
   }
   cudaStream_t *st = t->h_streams;
@@ -1051,6 +1056,9 @@ int alloc_packed_scratch(cb_tissue *t) {
 }
 
 }  // namespace
+
+// cb_step_packed_static's array address on `device` (defined with the array below).
+int static_scratch(int device, double **out, bool refresh);
 
 extern "C" {
 
@@ -1234,6 +1242,7 @@ int cb_bind(const cb_tissue_desc *d, int device, cb_tissue **out) {
 
   cudaError_t ce = cudaSetDevice(device);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  if (int rc0 = static_scratch(device, nullptr, true)) return rc0;
   cb_tissue *t = new cb_tissue();
   t->device = device;
   t->W = W;
@@ -1630,21 +1639,28 @@ constexpr int kStaticMaxDevices = 64;
 double *g_static_ptr[kStaticMaxDevices] = {};
 std::mutex g_static_mutex;
 
+}  // namespace
+
 // The device address of g_static_scratch on the current device (host code may not use the
-// symbol itself: on the host it names a stand-in, not device memory). Looked up once per device.
-int static_scratch(int device, double **out) {
+// symbol itself: on the host it names a stand-in, not device memory). Looked up again at every
+// bind on the device (refresh), so a context rebuilt after cudaDeviceReset, whose handles must
+// be bound anew, never sees a stale address; otherwise once per device.
+int static_scratch(int device, double **out, bool refresh) {
   if (device < 0 || device >= kStaticMaxDevices)
-    return fail(CB_ERR_UNSUPPORTED, "device ordinal beyond the static scratch table");
+    return out ? fail(CB_ERR_UNSUPPORTED, "device ordinal beyond the static scratch table")
+               : CB_OK;
   std::lock_guard<std::mutex> lock(g_static_mutex);
-  if (!g_static_ptr[device]) {
+  if (refresh || !g_static_ptr[device]) {
     void *ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
     g_static_ptr[device] = static_cast<double *>(ptr);
   }
-  *out = g_static_ptr[device];
+  if (out) *out = g_static_ptr[device];
   return CB_OK;
 }
+
+namespace {
 
 template <int BLOCK, int NCH, bool BLK = false>
 int launch_packed_with(cb_tissue *t, const Packed &P, const double *in, double *out,
@@ -1688,7 +1704,7 @@ extern "C" int cb_step_packed_static(cb_tissue *t, const double *state_in, doubl
   cudaError_t ce = cudaSetDevice(t->device);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
   double *base = nullptr;
-  int rc = static_scratch(t->device, &base);
+  int rc = static_scratch(t->device, &base, false);
   if (rc) return rc;
   Packed P = t->pk;
   P.queue = reinterpret_cast<unsigned int *>(base);

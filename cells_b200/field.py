@@ -120,6 +120,28 @@ class FieldTissue:
                 "vector_doubles", "smem_bytes", "scratch_bytes")
         return dict(zip(keys, (int(v) for v in out), strict=True))
 
+    def counts(self):
+        """cb_field_counts: the last step call's launches, factorisations and solves."""
+        out = (ctypes.c_int64 * 3)()
+        _lib.check(self.lib.cb_field_counts(self.handle, out))
+        return {"launches": int(out[0]), "factorisations": int(out[1]), "solves": int(out[2])}
+
+    def flops(self):
+        """cb_field_flops: per world, the flops of one factorisation and of one solve."""
+        out = (ctypes.c_double * 2)()
+        _lib.check(self.lib.cb_field_flops(self.handle, out))
+        return {"factor": float(out[0]), "solve": float(out[1])}
+
+    def level_kinds(self):
+        """cb_field_levels: per level of the factor plan (leaves first), 0 when its fronts go one
+        per warp, 1 when one per CTA (the separators' group kernels)."""
+        n = int(self.lib.cb_field_levels(self.handle, None, 0))
+        if n < 0:
+            raise RuntimeError("cb_field_levels: null handle")
+        out = (ctypes.c_int32 * max(n, 1))()
+        self.lib.cb_field_levels(self.handle, out, n)
+        return [int(v) for v in out[:n]]
+
     def launches(self):
         """Kernels launched by the last step call (cb_field_launches)."""
         return int(self.lib.cb_field_launches(self.handle))

@@ -281,17 +281,20 @@ int cb_store_worlds(cb_tissue *t, const int32_t *keep, const int64_t *slot, cons
                     double *rows, int32_t n_rows, void *stream);
 
 /*
- * cb_step for a handle bound for the packed kernel, with the kernel's scratch (stage
+ * cb_step with method CB_METHOD_ARS222 (the FP64 ARS(2,2,2) step; there is no method argument)
+ * for a handle bound for the packed kernel, with the kernel's per-call scratch (stage
  * accumulators, junction fluxes, world-sum terms, the work-queue counter) taken from a 16 MiB
  * array that the library holds on every GPU it is loaded on, so the call allocates nothing. No
  * counterpart in the reference: it exists for callers that may not allocate device memory
- * while a step runs, such as a plugin inside a host runtime (an XLA/JAX custom call, a captured
- * CUDA graph) that hands it only its input and output buffers, or a process whose device memory
- * another allocator has already reserved. A batch needs (26 + 12 NCH) C + 9 E doubles of
- * scratch and must fit 2^21 - 32 doubles; a larger batch is refused (CB_ERR_UNSUPPORTED) and
- * should use cb_step. The first call on a device looks up the array's device address; make that
- * call before any stream capture. Every call shares the array: calls whose kernels overlap on a
- * GPU race and must be serialised by the caller. DEVICE pointers, as cb_step.
+ * while a step runs, such as a plugin inside a host runtime (an XLA/JAX custom call) that hands
+ * it only its input and output buffers, or a process whose device memory another allocator has
+ * already reserved. It saves no memory: the handle still holds what cb_bind allocated. A batch
+ * needs (26 + 12 NCH) C + 9 E doubles of scratch and must fit 2^21 - 32 doubles; a larger batch
+ * is refused (CB_ERR_UNSUPPORTED) and should use cb_step. The array's device address is looked
+ * up whenever a handle is bound on the device, and by the first call on a device if no bind
+ * has; make that first call before any stream capture. Every call shares the array, which keeps
+ * the last call's contents: calls whose kernels overlap on a GPU race and must be serialised by
+ * the caller. DEVICE pointers, as cb_step.
  */
 int cb_step_packed_static(cb_tissue *t, const double *state_in, double *state_out, double dt,
                           const double *control, int n_steps, uint32_t *world_status,
@@ -357,6 +360,12 @@ int cb_set_permeability(cb_tissue *t, const double *membrane, const double *junc
 int cb_set_channel_block(cb_tissue *t, int32_t modes, const double *weight,
                          const double *k0_mM, const double *steepness,
                          const double *concentration_mM);
+
+/* The device's FP64 fused multiply-add rate (FLOP/s), measured by one launch of independent FMA
+ * chains over every SM (iterations rounds per thread, CUDA events around it; ms its duration):
+ * the denominator of an FP64-pipe fraction. No counterpart in the reference. Allocates and
+ * synchronizes: a measurement call, not for a step's path. */
+int cb_probe_fp64(int device, int64_t iterations, double *flops_per_second, double *milliseconds);
 
 /* Message of the last error on this thread. */
 const char *cb_last_error(void);
@@ -431,6 +440,15 @@ int cb_field_state_layout(const cb_field *f, int64_t offsets[CB_FIELD_STATE_FIEL
  * levels, [3] factor doubles per world, [4] update-matrix doubles per world, [5] update-vector
  * doubles per world, [6] shared memory bytes per CTA, [7] scratch bytes (all worlds). */
 int cb_field_info(const cb_field *f, int64_t info[8]);
+/* Arithmetic of the bound plan per world (an FMA counts 2): out[0] flops of one factorisation
+ * (panels and update matrices), out[1] of one solve (forward and back substitution). */
+int cb_field_flops(const cb_field *f, double out[2]);
+/* The factor plan's levels (leaves first): kinds[l] (l < capacity; kinds may be NULL) = 0 when
+ * level l's fronts go one per warp (factor_warps, forward_warps, backward_warps), 1 when one per
+ * CTA (factor_group, forward_group, backward_group: separators whose front block exceeds 1280
+ * doubles or whose front has more than 256 rows). Returns the number of levels (-1: null
+ * handle). */
+int32_t cb_field_levels(const cb_field *f, int32_t *kinds, int32_t capacity);
 /* Control: membrane [W*N], junction [W*E], pump [W*N] availabilities, back to back. */
 int64_t cb_field_control_length(const cb_field *f);
 /* n_steps ARS(2,2,2) steps of every world (checked_step repeated; a refused world keeps its
@@ -443,6 +461,9 @@ int cb_field_step(cb_field *f, const double *state_in, double *state_out, double
                   int32_t *accepted_steps, void *stream);
 /* Kernels launched by the handle's last cb_field_step call. */
 int64_t cb_field_launches(const cb_field *f);
+/* The handle's last cb_field_step call: out[0] kernels launched, out[1] factorisations (every
+ * world's, counted once per level sweep), out[2] solves (forward and back sweeps). */
+int cb_field_counts(const cb_field *f, int64_t out[3]);
 /* cb_field_step with HOST buffers: copies in, steps, copies out, synchronizes. The device copies
  * are allocated by the handle's first host call and kept until cb_field_free. */
 int cb_field_step_host(cb_field *f, const double *state_in, double *state_out, double dt,

@@ -59,22 +59,20 @@ def run_world(task):
     return b.cells * steps, elapsed
 
 
-FIELD_CELLS_SIDE, FIELD_STRIDE = 6, 3  # the sampled field world: a 6 x 6 tissue, stride 3
-
-
 def run_field_world(task):
-    """("field", world index, seed, grid side, steps, dt) -> (cell-steps, seconds): the field
-    oracle's ARS(2,2,2) step (the reference's face-electromigration step with its dense factored
-    field, bit for bit) on one field world."""
+    """("field", world index, seed, (grid side, tissue side, stride), steps, dt) -> (cell-steps,
+    seconds): the field oracle's ARS(2,2,2) step (the reference's face-electromigration step;
+    dense node-space algebra on small grids, the same algebra in sparse containers on larger
+    ones) on one field world of that shape."""
     _pin_blas()
     from cells_b200 import field_worlds, worlds
     from oracle import field as OF
 
-    kind, w, seed, side, steps, dt = task
-    key = (kind, w, seed, side)
+    kind, w, seed, shape, steps, dt = task
+    key = (kind, w, seed, tuple(shape))
     if key not in _WORLDS:
-        world = field_worlds.field_world(side, FIELD_CELLS_SIDE, FIELD_STRIDE,
-                                         worlds.world_rng(seed, w))
+        side, cells_side, stride = shape
+        world = field_worlds.field_world(side, cells_side, stride, worlds.world_rng(seed, w))
         _WORLDS[key] = [world, OF.bind(world), OF.full_control(world), OF.initial_state(world)]
     entry = _WORLDS[key]
     world, tp, ctl, st = entry

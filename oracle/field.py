@@ -103,8 +103,20 @@ def full_control(w):
     return Control(np.ones(w.cells), np.ones(w.edges), np.ones(w.cells))
 
 
-def bind(w):
-    """surface_field.bind (:253-361) for a world with no gauge and every node active."""
+SPARSE_ABOVE = 3000  # node-space size above which bind(w) takes the sparse containers
+
+
+def bind(w, sparse=None):
+    """surface_field.bind (:253-361) for a world with no gauge and every node active.
+
+    sparse (default: node space above SPARSE_ABOVE): the same algebra in scipy.sparse containers
+    with sparse LU solves (``_bind_sparse``), for grids whose dense node-space matrices do not fit
+    (the 128x128 benchmark grid: 17,408 nodes, 16,4xx floating offsets). Dense is the branch
+    pinned bit for bit to the reference; sparse agrees with it to rounding (tests)."""
+    if sparse is None:
+        sparse = w.cells + w.nodes > SPARSE_ABOVE
+    if sparse:
+        return _bind_sparse(w)
     n, o = w.cells, w.nodes
     size = n + o
     parent = list(range(size))
@@ -152,19 +164,112 @@ def bind(w):
     )  # fmt: skip
 
 
+def _bind_sparse(w):
+    """bind's reduction with scipy.sparse containers: the same components (a cell joins its
+    node's; each other node is its own), representatives, clamps and scaled capacitor matrix; the
+    basis and incidences as sparse matrices; the scaled reduced capacitor matrix factored by a
+    sparse LU (SuperLU) instead of a dense Cholesky."""
+    import scipy.sparse as sp
+
+    n, o = w.cells, w.nodes
+    size = n + o
+    parent = list(range(size))
+
+    def root(i):
+        while parent[i] != i:
+            i = parent[i]
+        return i
+
+    rows, cols, vals = [], [], []
+    for k in range(n):
+        i, j = k, n + int(w.cell_node[k])
+        c = w.capacitance[k]
+        parent[root(j)] = root(i)
+        rows += [i, j, i, j]
+        cols += [i, j, j, i]
+        vals += [c, c, -c, -c]
+    capacitor = sp.csr_matrix((vals, (rows, cols)), shape=(size, size))
+    groups = {}
+    for i in range(size):
+        groups.setdefault(root(i), []).append(i)
+    reservoirs = set((n + np.flatnonzero(w.reservoir)).tolist())
+    fixed = np.zeros(size, dtype=bool)
+    fixed[list(reservoirs)] = True
+    brow, bcol, k_count = [], [], 0
+    for members in groups.values():
+        if reservoirs.intersection(members):
+            continue
+        chosen = min(i for i in members if i >= n)
+        fixed[chosen] = True
+        brow += members
+        bcol += [k_count] * len(members)
+        k_count += 1
+    basis = sp.csr_matrix((np.ones(len(brow)), (brow, bcol)), shape=(size, k_count))
+    scale = float(np.max(np.abs(capacitor.data)))
+    free = sp.diags((~fixed).astype(float))
+    solve_matrix = (free @ (capacitor / scale) @ free + sp.diags(fixed.astype(float))).tocsc()
+    factor = _SparseFactor(solve_matrix)
+    held_out = np.asarray(w.reservoir, dtype=bool)
+    clamp = np.r_[np.zeros(n, dtype=bool), held_out]
+    return Topo(
+        n, o, capacitor, scale, factor, fixed, basis,
+        (basis[n + w.face_sender] - basis[n + w.face_receiver]).T.tocsr(),
+        (basis[w.sender] - basis[w.receiver]).T.tocsr(),
+        ~np.r_[np.zeros(n, dtype=bool), held_out], ~clamp,
+        np.where(clamp, np.r_[np.zeros(n), w.boundary_V], 0.0),
+    )  # fmt: skip
+
+
+class _SparseFactor:
+    """A sparse LU of a symmetric positive definite matrix, standing in for its dense Cholesky
+    factor in the sparse branch (``solve`` in place of cholesky_solve)."""
+
+    def __init__(self, matrix):
+        from scipy.sparse.linalg import splu
+
+        self.lu = splu(matrix.tocsc())
+        diag = self.lu.U.diagonal()
+        self.valid = bool(np.all(np.isfinite(diag)) and np.all(diag > 0))
+
+    def solve(self, rhs):
+        return self.lu.solve(np.asarray(rhs, dtype=float))
+
+
+def _is_sparse(m):
+    return hasattr(m, "tocsr")
+
+
+def _factor_solve(factor, rhs):
+    return factor.solve(rhs) if isinstance(factor, _SparseFactor) else cholesky_solve(factor, rhs)
+
+
 def capacitor_solve(charge, boundary, tp):
     """_capacitor_solve (surface_field.py:596-600) with the factored layout's solve."""
     rhs = np.where(~tp.fixed, (charge - tp.capacitor @ boundary) / tp.scale, 0.0)
-    return cholesky_solve(tp.factor, rhs) + boundary
+    return _factor_solve(tp.factor, rhs) + boundary
 
 
 def offset_solve(matrix, rhs):
     """_offset_solve (:603-611): every offset free (no gauge)."""
     if rhs.size == 0:
         return np.zeros_like(rhs)
+    if _is_sparse(matrix):
+        from scipy.sparse.linalg import spsolve
+
+        scale = float(np.max(np.abs(matrix.data), initial=0.0)) or 1.0
+        return spsolve((matrix / scale).tocsc(), rhs / scale)
     scale = np.max(np.abs(matrix), initial=0.0)
     scale = np.where(scale > 0, scale, 1.0)
     return np.linalg.solve(matrix / scale, rhs / scale)
+
+
+def _weighted_gram(incidence, weight):
+    """incidence diag(weight) incidence^T, dense or sparse."""
+    if _is_sparse(incidence):
+        import scipy.sparse as sp
+
+        return (incidence @ sp.diags(weight) @ incidence.T).tocsr()
+    return (incidence * weight) @ incidence.T
 
 
 def logmean(left, right):
@@ -290,7 +395,7 @@ def field_solve(ci, co, q_cell, q_out, membrane_open, junction_open, w, tp):
     dv = base[n + w.face_sender] - base[n + w.face_receiver]
     face0 = F * np.sum(Z * weight * log, axis=0) + conductance * dv
     fi, ji = tp.face_incidence, tp.junction_incidence
-    matrix = (fi * conductance) @ fi.T
+    matrix = _weighted_gram(fi, conductance)
     initial_offset = offset_solve(matrix, -fi @ face0)
 
     def evaluate(offset):
@@ -311,7 +416,7 @@ def field_solve(ci, co, q_cell, q_out, membrane_open, junction_open, w, tp):
 
     def iteration(count, offset):
         _, _, residual, norm, slope, _ = evaluate(offset)
-        jac = matrix + (ji * slope) @ ji.T
+        jac = matrix + _weighted_gram(ji, slope)
         delta = offset_solve(jac, -residual)
         before = np.max(np.abs(residual), initial=0.0)
         step, proposal, accepted = 0, offset, False
@@ -431,11 +536,19 @@ def implicit_rates(weight, potential, state, w):
 
 
 def face_laplacian(weight, w, tp):
-    """surface_imex.face_laplacian (:144-156), dense in the node space."""
+    """surface_imex.face_laplacian (:144-156), dense in the node space (sparse for a sparse
+    bind)."""
     n = w.cells
     conductance = K * F / (R * w.temperature) * np.sum(Z**2 * weight, axis=0)
     a, b = n + w.face_sender, n + w.face_receiver
     size = tp.n + tp.o
+    if _is_sparse(tp.capacitor):
+        import scipy.sparse as sp
+
+        rows = np.concatenate((a, b, a, b))
+        cols = np.concatenate((a, b, b, a))
+        vals = np.concatenate((conductance, conductance, -conductance, -conductance))
+        return sp.csr_matrix((vals, (rows, cols)), shape=(size, size))
     parts = []
     for rows, cols in ((a, a), (b, b), (a, b), (b, a)):
         m = np.zeros((size, size))
@@ -453,9 +566,20 @@ class Operator(NamedTuple):
 
 
 def factor_operator(coefficient, laplacian, tp):
-    """surface_imex.factor_operator (:207-225), dense."""
+    """surface_imex.factor_operator (:207-225), dense (sparse LU for a sparse bind)."""
     free = tp.free
     matrix = tp.capacitor + coefficient * laplacian
+    if _is_sparse(matrix):
+        import scipy.sparse as sp
+
+        matrix = matrix.tocsr()
+        diagonal = np.where(free, matrix.diagonal(), 1.0)
+        scale = 1.0 / np.sqrt(np.where(diagonal > 0, diagonal, 1.0))
+        keep = sp.diags(free.astype(float) * scale)
+        reduced = (keep @ matrix @ keep + sp.diags((~free).astype(float))).tocsc()
+        factor = _SparseFactor(reduced)
+        valid = bool(np.all(diagonal > 0) and factor.valid)
+        return Operator(factor, scale, matrix, tp.held, free), valid
     diagonal = np.where(free, np.diagonal(matrix), 1.0)
     scale = 1.0 / np.sqrt(np.where(diagonal > 0, diagonal, 1.0))
     reduced = np.where(free[:, None] & free[None, :], matrix * scale[:, None] * scale[None, :], 0.0)
@@ -468,7 +592,7 @@ def factor_operator(coefficient, laplacian, tp):
 def solve_operator(charge, op):
     """surface_imex.solve_operator (:269-278), dense."""
     rhs = np.where(op.free, (charge - op.matrix @ op.held) * op.scale, 0.0)
-    phi = np.where(op.free, cholesky_solve(op.factor, rhs) * op.scale, op.held)
+    phi = np.where(op.free, _factor_solve(op.factor, rhs) * op.scale, op.held)
     return phi, np.where(op.free, op.matrix @ phi - charge, 0.0)
 
 

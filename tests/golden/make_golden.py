@@ -1,9 +1,10 @@
 """Generate the golden fixtures under tests/golden/ by running the REFERENCE's own step.
 
-Run in a container that holds the reference source (default /root/reference), never on the GPU
-box and never from the test suite:
+Run in a container that holds the reference source tree (its project root, the directory with
+``src/cells``), never on the GPU box and never from the test suite:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference project root>
+    CELLS_REFERENCE=<reference project root> python tests/golden/make_golden.py
 
 The reference is a JAX program; jax is absent here, so ``jax_shim/`` (a NumPy stand-in for the
 few jax names it touches) goes first on sys.path and the reference's step runs on its own
@@ -581,10 +582,13 @@ def make_field_trajectories():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("CELLS_REFERENCE"),
+                    help="the reference project's root (or set CELLS_REFERENCE)")
     ap.add_argument("--only", choices=("laws", "trajectories", "channels", "block", "n2",
                                        "checks", "field"))
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set CELLS_REFERENCE to the reference project's root")
     _setup(args.reference)
     if args.only in (None, "laws"):
         make_laws()

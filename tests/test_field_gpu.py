@@ -181,3 +181,60 @@ def test_field_single_cell_without_junctions(cuda):
     bad = {f: d for f in OF.FieldState._fields
            if (d := field_difference(got[f][0], getattr(st, f), st.face_transferred, w, f)) > TOL}
     assert not bad, bad
+
+
+def _oracle_run(ws, controls, dt, steps, sparse=None):
+    """Each world through the field oracle (dense node-space algebra, pinned bit for bit to the
+    reference; sparse containers for the 128x128 grid), steps steps; the final states."""
+    out = []
+    for w, ctl in zip(ws, controls, strict=True):
+        tp, st = OF.bind(w, sparse=sparse), OF.initial_state(w)
+        for _ in range(steps):
+            st, ok = OF.imex_step(st, dt, ctl, w, tp)
+            assert ok
+        out.append(st)
+    return out
+
+
+def test_field_group_kernels_match_the_oracle(cuda):
+    """A 48x48 grid (46x46 free nodes) with a gated 8x8 tissue: the top separators' fronts exceed
+    a warp's block (1280 doubles), so those levels run one front per CTA (factor_group,
+    forward_group, backward_group) beside the warp levels. Two worlds, partial random controls,
+    20 steps in two launches, against the dense oracle at 1e-10."""
+    ws = [FW.field_world(48, 8, 4, worlds.world_rng(31, k), gate=(0.015, 0.2, 1.0),
+                         junction_sigma=0.3) for k in range(2)]
+    tissue = FieldTissue(ws)
+    kinds = tissue.level_kinds()
+    assert 1 in kinds and 0 in kinds, kinds
+    rng = np.random.default_rng(8)
+    mem = rng.uniform(0.6, 1.0, (2, ws[0].cells))
+    jun = rng.uniform(0.6, 1.0, (2, ws[0].edges))
+    pmp = rng.uniform(0.6, 1.0, (2, ws[0].cells))
+    got, status, taken = run(cuda, tissue, tissue.initial_state(),
+                             tissue.pack_control(mem, jun, pmp), 5e-4, [7, 13])
+    assert np.all(status == 0) and np.all(taken == 20)
+    refs = _oracle_run(ws, [OF.Control(mem[k], jun[k], pmp[k]) for k in range(2)], 5e-4, 20,
+                       sparse=False)
+    for k, (w, st) in enumerate(zip(ws, refs, strict=True)):
+        bad = {f: d for f in OF.FieldState._fields
+               if (d := field_difference(got[f][k], getattr(st, f), st.face_transferred, w,
+                                         f)) > TOL}
+        assert not bad, (k, bad)
+
+
+def test_field_benchmark_grid_matches_the_sparse_oracle(cuda):
+    """One world of the benchmark's shape (a 32x32 tissue at stride 3 in the 128x128 grid,
+    15,876 free nodes, the root separator's 126-column front) for 3 steps against the oracle's
+    sparse restatement of the same algebra (scipy.sparse LU solves in place of its dense ones;
+    equal to the dense oracle to rounding on the golden worlds), at 1e-10."""
+    w = FW.field_world(128, 32, 3, worlds.world_rng(7, 0))
+    tissue = FieldTissue([w])
+    kinds = tissue.level_kinds()
+    assert sum(kinds) >= 4, kinds
+    got, status, taken = run(cuda, tissue, tissue.initial_state(), tissue.pack_control(), 5e-4,
+                             [3])
+    assert status[0] == 0 and taken[0] == 3
+    (st,) = _oracle_run([w], [OF.full_control(w)], 5e-4, 3, sparse=True)
+    bad = {f: d for f in OF.FieldState._fields
+           if (d := field_difference(got[f][0], getattr(st, f), st.face_transferred, w, f)) > TOL}
+    assert not bad, bad

@@ -66,3 +66,26 @@ def test_field_step_refuses_an_invalid_control_and_keeps_the_state():
     assert not ok
     for a, b in zip(state, start, strict=True):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["field_grid10.npz", "field_gated14.npz"])
+def test_sparse_restatement_matches_the_reference(name):
+    """bind(w, sparse=True): the same algebra in scipy.sparse containers with sparse LU solves
+    (what the 128x128 benchmark grid needs) reproduces the reference's trajectories to rounding
+    accumulated over the runs (1e-11 scaled over up to 200 steps, ten times inside the device
+    bar)."""
+    z, w = load_field_golden(name)
+    tp = OF.bind(w, sparse=True)
+    control = OF.Control(z["control_membrane"], z["control_junction"], z["control_pump"])
+    dt = float(z["dt"])
+    state, done, worst = OF.initial_state(w), 0, {}
+    for idx, target in enumerate(z["steps"]):
+        while done < target:
+            state, ok = OF.imex_step(state, dt, control, w, tp)
+            assert ok, done
+            done += 1
+        for f in OF.FieldState._fields:
+            worst[f] = max(worst.get(f, 0.0), scaled_difference(getattr(state, f),
+                                                                z["ref_" + f][idx]))
+    bad = {k: v for k, v in worst.items() if v > 1e-11}
+    assert not bad, (bad, worst)

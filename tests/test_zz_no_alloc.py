@@ -1,7 +1,7 @@
-"""cb_step_packed_static: the packed step with its scratch in the library's own static device
-array, for callers that may not allocate device memory while a step runs (a plugin that its host
-runtime hands only input and output buffers, such as an XLA/JAX custom call or a step inside a
-captured CUDA graph, or a process whose device memory another allocator already holds).
+"""cb_step_packed_static: the packed FP64 ARS(2,2,2) step with its scratch in the library's own
+static device array, for callers that may not allocate device memory while a step runs (a plugin
+that its host runtime hands only input and output buffers, such as an XLA/JAX custom call, or a
+process whose device memory another allocator already holds).
 
 Checked through the C ABI against cb_step on the same handle, inputs and controls, twice in a
 row (the array keeps the first call's contents; the second call must not depend on them), with
