@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
         bool ok = true;
         for (int q = 0; q < NCH; ++q) {
           double t[2], tau[2];
-          channel_kinetics<MIX>(__ldg(T.ch_code + q * C + gi), V - Vb, t, tau);
+          channel_kinetics<false>(__ldg(T.ch_code + q * C + gi), V - Vb, t, tau);
           ok = ok && channel_kinetics_ok(V - Vb, t, tau);
           for (int r = 0; r < 2; ++r) {
             CH(q, 6 + r, gi) = t[r];
@@ -173,11 +173,11 @@ __global__ void __launch_bounds__(BLOCK, 1)
                 chg[r][q] = cur[L.s[CB_CHANNEL_GATE] + (r * NCH + q) * C + gi];
               if (!first) {
                 double t[2], tau[2];
-                channel_kinetics<MIX>(code, V - Vb, t, tau);
+                channel_kinetics<false>(code, V - Vb, t, tau);
                 if (!channel_kinetics_ok(V - Vb, t, tau)) bits |= CB_WORLD_CHANNEL_DOMAIN;
                 for (int r = 0; r < 2; ++r) {
                   if (!(r == 1 && code == kHhKn4))
-                    chg[r][q] = advance_gate<MIX>(chg[r][q], CH(q, 6 + r, gi), CH(q, 8 + r, gi),
+                    chg[r][q] = advance_gate<false>(chg[r][q], CH(q, 6 + r, gi), CH(q, 8 + r, gi),
                                              t[r], tau[r], k.frac1_dt);
                   CH(q, 4 + r, gi) = chg[r][q];
                 }
@@ -188,10 +188,8 @@ __global__ void __launch_bounds__(BLOCK, 1)
           const double ivol = __ldg(T.ivol + gi);
           for (int s = 0; s < 3; ++s) {
             c[s] = (__ldg(T.ref + s * C + gi) + n[s]) * ivol;
-            if (!MIX) {  // the mixed step forms its logarithms from differences in FP32
-              lc[s] = log(c[s]);
-              sL[s * CAP + cl] = lc[s];
-            }
+            lc[s] = log(c[s]);
+            sL[s * CAP + cl] = lc[s];
             if (!(is_finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
             sC[s * CAP + cl] = c[s];
           }
@@ -215,11 +213,10 @@ __global__ void __launch_bounds__(BLOCK, 1)
               const float J = (float)gs * ((s < 2) ? d * fb + (float)c[s] * fx
                                                    : d * fb - (float)co * fx);
               jm[s] = J;
-              mu[s] = (float)RT * logf((float)c[s] / (float)co) + (float)zfdv;
             } else {
               jm[s] = (s < 2) ? gs * (c[s] * bm - co * bp) : gs * (c[s] * bp - co * bm);
-              mu[s] = RT * (lc[s] - __ldg(wc + WC_LOGCO + s)) + zfdv;
             }
+            mu[s] = RT * (lc[s] - __ldg(wc + WC_LOGCO + s)) + zfdv;
           }
           const double md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
           if (!(is_finite(jm[0]) && is_finite(jm[1]) && is_finite(jm[2]) && is_finite(md)))
@@ -267,8 +264,7 @@ __global__ void __launch_bounds__(BLOCK, 1)
               } else {
                 membrane += gterm;
               }
-              const double Jd = MIX ? (double)((float)1e-3 * (float)J * (float)mu[sp])
-                                    : 1e-3 * J * mu[sp];
+              const double Jd = 1e-3 * J * mu[sp];
               chm[sp] += J;
               if (first) {
                 CH(q, 0, gi) = cur[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi] + w_acc * J;
@@ -290,21 +286,11 @@ __global__ void __launch_bounds__(BLOCK, 1)
           const double capacity = __ldg(T.pcap + gi);
           if (capacity > 0.0 && pctl > 0.0) {
             const double ldc = __ldg(T.logpcap + gi) + log(pctl);
-            if constexpr (MIX) {
-              const float af = (float)a;
-              const float ls = ((-logaddexp0<float>(3.f * ((float)__ldg(wc + WC_LOGKMNA) -
-                                                           logf((float)c[0])))) -
-                                (float)__ldg(wc + WC_LK)) - (float)__ldg(wc + WC_LATP);
-              const float mag = expf(((float)ldc + ls) + fmaxf(af, 0.f));
-              const float dep = af >= 0.f ? expm1f(-af) : -expm1f(af);
-              cycles = mag * dep;
-            } else {
-              const double ls = ((-logaddexp0(3.0 * (__ldg(wc + WC_LOGKMNA) - lc[0]))) -
-                                 __ldg(wc + WC_LK)) - __ldg(wc + WC_LATP);
-              const double mag = exp((ldc + ls) + fmax(a, 0.0));
-              const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
-              cycles = mag * dep;
-            }
+            const double ls = ((-logaddexp0(3.0 * (__ldg(wc + WC_LOGKMNA) - lc[0]))) -
+                               __ldg(wc + WC_LK)) - __ldg(wc + WC_LATP);
+            const double mag = exp((ldc + ls) + fmax(a, 0.0));
+            const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
+            cycles = mag * dep;
           }
           const double pd = (-1e-3 * cycles) * energy;
           const double mw = (-1e-3 * cycles) * drive;
@@ -357,33 +343,24 @@ __global__ void __launch_bounds__(BLOCK, 1)
             const double cs = sC[s * CAP + s_], cr = sC[s * CAP + r_];
             const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
             if constexpr (MIX) {
-              // FP32 on the FP64 difference c_s - c_r; ln(c_s/c_r) = log1p(d / c_r).
+              // FP32 on the FP64 difference c_s - c_r.
               const float d = (float)(cs - cr), fb = (float)bp, fx = (float)x;
               jj[s] = (float)gs * ((s < 2) ? d * fb + (float)cs * fx : d * fb - (float)cr * fx);
-              mu[s] = (float)RT * log1pf(d / (float)cr) + (float)zfdv;
             } else {
               jj[s] = (s < 2) ? gs * (cs * bm - cr * bp) : gs * (cs * bp - cr * bm);
-              mu[s] = RT * (sL[s * CAP + s_] - sL[s * CAP + r_]) + zfdv;
             }
+            mu[s] = RT * (sL[s * CAP + s_] - sL[s * CAP + r_]) + zfdv;
             SCe(SE_J + s, ge) = jj[s];
           }
           const double jd = 1e-3 * ((jj[0] * mu[0] + jj[1] * mu[1]) + jj[2] * mu[2]);
           const double thr = __ldg(T.thr + ge), mn = __ldg(T.jmin + ge);
           double gr = 0.0;
           if (mn < 1.0) {
-            if constexpr (MIX) {
-              const float shift = (float)(fabs(dv) - thr);
-              const float alpha = 1.3f * expf(-77.f * shift);
-              const float log_beta = (float)kLog0065 + 140.f * shift;
-              const float beta = 20.f * expf(-logaddexp0<float>(-log_beta));
-              gr = alpha * (1.f - (float)g) - beta * (float)(g - mn);
-            } else {
-              const double shift = fabs(dv) - thr;
-              const double alpha = 1.3 * exp(-77.0 * shift);
-              const double log_beta = kLog0065 + 140.0 * shift;
-              const double beta = 20.0 * exp(-logaddexp0(-log_beta));
-              gr = alpha * (1.0 - g) - beta * (g - mn);
-            }
+            const double shift = fabs(dv) - thr;
+            const double alpha = 1.3 * exp(-77.0 * shift);
+            const double log_beta = kLog0065 + 140.0 * shift;
+            const double beta = 20.0 * exp(-logaddexp0(-log_beta));
+            gr = alpha * (1.0 - g) - beta * (g - mn);
           }
           const double led[5] = {jj[0], jj[1], jj[2], jd, gr};
           for (int f = 0; f < 5; ++f) {
@@ -454,13 +431,13 @@ __global__ void __launch_bounds__(BLOCK, 1)
               for (int q = 0; q < NCH; ++q) {
                 const int code = __ldg(T.ch_code + q * C + gi);
                 double t[2], tau[2];
-                channel_kinetics<MIX>(code, V2 - Vb, t, tau);
+                channel_kinetics<false>(code, V2 - Vb, t, tau);
                 k2 = k2 && channel_kinetics_ok(V2 - Vb, t, tau);
                 for (int r = 0; r < 2; ++r) {
                   const double g0 = cur[L.s[CB_CHANNEL_GATE] + (r * NCH + q) * C + gi];
                   double g = g0;
                   if (!(r == 1 && code == kHhKn4))
-                    g = advance_gate<MIX>(g0, CH(q, 6 + r, gi), CH(q, 8 + r, gi), t[r], tau[r],
+                    g = advance_gate<false>(g0, CH(q, 6 + r, gi), CH(q, 8 + r, gi), t[r], tau[r],
                                      k.frac2_dt);
                   CH(q, 2 + r, gi) = g;
                   // The end kinetics: the next step's start once this step is accepted.

@@ -102,10 +102,8 @@ __device__ __forceinline__ void stage(
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
       c[s] = (__ldg(T.ref + s * C + gi) + n[s]) * ivol;
-      if (!MIX) {
-        lc[s] = log(c[s]);
-        sL[s * BLOCK + i] = lc[s];
-      }
+      lc[s] = log(c[s]);
+      sL[s * BLOCK + i] = lc[s];
       if (!(is_finite(c[s]) && c[s] > 0.0)) bits |= CB_WORLD_TRANSPORT;
       sC[s * BLOCK + i] = c[s];
     }
@@ -131,12 +129,11 @@ __device__ __forceinline__ void stage(
         const float J = (float)gs * ((s < 2) ? d * fb + (float)c[s] * fx
                                              : d * fb - (float)co * fx);
         jm[s] = J;
-        mu[s] = (float)RT * logf((float)c[s] / (float)co) + (float)zfdv;
       } else {
         // Na, K: z = +1 -> (c_in B(-x) - c_out B(x)); Cl: z = -1 swaps the pair.
         jm[s] = (s < 2) ? gs * (c[s] * bm - co * bp) : gs * (c[s] * bp - co * bm);
-        mu[s] = RT * (lc[s] - wc[WC_LOGCO + s]) + zfdv;
       }
+      mu[s] = RT * (lc[s] - wc[WC_LOGCO + s]) + zfdv;
       cell_acc(3 + s, L.s[CB_MEMBRANE_TRANSFERRED] + s * C, jm[s]);
     }
     const double md = 1e-3 * ((jm[0] * mu[0] + jm[1] * mu[1]) + jm[2] * mu[2]);
@@ -174,13 +171,11 @@ __device__ __forceinline__ void stage(
         double J, Jd;
         if constexpr (MIX) {
           const float d = (float)(cs - cos_), fb = (float)bp, fx = (float)x;
-          const float Jf = (float)gq * (sp < 2 ? d * fb + (float)cs * fx : d * fb - (float)cos_ * fx);
-          J = Jf;
-          Jd = (float)1e-3 * Jf * (float)musp;
+          J = (float)gq * (sp < 2 ? d * fb + (float)cs * fx : d * fb - (float)cos_ * fx);
         } else {
           J = sp < 2 ? gq * (cs * bm - cos_ * bp) : gq * (cs * bp - cos_ * bm);
-          Jd = 1e-3 * J * musp;
         }
+        Jd = 1e-3 * J * musp;
         chm[sp] += J;
         membrane += ((__ldg(T.ch_ap + q * C + gi) * 1e-15) * (sp == 0 ? largest[0]
                      : sp == 1 ? largest[1] : largest[2])) * available;
@@ -202,20 +197,11 @@ __device__ __forceinline__ void stage(
     const double a = energy * wc[WC_INVRT];
     double cycles = 0.0;
     if (__ldg(T.pcap + gi) > 0.0 && pc_ctl > 0.0) {
-      if constexpr (MIX) {
-        const float af = (float)a;
-        const float ls = ((-logaddexp0<float>(3.f * ((float)wc[WC_LOGKMNA] - logf((float)c[0])))) -
-                          (float)wc[WC_LK]) - (float)wc[WC_LATP];
-        const float mag = expf(((float)log_drive_cap + ls) + fmaxf(af, 0.f));
-        const float dep = af >= 0.f ? expm1f(-af) : -expm1f(af);
-        cycles = mag * dep;
-      } else {
-        const double ls =
-            ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
-        const double mag = exp((log_drive_cap + ls) + fmax(a, 0.0));
-        const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
-        cycles = mag * dep;
-      }
+      const double ls =
+          ((-logaddexp0(3.0 * (wc[WC_LOGKMNA] - lc[0]))) - wc[WC_LK]) - wc[WC_LATP];
+      const double mag = exp((log_drive_cap + ls) + fmax(a, 0.0));
+      const double dep = a >= 0.0 ? expm1(-a) : -expm1(a);
+      cycles = mag * dep;
     }
     const double pd = (-1e-3 * cycles) * energy;
     const double mw = (-1e-3 * cycles) * drive;
@@ -260,14 +246,13 @@ __device__ __forceinline__ void stage(
         const double cs = sC[s * BLOCK + s_], cr = sC[s * BLOCK + r_];
         const double zfdv = (s < 2) ? kF * dv : (-kF) * dv;
         if constexpr (MIX) {
-          // FP32 on the FP64 difference c_s - c_r (as the patch); ln(c_s/c_r) = log1p(d / c_r).
+          // FP32 on the FP64 difference c_s - c_r (as the patch).
           const float d = (float)(cs - cr), fb = (float)bp, fx = (float)x;
           jj[s] = (float)gs * ((s < 2) ? d * fb + (float)cs * fx : d * fb - (float)cr * fx);
-          mu[s] = (float)RT * log1pf(d / (float)cr) + (float)zfdv;
         } else {
           jj[s] = (s < 2) ? gs * (cs * bm - cr * bp) : gs * (cs * bp - cr * bm);
-          mu[s] = RT * (sL[s * BLOCK + s_] - sL[s * BLOCK + r_]) + zfdv;
         }
+        mu[s] = RT * (sL[s * BLOCK + s_] - sL[s * BLOCK + r_]) + zfdv;
         sJ[s * EB + e] = jj[s];
       }
       const double jd = 1e-3 * ((jj[0] * mu[0] + jj[1] * mu[1]) + jj[2] * mu[2]);
@@ -275,19 +260,11 @@ __device__ __forceinline__ void stage(
       const double thr = __ldg(T.thr + ge), mn = __ldg(T.jmin + ge);
       double gr = 0.0;
       if (mn < 1.0) {
-        if constexpr (MIX) {
-          const float shift = (float)(fabs(dv) - thr);
-          const float alpha = 1.3f * expf(-77.f * shift);
-          const float log_beta = (float)kLog0065 + 140.f * shift;
-          const float beta = 20.f * expf(-logaddexp0<float>(-log_beta));
-          gr = alpha * (1.f - (float)g[q]) - beta * (float)(g[q] - mn);
-        } else {
-          const double shift = fabs(dv) - thr;
-          const double alpha = 1.3 * exp(-77.0 * shift);
-          const double log_beta = kLog0065 + 140.0 * shift;
-          const double beta = 20.0 * exp(-logaddexp0(-log_beta));
-          gr = alpha * (1.0 - g[q]) - beta * (g[q] - mn);
-        }
+        const double shift = fabs(dv) - thr;
+        const double alpha = 1.3 * exp(-77.0 * shift);
+        const double log_beta = kLog0065 + 140.0 * shift;
+        const double beta = 20.0 * exp(-logaddexp0(-log_beta));
+        gr = alpha * (1.0 - g[q]) - beta * (g[q] - mn);
       }
       if (FIRST) {
 #pragma unroll
@@ -434,7 +411,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
 #pragma unroll
       for (int q = 0; q < NCH; ++q) {
         double t[2], tau[2];
-        channel_kinetics<MIX>(__ldg(T.ch_code + q * C + gi), V - Vb, t, tau);
+        channel_kinetics<false>(__ldg(T.ch_code + q * C + gi), V - Vb, t, tau);
         k0_ok = k0_ok && channel_kinetics_ok(V - Vb, t, tau);
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
@@ -490,12 +467,12 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       if (NCH > 0 && has_cell) {
         const int code = __ldg(T.ch_code + q * C + gi);
         double t[2], tau[2];
-        channel_kinetics<MIX>(code, V1 - Vb, t, tau);
+        channel_kinetics<false>(code, V1 - Vb, t, tau);
         if (!channel_kinetics_ok(V1 - Vb, t, tau)) bits |= CB_WORLD_CHANNEL_DOMAIN;
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
           if (r == 1 && code == kHhKn4) continue;
-          chg1[r][q] = advance_gate<MIX>(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
+          chg1[r][q] = advance_gate<false>(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
                                     sK[((2 + r) * NCH + q) * BLOCK + i], t[r], tau[r], k.frac1_dt);
         }
       }
@@ -525,7 +502,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         for (int q = 0; q < NCH; ++q) {
           const int code = __ldg(T.ch_code + q * C + gi);
           double t[2], tau[2];
-          channel_kinetics<MIX>(code, V2 - Vb, t, tau);
+          channel_kinetics<false>(code, V2 - Vb, t, tau);
           k2_ok = k2_ok && channel_kinetics_ok(V2 - Vb, t, tau);
 #pragma unroll
           for (int r = 0; r < 2; ++r) {
@@ -533,7 +510,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
             k2tau[r][q] = tau[r];
             double g = chg0[r][q];
             if (!(r == 1 && code == kHhKn4))
-              g = advance_gate<MIX>(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
+              g = advance_gate<false>(chg0[r][q], sK[(r * NCH + q) * BLOCK + i],
                                sK[((2 + r) * NCH + q) * BLOCK + i], t[r], tau[r], k.frac2_dt);
             sG[(r * NCH + q) * BLOCK + i] = g;
             ok = ok && is_finite(g) && g >= 0.0 && g <= 1.0;

@@ -140,12 +140,16 @@ enum cb_control_field {
 
 /* Step methods. */
 #define CB_METHOD_ARS222 0 /* cells.solver.imex_ars222_face_electromigration@1 */
-/* The same ARS(2,2,2) step with its rates in FP32 (this library's
- * cells_b200.solver.imex_ars222_mixed_fp32@1; no reference method): transcendentals, fluxes,
- * the pump and channel kinetics in FP32 on FP64 concentration and potential differences; the
- * near-zero Bernoulli series, concentrations, potentials, world sums and every state and ledger
- * accumulation in FP64. Both kernels (one world per CTA, and the packed kernel for uneven
- * batches); not with an open-channel block. */
+/* The same ARS(2,2,2) step with its constant-field fluxes in FP32 (this library's
+ * cells_b200.solver.imex_ars222_mixed_fp32@1; no reference method): the Bernoulli pair's
+ * exponential form and the membrane, channel and junction flux products in FP32 on FP64
+ * concentration differences; the near-zero Bernoulli series, concentrations, their logarithms
+ * and potentials, the pump, the channel and junction gate laws and the gates' updates, world
+ * sums and every state and ledger accumulation in FP64. The amounts stay within 1e-8 (about
+ * 1e-11) of the FP64 step's and the ledgers balance to 1e-12; the gates, which follow the
+ * membrane voltage, within about 5e-8 of their scale, and the ledgers that integrate a flux carry
+ * its FP32 rounding (about 1e-7 of their scale). Both kernels (one world per CTA, and the packed
+ * kernel for uneven batches); not with an open-channel block. */
 #define CB_METHOD_ARS222_MIXED 1
 /* N2 (cells.solver.imex_ars222_implicit_conductances@1, models/surface_pump_v3.py:3547-3955 under
  * an N2 ID): ARS(2,2,2) with every patch's, channel population's and junction's slope

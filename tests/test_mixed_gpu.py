@@ -1,9 +1,16 @@
-"""The mixed-precision ARS(2,2,2) step (CB_METHOD_ARS222_MIXED: FP32 rates on FP64 differences,
-FP64 near-zero GHK series and FP64 accumulation) against the FP64 device step.
+"""The mixed-precision ARS(2,2,2) step (CB_METHOD_ARS222_MIXED: FP32 constant-field fluxes on
+FP64 concentration differences; everything else, the near-zero GHK series and every accumulation
+in FP64) against the FP64 device step.
 
-Per-output errors are printed (pytest -s shows them) and bounded: state amounts within 1e-8 of
-the FP64 amounts (relative to the cells' physical amounts), every field's scaled difference
-within 1e-5, and the conservation ledgers within 1e-12 relative, every launch, as the FP64 step.
+Per-output errors are printed (pytest -s shows them) and bounded, in four classes:
+* the amounts within 1e-8 of the cells' physical amounts (measured about 1e-11);
+* conservation: the ledgers balance within 1e-12 relative, every launch, as the FP64 step;
+* the gates within 1e-7 scaled (measured 5e-8 for channel gates, 0 for junction gates): their
+  laws run in FP64, but they follow the membrane voltage, a small net charge over C, which
+  carries the amount increments' FP32-flux rounding;
+* the ledgers that integrate a flux (amount increments over the reference, membrane, junction
+  and channel transfers and heats; the pump's ledgers, in FP64, only through the voltage) carry
+  the FP32 flux's rounding: within 5e-7 scaled difference (measured about 1e-7).
 """
 
 import numpy as np
@@ -62,6 +69,8 @@ def test_mixed_step_error_against_fp64(cuda, kind):
     print(f"\nmixed vs fp64 ({kind}, 500 steps): amounts {amount_err:.2e}; " +
           ", ".join(f"{f} {v:.1e}" for f, v in errors.items()))
     assert amount_err <= 1e-8
-    assert max(errors.values()) <= 1e-5
+    gates = {f: errors[f] for f in ("junction_gate", "channel_gate") if f in errors}
+    assert all(v <= 1e-7 for v in gates.values()), gates
+    assert max(errors.values()) <= 5e-7, errors
     scale = float(np.max(np.abs(b.amount_reference)))
     assert ledgers[0] <= 1e-12 * scale  # local material balance per cell
