@@ -53,6 +53,7 @@ METHOD = "cells.solver.imex_ars222_face_electromigration@1"
 METHOD_MIXED = "cells_b200.solver.imex_ars222_mixed_fp32@1"
 METHOD_N2 = "cells.solver.imex_ars222_implicit_conductances@1"
 METHOD_N2_MIXED = "cells_b200.solver.imex_ars222_implicit_conductances_mixed@1"
+METHOD_ROS2 = "cells_b200.solver.ros2_verwer@1"
 
 
 def bytes_per_cell_step(batch):
@@ -91,8 +92,9 @@ def parse():
                     help="end-to-end host calls timed (default 3; adjoint: 1 gradient)")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
                     help="mixed: the ARS(2,2,2) step with FP32 rates and FP64 accumulation")
-    ap.add_argument("--method", choices=("ars222", "n2"), default="ars222",
-                    help="n2: slope conductances implicit, a sparse Cholesky per world per step")
+    ap.add_argument("--method", choices=("ars222", "n2", "ros2"), default="ars222",
+                    help="n2: slope conductances implicit, a sparse Cholesky per world per step; "
+                         "ros2: the two-stage Rosenbrock method on the same operator")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the bind's launch configuration instead of the autotuner's")
     ap.add_argument("--no-graph", action="store_true",
@@ -799,7 +801,9 @@ def run_grid(args, rank, world_size, local_rank, dist, base):
     dev = torch.device("cuda", local_rank)
     from cells_b200 import _lib as _lib_methods
 
-    if args.method == "n2":
+    if args.method == "ros2":
+        method = _lib_methods.METHOD_ROS2
+    elif args.method == "n2":
         method = (_lib_methods.METHOD_N2_MIXED if args.precision == "mixed"
                   else _lib_methods.METHOD_N2)
     else:
@@ -820,7 +824,7 @@ def run_grid(args, rank, world_size, local_rank, dist, base):
             dist.barrier()
 
     tuned = None
-    if not args.no_autotune and args.method != "n2":
+    if not args.no_autotune and args.method == "ars222":
         from cells_b200 import autotune
 
         best, timings = autotune.tune(tissue, state, control, args.dt,
@@ -917,16 +921,17 @@ def run_grid(args, rank, world_size, local_rank, dist, base):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": ("f64" if args.precision == "fp64" else
                       "f32 factor / f64 refinement" if args.method == "n2" else
-                      "f32 rates / f64 accumulation"),
+                      "f32 fluxes / f64 rest"),
             "data": "synthetic (seeded pump-leak tissues)",
             "config": {
                 "workload": workload_name(args),
-                "method": ((METHOD_N2 if args.precision == "fp64" else METHOD_N2_MIXED)
+                "method": (METHOD_ROS2 if args.method == "ros2" else
+                           (METHOD_N2 if args.precision == "fp64" else METHOD_N2_MIXED)
                            if args.method == "n2" else
                            METHOD if args.precision == "fp64" else METHOD_MIXED),
                 "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
-                "launch": ({"kernel": "n2 (one world per CTA)", "block": 256}
-                           if args.method == "n2" else
+                "launch": ({"kernel": f"{args.method} (one world per CTA)", "block": 256}
+                           if args.method in ("n2", "ros2") else
                            dict(zip(("kernel", "block", "occupancy"), tissue.get_launch()))),
                 "autotune": tuned, "cuda_graph": graph is not None,
                 "cells_per_gpu": cells, "junctions_per_gpu": batch.edges,
@@ -1006,6 +1011,9 @@ def main():
         subs = {}
         for name, kw in (("grid", dict(workload="grid", worlds=4096, side=16, dt=1e-3,
                                        steps=200, warmup=100, e2e_calls=1, fuse=100)),
+                         ("grid_ros2", dict(workload="grid", worlds=4096, side=16, dt=1e-3,
+                                            steps=20, warmup=5, e2e_calls=0, fuse=10,
+                                            method="ros2")),
                          ("adjoint", dict(workload="adjoint", worlds=512, dt=1e-3, steps=1,
                                           warmup=1, e2e_calls=0))):
             sub = argparse.Namespace(**{**vars(args), **kw})

@@ -37,6 +37,8 @@ METHOD_ARS222 = 0
 METHOD_ARS222_MIXED = 1
 METHOD_N2 = 2
 METHOD_N2_MIXED = 3
+METHOD_ROS2 = 4
+METHOD_RK4 = 5
 KERNEL_SHARED, KERNEL_PACKED = 0, 1
 WORLD_BITS = {
     1: "transport",

@@ -44,6 +44,11 @@ int n2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
             const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
             cudaStream_t stream, bool mix);
 void n2_release(cb_tissue *t);
+// The ROS2 method (n2_step.cu, on N2's factor plan), or with rk4 the classical RK4 of the same
+// right-hand side in the same kernel: n_steps steps of every world.
+int ros2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
+              const double *control, int n_steps, uint32_t *world_status,
+              int32_t *accepted_steps, cudaStream_t stream, bool rk4);
 }  // namespace cbk
 
 struct cb_tissue {

@@ -332,4 +332,78 @@ inline StepCoef step_coef(double dt) {
   return k;
 }
 
+// B'(x) and B'(-x) from one expm1 of -|x|:
+//   x > 0: B'(x) = -(1 + em)(x + em) / em^2,  x < 0: B'(x) = (em + |x| (1 + em)) / em^2,
+// em = expm1(-|x|); below |x| < 1e-2 the series -1/2 + x/6 - x^3/180 + x^5/5040 - x^7/151200.
+__device__ __forceinline__ void bernoulli_slope_pair(double x, double &sp, double &sm) {
+  const double ax = fabs(x);
+  if (ax < 1e-2) {
+    const double x2 = x * x;
+    const double even = -0.5;
+    const double odd = x * (1.0 / 6.0 + x2 * (-1.0 / 180.0 + x2 * (1.0 / 5040.0 - x2 / 151200.0)));
+    sp = even + odd;
+    sm = even - odd;
+    return;
+  }
+  const double em = expm1(-ax);
+  const double d = em * em;
+  const double at_pos = -(1.0 + em) * (ax + em) / d;  // B'(|x|)
+  const double at_neg = (em + ax * (1.0 + em)) / d;   // B'(-|x|)
+  sp = x > 0.0 ? at_pos : at_neg;
+  sm = x > 0.0 ? at_neg : at_pos;
+}
+
+__device__ __forceinline__ double bernoulli_slope(double x) {
+  double sp, sm;
+  bernoulli_slope_pair(x, sp, sm);
+  return sp;
+}
+
+__device__ __forceinline__ double sigmoid(double u) {
+  const double e = exp(-fabs(u));
+  return u >= 0.0 ? 1.0 / (1.0 + e) : e / (1.0 + e);
+}
+
+// Voltage derivatives of a channel law's targets dt[2] and time constants dtau[2] at v.
+__device__ inline void channel_slope(int code, double v, double (&dt)[2], double (&dtau)[2]) {
+  if (code == kNav1p2) {
+    const double sh = (v + 0.025) / 0.009;
+    double bp, bm;
+    bernoulli_pair<double>(sh, bp, bm);
+    double sp, sm;
+    bernoulli_slope_pair(sh, sp, sm);
+    const double act = (0.182 * 9) * bm, dact = -(0.182 * 9) * sm / 0.009;
+    const double deact = (0.124 * 9) * bp, ddeact = (0.124 * 9) * sp / 0.009;
+    const double ur = -(v + 0.040) / 0.005, ui = (v + 0.065000123) / 0.005;
+    const double rec = (0.024 * 5) * bernoulli<double>(ur);
+    const double drec = -(0.024 * 5) * bernoulli_slope(ur) / 0.005;
+    const double ina = (0.0091 * 5) * bernoulli<double>(ui);
+    const double dina = (0.0091 * 5) * bernoulli_slope(ui) / 0.005;
+    const double s = act + deact, ds = dact + ddeact;
+    const double t1 = 1.0 / (1.0 + exp((v + 0.055) / 0.0062));
+    const double q = rec + ina, dq = drec + dina;
+    dt[0] = (dact * s - act * ds) / (s * s);
+    dt[1] = -t1 * (1.0 - t1) / 0.0062;
+    dtau[0] = -0.001 * ds / (s * s);
+    dtau[1] = -0.001 * dq / (q * q);
+  } else if (code == kHhKn4) {
+    const double ua = -(1000.0 * v + 55.0) / 10.0;
+    const double alpha = 100.0 * bernoulli<double>(ua);
+    const double dalpha = -100.0 * 100.0 * bernoulli_slope(ua);
+    const double beta = 125.0 * exp(-(1000.0 * v + 65.0) / 80.0);
+    const double dbeta = -12.5 * beta;
+    const double s = alpha + beta, ds = dalpha + dbeta;
+    dt[0] = (dalpha * beta - alpha * dbeta) / (s * s);
+    dt[1] = 0.0;
+    dtau[0] = -ds / (s * s);
+    dtau[1] = 0.0;
+  } else {  // Kv1.5
+    const double s0 = sigmoid((v + 0.0060) / 0.0064), s1 = sigmoid(-(v + 0.0253) / 0.0035);
+    dt[0] = s0 * (1.0 - s0) / 0.0064;
+    dt[1] = -s1 * (1.0 - s1) / 0.0035;
+    dtau[0] = -0.1163;
+    dtau[1] = -15.5;
+  }
+}
+
 }  // namespace cbk

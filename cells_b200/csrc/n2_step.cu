@@ -291,6 +291,132 @@ __device__ __forceinline__ void patch_mu(const double *__restrict__ wc, const do
     mu[s] = wc[WC_RT] * (lc[s] - wc[WC_LOGCO + s]) + ((s < 2) ? kF * dv : (-kF) * dv);
 }
 
+// One world's sparse Cholesky on its plan (local indices; values and vectors by position), as one
+// CTA of BLOCK threads runs it: left-looking factor by levels of the elimination tree, a warp per
+// column (update terms in ascending k, each term's rows at precomputed offsets in the column,
+// so no atomics); a run of one-column levels (the top separator's chain) by warp 0 alone with
+// warp syncs only; forward and back substitution of L L^T x = b (b in Yv, x to Xv), a thread per
+// column, or warp 0 with the dot products across its lanes (a fixed xor tree) on those runs.
+template <typename FT, int BLOCK>
+struct WorldCholesky {
+  const int *colp, *lrow, *ukp, *ukc, *ukpos, *ukrel, *rel, *lvp, *lvc;
+  FT *lval, *Yv, *Xv;
+  int lv0, lv1;
+
+  __device__ uint32_t factor_column(int j, int lane) const {
+    uint32_t bad = 0;
+    const int cj = colp[j];
+    for (int u = ukp[j]; u < ukp[j + 1]; ++u) {
+      const int kk = ukc[u], p = ukpos[u], r0 = ukrel[u];
+      const int cnt = colp[kk + 1] - p;
+      const FT ljk = lval[p];
+      for (int t = lane; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
+      __syncwarp();
+    }
+    FT piv = 0;
+    if (lane == 0) {
+      const FT d = lval[cj];
+      if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+      piv = sqrt(d);
+      lval[cj] = piv;
+    }
+    piv = __shfl_sync(0xffffffffu, piv, 0);
+    const FT inv = FT(1) / piv;
+    const int len = colp[j + 1] - cj;
+    for (int t = 1 + lane; t < len; t += 32) lval[cj + t] *= inv;
+    __syncwarp();
+    return bad;
+  }
+  // The end of the run of one-column levels starting at lv (uniform across the CTA).
+  __device__ int single_run_end(int lv) const {
+    int end = lv;
+    while (end < lv1 && lvp[end + 1] - lvp[end] == 1) ++end;
+    return end;
+  }
+  __device__ uint32_t factor() const {
+    constexpr int WARPS = BLOCK / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t bad = 0;
+    for (int lv = lv0; lv < lv1;) {
+      const int a0 = lvp[lv], a1 = lvp[lv + 1];
+      if (a1 - a0 == 1) {
+        const int end = single_run_end(lv);
+        if (warp == 0)
+          for (int l = lv; l < end; ++l) bad |= factor_column(lvc[lvp[l]], lane);
+        lv = end;
+      } else {
+        for (int a = a0 + warp; a < a1; a += WARPS) bad |= factor_column(lvc[a], lane);
+        ++lv;
+      }
+      __syncthreads();
+    }
+    return bad;
+  }
+  __device__ static FT warp_sum(FT v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  }
+  __device__ void solve() const {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int lv = lv0; lv < lv1;) {
+      const int a0 = lvp[lv], a1 = lvp[lv + 1];
+      if (a1 - a0 == 1) {
+        const int end = single_run_end(lv);
+        if (warp == 0) {
+          for (int l = lv; l < end; ++l) {
+            const int j = lvc[lvp[l]];
+            FT part = 0;
+            for (int u = ukp[j] + lane; u < ukp[j + 1]; u += 32)
+              part += lval[ukpos[u]] * Yv[ukc[u]];
+            part = warp_sum(part);
+            if (lane == 0) Yv[j] = (Yv[j] - part) / lval[colp[j]];
+            __syncwarp();
+          }
+        }
+        lv = end;
+      } else {
+        for (int a = a0 + tid; a < a1; a += BLOCK) {
+          const int j = lvc[a];
+          FT b = Yv[j];
+          for (int u = ukp[j]; u < ukp[j + 1]; ++u) b -= lval[ukpos[u]] * Yv[ukc[u]];
+          Yv[j] = b / lval[colp[j]];
+        }
+        ++lv;
+      }
+      __syncthreads();
+    }
+    for (int lv = lv1 - 1; lv >= lv0;) {
+      const int a0 = lvp[lv], a1 = lvp[lv + 1];
+      if (a1 - a0 == 1) {
+        int begin = lv;  // the run of one-column levels ending at lv
+        while (begin > lv0 && lvp[begin] - lvp[begin - 1] == 1) --begin;
+        if (warp == 0) {
+          for (int l = lv; l >= begin; --l) {
+            const int j = lvc[lvp[l]];
+            const int cj = colp[j], len = colp[j + 1] - cj;
+            FT part = 0;
+            for (int t = 1 + lane; t < len; t += 32) part += lval[cj + t] * Xv[lrow[cj + t]];
+            part = warp_sum(part);
+            if (lane == 0) Xv[j] = (Yv[j] - part) / lval[cj];
+            __syncwarp();
+          }
+        }
+        lv = begin - 1;
+      } else {
+        for (int a = a0 + tid; a < a1; a += BLOCK) {
+          const int j = lvc[a];
+          const int cj = colp[j], len = colp[j + 1] - cj;
+          FT x = Yv[j];
+          for (int t = 1; t < len; ++t) x -= lval[cj + t] * Xv[lrow[cj + t]];
+          Xv[j] = x / lval[cj];
+        }
+        --lv;
+      }
+      __syncthreads();
+    }
+  }
+};
+
 // Each world's factor values, solve vectors and plan are copied to dynamic shared memory once per
 // launch when they fit (`smem_bytes`): all of it, or all but the relative positions; otherwise the
 // world works from global memory. The choice is per world (uniform within its CTA).
@@ -308,8 +434,6 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   __shared__ double sRed[(BLOCK / 32) * 16];
   __shared__ unsigned int sBits;
   const int w = blockIdx.x, tid = threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  constexpr int WARPS = BLOCK / 32;
   const int c0 = T.cell_offset[w], nc = T.cell_offset[w + 1] - c0;
   const int e0 = T.edge_offset[w], ne = T.edge_offset[w + 1] - e0;
   const long long C = T.C, E = T.E, W = T.W;
@@ -385,122 +509,10 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   int taken = 0;
   uint32_t refused = 0u;
 
-  // One column of the left-looking factor, by one warp: its update terms in ascending k (each
-  // term's rows at their precomputed offsets in the column), the pivot, the scaling.
-  auto factor_column = [&](int j) -> uint32_t {
-    uint32_t bad = 0;
-    const int cj = colp[j];
-    for (int u = ukp[j]; u < ukp[j + 1]; ++u) {
-      const int kk = ukc[u], p = ukpos[u], r0 = ukrel[u];
-      const int cnt = colp[kk + 1] - p;
-      const FT ljk = lval[p];
-      for (int t = lane; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
-      __syncwarp();
-    }
-    FT piv = 0;
-    if (lane == 0) {
-      const FT d = lval[cj];
-      if (!(d > 0.0) || !is_finite(d)) bad = 1u;
-      piv = sqrt(d);
-      lval[cj] = piv;
-    }
-    piv = __shfl_sync(0xffffffffu, piv, 0);
-    const FT inv = FT(1) / piv;
-    const int len = colp[j + 1] - cj;
-    for (int t = 1 + lane; t < len; t += 32) lval[cj + t] *= inv;
-    __syncwarp();
-    return bad;
-  };
-  // The end of the run of one-column levels starting at lv (uniform across the CTA).
-  auto single_run_end = [&](int lv) {
-    int end = lv;
-    while (end < lv1 && lvp[end + 1] - lvp[end] == 1) ++end;
-    return end;
-  };
-  // Left-looking factor of the world's pattern, level by level; a warp per column; a run of
-  // one-column levels (the top separator's chain) by warp 0 alone, with warp syncs only.
-  auto factor = [&]() {
-    uint32_t bad = 0;
-    for (int lv = lv0; lv < lv1;) {
-      const int a0 = lvp[lv], a1 = lvp[lv + 1];
-      if (a1 - a0 == 1) {
-        const int end = single_run_end(lv);
-        if (warp == 0)
-          for (int l = lv; l < end; ++l) bad |= factor_column(lvc[lvp[l]]);
-        lv = end;
-      } else {
-        for (int a = a0 + warp; a < a1; a += WARPS) bad |= factor_column(lvc[a]);
-        ++lv;
-      }
-      __syncthreads();
-    }
-    return bad;
-  };
-  // Forward and back substitution of L L^T x = b (b in Yv, x to Xv, position-indexed): a thread
-  // per column, or for a run of one-column levels warp 0 with the dot products across its lanes
-  // (a fixed xor tree).
-  auto warp_sum = [&](FT v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-  };
-  auto solve = [&]() {
-    for (int lv = lv0; lv < lv1;) {
-      const int a0 = lvp[lv], a1 = lvp[lv + 1];
-      if (a1 - a0 == 1) {
-        const int end = single_run_end(lv);
-        if (warp == 0) {
-          for (int l = lv; l < end; ++l) {
-            const int j = lvc[lvp[l]];
-            FT part = 0;
-            for (int u = ukp[j] + lane; u < ukp[j + 1]; u += 32)
-              part += lval[ukpos[u]] * Yv[ukc[u]];
-            part = warp_sum(part);
-            if (lane == 0) Yv[j] = (Yv[j] - part) / lval[colp[j]];
-            __syncwarp();
-          }
-        }
-        lv = end;
-      } else {
-        for (int a = a0 + tid; a < a1; a += BLOCK) {
-          const int j = lvc[a];
-          FT b = Yv[j];
-          for (int u = ukp[j]; u < ukp[j + 1]; ++u) b -= lval[ukpos[u]] * Yv[ukc[u]];
-          Yv[j] = b / lval[colp[j]];
-        }
-        ++lv;
-      }
-      __syncthreads();
-    }
-    for (int lv = lv1 - 1; lv >= lv0;) {
-      const int a0 = lvp[lv], a1 = lvp[lv + 1];
-      if (a1 - a0 == 1) {
-        int begin = lv;  // the run of one-column levels ending at lv
-        while (begin > lv0 && lvp[begin] - lvp[begin - 1] == 1) --begin;
-        if (warp == 0) {
-          for (int l = lv; l >= begin; --l) {
-            const int j = lvc[lvp[l]];
-            const int cj = colp[j], len = colp[j + 1] - cj;
-            FT part = 0;
-            for (int t = 1 + lane; t < len; t += 32) part += lval[cj + t] * Xv[lrow[cj + t]];
-            part = warp_sum(part);
-            if (lane == 0) Xv[j] = (Yv[j] - part) / lval[cj];
-            __syncwarp();
-          }
-        }
-        lv = begin - 1;
-      } else {
-        for (int a = a0 + tid; a < a1; a += BLOCK) {
-          const int j = lvc[a];
-          const int cj = colp[j], len = colp[j + 1] - cj;
-          FT x = Yv[j];
-          for (int t = 1; t < len; ++t) x -= lval[cj + t] * Xv[lrow[cj + t]];
-          Xv[j] = x / lval[cj];
-        }
-        --lv;
-      }
-      __syncthreads();
-    }
-  };
+  const WorldCholesky<FT, BLOCK> chol{colp, lrow, ukp, ukc, ukpos, ukrel, rel, lvp, lvc,
+                                       lval, Yv, Xv, lv0, lv1};
+  auto factor = [&]() { return chol.factor(); };
+  auto solve = [&]() { chol.solve(); };
   // A cell's gather over its junctions (senders first, then receivers, edge order) of field f.
   auto gather = [&](long long gi, int f, double (&send)[3], double (&recv)[3]) {
 #pragma unroll
@@ -1136,6 +1148,680 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// ROS2 (CB_METHOD_ROS2, this library's cells_b200.solver.ros2_verwer@1; the reference has no
+// Rosenbrock method on its tissue path): Verwer, Spee, Blom and Hundsdorfer's two-stage,
+// second-order, L-stable scheme, gamma = 1 + 1/sqrt(2),
+//   W k1 = F(y),  W k2 = F(y + h k1) - 2 k1,  y' = y + (3/2) h k1 + (1/2) h k2,  W = I - gamma h J,
+// the stage structure of the reference's only Rosenbrock integrator (numerics/
+// rosenbrock_dense.py:123-141) on the held-bath step's whole right-hand side F (the readouts'
+// derivative, models/surface_kinetic.py:221-410). J, fixed at y for the step: every route's slope
+// conductance dJ/d(dv) (N2's route_slope) through each cell's dV/dn_s = z_s F/C, applied alike to
+// the amounts and to every ledger whose rate is a route flux (so the ledgers balance to rounding);
+// each gate's relaxation rate on the diagonal and, for channel gates, d/dV of (target - g)/tau;
+// nothing for the pump. W k = r then reduces per world to (C + gamma h G) u = K sum_s z_s r_s in
+// the cells' voltage rates u (G the conductance Laplacian of N2's operator, the bath held: the
+// same sparse factor plan), after which a route's rate is r + gamma h W du and a gate's
+// (r + gamma h dg'/dV u) / (1 + gamma h lambda). One factorisation and two solves per step.
+
+// Cell scratch ([field][C]).
+enum R2Cell {
+  RC_CX = 0,    // 3: the evaluated state's concentrations
+  RC_LX = 3,    // 3: their logs
+  RC_VX = 6,    // its potential
+  RC_WM = 7,    // 3: patch slopes W (fmol/s per V) at the step start
+  RC_MD = 10,   // the operator's diagonal M_ii
+  RC_S = 11,    // Jacobi scale 1/sqrt(M_ii)
+  RC_JM0 = 12,  // 3: the start's patch fluxes
+  RC_MU0 = 15,  // 3: the start's patch electrochemical differences
+  RC_R = 18,    // 10: the evaluation's right-hand side: n[3], mt[3], md, cycles, pd, mw
+  RC_K = 28,    // 10: k1 of those rows, then the step's new values
+  RC_U = 38,    // the voltage rate u
+  RC_YV = 39,   // forward solve (position-indexed)
+  RC_XV = 40,   // back solve (position-indexed)
+  RC_CH = 41    // per channel slot q: R2ChField
+};
+enum R2ChField {
+  RH_W = 0,     // slope at the start
+  RH_J0 = 1,    // flux at the start
+  RH_DEC = 2,   // 2: each gate row's relaxation rate 1/tau at the start (0: no law)
+  RH_CPL = 4,   // 2: d/dV of (target - g)/tau at the start
+  RH_R = 6,     // 4: the evaluation's gate rates m, h, transferred, dissipated
+  RH_K = 10,    // 4: k1 of those rows, then the new values
+  RH_FIELDS = 14
+};
+__host__ __device__ constexpr int ros2_cell_fields(int nch) { return RC_CH + RH_FIELDS * nch; }
+// Junction scratch ([field][E]).
+enum R2Edge {
+  RE_J = 0,     // 3: fluxes for the cells' gather (the evaluation's, then the corrections)
+  RE_W = 3,     // 3: slopes at the start
+  RE_G = 6,     // conductance
+  RE_JJ0 = 7,   // 3: the start's fluxes
+  RE_MU0 = 10,  // 3: the start's electrochemical differences
+  RE_DEC = 13,  // the gate law's relaxation rate alpha + beta at the start
+  RE_R = 14,    // 5: the evaluation's jt[3], jd, gate rate
+  RE_K = 19,    // 5: k1 of those rows, then the new values
+  RE_FIELDS = 24
+};
+
+template <int BLOCK, int NCH, int MINB, bool RK4>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    ros2_kernel(const Tissue T, const Layout L, const N2Dev D, const double *state_in,
+                double *state_out, const double *__restrict__ control, const StepCoef k,
+                int n_steps, uint32_t *__restrict__ world_status,
+                int32_t *__restrict__ accepted_steps, size_t smem_bytes) {
+  extern __shared__ double n2_smem[];
+  constexpr int NQ = NCH > 0 ? NCH : 1;
+  __shared__ double sW[WC_STRIDE];
+  __shared__ double sRed[(BLOCK / 32) * 16];
+  __shared__ unsigned int sBits;
+  const int w = blockIdx.x, tid = threadIdx.x;
+  const int c0 = T.cell_offset[w], nc = T.cell_offset[w + 1] - c0;
+  const int e0 = T.edge_offset[w], ne = T.edge_offset[w + 1] - e0;
+  const long long C = T.C, E = T.E, W = T.W;
+  if (tid < WC_STRIDE) sW[tid] = T.world[(size_t)w * WC_STRIDE + tid];
+  if (tid == 0) sBits = 0u;
+  double *cs = D.cs;
+  double *es = D.es;
+  // The world's factor plan (local indices), factor values and solve vectors (by position),
+  // staged into shared memory as n2_kernel stages them.
+  const int wF = D.fb[w + 1] - D.fb[w];
+  const int wU = D.ub[w + 1] - D.ub[w];
+  const int wR = D.rb[w + 1] - D.rb[w];
+  const int wL = D.lb[w + 1] - D.lb[w];
+  const int wn = nc;
+  const int *colp = D.colp + c0 + w, *lrow = D.lrow + D.fb[w];
+  const int *ukp = D.uk_ptr + c0 + w, *ukc = D.uk_col + D.ub[w];
+  const int *ukpos = D.uk_pos + D.ub[w], *ukrel = D.uk_rel + D.ub[w];
+  const int *rel = D.rel + D.rb[w];
+  const int *lvp = D.lv_ptr + D.lb[w] + w, *lvc = D.lv_cols + c0;
+  double *lval = D.lval + D.fb[w];
+  double *Yv = cs + (long long)RC_YV * C + c0;
+  double *Xv = cs + (long long)RC_XV * C + c0;
+  const size_t values = sizeof(double) * (size_t)(wF + 2 * wn);
+  const size_t plan_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wF + 3 * wU + wL + 1 + wn);
+  const int mode = values + plan_ints + sizeof(int) * (size_t)wR <= smem_bytes ? 2
+                   : values + plan_ints <= smem_bytes                           ? 1
+                                                                                : 0;
+  if (mode > 0) {
+    lval = n2_smem;
+    Yv = lval + wF;
+    Xv = Yv + wn;
+    int *si = reinterpret_cast<int *>(Xv + wn);
+    auto stage_ints = [&](const int *src, int count) {
+      for (int i = threadIdx.x; i < count; i += BLOCK) si[i] = src[i];
+      const int *out = si;
+      si += count;
+      return out;
+    };
+    colp = stage_ints(colp, wn + 1);
+    lrow = stage_ints(lrow, wF);
+    ukp = stage_ints(ukp, wn + 1);
+    ukc = stage_ints(ukc, wU);
+    ukpos = stage_ints(ukpos, wU);
+    ukrel = stage_ints(ukrel, wU);
+    lvp = stage_ints(lvp, wL + 1);
+    lvc = stage_ints(lvc, wn);
+    if (mode == 2) rel = stage_ints(rel, wR);
+  }
+  const WorldCholesky<double, BLOCK> chol{colp, lrow, ukp, ukc, ukpos, ukrel, rel, lvp, lvc,
+                                          lval, Yv, Xv, 0, wL};
+  const long long oN = L.s[CB_AMOUNT_INCREMENT], oG = L.s[CB_JUNCTION_GATE];
+  const long long oH = L.s[CB_CHANNEL_GATE];
+  const double *mctl = control + L.c[CB_CONTROL_MEMBRANE];
+  const double *pctlp = control + L.c[CB_CONTROL_PUMP];
+  const double *jctl = control + L.c[CB_CONTROL_JUNCTION];
+  const double *chctl0 = control + L.c[CB_CONTROL_CHANNEL];
+  const double Kc = kChargePerFmol;
+  const double h = k.dt;
+  const double gh = (1.0 + 1.0 / sqrt(2.0)) * h;  // gamma h
+  auto CF = [&](int f, long long gi) -> double & { return cs[(long long)f * C + gi]; };
+  auto EF = [&](int f, long long ge) -> double & { return es[(long long)f * E + ge]; };
+  auto CH = [&](int q, int f, long long gi) -> double & {
+    return cs[(long long)(RC_CH + q * RH_FIELDS + f) * C + gi];
+  };
+  __syncthreads();
+  const double Vb = sW[WC_VB];
+  // The ledger fields of a cell's k / new-value rows (RC_K + f) in the state layout.
+  const int kCellField[10] = {CB_AMOUNT_INCREMENT, CB_AMOUNT_INCREMENT, CB_AMOUNT_INCREMENT,
+                              CB_MEMBRANE_TRANSFERRED, CB_MEMBRANE_TRANSFERRED,
+                              CB_MEMBRANE_TRANSFERRED, CB_MEMBRANE_DISSIPATED, CB_PUMP_CYCLES,
+                              CB_PUMP_DISSIPATED, CB_METABOLIC_WORK};
+  auto cell_state = [&](const double *src, int f, long long gi) {
+    return src[L.s[kCellField[f]] + (f < 6 ? (f % 3) * C : 0) + gi];
+  };
+  auto edge_state = [&](const double *src, int f, long long ge) {
+    return f < 3 ? src[L.s[CB_JUNCTION_TRANSFERRED] + f * E + ge]
+           : f == 3 ? src[L.s[CB_JUNCTION_DISSIPATED] + ge]
+                    : src[oG + ge];
+  };
+  auto chan_state = [&](const double *src, int q, int f, long long gi) {
+    return f < 2 ? src[oH + (f * NCH + q) * C + gi]
+           : f == 2 ? src[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi]
+                    : src[L.s[CB_CHANNEL_DISSIPATED] + q * C + gi];
+  };
+  auto gather = [&](long long gi, int f, double (&send)[3], double (&recv)[3]) {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) send[s] = recv[s] = 0.0;
+    for (int a = __ldg(T.adj_ptr + gi); a < __ldg(T.adj_ptr + gi + 1); ++a) {
+      const int code = __ldg(T.adj_idx + a);
+      const long long ge = e0 + (code >> 1);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        if (code & 1) recv[s] += EF(f + s, ge);
+        else send[s] += EF(f + s, ge);
+      }
+    }
+  };
+  auto potential_of = [&](long long gi, const double (&n)[3]) {
+    return (__ldg(T.q0 + gi) + Kc * ((n[0] + n[1]) + (-n[2]))) * __ldg(T.icap + gi) + Vb;
+  };
+  double res[3], ec, rw, ew;
+  for (int s = 0; s < 3; ++s) res[s] = state_in[L.s[CB_RESERVOIR_SUPPLIED] + s * W + w];
+  ec = state_in[L.s[CB_ELECTRODE_CHARGE] + w];
+  rw = state_in[L.s[CB_RESERVOIR_WORK] + w];
+  ew = state_in[L.s[CB_ELECTRODE_WORK] + w];
+  const double *cur = state_in;
+  int taken = 0;
+  uint32_t refused = 0u;
+
+  // The rows that give a stage's state: ROS2's k1, or RK4's previous evaluation.
+  constexpr int kCell = RK4 ? RC_R : RC_K, kChan = RK4 ? RH_R : RH_K, kEdge = RK4 ? RE_R : RE_K;
+  // The evaluated state of a cell: y + (c h) k (c = 0 at the step's start).
+  auto cell_amounts = [&](double c, long long gi, double (&n)[3]) {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      n[s] = cur[oN + s * C + gi];
+      if (c != 0.0) n[s] = n[s] + (c * h) * CF(kCell + s, gi);
+    }
+  };
+  // Right-hand side r at stage st of the state y + (c h) k for every row (ROS2: r = F(y) at
+  // st = 0, F(y + h k1) - 2 k1 at st = 1; RK4: r = F), its validity bits, and the world sums it
+  // needs: v[0..2] the bath inflow, v[3] the cells' charge rate. At ROS2's st = 0 also the
+  // start's slopes, kinetics and the operator's entries.
+  auto evaluate = [&](int st, double c_stage, double (&v)[4]) -> uint32_t {
+    uint32_t bits = 0;
+    const bool sub = !RK4 && st;      // r = F - 2 k1
+    const bool start = !RK4 && !st;   // the start's slopes and operator
+    for (int q = 0; q < 4; ++q) v[q] = 0.0;
+    // Cells: concentrations, potential, own rates (patch, pump, channels), gate rates.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      double n[3], c[3], lc[3], gl[2 * NQ];
+      cell_amounts(c_stage, gi, n);
+      const double V = potential_of(gi, n);
+      const double ivol = __ldg(T.ivol + gi);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        c[s] = (__ldg(T.ref + s * C + gi) + n[s]) * ivol;
+        lc[s] = log(c[s]);
+        CF(RC_CX + s, gi) = c[s];
+        CF(RC_LX + s, gi) = lc[s];
+      }
+      CF(RC_VX, gi) = V;
+      for (int q = 0; q < NCH; ++q)
+        for (int r = 0; r < 2; ++r) {
+          double g = cur[oH + (r * NCH + q) * C + gi];
+          if (c_stage != 0.0) g = g + (c_stage * h) * CH(q, kChan + r, gi);
+          gl[r * NQ + q] = g;
+          if (!(is_finite(g) && g >= 0.0 && g <= 1.0)) bits |= CB_WORLD_DOMAIN;
+        }
+      const double mc = mctl[gi], pctl = pctlp[gi];
+      const double ldc = pctl > 0.0 ? __ldg(T.logpcap + gi) + log(pctl) : 0.0;
+      double jm[3], ex[3], r4[4], chj[NQ], chd[NQ];
+      bits |= own_rates<NCH>(T, sW, gi, c, lc, V, gl, 1, NQ, mc, pctl, ldc, chctl0 + gi, jm, ex,
+                             r4, chj, chd);
+      const double dv = V - Vb;
+      for (int s = 0; s < 3; ++s) {
+        v[s] += jm[s] + ex[s];
+        CF(RC_R + s, gi) = ex[s];  // the amounts' rate follows in the gather pass
+        CF(RC_R + 3 + s, gi) = sub ? jm[s] - 2.0 * CF(RC_K + 3 + s, gi) : jm[s];
+      }
+      for (int f = 0; f < 4; ++f)
+        CF(RC_R + 6 + f, gi) = sub ? r4[f] - 2.0 * CF(RC_K + 6 + f, gi) : r4[f];
+      for (int q = 0; q < NCH; ++q) {
+        const int code = __ldg(T.ch_code + q * C + gi);
+        double t[2], tau[2];
+        channel_kinetics<false>(code, dv, t, tau);
+        if (!channel_kinetics_ok(dv, t, tau)) bits |= CB_WORLD_CHANNEL_DOMAIN;
+        // Gate rates (target - g)/tau of the rows with a law (HH K's h row has none).
+        const double rr[4] = {(t[0] - gl[q]) / tau[0],
+                              code == kHhKn4 ? 0.0 : (t[1] - gl[NQ + q]) / tau[1], chj[q],
+                              chd[q]};
+        for (int f = 0; f < 4; ++f)
+          CH(q, RH_R + f, gi) = sub ? rr[f] - 2.0 * CH(q, RH_K + f, gi) : rr[f];
+        if (start) {
+          double dtg[2], dtau[2];
+          channel_slope(code, dv, dtg, dtau);
+          for (int r = 0; r < 2; ++r) {
+            const bool live = !(r == 1 && code == kHhKn4);
+            const double cpl = dtg[r] / tau[r] - (t[r] - gl[r * NQ + q]) * dtau[r] / (tau[r] * tau[r]);
+            CH(q, RH_DEC + r, gi) = live ? 1.0 / tau[r] : 0.0;
+            CH(q, RH_CPL + r, gi) = live && is_finite(cpl) ? cpl : 0.0;
+          }
+          CH(q, RH_J0, gi) = chj[q];
+        }
+      }
+      if (start) {
+        // The start's slopes (N2's route_slope at y), fluxes and differences for the heat rows;
+        // the patch conductance into RC_MD until the operator pass.
+        double mu[3], zw[3];
+        patch_mu(sW, lc, dv, mu);
+        for (int s = 0; s < 3; ++s) {
+          const double zfrt = (s < 2 ? 1.0 : -1.0) * sW[WC_FRT];
+          const double W_ = route_slope(__ldg(T.ap + s * C + gi) * mc, c[s], sW[WC_CO + s], dv,
+                                        zfrt);
+          CF(RC_WM + s, gi) = W_;
+          CF(RC_JM0 + s, gi) = jm[s];
+          CF(RC_MU0 + s, gi) = mu[s];
+          zw[s] = (s < 2 ? 1.0 : -1.0) * W_;
+          if (!is_finite(W_)) bits |= CB_WORLD_OPERATOR;
+        }
+        double gp = Kc * ((zw[0] + zw[1]) + zw[2]);
+        if constexpr (NCH > 0) {
+          double extra = 0.0;
+          for (int q = 0; q < NCH; ++q) {
+            const int code = __ldg(T.ch_code + q * C + gi);
+            const int sp = __ldg(T.ch_species + q * C + gi);
+            const double available =
+                (__ldg(T.ch_ab + q * C + gi) * channel_opening(code, gl[q], gl[NQ + q])) *
+                __ldg(chctl0 + q * C + gi);
+            const double zfrt = (sp < 2 ? 1.0 : -1.0) * sW[WC_FRT];
+            const double W_ = route_slope(__ldg(T.ch_ap + q * C + gi) * available, c[sp],
+                                          sW[WC_CO + sp], dv, zfrt);
+            CH(q, RH_W, gi) = W_;
+            if (!is_finite(W_)) bits |= CB_WORLD_OPERATOR;
+            extra = extra + Kc * ((sp < 2 ? 1.0 : -1.0) * W_);
+          }
+          gp = gp + extra;
+        }
+        CF(RC_MD, gi) = gp;
+        const int P = __ldg(D.rank + gi);
+        for (int f = colp[P]; f < colp[P + 1]; ++f) lval[f] = 0.0;
+      }
+    }
+    __syncthreads();
+    // Junctions: fluxes, heat, the gate law's rate; at st = 0 the start's slopes and kinetics.
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      const long long ga = c0 + __ldg(T.snd + ge), gb = c0 + __ldg(T.rcv + ge);
+      double ca[3], cb[3], la[3], lb[3], jj[3], jd;
+      for (int s = 0; s < 3; ++s) {
+        ca[s] = CF(RC_CX + s, ga);
+        cb[s] = CF(RC_CX + s, gb);
+        la[s] = CF(RC_LX + s, ga);
+        lb[s] = CF(RC_LX + s, gb);
+      }
+      const double dv = CF(RC_VX, ga) - CF(RC_VX, gb);
+      double g = cur[oG + ge];
+      if (c_stage != 0.0) g = g + (c_stage * h) * EF(kEdge + 4, ge);
+      const double jc = jctl[ge];
+      bits |= junction_flux(T, sW, ge, ca, cb, la, lb, dv, jc * g, jj, jd);
+      const double thr = __ldg(T.thr + ge), mn = __ldg(T.jmin + ge);
+      if (!gate_domain(g, dv, thr, mn, jc)) bits |= CB_WORLD_GATE_DOMAIN;
+      // junction_voltage_relaxation's rate; pinned gates (minimum 1) exactly 0.
+      double gr = 0.0, relax = 0.0;
+      if (mn < 1.0) {
+        const double shift = fabs(dv) - thr;
+        const double alpha = 1.3 * exp(-77.0 * shift);
+        const double log_beta = kLog0065 + 140.0 * shift;
+        const double beta = 20.0 * exp(-logaddexp0(-log_beta));
+        gr = alpha * (1.0 - g) - beta * (g - mn);
+        relax = alpha + beta;
+      }
+      if (!is_finite(gr)) bits |= CB_WORLD_TRANSPORT;
+      const double rr[5] = {jj[0], jj[1], jj[2], jd, gr};
+      for (int s = 0; s < 3; ++s) EF(RE_J + s, ge) = jj[s];
+      for (int f = 0; f < 5; ++f) EF(RE_R + f, ge) = sub ? rr[f] - 2.0 * EF(RE_K + f, ge) : rr[f];
+      if (start) {
+        double mu[3], zw[3];
+        junction_mu(sW, la, lb, dv, mu);
+        for (int s = 0; s < 3; ++s) {
+          const double zfrt = (s < 2 ? 1.0 : -1.0) * sW[WC_FRT];
+          const double W_ = route_slope(__ldg(T.jap + s * E + ge) * (jc * g), ca[s], cb[s], dv,
+                                        zfrt);
+          EF(RE_W + s, ge) = W_;
+          EF(RE_JJ0 + s, ge) = jj[s];
+          EF(RE_MU0 + s, ge) = mu[s];
+          zw[s] = (s < 2 ? 1.0 : -1.0) * W_;
+          if (!is_finite(W_)) bits |= CB_WORLD_OPERATOR;
+        }
+        EF(RE_G, ge) = Kc * ((zw[0] + zw[1]) + zw[2]);
+        EF(RE_DEC, ge) = is_finite(relax) ? relax : 0.0;
+      }
+    }
+    __syncthreads();
+    // Cells: the amounts' rate (own parts, then the junctions in edge order), the charge rate
+    // and the scaled right-hand side of the voltage solve; at st = 0 the operator's diagonal.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      double send[3], recv[3], r[3];
+      gather(gi, RE_J, send, recv);
+      for (int s = 0; s < 3; ++s) {
+        // the patch flux J_m (RC_R + 3 holds J_m - 2 k1 at st = 1)
+        const double jm = sub ? CF(RC_R + 3 + s, gi) + 2.0 * CF(RC_K + 3 + s, gi)
+                              : CF(RC_R + 3 + s, gi);
+        const double whole = ((-jm + (-send[s])) + recv[s]) - CF(RC_R + s, gi);
+        r[s] = sub ? whole - 2.0 * CF(RC_K + s, gi) : whole;
+        CF(RC_R + s, gi) = r[s];
+        if (!is_finite(r[s])) bits |= CB_WORLD_TRANSPORT;
+      }
+      const double qdot = Kc * ((r[0] + r[1]) + (-r[2]));
+      // F's charge rate for the electrode row (r = F - 2 k1 at st = 1)
+      v[3] += sub ? Kc * (((r[0] + 2.0 * CF(RC_K, gi)) + (r[1] + 2.0 * CF(RC_K + 1, gi))) +
+                         (-(r[2] + 2.0 * CF(RC_K + 2, gi))))
+                 : qdot;
+      if (start) {
+        double gs = 0.0, gq = 0.0;
+        for (int a = __ldg(T.adj_ptr + gi); a < __ldg(T.adj_ptr + gi + 1); ++a) {
+          const int code = __ldg(T.adj_idx + a);
+          const double g = EF(RE_G, e0 + (code >> 1));
+          if (code & 1) gq += g;
+          else gs += g;
+        }
+        const double cap = 1.0 / __ldg(T.icap + gi);
+        const double mii = cap + gh * (CF(RC_MD, gi) + (gs + gq));
+        CF(RC_MD, gi) = mii;
+        if (!(mii > 0.0)) bits |= CB_WORLD_OPERATOR;
+        const double sc = 1.0 / sqrt(mii > 0.0 ? mii : 1.0);
+        CF(RC_S, gi) = sc;
+        lval[colp[__ldg(D.rank + gi)]] = (mii * sc) * sc;
+      }
+      if (!RK4) Yv[__ldg(D.rank + gi)] = qdot * CF(RC_S, gi);
+    }
+    __syncthreads();
+    if (start) {
+      // Junctions: the operator's off-diagonal entries, scaled (row then column).
+      for (int e = tid; e < ne; e += BLOCK) {
+        const long long ge = e0 + e;
+        const long long ga = c0 + __ldg(T.snd + ge), gb = c0 + __ldg(T.rcv + ge);
+        const int ra = __ldg(D.rank + ga), rb = __ldg(D.rank + gb);
+        const double m = 0.0 + gh * (-EF(RE_G, ge));
+        const double s_row = ra > rb ? CF(RC_S, ga) : CF(RC_S, gb);
+        const double s_col = ra > rb ? CF(RC_S, gb) : CF(RC_S, ga);
+        lval[__ldg(D.edge_pos + ge)] = (m * s_row) * s_col;
+      }
+      __syncthreads();
+    }
+    return bits;
+  };
+  // k = W^-1 r after the voltage solve: u, each route's rate r + gamma h W du, the heat rows
+  // through W du mu + J z F du at the start, the gates' (r + gamma h dg'/dV u)/(1 + gamma h
+  // lambda), the pump's k = r. st = 0 keeps k1; st = 1 writes the step's new values
+  // y + 3/2 h k1 + 1/2 h k2 over it. v[0..2]: the bath's correction sum of the patches' route
+  // corrections, v[3] the cells' charge correction.
+  auto correct = [&](int st, double (&v)[4]) -> uint32_t {
+    uint32_t bits = 0;
+    for (int q = 0; q < 4; ++q) v[q] = 0.0;
+    chol.solve();
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      const double u = Xv[__ldg(D.rank + gi)] * CF(RC_S, gi);
+      CF(RC_U, gi) = u;
+      if (!is_finite(u)) bits |= CB_WORLD_RESIDUAL;
+    }
+    __syncthreads();
+    auto finish = [&](double r, double &kslot, double y) {
+      const double kv = r;
+      if (st == 0) {
+        kslot = kv;
+      } else {
+        kslot = (y + (1.5 * h) * kslot) + (0.5 * h) * kv;
+      }
+    };
+    // Junctions: route corrections W du (for the cells' gather), transfers, heat, gate.
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      const long long ga = c0 + __ldg(T.snd + ge), gb = c0 + __ldg(T.rcv + ge);
+      const double du = CF(RC_U, ga) - CF(RC_U, gb);
+      double dj[3], hm[3];
+      for (int s = 0; s < 3; ++s) {
+        dj[s] = EF(RE_W + s, ge) * du;
+        EF(RE_J + s, ge) = dj[s];
+        hm[s] = dj[s] * EF(RE_MU0 + s, ge) + EF(RE_JJ0 + s, ge) * ((s < 2 ? kF : -kF) * du);
+      }
+      const double heat = 1e-3 * ((hm[0] + hm[1]) + hm[2]);
+      double kv[5];
+      for (int s = 0; s < 3; ++s) kv[s] = EF(RE_R + s, ge) + gh * dj[s];
+      kv[3] = EF(RE_R + 3, ge) + gh * heat;
+      kv[4] = EF(RE_R + 4, ge) / (1.0 + gh * EF(RE_DEC, ge));
+      for (int f = 0; f < 5; ++f) {
+        if (!is_finite(kv[f])) bits |= CB_WORLD_TRANSPORT;
+        finish(kv[f], EF(RE_K + f, ge), st ? edge_state(cur, f, ge) : 0.0);
+      }
+    }
+    __syncthreads();
+    // Cells: the amounts through the patches' and junctions' corrections (route_rates' order:
+    // receivers less senders less patches), the patch ledgers, the pump's rows, the channels.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      const double u = CF(RC_U, gi);
+      double send[3], recv[3], dm[3], pm[3], hm[3];
+      gather(gi, RE_J, send, recv);
+      for (int s = 0; s < 3; ++s) {
+        dm[s] = CF(RC_WM + s, gi) * u;
+        pm[s] = dm[s];
+        hm[s] = dm[s] * CF(RC_MU0 + s, gi) + CF(RC_JM0 + s, gi) * ((s < 2 ? kF : -kF) * u);
+      }
+      double kch[NQ][4];
+      for (int q = 0; q < NCH; ++q) {
+        const int sp = __ldg(T.ch_species + q * C + gi);
+        const double dc = CH(q, RH_W, gi) * u;
+        pm[sp] = pm[sp] + dc;
+        const double zf = sp < 2 ? kF : -kF;
+        const double musp = CF(RC_MU0 + sp, gi);
+        for (int r = 0; r < 2; ++r)
+          kch[q][r] = (CH(q, RH_R + r, gi) + gh * (CH(q, RH_CPL + r, gi) * u)) /
+                      (1.0 + gh * CH(q, RH_DEC + r, gi));
+        kch[q][2] = CH(q, RH_R + 2, gi) + gh * dc;
+        kch[q][3] = CH(q, RH_R + 3, gi) + gh * (1e-3 * (dc * musp + CH(q, RH_J0, gi) * (zf * u)));
+      }
+      double kv[10], corr[3];
+      for (int s = 0; s < 3; ++s) {
+        corr[s] = (recv[s] - send[s]) - pm[s];
+        kv[s] = CF(RC_R + s, gi) + gh * corr[s];
+        kv[3 + s] = CF(RC_R + 3 + s, gi) + gh * dm[s];
+        v[s] += pm[s];
+      }
+      v[3] += Kc * ((corr[0] + corr[1]) + (-corr[2]));
+      kv[6] = CF(RC_R + 6, gi) + gh * (1e-3 * ((hm[0] + hm[1]) + hm[2]));
+      for (int f = 7; f < 10; ++f) kv[f] = CF(RC_R + f, gi);
+      for (int f = 0; f < 10; ++f) {
+        if (!is_finite(kv[f])) bits |= CB_WORLD_TRANSPORT;
+        finish(kv[f], CF(RC_K + f, gi), st ? cell_state(cur, f, gi) : 0.0);
+      }
+      for (int q = 0; q < NCH; ++q)
+        for (int f = 0; f < 4; ++f) {
+          if (!is_finite(kch[q][f])) bits |= CB_WORLD_TRANSPORT;
+          finish(kch[q][f], CH(q, RH_K + f, gi), st ? chan_state(cur, q, f, gi) : 0.0);
+        }
+    }
+    __syncthreads();
+    return bits;
+  };
+  // The world rows (bath supply [3], electrode charge, reservoir work, electrode work): F's
+  // from an evaluation's sums (the supply -inflow, the electrode -sum of the cells' charge
+  // rates, the works 1e-3 mu_bath . supply and 1e12 V_bath electrode), and their correction
+  // rows from the corrections' sums, the same linear maps.
+  const double mub[3] = {sW[WC_MUB], sW[WC_MUB + 1], sW[WC_MUB + 2]};
+  auto world_map = [&](const double (&v)[4], double (&out)[6]) {
+    for (int s = 0; s < 3; ++s) out[s] = -v[s];
+    out[3] = -v[3];
+    out[4] = 1e-3 * ((mub[0] * out[0] + mub[1] * out[1]) + mub[2] * out[2]);
+    out[5] = (1e12 * Vb) * out[3];
+  };
+
+  // RK4: the evaluation's rows into the running sum k1 + 2 k2 + 2 k3 + k4 (RC_K, RH_K, RE_K).
+  auto accumulate = [&](int st, double wgt) {
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      for (int f = 0; f < 10; ++f)
+        CF(RC_K + f, gi) = st ? CF(RC_K + f, gi) + wgt * CF(RC_R + f, gi) : CF(RC_R + f, gi);
+      for (int q = 0; q < NCH; ++q)
+        for (int f = 0; f < 4; ++f)
+          CH(q, RH_K + f, gi) = st ? CH(q, RH_K + f, gi) + wgt * CH(q, RH_R + f, gi)
+                                   : CH(q, RH_R + f, gi);
+    }
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      for (int f = 0; f < 5; ++f)
+        EF(RE_K + f, ge) = st ? EF(RE_K + f, ge) + wgt * EF(RE_R + f, ge) : EF(RE_R + f, ge);
+    }
+  };
+  // RK4: the new values y + (h / 6) (k1 + 2 k2 + 2 k3 + k4) over the sum.
+  auto rk4_finish = [&]() {
+    const double h6 = h / 6.0;
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      for (int f = 0; f < 10; ++f) CF(RC_K + f, gi) = cell_state(cur, f, gi) + h6 * CF(RC_K + f, gi);
+      for (int q = 0; q < NCH; ++q)
+        for (int f = 0; f < 4; ++f)
+          CH(q, RH_K + f, gi) = chan_state(cur, q, f, gi) + h6 * CH(q, RH_K + f, gi);
+    }
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      for (int f = 0; f < 5; ++f) EF(RE_K + f, ge) = edge_state(cur, f, ge) + h6 * EF(RE_K + f, ge);
+    }
+  };
+
+  for (int step = 0; step < n_steps; ++step) {
+    uint32_t bits = 0;
+    double ve[4], vc[4], fw[6], cw[6], k1w[6], k2w[6], neww[6];
+    const double yw[6] = {res[0], res[1], res[2], ec, rw, ew};
+    if constexpr (RK4) {
+      // fixed_step.rk4_checked_step (:25-71): four evaluations at y, y + h/2 k1, y + h/2 k2,
+      // y + h k3, each of a valid trial state.
+      const double cst[4] = {0.0, 0.5, 0.5, 1.0}, wst[4] = {1.0, 2.0, 2.0, 1.0};
+      for (int st = 0; st < 4; ++st) {
+        bits |= evaluate(st, cst[st], ve);
+        block_sum<BLOCK, 4>(ve, sRed);
+        world_map(ve, fw);
+        for (int f = 0; f < 6; ++f) k1w[f] = st ? k1w[f] + wst[st] * fw[f] : fw[f];
+        accumulate(st, wst[st]);
+        __syncthreads();
+      }
+      rk4_finish();
+      __syncthreads();
+      for (int f = 0; f < 6; ++f) {
+        neww[f] = yw[f] + (h / 6.0) * k1w[f];
+        if (!is_finite(neww[f])) bits |= CB_WORLD_DOMAIN;
+      }
+      (void)vc;
+      (void)cw;
+      (void)k2w;
+    } else {
+      // Stage 1: F(y), the operator at y, k1.
+      bits |= evaluate(0, 0.0, ve);
+      block_sum<BLOCK, 4>(ve, sRed);
+      if (chol.factor()) bits |= CB_WORLD_OPERATOR;
+      bits |= correct(0, vc);
+      block_sum<BLOCK, 4>(vc, sRed);
+      world_map(ve, fw);
+      world_map(vc, cw);
+      for (int f = 0; f < 6; ++f) k1w[f] = fw[f] + gh * cw[f];
+      // Stage 2: F(y + h k1) - 2 k1 through the same factor; the new values.
+      bits |= evaluate(1, 1.0, ve);
+      block_sum<BLOCK, 4>(ve, sRed);
+      bits |= correct(1, vc);
+      block_sum<BLOCK, 4>(vc, sRed);
+      world_map(ve, fw);
+      world_map(vc, cw);
+      for (int f = 0; f < 6; ++f) {
+        k2w[f] = (fw[f] - 2.0 * k1w[f]) + gh * cw[f];
+        neww[f] = (yw[f] + (1.5 * h) * k1w[f]) + (0.5 * h) * k2w[f];
+        if (!is_finite(neww[f])) bits |= CB_WORLD_DOMAIN;
+      }
+    }
+    // The new state's domain: positive amounts, gates in range, finite ledgers.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      bool ok = true;
+      for (int f = 0; f < 10; ++f) ok = ok && is_finite(CF(RC_K + f, gi));
+      for (int s = 0; s < 3; ++s) ok = ok && (__ldg(T.ref + s * C + gi) + CF(RC_K + s, gi)) > 0.0;
+      for (int q = 0; q < NCH; ++q) {
+        for (int f = 0; f < 4; ++f) ok = ok && is_finite(CH(q, RH_K + f, gi));
+        for (int r = 0; r < 2; ++r) {
+          const double g = CH(q, RH_K + r, gi);
+          ok = ok && g >= 0.0 && g <= 1.0;
+        }
+      }
+      if (!ok) bits |= CB_WORLD_DOMAIN;
+    }
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      bool ok = true;
+      for (int f = 0; f < 5; ++f) ok = ok && is_finite(EF(RE_K + f, ge));
+      const double g = EF(RE_K + 4, ge);
+      ok = ok && g >= __ldg(T.jmin + ge) && g <= 1.0;
+      if (!ok) bits |= CB_WORLD_DOMAIN;
+    }
+    if (bits) atomicOr(&sBits, bits);
+    __syncthreads();
+    const uint32_t world_bits = sBits;
+    if (world_bits) {
+      refused = world_bits;
+      break;
+    }
+    // Commit the accepted state.
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      for (int f = 0; f < 10; ++f)
+        state_out[L.s[kCellField[f]] + (f < 6 ? (f % 3) * C : 0) + gi] = CF(RC_K + f, gi);
+      for (int q = 0; q < NCH; ++q) {
+        for (int r = 0; r < 2; ++r) state_out[oH + (r * NCH + q) * C + gi] = CH(q, RH_K + r, gi);
+        state_out[L.s[CB_CHANNEL_TRANSFERRED] + q * C + gi] = CH(q, RH_K + 2, gi);
+        state_out[L.s[CB_CHANNEL_DISSIPATED] + q * C + gi] = CH(q, RH_K + 3, gi);
+      }
+    }
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      for (int s = 0; s < 3; ++s)
+        state_out[L.s[CB_JUNCTION_TRANSFERRED] + s * E + ge] = EF(RE_K + s, ge);
+      state_out[L.s[CB_JUNCTION_DISSIPATED] + ge] = EF(RE_K + 3, ge);
+      state_out[oG + ge] = EF(RE_K + 4, ge);
+    }
+    for (int s = 0; s < 3; ++s) res[s] = neww[s];
+    ec = neww[3];
+    rw = neww[4];
+    ew = neww[5];
+    ++taken;
+    cur = state_out;
+    __syncthreads();
+  }
+  // A world refused at its first step keeps its input state.
+  if (taken == 0 && state_in != state_out) {
+    for (int i = tid; i < nc; i += BLOCK) {
+      const long long gi = c0 + i;
+      for (int f = CB_AMOUNT_INCREMENT; f <= CB_METABOLIC_WORK; ++f) {
+        const int reps = (f <= CB_MEMBRANE_TRANSFERRED) ? 3 : 1;
+        for (int s = 0; s < reps; ++s)
+          state_out[L.s[f] + s * C + gi] = state_in[L.s[f] + s * C + gi];
+      }
+      for (int f = CB_CHANNEL_GATE; f <= CB_CHANNEL_DISSIPATED; ++f) {
+        const int reps = (f == CB_CHANNEL_GATE) ? 2 * NCH : NCH;
+        for (int s = 0; s < reps; ++s)
+          state_out[L.s[f] + s * C + gi] = state_in[L.s[f] + s * C + gi];
+      }
+    }
+    for (int e = tid; e < ne; e += BLOCK) {
+      const long long ge = e0 + e;
+      for (int f = CB_JUNCTION_TRANSFERRED; f <= CB_JUNCTION_GATE; ++f) {
+        const int reps = (f == CB_JUNCTION_TRANSFERRED) ? 3 : 1;
+        for (int s = 0; s < reps; ++s)
+          state_out[L.s[f] + s * E + ge] = state_in[L.s[f] + s * E + ge];
+      }
+    }
+  }
+  if (tid == 0) {
+    for (int s = 0; s < 3; ++s) state_out[L.s[CB_RESERVOIR_SUPPLIED] + s * W + w] = res[s];
+    state_out[L.s[CB_ELECTRODE_CHARGE] + w] = ec;
+    state_out[L.s[CB_RESERVOIR_WORK] + w] = rw;
+    state_out[L.s[CB_ELECTRODE_WORK] + w] = ew;
+    world_status[w] = refused;
+    if (accepted_steps) accepted_steps[w] = taken;
+  }
+}
+
 template <typename V>
 int upload_vec(N2Plan *plan, const std::vector<V> &host, V **dst) {
   void *ptr = nullptr;
@@ -1230,9 +1916,11 @@ int build_plan(cb_tissue *t) {
   if (!rc) rc = upload_vec(plan, rb, &d.rb);
   if (!rc) rc = upload_vec(plan, lb, &d.lb);
   if (!rc) rc = upload_vec(plan, std::vector<double>((size_t)fb.back()), &d.lval);
-  if (!rc)
-    rc = upload_vec(plan, std::vector<double>((size_t)n2_cell_fields(t->t.nch) * C), &d.cs);
-  if (!rc) rc = upload_vec(plan, std::vector<double>((size_t)NE_FIELDS * std::max(E, 1LL)), &d.es);
+  // Scratch for either kernel (N2's or ROS2's fields, whichever needs more).
+  const size_t cell_fields = std::max(n2_cell_fields(t->t.nch), ros2_cell_fields(t->t.nch));
+  const size_t edge_fields = std::max<size_t>(NE_FIELDS, RE_FIELDS);
+  if (!rc) rc = upload_vec(plan, std::vector<double>(cell_fields * C), &d.cs);
+  if (!rc) rc = upload_vec(plan, std::vector<double>(edge_fields * std::max(E, 1LL)), &d.es);
   if (rc) {
     for (void *ptr : plan->owned) cudaFree(ptr);
     delete plan;
@@ -1264,9 +1952,41 @@ int launch_n2(cb_tissue *t, const double *in, double *out, const double *control
   return CB_OK;
 }
 
+template <int NCH>
+int launch_ros2(cb_tissue *t, const double *in, double *out, const double *control,
+                const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
+                cudaStream_t stream, bool rk4) {
+  const size_t smem = t->n2->smem_bytes;
+  auto kern = rk4 ? ros2_kernel<256, NCH, 1, true> : ros2_kernel<256, NCH, 1, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (ros2)");
+  kern<<<t->W, 256, smem, stream>>>(t->t, t->layout, t->n2->d, in, out, control, k, n_steps,
+                                    status, taken, smem);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "ros2 launch");
+  return CB_OK;
+}
+
 }  // namespace
 
 namespace cbk {
+
+int ros2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
+              const double *control, int n_steps, uint32_t *world_status,
+              int32_t *accepted_steps, cudaStream_t stream, bool rk4) {
+  int rc = build_plan(t);
+  if (rc) return rc;
+  const StepCoef k = step_coef(dt);
+  if (t->t.nch == 2)
+    return launch_ros2<2>(t, state_in, state_out, control, k, n_steps, world_status,
+                          accepted_steps, stream, rk4);
+  if (t->t.nch == 0)
+    return launch_ros2<0>(t, state_in, state_out, control, k, n_steps, world_status,
+                          accepted_steps, stream, rk4);
+  return fail(CB_ERR_UNSUPPORTED, "channel slots must be 0 or 2");
+}
+
 
 int n2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
             const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,

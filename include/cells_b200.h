@@ -166,6 +166,26 @@ enum cb_control_field {
  * accumulation in FP64 (this library's cells_b200.solver.imex_ars222_implicit_conductances_
  * mixed@1; no reference method). */
 #define CB_METHOD_N2_MIXED 3
+/* ROS2 (this library's cells_b200.solver.ros2_verwer@1; the reference has no Rosenbrock method
+ * on its tissue path): the two-stage, second-order, L-stable Rosenbrock method of Verwer, Spee,
+ * Blom and Hundsdorfer (gamma = 1 + 1/sqrt(2); W k1 = F(y), W k2 = F(y + h k1) - 2 k1,
+ * y' = y + 3/2 h k1 + 1/2 h k2, W = I - gamma h J), the stage structure of the reference's
+ * dense Rodas (numerics/rosenbrock_dense.py:123-141) on the held-bath step's whole right-hand
+ * side. J at y: every route's slope conductance through each cell's dV/dn = z F/C, applied alike
+ * to the amounts and the route ledgers (so the ledgers balance to rounding); each gate's
+ * relaxation rate and, for channel gates, their voltage slope; nothing for the pump. Each world's
+ * W reduces to (C + gamma h G) u = K sum_s z_s r_s in the cells' voltage rates (N2's operator
+ * pattern and sparse factor plan): one factorisation and two solves per step, one CTA per world.
+ * A world is refused (state kept) when an evaluation is invalid, the operator is not positive
+ * definite or the new state leaves the domain; no explicit-stability refusal applies. FP64. */
+#define CB_METHOD_ROS2 4
+/* The reference's reference-run method: classical RK4 over the same whole right-hand side
+ * (numerics/fixed_step.py:25-71 rk4_checked_step, taken by checked_step for an empty tableau,
+ * models/surface_pump_v3.py:3989-4001): four evaluations, each of a state that must be valid,
+ * y' = y + h/6 (k1 + 2 k2 + 2 k3 + k4) for every state field, the new state's domain checked.
+ * No explicit-stability refusal (the reference's RK4 has none). One CTA per world (ROS2's kernel
+ * without its operator). FP64. */
+#define CB_METHOD_RK4 5
 
 /*
  * Host symbolic bind (replaces initial_values' layout binding, surface_tissue.py:135-257 and
