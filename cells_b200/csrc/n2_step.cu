@@ -1957,7 +1957,10 @@ int launch_ros2(cb_tissue *t, const double *in, double *out, const double *contr
                 const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
                 cudaStream_t stream, bool rk4) {
   const size_t smem = t->n2->smem_bytes;
-  auto kern = rk4 ? ros2_kernel<256, NCH, 1, true> : ros2_kernel<256, NCH, 1, false>;
+  // Registers capped for two CTAs per SM (N2's measured choice), unless CELLS_B200_N2_MINB=1.
+  auto kern = rk4 ? ros2_kernel<256, NCH, 2, true> : ros2_kernel<256, NCH, 2, false>;
+  if (t->n2->min_blocks < 2)
+    kern = rk4 ? ros2_kernel<256, NCH, 1, true> : ros2_kernel<256, NCH, 1, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (ros2)");

@@ -24,12 +24,15 @@ def fori_loop(lower, upper, body_fun, init_val):
 
 
 def scan(f, init, xs=None, length=None):
+    """lax.scan over the leading axis of xs (a pytree of arrays)."""
     import numpy as np
 
+    from . import tree
+
     carry, ys = init, []
-    n = length if xs is None else len(xs)
+    n = length if xs is None else np.shape(tree.leaves(xs)[0])[0]
     for i in range(n):
-        carry, y = f(carry, None if xs is None else xs[i])
+        carry, y = f(carry, None if xs is None else tree.map(lambda x: x[i], xs))
         ys.append(y)
     return carry, (np.stack(ys) if ys and ys[0] is not None else None)
 

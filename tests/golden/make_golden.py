@@ -40,6 +40,10 @@ Fixtures:
                          junctions, partial controls, a -4 mV bath, under N2, 200 steps.
   pytrees_n2_padded.npz  That world's @3 pytrees under N2 (capacities 2 above the counts, 40
                          steps), for the drop-in step.
+  vector_window.npz      The reference's own vector window (execution/vector_windows.py:348-410)
+                         over @3 on three gated 4x4 worlds with per-world step sizes, held
+                         controls, observation slots, counts and first steps, one world refused
+                         (vmap and scan of the jax stand-in loop over worlds and rows).
   device_checks.npz      The reference's accepted-row device checks (@3) on rows of its own
                          trajectory of a 36-cell gated Delaunay world with channels: accepted
                          rows after 1-120 steps and two planted faults (failed bits, values).
@@ -468,6 +472,92 @@ def make_checks():
     print("device_checks.npz written:", [c[3] for c in cases])
 
 
+# The vector window (execution/vector_windows.py:348-410, _vector_window) on three gated 4x4 @3
+# worlds: per-world step sizes, held-control indices and observation slots per row, per-world
+# counts and first steps; world 1's second control has an availability above 1 (its step is
+# refused at the first row that holds it). The same tables as tests/test_windows_gpu.py's
+# per-world case.
+WINDOW_DT = np.array([[1e-3] * 6, [5e-4] * 6, [1e-3, 2e-3, 1e-3, 2e-3, 1e-3, 2e-3]])
+WINDOW_HELD = np.array([[0, 0, 1, 1, 0, 1], [1, 0, 0, 1, 1, 0], [0, 1, 0, 1, 0, 1]])
+WINDOW_ROWS = 3
+# A row without an observation takes slot WINDOW_ROWS (out of range: dropped), as the reference's
+# window plan fills its slot table (vector_windows.py:676).
+WINDOW_SLOTS = np.array([[0, 3, 1, 3, 3, 2], [3, 0, 3, 1, 2, 3], [2, 3, 3, 0, 1, 3]])
+WINDOW_FIRST = np.array([0, 7, 3])
+WINDOW_COUNTS = np.array([6, 6, 4])
+
+
+def make_windows():
+    """The reference's own _vector_window (run through the NumPy jax stand-in: vmap as a loop
+    over worlds, scan as a loop over rows) over @3's checked_step and device_checks."""
+    import jax
+
+    from cells.definitions.specs import parse_spec
+    from cells.definitions.surface_pump_v3_spec import control_values
+    from cells.execution import vector_windows as VW
+    from cells.registry.models import get_model
+
+    from cells_b200 import worlds
+
+    rng = np.random.default_rng(31)
+    ws = [worlds.grid_world(4, 4, worlds.world_rng(31, k), gate=(0.015, 0.2, 1.0))
+          for k in range(3)]
+    b = worlds.pack(ws)
+    membrane = rng.uniform(0.6, 1, b.cells)
+    junction = rng.uniform(0.6, 1, b.edges)
+    pump = rng.uniform(0.6, 1, b.cells)
+    m1 = membrane.copy()
+    m1[b.cell_offset[1] + 3] = 1.2
+    controls = [(membrane, junction, pump), (m1, junction * 0.9, pump)]
+    v3 = "cells.model.resolved_pump_tissue@3"
+    states, params, constants, tables = [], [], [], []
+    model = None
+    for w, world in enumerate(ws):
+        c0, c1 = b.cell_offset[w], b.cell_offset[w + 1]
+        e0, e1 = b.edge_offset[w], b.edge_offset[w + 1]
+        entries = []
+        for mem, jun, pmp in controls:
+            raw = worlds.reference_definition(
+                world, dt=1e-3, steps=10, model=v3, membrane_control=np.minimum(mem[c0:c1], 1.0),
+                junction_control=jun[e0:e1], pump_control=pmp[c0:c1])
+            spec = parse_spec(raw)
+            model = get_model(spec.model)
+            cv = control_values(spec, [0.0])
+            control = type(cv)(*(np.asarray(v[0]) for v in cv))
+            membrane_field = control._fields[0]
+            row = np.array(getattr(control, membrane_field), copy=True)
+            row[:c1 - c0] = mem[c0:c1]  # an availability above 1 is the step's to refuse
+            entries.append(control._replace(**{membrane_field: row}))
+        state, p = model.initial_values(spec)
+        states.append(state)
+        params.append(p)
+        constants.append(model.device_check_constants(spec))
+        tables.append(jax.tree.map(lambda *v: np.stack(v), *entries))
+    stack = lambda trees: jax.tree.map(lambda *v: np.stack([np.asarray(x) for x in v]), *trees)
+    state, p, table, const = stack(states), stack(params), stack(tables), stack(constants)
+    final, first, bits, maxima, stored = VW._vector_window(
+        state, WINDOW_DT, WINDOW_COUNTS, table, WINDOW_HELD, WINDOW_SLOTS, WINDOW_FIRST, p,
+        p.active, const, step=model.checked_step, checks=model.device_checks, rows=WINDOW_ROWS)
+    out = {"first": np.asarray(first), "bits": np.asarray(bits), "maxima": np.asarray(maxima),
+           "dt": WINDOW_DT, "held": WINDOW_HELD, "slots": WINDOW_SLOTS,
+           "first_step": WINDOW_FIRST, "counts": WINDOW_COUNTS, "rows": np.asarray(WINDOW_ROWS),
+           "material_atol": np.asarray(constants[0].material_atol),
+           "energy_rtol": np.asarray(constants[0].energy_rtol)}
+    for k, (mem, jun, pmp) in enumerate(controls):
+        out[f"control{k}_membrane"], out[f"control{k}_junction"] = mem, jun
+        out[f"control{k}_pump"] = pmp
+    per_world = lambda tree, w: type(tree)(*(np.asarray(v)[w] for v in tree))
+    for w in range(b.worlds):
+        for f, v in _state_to_packed(per_world(final, w)).items():
+            out[f"final{w}_{f}"] = v
+        for r in range(WINDOW_ROWS):
+            row = type(stored)(*(np.asarray(v)[w, r] for v in stored))
+            for f, v in _state_to_packed(row).items():
+                out[f"stored{w}_{r}_{f}"] = v
+    np.savez_compressed(os.path.join(HERE, "vector_window.npz"), **_batch_arrays(b), **out)
+    print("vector_window.npz written: first", out["first"], "bits", out["bits"])
+
+
 def make_laws():
     from cells.laws import electrochemistry as ec
     from cells.laws.junctions import junction_voltage_relaxation as jg
@@ -585,7 +675,7 @@ def main():
     ap.add_argument("--reference", default=os.environ.get("CELLS_REFERENCE"),
                     help="the reference project's root (or set CELLS_REFERENCE)")
     ap.add_argument("--only", choices=("laws", "trajectories", "channels", "block", "n2",
-                                       "checks", "field"))
+                                       "checks", "field", "windows"))
     args = ap.parse_args()
     if not args.reference:
         ap.error("give --reference or set CELLS_REFERENCE to the reference project's root")
@@ -604,6 +694,8 @@ def main():
         make_checks()
     if args.only in (None, "field"):
         make_field_trajectories()
+    if args.only in (None, "windows"):
+        make_windows()
 
 
 if __name__ == "__main__":

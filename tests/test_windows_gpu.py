@@ -13,7 +13,7 @@ import pytest
 
 from cells_b200 import windows, worlds
 from cells_b200.tissue import Tissue
-from conftest import scaled_difference
+from conftest import load_golden, scaled_difference
 from gpu_util import oracle_state
 from oracle import checks as CK
 from oracle import tissue as T
@@ -221,3 +221,56 @@ def test_copy_worlds_is_a_masked_select(cuda):
     tissue.copy_worlds(mask, src, dst)
     torch.cuda.synchronize(dev)
     assert torch.equal(dst, want)
+
+
+def test_window_matches_the_reference_window(cuda):
+    """The reference's own _vector_window (tests/golden/vector_window.npz: run by
+    tests/golden/make_golden.py over @3's checked_step and device_checks, vmap a loop over worlds)
+    on the per-world tables above: first failing rows and bits equal, the final states and the
+    stored rows within 1e-10 scaled difference, the energy diagnostics' maxima to 1e-8."""
+    torch = cuda
+    z, b = load_golden("vector_window.npz")
+    tissue = Tissue(b)
+    dev = torch.device("cuda", tissue.device)
+    table = torch.from_numpy(np.stack([
+        tissue.pack_control(z[f"control{k}_membrane"], z[f"control{k}_junction"],
+                            z[f"control{k}_pump"]) for k in range(2)])).to(dev)
+    state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    rows = int(z["rows"])
+    win = windows.vector_window(tissue, state, z["dt"], table, z["held"], slots=z["slots"],
+                                counts=z["counts"], first_step=z["first_step"],
+                                material_atol=z["material_atol"],
+                                energy_rtol=float(z["energy_rtol"]), rows=rows)
+    torch.cuda.synchronize(dev)
+    assert np.array_equal(win.first.cpu().numpy(), z["first"])
+    assert np.array_equal(win.bits.cpu().numpy(), z["bits"])
+    got = tissue.unpack_state(win.state.cpu().numpy())
+    topo = T.topology(b)
+    stored = win.rows.cpu().numpy()
+    for w in range(b.worlds):
+        cells, edges = topo.cell_world == w, topo.edge_world == w
+
+        def part(f, v):
+            v = np.asarray(v)
+            if f in T.CELL_FIELDS:
+                return v[..., cells]
+            if f in T.EDGE_FIELDS:
+                return v[..., edges]
+            return v[..., w]
+
+        for f in T.State._fields:
+            if f"final{w}_{f}" not in z.files:
+                continue
+            ref = z[f"final{w}_{f}"]
+            if f in T.WORLD_FIELDS:  # the reference's one outside node: slot 0
+                ref = ref[..., 0]
+            assert scaled_difference(part(f, got[f]), ref) <= 1e-10, (w, f)
+        for r in range(rows):
+            row = tissue.unpack_state(stored[r])
+            for f in ("amount_increment", "membrane_transferred", "pump_cycles",
+                      "junction_transferred", "junction_gate"):
+                assert scaled_difference(part(f, row[f]), z[f"stored{w}_{r}_{f}"]) <= 1e-10, \
+                    (w, r, f)
+    m, ref = win.maxima.cpu().numpy(), z["maxima"]
+    for k in (6, 10):
+        assert np.all(np.abs(m[:, k] - ref[:, k]) <= 1e-8 * np.abs(ref[:, k])), k
