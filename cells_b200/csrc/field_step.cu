@@ -295,11 +295,36 @@ __device__ void front_forward(const Topo &T, const double *LF, double *WV, doubl
     for (int i = gid; i < bc; i += gsize) v[mp[i]] += vc[i];
     sync();
   }
-  for (int k = 0; k < sc; ++k) {
-    const double vk = v[k] / A[k + k * m];
-    for (int i = k + 1 + gid; i < m; i += gsize) v[i] -= A[i + k * m] * vk;
-    sync();
-    if (gid == 0) v[k] = vk;
+  if (gsize == 32) {
+    for (int k = 0; k < sc; ++k) {
+      const double vk = v[k] / A[k + k * m];
+      for (int i = k + 1 + gid; i < m; i += gsize) v[i] -= A[i + k * m] * vk;
+      sync();
+      if (gid == 0) v[k] = vk;
+    }
+  } else {
+    // Blocks of 32 columns: the diagonal block by warp 0 (a lane per row, the column's value
+    // by shuffle), then every row below it by the group, each row's subtractions in column
+    // order (the same arithmetic as column by column, two barriers per block).
+    for (int kb = 0; kb < sc; kb += 32) {
+      const int kw = min(32, sc - kb);
+      if (gid < 32) {
+        double x = gid < kw ? v[kb + gid] : 0.0;
+        for (int k = 0; k < kw; ++k) {
+          const double xk = __shfl_sync(0xffffffffu, x, k) / A[(kb + k) + (kb + k) * m];
+          if (gid == k) x = xk;
+          if (gid > k && gid < kw) x -= A[(kb + gid) + (kb + k) * m] * xk;
+        }
+        if (gid < kw) v[kb + gid] = x;
+      }
+      sync();
+      for (int i = kb + kw + gid; i < m; i += gsize) {
+        double t = v[i];
+        for (int k = 0; k < kw; ++k) t -= A[i + (kb + k) * m] * v[kb + k];
+        v[i] = t;
+      }
+      sync();
+    }
   }
   sync();
   double *vq = WV + T.sn_voff[q];
@@ -326,10 +351,35 @@ __device__ void front_backward(const Topo &T, const double *LF, const double *Y,
     v[k] = t;
   }
   sync();
-  for (int k = sc - 1; k > 0; --k) {
-    const double xk = v[k] / A[k + k * m];
-    for (int j = gid; j < k; j += gsize) v[j] -= A[k + j * m] * xk;
-    sync();
+  if (gsize == 32) {
+    for (int k = sc - 1; k > 0; --k) {
+      const double xk = v[k] / A[k + k * m];
+      for (int j = gid; j < k; j += gsize) v[j] -= A[k + j * m] * xk;
+      sync();
+    }
+  } else {
+    // Blocks of 32 columns from the last: the diagonal block by warp 0, then every column
+    // before it by the group, each one's subtractions in descending column order (the same
+    // arithmetic as the column sweep, two barriers per block).
+    for (int ke = sc; ke > 0; ke -= 32) {
+      const int kb = max(0, ke - 32), kw = ke - kb;
+      if (gid < 32) {
+        double x = gid < kw ? v[kb + gid] : 0.0;
+        for (int k = kw - 1; k > 0; --k) {
+          const double xk = __shfl_sync(0xffffffffu, x, k) / A[(kb + k) + (kb + k) * m];
+          if (gid < k) x -= A[(kb + k) + (kb + gid) * m] * xk;
+        }
+        if (gid < kw) v[kb + gid] = x;
+      }
+      sync();
+      for (int j = gid; j < kb; j += gsize) {
+        double t = v[j];
+        for (int k = kw - 1; k >= 0; --k)
+          t -= A[(kb + k) + j * m] * (v[kb + k] / A[(kb + k) + (kb + k) * m]);
+        v[j] = t;
+      }
+      sync();
+    }
   }
   for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k] / A[k + k * m];
 }
@@ -1381,6 +1431,9 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
   // Supernodes and each front's face entries (row = the later column, column = the earlier).
   SuperPlan sp;
   if ((rc = build_supernodes(plan, sp, grid ? &group : nullptr))) return bail(rc);
+  // Fewer levels: fronts merged into their parents where that adds at most 5% zeros and keeps
+  // the front within 16384 entries (the 126-column root of the 128x128 grid is 15876).
+  if ((rc = amalgamate(plan, sp, 0.05, 16384))) return bail(rc);
   std::vector<int> col_node(U), af_ptr(sp.count + 1, 0), af_face, af_pos;
   for (int u = 0; u < U; ++u) col_node[plan.rank[u]] = free_nodes[u];
   {

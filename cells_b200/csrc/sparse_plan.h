@@ -277,4 +277,40 @@ inline int build_supernodes(const WorldPlan &p, SuperPlan &sp,
   return CB_OK;
 }
 
+// Relaxed amalgamation of a supernode plan: a supernode q whose columns end where its parent p's
+// begin joins p when the zeros the merge adds to q's columns (s_q (s_q + m_p - m_q) entries: p's
+// rows that q's own structure lacks) are at most `frac` of the merged front block and that block
+// stays within `cap` entries; repeated until nothing merges. On a nested-dissection grid plan the
+// single-column fronts where two separators cross each become a level of their own; merged into
+// the separator above, they leave fewer, larger fronts: fewer levels (level-synchronous launches)
+// and update matrices for a few percent more factor entries and flops.
+inline int amalgamate(const WorldPlan &p, SuperPlan &sp, double frac, long long cap) {
+  const int n = (int)p.colp.size() - 1;
+  std::vector<int> group(n);
+  for (int pass = 0; pass < 64; ++pass) {
+    std::vector<int> target(sp.count);
+    for (int q = 0; q < sp.count; ++q) target[q] = q;
+    int merges = 0;
+    for (int q = sp.count - 1; q >= 0; --q) {
+      const int pq = sp.parent[q];
+      if (pq < 0 || sp.c0[q] + sp.s[q] != sp.c0[pq] || target[pq] != pq) continue;
+      const long long extra = (long long)sp.s[q] * (sp.s[q] + sp.m[pq] - sp.m[q]);
+      const long long merged = (long long)(sp.s[q] + sp.m[pq]) * (sp.s[q] + sp.s[pq]);
+      if (extra > frac * (double)merged || merged > cap) continue;
+      target[q] = pq;
+      ++merges;
+    }
+    if (!merges) return CB_OK;
+    for (int q = 0; q < sp.count; ++q) {
+      int t = q;
+      while (target[t] != t) t = target[t];
+      for (int k = 0; k < sp.s[q]; ++k) group[sp.c0[q] + k] = t;
+    }
+    SuperPlan merged;
+    if (int rc = build_supernodes(p, merged, &group)) return rc;
+    sp = std::move(merged);
+  }
+  return CB_OK;
+}
+
 }  // namespace cbk
