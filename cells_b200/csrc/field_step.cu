@@ -196,6 +196,52 @@ __device__ __forceinline__ long long packed_start(int n, int j) {
   return (long long)j * n - (long long)j * (j - 1) / 2;
 }
 
+// Stage a front's factor block (count doubles, global, 16-byte aligned, padded by the plan to an
+// even count) into shared memory with one TMA bulk copy (cp.async.bulk, completion on an
+// mbarrier that thread gid 0 initialises and arms). The wait is bounded: false when the copy did
+// not complete (the caller flags the world; the copy is waited for once more before the CTA
+// leaves, see drain_block).
+constexpr int kBulkWaitRounds = 1 << 22;
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ bool bulk_done(uint64_t *mbar) {
+  unsigned ok = 0;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(mbar))
+      : "memory");
+  return ok != 0;
+}
+template <class Sync>
+__device__ bool stage_block(double *dst, const double *src, int count, uint64_t *mbar, int gid,
+                            Sync sync) {
+  const unsigned bytes = (unsigned)((count + 1) & ~1) * 8u;
+  if (gid == 0) {
+    const unsigned mb = smem_addr(mbar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(mb)
+        : "memory");
+  }
+  sync();
+  bool done = false;
+  for (int round = 0; round < kBulkWaitRounds && !done; ++round) done = bulk_done(mbar);
+  return done;
+}
+// A copy that stage_block gave up on, waited for once more (bounded) so that it does not land in
+// shared memory the CTA no longer owns.
+__device__ void drain_block(uint64_t *mbar) {
+  for (int round = 0; round < kBulkWaitRounds && !bulk_done(mbar); ++round) {
+  }
+}
+
 // One front q of one world by a group of gsize threads (gid in [0, gsize)) with shared region A
 // (its m x s block) and piv (s doubles): assemble the face Laplacian's entries of its columns and
 // the entries of its children's update matrices that fall in its columns (children ascending);
@@ -233,29 +279,104 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
   }
   // Warps of the group over columns, lanes over rows.
   const int nw = gsize >> 5, wid = gid >> 5, ln = gid & 31;
-  for (int k = 0; k < sc; ++k) {
-    const double d = A[k + k * m];
-    if (gid == 0) {
-      if (!(d > 0.0) || !is_finite(d)) bad = 1u;
-      piv[k] = sqrt(d);
+  if (gsize == 32) {
+    for (int k = 0; k < sc; ++k) {
+      const double d = A[k + k * m];
+      if (gid == 0) {
+        if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+        piv[k] = sqrt(d);
+      }
+      const double inv_d = 1.0 / d, inv_p = 1.0 / sqrt(d);
+      for (int j = k + 1 + wid; j < sc; j += nw) {
+        const double ljk = A[j + k * m] * inv_d;
+        for (int i = j + ln; i < m; i += 32) A[i + j * m] -= A[i + k * m] * ljk;
+      }
+      sync();
+      for (int i = k + 1 + gid; i < m; i += gsize) A[i + k * m] *= inv_p;
     }
-    const double inv_d = 1.0 / d, inv_p = 1.0 / sqrt(d);
-    for (int j = k + 1 + wid; j < sc; j += nw) {
-      const double ljk = A[j + k * m] * inv_d;
-      for (int i = j + ln; i < m; i += 32) A[i + j * m] -= A[i + k * m] * ljk;
+  } else {
+    // Blocks of kPanel columns: warp 0 factors a block's columns over every row below them
+    // (right-looking, each column scaled before it updates the block's later columns; warp
+    // syncs only), then the group takes the block's contribution out of the later columns,
+    // 8x8 tiles of their lower part on the FP64 tensor cores (mma.m8n8k4, k over the block's
+    // columns). Two barriers per block instead of one per column.
+    constexpr int kPanel = 16;
+    const int r = ln >> 2, c = ln & 3;
+    for (int kb = 0; kb < sc; kb += kPanel) {
+      const int ke = min(kb + kPanel, sc);
+      if (wid == 0) {
+        for (int k = kb; k < ke; ++k) {
+          const double d = A[k + k * m];
+          if (ln == 0) {
+            if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+            piv[k] = sqrt(d);
+          }
+          const double inv_p = 1.0 / sqrt(d);
+          for (int i = k + 1 + ln; i < m; i += 32) A[i + k * m] *= inv_p;
+          __syncwarp();
+          for (int j = k + 1; j < ke; ++j) {
+            const double ljk = A[j + k * m];
+            for (int i = j + ln; i < m; i += 32) A[i + j * m] -= A[i + k * m] * ljk;
+          }
+          __syncwarp();
+        }
+      }
+      sync();
+      if (ke < sc) {
+        const int ti = (m - ke + 7) >> 3, tj = (sc - ke + 7) >> 3;
+        for (int tile = wid; tile < ti * tj; tile += nw) {
+          const int it = tile / tj, jt = tile % tj;
+          if (jt > it) continue;  // wholly above the diagonal
+          const int ia = ke + it * 8 + r, jb = ke + jt * 8 + r;
+          double acc0 = 0.0, acc1 = 0.0;
+          for (int k0 = kb; k0 < ke; k0 += 4) {
+            const int k = k0 + c;
+            const double av = (ia < m && k < ke) ? A[ia + k * m] : 0.0;
+            const double bv = (jb < sc && k < ke) ? A[jb + k * m] : 0.0;
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, "
+                         "{%3}, {%0, %1};"
+                         : "+d"(acc0), "+d"(acc1)
+                         : "d"(av), "d"(bv));
+          }
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int j = ke + jt * 8 + 2 * c + e;
+            if (ia < m && j < sc && j <= ia) A[ia + j * m] -= e ? acc1 : acc0;
+          }
+        }
+      }
+      sync();
     }
-    sync();
-    for (int i = k + 1 + gid; i < m; i += gsize) A[i + k * m] *= inv_p;
   }
   sync();
   for (int k = gid; k < sc; k += gsize) A[k + k * m] = piv[k];
   sync();
-  for (int j = wid; j < b; j += nw) {
-    double *Uj = Uq + packed_start(b, j) - j;
-    for (int i = j + ln; i < b; i += 32) {
-      double acc = 0.0;
-      for (int k = 0; k < sc; ++k) acc -= A[sc + i + k * m] * A[sc + j + k * m];
-      Uj[i] = acc;
+  // The update matrix -L_B L_B^T on the FP64 tensor cores: 8x8 tiles of its lower triangle,
+  // one warp per tile, k in steps of 4 (mma.m8n8k4.f64; rows past b and columns past sc read 0).
+  {
+    const int nt = (b + 7) >> 3;
+    const int r = ln >> 2, c = ln & 3;
+    for (int tile = wid; tile < nt * (nt + 1) / 2; tile += nw) {
+      int it = 0;
+      while ((it + 1) * (it + 2) / 2 <= tile) ++it;
+      const int jt = tile - it * (it + 1) / 2;
+      const int ia = it * 8 + r, jb = jt * 8 + r;
+      double acc0 = 0.0, acc1 = 0.0;
+      for (int k0 = 0; k0 < sc; k0 += 4) {
+        const int k = k0 + c;
+        const double av = (ia < b && k < sc) ? A[sc + ia + k * m] : 0.0;
+        const double bv = (jb < b && k < sc) ? A[sc + jb + k * m] : 0.0;
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, "
+                     "{%0, %1};"
+                     : "+d"(acc0), "+d"(acc1)
+                     : "d"(av), "d"(bv));
+      }
+      const int i = it * 8 + r;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int j = jt * 8 + 2 * c + e;
+        if (i < b && j <= i) Uq[packed_start(b, j) + (i - j)] = -(e ? acc1 : acc0);
+      }
     }
   }
   sync();
@@ -280,12 +401,16 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
 // Forward substitution of front q: its columns' right-hand side (Y) plus its children's update
 // vectors, the dense triangular solve on the staged block, the update vector for its parent.
 template <class Sync>
-__device__ void front_forward(const Topo &T, const double *LF, double *WV, double *Y, int q,
-                              double *A, double *v, int gid, int gsize, Sync sync) {
+__device__ bool front_forward(const Topo &T, const double *LF, double *WV, double *Y, int q,
+                              double *A, double *v, uint64_t *mbar, int gid, int gsize,
+                              Sync sync) {
   const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
   const double *Lq = LF + T.sn_loff[q];
-  for (int a = gid; a < m * sc; a += gsize) A[a] = Lq[a];
   for (int i = gid; i < m; i += gsize) v[i] = i < sc ? Y[c0 + i] : 0.0;
+  if (!stage_block(A, Lq, m * sc, mbar, gid, sync)) {
+    drain_block(mbar);
+    return false;
+  }
   sync();
   for (int t = T.ch_ptr[q]; t < T.ch_ptr[q + 1]; ++t) {
     const int c = T.ch[t];
@@ -332,18 +457,23 @@ __device__ void front_forward(const Topo &T, const double *LF, double *WV, doubl
     if (i < sc) Y[c0 + i] = v[i];
     else vq[i - sc] = v[i];
   }
+  return true;
 }
 
 // Back substitution of front q: t = y_S - L_BS^T x_B (x_B from its ancestors, in out), one
 // column per thread; then L_SS^T x_S = t by a column sweep, one barrier per column.
 template <class Sync>
-__device__ void front_backward(const Topo &T, const double *LF, const double *Y, double *out,
-                               int q, double *A, double *v, int gid, int gsize, Sync sync) {
+__device__ bool front_backward(const Topo &T, const double *LF, const double *Y, double *out,
+                               int q, double *A, double *v, uint64_t *mbar, int gid, int gsize,
+                               Sync sync) {
   const int c0 = T.sn_c0[q], sc = T.sn_s[q], m = T.sn_m[q];
   const double *Lq = LF + T.sn_loff[q];
   const int *rq = T.rows + T.rows_ptr[q];
-  for (int a = gid; a < m * sc; a += gsize) A[a] = Lq[a];
   for (int i = sc + gid; i < m; i += gsize) v[i] = out[rq[i]];
+  if (!stage_block(A, Lq, m * sc, mbar, gid, sync)) {
+    drain_block(mbar);
+    return false;
+  }
   sync();
   for (int k = gid; k < sc; k += gsize) {
     double t = Y[c0 + k];
@@ -382,6 +512,7 @@ __device__ void front_backward(const Topo &T, const double *LF, const double *Y,
     }
   }
   for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k] / A[k + k * m];
+  return true;
 }
 
 // Level kernels. Warp form: each warp one (front, world) task of the level, world-major, with a
@@ -389,6 +520,13 @@ __device__ void front_backward(const Topo &T, const double *LF, const double *Y,
 // one CTA of kGroupThreads per (front, world). Refused worlds are skipped.
 constexpr int kWarpsPerCta = 8;
 constexpr int kGroupThreads = 256;
+// Shared memory of a level's task: the front block (its TMA copy rounded up to an even count of
+// doubles, 16 bytes), then the front's vector; a warp task's slice kept even so every block
+// starts on a 16-byte boundary.
+__host__ __device__ constexpr long long level_vec(long long block) { return (block + 1) & ~1LL; }
+__host__ __device__ constexpr long long level_slice(long long block, long long rows) {
+  return (level_vec(block) + rows + 1) & ~1LL;
+}
 
 struct LevelTask {
   int q, w;
@@ -408,7 +546,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
     factor_warps(const Topo T, const Params P, const Scratch S, double *scratch,
                  const uint32_t *status, int kind, double gamma_dt, int a0, int fronts, int W,
                  int slice, int vec) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
   const LevelTask t = warp_task(T, status, a0, fronts, W);
   if (!t.ok) return;
   double *base = scratch + (size_t)t.w * S.stride;
@@ -422,7 +560,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
 __global__ void __launch_bounds__(kGroupThreads)
     factor_group(const Topo T, const Params P, const Scratch S, double *scratch,
                  const uint32_t *status, int kind, double gamma_dt, int a0, int vec) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
   const int w = blockIdx.y;
   if (status[w] != 0u) return;
   double *base = scratch + (size_t)w * S.stride;
@@ -435,47 +573,57 @@ __global__ void __launch_bounds__(kGroupThreads)
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
     forward_warps(const Topo T, const Scratch S, double *scratch, const uint32_t *status, int a0,
                   int fronts, int W, int slice, int vec) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint64_t mbar[kWarpsPerCta];
   const LevelTask t = warp_task(T, status, a0, fronts, W);
   if (!t.ok) return;
   double *base = scratch + (size_t)t.w * S.stride;
   double *A = sm + (size_t)(threadIdx.x >> 5) * slice;
-  front_forward(T, base + S.lval, base + S.wv, base + S.y, t.q, A, A + vec, threadIdx.x & 31, 32,
-                [] { __syncwarp(); });
+  if (!front_forward(T, base + S.lval, base + S.wv, base + S.y, t.q, A, A + vec,
+                     mbar + (threadIdx.x >> 5), threadIdx.x & 31, 32, [] { __syncwarp(); }))
+    base[S.ctl + 7] = 1.0;
 }
 
 __global__ void __launch_bounds__(kGroupThreads)
     forward_group(const Topo T, const Scratch S, double *scratch, const uint32_t *status, int a0,
                   int vec) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint64_t mbar;
   const int w = blockIdx.y;
   if (status[w] != 0u) return;
   double *base = scratch + (size_t)w * S.stride;
-  front_forward(T, base + S.lval, base + S.wv, base + S.y, T.lv_sn[a0 + blockIdx.x], sm, sm + vec,
-                threadIdx.x, kGroupThreads, [] { __syncthreads(); });
+  if (!front_forward(T, base + S.lval, base + S.wv, base + S.y, T.lv_sn[a0 + blockIdx.x], sm,
+                     sm + vec, &mbar, threadIdx.x, kGroupThreads, [] { __syncthreads(); }) &&
+      threadIdx.x == 0)
+    base[S.ctl + 7] = 1.0;
 }
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
     backward_warps(const Topo T, const Scratch S, double *scratch, const uint32_t *status,
                    long long out_off, int a0, int fronts, int W, int slice, int vec) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint64_t mbar[kWarpsPerCta];
   const LevelTask t = warp_task(T, status, a0, fronts, W);
   if (!t.ok) return;
   double *base = scratch + (size_t)t.w * S.stride;
   double *A = sm + (size_t)(threadIdx.x >> 5) * slice;
-  front_backward(T, base + S.lval, base + S.y, base + out_off, t.q, A, A + vec, threadIdx.x & 31,
-                 32, [] { __syncwarp(); });
+  if (!front_backward(T, base + S.lval, base + S.y, base + out_off, t.q, A, A + vec,
+                      mbar + (threadIdx.x >> 5), threadIdx.x & 31, 32, [] { __syncwarp(); }))
+    base[S.ctl + 7] = 1.0;
 }
 
 __global__ void __launch_bounds__(kGroupThreads)
     backward_group(const Topo T, const Scratch S, double *scratch, const uint32_t *status,
                    long long out_off, int a0, int vec) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint64_t mbar;
   const int w = blockIdx.y;
   if (status[w] != 0u) return;
   double *base = scratch + (size_t)w * S.stride;
-  front_backward(T, base + S.lval, base + S.y, base + out_off, T.lv_sn[a0 + blockIdx.x], sm,
-                 sm + vec, threadIdx.x, kGroupThreads, [] { __syncthreads(); });
+  if (!front_backward(T, base + S.lval, base + S.y, base + out_off, T.lv_sn[a0 + blockIdx.x], sm,
+                      sm + vec, &mbar, threadIdx.x, kGroupThreads, [] { __syncthreads(); }) &&
+      threadIdx.x == 0)
+    base[S.ctl + 7] = 1.0;
 }
 
 // One instantiation per phase, so each gets its own register allocation (MINB: CTAs per SM).
@@ -962,7 +1110,8 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     return;
   }
   if (phase == PH_AFTER_NEWTON) {
-    unsigned bits = bits_in();
+    // ctl[7]: a pivot or a staged copy that failed in the start field's factor or solves.
+    unsigned bits = bits_in() | (ctl[7] != 0.0 ? (unsigned)CB_WORLD_FIELD : 0u);
     set_phi(X);
     {
       double rm2, n2;
@@ -1036,7 +1185,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   }
   // PH_FINISH: the stage-2 solution, its drift, the step's end.
   {
-    unsigned bits = bits_in();
+    unsigned bits = bits_in() | (ctl[7] != 0.0 ? (unsigned)CB_WORLD_OPERATOR : 0u);
     bits |= stage_post(known2_cell);
     drift(D2);
     // ---- the step's end: ledgers, heat, domain; write or refuse ---------------------------
@@ -1471,7 +1620,8 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
     f->lv_block[l] = (int)mb;
     f->lv_m[l] = mm;
     f->lv_warp[l] = (mb <= kWarpBlock && mm <= kWarpVector) ? 1 : 0;
-    const long long need = f->lv_warp[l] ? (long long)kWarpsPerCta * (mb + mm) : mb + mm;
+    const long long need =
+        f->lv_warp[l] ? (long long)kWarpsPerCta * level_slice(mb, mm) : level_vec(mb) + mm;
     f->smem_doubles = std::max(f->smem_doubles, need);
   }
   if (f->smem_doubles * (long long)sizeof(double) > kMaxSmemBytes)
@@ -1600,6 +1750,10 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
   S.rk_ex = S.rk_s + 3LL * O;
   S.rk_size = S.rk_ex + 3LL * N;
   S.lval = take(f->lsize), S.uf = take(f->usize), S.wv = take(std::max(f->vsize, 1LL));
+  // The solves stage each front block with a TMA bulk copy: its global start must be 16-byte
+  // aligned (world slices and sub-arrays are 256-byte aligned; blocks start at even offsets).
+  for (int q = 0; q < sp.count; ++q)
+    if (sp.loff[q] % 2 != 0) return bail(fail(CB_ERR_LAYOUT, "field: a factor block is not 16-byte aligned"));
   S.ctl = take(8);
   S.x = take(U), S.xt = take(U), S.dx = take(U), S.r = take(U), S.rt = take(U), S.y = take(U);
   S.phi = take(O), S.pc = take(N);
@@ -1748,15 +1902,15 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
   };
   auto level_launch = [&](int l, auto warps, auto group) {
     const int a0 = f->lv_ptr[l], fronts = f->lv_ptr[l + 1] - a0;
-    const int vec = f->lv_block[l];
+    const int vec = (int)level_vec(f->lv_block[l]);
     ++f->launches;
     if (f->lv_warp[l]) {
-      const int slice = f->lv_block[l] + f->lv_m[l];
+      const int slice = (int)level_slice(f->lv_block[l], f->lv_m[l]);
       const long long tasks = (long long)fronts * f->W;
       const int ctas = (int)((tasks + kWarpsPerCta - 1) / kWarpsPerCta);
       warps(ctas, (size_t)kWarpsPerCta * slice * sizeof(double), a0, fronts, slice, vec);
     } else {
-      group(dim3(fronts, f->W), (size_t)(f->lv_block[l] + f->lv_m[l]) * sizeof(double), a0, vec);
+      group(dim3(fronts, f->W), (size_t)(vec + f->lv_m[l]) * sizeof(double), a0, vec);
     }
     return cudaGetLastError();
   };

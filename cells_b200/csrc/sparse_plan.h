@@ -266,7 +266,7 @@ inline int build_supernodes(const WorldPlan &p, SuperPlan &sp,
   for (int q = 0; q < S; ++q) {
     const long long mm = sp.m[q], ss = sp.s[q], b = mm - ss;
     sp.loff[q] = sp.lsize;
-    sp.lsize += mm * ss;
+    sp.lsize += (mm * ss + 1) & ~1LL;  // even: every block 16-byte aligned, its copy padded
     sp.uoff[q] = sp.usize;
     sp.usize += b * (b + 1) / 2;  // the update matrix's lower triangle, packed by columns
     sp.voff[q] = sp.vsize;
