@@ -635,16 +635,6 @@ def fp64_peak(device):
     return _FP64_PEAK[device]
 
 
-def field_traffic_per_world_step():
-    """DRAM bytes per world·step of the field step (ncu, committed summary)."""
-    path = os.path.join(ROOT, "profiles", "field_traffic.json")
-    try:
-        with open(path) as f:
-            return float(json.load(f)["dram_bytes_per_world_step"])
-    except (OSError, KeyError, ValueError):
-        return None
-
-
 def run_field(args, rank, world_size, local_rank, dist, base):
     """The spatial-field workload: each bench step is one ARS(2,2,2) step of every world."""
     import torch
@@ -756,9 +746,10 @@ def run_field(args, rank, world_size, local_rank, dist, base):
                 "kernel": "field step (field_phase, factor_*, forward_*, backward_* launches)",
                 "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": (None if field_traffic_per_world_step() is None
-                            else field_traffic_per_world_step() * tissue.W),
-                "traffic_note": "DRAM bytes of one step of 32 worlds (ncu), scaled per world",
+                "traffic": None,
+                "traffic_note": ("a step is ~700 launches of 13 kernels: no one-kernel capture "
+                                 "gives its DRAM bytes; the per-kernel DRAM figures are in the "
+                                 "committed ncu summaries (factor_group, field_phase)"),
                 "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms,
                 "bytes_per_world_step": alg / tissue.W,
                 "count": ("minimal traffic: state read and written once, parameters read once, "

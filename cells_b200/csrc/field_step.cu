@@ -54,6 +54,7 @@ constexpr int kFieldBlock = 512;
 constexpr int kPhaseMinBlocks = 2;  // phase CTAs per SM the register budget aims for
 constexpr int kWarpBlock = 1280;  // a level's fronts go one per warp when their blocks fit this
 constexpr int kWarpVector = 256;  // ... and their fronts' rows this
+constexpr int kWideColumns = 48;  // a CTA level's fronts take the wide factor from this many columns
 // Dynamic shared memory a level kernel may ask for: the 227 KB per CTA less room for its static
 // shared memory.
 constexpr long long kMaxSmemBytes = 227 * 1024 - 1024;
@@ -242,15 +243,51 @@ __device__ void drain_block(uint64_t *mbar) {
   }
 }
 
+// The trailing update of a block of columns [kb, ke) of an m x sc front in shared memory (column
+// major, leading dimension m): A[i][j] -= sum_k A[i][k] A[j][k] for ke <= j < sc, j <= i < m, k in
+// [kb, ke), 8x8 tiles of the lower part on the FP64 tensor cores (mma.m8n8k4, k in steps of 4;
+// entries past the front read 0), tiles over the group's nw warps (this one wid; lane row r,
+// column c of the fragments).
+__device__ __forceinline__ void trailing_update(double *A, int m, int sc, int kb, int ke, int wid,
+                                                int nw, int r, int c) {
+  const int ti = (m - ke + 7) >> 3, tj = (sc - ke + 7) >> 3;
+  for (int tile = wid; tile < ti * tj; tile += nw) {
+    const int it = tile / tj, jt = tile % tj;
+    if (jt > it) continue;  // wholly above the diagonal
+    const int ia = ke + it * 8 + r, jb = ke + jt * 8 + r;
+    double acc0 = 0.0, acc1 = 0.0;
+    for (int k0 = kb; k0 < ke; k0 += 4) {
+      const int k = k0 + c;
+      const double av = (ia < m && k < ke) ? A[ia + k * m] : 0.0;
+      const double bv = (jb < sc && k < ke) ? A[jb + k * m] : 0.0;
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, "
+                   "{%0, %1};"
+                   : "+d"(acc0), "+d"(acc1)
+                   : "d"(av), "d"(bv));
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int j = ke + jt * 8 + 2 * c + e;
+      if (ia < m && j < sc && j <= ia) A[ia + j * m] -= e ? acc1 : acc0;
+    }
+  }
+}
+
 // One front q of one world by a group of gsize threads (gid in [0, gsize)) with shared region A
 // (its m x s block) and piv (s doubles): assemble the face Laplacian's entries of its columns and
 // the entries of its children's update matrices that fall in its columns (children ascending);
-// factor its m x s panel right-looking with one barrier per column (the trailing update uses the
-// unscaled pivot column over the pivot; the column is scaled after the barrier, the pivots kept
-// apart); write its update matrix as minus the panel's product, then add the children's entries
-// that fall in it (children ascending); store the panel. Update matrices are packed lower
-// triangles. Returns nonzero (at gid 0) on a pivot that is not positive.
-template <class Sync>
+// factor its m x s panel right-looking; write its update matrix as minus the panel's product,
+// then add the children's entries that fall in it (children ascending); store the panel. Update
+// matrices are packed lower triangles. The stored panel holds each column's inverse pivot
+// 1/sqrt(d) on its diagonal (the solves multiply by it). Returns nonzero (at gid 0) on a pivot
+// that is not positive.
+//
+// Two factor forms:
+//  * !WIDE (a warp, or a CTA): column by column, warps over the later columns, lanes over rows,
+//    one sync per column. Few registers, many CTAs per SM: the fronts below the top of the tree;
+//  * WIDE (a CTA): blocks of 16 columns, three barriers per block (below); more registers, two
+//    CTAs per SM: the wide separators at the top of the tree, whose columns are the critical path.
+template <bool WIDE, class Sync>
 __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
                                  const Conductance &g, double *A, double *piv, int gid,
                                  int gsize, Sync sync) {
@@ -277,16 +314,84 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
     });
     sync();
   }
-  // Warps of the group over columns, lanes over rows.
   const int nw = gsize >> 5, wid = gid >> 5, ln = gid & 31;
-  if (gsize == 32) {
+  if constexpr (WIDE) {
+    // WIDE: blocks of kPanel columns, three barriers per block:
+    //  * the block's diagonal part by warp 0 in registers (a lane per row, right-looking: each
+    //    column scaled by its inverse pivot, then its products taken out of the block's later
+    //    columns, the other rows' values by shuffle), its inverse pivots left on its diagonal;
+    //  * every row below the block by the group, a thread per row in registers (the same scalings
+    //    and subtractions, in the same column order);
+    //  * the block's contribution taken out of the later columns by the group, 8x8 tiles of their
+    //    lower part on the FP64 tensor cores (mma.m8n8k4, k over the block's columns).
+    // Each entry sees the same operations in the same order as a column-by-column factor.
+    constexpr int kPanel = 16;
+    const int r = ln >> 2, c = ln & 3;
+    for (int kb = 0; kb < sc; kb += kPanel) {
+      const int ke = min(kb + kPanel, sc), nb = ke - kb;
+      if (wid == 0) {
+        const bool mine = ln < nb;
+        double a[kPanel];
+#pragma unroll
+        for (int j = 0; j < kPanel; ++j)
+          a[j] = (mine && j <= ln) ? A[(kb + ln) + (kb + j) * m] : 0.0;
+#pragma unroll
+        for (int k = 0; k < kPanel; ++k) {
+          if (k < nb) {
+            const double d = __shfl_sync(0xffffffffu, a[k], k);
+            if (ln == 0 && (!(d > 0.0) || !is_finite(d))) bad = 1u;
+            const double inv_p = 1.0 / sqrt(d);
+            if (ln == k) A[(kb + k) + (kb + k) * m] = inv_p;  // for the rows below
+            if (ln > k) a[k] *= inv_p;
+#pragma unroll
+            for (int j = k + 1; j < kPanel; ++j) {
+              if (j < nb) {
+                const double ljk = __shfl_sync(0xffffffffu, a[k], j);
+                if (ln >= j) a[j] -= a[k] * ljk;
+              }
+            }
+          }
+        }
+        if (mine) {
+#pragma unroll
+          for (int j = 0; j < kPanel; ++j)
+            if (j < ln) A[(kb + ln) + (kb + j) * m] = a[j];
+        }
+      }
+      sync();
+      for (int i = ke + gid; i < m; i += gsize) {
+        double x[kPanel];
+#pragma unroll
+        for (int k = 0; k < kPanel; ++k) x[k] = k < nb ? A[i + (kb + k) * m] : 0.0;
+#pragma unroll
+        for (int k = 0; k < kPanel; ++k) {
+          if (k < nb) {
+            x[k] *= A[(kb + k) + (kb + k) * m];
+#pragma unroll
+            for (int j = k + 1; j < kPanel; ++j)
+              if (j < nb) x[j] -= x[k] * A[(kb + j) + (kb + k) * m];
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < kPanel; ++k)
+          if (k < nb) A[i + (kb + k) * m] = x[k];
+      }
+      sync();
+      if (ke < sc) {
+        trailing_update(A, m, sc, kb, ke, wid, nw, r, c);
+        sync();
+      }
+    }
+    sync();
+  } else {
+    // Column by column: warps of the group over the later columns, lanes over rows, a sync per
+    // column (the trailing update uses the unscaled pivot column over the pivot; the column is
+    // scaled after the sync).
     for (int k = 0; k < sc; ++k) {
       const double d = A[k + k * m];
-      if (gid == 0) {
-        if (!(d > 0.0) || !is_finite(d)) bad = 1u;
-        piv[k] = sqrt(d);
-      }
+      if (gid == 0 && (!(d > 0.0) || !is_finite(d))) bad = 1u;
       const double inv_d = 1.0 / d, inv_p = 1.0 / sqrt(d);
+      if (gid == 0) piv[k] = inv_p;
       for (int j = k + 1 + wid; j < sc; j += nw) {
         const double ljk = A[j + k * m] * inv_d;
         for (int i = j + ln; i < m; i += 32) A[i + j * m] -= A[i + k * m] * ljk;
@@ -294,63 +399,10 @@ __device__ unsigned front_factor(const Topo &T, double *LF, double *UF, int q,
       sync();
       for (int i = k + 1 + gid; i < m; i += gsize) A[i + k * m] *= inv_p;
     }
-  } else {
-    // Blocks of kPanel columns: warp 0 factors a block's columns over every row below them
-    // (right-looking, each column scaled before it updates the block's later columns; warp
-    // syncs only), then the group takes the block's contribution out of the later columns,
-    // 8x8 tiles of their lower part on the FP64 tensor cores (mma.m8n8k4, k over the block's
-    // columns). Two barriers per block instead of one per column.
-    constexpr int kPanel = 16;
-    const int r = ln >> 2, c = ln & 3;
-    for (int kb = 0; kb < sc; kb += kPanel) {
-      const int ke = min(kb + kPanel, sc);
-      if (wid == 0) {
-        for (int k = kb; k < ke; ++k) {
-          const double d = A[k + k * m];
-          if (ln == 0) {
-            if (!(d > 0.0) || !is_finite(d)) bad = 1u;
-            piv[k] = sqrt(d);
-          }
-          const double inv_p = 1.0 / sqrt(d);
-          for (int i = k + 1 + ln; i < m; i += 32) A[i + k * m] *= inv_p;
-          __syncwarp();
-          for (int j = k + 1; j < ke; ++j) {
-            const double ljk = A[j + k * m];
-            for (int i = j + ln; i < m; i += 32) A[i + j * m] -= A[i + k * m] * ljk;
-          }
-          __syncwarp();
-        }
-      }
-      sync();
-      if (ke < sc) {
-        const int ti = (m - ke + 7) >> 3, tj = (sc - ke + 7) >> 3;
-        for (int tile = wid; tile < ti * tj; tile += nw) {
-          const int it = tile / tj, jt = tile % tj;
-          if (jt > it) continue;  // wholly above the diagonal
-          const int ia = ke + it * 8 + r, jb = ke + jt * 8 + r;
-          double acc0 = 0.0, acc1 = 0.0;
-          for (int k0 = kb; k0 < ke; k0 += 4) {
-            const int k = k0 + c;
-            const double av = (ia < m && k < ke) ? A[ia + k * m] : 0.0;
-            const double bv = (jb < sc && k < ke) ? A[jb + k * m] : 0.0;
-            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, "
-                         "{%3}, {%0, %1};"
-                         : "+d"(acc0), "+d"(acc1)
-                         : "d"(av), "d"(bv));
-          }
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int j = ke + jt * 8 + 2 * c + e;
-            if (ia < m && j < sc && j <= ia) A[ia + j * m] -= e ? acc1 : acc0;
-          }
-        }
-      }
-      sync();
-    }
+    sync();
+    for (int k = gid; k < sc; k += gsize) A[k + k * m] = piv[k];
+    sync();
   }
-  sync();
-  for (int k = gid; k < sc; k += gsize) A[k + k * m] = piv[k];
-  sync();
   // The update matrix -L_B L_B^T on the FP64 tensor cores: 8x8 tiles of its lower triangle,
   // one warp per tile, k in steps of 4 (mma.m8n8k4.f64; rows past b and columns past sc read 0).
   {
@@ -420,36 +472,28 @@ __device__ bool front_forward(const Topo &T, const double *LF, double *WV, doubl
     for (int i = gid; i < bc; i += gsize) v[mp[i]] += vc[i];
     sync();
   }
-  if (gsize == 32) {
-    for (int k = 0; k < sc; ++k) {
-      const double vk = v[k] / A[k + k * m];
-      for (int i = k + 1 + gid; i < m; i += gsize) v[i] -= A[i + k * m] * vk;
-      sync();
-      if (gid == 0) v[k] = vk;
-    }
-  } else {
-    // Blocks of 32 columns: the diagonal block by warp 0 (a lane per row, the column's value
-    // by shuffle), then every row below it by the group, each row's subtractions in column
-    // order (the same arithmetic as column by column, two barriers per block).
-    for (int kb = 0; kb < sc; kb += 32) {
-      const int kw = min(32, sc - kb);
-      if (gid < 32) {
-        double x = gid < kw ? v[kb + gid] : 0.0;
-        for (int k = 0; k < kw; ++k) {
-          const double xk = __shfl_sync(0xffffffffu, x, k) / A[(kb + k) + (kb + k) * m];
-          if (gid == k) x = xk;
-          if (gid > k && gid < kw) x -= A[(kb + gid) + (kb + k) * m] * xk;
-        }
-        if (gid < kw) v[kb + gid] = x;
+  // Blocks of 32 columns: the diagonal block by warp 0 (a lane per row, the column's value by
+  // shuffle, times the column's inverse pivot), then every row below it by the group, each
+  // row's subtractions in column order (the same arithmetic as column by column, two barriers
+  // per block).
+  for (int kb = 0; kb < sc; kb += 32) {
+    const int kw = min(32, sc - kb);
+    if (gid < 32) {
+      double x = gid < kw ? v[kb + gid] : 0.0;
+      for (int k = 0; k < kw; ++k) {
+        const double xk = __shfl_sync(0xffffffffu, x, k) * A[(kb + k) + (kb + k) * m];
+        if (gid == k) x = xk;
+        if (gid > k && gid < kw) x -= A[(kb + gid) + (kb + k) * m] * xk;
       }
-      sync();
-      for (int i = kb + kw + gid; i < m; i += gsize) {
-        double t = v[i];
-        for (int k = 0; k < kw; ++k) t -= A[i + (kb + k) * m] * v[kb + k];
-        v[i] = t;
-      }
-      sync();
+      if (gid < kw) v[kb + gid] = x;
     }
+    sync();
+    for (int i = kb + kw + gid; i < m; i += gsize) {
+      double t = v[i];
+      for (int k = 0; k < kw; ++k) t -= A[i + (kb + k) * m] * v[kb + k];
+      v[i] = t;
+    }
+    sync();
   }
   sync();
   double *vq = WV + T.sn_voff[q];
@@ -461,7 +505,7 @@ __device__ bool front_forward(const Topo &T, const double *LF, double *WV, doubl
 }
 
 // Back substitution of front q: t = y_S - L_BS^T x_B (x_B from its ancestors, in out), one
-// column per thread; then L_SS^T x_S = t by a column sweep, one barrier per column.
+// column per thread; then L_SS^T x_S = t in blocks of 32 columns.
 template <class Sync>
 __device__ bool front_backward(const Topo &T, const double *LF, const double *Y, double *out,
                                int q, double *A, double *v, uint64_t *mbar, int gid, int gsize,
@@ -481,37 +525,29 @@ __device__ bool front_backward(const Topo &T, const double *LF, const double *Y,
     v[k] = t;
   }
   sync();
-  if (gsize == 32) {
-    for (int k = sc - 1; k > 0; --k) {
-      const double xk = v[k] / A[k + k * m];
-      for (int j = gid; j < k; j += gsize) v[j] -= A[k + j * m] * xk;
-      sync();
-    }
-  } else {
-    // Blocks of 32 columns from the last: the diagonal block by warp 0, then every column
-    // before it by the group, each one's subtractions in descending column order (the same
-    // arithmetic as the column sweep, two barriers per block).
-    for (int ke = sc; ke > 0; ke -= 32) {
-      const int kb = max(0, ke - 32), kw = ke - kb;
-      if (gid < 32) {
-        double x = gid < kw ? v[kb + gid] : 0.0;
-        for (int k = kw - 1; k > 0; --k) {
-          const double xk = __shfl_sync(0xffffffffu, x, k) / A[(kb + k) + (kb + k) * m];
-          if (gid < k) x -= A[(kb + k) + (kb + gid) * m] * xk;
-        }
-        if (gid < kw) v[kb + gid] = x;
+  // Blocks of 32 columns from the last: the diagonal block by warp 0, then every column before
+  // it by the group, each one's subtractions in descending column order (the same arithmetic as
+  // the column sweep, two barriers per block; the inverse pivots on the diagonal).
+  for (int ke = sc; ke > 0; ke -= 32) {
+    const int kb = max(0, ke - 32), kw = ke - kb;
+    if (gid < 32) {
+      double x = gid < kw ? v[kb + gid] : 0.0;
+      for (int k = kw - 1; k > 0; --k) {
+        const double xk = __shfl_sync(0xffffffffu, x, k) * A[(kb + k) + (kb + k) * m];
+        if (gid < k) x -= A[(kb + k) + (kb + gid) * m] * xk;
       }
-      sync();
-      for (int j = gid; j < kb; j += gsize) {
-        double t = v[j];
-        for (int k = kw - 1; k >= 0; --k)
-          t -= A[(kb + k) + j * m] * (v[kb + k] / A[(kb + k) + (kb + k) * m]);
-        v[j] = t;
-      }
-      sync();
+      if (gid < kw) v[kb + gid] = x;
     }
+    sync();
+    for (int j = gid; j < kb; j += gsize) {
+      double t = v[j];
+      for (int k = kw - 1; k >= 0; --k)
+        t -= A[(kb + k) + j * m] * (v[kb + k] * A[(kb + k) + (kb + k) * m]);
+      v[j] = t;
+    }
+    sync();
   }
-  for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k] / A[k + k * m];
+  for (int k = gid; k < sc; k += gsize) out[c0 + k] = v[k] * A[k + k * m];
   return true;
 }
 
@@ -551,22 +587,26 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
   if (!t.ok) return;
   double *base = scratch + (size_t)t.w * S.stride;
   double *A = sm + (size_t)(threadIdx.x >> 5) * slice;
-  const unsigned bad = front_factor(T, base + S.lval, base + S.uf, t.q,
-                                    conductance(P, S, base, t.w, T.F, kind, gamma_dt), A, A + vec,
-                                    threadIdx.x & 31, 32, [] { __syncwarp(); });
+  const unsigned bad = front_factor<false>(T, base + S.lval, base + S.uf, t.q,
+                                           conductance(P, S, base, t.w, T.F, kind, gamma_dt), A,
+                                           A + vec, threadIdx.x & 31, 32, [] { __syncwarp(); });
   if (bad) base[S.ctl + 7] = 1.0;
 }
 
-__global__ void __launch_bounds__(kGroupThreads)
+// The narrow form's registers held to six CTAs per SM, the wide form's to two.
+template <bool WIDE>
+__global__ void __launch_bounds__(kGroupThreads, WIDE ? 2 : 6)
     factor_group(const Topo T, const Params P, const Scratch S, double *scratch,
                  const uint32_t *status, int kind, double gamma_dt, int a0, int vec) {
   extern __shared__ __align__(16) double sm[];
   const int w = blockIdx.y;
   if (status[w] != 0u) return;
   double *base = scratch + (size_t)w * S.stride;
-  const unsigned bad = front_factor(T, base + S.lval, base + S.uf, T.lv_sn[a0 + blockIdx.x],
-                                    conductance(P, S, base, w, T.F, kind, gamma_dt), sm, sm + vec,
-                                    threadIdx.x, kGroupThreads, [] { __syncthreads(); });
+  const unsigned bad = front_factor<WIDE>(T, base + S.lval, base + S.uf,
+                                          T.lv_sn[a0 + blockIdx.x],
+                                          conductance(P, S, base, w, T.F, kind, gamma_dt), sm,
+                                          sm + vec, threadIdx.x, kGroupThreads,
+                                          [] { __syncthreads(); });
   if (bad) base[S.ctl + 7] = 1.0;
 }
 
@@ -1326,7 +1366,7 @@ struct cb_field {
   int supernodes = 0;
   // Levels of the fronts (host copies): first entry in lv_sn, one warp per front, the largest
   // block (m x s) and front rows.
-  std::vector<int> lv_ptr, lv_warp, lv_block, lv_m;
+  std::vector<int> lv_ptr, lv_warp, lv_wide, lv_block, lv_m;
   double factor_flops = 0.0, solve_flops = 0.0;  // per world: one factorisation, one solve
   long long launches = 0;   // kernels launched by the last cb_field_step
   long long solves = 0, factorisations = 0;  // ... and the solves and factorisations it ran
@@ -1607,19 +1647,22 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
   // A level's fronts go one per warp (their blocks and rows small) or one per CTA.
   f->lv_ptr = sp.lv_ptr;
   f->lv_warp.assign(sp.levels, 0);
+  f->lv_wide.assign(sp.levels, 0);
   f->lv_block.assign(sp.levels, 0);
   f->lv_m.assign(sp.levels, 0);
   for (int l = 0; l < sp.levels; ++l) {
     long long mb = 0;
-    int mm = 0;
+    int mm = 0, ms = 0;
     for (int a = sp.lv_ptr[l]; a < sp.lv_ptr[l + 1]; ++a) {
       const int q = sp.lv_sn[a];
       mb = std::max(mb, (long long)sp.m[q] * sp.s[q]);
       mm = std::max(mm, sp.m[q]);
+      ms = std::max(ms, sp.s[q]);
     }
     f->lv_block[l] = (int)mb;
     f->lv_m[l] = mm;
     f->lv_warp[l] = (mb <= kWarpBlock && mm <= kWarpVector) ? 1 : 0;
+    f->lv_wide[l] = (!f->lv_warp[l] && ms >= kWideColumns) ? 1 : 0;
     const long long need =
         f->lv_warp[l] ? (long long)kWarpsPerCta * level_slice(mb, mm) : level_vec(mb) + mm;
     f->smem_doubles = std::max(f->smem_doubles, need);
@@ -1789,8 +1832,8 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
     }
     f->any_host = static_cast<int *>(p);
   }
-  for (const void *fn : {(const void *)factor_warps, (const void *)factor_group,
-                         (const void *)forward_warps, (const void *)forward_group,
+  for (const void *fn : {(const void *)factor_warps, (const void *)factor_group<false>,
+                         (const void *)factor_group<true>, (const void *)forward_warps, (const void *)forward_group,
                          (const void *)backward_warps, (const void *)backward_group})
     if ((ce = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)kMaxSmemBytes)) != cudaSuccess) {
@@ -1839,7 +1882,8 @@ extern "C" int cb_field_flops(const cb_field *f, double out[2]) {
 
 extern "C" int32_t cb_field_levels(const cb_field *f, int32_t *kinds, int32_t capacity) {
   if (!f) return fail(CB_ERR_ARGUMENT, "null argument"), -1;
-  for (int l = 0; l < f->levels && kinds && l < capacity; ++l) kinds[l] = f->lv_warp[l] ? 0 : 1;
+  for (int l = 0; l < f->levels && kinds && l < capacity; ++l)
+    kinds[l] = f->lv_warp[l] ? 0 : f->lv_wide[l] ? 2 : 1;
   return f->levels;
 }
 
@@ -1925,8 +1969,9 @@ extern "C" int cb_field_step(cb_field *f, const double *state_in, double *state_
                                                                slice, vec);
           },
           [&](dim3 grid, size_t smem, int a0, int vec) {
-            factor_group<<<grid, kGroupThreads, smem, s>>>(T, f->params, S, sc, world_status, kind,
-                                                            k.gamma_dt, a0, vec);
+            auto kern = f->lv_wide[l] ? factor_group<true> : factor_group<false>;
+            kern<<<grid, kGroupThreads, smem, s>>>(T, f->params, S, sc, world_status, kind,
+                                                   k.gamma_dt, a0, vec);
           });
       if (ce != cudaSuccess) return ce;
     }

@@ -134,7 +134,8 @@ class FieldTissue:
 
     def level_kinds(self):
         """cb_field_levels: per level of the factor plan (leaves first), 0 when its fronts go one
-        per warp, 1 when one per CTA (the separators' group kernels)."""
+        per warp, 1 when one per CTA (the separators' group kernels), 2 when one per CTA with the
+        wide factor (fronts of 48 columns or more)."""
         n = int(self.lib.cb_field_levels(self.handle, None, 0))
         if n < 0:
             raise RuntimeError("cb_field_levels: null handle")

@@ -470,7 +470,8 @@ int cb_field_flops(const cb_field *f, double out[2]);
 /* The factor plan's levels (leaves first): kinds[l] (l < capacity; kinds may be NULL) = 0 when
  * level l's fronts go one per warp (factor_warps, forward_warps, backward_warps), 1 when one per
  * CTA (factor_group, forward_group, backward_group: separators whose front block exceeds 1280
- * doubles or whose front has more than 256 rows). Returns the number of levels (-1: null
+ * doubles or whose front has more than 256 rows), 2 when one per CTA with the wide factor (such
+ * a level whose widest front has 48 columns or more). Returns the number of levels (-1: null
  * handle). */
 int32_t cb_field_levels(const cb_field *f, int32_t *kinds, int32_t capacity);
 /* Control: membrane [W*N], junction [W*E], pump [W*N] availabilities, back to back. */
