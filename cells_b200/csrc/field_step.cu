@@ -610,7 +610,8 @@ __global__ void __launch_bounds__(kGroupThreads, WIDE ? 2 : 6)
   if (bad) base[S.ctl + 7] = 1.0;
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
+// The substitutions' warp kernels at eight CTAs per SM's registers (their small leaf slices fit).
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 8)
     forward_warps(const Topo T, const Scratch S, double *scratch, const uint32_t *status, int a0,
                   int fronts, int W, int slice, int vec) {
   extern __shared__ __align__(16) double sm[];
@@ -638,7 +639,7 @@ __global__ void __launch_bounds__(kGroupThreads)
     base[S.ctl + 7] = 1.0;
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 8)
     backward_warps(const Topo T, const Scratch S, double *scratch, const uint32_t *status,
                    long long out_off, int a0, int fronts, int W, int slice, int vec) {
   extern __shared__ __align__(16) double sm[];
@@ -754,8 +755,9 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   };
   // Explicit rates at a stage (surface_pump.explicit_rates): concentrations in CI/CO, cell
   // potentials PC, node potentials PHI, gates g(e), into rate block K. Face diffusion uses the
-  // stage's own weights (W ln(a/b)).
-  auto explicit_rates = [&](double *Kb, auto gate) -> unsigned {
+  // stage's own weights (W ln(a/b)); at the step start (start) those are the start field's
+  // factor means FM and log differences LD, the same values the logmean gives.
+  auto explicit_rates = [&](double *Kb, auto gate, bool start) -> unsigned {
     unsigned bits = 0;
     double *kn = Kb + S.rk_n, *kmt = Kb + S.rk_mt, *kmd = Kb + S.rk_md, *kcy = Kb + S.rk_cy,
            *kpd = Kb + S.rk_pd, *kmw = Kb + S.rk_mw, *kjt = Kb + S.rk_jt, *kjd = Kb + S.rk_jd,
@@ -845,10 +847,15 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       const double dv = PHI[a] - PHI[b];
       if (!(fabs(dv * FRT) <= kMaxAbsX)) bits |= CB_WORLD_TRANSPORT;
       for (int s = 0; s < 3; ++s) {
-        double mean, lg;
-        logmean(CO[s * O + a], CO[s * O + b], mean, lg);
-        const double wgt = P.ff[s * WF + f0 + f] * mean / 1e-15;
-        const double d = wgt * (LCO[s * O + a] - LCO[s * O + b]);
+        double d;
+        if (start) {  // the step start's concentrations: their factor mean and log difference
+          d = (FM[s * F + f] / 1e-15) * LD[s * F + f];
+        } else {
+          double mean, lg;
+          logmean(CO[s * O + a], CO[s * O + b], mean, lg);
+          const double wgt = P.ff[s * WF + f0 + f] * mean / 1e-15;
+          d = wgt * (LCO[s * O + a] - LCO[s * O + b]);
+        }
         kfd[s * F + f] = d;
         if (!is_finite(d)) bits |= CB_WORLD_TRANSPORT;
       }
@@ -965,13 +972,15 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       }
       __syncthreads();
     };
-  // The stage solve's right-hand side on known amounts (cells n(s,i), nodes o(s,m)), into Y (and
-  // RTv, kept for the residual check).
-  auto stage_rhs = [&](auto n, auto o) {
+  // The stage solve's right-hand side on known amounts (cells n(s,i), nodes o3(m, v[3])), into Y
+  // (and RTv, kept for the residual check).
+  auto stage_rhs = [&](auto n, auto o3) {
     for (int m = tid; m < O; m += BLOCK) {
       const int u = T.upos[m];
       if (u < 0) continue;
-      double q = P.q0o[o0 + m] + kChargePerFmol * ((o(0, m) + o(1, m)) + (-o(2, m)));
+      double ov[3];
+      o3(m, ov);
+      double q = P.q0o[o0 + m] + kChargePerFmol * ((ov[0] + ov[1]) + (-ov[2]));
       const int i = T.ncell[m];
       if (i >= 0)
         q = q + (P.q0[c0 + i] + kChargePerFmol * ((n(0, i) + n(1, i)) + (-n(2, i))));
@@ -1029,15 +1038,18 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       }
       __syncthreads();
     };
-    // A node's drift inflow of species s (scatter to receivers less scatter from senders).
-    auto drift_inflow = [&](const double *D, int s, int m) {
-      double in = 0.0, out = 0.0;
+    // A node's drift inflow of each species (scatter to receivers less scatter from senders), in
+    // one pass over its faces.
+    auto drift_inflow3 = [&](const double *D, int m, double (&r)[3]) {
+      double in[3] = {0.0, 0.0, 0.0}, out[3] = {0.0, 0.0, 0.0};
       for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
-        const int code = T.nf_idx[q];
-        if (code & 1) in += D[s * F + (code >> 1)];
-        else out += D[s * F + (code >> 1)];
+        const int code = T.nf_idx[q], f = code >> 1;
+        for (int s = 0; s < 3; ++s) {
+          if (code & 1) in[s] += D[s * F + f];
+          else out[s] += D[s * F + f];
+        }
       }
-      return in - out;
+      for (int s = 0; s < 3; ++s) r[s] = in[s] - out[s];
     };
   auto known1_cell = [&](int s, int i) {
     return n0[s * WN + c0 + i] + k.gamma_dt * K0[S.rk_n + s * N + i];
@@ -1049,11 +1061,17 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     return (n0[s * WN + c0 + i] + k.delta_dt * K0[S.rk_n + s * N + i]) +
            k.omdelta_dt * K1[S.rk_n + s * N + i];
   };
-  auto known2_node = [&](int s, int m) {
+  auto known1_node3 = [&](int m, double (&v)[3]) {
+    for (int s = 0; s < 3; ++s) v[s] = known1_node(s, m);
+  };
+  auto known2_node3 = [&](int m, double (&v)[3]) {
     const bool held = T.upos[m] < 0;
-    return ((x0[s * WO + o0 + m] + k.delta_dt * K0[S.rk_x + s * O + m]) +
-            k.omdelta_dt * K1[S.rk_x + s * O + m]) +
-           omgamma_dt * (held ? 0.0 : drift_inflow(D1, s, m));
+    double d1[3] = {0.0, 0.0, 0.0};
+    if (!held) drift_inflow3(D1, m, d1);
+    for (int s = 0; s < 3; ++s)
+      v[s] = ((x0[s * WO + o0 + m] + k.delta_dt * K0[S.rk_x + s * O + m]) +
+              k.omdelta_dt * K1[S.rk_x + s * O + m]) +
+             omgamma_dt * (held ? 0.0 : d1[s]);
   };
   // The Newton's next right-hand side: -R for an active world, 0 otherwise.
   auto newton_rhs = [&](bool active) {
@@ -1159,24 +1177,28 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       if (!(valid && ctl[2] != 0.0 && n2 <= kNewtonTarget)) bits |= CB_WORLD_FIELD;
     }
     // ---- stage 0: explicit rates at the start potentials ---------------------------------
-    bits |= explicit_rates(K0, [&](int e) { return g0[e]; });
+    bits |= explicit_rates(K0, [&](int e) { return g0[e]; }, true);
     // The readouts' extracellular rate (membrane flux, whole face flux at the start field, the
     // pump's transfer) and the half-step prediction of the node concentrations.
     for (int m = tid; m < O; m += BLOCK) {
       const int i = T.ncell[m];
       const bool held = T.upos[m] < 0;
-      for (int s = 0; s < 3; ++s) {
-        const double z = s < 2 ? 1.0 : -1.0;
-        double a = 0.0, out = 0.0, in = 0.0;
-        if (i >= 0) a = 0.0 + K0[S.rk_mt + s * N + i];
-        for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
-          const int code = T.nf_idx[q], f = code >> 1;
-          const double mu = RT * LD[s * F + f] + z * kF * (PHI[T.fs[f]] - PHI[T.fr[f]]);
+      double outs[3] = {0.0, 0.0, 0.0}, ins[3] = {0.0, 0.0, 0.0};
+      for (int q = T.nf_ptr[m]; q < T.nf_ptr[m + 1]; ++q) {
+        const int code = T.nf_idx[q], f = code >> 1;
+        const double dv = PHI[T.fs[f]] - PHI[T.fr[f]];
+        for (int s = 0; s < 3; ++s) {
+          const double z = s < 2 ? 1.0 : -1.0;
+          const double mu = RT * LD[s * F + f] + z * kF * dv;
           const double flux = FM[s * F + f] * mu / (RT * 1e-15);
-          if (code & 1) in += flux;
-          else out += flux;
+          if (code & 1) ins[s] += flux;
+          else outs[s] += flux;
         }
-        double rate = held ? 0.0 : (a - out) + in;
+      }
+      for (int s = 0; s < 3; ++s) {
+        double a = 0.0;
+        if (i >= 0) a = 0.0 + K0[S.rk_mt + s * N + i];
+        double rate = held ? 0.0 : (a - outs[s]) + ins[s];
         if (!held && i >= 0) rate = rate + K0[S.rk_ex + s * N + i];
         const double amount = P.oref[s * WO + o0 + m] +
                               st(CB_FIELD_EXTRACELLULAR_INCREMENT)[s * WO + o0 + m];
@@ -1198,7 +1220,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     __syncthreads();
     __syncthreads();
     if (tid == 0) ctl[7] = 0.0;  // the operator factor's pivot flag
-    stage_rhs(known1_cell, known1_node);
+    stage_rhs(known1_cell, known1_node3);
     bits_out(bits);
     return;
   }
@@ -1210,16 +1232,18 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       for (int s = 0; s < 3; ++s) N1[s * N + i] = known1_cell(s, i);
     for (int m = tid; m < O; m += BLOCK) {
       const bool held = T.upos[m] < 0;
+      double d1[3] = {0.0, 0.0, 0.0};
+      if (!held) drift_inflow3(D1, m, d1);
       for (int s = 0; s < 3; ++s)
-        O1[s * O + m] = known1_node(s, m) + k.gamma_dt * (held ? 0.0 : drift_inflow(D1, s, m));
+        O1[s * O + m] = known1_node(s, m) + k.gamma_dt * (held ? 0.0 : d1[s]);
     }
     for (int e = tid; e < E; e += BLOCK) G1[e] = g0[e] + k.gamma_dt * K0[S.rk_g + e];
     __syncthreads();
     bits |= set_conc([&](int s, int i) { return N1[s * N + i]; },
                      [&](int s, int m) { return O1[s * O + m]; });
     __syncthreads();
-    bits |= explicit_rates(K1, [&](int e) { return G1[e]; });
-    stage_rhs(known2_cell, known2_node);
+    bits |= explicit_rates(K1, [&](int e) { return G1[e]; }, false);
+    stage_rhs(known2_cell, known2_node3);
     bits_out(bits);
     return;
   }
@@ -1264,12 +1288,17 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       const double g = (g0[e] + ddt * K0[S.rk_g + e]) + odt * K1[S.rk_g + e];
       if (!(is_finite(jd) && is_finite(g))) dom = 1u;
     }
-    for (int m = tid; m < O; m += BLOCK)
+    for (int m = tid; m < O; m += BLOCK) {
+      const bool held = T.upos[m] < 0;
+      double k2[3], d2[3] = {0.0, 0.0, 0.0};
+      known2_node3(m, k2);
+      if (!held) drift_inflow3(D2, m, d2);
       for (int s = 0; s < 3; ++s) {
-        const double v = known2_node(s, m) + gdt * (T.upos[m] < 0 ? 0.0 : drift_inflow(D2, s, m));
+        const double v = k2[s] + gdt * (held ? 0.0 : d2[s]);
         O1[s * O + m] = v;
         if (!(is_finite(v) && P.oref[s * WO + o0 + m] + v > 0.0)) dom = 1u;
       }
+    }
     if (block_or<BLOCK>(dom, sBits)) bits |= CB_WORLD_DOMAIN;
     bits = block_or<BLOCK>(bits, sBits);
     if (bits) {
@@ -1322,11 +1351,15 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     // so their electrodes deliver nothing (electrode charge and work unchanged).
     for (int m = tid; m < O; m += BLOCK) {
       const bool held = T.upos[m] < 0;
-      double nv[3], sup[3];
+      double nv[3], sup[3], h1[3] = {0.0, 0.0, 0.0}, h2[3] = {0.0, 0.0, 0.0};
+      if (held) {
+        drift_inflow3(D1, m, h1);
+        drift_inflow3(D2, m, h2);
+      }
       for (int s = 0; s < 3; ++s) {
         nv[s] = O1[s * O + m];
-        const double i1 = held ? -drift_inflow(D1, s, m) : 0.0;
-        const double i2 = held ? -drift_inflow(D2, s, m) : 0.0;
+        const double i1 = held ? -h1[s] : 0.0;
+        const double i2 = held ? -h2[s] : 0.0;
         const double k0s = K0[S.rk_s + s * O + m], k1s = K1[S.rk_s + s * O + m];
         double *v = st(CB_FIELD_RESERVOIR_SUPPLIED) + s * WO + o0 + m;
         *v = (((*v + ddt * k0s) + odt * k1s) + omgamma_dt * i1) + gdt * i2;
