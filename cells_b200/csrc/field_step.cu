@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -1677,7 +1678,11 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
       af_ptr[q + 1] = (int)af_face.size();
     }
   }
-  // A level's fronts go one per warp (their blocks and rows small) or one per CTA.
+  // A level's fronts go one per warp (their blocks and rows small) or one per CTA. Override for
+  // sweeps: CELLS_B200_FIELD_WARP_BLOCK (the largest block, in doubles, a warp takes).
+  long long warp_block = kWarpBlock;
+  if (const char *env = std::getenv("CELLS_B200_FIELD_WARP_BLOCK"))
+    warp_block = std::max(1, std::min(std::atoi(env), kWarpBlock));
   f->lv_ptr = sp.lv_ptr;
   f->lv_warp.assign(sp.levels, 0);
   f->lv_wide.assign(sp.levels, 0);
@@ -1694,7 +1699,7 @@ extern "C" int cb_field_bind(const cb_field_desc *d, int device, cb_field **out)
     }
     f->lv_block[l] = (int)mb;
     f->lv_m[l] = mm;
-    f->lv_warp[l] = (mb <= kWarpBlock && mm <= kWarpVector) ? 1 : 0;
+    f->lv_warp[l] = (mb <= warp_block && mm <= kWarpVector) ? 1 : 0;
     f->lv_wide[l] = (!f->lv_warp[l] && ms >= kWideColumns) ? 1 : 0;
     const long long need =
         f->lv_warp[l] ? (long long)kWarpsPerCta * level_slice(mb, mm) : level_vec(mb) + mm;
