@@ -291,28 +291,69 @@ __device__ __forceinline__ void patch_mu(const double *__restrict__ wc, const do
     mu[s] = wc[WC_RT] * (lc[s] - wc[WC_LOGCO + s]) + ((s < 2) ? kF * dv : (-kF) * dv);
 }
 
+// The dense tail of a world's plan: the longest end of its final run of one-column levels (the
+// top separator's chain) whose columns are the plan's last t columns n - t .. n - 1 in order, each
+// dense below its diagonal. Returns t (0 when shorter than 2).
+__device__ inline int dense_tail(const int *colp, const int *lvp, const int *lvc, int lv0, int lv1,
+                                 int n) {
+  int t = 0;
+  for (int l = lv1 - 1; l >= lv0 && lvp[l + 1] - lvp[l] == 1; --l) {
+    const int j = lvc[lvp[l]];
+    if (j != n - 1 - t || colp[j + 1] - colp[j] != n - j) break;
+    ++t;
+  }
+  return t >= 2 ? t : 0;
+}
+
 // One world's sparse Cholesky on its plan (local indices; values and vectors by position), as one
 // CTA of BLOCK threads runs it: left-looking factor by levels of the elimination tree, a warp per
 // column (update terms in ascending k, each term's rows at precomputed offsets in the column,
 // so no atomics); a run of one-column levels (the top separator's chain) by warp 0 alone with
-// warp syncs only; forward and back substitution of L L^T x = b (b in Yv, x to Xv), a thread per
-// column, or warp 0 with the dot products across its lanes (a fixed xor tree) on those runs.
+// warp syncs only, except a dense tail (dense_tail), whose columns' updates from the columns
+// before it go one column per warp and whose own block is factored right-looking by the CTA;
+// forward and back substitution of L L^T x = b (b in Yv, x to Xv), a thread per column on wide
+// levels, a warp per column with the dot products across its lanes (a fixed xor tree) on narrow
+// levels and on the runs. Each factor entry sees the same operations in the same order in every
+// form.
 template <typename FT, int BLOCK>
 struct WorldCholesky {
   const int *colp, *lrow, *ukp, *ukc, *ukpos, *ukrel, *rel, *lvp, *lvc;
   FT *lval, *Yv, *Xv;
   int lv0, lv1;
+  int n, tail;  // the world's columns; its dense tail's length (0: none)
 
+  // Update terms u0 .. u1 of the column at cj (ascending k), those with k below klim, in order:
+  // lanes over a term's rows, a warp sync between terms. The next term's indices and multiplier
+  // are read before this term's rows are written: they lie in finished columns.
+  __device__ void apply_updates(int cj, int u0, int u1, int klim, int lane) const {
+    if (u0 >= u1 || ukc[u0] >= klim) return;
+    int kk = ukc[u0], p = ukpos[u0], r0 = ukrel[u0];
+    int cnt = colp[kk + 1] - p;
+    FT ljk = lval[p];
+    for (int u = u0;; ++u) {
+      const bool more = u + 1 < u1 && ukc[u + 1] < klim;
+      int np = 0, nr0 = 0, ncnt = 0;
+      FT nl = 0;
+      if (more) {
+        const int nk = ukc[u + 1];
+        np = ukpos[u + 1];
+        nr0 = ukrel[u + 1];
+        ncnt = colp[nk + 1] - np;
+        nl = lval[np];
+      }
+      for (int t = lane; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
+      __syncwarp();
+      if (!more) break;
+      p = np;
+      r0 = nr0;
+      cnt = ncnt;
+      ljk = nl;
+    }
+  }
   __device__ uint32_t factor_column(int j, int lane) const {
     uint32_t bad = 0;
     const int cj = colp[j];
-    for (int u = ukp[j]; u < ukp[j + 1]; ++u) {
-      const int kk = ukc[u], p = ukpos[u], r0 = ukrel[u];
-      const int cnt = colp[kk + 1] - p;
-      const FT ljk = lval[p];
-      for (int t = lane; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
-      __syncwarp();
-    }
+    apply_updates(cj, ukp[j], ukp[j + 1], j, lane);
     FT piv = 0;
     if (lane == 0) {
       const FT d = lval[cj];
@@ -333,6 +374,41 @@ struct WorldCholesky {
     while (end < lv1 && lvp[end + 1] - lvp[end] == 1) ++end;
     return end;
   }
+  // The dense tail j0 .. n - 1: first each tail column's updates from the columns before the
+  // tail (ascending k, as factor_column takes them), warps over the tail's columns, which touch
+  // only their own column; then the tail block right-looking, a column at a time: warp 0 takes
+  // the pivot and scales the column, the warps take its products out of the later columns (each
+  // entry's updates still in ascending k, the same products as factor_column's).
+  __device__ uint32_t factor_tail(int j0) const {
+    constexpr int WARPS = BLOCK / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t bad = 0;
+    for (int j = j0 + warp; j < n; j += WARPS) apply_updates(colp[j], ukp[j], ukp[j + 1], j0, lane);
+    __syncthreads();
+    for (int j = j0; j < n; ++j) {
+      const int cj = colp[j], len = n - j;
+      if (warp == 0) {
+        FT piv = 0;
+        if (lane == 0) {
+          const FT d = lval[cj];
+          if (!(d > 0.0) || !is_finite(d)) bad = 1u;
+          piv = sqrt(d);
+          lval[cj] = piv;
+        }
+        piv = __shfl_sync(0xffffffffu, piv, 0);
+        const FT inv = FT(1) / piv;
+        for (int t = 1 + lane; t < len; t += 32) lval[cj + t] *= inv;
+      }
+      __syncthreads();
+      for (int jj = j + 1 + warp; jj < n; jj += WARPS) {
+        const FT l = lval[cj + (jj - j)];
+        const int cjj = colp[jj];
+        for (int r = jj + lane; r < n; r += 32) lval[cjj + (r - jj)] -= lval[cj + (r - j)] * l;
+      }
+      __syncthreads();
+    }
+    return bad;
+  }
   __device__ uint32_t factor() const {
     constexpr int WARPS = BLOCK / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -341,6 +417,15 @@ struct WorldCholesky {
       const int a0 = lvp[lv], a1 = lvp[lv + 1];
       if (a1 - a0 == 1) {
         const int end = single_run_end(lv);
+        if (tail > 0 && end == lv1) {  // the final run: its head by warp 0, then the dense tail
+          const int head = end - tail;
+          if (warp == 0)
+            for (int l = lv; l < head; ++l) bad |= factor_column(lvc[lvp[l]], lane);
+          __syncthreads();
+          bad |= factor_tail(lvc[lvp[head]]);
+          lv = end;
+          continue;
+        }
         if (warp == 0)
           for (int l = lv; l < end; ++l) bad |= factor_column(lvc[lvp[l]], lane);
         lv = end;
@@ -357,6 +442,7 @@ struct WorldCholesky {
     return v;
   }
   __device__ void solve() const {
+    constexpr int WARPS = BLOCK / 32;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int lv = lv0; lv < lv1;) {
       const int a0 = lvp[lv], a1 = lvp[lv + 1];
@@ -374,6 +460,16 @@ struct WorldCholesky {
           }
         }
         lv = end;
+      } else if (a1 - a0 <= 2 * WARPS) {  // a narrow level: a warp per column
+        for (int a = a0 + warp; a < a1; a += WARPS) {
+          const int j = lvc[a];
+          FT part = 0;
+          for (int u = ukp[j] + lane; u < ukp[j + 1]; u += 32)
+            part += lval[ukpos[u]] * Yv[ukc[u]];
+          part = warp_sum(part);
+          if (lane == 0) Yv[j] = (Yv[j] - part) / lval[colp[j]];
+        }
+        ++lv;
       } else {
         for (int a = a0 + tid; a < a1; a += BLOCK) {
           const int j = lvc[a];
@@ -402,6 +498,16 @@ struct WorldCholesky {
           }
         }
         lv = begin - 1;
+      } else if (a1 - a0 <= 2 * WARPS) {  // a narrow level: a warp per column
+        for (int a = a0 + warp; a < a1; a += WARPS) {
+          const int j = lvc[a];
+          const int cj = colp[j], len = colp[j + 1] - cj;
+          FT part = 0;
+          for (int t = 1 + lane; t < len; t += 32) part += lval[cj + t] * Xv[lrow[cj + t]];
+          part = warp_sum(part);
+          if (lane == 0) Xv[j] = (Yv[j] - part) / lval[cj];
+        }
+        --lv;
       } else {
         for (int a = a0 + tid; a < a1; a += BLOCK) {
           const int j = lvc[a];
@@ -510,7 +616,8 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   uint32_t refused = 0u;
 
   const WorldCholesky<FT, BLOCK> chol{colp, lrow, ukp, ukc, ukpos, ukrel, rel, lvp, lvc,
-                                       lval, Yv, Xv, lv0, lv1};
+                                       lval, Yv, Xv, lv0, lv1, wn,
+                                       dense_tail(colp, lvp, lvc, lv0, lv1, wn)};
   auto factor = [&]() { return chol.factor(); };
   auto solve = [&]() { chol.solve(); };
   // A cell's gather over its junctions (senders first, then receivers, edge order) of field f.
@@ -1264,8 +1371,10 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     lvc = stage_ints(lvc, wn);
     if (mode == 2) rel = stage_ints(rel, wR);
   }
+  __syncthreads();  // the staged plan, read by dense_tail
   const WorldCholesky<double, BLOCK> chol{colp, lrow, ukp, ukc, ukpos, ukrel, rel, lvp, lvc,
-                                          lval, Yv, Xv, 0, wL};
+                                          lval, Yv, Xv, 0, wL, wn,
+                                          dense_tail(colp, lvp, lvc, 0, wL, wn)};
   const long long oN = L.s[CB_AMOUNT_INCREMENT], oG = L.s[CB_JUNCTION_GATE];
   const long long oH = L.s[CB_CHANNEL_GATE];
   const double *mctl = control + L.c[CB_CONTROL_MEMBRANE];
