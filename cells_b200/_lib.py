@@ -73,6 +73,8 @@ EXPORTS = (
     "cb_balances",
     "cb_step_vjp",
     "cb_vjp_workspace",
+    "cb_step_vjp_method",
+    "cb_vjp_workspace_method",
     "cb_set_permeability",
     "cb_set_channel_block",
     "cb_device_checks",
@@ -222,6 +224,12 @@ def load(path=LIBRARY):
     lib.cb_step_vjp.restype = ctypes.c_int
     lib.cb_vjp_workspace.argtypes = [_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
     lib.cb_vjp_workspace.restype = ctypes.c_int
+    lib.cb_step_vjp_method.argtypes = [_p, ctypes.c_int, _p, ctypes.c_double, _p, ctypes.c_int,
+                                       _p, _p, _p, _p, _p, _p, ctypes.c_size_t, _p, _p]
+    lib.cb_step_vjp_method.restype = ctypes.c_int
+    lib.cb_vjp_workspace_method.argtypes = [_p, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_size_t)]
+    lib.cb_vjp_workspace_method.restype = ctypes.c_int
     lib.cb_set_permeability.argtypes = [_p, _p, _p, _p, _p]
     lib.cb_set_permeability.restype = ctypes.c_int
     lib.cb_set_channel_block.argtypes = [_p, ctypes.c_int32, _d, _d, _d, _d]

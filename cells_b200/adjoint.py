@@ -7,12 +7,14 @@ checkpoints every K steps and recomputation.
     loss = adjoint.voltage_loss(tissue, final, target).sum()
     loss.backward()            # membrane.grad [3, C], junction.grad [3, E], channel.grad [NCH, C]
 
-The forward runs the FP64 ARS(2,2,2) step (CB_METHOD_ARS222) for n_steps steps in segments of
-``every`` steps and keeps each segment's first state (the checkpoints). The reverse walks the
-segments last to first: cb_step_vjp recomputes a segment from its checkpoint (one step per
-launch, each step-start state kept in a workspace of one segment) and applies the transposed
-step, carrying the state's cotangent and adding the permeability gradients. Peak device memory:
-the checkpoints (n_steps / every states) plus one segment of states.
+The forward runs the FP64 step of ``method`` (METHOD_ARS222, the reference's ARS(2,2,2), or
+METHOD_ROS2, the Rosenbrock step) for n_steps steps in segments of ``every`` steps and keeps each
+segment's first state (the checkpoints). The reverse walks the segments last to first:
+cb_step_vjp_method recomputes a segment from its checkpoint (one step per launch, each
+step-start state kept in a workspace of one segment; for ROS2 also each step's factor of its
+voltage operator, which the transposed stage solves reuse) and applies the transposed step,
+carrying the state's cotangent and adding the permeability gradients. Peak device memory: the
+checkpoints (n_steps / every states) plus one segment of states (and, for ROS2, records).
 
 The reference differentiates its step with JAX (``jax.jvp``/``jacfwd`` in
 src/cells/analysis/stationary.py:505-514); a loss gradient there would be ``jax.grad`` of the
@@ -45,7 +47,7 @@ class _Trajectory:
             class Trajectory(torch.autograd.Function):
                 @staticmethod
                 def forward(ctx, membrane, junction, channel, state0, tissue, control, dt,
-                            n_steps, every):
+                            n_steps, every, method):
                     nch = tissue.batch.channel_slots
                     tissue.set_permeability(membrane.contiguous(), junction.contiguous(),
                                             channel.contiguous() if nch else None)
@@ -61,11 +63,11 @@ class _Trajectory:
                         checkpoints.append(state)
                         lengths.append(k)
                         nxt = torch.empty_like(state)
-                        tissue.step(state, nxt, control, dt, k, status)
+                        tissue.step(state, nxt, control, dt, k, status, method=method)
                         refused |= status
                         state = nxt
                         done += k
-                    ctx.tissue, ctx.control, ctx.dt = tissue, control, dt
+                    ctx.tissue, ctx.control, ctx.dt, ctx.method = tissue, control, dt, method
                     ctx.checkpoints, ctx.lengths = checkpoints, lengths
                     ctx.save_for_backward(membrane, junction, channel)
                     ctx.mark_non_differentiable(refused)
@@ -89,18 +91,18 @@ class _Trajectory:
                     status = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
                     bits = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
                     if ctx.lengths:
-                        ws = torch.empty(tissue.vjp_workspace_bytes(max(ctx.lengths)),
+                        ws = torch.empty(tissue.vjp_workspace_bytes(max(ctx.lengths), ctx.method),
                                          dtype=torch.uint8, device=dev)
                     for start, k in zip(reversed(ctx.checkpoints), reversed(ctx.lengths),
                                         strict=True):
                         tissue.step_vjp(start, ctx.control, ctx.dt, k, cot, cot, gm, gj,
-                                        gch if nch else None, ws, status)
+                                        gch if nch else None, ws, status, method=ctx.method)
                         bits |= status
                     ctx.checkpoints = None
                     tissue.last_vjp_status = bits
                     return (gm.view(3, b.cells), gj[:3 * b.edges].view(3, b.edges),
                             gch[:nch * b.cells].view(nch, b.cells), cot,
-                            None, None, None, None, None)
+                            None, None, None, None, None, None)
 
             cls.fn = Trajectory
         return cls.fn
@@ -119,9 +121,11 @@ def permeabilities(tissue, device=None):
     return t(b.permeability), t(b.junction_permeability), t(b.channel_permeability)
 
 
-def trajectory(tissue, state, control, dt, n_steps, membrane, junction, channel=None, every=100):
-    """The state after n_steps FP64 steps from ``state`` (a float64 device tensor in the state
-    layout), differentiable with respect to the permeabilities (and ``state``). Returns
+def trajectory(tissue, state, control, dt, n_steps, membrane, junction, channel=None, every=100,
+               method=None):
+    """The state after n_steps FP64 steps of ``method`` (default METHOD_ARS222; or METHOD_ROS2)
+    from ``state`` (a float64 device tensor in the state layout), differentiable with respect to
+    the permeabilities (and ``state``). Returns
     (final state, refused[W]): refused holds the refusal bits met on the way (a world refused at
     a step stays where it was for that step, and its gradient is that of the map it followed)."""
     torch = _torch()
@@ -130,8 +134,13 @@ def trajectory(tissue, state, control, dt, n_steps, membrane, junction, channel=
     if channel is None:
         channel = torch.zeros((tissue.batch.channel_slots, tissue.batch.cells),
                               dtype=torch.float64, device=state.device)
+    from . import _lib
+
+    method = _lib.METHOD_ARS222 if method is None else int(method)
+    if method not in (_lib.METHOD_ARS222, _lib.METHOD_ROS2):
+        raise ValueError("the reverse covers METHOD_ARS222 and METHOD_ROS2")
     return _Trajectory.get().apply(membrane, junction, channel, state, tissue, control, float(dt),
-                                   int(n_steps), int(every))
+                                   int(n_steps), int(every), method)
 
 
 def _cell_constants(tissue, device):

@@ -49,6 +49,13 @@ void n2_release(cb_tissue *t);
 int ros2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
               const double *control, int n_steps, uint32_t *world_status,
               int32_t *accepted_steps, cudaStream_t stream, bool rk4);
+// One ROS2 step that also records what the reverse needs (R2Tape, n2_common.cuh).
+struct R2Tape;
+int ros2_step_tape(cb_tissue *t, const double *state_in, double *state_out, double dt,
+                   const double *control, int n_steps, uint32_t *world_status,
+                   int32_t *accepted_steps, cudaStream_t stream, bool rk4, const R2Tape &tape);
+// The N2 plan's build (idempotent), for the ROS2 reverse.
+int n2_build_plan(cb_tissue *t);
 }  // namespace cbk
 
 struct cb_tissue {

@@ -14,7 +14,7 @@ This mirrors the reference's model-module protocol for the resolved pump-leak ti
 * ``Tissue.device_checks(...)`` ~ @3's ``device_checks(previous, row, p, constants, steps)``
   (surface_pump_v3.py:5572-5597): the accepted-row checks, bitmask and diagnostics per world.
 * ``Tissue.step_vjp(...)``     ~ ``jax.vjp`` of ``checked_step`` repeated ``n_steps`` times
-  (cb_step_vjp); ``Tissue.set_permeability`` rebinds the permeabilities on the device.
+  (cb_step_vjp_method: the ARS(2,2,2) step or ROS2); ``Tissue.set_permeability`` rebinds the permeabilities on the device.
 
 State is a dict of NumPy arrays in the packed layout (``_lib.STATE_FIELDS``; cell fields [3, C]
 or [C], junction fields [3, E] or [E], world fields [3, W] or [W]). Device buffers are torch
@@ -304,23 +304,26 @@ class Tissue:
         _lib.check(self.lib.cb_set_channel_block(
             self.handle, block.modes, *(_ptr(a, ctypes.c_double) for a in arrays)))
 
-    def vjp_workspace_bytes(self, n_steps):
+    def vjp_workspace_bytes(self, n_steps, method=_lib.METHOD_ARS222):
         out = ctypes.c_size_t()
-        _lib.check(self.lib.cb_vjp_workspace(self.handle, int(n_steps), ctypes.byref(out)))
+        _lib.check(self.lib.cb_vjp_workspace_method(self.handle, int(method), int(n_steps),
+                                                    ctypes.byref(out)))
         return int(out.value)
 
     def step_vjp(self, state_in, control, dt, n_steps, cot_out, cot_in, grad_membrane,
-                 grad_junction, grad_channel, workspace, status, stream=None):
-        """cb_step_vjp on device tensors: cotangent of the state after n_steps steps in, of
-        state_in out (may alias); permeability gradients added to grad_* (float64 [3C], [3E],
-        [NCH C]); workspace a uint8 tensor of vjp_workspace_bytes(n_steps); status int32 [W]."""
+                 grad_junction, grad_channel, workspace, status, stream=None,
+                 method=_lib.METHOD_ARS222):
+        """cb_step_vjp_method on device tensors (METHOD_ARS222 or METHOD_ROS2): cotangent of the
+        state after n_steps steps in, of state_in out (may alias); permeability gradients added
+        to grad_* (float64 [3C], [3E], [NCH C]); workspace a uint8 tensor of
+        vjp_workspace_bytes(n_steps, method); status int32 [W]."""
 
         def ptr(t):
             return None if t is None else ctypes.c_void_p(t.data_ptr())
 
-        _lib.check(self.lib.cb_step_vjp(
-            self.handle, ptr(state_in), float(dt), ptr(control), int(n_steps), ptr(cot_out),
-            ptr(cot_in), ptr(grad_membrane), ptr(grad_junction), ptr(grad_channel),
+        _lib.check(self.lib.cb_step_vjp_method(
+            self.handle, int(method), ptr(state_in), float(dt), ptr(control), int(n_steps),
+            ptr(cot_out), ptr(cot_in), ptr(grad_membrane), ptr(grad_junction), ptr(grad_channel),
             ptr(workspace), int(workspace.numel()), ptr(status),
             None if stream is None else ctypes.c_void_p(stream),
         ))  # fmt: skip

@@ -351,6 +351,31 @@ int cb_step_vjp(cb_tissue *t, const double *state_in, double dt, const double *c
 int cb_vjp_workspace(const cb_tissue *t, int n_steps, size_t *bytes);
 
 /*
+ * The reverse-mode derivative of n_steps steps of `method`: CB_METHOD_ARS222 (cb_step_vjp) or
+ * CB_METHOD_ROS2, the same arguments and contract as cb_step_vjp. Replaces jax.vjp / jax.grad of
+ * the composed checked_step (models/surface_pump_v3.py:3989) for this library's ROS2 method, which
+ * has no counterpart in the reference (its only Rosenbrock integrator is the dense Rodas4 of
+ * numerics/rosenbrock_dense.py:123-141). For ROS2 the call first runs the n_steps steps forward,
+ * one step per launch, keeping in the workspace every state and each step's record: the factor of
+ * its voltage operator M = C + gamma h (G_patch + L(G_junction)), both stage solves' voltage
+ * rates, k1's dynamic rows and k2's gate rows. The reverse launch then transposes each step: its
+ * two stage solves reuse the step's recorded factor (M is symmetric), and the W-matrix's own
+ * dependence on the state and the permeabilities enters through the laws' second derivatives.
+ * Only the amounts, junction gates and channel gates carry the dynamics (ledger cotangents must be
+ * zero; CB_WORLD_LEDGER_COTANGENT otherwise). Gradients are ADDED to grad_membrane [3*C],
+ * grad_junction [3*E], grad_channel [NCH*C]. DEVICE pointers; stream-ordered, no host sync.
+ */
+int cb_step_vjp_method(cb_tissue *t, int method, const double *state_in, double dt,
+                       const double *control, int n_steps, const double *cot_out,
+                       double *cot_in, double *grad_membrane, double *grad_junction,
+                       double *grad_channel, void *workspace, size_t workspace_bytes,
+                       uint32_t *world_status, void *stream);
+/* Bytes of cb_step_vjp_method's workspace for n_steps steps of `method`. For CB_METHOD_ROS2 the
+ * first call builds the batch's sparse factor plan (device memory the handle keeps, as the first
+ * ROS2 step does): make it outside any stream capture. */
+int cb_vjp_workspace_method(cb_tissue *t, int method, int n_steps, size_t *bytes);
+
+/*
  * Replace the bound permeabilities (m/s) from DEVICE arrays: membrane [3*C], junction [3*E],
  * channel [NCH*C]; a NULL array keeps what is bound. The prefactors are formed by the same device
  * code as cb_bind's (area * P / 1e-15), so a step after this call is bit-identical to a step of a

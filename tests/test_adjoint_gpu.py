@@ -195,7 +195,7 @@ def test_set_permeability_matches_a_fresh_bind(cuda):
     outs = []
     for t in (tissue, fresh):
         st = torch.from_numpy(t.pack_state(t.initial_state())).to(dev)
-        out = torch.empty_like(st)
+        out = torch.zeros_like(st)  # the fields' 256-byte padding is never written
         status = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
         t.step(st, out, torch.from_numpy(t.pack_control()).to(dev), 1e-3, 30, status)
         outs.append(out.cpu().numpy())
