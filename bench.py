@@ -258,7 +258,8 @@ def sample_tasks(args, n, steps):
 
     stride = max(1, args.worlds // n)
     if args.workload == "adjoint":
-        return [("adjoint", w * stride, 4, args.cells, steps, args.dt) for w in range(n)], stride
+        kind = "adjoint_ros2" if args.method == "ros2" else "adjoint"
+        return [(kind, w * stride, 4, args.cells, steps, args.dt) for w in range(n)], stride
     if args.workload == "uneven":
         sizes = np.sort(worlds.uneven_sizes(args.worlds, seed=2))[::-1]
         return [("uneven", w * stride, 2, int(sizes[w * stride]), steps, args.dt)
@@ -276,7 +277,8 @@ def workload_name(args):
         return (f"adjoint sensitivities: {args.worlds} worlds per GPU x {args.cells}-cell "
                 "Delaunay tissues, NaV1.2 m^3 h + HH K n^4 populations, gradient of each world's "
                 "voltage-pattern loss after "
-                f"{args.trajectory} FP64 steps (dt {args.dt:g} s) w.r.t. all membrane, junction "
+                f"{args.trajectory} FP64 {'ROS2' if args.method == 'ros2' else 'ARS(2,2,2)'} "
+                f"steps (dt {args.dt:g} s) w.r.t. all membrane, junction "
                 f"and channel permeabilities, checkpoints every {args.every} steps")
     if args.workload == "uneven":
         return (f"uneven batch: {args.worlds} worlds per GPU of 32-4096 cells (log-uniform), "
@@ -301,7 +303,8 @@ def cpu_baseline(args, samples_per_core=2, steps=100):
             "value": rate / (args.cells * args.trajectory), "unit": ADJOINT_UNIT,
             "cores": procs, "kind": "port",
             "adjoint_cell_steps_per_s": rate,
-            "sample": (f"{n} of the {args.worlds} worlds (every {stride}th): 20 steps forward "
+            "sample": (f"{n} of the {args.worlds} worlds (every {stride}th): 20 "
+                       f"{'ROS2' if args.method == 'ros2' else 'ARS(2,2,2)'} steps forward "
                        "then the oracle adjoint back over them, one world per process, 1 BLAS "
                        f"thread, {wall:.1f} s wall; world-gradients/s = that rate of world-"
                        f"cell-steps / ({args.cells} cells x {args.trajectory} steps)"),
@@ -416,11 +419,18 @@ def vjp_bytes_per_cell_step(batch):
 
 def run_adjoint(args, rank, world_size, local_rank, dist, base):
     """The adjoint workload: each bench step is the gradient of every world's voltage-pattern
-    loss through cells_b200.adjoint (forward in checkpointed segments, cb_step_vjp back)."""
+    loss through cells_b200.adjoint (forward in checkpointed segments, cb_step_vjp_method back),
+    of the ARS(2,2,2) step or, with --method ros2, of the ROS2 step."""
     import torch
 
+    from cells_b200 import _lib as _lib_methods
     from cells_b200 import adjoint, worlds
     from cells_b200.tissue import Tissue
+
+    ros2 = args.method == "ros2"
+    method = _lib_methods.METHOD_ROS2 if ros2 else _lib_methods.METHOD_ARS222
+    fwd_name = "ros2_kernel" if ros2 else "packed_kernel"
+    rev_name = "ros2_vjp_kernel" if ros2 else "vjp_kernel"
 
     dev = torch.device("cuda", local_rank)
     batch = build_batch(args, rank)
@@ -434,7 +444,7 @@ def run_adjoint(args, rank, world_size, local_rank, dist, base):
 
     def gradient(state, perms):
         final, bits = adjoint.trajectory(tissue, state, control, args.dt, args.trajectory, *perms,
-                                         every=args.every)
+                                         every=args.every, method=method)
         loss = adjoint.voltage_loss(tissue, final, target)
         loss.sum().backward()
         return loss, bits
@@ -479,7 +489,7 @@ def run_adjoint(args, rank, world_size, local_rank, dist, base):
     k = min(args.every, args.trajectory)
     status = torch.zeros(w_count, dtype=torch.int32, device=dev)
     out = torch.empty_like(state0)
-    ws = torch.empty(tissue.vjp_workspace_bytes(k), dtype=torch.uint8, device=dev)
+    ws = torch.empty(tissue.vjp_workspace_bytes(k, method), dtype=torch.uint8, device=dev)
     cot = torch.zeros_like(state0)
     o = tissue.state_offsets["amount_increment"]
     cot[o:o + 3 * cells] = 1e-3
@@ -503,35 +513,36 @@ def run_adjoint(args, rank, world_size, local_rank, dist, base):
     def one_step_segment():
         src = state0
         for _ in range(k):
-            tissue.step(src, out, control, args.dt, 1, status)
+            tissue.step(src, out, control, args.dt, 1, status, method=method)
             src = out
 
-    fused_ms = timed(lambda: tissue.step(state0, out, control, args.dt, k, status))
+    fused_ms = timed(lambda: tissue.step(state0, out, control, args.dt, k, status,
+                                         method=method))
     onestep_ms = timed(one_step_segment)
     vjp_ms = timed(lambda: tissue.step_vjp(state0, control, args.dt, k, cot, out, gm, gj,
-                                           gch if nch else None, ws, status))
+                                           gch if nch else None, ws, status, method=method))
     reverse_ms = max(vjp_ms - onestep_ms, 1e-6)
     segments = -(-args.trajectory // args.every)
-    per_gradient = {"packed_kernel (forward, fused)": fused_ms * segments,
-                    "packed_kernel (recompute, one step per launch)": onestep_ms * segments,
-                    "vjp_kernel (reverse)": reverse_ms * segments}
+    per_gradient = {f"{fwd_name} (forward, fused)": fused_ms * segments,
+                    f"{fwd_name} (recompute, one step per launch)": onestep_ms * segments,
+                    f"{rev_name} (reverse)": reverse_ms * segments}
     total = sum(per_gradient.values())
     fwd_bytes = bytes_per_cell_step(batch) * cells
     rev_bytes = vjp_bytes_per_cell_step(batch) * cells
     peak, peak_kind = peaks()
     kernels = {
-        "packed_kernel": {"ms_per_gradient": (fused_ms + onestep_ms) * segments,
+        fwd_name: {"ms_per_gradient": (fused_ms + onestep_ms) * segments,
                           "share": (fused_ms + onestep_ms) * segments / total,
                           "achieved_gbs_fused": fwd_bytes * k / (fused_ms * 1e-3) / 1e9,
                           "achieved_gbs_one_step": fwd_bytes * k / (onestep_ms * 1e-3) / 1e9,
                           "bytes_per_cell_step": bytes_per_cell_step(batch)},
-        "vjp_kernel": {"ms_per_gradient": reverse_ms * segments,
+        rev_name: {"ms_per_gradient": reverse_ms * segments,
                        "share": reverse_ms * segments / total,
                        "achieved_gbs": rev_bytes * k / (reverse_ms * 1e-3) / 1e9,
                        "bytes_per_cell_step": vjp_bytes_per_cell_step(batch)},
     }
     dominant = max(kernels, key=lambda name: kernels[name]["share"])
-    if dominant == "vjp_kernel":
+    if dominant == rev_name:
         launch_ms, alg = reverse_ms, rev_bytes * k
     else:
         launch_ms, alg = fused_ms, fwd_bytes * k
@@ -575,7 +586,7 @@ def run_adjoint(args, rank, world_size, local_rank, dist, base):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded pump-leak tissues)",
             "config": {
-                "workload": workload_name(args), "method": METHOD,
+                "workload": workload_name(args), "method": METHOD_ROS2 if ros2 else METHOD,
                 "worlds_per_gpu": args.worlds, "cells_per_world": args.cells,
                 "cells_per_gpu": cells, "junctions_per_gpu": batch.edges,
                 "trajectory_steps": args.trajectory, "checkpoint_every": args.every,

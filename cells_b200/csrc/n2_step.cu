@@ -281,8 +281,10 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   FT *Xv = reinterpret_cast<FT *>(cs + (long long)NC_X * T.C) + wc0;
   const size_t values = sizeof(FT) * (size_t)(wF + 2 * wn);
   const size_t plan_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wF + 3 * wU + wL + 1 + wn);
+  const size_t small_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wL + 1 + wn);
   const int mode = values + plan_ints + sizeof(int) * (size_t)wR <= smem_bytes ? 2
                    : values + plan_ints <= smem_bytes                           ? 1
+                   : values + small_ints <= smem_bytes                          ? 3
                                                                                 : 0;
   if (mode > 0) {
     lval = reinterpret_cast<FT *>(n2_smem);
@@ -296,11 +298,13 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       return out;
     };
     colp = stage_ints(colp, wn + 1);
-    lrow = stage_ints(lrow, wF);
+    if (mode != 3) lrow = stage_ints(lrow, wF);
     ukp = stage_ints(ukp, wn + 1);
-    ukc = stage_ints(ukc, wU);
-    ukpos = stage_ints(ukpos, wU);
-    ukrel = stage_ints(ukrel, wU);
+    if (mode != 3) {
+      ukc = stage_ints(ukc, wU);
+      ukpos = stage_ints(ukpos, wU);
+      ukrel = stage_ints(ukrel, wU);
+    }
     lvp = stage_ints(lvp, wL + 1);
     lvc = stage_ints(lvc, wn);
     if (mode == 2) rel = stage_ints(rel, wR);
@@ -1064,8 +1068,10 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   double *Xv = cs + (long long)RC_XV * C + c0;
   const size_t values = sizeof(double) * (size_t)(wF + 2 * wn);
   const size_t plan_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wF + 3 * wU + wL + 1 + wn);
+  const size_t small_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wL + 1 + wn);
   const int mode = values + plan_ints + sizeof(int) * (size_t)wR <= smem_bytes ? 2
                    : values + plan_ints <= smem_bytes                           ? 1
+                   : values + small_ints <= smem_bytes                          ? 3
                                                                                 : 0;
   if (mode > 0) {
     lval = n2_smem;
@@ -1079,11 +1085,13 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       return out;
     };
     colp = stage_ints(colp, wn + 1);
-    lrow = stage_ints(lrow, wF);
+    if (mode != 3) lrow = stage_ints(lrow, wF);
     ukp = stage_ints(ukp, wn + 1);
-    ukc = stage_ints(ukc, wU);
-    ukpos = stage_ints(ukpos, wU);
-    ukrel = stage_ints(ukrel, wU);
+    if (mode != 3) {
+      ukc = stage_ints(ukc, wU);
+      ukpos = stage_ints(ukpos, wU);
+      ukrel = stage_ints(ukrel, wU);
+    }
     lvp = stage_ints(lvp, wL + 1);
     lvc = stage_ints(lvc, wn);
     if (mode == 2) rel = stage_ints(rel, wR);
@@ -1682,7 +1690,21 @@ int build_plan(cb_tissue *t) {
   const long long C = t->C, E = t->E;
   std::vector<int> rank(C), colp, lrow, uk_ptr, uk_col, uk_pos, uk_rel, rel, lv_ptr, lv_cols(C),
       edge_pos(E), fb{0}, ub{0}, rb{0}, lb{0};
-  size_t shared_all = 0, shared_plan = 0;
+  // Shared memory per CTA: for each world the largest of its stagings that fits the cap (the
+  // whole plan; all but the relative positions; the factor values, solve vectors and the
+  // per-column index arrays), the batch's maximum of those. The cap keeps the register budget's
+  // CTAs per SM resident (110 KB at two, 200 KB at one): measured on 512 1024-cell worlds, whose
+  // factor values alone take 136 KB, the ROS2 step runs at 9.1 ms from global memory at two CTAs
+  // per SM against 12.4 ms with the values staged at one. Overrides for sweeps:
+  // CELLS_B200_N2_SMEM (KB), CELLS_B200_N2_BLOCK (128 or 256), CELLS_B200_N2_MINB (1, or 2:
+  // registers capped for more resident CTAs).
+  if (const char *env = std::getenv("CELLS_B200_N2_BLOCK"))
+    plan->block = std::atoi(env) == 128 ? 128 : 256;
+  if (const char *env = std::getenv("CELLS_B200_N2_MINB"))
+    plan->min_blocks = std::atoi(env) >= 2 ? 2 : 1;
+  size_t cap = plan->min_blocks >= 2 ? 110 * 1024 : 200 * 1024;
+  if (const char *env = std::getenv("CELLS_B200_N2_SMEM")) cap = (size_t)std::atoi(env) * 1024;
+  size_t shared = 0;
   int rc = CB_OK;
   for (int w = 0; w < W && !rc; ++w) {
     const long long c0 = t->h_cell_offset[w], n = t->h_cell_offset[w + 1] - c0;
@@ -1716,8 +1738,11 @@ int build_plan(cb_tissue *t) {
     // Shared-memory footprint: values and vectors, then the plan's integers.
     const size_t values = sizeof(double) * (size_t)(F + 2 * n);
     const size_t ints = sizeof(int) * (size_t)(2 * (n + 1) + F + 3 * U + L + 1 + n);
-    shared_plan = std::max(shared_plan, values + ints);
-    shared_all = std::max(shared_all, values + ints + sizeof(int) * (size_t)R);
+    const size_t all = values + ints + sizeof(int) * (size_t)R;
+    const size_t small = values + sizeof(int) * (size_t)(2 * (n + 1) + L + 1 + n);
+    const size_t fits = all <= cap ? all : values + ints <= cap ? values + ints
+                        : small <= cap ? small : 0;
+    shared = std::max(shared, fits);
   }
   if (rc) {
     delete plan;
@@ -1726,17 +1751,8 @@ int build_plan(cb_tissue *t) {
   plan->factor_entries = fb.back();
   plan->update_terms = rb.back();
   plan->levels = lb.back();
-  // Shared memory per CTA: the largest world's whole footprint, at most 200 KB (larger worlds
-  // stage less or work from global memory). Overrides for sweeps: CELLS_B200_N2_SMEM (KB),
-  // CELLS_B200_N2_BLOCK (128 or 256), CELLS_B200_N2_MINB (1, or 2: registers capped for more
-  // resident CTAs).
-  size_t cap = 200 * 1024;
-  if (const char *env = std::getenv("CELLS_B200_N2_SMEM")) cap = (size_t)std::atoi(env) * 1024;
-  plan->smem_bytes = std::min(std::max(shared_all, shared_plan), cap);
-  if (const char *env = std::getenv("CELLS_B200_N2_BLOCK"))
-    plan->block = std::atoi(env) == 128 ? 128 : 256;
-  if (const char *env = std::getenv("CELLS_B200_N2_MINB"))
-    plan->min_blocks = std::atoi(env) >= 2 ? 2 : 1;
+  // A world none of whose stagings fits works from global memory.
+  plan->smem_bytes = shared;
   N2Dev &d = plan->d;
   if (!rc) rc = upload_vec(plan, rank, &d.rank);
   if (!rc) rc = upload_vec(plan, colp, &d.colp);

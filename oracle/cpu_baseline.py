@@ -34,7 +34,8 @@ def _world(kind, w, seed, size):
 
         if kind == "grid":
             world = worlds.grid_world(size, size, worlds.world_rng(seed, w))
-        elif kind in ("uneven", "adjoint"):  # world w of an uneven or adjoint batch (size given)
+        elif kind in ("uneven", "adjoint", "adjoint_ros2"):  # world w of an uneven or adjoint
+            # batch (size given)
             world = worlds.uneven_world(w, size, seed, worlds.UNEVEN_CHANNELS)
         else:
             world = worlds.delaunay_world(size, worlds.world_rng(seed, w))
@@ -87,24 +88,29 @@ def run_field_world(task):
 def run_adjoint_world(task):
     """(kind, world index, seed, size, steps, dt) -> (cell-steps, seconds): steps forward steps
     of the oracle, each state kept, then the oracle adjoint back over them from the cotangent of
-    the voltage-pattern loss (the gradient a trajectory of that many steps takes)."""
+    the voltage-pattern loss (the gradient a trajectory of that many steps takes). Kind
+    "adjoint": the ARS(2,2,2) step and its adjoint; "adjoint_ros2": the ROS2 step and its."""
     _pin_blas()
     from cells_b200 import worlds
     from oracle import adjoint as A
+    from oracle import ros2 as R2
+    from oracle import ros2_adjoint as RA
     from oracle import tissue as T
 
     kind, w, seed, size, steps, dt = task
     entry = _world(kind, w, seed, size)
     b, topo, ctl, st = entry
     target = worlds.voltage_target(b)
+    forward = R2.ros2_step if kind == "adjoint_ros2" else T.ars222_step
+    reverse = RA.step_vjp if kind == "adjoint_ros2" else A.step_vjp
     t0 = time.perf_counter()
     states = [st]
     for _ in range(steps):
-        states.append(T.ars222_step(states[-1], dt, ctl, b, topo)[0])
+        states.append(forward(states[-1], dt, ctl, b, topo)[0])
     _, cot_n = A.voltage_loss(states[-1], b, topo, target)
     cot = (cot_n, np.zeros(b.edges), np.zeros_like(st.channel_gate))
     for t in range(steps - 1, -1, -1):
-        cot, _, _, _ = A.step_vjp(states[t], dt, ctl, b, topo, *cot)
+        cot, _, _, _ = reverse(states[t], dt, ctl, b, topo, *cot)
     return b.cells * steps, time.perf_counter() - t0
 
 
