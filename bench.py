@@ -11,9 +11,10 @@ Workloads (``--workload``):
           persistent kernel;
   adjoint 512 worlds of 1024-cell Delaunay tissues with the uneven batch's laws: the gradient of
           each world's voltage-pattern loss (squared error of the final membrane voltages against
-          -50 mV plus three 20 mV Gaussian bumps) after 2000 FP64 steps at dt = 1 ms with respect
-          to every cell's P_Na, P_K, P_Cl, every junction's permeabilities and every channel
-          population's permeability, checkpoints every 100 steps with recomputation.
+          -50 mV plus three 20 mV Gaussian bumps) after 2000 FP64 steps at dt = 1 ms (the
+          ARS(2,2,2) step, or the ROS2 Rosenbrock step with --method ros2) with respect to every
+          cell's P_Na, P_K, P_Cl, every junction's permeabilities and every channel population's
+          permeability, checkpoints every 100 steps with recomputation.
   field   256 worlds of 1024 cells in a 128x128 extracellular grid (10 um spacing, the boundary
           ring held at the bath), 4-neighbour faces with log-normal conductivity (sigma 0.5),
           ARS(2,2,2) with implicit face electromigration at dt = 0.5 ms, the start field by the
@@ -1009,7 +1010,8 @@ def main():
     line = runner(args, rank, world_size, local_rank, dist, base)
     if field and not args.no_sub:
         # The metric's other two numbers, measured in the same run: the batched plain step on
-        # 4096 16x16-grid worlds, and adjoint world-gradients/s on 512 1024-cell Delaunay worlds.
+        # 4096 16x16-grid worlds, and adjoint world-gradients/s on 512 1024-cell Delaunay worlds
+        # (2000 Rosenbrock steps, the ROS2 adjoint; the ARS(2,2,2) adjoint beside it).
         subs = {}
         for name, kw in (("grid", dict(workload="grid", worlds=4096, side=16, dt=1e-3,
                                        steps=200, warmup=100, e2e_calls=1, fuse=100)),
@@ -1017,9 +1019,12 @@ def main():
                                             steps=20, warmup=5, e2e_calls=0, fuse=10,
                                             method="ros2")),
                          ("adjoint", dict(workload="adjoint", worlds=512, dt=1e-3, steps=1,
-                                          warmup=1, e2e_calls=0))):
+                                          warmup=1, e2e_calls=0, method="ros2")),
+                         ("adjoint_ars222", dict(workload="adjoint", worlds=512, dt=1e-3,
+                                                 steps=1, warmup=1, e2e_calls=0,
+                                                 method="ars222"))):
             sub = argparse.Namespace(**{**vars(args), **kw})
-            fn = run_adjoint if name == "adjoint" else run_grid
+            fn = run_adjoint if name.startswith("adjoint") else run_grid
             subs[name] = fn(sub, rank, world_size, local_rank, dist, None)
         if line is not None:
             line["sub_records"] = {k: sub_record(v) for k, v in subs.items()}
