@@ -37,6 +37,8 @@ struct N2Plan {
   int levels = 0, max_level = 0;
   size_t smem_bytes = 0;  // dynamic shared memory per CTA (worlds that fit stage into it)
   int block = 256;        // CTA threads (256, or 128 for small worlds)
+  int ros2_block = 256;   // the ROS2/RK4 kernel's CTA threads: 128 (four CTAs per SM) when no
+                          // world's plan is staged in shared memory, else 256 (two)
   int min_blocks = 2;     // the register budget's target CTAs per SM (2: capped at 128
                           // registers, measured fastest on 16x16 grids; 1: uncapped)
 };

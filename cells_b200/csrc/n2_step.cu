@@ -1751,8 +1751,13 @@ int build_plan(cb_tissue *t) {
   plan->factor_entries = fb.back();
   plan->update_terms = rb.back();
   plan->levels = lb.back();
-  // A world none of whose stagings fits works from global memory.
+  // A world none of whose stagings fits works from global memory. With nothing staged the ROS2
+  // kernel runs 128-thread CTAs, four per SM (512 1024-cell worlds: 7.2 ms per step against 8.97
+  // at 256 threads, two per SM; the 16x16 grid, whose plans are staged: 5.3 against 4.4).
   plan->smem_bytes = shared;
+  plan->ros2_block = shared == 0 ? 128 : 256;
+  if (const char *env = std::getenv("CELLS_B200_N2_BLOCK"))
+    plan->ros2_block = std::atoi(env) == 128 ? 128 : 256;
   N2Dev &d = plan->d;
   if (!rc) rc = upload_vec(plan, rank, &d.rank);
   if (!rc) rc = upload_vec(plan, colp, &d.colp);
@@ -1811,15 +1816,19 @@ int launch_ros2(cb_tissue *t, const double *in, double *out, const double *contr
                 const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
                 cudaStream_t stream, bool rk4, const R2Tape &tape) {
   const size_t smem = t->n2->smem_bytes;
-  // Registers capped for two CTAs per SM (N2's measured choice), unless CELLS_B200_N2_MINB=1.
+  // Registers capped for two CTAs per SM (N2's measured choice), unless CELLS_B200_N2_MINB=1;
+  // 128-thread CTAs at four per SM where the plan chose them (ros2_block).
+  const int block = t->n2->ros2_block;
   auto kern = rk4 ? ros2_kernel<256, NCH, 2, true> : ros2_kernel<256, NCH, 2, false>;
-  if (t->n2->min_blocks < 2)
+  if (block == 128)
+    kern = rk4 ? ros2_kernel<128, NCH, 4, true> : ros2_kernel<128, NCH, 4, false>;
+  else if (t->n2->min_blocks < 2)
     kern = rk4 ? ros2_kernel<256, NCH, 1, true> : ros2_kernel<256, NCH, 1, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (ros2)");
-  kern<<<t->W, 256, smem, stream>>>(t->t, t->layout, t->n2->d, in, out, control, k, n_steps,
-                                    status, taken, smem, tape);
+  kern<<<t->W, block, smem, stream>>>(t->t, t->layout, t->n2->d, in, out, control, k, n_steps,
+                                      status, taken, smem, tape);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "ros2 launch");
   return CB_OK;

@@ -732,8 +732,12 @@ R2Workspace plan_workspace(const cb_tissue *t, int n_steps) {
 template <int NCH>
 int launch_ros2_vjp(cb_tissue *t, const Adj &A, const R2Rev &R, const double *control, double h,
                     int n_steps, cudaStream_t stream) {
-  ros2_vjp_kernel<256, NCH, 2><<<t->W, 256, 0, stream>>>(t->t, t->layout, t->n2->d, A, R, control,
-                                                         h, n_steps);
+  if (t->n2->block == 128)  // CELLS_B200_N2_BLOCK=128: four 128-thread CTAs per SM
+    ros2_vjp_kernel<128, NCH, 4><<<t->W, 128, 0, stream>>>(t->t, t->layout, t->n2->d, A, R,
+                                                           control, h, n_steps);
+  else
+    ros2_vjp_kernel<256, NCH, 2><<<t->W, 256, 0, stream>>>(t->t, t->layout, t->n2->d, A, R,
+                                                           control, h, n_steps);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "ros2 vjp launch");
   return CB_OK;
