@@ -55,6 +55,7 @@ METHOD_MIXED = "cells_b200.solver.imex_ars222_mixed_fp32@1"
 METHOD_N2 = "cells.solver.imex_ars222_implicit_conductances@1"
 METHOD_N2_MIXED = "cells_b200.solver.imex_ars222_implicit_conductances_mixed@1"
 METHOD_ROS2 = "cells_b200.solver.ros2_verwer@1"
+METHOD_ROS2_MIXED = "cells_b200.solver.ros2_verwer_fp32_factor@1"
 
 
 def bytes_per_cell_step(batch):
@@ -92,7 +93,8 @@ def parse():
     ap.add_argument("--e2e-calls", type=int, default=None,
                     help="end-to-end host calls timed (default 3; adjoint: 1 gradient)")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
-                    help="mixed: the ARS(2,2,2) step with FP32 rates and FP64 accumulation")
+                    help="mixed: FP32 fluxes (ars222), an FP32 factor with FP64 refinement (n2), "
+                         "an FP32 factor and substitutions without refinement (ros2)")
     ap.add_argument("--method", choices=("ars222", "n2", "ros2"), default="ars222",
                     help="n2: slope conductances implicit, a sparse Cholesky per world per step; "
                          "ros2: the two-stage Rosenbrock method on the same operator")
@@ -805,7 +807,8 @@ def run_grid(args, rank, world_size, local_rank, dist, base):
     from cells_b200 import _lib as _lib_methods
 
     if args.method == "ros2":
-        method = _lib_methods.METHOD_ROS2
+        method = (_lib_methods.METHOD_ROS2_MIXED if args.precision == "mixed"
+                  else _lib_methods.METHOD_ROS2)
     elif args.method == "n2":
         method = (_lib_methods.METHOD_N2_MIXED if args.precision == "mixed"
                   else _lib_methods.METHOD_N2)
@@ -924,11 +927,13 @@ def run_grid(args, rank, world_size, local_rank, dist, base):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": ("f64" if args.precision == "fp64" else
                       "f32 factor / f64 refinement" if args.method == "n2" else
+                      "f32 factor and substitutions / f64 rest" if args.method == "ros2" else
                       "f32 fluxes / f64 rest"),
             "data": "synthetic (seeded pump-leak tissues)",
             "config": {
                 "workload": workload_name(args),
-                "method": (METHOD_ROS2 if args.method == "ros2" else
+                "method": ((METHOD_ROS2 if args.precision == "fp64" else METHOD_ROS2_MIXED)
+                           if args.method == "ros2" else
                            (METHOD_N2 if args.precision == "fp64" else METHOD_N2_MIXED)
                            if args.method == "n2" else
                            METHOD if args.precision == "fp64" else METHOD_MIXED),

@@ -39,6 +39,7 @@ METHOD_N2 = 2
 METHOD_N2_MIXED = 3
 METHOD_ROS2 = 4
 METHOD_RK4 = 5
+METHOD_ROS2_MIXED = 6
 KERNEL_SHARED, KERNEL_PACKED = 0, 1
 WORLD_BITS = {
     1: "transport",

@@ -44,16 +44,17 @@ int n2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
             const double *control, int n_steps, uint32_t *world_status, int32_t *accepted_steps,
             cudaStream_t stream, bool mix);
 void n2_release(cb_tissue *t);
-// The ROS2 method (n2_step.cu, on N2's factor plan), or with rk4 the classical RK4 of the same
-// right-hand side in the same kernel: n_steps steps of every world.
+// The ROS2 method (n2_step.cu, on N2's factor plan; with mix its FP32-factor form), or with rk4
+// the classical RK4 of the same right-hand side in the same kernel: n_steps steps of every world.
 int ros2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
               const double *control, int n_steps, uint32_t *world_status,
-              int32_t *accepted_steps, cudaStream_t stream, bool rk4);
+              int32_t *accepted_steps, cudaStream_t stream, bool rk4, bool mix);
 // One ROS2 step that also records what the reverse needs (R2Tape, n2_common.cuh).
 struct R2Tape;
 int ros2_step_tape(cb_tissue *t, const double *state_in, double *state_out, double dt,
                    const double *control, int n_steps, uint32_t *world_status,
-                   int32_t *accepted_steps, cudaStream_t stream, bool rk4, const R2Tape &tape);
+                   int32_t *accepted_steps, cudaStream_t stream, bool rk4, bool mix,
+                   const R2Tape &tape);
 // The N2 plan's build (idempotent), for the ROS2 reverse.
 int n2_build_plan(cb_tissue *t);
 }  // namespace cbk

@@ -39,6 +39,8 @@ struct N2Plan {
   int block = 256;        // CTA threads (256, or 128 for small worlds)
   int ros2_block = 256;   // the ROS2/RK4 kernel's CTA threads: 128 (four CTAs per SM) when no
                           // world's plan is staged in shared memory, else 256 (two)
+  size_t smem_f32 = 0;    // the same staging with FP32 factor values (CB_METHOD_ROS2_MIXED)
+  int ros2_block_f32 = 256;
   int min_blocks = 2;     // the register budget's target CTAs per SM (2: capped at 128
                           // registers, measured fastest on 16x16 grids; 1: uncapped)
 };

@@ -1032,7 +1032,11 @@ enum R2Edge {
   RE_FIELDS = 24
 };
 
-template <int BLOCK, int NCH, int MINB, bool RK4>
+// MIX (CB_METHOD_ROS2_MIXED): the voltage operator factored and both stage solves substituted in
+// FP32, with no refinement. ROS2 is a W-method: its order and its ledger bookkeeping hold for any
+// W, and an FP32 factor is the exact factor of a W within FP32 rounding of the FP64 one, so every
+// rate, slope and accumulation stays FP64 and the step stays second order and conservative.
+template <int BLOCK, int NCH, int MINB, bool RK4, bool MIX>
 __global__ void __launch_bounds__(BLOCK, MINB)
     ros2_kernel(const Tissue T, const Layout L, const N2Dev D, const double *state_in,
                 double *state_out, const double *__restrict__ control, const StepCoef k,
@@ -1063,10 +1067,11 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   const int *ukpos = D.uk_pos + D.ub[w], *ukrel = D.uk_rel + D.ub[w];
   const int *rel = D.rel + D.rb[w];
   const int *lvp = D.lv_ptr + D.lb[w] + w, *lvc = D.lv_cols + c0;
-  double *lval = D.lval + D.fb[w];
-  double *Yv = cs + (long long)RC_YV * C + c0;
-  double *Xv = cs + (long long)RC_XV * C + c0;
-  const size_t values = sizeof(double) * (size_t)(wF + 2 * wn);
+  using FT = typename std::conditional<MIX, float, double>::type;
+  FT *lval = reinterpret_cast<FT *>(D.lval) + D.fb[w];
+  FT *Yv = reinterpret_cast<FT *>(cs + (long long)RC_YV * C) + c0;
+  FT *Xv = reinterpret_cast<FT *>(cs + (long long)RC_XV * C) + c0;
+  const size_t values = sizeof(FT) * (size_t)(wF + 2 * wn);
   const size_t plan_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wF + 3 * wU + wL + 1 + wn);
   const size_t small_ints = sizeof(int) * (size_t)(2 * (wn + 1) + wL + 1 + wn);
   const int mode = values + plan_ints + sizeof(int) * (size_t)wR <= smem_bytes ? 2
@@ -1074,7 +1079,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                    : values + small_ints <= smem_bytes                          ? 3
                                                                                 : 0;
   if (mode > 0) {
-    lval = n2_smem;
+    lval = reinterpret_cast<FT *>(n2_smem);
     Yv = lval + wF;
     Xv = Yv + wn;
     int *si = reinterpret_cast<int *>(Xv + wn);
@@ -1097,7 +1102,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     if (mode == 2) rel = stage_ints(rel, wR);
   }
   __syncthreads();  // the staged plan, read by dense_tail
-  const WorldCholesky<double, BLOCK> chol{colp, lrow, ukp, ukc, ukpos, ukrel, rel, lvp, lvc,
+  const WorldCholesky<FT, BLOCK> chol{colp, lrow, ukp, ukc, ukpos, ukrel, rel, lvp, lvc,
                                           lval, Yv, Xv, 0, wL, wn,
                                           dense_tail(colp, lvp, lvc, 0, wL, wn)};
   const long long oN = L.s[CB_AMOUNT_INCREMENT], oG = L.s[CB_JUNCTION_GATE];
@@ -1359,9 +1364,9 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         if (!(mii > 0.0)) bits |= CB_WORLD_OPERATOR;
         const double sc = 1.0 / sqrt(mii > 0.0 ? mii : 1.0);
         CF(RC_S, gi) = sc;
-        lval[colp[__ldg(D.rank + gi)]] = (mii * sc) * sc;
+        lval[colp[__ldg(D.rank + gi)]] = (FT)((mii * sc) * sc);
       }
-      if (!RK4) Yv[__ldg(D.rank + gi)] = qdot * CF(RC_S, gi);
+      if (!RK4) Yv[__ldg(D.rank + gi)] = (FT)(qdot * CF(RC_S, gi));
     }
     __syncthreads();
     if (start) {
@@ -1373,7 +1378,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         const double m = 0.0 + gh * (-EF(RE_G, ge));
         const double s_row = ra > rb ? CF(RC_S, ga) : CF(RC_S, gb);
         const double s_col = ra > rb ? CF(RC_S, gb) : CF(RC_S, ga);
-        lval[__ldg(D.edge_pos + ge)] = (m * s_row) * s_col;
+        lval[__ldg(D.edge_pos + ge)] = (FT)((m * s_row) * s_col);
       }
       __syncthreads();
     }
@@ -1390,7 +1395,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     chol.solve();
     for (int i = tid; i < nc; i += BLOCK) {
       const long long gi = c0 + i;
-      const double u = Xv[__ldg(D.rank + gi)] * CF(RC_S, gi);
+      const double u = (double)Xv[__ldg(D.rank + gi)] * CF(RC_S, gi);
       CF(RC_U, gi) = u;
       if (tp.factor) tp.u[st * C + gi] = u;
       if (!is_finite(u)) bits |= CB_WORLD_RESIDUAL;
@@ -1557,7 +1562,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       block_sum<BLOCK, 4>(ve, sRed);
       if (chol.factor()) bits |= CB_WORLD_OPERATOR;
       if (tp.factor) {  // the reverse's record: the factor and its scale
-        for (int f = tid; f < wF; f += BLOCK) tp.factor[D.fb[w] + f] = lval[f];
+        for (int f = tid; f < wF; f += BLOCK) tp.factor[D.fb[w] + f] = (double)lval[f];
         for (int i = tid; i < nc; i += BLOCK) tp.scale[c0 + i] = CF(RC_S, c0 + i);
       }
       bits |= correct(0, vc);
@@ -1704,7 +1709,7 @@ int build_plan(cb_tissue *t) {
     plan->min_blocks = std::atoi(env) >= 2 ? 2 : 1;
   size_t cap = plan->min_blocks >= 2 ? 110 * 1024 : 200 * 1024;
   if (const char *env = std::getenv("CELLS_B200_N2_SMEM")) cap = (size_t)std::atoi(env) * 1024;
-  size_t shared = 0;
+  size_t shared = 0, shared_f32 = 0;  // FP64 values; FP32 values (CB_METHOD_ROS2_MIXED)
   int rc = CB_OK;
   for (int w = 0; w < W && !rc; ++w) {
     const long long c0 = t->h_cell_offset[w], n = t->h_cell_offset[w + 1] - c0;
@@ -1743,6 +1748,9 @@ int build_plan(cb_tissue *t) {
     const size_t fits = all <= cap ? all : values + ints <= cap ? values + ints
                         : small <= cap ? small : 0;
     shared = std::max(shared, fits);
+    const size_t v32 = values / 2, a32 = all - values / 2, s32 = small - values / 2;
+    const size_t fits32 = a32 <= cap ? a32 : v32 + ints <= cap ? v32 + ints : s32 <= cap ? s32 : 0;
+    shared_f32 = std::max(shared_f32, fits32);
   }
   if (rc) {
     delete plan;
@@ -1755,9 +1763,11 @@ int build_plan(cb_tissue *t) {
   // kernel runs 128-thread CTAs, four per SM (512 1024-cell worlds: 7.2 ms per step against 8.97
   // at 256 threads, two per SM; the 16x16 grid, whose plans are staged: 5.3 against 4.4).
   plan->smem_bytes = shared;
+  plan->smem_f32 = shared_f32;
   plan->ros2_block = shared == 0 ? 128 : 256;
+  plan->ros2_block_f32 = shared_f32 == 0 ? 128 : 256;
   if (const char *env = std::getenv("CELLS_B200_N2_BLOCK"))
-    plan->ros2_block = std::atoi(env) == 128 ? 128 : 256;
+    plan->ros2_block = plan->ros2_block_f32 = std::atoi(env) == 128 ? 128 : 256;
   N2Dev &d = plan->d;
   if (!rc) rc = upload_vec(plan, rank, &d.rank);
   if (!rc) rc = upload_vec(plan, colp, &d.colp);
@@ -1814,16 +1824,22 @@ int launch_n2(cb_tissue *t, const double *in, double *out, const double *control
 template <int NCH>
 int launch_ros2(cb_tissue *t, const double *in, double *out, const double *control,
                 const StepCoef &k, int n_steps, uint32_t *status, int32_t *taken,
-                cudaStream_t stream, bool rk4, const R2Tape &tape) {
-  const size_t smem = t->n2->smem_bytes;
+                cudaStream_t stream, bool rk4, bool mix, const R2Tape &tape) {
   // Registers capped for two CTAs per SM (N2's measured choice), unless CELLS_B200_N2_MINB=1;
   // 128-thread CTAs at four per SM where the plan chose them (ros2_block).
-  const int block = t->n2->ros2_block;
-  auto kern = rk4 ? ros2_kernel<256, NCH, 2, true> : ros2_kernel<256, NCH, 2, false>;
+  const int block = mix ? t->n2->ros2_block_f32 : t->n2->ros2_block;
+  const size_t smem = mix ? t->n2->smem_f32 : t->n2->smem_bytes;
+  auto kern = rk4   ? ros2_kernel<256, NCH, 2, true, false>
+              : mix ? ros2_kernel<256, NCH, 2, false, true>
+                    : ros2_kernel<256, NCH, 2, false, false>;
   if (block == 128)
-    kern = rk4 ? ros2_kernel<128, NCH, 4, true> : ros2_kernel<128, NCH, 4, false>;
+    kern = rk4   ? ros2_kernel<128, NCH, 4, true, false>
+           : mix ? ros2_kernel<128, NCH, 4, false, true>
+                 : ros2_kernel<128, NCH, 4, false, false>;
   else if (t->n2->min_blocks < 2)
-    kern = rk4 ? ros2_kernel<256, NCH, 1, true> : ros2_kernel<256, NCH, 1, false>;
+    kern = rk4   ? ros2_kernel<256, NCH, 1, true, false>
+           : mix ? ros2_kernel<256, NCH, 1, false, true>
+                 : ros2_kernel<256, NCH, 1, false, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (ros2)");
@@ -1840,25 +1856,26 @@ namespace cbk {
 
 int ros2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
               const double *control, int n_steps, uint32_t *world_status,
-              int32_t *accepted_steps, cudaStream_t stream, bool rk4) {
+              int32_t *accepted_steps, cudaStream_t stream, bool rk4, bool mix) {
   return ros2_step_tape(t, state_in, state_out, dt, control, n_steps, world_status,
-                        accepted_steps, stream, rk4, R2Tape{});
+                        accepted_steps, stream, rk4, mix, R2Tape{});
 }
 
 int ros2_step_tape(cb_tissue *t, const double *state_in, double *state_out, double dt,
                    const double *control, int n_steps, uint32_t *world_status,
-                   int32_t *accepted_steps, cudaStream_t stream, bool rk4, const R2Tape &tape) {
-  if (tape.factor && (rk4 || n_steps != 1))
-    return fail(CB_ERR_ARGUMENT, "a ROS2 record covers one ROS2 step");
+                   int32_t *accepted_steps, cudaStream_t stream, bool rk4, bool mix,
+                   const R2Tape &tape) {
+  if (tape.factor && (rk4 || mix || n_steps != 1))
+    return fail(CB_ERR_ARGUMENT, "a ROS2 record covers one FP64 ROS2 step");
   int rc = build_plan(t);
   if (rc) return rc;
   const StepCoef k = step_coef(dt);
   if (t->t.nch == 2)
     return launch_ros2<2>(t, state_in, state_out, control, k, n_steps, world_status,
-                          accepted_steps, stream, rk4, tape);
+                          accepted_steps, stream, rk4, mix, tape);
   if (t->t.nch == 0)
     return launch_ros2<0>(t, state_in, state_out, control, k, n_steps, world_status,
-                          accepted_steps, stream, rk4, tape);
+                          accepted_steps, stream, rk4, mix, tape);
   return fail(CB_ERR_UNSUPPORTED, "channel slots must be 0 or 2");
 }
 

@@ -788,7 +788,8 @@ int ros2_vjp(cb_tissue *t, const double *state_in, double dt, const double *cont
                     rec + p.rev.o_k1n,    rec + p.rev.o_k1gc,  rec + p.rev.o_k1g,
                     rec + p.rev.o_k2gc,   rec + p.rev.o_k2g};
     rc = ros2_step_tape(t, in, states + (size_t)step * t->state_total, dt, control, 1,
-                        status + (size_t)step * t->W, taken + (size_t)step * t->W, s, false, tp);
+                        status + (size_t)step * t->W, taken + (size_t)step * t->W, s, false,
+                        false, tp);
     if (rc) return rc;
   }
   if (cot_in != cot_out) {

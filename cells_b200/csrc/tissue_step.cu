@@ -1444,13 +1444,14 @@ int cb_step(cb_tissue *t, int method, const double *state_in, double *state_out,
     return n2_step(t, state_in, state_out, dt, control, n_steps, world_status, accepted_steps,
                    static_cast<cudaStream_t>(stream), method == CB_METHOD_N2_MIXED);
   }
-  if (method == CB_METHOD_ROS2 || method == CB_METHOD_RK4) {
+  if (method == CB_METHOD_ROS2 || method == CB_METHOD_RK4 || method == CB_METHOD_ROS2_MIXED) {
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
     if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
     cudaError_t ce = cudaSetDevice(t->device);
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
     return ros2_step(t, state_in, state_out, dt, control, n_steps, world_status, accepted_steps,
-                     static_cast<cudaStream_t>(stream), method == CB_METHOD_RK4);
+                     static_cast<cudaStream_t>(stream), method == CB_METHOD_RK4,
+                     method == CB_METHOD_ROS2_MIXED);
   }
   if (method != CB_METHOD_ARS222 && method != CB_METHOD_ARS222_MIXED)
     return fail(CB_ERR_UNSUPPORTED, "unknown step method");

@@ -186,6 +186,15 @@ enum cb_control_field {
  * No explicit-stability refusal (the reference's RK4 has none). One CTA per world (ROS2's kernel
  * without its operator). FP64. */
 #define CB_METHOD_RK4 5
+/* This library's cells_b200.solver.ros2_verwer_fp32_factor@1: CB_METHOD_ROS2 with its voltage
+ * operator factored and both stage solves substituted in FP32 and no refinement; every rate,
+ * slope, potential and accumulation stays FP64. ROS2 is a W-method: its order and its ledgers'
+ * balance hold for any W, and the FP32 factor is the exact factor of a W within FP32 rounding of
+ * the FP64 one, so the step stays second order and conservative. Measured against the FP64 ROS2
+ * (tests/test_ros2_gpu.py): within 1e-8 scaled difference on every state field over hundreds of
+ * steps, ledgers balanced to 1e-12. Half the factor's bytes: 1024-cell worlds' factor values fit
+ * shared memory beside a second CTA. */
+#define CB_METHOD_ROS2_MIXED 6
 
 /*
  * Host symbolic bind (replaces initial_values' layout binding, surface_tissue.py:135-257 and

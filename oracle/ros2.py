@@ -34,7 +34,10 @@ models/surface_kinetic.py:221-410, as ``oracle.tissue.readout_rates``); J is:
   coupling loses an order on them;
 * zero for the pump (its rates stay explicit in k = r) and for the gates' effect on the fluxes.
 
-The operator is factored once per step at y. A world's step is refused (its state kept) when a
+The operator is factored once per step at y. ``ros2_step(..., factor32=True)`` restates this
+library's CB_METHOD_ROS2_MIXED: the Jacobi-scaled factor rounded to FP32 and both substitutions
+in FP32, nothing refined (a W-method keeps its order and its ledgers for any W; the FP32 factor
+is the exact factor of a W within FP32 rounding of this one). A world's step is refused (its state kept) when a
 rate evaluation is invalid (the reference's RK4 rule, numerics/fixed_step.py:25-71: the trial
 state's domain first, then its rates), a slope is not finite, the operator is not positive
 definite, or the new state leaves the domain.
@@ -45,6 +48,7 @@ from __future__ import annotations
 import math
 
 import numpy as np
+import scipy.linalg as sl
 
 from oracle import adjoint as A
 from oracle import n2 as N
@@ -60,7 +64,8 @@ class Jacobian:
     """The step's W-matrix pieces at y: route slopes, the factored voltage operator, the gates'
     relaxation rates, and the start fluxes and potential differences the heat rows need."""
 
-    def __init__(self, state, control, b, topo, h):
+    def __init__(self, state, control, b, topo, h, factor32=False):
+        self.factor32 = factor32
         w = topo.cell_world
         bath = b.bath_potential[w]
         self.h = h
@@ -111,7 +116,13 @@ class Jacobian:
             c0, c1 = b.cell_offset[wi], b.cell_offset[wi + 1]
             rhs = np.where(free, np.r_[rho[c0:c1], 0.0] * scale, 0.0)
             with np.errstate(all="ignore"):
-                x = np.where(free, N.cholesky_solve(factor, rhs) * scale, 0.0)
+                if self.factor32:
+                    lower = np.asarray(factor, dtype=np.float32)
+                    y = sl.solve_triangular(lower, rhs.astype(np.float32), lower=True)
+                    sol = sl.solve_triangular(lower.T, y, lower=False).astype(np.float64)
+                else:
+                    sol = N.cholesky_solve(factor, rhs)
+                x = np.where(free, sol * scale, 0.0)
             u[c0:c1] = x[:-1]
         return u
 
@@ -168,13 +179,13 @@ def _minus(a, b, factor):
     return T.State(*(x - factor * y for x, y in zip(a, b, strict=True)))
 
 
-def ros2_step(state, dt, control, b, topo=None):
-    """One ROS2 step for every world; returns (state, valid[W])."""
+def ros2_step(state, dt, control, b, topo=None, factor32=False):
+    """One ROS2 step for every world; returns (state, valid[W]). factor32: the FP32-factor form."""
     topo = T.topology(b) if topo is None else topo
     valid = T.domain_valid(state, b, topo)
     f0, ok = T.readout_rates(state, control, b, topo)
     valid &= ok
-    jac = Jacobian(state, control, b, topo, dt)
+    jac = Jacobian(state, control, b, topo, dt, factor32)
     valid &= jac.valid
     k1 = jac.solve(f0, b, topo)
     trial = _axpy(state, [(dt, k1)])

@@ -119,3 +119,59 @@ def test_ros2_refusal_keeps_the_state():
     assert ok[0] and not ok[1]
     assert np.array_equal(st.amount_increment[:, 16:], start.amount_increment[:, 16:])
     assert not np.array_equal(st.amount_increment[:, :16], start.amount_increment[:, :16])
+
+
+def test_fp32_factor_form_stays_within_1e8_of_fp64_and_conserves():
+    """CB_METHOD_ROS2_MIXED's restatement (ros2_step(factor32=True): the voltage operator's factor
+    and substitutions in FP32, no refinement): after 300 steps of 1 ms on uneven channel worlds
+    with gated junctions and partial controls, every state field within 1e-8 scaled difference of
+    the FP64 ROS2 (measured about 4e-10), and every ledger balanced to 1e-12 every step: the
+    W-method's bookkeeping does not depend on W being exact."""
+    from conftest import scaled_difference
+
+    rng = np.random.default_rng(9)
+    ws = [worlds.with_channels(worlds.delaunay_world(n, worlds.world_rng(26, k),
+                                                     junction_sigma=0.3, gate=(0.02, 0.2, 0.9)),
+                               rng, na=("nav", 1e-9, 0.5), k=("hh", 5e-10, 0.5), sigma=0.3)
+          for k, n in enumerate((60, 25))]
+    b = worlds.pack(ws)
+    topo = T.topology(b)
+    control = T.Control(rng.uniform(0.6, 1, b.cells), rng.uniform(0.6, 1, b.edges),
+                        rng.uniform(0.6, 1, b.cells), rng.uniform(0.4, 1, (2, b.cells)))
+    a = m = T.initial_state(b)
+    material = np.abs(b.amount_reference).sum()
+    for _ in range(300):
+        a, ok = RO.ros2_step(a, 1e-3, control, b, topo)
+        assert np.all(ok)
+        m, ok = RO.ros2_step(m, 1e-3, control, b, topo, factor32=True)
+        assert np.all(ok)
+        bal = T.balances(m, b, topo)
+        for name in ("local", "outside", "total"):
+            assert np.max(np.abs(bal[name])) <= 1e-12 * material, name
+        assert np.max(np.abs(bal["global_charge"])) <= 1e-12 * T.CHARGE_PER_FMOL * material
+    diffs = {f: scaled_difference(getattr(m, f), getattr(a, f)) for f in T.State._fields}
+    assert max(diffs.values()) <= 1e-8, diffs
+    assert max(diffs.values()) > 0.0  # the FP32 factor is in use
+
+
+def test_fp32_factor_form_is_second_order_against_rk4():
+    """The FP32-factor form keeps ROS2's order (the grid world of the order test above)."""
+    b = worlds.pack([worlds.single_grid_tissue(0)])
+    topo = T.topology(b)
+    control = T.full_control(b)
+    start = T.initial_state(b)
+    for _ in range(1500):
+        start, ok = T.ars222_step(start, 2e-5, control, b, topo)
+    ref = start
+    for _ in range(int(round(SPAN / 5e-6))):
+        ref, _ = T.rk4_step(ref, 5e-6, control, b, topo)
+    errors = []
+    for dt in (1e-3, 5e-4, 2.5e-4):
+        st = start
+        for _ in range(int(round(SPAN / dt))):
+            st, ok = RO.ros2_step(st, dt, control, b, topo, factor32=True)
+            assert np.all(ok)
+        errors.append(float(np.max(np.abs(st.amount_increment - ref.amount_increment)))
+                      / float(np.max(np.abs(ref.amount_increment - start.amount_increment))))
+    orders = [np.log2(errors[i] / errors[i + 1]) for i in range(2)]
+    assert all(p >= 1.8 for p in orders), (errors, orders)

@@ -140,3 +140,33 @@ def test_ros2_refusal_keeps_the_state(cuda):
     assert status[0] == 0 and status[2] == 0 and status[1] & 8
     assert taken[1] == 0 and taken[0] == 5
     assert np.array_equal(got["amount_increment"][:, 16:32], start["amount_increment"][:, 16:32])
+
+
+def test_fp32_factor_ros2_within_1e8_of_fp64_and_conserves(cuda):
+    """CB_METHOD_ROS2_MIXED (the voltage operator factored and substituted in FP32, no
+    refinement): the uneven channel worlds with gated junctions and partial controls, 200 steps of
+    1 ms, every state field within 1e-8 scaled difference of the FP64 oracle and of the device's
+    FP64 ROS2 (each maximum printed), the ledgers balanced to 1e-12 of the material scale."""
+    b, rng = uneven_batch(63)
+    tissue = Tissue(b)
+    mem, jun = rng.uniform(0.6, 1, b.cells), rng.uniform(0.6, 1, b.edges)
+    pmp, chn = rng.uniform(0.6, 1, b.cells), rng.uniform(0.4, 1, (2, b.cells))
+    control = tissue.pack_control(mem, jun, pmp, chn)
+    mixed, s1, _ = run(cuda, tissue, tissue.initial_state(), control, 1e-3, [100, 100],
+                       method=_lib.METHOD_ROS2_MIXED)
+    fp64, s2, _ = run(cuda, tissue, tissue.initial_state(), control, 1e-3, [100, 100])
+    assert np.all(s1 == 0) and np.all(s2 == 0)
+    ref = oracle_run(b, T.Control(mem, jun, pmp, chn), 1e-3, 200)
+    vs_oracle = {f: scaled_difference(mixed[f], r) for f, r in oracle_state(ref).items()}
+    vs_device = {f: scaled_difference(mixed[f], fp64[f]) for f in fp64}
+    print("ROS2 FP32-factor vs FP64 oracle:", {k: f"{v:.1e}" for k, v in vs_oracle.items()})
+    assert max(vs_oracle.values()) <= 1e-8, vs_oracle
+    assert max(vs_device.values()) <= 1e-8, vs_device
+    assert max(vs_device.values()) > 0.0  # the FP32 factor is in use
+    dev = cuda.device("cuda", tissue.device)
+    buf = cuda.from_numpy(tissue.pack_state(mixed)).to(dev)
+    out = cuda.zeros(b.worlds * 8, dtype=cuda.float64, device=dev)
+    tissue.balances(buf, out)
+    worst = out.view(-1, 8).max(dim=0).values.cpu().numpy()
+    scale = float(np.max(np.abs(b.amount_reference)))
+    assert worst[0] <= 1e-12 * scale and worst[2] <= 1e-12 * scale, worst
