@@ -9,10 +9,14 @@ outside nodes and faces (src/cells/models/surface_pump.py:124-369):
   junctions' initial gates);
 * ``FieldTissue.step(...)``     ~ ``checked_step`` repeated ``n_steps`` times for every world on
   device buffers (cb_field_step); a refused world keeps its last accepted state;
-* ``FieldTissue.step_host(...)`` the same with host arrays (cb_field_step_host).
+* ``FieldTissue.step_host(...)`` the same with host arrays (cb_field_step_host);
+* ``FieldBatch(worlds)``        worlds of different geometries in one batch, as the reference's
+  vector windows take them (src/cells/execution/vector_windows.py:348-410: each world its own
+  layout, padded to common capacities): one FieldTissue per distinct topology, each with its own
+  nested-dissection plan, stepped in turn; states and controls per world.
 
-Every world of a batch shares one topology (grid, cells' nodes, junction graph); parameters are
-per world. State is a dict of NumPy arrays [W, ...] per field (``_lib.FIELD_STATE_FIELDS``; cell
+Every world of a FieldTissue shares one topology (grid, cells' nodes, junction graph);
+parameters are per world. State is a dict of NumPy arrays [W, ...] per field (``_lib.FIELD_STATE_FIELDS``; cell
 fields [W, 3, N] or [W, N], node fields [W, 3, O] or [W, O], junction fields [W, 3, E] or [W, E],
 face fields [W, 3, F] or [W, F]); on the device it is one packed float64 buffer, species-major
 ([3][W*X]) within a field.
@@ -34,6 +38,22 @@ SCALAR = {"membrane_dissipated": "N", "junction_dissipated": "E", "face_dissipat
           "metabolic_work": "N"}
 TOPOLOGY = ("side", "cell_node", "sender", "receiver", "face_sender", "face_receiver",
             "reservoir")
+
+
+def topology_key(world):
+    """A world's topology as a hashable key: the fields a FieldTissue's worlds must share."""
+    return tuple((name, np.asarray(getattr(world, name)).dtype.str,
+                  np.asarray(getattr(world, name)).shape,
+                  np.ascontiguousarray(getattr(world, name)).tobytes()) for name in TOPOLOGY)
+
+
+def group_by_topology(worlds):
+    """Index lists of the worlds that share a topology, in order of first appearance; each list
+    ascending."""
+    groups = {}
+    for i, w in enumerate(worlds):
+        groups.setdefault(topology_key(w), []).append(i)
+    return list(groups.values())
 
 
 def _same_topology(worlds):
@@ -235,3 +255,55 @@ class FieldTissue:
             taken.ctypes.data_as(_lib._i32),
         ))  # fmt: skip
         return self.unpack_state(dst), status, taken
+
+
+class FieldBatch:
+    """Field worlds of different geometries (grids, tissues, contact graphs) in one batch: the
+    worlds grouped by topology (group_by_topology), each group bound as one FieldTissue with its
+    own factor plan; a step advances every group in turn on one device. States, controls and the
+    per-world status are in the batch's world order."""
+
+    def __init__(self, worlds, device=0):
+        if not worlds:
+            raise ValueError("no worlds")
+        self.worlds = list(worlds)
+        self.W = len(self.worlds)
+        self.device = int(device)
+        self.groups = [(idx, FieldTissue([self.worlds[i] for i in idx], device=device))
+                       for idx in group_by_topology(self.worlds)]
+
+    def initial_state(self):
+        """One state dict per world (each field [3, X] or [X])."""
+        out = [None] * self.W
+        for idx, tissue in self.groups:
+            st = tissue.initial_state()
+            for k, i in enumerate(idx):
+                out[i] = {name: a[k].copy() for name, a in st.items()}
+        return out
+
+    def step_host(self, states, dt, n_steps, controls=None):
+        """n_steps steps of every world (cb_field_step_host per group). states: one dict per
+        world; controls: None (every availability 1) or one dict per world with optional
+        membrane [N], junction [E] and pump [N] availabilities. Returns (states, status [W],
+        taken [W]) in the batch's order; a refused world keeps its last accepted state."""
+        if len(states) != self.W or (controls is not None and len(controls) != self.W):
+            raise ValueError("one state (and control) per world")
+        out = [None] * self.W
+        status = np.zeros(self.W, dtype=np.uint32)
+        taken = np.zeros(self.W, dtype=np.int32)
+        for idx, tissue in self.groups:
+            st = {name: np.stack([np.asarray(states[i][name], dtype=np.float64) for i in idx])
+                  for name in _lib.FIELD_STATE_FIELDS}
+            if controls is None:
+                ctl = tissue.pack_control()
+            else:
+                ctl = tissue.pack_control(*(
+                    np.stack([np.broadcast_to(np.asarray(
+                        controls[i].get(key, 1.0), dtype=np.float64), (size,)) for i in idx])
+                    for key, size in (("membrane", tissue.N), ("junction", tissue.E),
+                                      ("pump", tissue.N))))
+            new, s, t = tissue.step_host(st, ctl, dt, n_steps)
+            for k, i in enumerate(idx):
+                out[i] = {name: a[k].copy() for name, a in new.items()}
+                status[i], taken[i] = s[k], t[k]
+        return out, status, taken

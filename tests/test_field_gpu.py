@@ -250,3 +250,32 @@ def test_field_benchmark_grid_matches_the_sparse_oracle(cuda):
            if (d := field_difference(got[f][0], getattr(st, f), st.face_transferred, w, f))
            > (FACE_TOL_128 if f == "face_transferred" else TOL)}
     assert not bad, bad
+
+
+def test_field_batch_of_two_geometries_matches_the_oracle(cuda):
+    """FieldBatch: three worlds of two geometries (16x16 grids with a 4x4 tissue, a 12x12 grid
+    with a 3x3 tissue), gated junctions and partial random controls, 12 steps: each world against
+    the dense oracle at 1e-10, in the batch's order."""
+    from cells_b200.field import FieldBatch
+
+    ws = [FW.field_world(16, 4, 3, worlds.world_rng(41, 0), gate=(0.015, 0.2, 1.0),
+                         junction_sigma=0.3),
+          FW.field_world(12, 3, 3, worlds.world_rng(41, 1), gate=(0.015, 0.2, 1.0)),
+          FW.field_world(16, 4, 3, worlds.world_rng(41, 2), gate=(0.015, 0.2, 1.0),
+                         junction_sigma=0.3)]
+    batch = FieldBatch(ws)
+    assert [idx for idx, _ in batch.groups] == [[0, 2], [1]]
+    rng = np.random.default_rng(42)
+    controls = [dict(membrane=rng.uniform(0.6, 1, w.cells), junction=rng.uniform(0.6, 1, w.edges),
+                     pump=rng.uniform(0.6, 1, w.cells)) for w in ws]
+    states, status, taken = batch.step_host(batch.initial_state(), 5e-4, 5, controls)
+    states, status, taken2 = batch.step_host(states, 5e-4, 7, controls)
+    assert np.all(status == 0) and np.all(taken == 5) and np.all(taken2 == 7)
+    for w, ctl, got in zip(ws, controls, states, strict=True):
+        control = OF.full_control(w)._replace(membrane=ctl["membrane"], junction=ctl["junction"],
+                                              pump=ctl["pump"])
+        (ref,) = _oracle_run([w], [control], 5e-4, 12)
+        bad = {f: d for f in OF.FieldState._fields
+               if (d := field_difference(got[f], getattr(ref, f), ref.face_transferred, w, f))
+               > TOL}
+        assert not bad, bad

@@ -60,3 +60,17 @@ def test_a_batch_shares_one_topology():
     b = FW.field_world(12, 3, 2, W.world_rng(1, 1))
     with pytest.raises(ValueError, match="share their topology"):
         FieldTissue([a, b])
+
+
+def test_field_worlds_group_by_topology():
+    """FieldBatch's grouping: worlds of one grid, tissue and contact graph share a group whatever
+    their parameters; the groups keep first-appearance order and each lists its worlds ascending."""
+    from cells_b200 import field as FD
+
+    a = [FW.field_world(16, 4, 3, W.world_rng(3, k)) for k in range(3)]
+    b = FW.field_world(12, 3, 3, W.world_rng(3, 9))
+    gated = FW.field_world(16, 4, 3, W.world_rng(3, 7), gate=(0.015, 0.2, 1.0),
+                           junction_sigma=0.3)
+    assert FD.group_by_topology([a[0], b, a[1], gated, a[2]]) == [[0, 2, 3, 4], [1]]
+    assert FD.group_by_topology([b]) == [[0]]
+    assert FD.topology_key(a[0]) == FD.topology_key(a[2]) != FD.topology_key(b)
