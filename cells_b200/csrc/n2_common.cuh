@@ -119,31 +119,41 @@ struct WorldCholesky {
   int n, tail;  // the world's columns; its dense tail's length (0: none)
 
   // Update terms u0 .. u1 of the column at cj (ascending k), those with k below klim, in order:
-  // lanes over a term's rows, a warp sync between terms. The next term's indices and multiplier
-  // are read before this term's rows are written: they lie in finished columns.
+  // lanes over a term's rows, a warp sync between terms. The next term's indices, multiplier and
+  // first 32 rows (their offsets in column j and their values) are read before this term's rows
+  // are written: they lie in finished columns, so the loads overlap this term's scatter.
   __device__ void apply_updates(int cj, int u0, int u1, int klim, int lane) const {
     if (u0 >= u1 || ukc[u0] >= klim) return;
     int kk = ukc[u0], p = ukpos[u0], r0 = ukrel[u0];
     int cnt = colp[kk + 1] - p;
     FT ljk = lval[p];
+    int off = lane < cnt ? rel[r0 + lane] : 0;
+    FT src = lane < cnt ? lval[p + lane] : FT(0);
     for (int u = u0;; ++u) {
       const bool more = u + 1 < u1 && ukc[u + 1] < klim;
-      int np = 0, nr0 = 0, ncnt = 0;
-      FT nl = 0;
+      int np = 0, nr0 = 0, ncnt = 0, noff = 0;
+      FT nl = 0, nsrc = 0;
       if (more) {
         const int nk = ukc[u + 1];
         np = ukpos[u + 1];
         nr0 = ukrel[u + 1];
         ncnt = colp[nk + 1] - np;
         nl = lval[np];
+        if (lane < ncnt) {
+          noff = rel[nr0 + lane];
+          nsrc = lval[np + lane];
+        }
       }
-      for (int t = lane; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
+      if (lane < cnt) lval[cj + off] -= src * ljk;
+      for (int t = lane + 32; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
       __syncwarp();
       if (!more) break;
       p = np;
       r0 = nr0;
       cnt = ncnt;
       ljk = nl;
+      off = noff;
+      src = nsrc;
     }
   }
   __device__ uint32_t factor_column(int j, int lane) const {
