@@ -119,41 +119,58 @@ struct WorldCholesky {
   int n, tail;  // the world's columns; its dense tail's length (0: none)
 
   // Update terms u0 .. u1 of the column at cj (ascending k), those with k below klim, in order:
-  // lanes over a term's rows, a warp sync between terms. The next term's indices, multiplier and
-  // first 32 rows (their offsets in column j and their values) are read before this term's rows
-  // are written: they lie in finished columns, so the loads overlap this term's scatter.
+  // lanes over a term's rows, a warp sync between terms. While a term's rows are written, the
+  // next term's multiplier, length and first 32 rows (their offsets in column j and their values)
+  // are read, and the indices of the term after it: all lie in finished columns, so each term
+  // waits on one round of loads, not on the index loads and the loads they address in turn.
   __device__ void apply_updates(int cj, int u0, int u1, int klim, int lane) const {
     if (u0 >= u1 || ukc[u0] >= klim) return;
-    int kk = ukc[u0], p = ukpos[u0], r0 = ukrel[u0];
-    int cnt = colp[kk + 1] - p;
+    int p = ukpos[u0], r0 = ukrel[u0];
+    int cnt = colp[ukc[u0] + 1] - p;
     FT ljk = lval[p];
     int off = lane < cnt ? rel[r0 + lane] : 0;
     FT src = lane < cnt ? lval[p + lane] : FT(0);
+    bool m1 = u0 + 1 < u1;
+    int k1 = 0, p1 = 0, r1 = 0;
+    if (m1) {
+      k1 = ukc[u0 + 1];
+      p1 = ukpos[u0 + 1];
+      r1 = ukrel[u0 + 1];
+      m1 = k1 < klim;
+    }
     for (int u = u0;; ++u) {
-      const bool more = u + 1 < u1 && ukc[u + 1] < klim;
-      int np = 0, nr0 = 0, ncnt = 0, noff = 0;
+      int ncnt = 0, noff = 0;
       FT nl = 0, nsrc = 0;
-      if (more) {
-        const int nk = ukc[u + 1];
-        np = ukpos[u + 1];
-        nr0 = ukrel[u + 1];
-        ncnt = colp[nk + 1] - np;
-        nl = lval[np];
+      if (m1) {
+        ncnt = colp[k1 + 1] - p1;
+        nl = lval[p1];
         if (lane < ncnt) {
-          noff = rel[nr0 + lane];
-          nsrc = lval[np + lane];
+          noff = rel[r1 + lane];
+          nsrc = lval[p1 + lane];
         }
+      }
+      bool m2 = m1 && u + 2 < u1;
+      int k2 = 0, p2 = 0, r2 = 0;
+      if (m2) {
+        k2 = ukc[u + 2];
+        p2 = ukpos[u + 2];
+        r2 = ukrel[u + 2];
+        m2 = k2 < klim;
       }
       if (lane < cnt) lval[cj + off] -= src * ljk;
       for (int t = lane + 32; t < cnt; t += 32) lval[cj + rel[r0 + t]] -= lval[p + t] * ljk;
       __syncwarp();
-      if (!more) break;
-      p = np;
-      r0 = nr0;
+      if (!m1) break;
+      p = p1;
+      r0 = r1;
       cnt = ncnt;
       ljk = nl;
       off = noff;
       src = nsrc;
+      m1 = m2;
+      k1 = k2;
+      p1 = p2;
+      r1 = r2;
     }
   }
   __device__ uint32_t factor_column(int j, int lane) const {
