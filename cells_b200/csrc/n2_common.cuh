@@ -272,14 +272,36 @@ struct WorldCholesky {
       if (a1 - a0 == 1) {
         const int end = single_run_end(lv);
         if (warp == 0) {
+          // A chain of columns, each after the last: the next column's term indices, factor
+          // entries and pivot are read while this one's dot product completes.
+          int j = lvc[lvp[lv]], ue = ukp[j + 1], u0 = ukp[j] + lane;
+          int col = u0 < ue ? ukc[u0] : 0;
+          FT val = u0 < ue ? lval[ukpos[u0]] : FT(0), piv = lval[colp[j]];
           for (int l = lv; l < end; ++l) {
-            const int j = lvc[lvp[l]];
+            int jn = 0, uen = 0, u0n = 0, coln = 0;
+            FT valn = 0, pivn = 0;
+            if (l + 1 < end) {
+              jn = lvc[lvp[l + 1]];
+              uen = ukp[jn + 1];
+              u0n = ukp[jn] + lane;
+              if (u0n < uen) {
+                coln = ukc[u0n];
+                valn = lval[ukpos[u0n]];
+              }
+              pivn = lval[colp[jn]];
+            }
             FT part = 0;
-            for (int u = ukp[j] + lane; u < ukp[j + 1]; u += 32)
-              part += lval[ukpos[u]] * Yv[ukc[u]];
+            if (u0 < ue) part += val * Yv[col];
+            for (int u = u0 + 32; u < ue; u += 32) part += lval[ukpos[u]] * Yv[ukc[u]];
             part = warp_sum(part);
-            if (lane == 0) Yv[j] = (Yv[j] - part) / lval[colp[j]];
+            if (lane == 0) Yv[j] = (Yv[j] - part) / piv;
             __syncwarp();
+            j = jn;
+            ue = uen;
+            u0 = u0n;
+            col = coln;
+            val = valn;
+            piv = pivn;
           }
         }
         lv = end;
@@ -310,14 +332,35 @@ struct WorldCholesky {
         int begin = lv;  // the run of one-column levels ending at lv
         while (begin > lv0 && lvp[begin] - lvp[begin - 1] == 1) --begin;
         if (warp == 0) {
+          // The chain backwards, the next column's rows, entries and pivot read ahead.
+          int j = lvc[lvp[lv]], cj = colp[j], len = colp[j + 1] - cj;
+          int row = 1 + lane < len ? lrow[cj + 1 + lane] : 0;
+          FT val = 1 + lane < len ? lval[cj + 1 + lane] : FT(0), piv = lval[cj];
           for (int l = lv; l >= begin; --l) {
-            const int j = lvc[lvp[l]];
-            const int cj = colp[j], len = colp[j + 1] - cj;
+            int jn = 0, cjn = 0, lenn = 0, rown = 0;
+            FT valn = 0, pivn = 0;
+            if (l - 1 >= begin) {
+              jn = lvc[lvp[l - 1]];
+              cjn = colp[jn];
+              lenn = colp[jn + 1] - cjn;
+              if (1 + lane < lenn) {
+                rown = lrow[cjn + 1 + lane];
+                valn = lval[cjn + 1 + lane];
+              }
+              pivn = lval[cjn];
+            }
             FT part = 0;
-            for (int t = 1 + lane; t < len; t += 32) part += lval[cj + t] * Xv[lrow[cj + t]];
+            if (1 + lane < len) part += val * Xv[row];
+            for (int t = 33 + lane; t < len; t += 32) part += lval[cj + t] * Xv[lrow[cj + t]];
             part = warp_sum(part);
-            if (lane == 0) Xv[j] = (Yv[j] - part) / lval[cj];
+            if (lane == 0) Xv[j] = (Yv[j] - part) / piv;
             __syncwarp();
+            j = jn;
+            cj = cjn;
+            len = lenn;
+            row = rown;
+            val = valn;
+            piv = pivn;
           }
         }
         lv = begin - 1;
