@@ -98,6 +98,9 @@ def parse():
     ap.add_argument("--method", choices=("ars222", "n2", "ros2"), default="ars222",
                     help="n2: slope conductances implicit, a sparse Cholesky per world per step; "
                          "ros2: the two-stage Rosenbrock method on the same operator")
+    ap.add_argument("--precision-steps", type=int, default=500,
+                    help="field: steps after which the precision sub-record compares each mixed "
+                         "form's state with its FP64 step's")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the bind's launch configuration instead of the autotuner's")
     ap.add_argument("--no-graph", action="store_true",
@@ -796,6 +799,76 @@ def run_field(args, rank, world_size, local_rank, dist, base):
     return line if rank == 0 else None
 
 
+def run_precision(args, rank, world_size, local_rank, dist, base):
+    """The precision forms against their FP64 steps on the 4096-world 16x16 grid batch: per pair
+    (ROS2 and its FP32-factor form; ARS(2,2,2) and its FP32-flux form), ms per step of each (CUDA
+    events over fused launches after warm-up), the mixed/plain speed ratio, and each state field's
+    scaled difference max |mixed - plain| / max |plain| after a run from the same start."""
+    import torch
+
+    from cells_b200 import _lib as L
+    from cells_b200.tissue import Tissue
+
+    del base
+    dev = torch.device("cuda", local_rank)
+    batch = build_batch(args, rank)
+    tissue = Tissue(batch, device=local_rank)
+    state0 = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    control = torch.from_numpy(tissue.pack_control()).to(dev)
+    status = torch.zeros(batch.worlds, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(method, steps):
+        out = torch.empty_like(state0)
+        tissue.step(state0, out, control, args.dt, 5, status, method=method)  # warm-up
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        tissue.step(state0, out, control, args.dt, steps, status, method=method)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / steps
+
+    def final(method, steps):
+        out = torch.zeros_like(state0)
+        tissue.step(state0, out, control, args.dt, steps, status, method=method)
+        torch.cuda.synchronize(dev)
+        refused = int((status != 0).sum().item())
+        return tissue.unpack_state(out.cpu().numpy()), refused
+
+    pairs = {"ros2": (L.METHOD_ROS2, L.METHOD_ROS2_MIXED, METHOD_ROS2, METHOD_ROS2_MIXED, 20),
+             "ars222": (L.METHOD_ARS222, L.METHOD_ARS222_MIXED, METHOD, METHOD_MIXED, 100)}
+    out = {}
+    for name, (plain, mixed, plain_id, mixed_id, steps) in pairs.items():
+        ms_p, ms_m = timed(plain, steps), timed(mixed, steps)
+        run = args.precision_steps
+        ref, refused_p = final(plain, run)
+        got, refused_m = final(mixed, run)
+        errors = {}
+        for f, r in ref.items():
+            r, g = np.asarray(r), np.asarray(got[f])
+            scale = float(np.max(np.abs(r), initial=0.0))
+            if scale > 0.0:
+                errors[f] = float(np.max(np.abs(g - r)) / scale)
+        out[name] = {
+            "plain": {"method": plain_id, "ms_per_step": ms_p,
+                      "value": batch.cells * world_size / (ms_p * 1e-3)},
+            "mixed": {"method": mixed_id, "ms_per_step": ms_m,
+                      "value": batch.cells * world_size / (ms_m * 1e-3)},
+            "mixed_over_plain": ms_p / ms_m,
+            "max_scaled_error": max(errors.values()),
+            "scaled_error_per_field": errors,
+            "error_after_steps": run,
+            "refused_worlds": {"plain": refused_p, "mixed": refused_m},
+        }
+    tissue.close()
+    if rank != 0:
+        return None
+    return {"metric": METRIC, "unit": UNIT, "dtype": "f64 vs mixed",
+            "config": {"workload": workload_name(args), "worlds_per_gpu": args.worlds,
+                       "cells_per_gpu": batch.cells},
+            "pairs": out}
+
+
 def run_grid(args, rank, world_size, local_rank, dist, base):
     """The held-bath workloads (grid, uneven): each bench step is one time step of every world,
     the timed launches replayed from one CUDA graph."""
@@ -1023,13 +1096,16 @@ def main():
                          ("grid_ros2", dict(workload="grid", worlds=4096, side=16, dt=1e-3,
                                             steps=20, warmup=5, e2e_calls=0, fuse=10,
                                             method="ros2")),
+                         ("precision", dict(workload="grid", worlds=4096, side=16, dt=1e-3,
+                                            steps=20, warmup=5, e2e_calls=0)),
                          ("adjoint", dict(workload="adjoint", worlds=512, dt=1e-3, steps=1,
                                           warmup=1, e2e_calls=0, method="ros2")),
                          ("adjoint_ars222", dict(workload="adjoint", worlds=512, dt=1e-3,
                                                  steps=1, warmup=1, e2e_calls=0,
                                                  method="ars222"))):
             sub = argparse.Namespace(**{**vars(args), **kw})
-            fn = run_adjoint if name.startswith("adjoint") else run_grid
+            fn = (run_adjoint if name.startswith("adjoint") else
+                  run_precision if name == "precision" else run_grid)
             subs[name] = fn(sub, rank, world_size, local_rank, dist, None)
         if line is not None:
             line["sub_records"] = {k: sub_record(v) for k, v in subs.items()}
@@ -1044,7 +1120,7 @@ def main():
 def sub_record(line):
     """The keys of a workload's line that a sub-record keeps."""
     keep = ("metric", "value", "unit", "ms_per_step", "dtype", "config", "roofline", "e2e",
-            "gpu_launches", "refused_worlds", "clocks", "kernels")
+            "gpu_launches", "refused_worlds", "clocks", "kernels", "pairs")
     return {k: line[k] for k in keep if k in line}
 
 
