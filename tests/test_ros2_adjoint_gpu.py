@@ -204,3 +204,37 @@ def test_ros2_refused_world_and_ledger_cotangent(cuda):
     assert np.array_equal(got["amount_increment"][:, :9], cot_n[:, :9])
     assert not gm[:, :9].any() and gm[:, 9:].any()
     assert np.array_equal(got["pump_cycles"], pump)  # ledger cotangents pass through
+
+
+def test_ros2_vjp_arguments(cuda):
+    """The reverse refuses an undersized workspace and a method it does not cover (the
+    FP32-factor form), with an error and no launch; zero steps pass the cotangent through and add
+    nothing to the gradients."""
+    torch = cuda
+    b = worlds.pack([worlds.grid_world(3, 3, worlds.world_rng(9, 0))])
+    tissue = Tissue(b)
+    dev = torch.device("cuda", tissue.device)
+    state = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    control = torch.from_numpy(tissue.pack_control()).to(dev)
+    rng = np.random.default_rng(3)
+    cot = {f: np.zeros_like(v) for f, v in tissue.initial_state().items()}
+    cot["amount_increment"] = rng.normal(size=(3, b.cells))
+    cot_out = torch.from_numpy(tissue.pack_state(cot)).to(dev)
+    cot_in = torch.zeros_like(cot_out)
+    gm = torch.zeros(3 * b.cells, dtype=torch.float64, device=dev)
+    gj = torch.zeros(3 * b.edges, dtype=torch.float64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    need = tissue.vjp_workspace_bytes(4, ROS2)
+    small = torch.empty(need - 256, dtype=torch.uint8, device=dev)
+    with pytest.raises(RuntimeError, match="workspace too small"):
+        tissue.step_vjp(state, control, 1e-3, 4, cot_out, cot_in, gm, gj, None, small, status,
+                        method=ROS2)
+    ws = torch.empty(need, dtype=torch.uint8, device=dev)
+    with pytest.raises(RuntimeError, match="the reverse covers"):
+        tissue.step_vjp(state, control, 1e-3, 4, cot_out, cot_in, gm, gj, None, ws, status,
+                        method=_lib.METHOD_ROS2_MIXED)
+    tissue.step_vjp(state, control, 1e-3, 0, cot_out, cot_in, gm, gj, None, ws, status,
+                    method=ROS2)
+    torch.cuda.synchronize(dev)
+    assert torch.equal(cot_in, cot_out)
+    assert not gm.any() and not gj.any() and int(status.item()) == 0
