@@ -799,6 +799,73 @@ def run_field(args, rank, world_size, local_rank, dist, base):
     return line if rank == 0 else None
 
 
+def load_reference_pytrees(name):
+    """The reference's own padded pytrees (layout, control, the first state) from a committed
+    golden fixture, as NamedTuples with the reference's field names."""
+    from collections import namedtuple
+
+    z = np.load(os.path.join(ROOT, "tests", "golden", name))
+    lf = [k[len("layout_"):] for k in z.files if k.startswith("layout_")]
+    cf = [k[len("control_ref_"):] for k in z.files if k.startswith("control_ref_")]
+    sf = [str(f) for f in z["state_fields"]]
+    p = namedtuple("ReferenceLayout", lf)(*(z["layout_" + f] for f in lf))
+    control = namedtuple("ReferenceControl", cf)(*(z["control_ref_" + f] for f in cf))
+    state = namedtuple("ReferenceState", sf)(*(z["refstate_" + f][0] for f in sf))
+    return z, p, control, state
+
+
+def run_dropin(args, rank, world_size, local_rank, dist, base):
+    """The drop-in boundary timed as a caller of the reference's model protocol uses it:
+    cells_b200.model.DeviceStep(p)(state, dt, control, p, active) on the reference's own padded
+    @3 pytrees (one world with channel populations, from a committed fixture), one step per call
+    with host pytrees in and out; its CPU baseline the oracle's step of the same world (the
+    reference's step restated), one host core."""
+    del base, world_size, dist
+    if rank != 0:
+        return None
+    from cells_b200 import model
+    from oracle import tissue as T
+
+    z, p, control, state = load_reference_pytrees("pytrees_v3_channels_padded.npz")
+    dt = float(z["dt"])
+    step = model.DeviceStep(p, device=local_rank)
+    cells = int(step.batch.cells)
+    st = state
+    for _ in range(5):
+        st, _ = step(st, dt, control, p, p.active)
+    calls = args.steps
+    t0 = time.perf_counter()
+    st = state
+    for _ in range(calls):
+        st, valid = step(st, dt, control, p, p.active)
+    wall = time.perf_counter() - t0
+    b = step.batch
+    topo = T.topology(b)
+    ost = T.initial_state(b)
+    octl = T.full_control(b)
+    t1 = time.perf_counter()
+    n_cpu = max(1, min(calls, 50))
+    for _ in range(n_cpu):
+        ost, _ = T.ars222_step(ost, dt, octl, b, topo)
+    cpu = (time.perf_counter() - t1) / n_cpu
+    step.close()
+    per_call = wall / calls
+    return {
+        "metric": METRIC, "value": cells / per_call, "unit": UNIT,
+        "ms_per_step": 1e3 * per_call, "dtype": "f64",
+        "config": {"workload": "drop-in: model.DeviceStep on the reference's own padded @3 "
+                               f"pytrees ({cells} active cells, NaV1.2 + Kv1.5 populations), one "
+                               "step per call, host pytrees in and out",
+                   "calls": calls, "valid": bool(valid)},
+        "cpu_baseline": {"value": cells / cpu, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"the oracle's ARS(2,2,2) step of the same world, {n_cpu} "
+                                   "steps on one host core"},
+        "note": ("each call maps the padded pytrees to the packed layout, copies them to the "
+                 "device, steps once and copies back: call latency, not throughput; batches of "
+                 "worlds go through Tissue or vector_window"),
+    }
+
+
 def run_precision(args, rank, world_size, local_rank, dist, base):
     """The precision forms against their FP64 steps on the 4096-world 16x16 grid batch: per pair
     (ROS2 and its FP32-factor form; ARS(2,2,2) and its FP32-flux form), ms per step of each (CUDA
@@ -1098,6 +1165,7 @@ def main():
                                             method="ros2")),
                          ("precision", dict(workload="grid", worlds=4096, side=16, dt=1e-3,
                                             steps=20, warmup=5, e2e_calls=0)),
+                         ("drop_in", dict(workload="grid", steps=200)),
                          ("adjoint", dict(workload="adjoint", worlds=512, dt=1e-3, steps=1,
                                           warmup=1, e2e_calls=0, method="ros2")),
                          ("adjoint_ars222", dict(workload="adjoint", worlds=512, dt=1e-3,
@@ -1105,7 +1173,8 @@ def main():
                                                  method="ars222"))):
             sub = argparse.Namespace(**{**vars(args), **kw})
             fn = (run_adjoint if name.startswith("adjoint") else
-                  run_precision if name == "precision" else run_grid)
+                  run_precision if name == "precision" else
+                  run_dropin if name == "drop_in" else run_grid)
             subs[name] = fn(sub, rank, world_size, local_rank, dist, None)
         if line is not None:
             line["sub_records"] = {k: sub_record(v) for k, v in subs.items()}
@@ -1120,7 +1189,8 @@ def main():
 def sub_record(line):
     """The keys of a workload's line that a sub-record keeps."""
     keep = ("metric", "value", "unit", "ms_per_step", "dtype", "config", "roofline", "e2e",
-            "gpu_launches", "refused_worlds", "clocks", "kernels", "pairs")
+            "gpu_launches", "refused_worlds", "clocks", "kernels", "pairs", "cpu_baseline",
+            "note")
     return {k: line[k] for k in keep if k in line}
 
 
