@@ -238,3 +238,28 @@ def test_ros2_vjp_arguments(cuda):
     torch.cuda.synchronize(dev)
     assert torch.equal(cot_in, cot_out)
     assert not gm.any() and not gj.any() and int(status.item()) == 0
+
+
+def test_ros2_vjp_on_a_benchmark_world(cuda):
+    """One world of the adjoint benchmark (a 1024-cell Delaunay tissue with NaV1.2 and HH K
+    populations, the config-4 generator): its factor plan does not fit shared memory, so the
+    forward runs the four-CTAs-per-SM shape from global memory. 10 ROS2 steps: the device's
+    reverse against the oracle's at 1e-9 on the cotangents and gradients."""
+    b = worlds.pack([worlds.uneven_world(0, 1024, 4, worlds.UNEVEN_CHANNELS)])
+    tissue = Tissue(b)
+    rng = np.random.default_rng(8)
+    cot = (rng.normal(size=(3, b.cells)), rng.normal(size=b.edges),
+           rng.normal(size=(2, b.channel_slots, b.cells)))
+    dt, n = 1e-3, 10
+    got, gm, gj, gch, status = device_vjp(cuda, tissue, tissue.pack_control(), dt, n, {
+        "amount_increment": cot[0], "junction_gate": cot[1], "channel_gate": cot[2]})
+    assert np.all(status == 0)
+    (lam_n, lam_g, lam_c), ref = oracle_vjp(b, T.full_control(b), dt, n, cot)
+    bad = {name: d for name, a, r in (("amount", got["amount_increment"], lam_n),
+                                       ("junction_gate", got["junction_gate"], lam_g),
+                                       ("channel_gate", got["channel_gate"], lam_c),
+                                       ("grad_membrane", gm, ref.membrane),
+                                       ("grad_junction", gj, ref.junction),
+                                       ("grad_channel", gch, ref.channel))
+           if (d := scaled_difference(a, r)) > VJP_TOL}
+    assert not bad, bad
