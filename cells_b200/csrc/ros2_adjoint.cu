@@ -418,7 +418,8 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       EF(AJ_KB1, ge) = (1.5 * h) * yb - 2.0 * rb;
       double uj = 0.0;
       for (int s = 0; s < 3; ++s) {
-        const double phi = gh * ((0.5 * h) * cot[oN + s * C + gb] - (0.5 * h) * cot[oN + s * C + ga]);
+        const double phi =
+            gh * ((0.5 * h) * cot[oN + s * C + gb] - (0.5 * h) * cot[oN + s * C + ga]);
         EF(AJ_JW + s, ge) += phi * du;
         uj += phi * EF(AJ_W + s, ge);
       }
@@ -490,8 +491,9 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       }
       gather_terms(gi, lc, lv);
       const double V1 = CF(AR_V1, gi);
-      cell_terms<NCH, false, true>(T, A, sW, gi, c, V1, cs + (long long)(AR_CH + AH_GC1 * NQ) * C + gi,
-                                   NQ * C, mc, pctl, ldc, chctl0 + gi, mu, lc, lv, lgc, own);
+      const double *gc1 = cs + (long long)(AR_CH + AH_GC1 * NQ) * C + gi;
+      cell_terms<NCH, false, true>(T, A, sW, gi, c, V1, gc1, NQ * C, mc, pctl, ldc, chctl0 + gi,
+                                   mu, lc, lv, lgc, own);
       for (int q = 0; q < NCH; ++q) {
         const int code = __ldg(T.ch_code + q * C + gi);
         const GateCurve gk = gate_curve(code, V1 - Vb);
@@ -765,7 +767,8 @@ int ros2_vjp(cb_tissue *t, const double *state_in, double dt, const double *cont
     return fail(CB_ERR_UNSUPPORTED, "the adjoint step has no open-channel block");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(CB_ERR_ARGUMENT, "dt must be positive");
   if (n_steps < 0) return fail(CB_ERR_ARGUMENT, "n_steps must be non-negative");
-  if (t->t.nch != 0 && t->t.nch != 2) return fail(CB_ERR_UNSUPPORTED, "channel slots must be 0 or 2");
+  if (t->t.nch != 0 && t->t.nch != 2)
+    return fail(CB_ERR_UNSUPPORTED, "channel slots must be 0 or 2");
   cudaError_t ce = cudaSetDevice(t->device);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
   int rc = n2_build_plan(t);

@@ -16,10 +16,10 @@ outside nodes and faces (src/cells/models/surface_pump.py:124-369):
   nested-dissection plan, stepped in turn; states and controls per world.
 
 Every world of a FieldTissue shares one topology (grid, cells' nodes, junction graph);
-parameters are per world. State is a dict of NumPy arrays [W, ...] per field (``_lib.FIELD_STATE_FIELDS``; cell
-fields [W, 3, N] or [W, N], node fields [W, 3, O] or [W, O], junction fields [W, 3, E] or [W, E],
-face fields [W, 3, F] or [W, F]); on the device it is one packed float64 buffer, species-major
-([3][W*X]) within a field.
+parameters are per world. State is a dict of NumPy arrays [W, ...] per field
+(``_lib.FIELD_STATE_FIELDS``; cell fields [W, 3, N] or [W, N], node fields [W, 3, O] or [W, O],
+junction fields [W, 3, E] or [W, E], face fields [W, 3, F] or [W, F]); on the device it is one
+packed float64 buffer, species-major ([3][W*X]) within a field.
 """
 
 from __future__ import annotations

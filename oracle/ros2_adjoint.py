@@ -62,7 +62,8 @@ CURVATURE_SERIES_BELOW = 0.1
 def curvature(x):
     """B''(x) for B(x) = x / expm1(x). B'' is even (B(-x) = B(x) + x); with a = |x|,
     om = -expm1(-a) = 1 - e^-a:  B'' = (1 - om)(a (2 - om) - 2 om) / om^3. Below a < 0.1 the
-    series 1/6 - x^2/60 + x^4/1008 - x^6/21600 + x^8/532224 (from the Bernoulli numbers B_2..B_10)."""
+    series 1/6 - x^2/60 + x^4/1008 - x^6/21600 + x^8/532224 (from the Bernoulli numbers
+    B_2 .. B_10)."""
     x = np.asarray(x, dtype=float)
     a = np.abs(x)
     small = a < CURVATURE_SERIES_BELOW

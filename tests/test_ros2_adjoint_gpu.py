@@ -242,8 +242,8 @@ def test_ros2_vjp_arguments(cuda):
 
 def test_ros2_vjp_on_a_benchmark_world(cuda):
     """One world of the adjoint benchmark (a 1024-cell Delaunay tissue with NaV1.2 and HH K
-    populations, the config-4 generator): its factor plan does not fit shared memory, so the
-    forward runs the four-CTAs-per-SM shape from global memory. 10 ROS2 steps: the device's
+    populations, from the benchmark's generator): its factor plan does not fit shared memory, so
+    the forward runs the four-CTAs-per-SM shape from global memory. 10 ROS2 steps: the device's
     reverse against the oracle's at 1e-9 on the cotangents and gradients."""
     b = worlds.pack([worlds.uneven_world(0, 1024, 4, worlds.UNEVEN_CHANNELS)])
     tissue = Tissue(b)

@@ -72,7 +72,7 @@ def test_ros2_matches_the_oracle_on_uneven_worlds(cuda):
     assert not bad, bad
 
 
-def test_ros2_config0_world_for_10000_steps(cuda):
+def test_ros2_4x4_world_for_10000_steps(cuda):
     """The single 4x4 CPU world (seed 0) by ROS2 at dt = 1 ms for 10,000 steps, against the oracle
     at steps 1, 100, 1000 and 10000."""
     b = worlds.pack([worlds.single_grid_tissue(0)])
