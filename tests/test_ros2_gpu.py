@@ -74,15 +74,23 @@ def test_ros2_matches_the_oracle_on_uneven_worlds(cuda):
 
 def test_ros2_4x4_world_for_10000_steps(cuda):
     """The single 4x4 CPU world (seed 0) by ROS2 at dt = 1 ms for 10,000 steps, against the oracle
-    at steps 1, 100, 1000 and 10000."""
+    at steps 1, 100, 1000 and 10000 (1e-10); the FP32-factor form beside it, against the same
+    FP64 oracle states at 1e-8 from step 100: its factor's rounding does not accumulate over the
+    run. (After one step the junction transfers are a single step's flux between near-equal
+    cells, the difference of nearly equal voltage rates; there the FP32 factor shows at 2.3e-8 of
+    that field's own small scale.)"""
     b = worlds.pack([worlds.single_grid_tissue(0)])
     tissue = Tissue(b)
     control = tissue.pack_control()
     topo = T.topology(b)
     st = T.initial_state(b)
     state, done = tissue.initial_state(), 0
+    mixed = tissue.initial_state()
     for target in (1, 100, 1000, 10000):
         state, status, taken = run(cuda, tissue, state, control, 1e-3, [target - done])
+        assert status[0] == 0 and taken[0] == target - done
+        mixed, status, taken = run(cuda, tissue, mixed, control, 1e-3, [target - done],
+                                   method=_lib.METHOD_ROS2_MIXED)
         assert status[0] == 0 and taken[0] == target - done
         for _ in range(target - done):
             st, ok = RO.ros2_step(st, 1e-3, T.full_control(b), b, topo)
@@ -91,6 +99,9 @@ def test_ros2_4x4_world_for_10000_steps(cuda):
         bad = {f: d for f, r in oracle_state(st).items()
                if (d := scaled_difference(state[f], r)) > TOL}
         assert not bad, (target, bad)
+        bad = {f: d for f, r in oracle_state(st).items()
+               if (d := scaled_difference(mixed[f], r)) > (1e-8 if target >= 100 else 1e-7)}
+        assert not bad, ("fp32 factor", target, bad)
 
 
 def test_ros2_fused_equals_one_step_launches_and_conserves(cuda):
