@@ -868,9 +868,10 @@ def run_dropin(args, rank, world_size, local_rank, dist, base):
 
 def run_precision(args, rank, world_size, local_rank, dist, base):
     """The precision forms against their FP64 steps on the 4096-world 16x16 grid batch: per pair
-    (ROS2 and its FP32-factor form; ARS(2,2,2) and its FP32-flux form), ms per step of each (CUDA
-    events over fused launches after warm-up), the mixed/plain speed ratio, and each state field's
-    scaled difference max |mixed - plain| / max |plain| after a run from the same start."""
+    (ROS2 and its FP32-factor form; N2 and its FP32 factor with FP64 refinement; ARS(2,2,2) and
+    its FP32-flux form), ms per step of each (CUDA events over fused launches after warm-up), the
+    mixed/plain speed ratio, and each state field's scaled difference max |mixed - plain| /
+    max |plain| after a run from the same start."""
     import torch
 
     from cells_b200 import _lib as L
@@ -903,6 +904,7 @@ def run_precision(args, rank, world_size, local_rank, dist, base):
         return tissue.unpack_state(out.cpu().numpy()), refused
 
     pairs = {"ros2": (L.METHOD_ROS2, L.METHOD_ROS2_MIXED, METHOD_ROS2, METHOD_ROS2_MIXED, 20),
+             "n2": (L.METHOD_N2, L.METHOD_N2_MIXED, METHOD_N2, METHOD_N2_MIXED, 20),
              "ars222": (L.METHOD_ARS222, L.METHOD_ARS222_MIXED, METHOD, METHOD_MIXED, 100)}
     out = {}
     for name, (plain, mixed, plain_id, mixed_id, steps) in pairs.items():
