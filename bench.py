@@ -979,6 +979,13 @@ def run_grid(args, rank, world_size, local_rank, dist, base):
                                       steps=min(20, fuse), repeats=2, method=method)
         tuned = {"selected": list(best),
                  "ms_per_step": {f"{k[0]}/{k[1]}/{k[2]}": round(v, 5) for k, v in timings.items()}}
+    elif not args.no_autotune and args.method == "ros2":
+        from cells_b200 import autotune
+
+        best, timings = autotune.tune_sparse(tissue, state, control, args.dt, steps=3, repeats=2,
+                                             method=method)
+        tuned = {"selected": {"block": best},
+                 "ms_per_step": {str(k): round(v, 5) for k, v in timings.items()}}
     left = max(args.warmup, 1)
     while left > 0:  # warm-up steps, in launches of at most `fuse` steps
         tissue.step(state, state, control, args.dt, min(fuse, left), status, stream=handle,
@@ -1080,7 +1087,8 @@ def run_grid(args, rank, world_size, local_rank, dist, base):
                            if args.method == "n2" else
                            METHOD if args.precision == "fp64" else METHOD_MIXED),
                 "worlds_per_gpu": args.worlds, "steps_per_launch": fuse,
-                "launch": ({"kernel": f"{args.method} (one world per CTA)", "block": 256}
+                "launch": ({"kernel": f"{args.method} (one world per CTA)",
+                            "block": tissue.get_sparse_launch() if args.method == "ros2" else 256}
                            if args.method in ("n2", "ros2") else
                            dict(zip(("kernel", "block", "occupancy"), tissue.get_launch()))),
                 "autotune": tuned, "cuda_graph": graph is not None,

@@ -76,6 +76,8 @@ EXPORTS = (
     "cb_vjp_workspace",
     "cb_step_vjp_method",
     "cb_vjp_workspace_method",
+    "cb_set_sparse_launch",
+    "cb_get_sparse_launch",
     "cb_set_permeability",
     "cb_set_channel_block",
     "cb_device_checks",
@@ -231,6 +233,10 @@ def load(path=LIBRARY):
     lib.cb_vjp_workspace_method.argtypes = [_p, ctypes.c_int, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_size_t)]
     lib.cb_vjp_workspace_method.restype = ctypes.c_int
+    lib.cb_set_sparse_launch.argtypes = [_p, ctypes.c_int]
+    lib.cb_set_sparse_launch.restype = ctypes.c_int
+    lib.cb_get_sparse_launch.argtypes = [_p, ctypes.POINTER(ctypes.c_int)]
+    lib.cb_get_sparse_launch.restype = ctypes.c_int
     lib.cb_set_permeability.argtypes = [_p, _p, _p, _p, _p]
     lib.cb_set_permeability.restype = ctypes.c_int
     lib.cb_set_channel_block.argtypes = [_p, ctypes.c_int32, _d, _d, _d, _d]

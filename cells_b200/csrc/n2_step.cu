@@ -1897,6 +1897,38 @@ int n2_step(cb_tissue *t, const double *state_in, double *state_out, double dt,
 
 int n2_build_plan(cb_tissue *t) { return build_plan(t); }
 
+}  // namespace cbk
+
+extern "C" {
+
+int cb_set_sparse_launch(cb_tissue *t, int block) {
+  if (!t) return fail(CB_ERR_ARGUMENT, "null argument");
+  if (block != 0 && block != 128 && block != 256)
+    return fail(CB_ERR_ARGUMENT, "the sparse kernels' block is 128 or 256 (0: the plan's choice)");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  const int rc = build_plan(t);
+  if (rc) return rc;
+  N2Plan *p = t->n2;
+  p->ros2_block = block ? block : (p->smem_bytes == 0 ? 128 : 256);
+  p->ros2_block_f32 = block ? block : (p->smem_f32 == 0 ? 128 : 256);
+  return CB_OK;
+}
+
+int cb_get_sparse_launch(cb_tissue *t, int *block) {
+  if (!t || !block) return fail(CB_ERR_ARGUMENT, "null argument");
+  cudaError_t ce = cudaSetDevice(t->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
+  const int rc = build_plan(t);
+  if (rc) return rc;
+  *block = t->n2->ros2_block;
+  return CB_OK;
+}
+
+}  // extern "C"
+
+namespace cbk {
+
 void n2_release(cb_tissue *t) {
   if (!t->n2) return;
   for (void *ptr : t->n2->owned) cudaFree(ptr);

@@ -205,6 +205,16 @@ class Tissue:
                                           ctypes.byref(o)))
         return k.value, b.value, o.value
 
+    def set_sparse_launch(self, block):
+        """cb_set_sparse_launch: the ROS2/RK4 kernel's CTA threads (128 or 256; 0: the plan's
+        own choice)."""
+        _lib.check(self.lib.cb_set_sparse_launch(self.handle, int(block)))
+
+    def get_sparse_launch(self):
+        out = ctypes.c_int()
+        _lib.check(self.lib.cb_get_sparse_launch(self.handle, ctypes.byref(out)))
+        return out.value
+
     def capture(self, state_in, state_out, control, dt, n_steps, status, launches=1,
                 accepted=None, method=_lib.METHOD_ARS222):
         """A CUDA graph of ``launches`` cb_step launches of ``n_steps`` steps each (device

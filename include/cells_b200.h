@@ -214,6 +214,15 @@ void cb_free(cb_tissue *t);
 int cb_set_launch(cb_tissue *t, int kernel, int block, int occupancy);
 int cb_get_launch(const cb_tissue *t, int *kernel, int *block, int *occupancy);
 
+/* CTA threads of the ROS2 and RK4 kernel (CB_METHOD_ROS2, CB_METHOD_ROS2_MIXED, CB_METHOD_RK4) on
+ * the batch's sparse factor plan: 128 (four CTAs per SM) or 256 (two); 0 restores the plan's own
+ * choice (128 when no world's plan is staged in shared memory). The first call builds the plan
+ * (device memory the handle keeps, as the first step of these methods does): make it outside any
+ * stream capture. cb_get_sparse_launch reports the block in use (building the plan if needed).
+ * An autotuner's knob (cells_b200.autotune.tune_sparse); no counterpart in the reference. */
+int cb_set_sparse_launch(cb_tissue *t, int block);
+int cb_get_sparse_launch(cb_tissue *t, int *block);
+
 /* Offsets (in doubles) of each state field in a packed state buffer, and its total length. */
 int cb_state_layout(const cb_tissue *t, int64_t offsets[CB_STATE_FIELDS], int64_t *total);
 /* Offsets (in doubles) of each control field in a packed control buffer, and its total length. */

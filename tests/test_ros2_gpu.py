@@ -181,3 +181,36 @@ def test_fp32_factor_ros2_within_1e8_of_fp64_and_conserves(cuda):
     worst = out.view(-1, 8).max(dim=0).values.cpu().numpy()
     scale = float(np.max(np.abs(b.amount_reference)))
     assert worst[0] <= 1e-12 * scale and worst[2] <= 1e-12 * scale, worst
+
+
+def test_sparse_launch_setter_and_tuner(cuda):
+    """cb_set_sparse_launch / cb_get_sparse_launch and autotune.tune_sparse: both CTA shapes step
+    the same uneven worlds to within 1e-12 (the substitutions' narrow levels change form with
+    the warp count, so the last bits may differ); 0 restores the plan's choice; other blocks are
+    refused; the tuner times both and leaves the faster selected."""
+    from cells_b200 import autotune
+
+    b, rng = uneven_batch(64)
+    tissue = Tissue(b)
+    control = tissue.pack_control()
+    default = tissue.get_sparse_launch()
+    assert default in (128, 256)
+    outs = {}
+    for block in (128, 256):
+        tissue.set_sparse_launch(block)
+        assert tissue.get_sparse_launch() == block
+        got, status, _ = run(cuda, tissue, tissue.initial_state(), control, 1e-3, [20])
+        assert np.all(status == 0)
+        outs[block] = got
+    for f in outs[128]:
+        assert scaled_difference(outs[128][f], outs[256][f]) <= 1e-12, f
+    tissue.set_sparse_launch(0)
+    assert tissue.get_sparse_launch() == default
+    with pytest.raises(RuntimeError, match="128 or 256"):
+        tissue.set_sparse_launch(64)
+    dev = cuda.device("cuda", tissue.device)
+    state = cuda.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    ctl = cuda.from_numpy(control).to(dev)
+    best, timings = autotune.tune_sparse(tissue, state, ctl, 1e-3, steps=2, repeats=1, torch=cuda)
+    assert best in (128, 256) and set(timings) == {128, 256}
+    assert tissue.get_sparse_launch() == best
