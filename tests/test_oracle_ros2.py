@@ -175,3 +175,57 @@ def test_fp32_factor_form_is_second_order_against_rk4():
                       / float(np.max(np.abs(ref.amount_increment - start.amount_increment))))
     orders = [np.log2(errors[i] / errors[i + 1]) for i in range(2)]
     assert all(p >= 1.8 for p in orders), (errors, orders)
+
+
+def test_tf32_rounded_factor_misses_the_bar_but_conserves():
+    """Why the FP32-factor form stops at FP32: the same run with the factor rounded to TF32's
+    10-bit mantissa (the tensor cores' FP32-class input format) stays conservative (ledgers to
+    1e-12) and within 1e-6 of the FP64 step, but not within the 1e-8 bar (measured 1.0e-7 on the
+    junction heat, 2.3e-8 on the amounts after 300 steps)."""
+    import scipy.linalg as sl
+
+    from conftest import scaled_difference
+
+    def tf32(a):
+        a = np.asarray(a, dtype=np.float32).copy()
+        bits = a.view(np.int32)
+        bits[:] = (bits + np.int32(0x1000)) & np.int32(-8192)  # round to 10 mantissa bits
+        return a
+
+    def voltage_rate_tf32(self, rho, b):
+        u = np.zeros(b.cells)
+        for wi, (_, scale, factor, free, _) in enumerate(self.operator.worlds):
+            c0, c1 = b.cell_offset[wi], b.cell_offset[wi + 1]
+            rhs = np.where(free, np.r_[rho[c0:c1], 0.0] * scale, 0.0)
+            lower = tf32(factor)
+            y = sl.solve_triangular(lower, rhs.astype(np.float32), lower=True)
+            x = sl.solve_triangular(lower.T, y, lower=False).astype(np.float64)
+            u[c0:c1] = np.where(free, x * scale, 0.0)[:-1]
+        return u
+
+    rng = np.random.default_rng(9)
+    ws = [worlds.with_channels(worlds.delaunay_world(n, worlds.world_rng(26, k),
+                                                     junction_sigma=0.3, gate=(0.02, 0.2, 0.9)),
+                               rng, na=("nav", 1e-9, 0.5), k=("hh", 5e-10, 0.5), sigma=0.3)
+          for k, n in enumerate((60, 25))]
+    b = worlds.pack(ws)
+    topo = T.topology(b)
+    control = T.Control(rng.uniform(0.6, 1, b.cells), rng.uniform(0.6, 1, b.edges),
+                        rng.uniform(0.6, 1, b.cells), rng.uniform(0.4, 1, (2, b.cells)))
+    a = m = T.initial_state(b)
+    for _ in range(300):
+        a, _ = RO.ros2_step(a, 1e-3, control, b, topo)
+    saved = RO.Jacobian.voltage_rate
+    RO.Jacobian.voltage_rate = voltage_rate_tf32
+    try:
+        for _ in range(300):
+            m, ok = RO.ros2_step(m, 1e-3, control, b, topo)
+            assert np.all(ok)
+    finally:
+        RO.Jacobian.voltage_rate = saved
+    worst = max(scaled_difference(getattr(m, f), getattr(a, f)) for f in T.State._fields)
+    assert 1e-8 < worst < 1e-6, worst
+    bal = T.balances(m, b, topo)
+    material = np.abs(b.amount_reference).sum()
+    for name in ("local", "outside", "total"):
+        assert np.max(np.abs(bal[name])) <= 1e-12 * material, name
