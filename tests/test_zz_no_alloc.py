@@ -5,8 +5,9 @@ process whose device memory another allocator already holds).
 
 Checked through the C ABI against cb_step on the same handle, inputs and controls, twice in a
 row (the array keeps the first call's contents; the second call must not depend on them), with
-the parity tolerance of the other device tests (1e-10 scaled difference per field). This file
-is collected last and must pass alone in a fresh process as well as after the other tests.
+the parity tolerance of the other device tests (1e-10 scaled difference per field), and the same
+call captured into a CUDA graph and replayed twice. This file is collected last and must pass
+alone in a fresh process as well as after the other tests.
 """
 
 import ctypes
@@ -96,3 +97,62 @@ def test_static_scratch_refuses_a_batch_beyond_its_size(cuda, monkeypatch):
     assert "static scratch" in big.lib.cb_last_error().decode()
     big.close()
     del _lib
+
+
+def test_static_scratch_step_replays_from_a_cuda_graph(cuda, bound):
+    """The case the entry point exists for: the call captured into a CUDA graph (a memset of the
+    ticket counter and one launch, nothing allocated), replayed twice in a row with the state
+    carried between replays, matches cb_step over the same 80 steps."""
+    from cells_b200 import _lib
+
+    torch, tissue, lib = cuda, bound, bound.lib
+    dev = torch.device("cuda", tissue.device)
+    b = tissue.batch
+    rng = np.random.default_rng(8)
+    start = torch.from_numpy(tissue.pack_state(tissue.initial_state())).to(dev)
+    control = torch.from_numpy(tissue.pack_control(
+        rng.uniform(0.6, 1, b.cells), rng.uniform(0.6, 1, b.edges), rng.uniform(0.6, 1, b.cells),
+        rng.uniform(0.4, 1, (2, b.cells)))).to(dev)
+    graph_in = start.clone()
+    graph_out = torch.empty_like(start)
+    status = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
+    taken = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
+
+    def call(stream):
+        return lib.cb_step_packed_static(tissue.handle, _ptr(graph_in), _ptr(graph_out), 1e-3,
+                                         _ptr(control), 40, _ptr(status), _ptr(taken),
+                                         ctypes.c_void_p(stream.cuda_stream))
+
+    side = torch.cuda.Stream(dev)  # warm-up off the capture, so the kernel is loaded before it
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        _lib.check(call(side))
+    torch.cuda.current_stream(dev).wait_stream(side)
+    torch.cuda.synchronize(dev)
+
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        rc = call(torch.cuda.current_stream(dev))
+    _lib.check(rc)
+
+    reference = start.clone()
+    for replay in range(2):
+        ref_out = torch.empty_like(start)
+        ref_status = torch.zeros(b.worlds, dtype=torch.int32, device=dev)
+        _lib.check(lib.cb_step(tissue.handle, _lib.METHOD_ARS222, _ptr(reference), _ptr(ref_out),
+                               1e-3, _ptr(control), 40, _ptr(ref_status), None,
+                               ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+        graph_in.copy_(start if replay == 0 else graph_out)
+        status.fill_(99)
+        taken.zero_()
+        graph.replay()
+        torch.cuda.synchronize(dev)
+        assert int(ref_status.abs().max()) == 0
+        assert int(status.abs().max()) == 0, f"replay {replay}: a world was refused"
+        assert int(taken.min()) == 40
+        ref = tissue.unpack_state(ref_out.cpu().numpy())
+        got = tissue.unpack_state(graph_out.cpu().numpy())
+        for f in ref:
+            assert scaled_difference(got[f], ref[f]) <= TOL, (replay, f)
+        reference = ref_out
+    del graph
