@@ -1,7 +1,7 @@
 """CPU oracle of the resolved-field tissue step: cells facing finite extracellular nodes.
 
 TEST INFRASTRUCTURE ONLY, like oracle/tissue.py: only ``tests/`` and ``bench.py``'s CPU baseline
-leg may import it, as the checker or the timed CPU baseline.
+leg may import it, as the parity reference or the timed CPU baseline.
 
 Restates, for one world at a time with dense node-space algebra (small worlds), the reference's
 step of ``cells.model.resolved_pump_tissue@1`` under ``cells.solver.imex_ars222_face_

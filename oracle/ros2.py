@@ -2,7 +2,7 @@
 ``cells_b200.solver.ros2_verwer@1``; the reference has no Rosenbrock method on its tissue path).
 
 TEST INFRASTRUCTURE ONLY, like oracle/tissue.py: only ``tests/`` and ``bench.py``'s CPU baseline
-leg may import it, as the checker or the timed CPU baseline.
+leg may import it, as the parity reference or the timed CPU baseline.
 
 The method is the two-stage, second-order, L-stable Rosenbrock scheme of Verwer, Spee, Blom and
 Hundsdorfer (SIAM J. Sci. Comput. 20 (1999) 1456-1480), with gamma = 1 + 1/sqrt(2):

@@ -1,8 +1,9 @@
 """CPU oracle: a NumPy restatement of the reference's held-bath pump-leak tissue step.
 
 TEST INFRASTRUCTURE ONLY. Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU
-baseline leg may import this module, and only as the checker or the timed CPU baseline; the
-product path (``cells_b200``) never calls it and refuses to run without its CUDA library.
+baseline leg may import this module, and only as the parity reference or the timed CPU
+baseline; the product path (``cells_b200``) never calls it and refuses to run without its CUDA
+library.
 
 What it restates (citations are paths inside the reference project):
 

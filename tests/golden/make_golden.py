@@ -1,7 +1,8 @@
 """Generate the golden fixtures under tests/golden/ by running the REFERENCE's own step.
 
 Run in a container that holds the reference source tree (its project root, the directory with
-``src/cells``), never on the GPU box and never from the test suite:
+``src/cells``), by hand and never from the test suite (the committed fixtures are what the
+tests read; machines without the reference sources only read them):
 
     python tests/golden/make_golden.py --reference <reference project root>
     CELLS_REFERENCE=<reference project root> python tests/golden/make_golden.py
